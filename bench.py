@@ -1,0 +1,309 @@
+"""Benchmark: rigid body-steps/s of the Dynamis step on the 262,144-body mixed pile.
+
+One step = World::step over the whole world (broadphase, sort, pairs, narrowphase, islands,
+2 substeps of the contact solve, sleep), replayed as one CUDA graph. The workload is the seeded
+mixed pile (50% boxes, 30% spheres, 20% hulls, ground plane) advanced by --setup untimed steps so
+the timed steps run on a forming pile rather than on the free-falling lattice.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line. `value` is device-resident throughput (states stay in HBM); `e2e` is the
+same metric through the public C ABI with the body states uploaded from and downloaded to pinned
+host memory every step. The reference arm (--impl reference) times the CPU restatement of the
+step (the reference itself is Rust/WGSL on wgpu and cannot run on this machine).
+With N > 1 (torchrun) every rank steps its own replica of the world: the single-world step has no
+natural shard, so scaling is weak (replicas only) and there is no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "rigid body-steps/s at 256K bodies; batched-worlds & adjoint step/s vs plain"
+UNIT = "body-steps/s"
+DT = 1.0 / 60.0
+
+
+def peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                parts = [p.strip() for p in out.stdout.strip().split(",")]
+                if len(parts) == 6:
+                    self.samples.append(parts)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._thread.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def stage_bytes(stage: str, m: dict, params: dict) -> float:
+    """Algorithmic (compulsory) HBM bytes of one launch of a stage's kernel pair, from the counts
+    of the same step: K colliders, E entries, P pairs, C contacts, R solver rows, L live bodies."""
+    K, E, P, C, R_, L = m["K"], m["E"], m["P"], m["C"], m["R"], m["L"]
+    if stage == "velocity":     # one Jacobi iteration: solve over contacts + apply over rows
+        return 472.0 * C + 72.0 * R_
+    if stage == "position":     # one position iteration
+        return 200.0 * C + 64.0 * R_
+    if stage == "narrowphase":
+        return 596.0 * P
+    if stage == "aabb":
+        return 164.0 * K
+    if stage == "entries":
+        return 40.0 * E
+    if stage == "entry_sort":
+        return 16.0 * E * 4
+    if stage == "pair_sort":
+        return 16.0 * P * 2 * params["pair_words"]
+    if stage == "pairs":
+        return 40.0 * E + 8.0 * P
+    if stage == "compact":
+        return 4.0 * P + 2 * 352.0 * C
+    if stage == "integrate":
+        return 152.0 * L
+    return 0.0
+
+
+LAUNCHES = {"velocity": lambda p: p["substeps"] * p["solve_iterations"],
+            "position": lambda p: p["substeps"] * p["position_iterations"],
+            "integrate": lambda p: p["substeps"]}
+
+
+def build_world(workload: str, device: int):
+    from dynamis_b200 import World, scenes
+
+    scene = scenes.WORKLOADS[workload]()
+    world = World(device=device)
+    t0 = time.perf_counter()
+    scene.build(world)
+    return world, scene, time.perf_counter() - t0
+
+
+def run_ours(args, rank: int, world_size: int, local_rank: int):
+    import torch
+
+    from dynamis_b200 import records as R
+
+    torch.cuda.set_device(local_rank)
+    world, scene, build_s = build_world(args.workload, local_rank)
+    bodies = world.sizes()["bodies"]
+    stream = torch.cuda.Stream(device=local_rank)
+    world.set_stream(stream.cuda_stream)
+    for _ in range(args.setup):
+        world.step(DT)
+    world.wait()
+    for _ in range(args.warmup):
+        world.step(DT)
+    world.wait()
+    dist = None
+    if world_size > 1:
+        import torch.distributed as dist
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            world.step(DT)
+        end.record(stream)
+        end.synchronize()
+    world.wait()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    m = world.measured()
+    counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
+              "P": int(m[R.COUNTER["PAIRS"]]), "C": int(m[R.COUNTER["CONTACTS"]]), "R": int(m[R.COUNTER["SOLVER_ROWS"]]),
+              "L": int(m[R.COUNTER["LIVE"]])}
+    launches_per_step = world.step_kernel_count()
+    # per-stage breakdown: one more step run eagerly with CUDA events between stages
+    world.set_timing(True)
+    world.step(DT)
+    world.wait()
+    stages = world.stage_timings()
+    world.set_timing(False)
+    params = {"substeps": int(world.config["substeps"][0]), "solve_iterations": int(world.config["solve_iterations"][0]),
+              "position_iterations": int(world.config["position_iterations"][0]),
+              "pair_words": int(np.ceil(np.ceil(np.log2(max(counts["K"] - 1, 1) + 1)) / 8)) or 1}
+    dominant = max(stages, key=stages.get)
+    launches = LAUNCHES.get(dominant, lambda p: 1)(params)
+    per_launch_ms = stages[dominant] / launches
+    algo = stage_bytes(dominant, counts, params)
+    pk = peaks()
+    achieved = algo / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    # end to end through the C ABI with pinned host buffers
+    e2e_steps = max(3, min(args.steps, 10))
+    host = torch.empty(bodies * R.BODY_STATE.itemsize, dtype=torch.uint8, pin_memory=True)
+    host_out = torch.empty_like(host, pin_memory=True)
+    states_in = host.numpy().view(R.BODY_STATE)
+    states_out = host_out.numpy().view(R.BODY_STATE)
+    states_in[:] = world.read_states()
+    from dynamis_b200._native import lib, ptr
+
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        world.upload_states(states_in)
+        world.step(DT)
+        world._check(lib.dyn_download_states(world._h, ptr(states_out), bodies))
+        states_in[:] = states_out
+    e2e_s = time.perf_counter() - t0
+    result = {
+        "metric": METRIC, "value": bodies * args.steps * world_size / (ms * 1e-3), "unit": UNIT,
+        "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "bodies": bodies, "setup_steps": args.setup, "dt": DT,
+                   "parallelism": f"replicas{world_size}" if world_size > 1 else "single-world",
+                   "l2": "working set > 126 MB L2 (no flush between steps)", "counts_last_step": counts,
+                   "scene_build_s": round(build_s, 2)},
+        "e2e": {"value": bodies * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bodies * R.BODY_STATE.itemsize,
+                "d2h_bytes_per_step": bodies * R.BODY_STATE.itemsize},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk["source"],
+                     "algorithmic_bytes_per_launch": algo, "ms_per_launch": per_launch_ms},
+        "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget)
+    world.close()
+    return result
+
+
+def cpu_baseline(world, budget_s: float = 20.0) -> dict:
+    """The oracle (CPU restatement, one thread) stepping the same world state."""
+    from oracle.oracle import OracleWorld
+
+    scene = world.export_scene()
+    scene["states"] = world.read_states()
+    oracle = OracleWorld(scene, world.step_params(DT))
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        oracle.step(DT)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s / 2 or steps >= 3:
+            break
+    dt = time.perf_counter() - t0
+    n = len(scene["states"])
+    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} step(s) of the full {n}-body world from the GPU run's current state, one thread"}
+
+
+def run_reference(args) -> dict:
+    """The reference arm: the CPU restatement of the step on the host, all it can use (one thread)."""
+    from dynamis_b200 import World
+
+    world, scene, _ = build_world(args.workload, 0)
+    state_note = "initial lattice state"
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            for _ in range(args.setup + args.warmup):
+                world.step(DT)
+            world.wait()
+            state_note = f"state after {args.setup + args.warmup} steps (input prepared on the GPU, untimed)"
+    except Exception:
+        pass
+    base = cpu_baseline(world, budget_s=args.cpu_budget)
+    base["sample"] += f"; {state_note}"
+    world.close()
+    return {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "setup_steps": args.setup, "dt": DT},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--setup", type=int, default=120, help="untimed steps that form the pile before warm-up")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed_pile_262144")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+    if world_size > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    result = run_ours(args, rank, world_size, local_rank)
+    if rank == 0:
+        print(json.dumps(result))
+    if world_size > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,126 @@
+// layout.cuh - HBM layout of one world on the device.
+//
+// Bodies: one 128-byte BodyHot row per body holds every field the contact solver touches, so a
+// solver thread pulls a body in four 32-byte sectors; colder per-body fields live in parallel
+// arrays. Colliders and contacts are structure-of-arrays so warps read coalesced float4 columns.
+// The host converts the byte-exact ABI records (include/dynamis_abi.h) to and from this layout.
+#pragma once
+
+#include <cstdint>
+
+#include "dynamis_abi.h"
+
+namespace dyn {
+
+struct __align__(128) BodyHot {
+    float4 pos;  // position.xyz, inverse_mass
+    float4 rot;  // orientation (x, y, z, w)
+    float4 vel;  // velocity.xyz, 0
+    float4 ang;  // angular_velocity.xyz, 0
+    float4 com;  // local centre of mass.xyz, 0
+    float4 ii0;  // inverse inertia (xx, xy, xz, yy)
+    float4 ii1;  // inverse inertia (yz, zz), 0, 0
+    uint4 aux;   // sleeping, descriptor flags, contacts touching this body this step, 0
+};
+static_assert(sizeof(BodyHot) == 128, "BodyHot is one 128-byte row");
+
+// Contacts in manifold-slot-major structure-of-arrays: point slot p of contact i is at [p * cap + i].
+struct ContactSet {
+    float4* normal;  // normal.xyz, friction
+    uint4* rows;     // body row a, body row b, point_count | sensor << 8, events
+    float4* mat;     // rolling_friction, spin_friction, relaxation, damping_ratio
+    uint4* ids;      // collider a, collider b, first_body_id, second_body_id
+    uint4* ids2;     // first_generation, second_generation, surface, triangle
+    float4* extra;   // restitution, carried_normal, carried_tangent, 0
+    float4* la;      // local_a.xyz, depth
+    float4* lb;      // local_b.xyz, target speed
+    float4* acc;     // accumulated normal, tangent 1, tangent 2, feature (bits)
+    float4* pos;     // position.xyz, 0
+};
+
+// Control words (device-side counts the graph's kernels read instead of host values).
+enum Ctl : uint32_t {
+    CTL_ENTRIES = 0,
+    CTL_PAIRS = 1,
+    CTL_CONTACTS = 2,
+    CTL_TMP = 3,
+    CTL_LIVE = 4,
+    CTL_SOLVER_ROWS = 5,
+    CTL_ARCHIVED = 6,
+    CTL_ROUNDS = 7,
+    CTL_STATUS = 8,
+    CTL_VALID = 9,
+    CTL_COUNT = 16
+};
+
+struct DeviceWorld {
+    uint32_t n;   // body rows
+    uint32_t nd;  // dynamic rows (rows [0, nd))
+    uint32_t k;   // colliders
+    uint32_t e_cap, p_cap, c_cap;
+    // bodies
+    BodyHot* hot;
+    float4* prev_pos;
+    float4* prev_rot;
+    float4* force;
+    float4* torque;
+    uint4* ident;  // body_id, generation, collision_group, collision_mask
+    float* sleep_timer;
+    float4* damp;    // linear_damping, angular_damping, gravity_scale, 0
+    float2* thresh;  // sleep_velocity, sleep_angular_velocity
+    float4* inert0;  // inertia (xx, xy, xz, yy)
+    float2* inert1;  // inertia (yz, zz)
+    uint32_t* activity;
+    uint32_t* motion;
+    uint32_t* wake_flags;
+    uint32_t* row_of_id;
+    uint32_t id_count;
+    // colliders
+    uint32_t* c_owner;
+    uint4* c_kind;     // kind, flags, source, 0
+    float4* c_offset;  // local_offset.xyz, radius
+    float4* c_lrot;    // local_rotation
+    float4* c_half;    // half_extents.xyz, half_height
+    float4* c_mat;     // friction, restitution, rolling_friction, spin_friction
+    float4* c_mat2;    // relaxation, damping_ratio, impact_force, 0
+    uint2* c_filter;   // collision_group, collision_mask
+    float4* c_scale;   // scale.xyz, 0
+    const dyn_shape_source_record* sources;
+    const float4* vertices;
+    // broadphase
+    float4* aabb;  // [2k]: min.xyz, max.xyz
+    uint32_t* c_level;
+    uint32_t* entry_count;
+    uint32_t* entry_offset;
+    uint32_t* ekey;
+    uint32_t* eval;
+    uint32_t* ekey_alt;
+    uint32_t* eval_alt;
+    float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits
+    uint32_t* pmaj;
+    uint32_t* pmin;
+    uint32_t* pmaj_alt;
+    uint32_t* pmin_alt;
+    // narrowphase staging and compaction
+    ContactSet tmp;
+    uint32_t* pair_slot;
+    uint32_t* pair_flag;
+    uint32_t* pair_rank;
+    ContactSet cur;
+    ContactSet arc;
+    uint32_t* matched;
+    // islands, live list, solver
+    uint32_t* parents;
+    uint32_t* istate;
+    uint32_t* live;
+    uint32_t* solver_rows;
+    int32_t* vdelta;  // [8n]
+    int32_t* pdelta;  // [8n]
+    uint32_t* contributions;
+    float4* resolution;
+    // counters (reference slots) and control words
+    uint32_t* counters;
+    uint32_t* ctl;
+};
+
+}  // namespace dyn

@@ -1,0 +1,744 @@
+// scene.cpp - host-side scene building of the C ABI: configuration, hulls, spawning, records.
+//
+// Restates the reference's host set-up for the step path:
+//   PhysicsConfig::default                 crates/dynamis-model/src/config.rs:76-100
+//   BodyStateRecord::initial               crates/dynamis-abi/src/body.rs:36-58
+//   BodyDescriptorRecord::build            crates/dynamis-abi/src/body.rs:96-140
+//   ColliderRecord::build                  crates/dynamis-abi/src/collider.rs:47-103
+//   compute_mass_properties                crates/dynamis-model/src/mass.rs:155-212
+//   hull solid integrals                   crates/dynamis-hull/src/solid.rs:62-105
+//   StepParamsRecord::new                  crates/dynamis-abi/src/param.rs:110-158
+// The convex hull itself is an incremental quickhull (Barber, Dobkin and Huhdanpaa, 1996) in
+// double precision; it keeps input vertices that lie on the hull, in input order.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "world.h"
+
+namespace dyn {
+
+dyn_status fail(dyn_world* w, dyn_status status, const std::string& what) {
+    if (w) w->last_error = what;
+    return status;
+}
+
+namespace {
+
+using D3 = std::array<double, 3>;
+
+D3 sub(const D3& a, const D3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+D3 cross3(const D3& a, const D3& b) {
+    return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+double dot3(const D3& a, const D3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+double norm3(const D3& a) { return std::sqrt(dot3(a, a)); }
+
+struct QFace {
+    int a, b, c;
+    D3 n;
+    double d;
+    bool alive;
+    std::vector<int> outside;
+};
+
+QFace make_face(const std::vector<D3>& p, int a, int b, int c) {
+    QFace f{a, b, c, {0, 0, 0}, 0.0, true, {}};
+    D3 n = cross3(sub(p[b], p[a]), sub(p[c], p[a]));
+    double len = norm3(n);
+    if (len > 0) n = {n[0] / len, n[1] / len, n[2] / len};
+    f.n = n;
+    f.d = dot3(n, p[a]);
+    return f;
+}
+
+// Quickhull over points p; returns false when the points span no volume.
+bool quickhull(const std::vector<D3>& p, std::vector<std::array<int, 3>>* tris) {
+    int n = (int)p.size();
+    if (n < 4) return false;
+    double extent = 0.0;
+    for (const D3& q : p)
+        for (double v : q) extent = std::max(extent, std::fabs(v));
+    const double eps = 1e-10 * std::max(extent, 1e-30) * 8.0;
+    // initial simplex: widest pair among axis extremes, then farthest from line, then from plane
+    int ext[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            if (p[i][a] < p[ext[2 * a]][a]) ext[2 * a] = i;
+            if (p[i][a] > p[ext[2 * a + 1]][a]) ext[2 * a + 1] = i;
+        }
+    int i0 = 0, i1 = 0;
+    double best = -1;
+    for (int a = 0; a < 6; ++a)
+        for (int b = a + 1; b < 6; ++b) {
+            double d = norm3(sub(p[ext[a]], p[ext[b]]));
+            if (d > best) {
+                best = d;
+                i0 = ext[a];
+                i1 = ext[b];
+            }
+        }
+    if (best <= eps) return false;
+    D3 dir = sub(p[i1], p[i0]);
+    int i2 = -1;
+    best = eps;
+    for (int i = 0; i < n; ++i) {
+        double d = norm3(cross3(dir, sub(p[i], p[i0]))) / norm3(dir);
+        if (d > best) {
+            best = d;
+            i2 = i;
+        }
+    }
+    if (i2 < 0) return false;
+    D3 pn = cross3(sub(p[i1], p[i0]), sub(p[i2], p[i0]));
+    double pl = norm3(pn);
+    int i3 = -1;
+    best = eps;
+    for (int i = 0; i < n; ++i) {
+        double d = std::fabs(dot3(pn, sub(p[i], p[i0]))) / pl;
+        if (d > best) {
+            best = d;
+            i3 = i;
+        }
+    }
+    if (i3 < 0) return false;
+    D3 inner = {(p[i0][0] + p[i1][0] + p[i2][0] + p[i3][0]) / 4, (p[i0][1] + p[i1][1] + p[i2][1] + p[i3][1]) / 4,
+                (p[i0][2] + p[i1][2] + p[i2][2] + p[i3][2]) / 4};
+    std::vector<QFace> faces;
+    auto add = [&](int a, int b, int c) {
+        QFace f = make_face(p, a, b, c);
+        if (dot3(f.n, inner) - f.d > 0) {
+            f = make_face(p, a, c, b);
+        }
+        faces.push_back(f);
+    };
+    add(i0, i1, i2);
+    add(i0, i1, i3);
+    add(i0, i2, i3);
+    add(i1, i2, i3);
+    for (int i = 0; i < n; ++i) {
+        if (i == i0 || i == i1 || i == i2 || i == i3) continue;
+        for (QFace& f : faces) {
+            if (dot3(f.n, p[i]) - f.d > eps) {
+                f.outside.push_back(i);
+                break;
+            }
+        }
+    }
+    for (int guard = 0; guard < 4 * n + 16; ++guard) {
+        int fi = -1;
+        for (int i = 0; i < (int)faces.size(); ++i)
+            if (faces[i].alive && !faces[i].outside.empty()) {
+                fi = i;
+                break;
+            }
+        if (fi < 0) break;
+        int eye = faces[fi].outside[0];
+        double far = -1;
+        for (int q : faces[fi].outside) {
+            double d = dot3(faces[fi].n, p[q]) - faces[fi].d;
+            if (d > far) {
+                far = d;
+                eye = q;
+            }
+        }
+        std::vector<int> visible;
+        for (int i = 0; i < (int)faces.size(); ++i)
+            if (faces[i].alive && dot3(faces[i].n, p[eye]) - faces[i].d > eps) visible.push_back(i);
+        std::vector<std::pair<int, int>> edges;
+        for (int v : visible) {
+            const QFace& f = faces[v];
+            edges.push_back({f.a, f.b});
+            edges.push_back({f.b, f.c});
+            edges.push_back({f.c, f.a});
+        }
+        std::vector<std::pair<int, int>> horizon;
+        for (auto& e : edges) {
+            bool shared = false;
+            for (auto& o : edges)
+                if (o.first == e.second && o.second == e.first) {
+                    shared = true;
+                    break;
+                }
+            if (!shared) horizon.push_back(e);
+        }
+        std::vector<int> orphans;
+        for (int v : visible) {
+            faces[v].alive = false;
+            for (int q : faces[v].outside)
+                if (q != eye) orphans.push_back(q);
+            faces[v].outside.clear();
+        }
+        size_t first_new = faces.size();
+        for (auto& e : horizon) faces.push_back(make_face(p, e.first, e.second, eye));
+        for (int q : orphans) {
+            for (size_t i = first_new; i < faces.size(); ++i) {
+                if (dot3(faces[i].n, p[q]) - faces[i].d > eps) {
+                    faces[i].outside.push_back(q);
+                    break;
+                }
+            }
+        }
+    }
+    tris->clear();
+    for (const QFace& f : faces)
+        if (f.alive) tris->push_back({f.a, f.b, f.c});
+    return tris->size() >= 4;
+}
+
+// crates/dynamis-hull/src/solid.rs:3-105 (f64 accumulation about the vertex mean)
+void hull_solid(HullSource* h) {
+    size_t nv = h->vertices.size() / 3;
+    D3 apex = {0, 0, 0};
+    for (size_t i = 0; i < nv; ++i)
+        for (int a = 0; a < 3; ++a) apex[a] += (double)h->vertices[3 * i + a];
+    for (int a = 0; a < 3; ++a) apex[a] /= (double)nv;
+    auto shifted = [&](uint32_t v) {
+        return D3{(double)h->vertices[3 * v] - apex[0], (double)h->vertices[3 * v + 1] - apex[1],
+                  (double)h->vertices[3 * v + 2] - apex[2]};
+    };
+    auto squared = [](double a, double b, double c) { return (a * a + b * b + c * c + a * b + a * c + b * c) / 10.0; };
+    auto mixed = [](double ax, double bx, double cx, double ay, double by, double cy) {
+        return (2.0 * (ax * ay + bx * by + cx * cy) + ax * by + ay * bx + ax * cy + ay * cx + bx * cy + by * cx) / 20.0;
+    };
+    double volume = 0.0;
+    double first[3] = {0, 0, 0};
+    double second[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t t = 0; t + 2 < h->triangles.size(); t += 3) {
+        D3 a = shifted(h->triangles[t]), b = shifted(h->triangles[t + 1]), c = shifted(h->triangles[t + 2]);
+        if (dot3(cross3(a, b), c) < 0.0) std::swap(b, c);
+        double s = dot3(a, cross3(b, c)) / 6.0;
+        volume += s;
+        for (int k = 0; k < 3; ++k) first[k] += s * (a[k] + b[k] + c[k]) / 4.0;
+        second[0] += s * squared(a[0], b[0], c[0]);
+        second[3] += s * squared(a[1], b[1], c[1]);
+        second[5] += s * squared(a[2], b[2], c[2]);
+        second[1] += s * mixed(a[0], b[0], c[0], a[1], b[1], c[1]);
+        second[2] += s * mixed(a[0], b[0], c[0], a[2], b[2], c[2]);
+        second[4] += s * mixed(a[1], b[1], c[1], a[2], b[2], c[2]);
+    }
+    double cen[3] = {first[0] / volume, first[1] / volume, first[2] / volume};
+    h->volume = (float)volume;
+    for (int k = 0; k < 3; ++k) h->centroid[k] = (float)(apex[k] + cen[k]);
+    h->unit_second_moment[0] = (float)((second[0] - volume * cen[0] * cen[0]) / volume);
+    h->unit_second_moment[1] = (float)((second[1] - volume * cen[0] * cen[1]) / volume);
+    h->unit_second_moment[2] = (float)((second[2] - volume * cen[0] * cen[2]) / volume);
+    h->unit_second_moment[3] = (float)((second[3] - volume * cen[1] * cen[1]) / volume);
+    h->unit_second_moment[4] = (float)((second[4] - volume * cen[1] * cen[2]) / volume);
+    h->unit_second_moment[5] = (float)((second[5] - volume * cen[2] * cen[2]) / volume);
+}
+
+// ---- mass properties (crates/dynamis-model/src/mass.rs) ----
+struct Solid {
+    float volume;
+    float centroid[3];
+    float second[6];
+};
+constexpr float kPi = 3.14159265358979323846f;
+
+bool analytic_solid(const dyn_collider_record& c, const std::vector<HullSource>& hulls, Solid* s) {
+    std::memset(s, 0, sizeof(*s));
+    switch (c.kind) {
+        case DYN_SHAPE_SPHERE: {
+            float r = c.radius;
+            float m = r * r / 5.0f;
+            s->volume = 4.0f / 3.0f * kPi * r * r * r;
+            s->second[0] = m;
+            s->second[3] = m;
+            s->second[5] = m;
+            return true;
+        }
+        case DYN_SHAPE_CUBOID: {
+            float ex = c.half_extents[0] * 2.0f, ey = c.half_extents[1] * 2.0f, ez = c.half_extents[2] * 2.0f;
+            s->volume = ex * ey * ez;
+            s->second[0] = ex * ex / 12.0f;
+            s->second[3] = ey * ey / 12.0f;
+            s->second[5] = ez * ez / 12.0f;
+            return true;
+        }
+        case DYN_SHAPE_CAPSULE: {
+            float r = c.radius, hh = c.half_height;
+            float cyl = kPi * r * r * 2.0f * hh;
+            float sph = 4.0f / 3.0f * kPi * r * r * r;
+            float total = cyl + sph;
+            float lateral = (cyl * r * r / 4.0f + sph * r * r / 5.0f) / total;
+            float axial = (cyl * 4.0f * hh * hh / 12.0f + sph * (r * r / 5.0f + 3.0f / 4.0f * r * hh + hh * hh)) / total;
+            s->volume = total;
+            s->second[0] = lateral;
+            s->second[3] = axial;
+            s->second[5] = lateral;
+            return true;
+        }
+        case DYN_SHAPE_CYLINDER: {
+            float r = c.radius, height = c.half_height * 2.0f;
+            float lateral = r * r / 4.0f;
+            s->volume = kPi * r * r * height;
+            s->second[0] = lateral;
+            s->second[3] = height * height / 12.0f;
+            s->second[5] = lateral;
+            return true;
+        }
+        case DYN_SHAPE_HULL: {
+            if (c.source >= hulls.size()) return false;
+            const HullSource& h = hulls[c.source];
+            s->volume = h.volume;
+            for (int k = 0; k < 3; ++k) s->centroid[k] = h.centroid[k];
+            for (int k = 0; k < 6; ++k) s->second[k] = h.unit_second_moment[k];
+            return true;
+        }
+        default:
+            return false;
+    }
+}
+
+void model_rotate(const float q[4], const float v[3], float out[3]) {
+    // dynamis-model math::quat_rotate: v + 2w(u x v) + 2 u x (u x v)
+    float ux = q[0], uy = q[1], uz = q[2], w = q[3];
+    float tx = 2.0f * (uy * v[2] - uz * v[1]);
+    float ty = 2.0f * (uz * v[0] - ux * v[2]);
+    float tz = 2.0f * (ux * v[1] - uy * v[0]);
+    out[0] = v[0] + w * tx + (uy * tz - uz * ty);
+    out[1] = v[1] + w * ty + (uz * tx - ux * tz);
+    out[2] = v[2] + w * tz + (ux * ty - uy * tx);
+}
+
+using M3 = std::array<std::array<float, 3>, 3>;
+M3 mat_from_quat(const float q[4]) {
+    float x = q[0], y = q[1], z = q[2], w = q[3];
+    return M3{{{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - w * z), 2.0f * (x * z + w * y)},
+               {2.0f * (x * y + w * z), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - w * x)},
+               {2.0f * (x * z - w * y), 2.0f * (y * z + w * x), 1.0f - 2.0f * (x * x + y * y)}}};
+}
+M3 mat_mul(const M3& a, const M3& b) {
+    M3 r{};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) r[i][j] = a[i][0] * b[0][j] + a[i][1] * b[1][j] + a[i][2] * b[2][j];
+    return r;
+}
+
+bool inertia_inverse(const float in[6], float out[6]) {
+    float xx = in[0], xy = in[1], xz = in[2], yy = in[3], yz = in[4], zz = in[5];
+    float cxx = yy * zz - yz * yz, cxy = xz * yz - xy * zz, cxz = xy * yz - xz * yy;
+    float cyy = xx * zz - xz * xz, cyz = xy * xz - xx * yz, czz = xx * yy - xy * xy;
+    float det = xx * cxx + xy * cxy + xz * cxz;
+    if (!(xx > 0.0f && czz > 0.0f && det > 0.0f)) return false;
+    out[0] = cxx / det;
+    out[1] = cxy / det;
+    out[2] = cxz / det;
+    out[3] = cyy / det;
+    out[4] = cyz / det;
+    out[5] = czz / det;
+    return true;
+}
+
+}  // namespace
+
+void rebuild_rows(dyn_world* w) {
+    if (w->raw_rows || !w->rows_dirty) return;
+    uint32_t n = (uint32_t)w->spawn_states.size();
+    std::vector<uint32_t> order;
+    order.reserve(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const dyn_body_descriptor_record& d = w->spawn_descs[i];
+        if ((d.flags & DYN_BODY_KINEMATIC) == 0u && d.inverse_mass > 0.0f) order.push_back(i);
+    }
+    w->dynamic_count = (uint32_t)order.size();
+    for (uint32_t i = 0; i < n; ++i) {
+        const dyn_body_descriptor_record& d = w->spawn_descs[i];
+        if (!((d.flags & DYN_BODY_KINEMATIC) == 0u && d.inverse_mass > 0.0f)) order.push_back(i);
+    }
+    w->states.resize(n);
+    w->descs.resize(n);
+    w->row_of_id.assign(n, DYN_NO_BODY);
+    for (uint32_t r = 0; r < n; ++r) {
+        w->states[r] = w->spawn_states[order[r]];
+        w->descs[r] = w->spawn_descs[order[r]];
+        w->row_of_id[order[r]] = r;
+    }
+    w->colliders = w->spawn_colliders;
+    w->owners.resize(w->spawn_owner.size());
+    for (size_t i = 0; i < w->spawn_owner.size(); ++i) w->owners[i] = w->row_of_id[w->spawn_owner[i]];
+    w->rows_dirty = false;
+}
+
+std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vector<float>* verts) {
+    std::vector<dyn_shape_source_record> out(w->hulls.size());
+    verts->clear();
+    for (size_t s = 0; s < w->hulls.size(); ++s) {
+        const HullSource& h = w->hulls[s];
+        dyn_shape_source_record& r = out[s];
+        std::memset(&r, 0, sizeof(r));
+        r.kind = DYN_SHAPE_HULL;
+        r.vertex_offset = (uint32_t)(verts->size() / 4);
+        r.vertex_count = (uint32_t)(h.vertices.size() / 3);
+        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (size_t i = 0; i + 2 < h.vertices.size(); i += 3) {
+            for (int a = 0; a < 3; ++a) {
+                mn[a] = std::min(mn[a], h.vertices[i + a]);
+                mx[a] = std::max(mx[a], h.vertices[i + a]);
+                verts->push_back(h.vertices[i + a]);
+            }
+            verts->push_back(0.0f);
+        }
+        for (int a = 0; a < 3; ++a) {
+            r.local_min[a] = mn[a];
+            r.local_max[a] = mx[a];
+        }
+    }
+    return out;
+}
+
+}  // namespace dyn
+
+using namespace dyn;
+
+extern "C" {
+
+DYN_API uint32_t dyn_abi_version(void) { return 1u; }
+
+DYN_API const char* dyn_status_string(dyn_status s) {
+    switch (s) {
+        case DYN_OK: return "ok";
+        case DYN_ERR_INVALID: return "invalid argument";
+        case DYN_ERR_CAPACITY: return "capacity exceeded";
+        case DYN_ERR_CUDA: return "CUDA runtime error";
+        case DYN_ERR_NO_DEVICE: return "no CUDA device";
+        case DYN_ERR_DEVICE_STATUS: return "device gave up a bounded wait";
+        case DYN_ERR_DEGENERATE: return "degenerate hull";
+        default: return "unknown status";
+    }
+}
+
+DYN_API void dyn_config_default(dyn_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->gravity[1] = -9.81f;
+    c->damping = 0.05f;
+    c->angular_damping = 0.05f;
+    c->substeps = 2;
+    c->solve_iterations = 8;
+    c->position_iterations = 10;
+    c->relaxation = 0.8f;
+    c->slop = 0.005f;
+    c->contact_margin = 0.02f;
+    c->restitution_threshold = 1.0f;
+    c->max_velocity = 200.0f;
+    c->max_angular_velocity = 400.0f;
+    c->sleep_velocity = 0.2f;
+    c->sleep_angular_velocity = 0.5f;
+    c->sleep_time = 0.5f;
+    c->friction_combine = 0;     // Multiply
+    c->restitution_combine = 2;  // Max
+}
+
+DYN_API void dyn_collider_desc_default(dyn_collider_desc* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->shape = DYN_SHAPE_SPHERE;
+    c->radius = 0.5f;
+    c->rotation[3] = 1.0f;
+    c->scale[0] = c->scale[1] = c->scale[2] = 1.0f;
+    c->friction = 0.5f;
+    c->contact_frequency = INFINITY;
+    c->contact_damping_ratio = 1.0f;
+    c->collision_group = DYN_NO_COLLISION_FILTER;
+    c->collision_mask = DYN_NO_COLLISION_FILTER;
+    c->impact_force = INFINITY;
+}
+
+DYN_API void dyn_body_desc_default(dyn_body_desc* b) {
+    if (!b) return;
+    std::memset(b, 0, sizeof(*b));
+    b->orientation[3] = 1.0f;
+    b->mass = 1.0f;
+    b->gravity_scale = 1.0f;
+    b->linear_damping = -1.0f;
+    b->angular_damping = -1.0f;
+    b->sleep_velocity = -1.0f;
+    b->sleep_angular_velocity = -1.0f;
+    b->collision_group = 1u;
+    b->collision_mask = 0xFFFFFFFFu;
+}
+
+DYN_API const char* dyn_last_error(const dyn_world* w) { return w ? w->last_error.c_str() : "null world"; }
+
+DYN_API dyn_status dyn_add_hull(dyn_world* w, const float* xyz, uint32_t n, uint32_t* out_source) {
+    if (!w || !xyz || !out_source) return fail(w, DYN_ERR_INVALID, "dyn_add_hull: null argument");
+    std::vector<D3> pts;
+    pts.reserve(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int a = 0; a < 3; ++a)
+            if (!std::isfinite(xyz[3 * i + a])) return fail(w, DYN_ERR_INVALID, "dyn_add_hull: non-finite vertex");
+        pts.push_back({(double)xyz[3 * i], (double)xyz[3 * i + 1], (double)xyz[3 * i + 2]});
+    }
+    std::vector<std::array<int, 3>> tris;
+    if (!quickhull(pts, &tris)) return fail(w, DYN_ERR_DEGENERATE, "dyn_add_hull: points span no volume");
+    std::vector<int> used(n, -1);
+    for (auto& t : tris)
+        for (int v : t) used[v] = 0;
+    HullSource h;
+    int next = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (used[i] < 0) continue;
+        used[i] = next++;
+        h.vertices.push_back(xyz[3 * i]);
+        h.vertices.push_back(xyz[3 * i + 1]);
+        h.vertices.push_back(xyz[3 * i + 2]);
+    }
+    for (auto& t : tris)
+        for (int v : t) h.triangles.push_back((uint32_t)used[v]);
+    hull_solid(&h);
+    if (!(h.volume > 0.0f) || !std::isfinite(h.volume)) return fail(w, DYN_ERR_DEGENERATE, "dyn_add_hull: no volume");
+    *out_source = (uint32_t)w->hulls.size();
+    w->hulls.push_back(std::move(h));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_hull_info(const dyn_world* w, uint32_t source, uint32_t* vc, uint32_t* tc, float* volume,
+                                 float centroid[3]) {
+    if (!w || source >= w->hulls.size()) return DYN_ERR_INVALID;
+    const HullSource& h = w->hulls[source];
+    if (vc) *vc = (uint32_t)(h.vertices.size() / 3);
+    if (tc) *tc = (uint32_t)(h.triangles.size() / 3);
+    if (volume) *volume = h.volume;
+    if (centroid)
+        for (int k = 0; k < 3; ++k) centroid[k] = h.centroid[k];
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_spawn_bodies(dyn_world* w, const dyn_body_desc* bodies, uint32_t n, const dyn_collider_desc* cols,
+                                    uint32_t k, uint32_t* out_ids) {
+    if (!w || (n && !bodies)) return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: null argument");
+    if (w->raw_rows) return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: scene was replaced by dyn_upload_bodies");
+    for (uint32_t b = 0; b < n; ++b) {
+        const dyn_body_desc& bd = bodies[b];
+        if (bd.collider_count == 0 || (uint64_t)bd.collider_first + bd.collider_count > k || !cols)
+            return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: a body requires at least one collider in range");
+        if (bd.kinematic && bd.ccd) return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: kinematic bodies cannot declare ccd");
+        uint32_t body_id = (uint32_t)w->spawn_states.size();
+        // ColliderRecord::build for each collider
+        std::vector<dyn_collider_record> recs;
+        for (uint32_t c = 0; c < bd.collider_count; ++c) {
+            const dyn_collider_desc& cd = cols[bd.collider_first + c];
+            dyn_collider_record r;
+            std::memset(&r, 0, sizeof(r));
+            r.slot = (uint32_t)(w->spawn_colliders.size() + recs.size());
+            r.kind = cd.shape;
+            if (cd.shape == DYN_SHAPE_HULL && cd.source >= w->hulls.size())
+                return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: unknown hull source");
+            if (cd.shape == DYN_SHAPE_NONE || cd.shape > DYN_SHAPE_PLANE || cd.shape == DYN_SHAPE_MESH
+                || cd.shape == DYN_SHAPE_HEIGHTFIELD || cd.shape == DYN_SHAPE_TRIANGLE)
+                return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: shape outside the step path");
+            uint32_t flags = cd.sensor ? DYN_COLLIDER_SENSOR : 0u;
+            flags |= cd.events & (DYN_EVENT_MODE_BEGIN_END | DYN_EVENT_MODE_PERSIST);
+            if (cd.events & DYN_EVENT_MODE_PERSIST) flags |= DYN_EVENT_MODE_BEGIN_END;
+            r.flags = flags;
+            float f0 = cd.scale[0];
+            bool folded = cd.shape != DYN_SHAPE_HULL && cd.shape != DYN_SHAPE_PLANE;
+            float s0 = folded ? f0 : 1.0f;
+            r.radius = (cd.shape == DYN_SHAPE_SPHERE || cd.shape == DYN_SHAPE_CAPSULE || cd.shape == DYN_SHAPE_CYLINDER)
+                ? cd.radius * s0 : 0.0f;
+            r.half_height = (cd.shape == DYN_SHAPE_CAPSULE || cd.shape == DYN_SHAPE_CYLINDER) ? cd.half_height * s0 : 0.0f;
+            r.impact_force = cd.impact_force;
+            if (cd.shape == DYN_SHAPE_CUBOID) {
+                for (int a = 0; a < 3; ++a) r.half_extents[a] = cd.half_extents[a] * cd.scale[a];
+            }
+            r.collision_group = cd.collision_group;
+            r.collision_mask = cd.collision_mask;
+            for (int a = 0; a < 3; ++a) r.local_offset[a] = cd.offset[a];
+            for (int a = 0; a < 4; ++a) r.local_rotation[a] = cd.rotation[a];
+            r.friction = cd.friction;
+            r.restitution = cd.restitution;
+            r.source = cd.shape == DYN_SHAPE_HULL ? cd.source : 0u;
+            r.rolling_friction = cd.rolling_friction;
+            for (int a = 0; a < 3; ++a) r.scale[a] = cd.shape == DYN_SHAPE_HULL ? cd.scale[a] : 1.0f;
+            r.spin_friction = cd.spin_friction;
+            r.relaxation = std::isinf(cd.contact_frequency) ? 0.0f : 1.0f / (6.28318530717958647692f * cd.contact_frequency);
+            r.damping_ratio = cd.contact_damping_ratio;
+            recs.push_back(r);
+        }
+        // mass properties (mass.rs:155-212) over non-sensor solids
+        struct Item {
+            const dyn_collider_record* c;
+            const dyn_collider_desc* d;
+            Solid s;
+            float volume;
+        };
+        std::vector<Item> items;
+        for (uint32_t c = 0; c < bd.collider_count; ++c) {
+            const dyn_collider_desc& cd = cols[bd.collider_first + c];
+            if (cd.sensor) continue;
+            Solid s;
+            if (!analytic_solid(recs[c], w->hulls, &s)) continue;
+            float sv = recs[c].kind == DYN_SHAPE_HULL ? recs[c].scale[0] * recs[c].scale[1] * recs[c].scale[2] : 1.0f;
+            items.push_back(Item{&recs[c], &cd, s, sv * s.volume});
+        }
+        float total_volume = 0.0f;
+        for (const Item& it : items) total_volume += it.volume;
+        bool density_mode = bd.density > 0.0f;
+        float mass = density_mode ? bd.density * total_volume : bd.mass;
+        bool dynamic = !bd.kinematic && mass > 0.0f;
+        float com[3] = {0, 0, 0}, inertia[6] = {0, 0, 0, 0, 0, 0}, inv_inertia[6] = {0, 0, 0, 0, 0, 0};
+        if (!items.empty() && total_volume > 0.0f && mass > 0.0f) {
+            auto centroid_of = [&](const Item& it, float out[3]) {
+                float sc[3];
+                for (int a = 0; a < 3; ++a) sc[a] = it.c->scale[a] * it.s.centroid[a];
+                float rot[3];
+                model_rotate(it.c->local_rotation, sc, rot);
+                for (int a = 0; a < 3; ++a) out[a] = it.c->local_offset[a] + rot[a];
+            };
+            float sum[3] = {0, 0, 0};
+            for (const Item& it : items) {
+                float at[3];
+                centroid_of(it, at);
+                for (int a = 0; a < 3; ++a) sum[a] += at[a] * it.volume;
+            }
+            for (int a = 0; a < 3; ++a) com[a] = sum[a] / total_volume;
+            float second[6] = {0, 0, 0, 0, 0, 0};
+            for (const Item& it : items) {
+                float shape_mass = mass * it.volume / total_volume;
+                const float* u = it.s.second;
+                const float* sc = it.c->scale;
+                float local[6] = {u[0] * sc[0] * sc[0], u[1] * sc[0] * sc[1], u[2] * sc[0] * sc[2],
+                                  u[3] * sc[1] * sc[1], u[4] * sc[1] * sc[2], u[5] * sc[2] * sc[2]};
+                M3 r = mat_from_quat(it.c->local_rotation);
+                M3 s = {{{local[0], local[1], local[2]}, {local[1], local[3], local[4]}, {local[2], local[4], local[5]}}};
+                M3 rt = {{{r[0][0], r[1][0], r[2][0]}, {r[0][1], r[1][1], r[2][1]}, {r[0][2], r[1][2], r[2][2]}}};
+                M3 m = mat_mul(r, mat_mul(s, rt));
+                float rotated[6] = {m[0][0], (m[0][1] + m[1][0]) * 0.5f, (m[0][2] + m[2][0]) * 0.5f,
+                                    m[1][1], (m[1][2] + m[2][1]) * 0.5f, m[2][2]};
+                float at[3];
+                centroid_of(it, at);
+                float d[3] = {at[0] - com[0], at[1] - com[1], at[2] - com[2]};
+                float tr[6] = {rotated[0] + d[0] * d[0], rotated[1] + d[0] * d[1], rotated[2] + d[0] * d[2],
+                               rotated[3] + d[1] * d[1], rotated[4] + d[1] * d[2], rotated[5] + d[2] * d[2]};
+                for (int q = 0; q < 6; ++q) second[q] += tr[q] * shape_mass;
+            }
+            float xx = second[0], xy = second[1], xz = second[2], yy = second[3], yz = second[4], zz = second[5];
+            float I[6] = {yy + zz, -xy, -xz, xx + zz, -yz, xx + yy};
+            for (int q = 0; q < 6; ++q) inertia[q] = I[q];
+            if (!inertia_inverse(inertia, inv_inertia))
+                return fail(w, DYN_ERR_INVALID, "dyn_spawn_bodies: inertia tensor must be positive definite");
+        }
+        dyn_body_descriptor_record d;
+        std::memset(&d, 0, sizeof(d));
+        d.inverse_mass = dynamic ? 1.0f / mass : 0.0f;
+        d.linear_damping = bd.linear_damping >= 0.0f ? bd.linear_damping : w->config.damping;
+        d.angular_damping = bd.angular_damping >= 0.0f ? bd.angular_damping : w->config.angular_damping;
+        d.gravity_scale = bd.gravity_scale;
+        d.sleep_velocity = bd.sleep_velocity >= 0.0f ? bd.sleep_velocity : 0.0f;
+        d.sleep_angular_velocity = bd.sleep_angular_velocity >= 0.0f ? bd.sleep_angular_velocity : 0.0f;
+        uint32_t flags = 0;
+        if (bd.kinematic) flags |= DYN_BODY_KINEMATIC;
+        if (bd.ccd) flags |= DYN_BODY_CCD;
+        if (bd.sleep_velocity >= 0.0f) flags |= DYN_OVERRIDE_SLEEP_LINEAR;
+        if (bd.sleep_angular_velocity >= 0.0f) flags |= DYN_OVERRIDE_SLEEP_ANGULAR;
+        d.flags = flags;
+        d.collision_group = bd.collision_group;
+        d.collision_mask = bd.collision_mask;
+        for (int a = 0; a < 3; ++a) d.com[a] = com[a];
+        for (int q = 0; q < 6; ++q) {
+            d.inertia[q] = inertia[q];
+            d.inverse_inertia[q] = inv_inertia[q];
+        }
+        dyn_body_state_record s;
+        std::memset(&s, 0, sizeof(s));
+        for (int a = 0; a < 3; ++a) {
+            s.position[a] = bd.position[a];
+            s.prev_position[a] = bd.position[a];
+            s.velocity[a] = bd.velocity[a];
+            s.angular_velocity[a] = bd.angular_velocity[a];
+        }
+        for (int a = 0; a < 4; ++a) {
+            s.orientation[a] = bd.orientation[a];
+            s.prev_orientation[a] = bd.orientation[a];
+        }
+        s.body_id = body_id;
+        s.generation = 0;
+        w->spawn_states.push_back(s);
+        w->spawn_descs.push_back(d);
+        for (const dyn_collider_record& r : recs) {
+            w->spawn_colliders.push_back(r);
+            w->spawn_owner.push_back(body_id);
+        }
+        if (out_ids) out_ids[b] = body_id;
+    }
+    w->rows_dirty = true;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_scene_sizes(const dyn_world* cw, uint32_t* bodies, uint32_t* dyn_bodies, uint32_t* colliders,
+                                   uint32_t* sources, uint32_t* vertices) {
+    if (!cw) return DYN_ERR_INVALID;
+    dyn_world* w = const_cast<dyn_world*>(cw);
+    rebuild_rows(w);
+    if (bodies) *bodies = (uint32_t)w->states.size();
+    if (dyn_bodies) *dyn_bodies = w->dynamic_count;
+    if (colliders) *colliders = (uint32_t)w->colliders.size();
+    if (sources) *sources = (uint32_t)w->hulls.size();
+    if (vertices) {
+        uint32_t v = 0;
+        for (const HullSource& h : w->hulls) v += (uint32_t)(h.vertices.size() / 3);
+        *vertices = v;
+    }
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_export_scene(const dyn_world* cw, dyn_body_state_record* states, dyn_body_descriptor_record* descs,
+                                    dyn_collider_record* colliders, uint32_t* owners, dyn_shape_source_record* sources,
+                                    float* vertices) {
+    if (!cw) return DYN_ERR_INVALID;
+    dyn_world* w = const_cast<dyn_world*>(cw);
+    rebuild_rows(w);
+    if (states) std::memcpy(states, w->states.data(), w->states.size() * sizeof(*states));
+    if (descs) std::memcpy(descs, w->descs.data(), w->descs.size() * sizeof(*descs));
+    if (colliders) std::memcpy(colliders, w->colliders.data(), w->colliders.size() * sizeof(*colliders));
+    if (owners) std::memcpy(owners, w->owners.data(), w->owners.size() * sizeof(*owners));
+    std::vector<float> verts;
+    std::vector<dyn_shape_source_record> src = shape_sources(w, &verts);
+    if (sources) std::memcpy(sources, src.data(), src.size() * sizeof(*sources));
+    if (vertices) std::memcpy(vertices, verts.data(), verts.size() * sizeof(float));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_step_params_for(const dyn_world* cw, float dt, dyn_step_params* out) {
+    if (!cw || !out) return DYN_ERR_INVALID;
+    if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(const_cast<dyn_world*>(cw), DYN_ERR_INVALID, "a step timestep must be positive");
+    dyn_world* w = const_cast<dyn_world*>(cw);
+    rebuild_rows(w);
+    const dyn_config& c = w->config;
+    std::memset(out, 0, sizeof(*out));
+    out->gravity[0] = c.gravity[0];
+    out->gravity[1] = c.gravity[1];
+    out->gravity[2] = c.gravity[2];
+    out->dt = dt;
+    out->substep_dt = dt / (float)c.substeps;
+    out->damping = c.damping;
+    out->angular_damping = c.angular_damping;
+    out->body_count = (uint32_t)w->states.size();
+    out->substeps = c.substeps;
+    out->solve_iterations = c.solve_iterations;
+    out->relaxation = c.relaxation;
+    out->slop = c.slop;
+    out->restitution_threshold = c.restitution_threshold;
+    out->max_velocity = c.max_velocity;
+    out->max_angular_velocity = c.max_angular_velocity;
+    out->dynamic_count = w->dynamic_count;
+    out->sleep_velocity = c.sleep_velocity;
+    out->sleep_angular_velocity = c.sleep_angular_velocity;
+    out->sleep_time = c.sleep_time;
+    out->friction_combine = c.friction_combine;
+    out->restitution_combine = c.restitution_combine;
+    out->position_iterations = c.position_iterations;
+    out->contact_margin = c.contact_margin;
+    out->collider_count = (uint32_t)w->colliders.size();
+    out->soft_iterations = 1;
+    out->soft_substeps = 4;
+    out->soft_substep_dt = dt / 4.0f;
+    out->settle_velocity = 1.0e-4f;
+    return DYN_OK;
+}
+
+}  // extern "C"

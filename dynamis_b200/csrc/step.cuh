@@ -1,0 +1,1069 @@
+// step.cuh - the sm_100a kernels of one rigid-body step.
+//
+// One kernel per stage of World::step (crates/dynamis-rigid/src/lib.rs:119-153); each cites the
+// WGSL pass it replaces. Counts produced on the device (entries, pairs, contacts, live rows,
+// solver rows) stay on the device in the control words; kernels grid-stride over them, so the
+// whole step is replayed as one CUDA graph with no host round trip. Appends use coalesced-group
+// aggregated atomics; every order that depends on those atomics (pair emission, live list,
+// solver rows, staging slots) is either sorted afterwards or irrelevant to the result.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
+#include "dmath.cuh"
+#include "layout.cuh"
+#include "narrow.cuh"
+#include "sort.cuh"
+
+namespace dyn {
+
+namespace cg = cooperative_groups;
+
+__device__ __forceinline__ uint32_t append_slot(uint32_t* counter) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+__device__ __forceinline__ void add_counter(uint32_t* counter, uint32_t value) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t total = cg::reduce(g, value, cg::plus<uint32_t>());
+    if (g.thread_rank() == 0 && total) atomicAdd(counter, total);
+}
+__device__ __forceinline__ void max_counter(uint32_t* counter, uint32_t value) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t m = cg::reduce(g, value, cg::greater<uint32_t>());
+    if (g.thread_rank() == 0) atomicMax(counter, m);
+}
+__device__ __forceinline__ void or_counter(uint32_t* counter, uint32_t value) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t m = cg::reduce(g, value, cg::bit_or<uint32_t>());
+    if (g.thread_rank() == 0 && m) atomicOr(counter, m);
+}
+
+#define GRID_STRIDE(i, n) for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+// Counters that persist across steps (crates/dynamis-abi/src/counter.rs: Maintained).
+__global__ void k_reset(DeviceWorld w) {
+    for (uint32_t i = threadIdx.x; i < DYN_COUNTER_DEVICE_COUNT; i += blockDim.x) {
+        if (i == DYN_COUNTER_ARCHIVED || i == DYN_COUNTER_STEP) continue;
+        w.counters[i] = 0u;
+    }
+    for (uint32_t i = threadIdx.x; i < CTL_COUNT; i += blockDim.x) {
+        if (i == CTL_ARCHIVED || i == CTL_STATUS) continue;
+        w.ctl[i] = 0u;
+    }
+}
+
+// clear_inputs.wgsl, activity.wgsl (all rows); begin_step.wgsl, island_init.wgsl (dynamic rows);
+// solver_reset.wgsl (all rows). Folding them into one pass changes nothing: none of them reads
+// what another writes.
+__global__ void k_begin(DeviceWorld w, dyn_step_params p) {
+    GRID_STRIDE(i, w.n) {
+        w.force[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.torque[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        BodyHot& h = w.hot[i];
+        float im = h.pos.w;
+        uint32_t flags = h.aux.y;
+        uint32_t sleeping = h.aux.x;
+        bool mv = moves(im, flags);
+        bool sim = simulates(im, flags);
+        bool awake = mv && sleeping == 0u;
+        w.activity[i] = awake ? 1u : 0u;
+        f3 v = xyz(h.vel), av = xyz(h.ang);
+        bool moving;
+        if (mv && !sim && (!is_zero3(v) || !is_zero3(av))) {
+            moving = true;
+        } else if (!sim || sleeping != 0u) {
+            moving = false;
+        } else {
+            float2 th = w.thresh[i];
+            float sv = (flags & DYN_OVERRIDE_SLEEP_LINEAR) ? th.x : p.sleep_velocity;
+            float sw = (flags & DYN_OVERRIDE_SLEEP_ANGULAR) ? th.y : p.sleep_angular_velocity;
+            moving = length(v) > sv || length(av) > sw;
+        }
+        w.motion[i] = moving ? 1u : 0u;
+        if (awake) w.counters[DYN_COUNTER_ACTIVE] = 1u;
+        if (i < w.nd) {
+            if (sleeping == 0u) {
+                w.prev_pos[i] = make_float4(h.pos.x, h.pos.y, h.pos.z, 0.0f);
+                w.prev_rot[i] = h.rot;
+            }
+            w.parents[i] = i;
+            w.istate[i] = 0u;
+        }
+        h.aux.z = 0u;
+        w.resolution[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+__device__ __forceinline__ float grid_extent_of(f3 mn, f3 mx) { return wmax(wmax(mx.x - mn.x, mx.y - mn.y), mx.z - mn.z); }
+
+// broadphase_aabb.wgsl:11-62 (core.wgsl:109-126 for the grid resolution)
+__global__ void k_aabb(DeviceWorld w, dyn_step_params p) {
+    GRID_STRIDE(i, w.k) {
+        uint32_t owner = w.c_owner[i];
+        if (owner == DYN_NO_BODY) continue;
+        DBody b = load_dbody(w.hot, owner);
+        DColl c = load_dcoll(w, i);
+        WShape s = world_shape(b.position, b.orientation, c);
+        DAabb tight = world_aabb(w, s);
+        WShape up = s;
+        up.rotation = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        DAabb res = world_aabb(w, up);
+        float extent = grid_extent_of(res.min, res.max);
+        float scale = extent <= 0.0f ? 0.0f : wclamp(1.0f / extent, 1.0f / 1e12f, 1e12f);
+        max_counter(&w.counters[DYN_COUNTER_GRID_SCALE], fbits(scale));
+        max_counter(&w.counters[DYN_COUNTER_GRID_EXTENT], fbits(wmax(extent, 0.0f)));
+        DAabb swept = tight;
+        if (moves(b.inverse_mass, b.flags)) {
+            f3 travel = vabs(b.velocity * p.dt);
+            float spin = length(b.angular_velocity * p.dt);
+            f3 center = b.position + quat_rotate(b.orientation, c.offset);
+            float radius = length((tight.max - tight.min) * 0.5f) + length(center - dbody_com(b));
+            float rr = spin >= 3.141592653589793f ? 2.0f * radius : 2.0f * radius * dsin(0.5f * spin);
+            f3 reach = s3(p.contact_margin + rr);
+            swept.min = tight.min - travel - reach;
+            swept.max = tight.max + travel + reach;
+        }
+        w.aabb[2 * i] = mk4(swept.min, 0.0f);
+        w.aabb[2 * i + 1] = mk4(swept.max, 0.0f);
+    }
+}
+
+// ---- grid (grid_index.wgsl:28-287) ----
+struct I3 {
+    int x, y, z;
+};
+__device__ __forceinline__ float base_cell(const DeviceWorld& w) {
+    float scale = bitsf(w.counters[DYN_COUNTER_GRID_SCALE]);
+    float extent = bitsf(w.counters[DYN_COUNTER_GRID_EXTENT]);
+    float finest = scale > 0.0f ? 1.0f / scale : 1e12f;
+    return wmax(finest, extent * 9.31322574615478515625e-10f);
+}
+__device__ __forceinline__ I3 floor_div(f3 v, float cs) {
+    return I3{(int)floorf(v.x / cs), (int)floorf(v.y / cs), (int)floorf(v.z / cs)};
+}
+__device__ __forceinline__ float level_size(uint32_t level, float cs) { return cs * (float)(1u << level); }
+__device__ __forceinline__ uint32_t cell_hash(I3 c) {
+    uint32_t x = (uint32_t)c.x * 0x9E3779B9u;
+    uint32_t y = (uint32_t)c.y * 0x85EBCA77u;
+    uint32_t z = (uint32_t)c.z * 0xC2B2AE3Du;
+    return (x ^ y ^ z ^ (x << 7) ^ (y >> 3) ^ (z << 11)) & DYN_CELL_HASH_MASK;
+}
+__device__ __forceinline__ uint32_t cell_key(uint32_t level, I3 c) { return (level << DYN_LEVEL_KEY_SHIFT) | cell_hash(c); }
+__device__ __forceinline__ uint32_t shape_levels(f3 mn, f3 mx, float base) {
+    uint32_t level = 0;
+    for (;;) {
+        float cs = level_size(level, base);
+        I3 a = floor_div(mn, cs), b = floor_div(mx, cs);
+        uint32_t sx = (uint32_t)(b.x - a.x + 1), sy = (uint32_t)(b.y - a.y + 1), sz = (uint32_t)(b.z - a.z + 1);
+        uint32_t m = max(max(sx, sy), sz);
+        if (m <= DYN_MAX_CELLS_PER_AXIS || level >= DYN_GRID_LEVEL_LIMIT) break;
+        level += 1;
+    }
+    return level;
+}
+
+// collider_emit.wgsl:6-29 (level, cell budget) for every collider: entry counts for the scan.
+__global__ void k_entry_count(DeviceWorld w) {
+    float base = base_cell(w);
+    GRID_STRIDE(i, w.k) {
+        uint32_t owner = w.c_owner[i];
+        uint32_t emitted = 0;
+        if (owner != DYN_NO_BODY) {
+            float4 a = w.aabb[2 * i], b = w.aabb[2 * i + 1];
+            f3 mn = xyz(a), mx = xyz(b);
+            uint32_t level = shape_levels(mn, mx, base);
+            w.c_level[i] = level;
+            const BodyHot& h = w.hot[owner];
+            bool mv = moves(h.pos.w, h.aux.y);
+            bool awake = w.activity[owner] != 0u || w.wake_flags[owner] != 0u;
+            or_counter(&w.counters[mv ? DYN_COUNTER_GRID_LEVELS : DYN_COUNTER_IMMOVABLE_LEVELS], 1u << level);
+            float cs = level_size(level, base);
+            I3 lo = floor_div(mn, cs), hi = floor_div(mx, cs);
+            uint32_t count = (uint32_t)(hi.x - lo.x + 1) * (uint32_t)(hi.y - lo.y + 1) * (uint32_t)(hi.z - lo.z + 1);
+            emitted = min(count, DYN_MAX_CELLS_PER_COLLIDER);
+            if (count > emitted) add_counter(&w.counters[DYN_COUNTER_ENTRY_FAULTS], count - emitted);
+            if (level > 0u && awake) add_counter(&w.counters[DYN_COUNTER_COARSE_ACTIVE], 1u);
+            add_counter(&w.counters[mv ? DYN_COUNTER_ENTRIES : DYN_COUNTER_IMMOVABLE_ENTRIES], emitted);
+            if (!mv) add_counter(&w.counters[DYN_COUNTER_IMMOVABLE_EMITTED], emitted);
+        }
+        w.entry_count[i] = emitted;
+    }
+}
+
+// collider_emit.wgsl:31-63 at the scanned slots (collider order): key, payload = slot, GridEntry.
+__global__ void k_entry_emit(DeviceWorld w) {
+    float base = base_cell(w);
+    GRID_STRIDE(i, w.k) {
+        uint32_t emitted = w.entry_count[i];
+        if (emitted == 0u) continue;
+        uint32_t owner = w.c_owner[i];
+        uint32_t first = w.entry_offset[i];
+        float4 a = w.aabb[2 * i], b = w.aabb[2 * i + 1];
+        f3 mn = xyz(a), mx = xyz(b);
+        uint32_t level = w.c_level[i];
+        float cs = level_size(level, base);
+        I3 lo = floor_div(mn, cs), hi = floor_div(mx, cs);
+        uint32_t sy = (uint32_t)(hi.y - lo.y + 1), sz = (uint32_t)(hi.z - lo.z + 1);
+        uint32_t rows = sy * sz;
+        const BodyHot& h = w.hot[owner];
+        bool mv = moves(h.pos.w, h.aux.y);
+        bool awake = w.activity[owner] != 0u || w.wake_flags[owner] != 0u;
+        for (uint32_t ordinal = 0; ordinal < emitted; ++ordinal) {
+            I3 c = I3{lo.x + (int)(ordinal / rows), lo.y + (int)((ordinal / sz) % sy), lo.z + (int)(ordinal % sz)};
+            uint32_t offset = (uint32_t)(c.x - lo.x) | ((uint32_t)(c.y - lo.y) << 1) | ((uint32_t)(c.z - lo.z) << 2);
+            uint32_t info = i | (offset << DYN_ENTRY_CELL_SHIFT) | (DYN_ENTRY_KIND_COLLIDER << DYN_ENTRY_KIND_SHIFT);
+            if (mv && awake) info |= DYN_ENTRY_AWAKE;
+            if (mv) info |= DYN_ENTRY_MOBILE;
+            if (offset == 0u) info |= DYN_ENTRY_PRIMARY;
+            uint32_t slot = first + ordinal;
+            w.ekey[slot] = cell_key(level, c);
+            w.eval[slot] = slot;
+            w.entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(owner));
+            w.entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(info));
+        }
+    }
+}
+
+// ---- pair emission (cell_pairs.wgsl, level_links.wgsl, pair_emit.wgsl) ----
+struct GEntry {
+    f3 mn, mx;
+    uint32_t group, info;
+};
+__device__ __forceinline__ GEntry load_entry(const DeviceWorld& w, uint32_t node) {
+    float4 a = w.entries[2 * node], b = w.entries[2 * node + 1];
+    return GEntry{xyz(a), xyz(b), __float_as_uint(a.w), __float_as_uint(b.w)};
+}
+__device__ __forceinline__ bool entry_awake(const DeviceWorld& w, const GEntry& e) {
+    if ((e.info & DYN_ENTRY_MOBILE) == 0u) return w.wake_flags[e.group] != 0u;
+    return (e.info & DYN_ENTRY_AWAKE) != 0u;
+}
+__device__ __forceinline__ bool overlaps(const GEntry& a, const GEntry& b) {
+    return a.mn.x <= b.mx.x && a.mn.y <= b.mx.y && a.mn.z <= b.mx.z && b.mn.x <= a.mx.x && b.mn.y <= a.mx.y && b.mn.z <= a.mx.z;
+}
+__device__ __forceinline__ I3 entry_cell(const GEntry& e, float cs) {
+    uint32_t bits = (e.info & DYN_ENTRY_CELL_MASK) >> DYN_ENTRY_CELL_SHIFT;
+    I3 c = floor_div(e.mn, cs);
+    return I3{c.x + (int)(bits & 1u), c.y + (int)((bits >> 1) & 1u), c.z + (int)((bits >> 2) & 1u)};
+}
+__device__ __forceinline__ bool same_cell(I3 a, I3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+__device__ __forceinline__ bool overlap_cell_is(const GEntry& a, const GEntry& b, float cs, I3 cell) {
+    return same_cell(floor_div(vmax(a.mn, b.mn), cs), cell);
+}
+__device__ __forceinline__ void emit_pair(const DeviceWorld& w, const GEntry& a, const GEntry& b, bool same_node) {
+    if (((a.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) return;
+    if (((b.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) return;
+    if (same_node || a.group == b.group) return;
+    if ((a.info & DYN_ENTRY_MOBILE) == 0u && (b.info & DYN_ENTRY_MOBILE) == 0u) return;
+    uint32_t slot = append_slot(&w.counters[DYN_COUNTER_PAIRS]);
+    if (slot < w.p_cap) {
+        uint32_t ia = a.info & DYN_ENTRY_INDEX_MASK, ib = b.info & DYN_ENTRY_INDEX_MASK;
+        w.pmaj[slot] = min(ia, ib);
+        w.pmin[slot] = max(ia, ib);
+    } else {
+        add_counter(&w.counters[DYN_COUNTER_REFUSED_PAIRS], 1u);
+    }
+}
+__device__ __forceinline__ uint32_t lower_bound(const uint32_t* keys, uint32_t n, uint32_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(keys + mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One thread per sorted entry: coarse-level links of a primary entry, then same-cell mates.
+__global__ void k_pairs(DeviceWorld w) {
+    const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
+    const float grid = base_cell(w);
+    const uint32_t occupied =
+        w.counters[DYN_COUNTER_GRID_LEVELS] | w.counters[DYN_COUNTER_RESTING_LEVELS] | w.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
+    const bool coarse_active = w.counters[DYN_COUNTER_COARSE_ACTIVE] != 0u;
+    GRID_STRIDE(index, live) {
+        uint32_t node = w.eval[index];
+        GEntry e = load_entry(w, node);
+        if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
+        bool awake = entry_awake(w, e);
+        uint32_t level = w.c_level[e.info & DYN_ENTRY_INDEX_MASK];
+        if ((e.info & DYN_ENTRY_PRIMARY) != 0u && (awake || coarse_active)) {
+            uint32_t coarser = occupied & ~((1u << min(level + 1u, 31u)) - 1u);
+            while (coarser != 0u) {
+                uint32_t link = 31u - __clz(coarser);
+                coarser &= ~(1u << link);
+                float cs = level_size(link, grid);
+                I3 lo = floor_div(e.mn, cs), hi = floor_div(e.mx, cs);
+                // A box spans at most two cells per axis at any level coarser than its own; a
+                // wider span only comes from a non-finite box, whose walk is cut short and counted.
+                if ((long long)hi.x - lo.x > 3 || (long long)hi.y - lo.y > 3 || (long long)hi.z - lo.z > 3 || hi.x < lo.x ||
+                    hi.y < lo.y || hi.z < lo.z) {
+                    add_counter(&w.counters[DYN_COUNTER_ENTRY_FAULTS], 1u);
+                    continue;
+                }
+                for (int x = lo.x; x <= hi.x; ++x)
+                    for (int y = lo.y; y <= hi.y; ++y)
+                        for (int z = lo.z; z <= hi.z; ++z) {
+                            I3 cell = I3{x, y, z};
+                            uint32_t key = cell_key(link, cell);
+                            uint32_t j = lower_bound(w.ekey, live, key);
+                            for (; j < live && __ldg(w.ekey + j) == key; ++j) {
+                                uint32_t other = w.eval[j];
+                                if (other == node) continue;
+                                GEntry o = load_entry(w, other);
+                                if (!awake && !entry_awake(w, o)) continue;
+                                if (!overlaps(e, o)) continue;
+                                if (!same_cell(entry_cell(o, cs), cell)) continue;
+                                if (!overlap_cell_is(e, o, cs, cell)) continue;
+                                emit_pair(w, e, o, false);
+                            }
+                        }
+            }
+        }
+        if (!awake) continue;
+        float cs = level_size(level, grid);
+        I3 cell = entry_cell(e, cs);
+        uint32_t key = __ldg(w.ekey + index);
+        uint32_t j = index;
+        while (j > 0u && __ldg(w.ekey + j - 1u) == key) --j;
+        for (; j < live && __ldg(w.ekey + j) == key; ++j) {
+            if (j == index) continue;
+            uint32_t other = w.eval[j];
+            GEntry o = load_entry(w, other);
+            if (j < index && entry_awake(w, o)) continue;
+            if (!overlaps(e, o)) continue;
+            if (!same_cell(entry_cell(o, cs), cell)) continue;
+            if (!overlap_cell_is(e, o, cs, cell)) continue;
+            emit_pair(w, e, o, node == other);
+        }
+    }
+}
+
+// ---- narrowphase (narrowphase.wgsl:518-685) into the staging set, then ordered compaction ----
+__device__ __forceinline__ void write_contact(const ContactSet& s, uint32_t cap, uint32_t i, const Mani& m, uint32_t ra,
+                                              uint32_t rb, uint32_t ca, uint32_t cb, const DBody& fb, const DBody& sb,
+                                              uint32_t fid, uint32_t sid, uint32_t fgen, uint32_t sgen, bool sensor,
+                                              float4 fmat, float4 smat, float4 fmat2, float4 smat2, uint32_t fflags,
+                                              uint32_t sflags, uint32_t fcomb, uint32_t rcomb) {
+    auto combine = [](float a, float b, uint32_t mode) -> float {
+        if (mode == 1u) return wmin(a, b);
+        if (mode == 2u) return wmax(a, b);
+        if (mode == 3u) return (a + b) * 0.5f;
+        return sqrtf(a * b);
+    };
+    float friction = combine(fmat.x, smat.x, fcomb);
+    float restitution = combine(fmat.y, smat.y, rcomb);
+    uint32_t events = (fflags & sflags) & (DYN_EVENT_MODE_BEGIN_END | DYN_EVENT_MODE_PERSIST);
+    s.normal[i] = mk4(m.normal, friction);
+    s.rows[i] = make_uint4(ra, rb, m.count | ((sensor ? 1u : 0u) << 8), events);
+    s.mat[i] = make_float4(wmax(fmat.z, smat.z), wmax(fmat.w, smat.w), fmat2.x + smat2.x, wmax(fmat2.y, smat2.y));
+    s.ids[i] = make_uint4(ca, cb, fid, sid);
+    s.ids2[i] = make_uint4(fgen, sgen, DYN_NO_SURFACE, DYN_NO_TRIANGLE);
+    s.extra[i] = make_float4(restitution, 0.0f, 0.0f, 0.0f);
+    for (uint32_t p = 0; p < m.count; ++p) {
+        f3 point = m.p[p].position;
+        f3 la = quat_rotate(quat_conj(fb.orientation), point - fb.position);
+        f3 lb = quat_rotate(quat_conj(sb.orientation), point - sb.position);
+        size_t o = (size_t)p * cap + i;
+        s.la[o] = mk4(la, m.p[p].depth);
+        s.lb[o] = mk4(lb, 0.0f);
+        s.acc[o] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(m.p[p].feature));
+        s.pos[o] = mk4(point, 0.0f);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_narrowphase(DeviceWorld w, dyn_step_params p) {
+    const uint32_t pairs = min(w.counters[DYN_COUNTER_PAIRS], w.p_cap);
+    GRID_STRIDE(index, pairs) {
+        uint32_t fs = w.pmaj[index], ss = w.pmin[index];
+        uint32_t valid = 0u;
+        uint32_t fr = w.c_owner[fs], sr = w.c_owner[ss];
+        do {
+            if (fr == DYN_NO_BODY || sr == DYN_NO_BODY || fr == sr) break;
+            DBody fb = load_dbody(w.hot, fr), sb = load_dbody(w.hot, sr);
+            if (!moves(fb.inverse_mass, fb.flags) && !moves(sb.inverse_mass, sb.flags)) break;
+            DColl fc = load_dcoll(w, fs), sc = load_dcoll(w, ss);
+            if (fc.kind == 0u || sc.kind == 0u) break;
+            uint4 fi = w.ident[fr], si = w.ident[sr];
+            uint2 ff = w.c_filter[fs], sf = w.c_filter[ss];
+            uint32_t fg = ff.x != DYN_NO_COLLISION_FILTER ? ff.x : fi.z;
+            uint32_t fm = ff.y != DYN_NO_COLLISION_FILTER ? ff.y : fi.w;
+            uint32_t sg = sf.x != DYN_NO_COLLISION_FILTER ? sf.x : si.z;
+            uint32_t sm = sf.y != DYN_NO_COLLISION_FILTER ? sf.y : si.w;
+            if (!((fg & sm) != 0u && (sg & fm) != 0u)) break;
+            bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
+            bool fw = shape_world_geometry(fc.kind), sw = shape_world_geometry(sc.kind);
+            if (fw && sw) break;
+            float margin = p.contact_margin;
+            if ((fb.flags & DYN_BODY_CCD) || (sb.flags & DYN_BODY_CCD)) {
+                margin = p.contact_margin + length(sb.velocity - fb.velocity) * p.dt;
+            }
+            Mani m;
+            m.count = 0;
+            m.normal = s3(0.0f);
+            if (fw) {
+                if (fc.kind != 9u) break;
+                m = plane_convex(w, world_shape(fb.position, fb.orientation, fc), world_shape(sb.position, sb.orientation, sc), margin);
+            } else if (sw) {
+                if (sc.kind != 9u) break;
+                m = plane_convex(w, world_shape(sb.position, sb.orientation, sc), world_shape(fb.position, fb.orientation, fc), margin);
+                m.normal = -m.normal;
+                for (uint32_t q = 0; q < m.count; ++q) m.p[q].feature = feature_mirror(m.p[q].feature);
+            } else if (!veq(fc.scale, s3(1.0f)) || !veq(sc.scale, s3(1.0f)) || !shape_analytic(fc.kind) || !shape_analytic(sc.kind)
+                       || (fc.kind == 2u && sc.kind == 3u) || (fc.kind == 3u && sc.kind == 2u)) {
+                WShape a = world_shape(fb.position, fb.orientation, fc);
+                WShape b = world_shape(sb.position, sb.orientation, sc);
+                Hit hit = convex_hit(w, a, b);
+                if (hit.distance <= margin) {
+                    mani_emit(&m, hit.normal);
+                    if (!convex_pair_manifold(w, a, b, hit.normal, &m)) {
+                        if (hit.distance <= margin) mani_push(&m, hit.point, -hit.distance, kFeatPoint);
+                    }
+                }
+            } else if (fc.kind == 1u && sc.kind == 1u) {
+                m = sphere_sphere(fb, fc, sb, sc, margin);
+            } else if (fc.kind == 1u && sc.kind == 2u) {
+                m = sphere_box(fb, fc, sb, sc, margin);
+            } else if (fc.kind == 1u && sc.kind == 3u) {
+                m = sphere_capsule(fb, fc, sb, sc, margin);
+            } else if (fc.kind == 2u && sc.kind == 1u) {
+                m = sphere_box(sb, sc, fb, fc, margin);
+                m.normal = -m.normal;
+            } else if (fc.kind == 2u && sc.kind == 2u) {
+                m = box_box_sat(fb, fc, sb, sc, margin);
+            } else if (fc.kind == 3u && sc.kind == 1u) {
+                m = sphere_capsule(sb, sc, fb, fc, margin);
+                m.normal = -m.normal;
+            } else {
+                m = capsule_capsule(fb, fc, sb, sc, margin);
+            }
+            if (m.count == 0u) break;
+            uint32_t slot = append_slot(&w.ctl[CTL_TMP]);
+            if (slot >= w.c_cap) {
+                add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
+                break;
+            }
+            write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs], w.c_mat[ss],
+                          w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine, p.restitution_combine);
+            w.pair_slot[index] = slot;
+            valid = 1u;
+        } while (false);
+        w.pair_flag[index] = valid;
+    }
+}
+
+__device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi, const ContactSet& to, uint32_t ti, uint32_t cap) {
+    uint4 rows = from.rows[fi];
+    to.normal[ti] = from.normal[fi];
+    to.rows[ti] = rows;
+    to.mat[ti] = from.mat[fi];
+    to.ids[ti] = from.ids[fi];
+    to.ids2[ti] = from.ids2[fi];
+    float4 ex = from.extra[fi];
+    to.extra[ti] = make_float4(ex.x, 0.0f, 0.0f, 0.0f);
+    uint32_t count = rows.z & 0xFFu;
+    for (uint32_t p = 0; p < count; ++p) {
+        size_t f = (size_t)p * cap + fi, t = (size_t)p * cap + ti;
+        to.la[t] = from.la[f];
+        to.lb[t] = from.lb[f];
+        to.acc[t] = from.acc[f];
+        to.pos[t] = from.pos[f];
+    }
+}
+
+// compact_scatter.wgsl:12-27 (ranks from the pair-flag scan): contacts in sorted pair order.
+__global__ void k_compact(DeviceWorld w) {
+    const uint32_t pairs = min(w.counters[DYN_COUNTER_PAIRS], w.p_cap);
+    const uint32_t valid = w.ctl[CTL_VALID];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        uint32_t c = min(valid, w.c_cap);
+        w.counters[DYN_COUNTER_CONTACTS] = valid;
+        w.ctl[CTL_CONTACTS] = c;
+        w.counters[DYN_COUNTER_BLOCKS] = c;
+    }
+    GRID_STRIDE(index, pairs) {
+        if (w.pair_flag[index] == 0u) continue;
+        uint32_t dst = w.pair_rank[index];
+        if (dst >= w.c_cap) {
+            add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
+            continue;
+        }
+        copy_contact(w.tmp, w.pair_slot[index], w.cur, dst, w.c_cap);
+        w.matched[dst] = 0u;
+    }
+}
+
+// ---- warm-start identity (identity.wgsl, contact_relay.wgsl, contact_begin.wgsl) ----
+__device__ __forceinline__ bool same_pair(uint4 hi, uint4 hi2, uint4 ci, uint4 ci2) {
+    bool same = hi.z == ci.z && hi2.x == ci2.x && hi.w == ci.w && hi2.y == ci2.y && hi.x == ci.x && hi.y == ci.y;
+    bool flipped = hi.z == ci.w && hi2.x == ci2.y && hi.w == ci.z && hi2.y == ci2.x && hi.x == ci.y && hi.y == ci.x;
+    return same || flipped;
+}
+__device__ __forceinline__ uint32_t resolve_row(const DeviceWorld& w, uint32_t id, uint32_t gen) {
+    if (id >= w.id_count) return DYN_NO_BODY;
+    uint32_t row = w.row_of_id[id];
+    if (row == DYN_NO_BODY || w.ident[row].y != gen) return DYN_NO_BODY;
+    return row;
+}
+__device__ __forceinline__ bool touches(const ContactSet& s, uint32_t i, uint32_t cap, float threshold) {
+    uint32_t count = s.rows[i].z & 0xFFu;
+    for (uint32_t p = 0; p < count; ++p) {
+        if (s.la[(size_t)p * cap + i].w >= -threshold) return true;
+    }
+    return false;
+}
+
+// contact_relay.wgsl:34-71 over last step's contacts.
+__global__ void k_relay(DeviceWorld w) {
+    const uint32_t held_n = w.ctl[CTL_ARCHIVED];
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const uint32_t cap = w.c_cap;
+    GRID_STRIDE(h, held_n) {
+        uint4 hi = w.arc.ids[h], hi2 = w.arc.ids2[h];
+        uint4 hrows = w.arc.rows[h];
+        if (resolve_row(w, hi.z, hi2.x) == DYN_NO_BODY || resolve_row(w, hi.w, hi2.y) == DYN_NO_BODY) continue;
+        uint32_t lo = 0, hi_ = count;
+        while (lo < hi_) {
+            uint32_t mid = (lo + hi_) >> 1;
+            uint4 c = w.cur.ids[mid];
+            if (c.x < hi.x || (c.x == hi.x && c.y < hi.y)) lo = mid + 1;
+            else hi_ = mid;
+        }
+        if (!(lo < count)) continue;
+        uint4 ci = w.cur.ids[lo];
+        if (!(ci.x == hi.x && ci.y == hi.y)) continue;
+        uint4 ci2 = w.cur.ids2[lo];
+        if (!same_pair(hi, hi2, ci, ci2)) continue;
+        if ((hrows.w & DYN_CONTACT_ANNOUNCED) == 0u) continue;
+        w.matched[lo] = 1u;
+        uint4 crows = w.cur.rows[lo];
+        uint32_t ccount = crows.z & 0xFFu, hcount = hrows.z & 0xFFu;
+        bool taken[4] = {false, false, false, false};
+        float carried_n = 0.0f, carried_t = 0.0f;
+        for (uint32_t pi = 0; pi < ccount; ++pi) {
+            size_t co = (size_t)pi * cap + lo;
+            float4 cacc = w.cur.acc[co];
+            uint32_t feature = __float_as_uint(cacc.w);
+            f3 cla = xyz(w.cur.la[co]), clb = xyz(w.cur.lb[co]);
+            uint32_t picked = DYN_NO_SLOT;
+            float picked_d = 0.0f;
+            for (uint32_t hj = 0; hj < hcount; ++hj) {
+                if (taken[hj]) continue;
+                size_t ho = (size_t)hj * cap + h;
+                uint32_t hf = __float_as_uint(w.arc.acc[ho].w);
+                if (!(hf == feature || hf == feature_mirror(feature))) continue;
+                float d = length(xyz(w.arc.la[ho]) - cla) + length(xyz(w.arc.lb[ho]) - clb);
+                if (picked == DYN_NO_SLOT || d < picked_d) {
+                    picked = hj;
+                    picked_d = d;
+                }
+            }
+            float4 nacc = cacc;
+            if (picked != DYN_NO_SLOT) {
+                taken[picked] = true;
+                float4 hacc = w.arc.acc[(size_t)picked * cap + h];
+                nacc = make_float4(hacc.x, hacc.y, hacc.z, cacc.w);
+                w.cur.acc[co] = nacc;
+            }
+            carried_n = carried_n + wmax(nacc.x, 0.0f);
+            carried_t = carried_t + sqrtf(nacc.y * nacc.y + nacc.z * nacc.z);
+        }
+        float4 ex = w.cur.extra[lo];
+        w.cur.extra[lo] = make_float4(ex.x, carried_n, carried_t, 0.0f);
+        w.cur.rows[lo] = make_uint4(crows.x, crows.y, crows.z, crows.w | DYN_CONTACT_ANNOUNCED);
+    }
+}
+
+// contact_begin.wgsl:41-71 (no resting archive): unmatched touching contacts are announced.
+__global__ void k_contact_begin(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    GRID_STRIDE(i, count) {
+        if (w.matched[i] != 0u) continue;
+        if (touches(w.cur, i, w.c_cap, p.slop)) {
+            uint4 r = w.cur.rows[i];
+            w.cur.rows[i] = make_uint4(r.x, r.y, r.z, r.w | DYN_CONTACT_ANNOUNCED);
+        }
+    }
+}
+
+// ---- islands (island_link*.wgsl, island_flatten.wgsl, island_aggregate.wgsl, island_count.wgsl) ----
+__device__ __forceinline__ uint32_t island_find(const DeviceWorld& w, uint32_t node) {
+    uint32_t current = node;
+    uint32_t parent = atomicAdd(&w.parents[current], 0u);
+    for (uint32_t guard = 0; parent != current && guard < w.nd; ++guard) {
+        current = parent;
+        parent = atomicAdd(&w.parents[current], 0u);
+    }
+    return current;
+}
+__global__ void k_island_link(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    GRID_STRIDE(i, count) {
+        uint4 r = w.cur.rows[i];
+        uint32_t pc = r.z & 0xFFu, sensor = (r.z >> 8) & 0xFFu;
+        if (pc == 0u || sensor == 1u || !touches(w.cur, i, w.c_cap, p.slop)) continue;
+        uint32_t first = r.x, second = r.y;
+        uint32_t dc = w.nd;
+        if (second >= dc && w.wake_flags[second] != 0u) atomicOr(&w.wake_flags[first], 1u);
+        if (first >= dc && w.wake_flags[first] != 0u) atomicOr(&w.wake_flags[second], 1u);
+        if (first >= dc || second >= dc || first == second) continue;
+        bool joined = false;
+        for (uint32_t attempt = 0; attempt < 256u; ++attempt) {
+            uint32_t a = island_find(w, first), b = island_find(w, second);
+            if (a == b) {
+                joined = true;
+                break;
+            }
+            uint32_t lower = min(a, b), higher = max(a, b);
+            if (atomicCAS(&w.parents[higher], higher, lower) == higher) {
+                joined = true;
+                break;
+            }
+        }
+        if (!joined) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
+    }
+}
+__global__ void k_island_flatten(DeviceWorld w) {
+    GRID_STRIDE(i, w.nd) {
+        volatile uint32_t* par = w.parents;
+        uint32_t parent = par[i];
+        uint32_t grand = par[parent];
+        par[i] = min(parent, grand);
+    }
+}
+__global__ void k_island_aggregate(DeviceWorld w) {
+    GRID_STRIDE(i, w.nd) {
+        uint32_t root = w.parents[i];
+        if (root == i) add_counter(&w.counters[DYN_COUNTER_ISLANDS], 1u);
+        if (w.wake_flags[i] == 0u && w.motion[i] == 0u) continue;
+        atomicMax(&w.istate[root], DYN_ISLAND_WAKE);
+    }
+}
+// island_wake.wgsl:10-22 then live.wgsl:8-18 for the same row.
+__global__ void k_wake_live(DeviceWorld w) {
+    GRID_STRIDE(i, w.nd) {
+        uint32_t root = w.parents[i];
+        BodyHot& h = w.hot[i];
+        uint32_t sleeping = h.aux.x;
+        if (sleeping != 0u && (w.istate[root] & DYN_ISLAND_WAKE) != 0u) {
+            add_counter(&w.counters[DYN_COUNTER_WOKE], 1u);
+            add_counter(&w.counters[DYN_COUNTER_WOKE_DEFERRED], 1u);
+            h.aux.x = 0u;
+            sleeping = 0u;
+            w.sleep_timer[i] = 0.0f;
+        }
+        w.wake_flags[i] = 0u;
+        if (moves(h.pos.w, h.aux.y) && sleeping == 0u) {
+            uint32_t slot = append_slot(&w.ctl[CTL_LIVE]);
+            w.live[slot] = i;
+        }
+    }
+}
+
+// ---- solver (solver_blocks.wgsl, solver_contact_block.wgsl, solver_block_apply.wgsl) ----
+__device__ __forceinline__ bool resolves(uint4 rows) { return (rows.z & 0xFFu) > 0u && ((rows.z >> 8) & 0xFFu) == 0u; }
+
+__global__ void k_solver_blocks(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const uint32_t cap = w.c_cap;
+    GRID_STRIDE(i, count) {
+        uint4 r = w.cur.rows[i];
+        if (!resolves(r)) continue;
+        DBody fb = load_dbody(w.hot, r.x), sb = load_dbody(w.hot, r.y);
+        f3 normal = xyz(w.cur.normal[i]);
+        float restitution = w.cur.extra[i].x;
+        uint32_t pc = r.z & 0xFFu;
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            size_t o = (size_t)pi * cap + i;
+            f3 position = xyz(w.cur.pos[o]);
+            float depth = w.cur.la[o].w;
+            float speed = dot(relative_velocity(fb, sb, position, position), normal);
+            float target = 0.0f;
+            if (depth < 0.0f) {
+                target = depth / p.dt;
+            } else if (speed < -p.restitution_threshold) {
+                target = -speed * restitution;
+            }
+            float4 lb = w.cur.lb[o];
+            w.cur.lb[o] = make_float4(lb.x, lb.y, lb.z, target);
+        }
+        if (atomicAdd(&w.hot[r.x].aux.z, 1u) == 0u) w.solver_rows[append_slot(&w.ctl[CTL_SOLVER_ROWS])] = r.x;
+        if (atomicAdd(&w.hot[r.y].aux.z, 1u) == 0u) w.solver_rows[append_slot(&w.ctl[CTL_SOLVER_ROWS])] = r.y;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[DYN_COUNTER_BLOCKS] = count;
+}
+
+__device__ __forceinline__ int32_t solver_word(float value, float scale) { return (int32_t)wclamp(value * scale, -2.0e9f, 2.0e9f); }
+__device__ __forceinline__ void accumulate(int32_t* deltas, uint32_t row, f3 lin, f3 ang, float scale) {
+    int32_t* d = deltas + 8u * row;
+    atomicAdd(d + 0, solver_word(lin.x, scale));
+    atomicAdd(d + 1, solver_word(lin.y, scale));
+    atomicAdd(d + 2, solver_word(lin.z, scale));
+    atomicAdd(d + 3, solver_word(ang.x, scale));
+    atomicAdd(d + 4, solver_word(ang.y, scale));
+    atomicAdd(d + 5, solver_word(ang.z, scale));
+}
+__device__ __forceinline__ void make_tangents(f3 n, f3* t1, f3* t2) {
+    f3 t = fabsf(n.x) > 0.9f ? mk3(0.0f, 1.0f, 0.0f) : mk3(1.0f, 0.0f, 0.0f);
+    *t1 = normalize(cross(n, t));
+    *t2 = cross(n, *t1);
+}
+__device__ __forceinline__ f3 arm(const DBody& b, f3 local) { return quat_rotate(b.orientation, local) + b.position; }
+__device__ __forceinline__ void pair_impulse(DBody* a, DBody* b, f3 pa, f3 pb, f3 j) {
+    a->velocity = a->velocity - j * a->inverse_mass;
+    a->angular_velocity = a->angular_velocity - dbody_iinv(*a, cross(pa - dbody_com(*a), j));
+    b->velocity = b->velocity + j * b->inverse_mass;
+    b->angular_velocity = b->angular_velocity + dbody_iinv(*b, cross(pb - dbody_com(*b), j));
+}
+__device__ __forceinline__ float momentum_mass(const DBody& a, const DBody& b, f3 pa, f3 pb, f3 axis) {
+    f3 ra = pa - dbody_com(a), rb = pb - dbody_com(b);
+    f3 rax = cross(ra, axis), rbx = cross(rb, axis);
+    return a.inverse_mass + b.inverse_mass + dot(rax, dbody_iinv(a, rax)) + dot(rbx, dbody_iinv(b, rbx));
+}
+__device__ __forceinline__ DBody split_body(DBody b, float s) {
+    b.inverse_mass = b.inverse_mass * s;
+    b.ii0 = make_float4(b.ii0.x * s, b.ii0.y * s, b.ii0.z * s, b.ii0.w * s);
+    b.ii1 = make_float2(b.ii1.x * s, b.ii1.y * s);
+    return b;
+}
+
+// solver_contact_block.wgsl:195-233
+__global__ void k_warm(DeviceWorld w) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const uint32_t cap = w.c_cap;
+    GRID_STRIDE(i, count) {
+        uint4 r = w.cur.rows[i];
+        if (!resolves(r)) continue;  // zero deltas change nothing
+        DBody fl = load_dbody(w.hot, r.x), sl = load_dbody(w.hot, r.y);
+        DBody f = dbody_inert(fl) ? dbody_frozen(fl) : fl;
+        DBody s = dbody_inert(sl) ? dbody_frozen(sl) : sl;
+        f3 normal = xyz(w.cur.normal[i]);
+        f3 t1, t2;
+        make_tangents(normal, &t1, &t2);
+        uint32_t pc = r.z & 0xFFu;
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            size_t o = (size_t)pi * cap + i;
+            f3 af = arm(f, xyz(w.cur.la[o]));
+            f3 as = arm(s, xyz(w.cur.lb[o]));
+            float4 acc = w.cur.acc[o];
+            f3 j = normal * acc.x + t1 * acc.y + t2 * acc.z;
+            pair_impulse(&f, &s, af, as, j);
+        }
+        accumulate(w.vdelta, r.x, f.velocity - fl.velocity, f.angular_velocity - fl.angular_velocity, DYN_SOLVER_VELOCITY_SCALE);
+        accumulate(w.vdelta, r.y, s.velocity - sl.velocity, s.angular_velocity - sl.angular_velocity, DYN_SOLVER_VELOCITY_SCALE);
+    }
+}
+
+// solver_contact_block.wgsl:6-193 (Jacobi block with mass splitting)
+__global__ void __launch_bounds__(128) k_solve(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const uint32_t cap = w.c_cap;
+    const bool residual = w.ctl[CTL_ROUNDS] == p.solve_iterations;
+    GRID_STRIDE(i, count) {
+        uint4 r = w.cur.rows[i];
+        if (!resolves(r)) continue;
+        DBody pf = load_dbody(w.hot, r.x), ps = load_dbody(w.hot, r.y);
+        DBody sf = split_body(pf, (float)max(w.hot[r.x].aux.z, 1u));
+        DBody ss = split_body(ps, (float)max(w.hot[r.y].aux.z, 1u));
+        if (dbody_inert(pf)) {
+            pf = dbody_frozen(pf);
+            sf = dbody_frozen(sf);
+        }
+        if (dbody_inert(ps)) {
+            ps = dbody_frozen(ps);
+            ss = dbody_frozen(ss);
+        }
+        if (dbody_inert(pf) && dbody_inert(ps)) continue;
+        DBody first = pf, second = ps;
+        float4 nf = w.cur.normal[i];
+        f3 normal = xyz(nf);
+        float friction = nf.w;
+        float4 mat = w.cur.mat[i];
+        f3 t1, t2;
+        make_tangents(normal, &t1, &t2);
+        uint32_t pc = r.z & 0xFFu;
+        f3 la[4], lb[4], af[4], as[4];
+        float4 acc[4];
+        float depth[4], target[4];
+        f3 reach_f = s3(0.0f), reach_s = s3(0.0f);
+        float normal_total = 0.0f;
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            size_t o = (size_t)pi * cap + i;
+            float4 a4 = w.cur.la[o], b4 = w.cur.lb[o];
+            la[pi] = xyz(a4);
+            lb[pi] = xyz(b4);
+            depth[pi] = a4.w;
+            target[pi] = b4.w;
+            acc[pi] = w.cur.acc[o];
+            af[pi] = arm(pf, la[pi]);
+            as[pi] = arm(ps, lb[pi]);
+            reach_f = reach_f + (af[pi] - dbody_com(pf));
+            reach_s = reach_s + (as[pi] - dbody_com(ps));
+        }
+        for (uint32_t pi = 0; pi < pc; ++pi) normal_total = normal_total + wmax(acc[pi].x, 0.0f);
+        float count_f = (float)max(pc, 1u);
+        f3 impulses[4];
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            float an = acc[pi].x, at1 = acc[pi].y, at2 = acc[pi].z;
+            f3 rel = relative_velocity(pf, ps, af[pi], as[pi]);
+            float normal_speed = dot(rel, normal);
+            f3 arm_f = cross(af[pi] - dbody_com(sf), normal);
+            f3 arm_s = cross(as[pi] - dbody_com(ss), normal);
+            float normal_mass = count_f * (sf.inverse_mass + ss.inverse_mass) + dot(dbody_iinv(sf, cross(reach_f, normal)), arm_f)
+                + dot(dbody_iinv(ss, cross(reach_s, normal)), arm_s);
+            float truth = momentum_mass(pf, ps, af[pi], as[pi], normal);
+            float delta;
+            if (mat.z <= 0.0f) {
+                delta = (target[pi] - normal_speed) / normal_mass;
+            } else {
+                float bias = wmax(depth[pi] / p.dt, target[pi]);
+                float drag = 2.0f * mat.w * mat.z / p.dt;
+                float softness = mat.z * mat.z * truth / (p.dt * p.dt);
+                float prior = normal_speed - an * truth;
+                float wanted = (bias - (1.0f + drag) * prior) / (softness + (1.0f + drag) * truth);
+                delta = truth * (wanted - an) / normal_mass;
+            }
+            float next_n = wmax(0.0f, an + delta);
+            impulses[pi] = s3(0.0f) + normal * (next_n - an);
+            an = next_n;
+            float limit = friction * an;
+            float t1_mass = momentum_mass(sf, ss, af[pi], as[pi], t1) * count_f;
+            float t1_speed = dot(relative_velocity(pf, ps, af[pi], as[pi]), t1);
+            float next_t1 = wclamp(at1 - t1_speed / t1_mass, -limit, limit);
+            impulses[pi] = impulses[pi] + t1 * (next_t1 - at1);
+            at1 = next_t1;
+            float t2_mass = momentum_mass(sf, ss, af[pi], as[pi], t2) * count_f;
+            float t2_speed = dot(relative_velocity(pf, ps, af[pi], as[pi]), t2);
+            float remaining = sqrtf(wmax(limit * limit - at1 * at1, 0.0f));
+            float next_t2 = wclamp(at2 - t2_speed / t2_mass, -remaining, remaining);
+            impulses[pi] = impulses[pi] + t2 * (next_t2 - at2);
+            at2 = next_t2;
+            acc[pi] = make_float4(an, at1, at2, acc[pi].w);
+        }
+        for (uint32_t pi = 0; pi < pc; ++pi) pair_impulse(&first, &second, af[pi], as[pi], impulses[pi]);
+        f3 rel_spin = second.angular_velocity - first.angular_velocity;
+        f3 planar = rel_spin - normal * dot(rel_spin, normal);
+        float planar_len = length(planar);
+        if (planar_len > 1e-6f) {
+            f3 axis = planar / planar_len;
+            float mass = dot(axis, dbody_iinv(sf, axis)) + dot(axis, dbody_iinv(ss, axis));
+            if (mass > 0.0f) {
+                float limit = mat.x * normal_total;
+                float applied = wclamp(-planar_len / mass, -limit, limit);
+                first.angular_velocity = first.angular_velocity - dbody_iinv(first, axis * applied);
+                second.angular_velocity = second.angular_velocity + dbody_iinv(second, axis * applied);
+            }
+        }
+        float twist = dot(rel_spin, normal);
+        if (fabsf(twist) > 1e-6f) {
+            float mass = dot(normal, dbody_iinv(sf, normal)) + dot(normal, dbody_iinv(ss, normal));
+            if (mass > 0.0f) {
+                float limit = mat.y * normal_total;
+                float applied = wclamp(-twist / mass, -limit, limit);
+                first.angular_velocity = first.angular_velocity - dbody_iinv(first, normal * applied);
+                second.angular_velocity = second.angular_velocity + dbody_iinv(second, normal * applied);
+            }
+        }
+        for (uint32_t pi = 0; pi < pc; ++pi) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
+        f3 da = first.velocity - pf.velocity, sa = first.angular_velocity - pf.angular_velocity;
+        f3 db = second.velocity - ps.velocity, sb = second.angular_velocity - ps.angular_velocity;
+        accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
+        accumulate(w.vdelta, r.y, db, sb, DYN_SOLVER_VELOCITY_SCALE);
+        if (residual) {
+            max_counter(&w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL],
+                        (uint32_t)solver_word(wmax(length(da), length(db)), DYN_SOLVER_VELOCITY_SCALE));
+            max_counter(&w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL],
+                        (uint32_t)solver_word(wmax(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE));
+        }
+    }
+}
+
+// solver_block_apply.wgsl:7-29
+__global__ void k_vapply(DeviceWorld w) {
+    const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && rows > 0u) w.ctl[CTL_ROUNDS] += 1u;
+    GRID_STRIDE(i, rows) {
+        uint32_t row = w.solver_rows[i];
+        int4* d = reinterpret_cast<int4*>(w.vdelta + 8u * row);
+        int4 a = d[0], b = d[1];
+        d[0] = make_int4(0, 0, 0, 0);
+        d[1] = make_int4(0, 0, 0, 0);
+        f3 lin = mk3((float)a.x / DYN_SOLVER_VELOCITY_SCALE, (float)a.y / DYN_SOLVER_VELOCITY_SCALE,
+                     (float)a.z / DYN_SOLVER_VELOCITY_SCALE);
+        f3 ang = mk3((float)a.w / DYN_SOLVER_VELOCITY_SCALE, (float)b.x / DYN_SOLVER_VELOCITY_SCALE,
+                     (float)b.y / DYN_SOLVER_VELOCITY_SCALE);
+        if (is_zero3(lin) && is_zero3(ang)) continue;
+        BodyHot& h = w.hot[row];
+        float4 v = h.vel, av = h.ang;
+        h.vel = make_float4(v.x + lin.x, v.y + lin.y, v.z + lin.z, v.w);
+        h.ang = make_float4(av.x + ang.x, av.y + ang.y, av.z + ang.z, av.w);
+    }
+}
+
+// substep_integrate.wgsl:15-76 (no force fields)
+__global__ void k_integrate(DeviceWorld w, dyn_step_params p) {
+    const uint32_t live = w.ctl[CTL_LIVE];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && live > 0u) w.ctl[CTL_ROUNDS] = 0u;
+    const float h = p.substep_dt;
+    GRID_STRIDE(i, live) {
+        uint32_t row = w.live[i];
+        BodyHot& b = w.hot[row];
+        float im = b.pos.w;
+        uint32_t flags = b.aux.y;
+        if (!simulates(im, flags)) continue;
+        float4 q = b.rot;
+        float4 dm = w.damp[row];
+        f3 force = xyz(w.force[row]), torque = xyz(w.torque[row]);
+        f3 acceleration = mk3(p.gravity[0], p.gravity[1], p.gravity[2]) * dm.z + force * im;
+        f3 spin = xyz(b.ang);
+        f3 velocity = xyz(b.vel) + acceleration * h;
+        float4 ii0 = b.ii0;
+        float2 ii1 = make_float2(b.ii1.x, b.ii1.y);
+        float4 I0 = w.inert0[row];
+        float2 I1 = w.inert1[row];
+        f3 gyro = spin;
+        bool isotropic = I0.y == 0.0f && I0.z == 0.0f && I1.x == 0.0f && I0.x == I0.w && I0.w == I1.y;
+        if (!isotropic) {
+            f3 body_spin = quat_rotate(quat_conj(q), spin);
+            f3 momentum = sym_apply(I0, I1, body_spin);
+            if (!is_zero3(cross(body_spin, momentum))) {
+                f3 solved = momentum;
+                for (int it = 0; it < 4; ++it) {
+                    f3 mid = 0.5f * (momentum + solved);
+                    solved = rotate_about(-sym_apply(ii0, ii1, mid) * h, momentum);
+                }
+                gyro = quat_rotate(q, sym_apply(ii0, ii1, solved));
+            }
+        }
+        f3 angular = gyro + inv_inertia_world(ii0, ii1, q, torque * h);
+        float speed = length(velocity);
+        if (speed > p.max_velocity) velocity = velocity * (p.max_velocity / speed);
+        float spin_speed = length(angular);
+        if (spin_speed > p.max_angular_velocity) angular = angular * (p.max_angular_velocity / spin_speed);
+        velocity = velocity / (1.0f + dm.x * h);
+        angular = angular / (1.0f + dm.y * h);
+        b.vel = mk4(velocity, 0.0f);
+        b.ang = mk4(angular, 0.0f);
+    }
+}
+
+// substep_advance.wgsl:6-13
+__global__ void k_advance(DeviceWorld w, dyn_step_params p) {
+    const uint32_t live = w.ctl[CTL_LIVE];
+    const float h = p.substep_dt;
+    GRID_STRIDE(i, live) {
+        uint32_t row = w.live[i];
+        BodyHot& b = w.hot[row];
+        f3 pos = xyz(b.pos) + xyz(b.vel) * h;
+        float4 q = b.rot;
+        f3 av = xyz(b.ang);
+        float4 spin = make_float4(av.x, av.y, av.z, 0.0f);
+        b.pos = mk4(pos, b.pos.w);
+        b.rot = normalize4(add4(q, scale4(0.5f * h, quat_mul(spin, q))));
+    }
+}
+
+// position_correction.wgsl:5-46 with position_block.wgsl:11-33
+__global__ void k_position(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const uint32_t cap = w.c_cap;
+    GRID_STRIDE(i, count) {
+        uint4 r = w.cur.rows[i];
+        if (!resolves(r)) continue;
+        float4 mat = w.cur.mat[i];
+        if (mat.z > 0.0f) continue;
+        const BodyHot& ha = w.hot[r.x];
+        const BodyHot& hb = w.hot[r.y];
+        float ima = (!simulates(ha.pos.w, ha.aux.y) || ha.aux.x != 0u) ? 0.0f : ha.pos.w;
+        float imb = (!simulates(hb.pos.w, hb.aux.y) || hb.aux.x != 0u) ? 0.0f : hb.pos.w;
+        f3 normal = xyz(w.cur.normal[i]);
+        float resolved = dot(normal, xyz(w.resolution[r.y]) - xyz(w.resolution[r.x]));
+        f3 total = s3(0.0f);
+        uint32_t contributing = 0;
+        uint32_t pc = r.z & 0xFFu;
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            float error = wmax(w.cur.la[(size_t)pi * cap + i].w - p.slop - resolved, 0.0f);
+            if (error <= 0.0f) continue;
+            float k = ima + imb;
+            if (k == 0.0f) continue;
+            total = total + normal * (p.relaxation * error / k);
+            contributing += 1;
+        }
+        if (contributing == 0u) continue;
+        f3 correction = total / (float)contributing;
+        f3 la = -correction * ima;
+        f3 lb = correction * imb;
+        if (!(dot(la, la) > 0.0f || dot(lb, lb) > 0.0f)) continue;
+        atomicAdd(&w.contributions[r.x], 1u);
+        atomicAdd(&w.contributions[r.y], 1u);
+        accumulate(w.pdelta, r.x, la, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        accumulate(w.pdelta, r.y, lb, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+    }
+}
+
+// position_apply.wgsl:12-27
+__global__ void k_papply(DeviceWorld w) {
+    const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
+    GRID_STRIDE(i, rows) {
+        uint32_t row = w.solver_rows[i];
+        uint32_t contributing = w.contributions[row];
+        w.contributions[row] = 0u;
+        int4* d = reinterpret_cast<int4*>(w.pdelta + 8u * row);
+        int4 a = d[0], b = d[1];
+        d[0] = make_int4(0, 0, 0, 0);
+        d[1] = make_int4(0, 0, 0, 0);
+        if (contributing == 0u) continue;
+        f3 lin = mk3((float)a.x / DYN_SOLVER_POSITION_SCALE, (float)a.y / DYN_SOLVER_POSITION_SCALE,
+                     (float)a.z / DYN_SOLVER_POSITION_SCALE);
+        f3 ang = mk3((float)a.w / DYN_SOLVER_POSITION_SCALE, (float)b.x / DYN_SOLVER_POSITION_SCALE,
+                     (float)b.y / DYN_SOLVER_POSITION_SCALE);
+        f3 al = lin / (float)contributing;
+        f3 aa = ang / (float)contributing;
+        BodyHot& h = w.hot[row];
+        f3 pos = xyz(h.pos) + al;
+        h.pos = mk4(pos, h.pos.w);
+        f3 ha = aa * 0.5f;
+        h.rot = normalize4(quat_mul(make_float4(ha.x, ha.y, ha.z, 1.0f), h.rot));
+        float4 res = w.resolution[row];
+        w.resolution[row] = make_float4(res.x + al.x, res.y + al.y, res.z + al.z, 0.0f);
+    }
+}
+
+// island_sleep.wgsl:10-29, then commit (contact_archive + archive_count_sync).
+__global__ void k_sleep(DeviceWorld w, dyn_step_params p) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.ctl[CTL_ARCHIVED] = w.ctl[CTL_CONTACTS];
+        w.counters[DYN_COUNTER_ARCHIVED] = w.ctl[CTL_CONTACTS];
+        w.counters[DYN_COUNTER_LIVE] = w.ctl[CTL_LIVE];
+        w.counters[DYN_COUNTER_SOLVER_ROWS] = w.ctl[CTL_SOLVER_ROWS];
+        w.counters[DYN_COUNTER_STEP] += 1u;
+    }
+    GRID_STRIDE(i, w.nd) {
+        BodyHot& h = w.hot[i];
+        if (h.aux.x != 0u || !simulates(h.pos.w, h.aux.y)) continue;
+        uint32_t root = w.parents[i];
+        bool disturbed = (w.istate[root] & DYN_ISLAND_WAKE) != 0u || w.wake_flags[i] != 0u;
+        if (disturbed) {
+            w.sleep_timer[i] = 0.0f;
+        } else {
+            float t = w.sleep_timer[i] + p.dt;
+            if (t >= p.sleep_time) {
+                h.vel = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                h.ang = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                w.force[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                w.torque[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                w.prev_pos[i] = make_float4(h.pos.x, h.pos.y, h.pos.z, 0.0f);
+                w.prev_rot[i] = h.rot;
+                t = 0.0f;
+                h.aux.x = 1u;
+                add_counter(&w.counters[DYN_COUNTER_SLEPT], 1u);
+            }
+            w.sleep_timer[i] = t;
+        }
+    }
+}
+
+}  // namespace dyn

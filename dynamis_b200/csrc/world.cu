@@ -1,0 +1,985 @@
+// world.cu - device side of the C ABI: HBM allocation, record conversion, the step as a CUDA
+// graph, readback and the parity hooks.
+//
+// The step replays one captured graph per (dt, archive parity): the current and archived contact
+// sets swap roles every step (contact_archive.wgsl copies instead), so two graphs alternate.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "step.cuh"
+#include "world.h"
+
+namespace dyn {
+
+enum Stage : uint32_t {
+    ST_BEGIN = 0,
+    ST_AABB,
+    ST_ENTRIES,
+    ST_ENTRY_SORT,
+    ST_PAIRS,
+    ST_PAIR_SORT,
+    ST_NARROWPHASE,
+    ST_COMPACT,
+    ST_IDENTITY,
+    ST_ISLANDS,
+    ST_WAKE_LIVE,
+    ST_SOLVER_PREPARE,
+    ST_INTEGRATE,
+    ST_WARM,
+    ST_VELOCITY,
+    ST_ADVANCE,
+    ST_POSITION,
+    ST_SLEEP,
+    ST_COUNT
+};
+static const char* kStageNames[ST_COUNT] = {"begin",       "aabb",     "entries",   "entry_sort",     "pairs",
+                                            "pair_sort",   "narrowphase", "compact", "identity",       "islands",
+                                            "wake_live",   "solver_prepare", "integrate", "warm_start", "velocity",
+                                            "advance",     "position", "sleep"};
+
+struct DeviceState {
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    DeviceWorld dw{};
+    std::vector<void*> allocs;
+    uint32_t n_cap = 0, k_cap = 0, e_cap = 0, p_cap = 0, c_cap = 0;
+    uint32_t src_cap = 0, vert_cap = 0;
+    dyn_shape_source_record* sources = nullptr;
+    float4* vertices = nullptr;
+    // sort and scan scratch
+    uint32_t* hist = nullptr;          // 8 x 256
+    uint32_t* tile_counters = nullptr; // 16
+    uint32_t* lookback = nullptr;
+    size_t lookback_words = 0;
+    uint32_t* sort_alt0 = nullptr;  // operator scratch (dyn_radix_sort)
+    uint32_t* sort_alt1 = nullptr;
+    uint32_t* sort_alt2 = nullptr;
+    uint32_t sort_alt_cap = 0;
+    // graphs
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    float graph_dt = -1.0f;
+    uint32_t parity = 0;  // which contact set is current for the next step
+    uint32_t last_parity = 0;
+    bool stepped = false;
+    uint32_t graph_kernels = 0;  // kernel nodes in one step's graph
+    dyn_step_params params{};
+    // timing
+    std::vector<cudaEvent_t> events;
+    std::vector<uint32_t> event_stage;
+    float stage_ms[ST_COUNT] = {0};
+};
+
+namespace {
+
+#define DYN_CUDA(call)                                                                                  \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+dyn_status alloc(dyn_world* w, DeviceState* d, T** out, size_t count) {
+    void* p = nullptr;
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    DYN_CUDA(cudaMalloc(&p, bytes));
+    DYN_CUDA(cudaMemsetAsync(p, 0, bytes, d->stream));
+    d->allocs.push_back(p);
+    *out = static_cast<T*>(p);
+    return DYN_OK;
+}
+
+dyn_status alloc_contacts(dyn_world* w, DeviceState* d, ContactSet* s, uint32_t cap) {
+    dyn_status st;
+    if ((st = alloc(w, d, &s->normal, cap))) return st;
+    if ((st = alloc(w, d, &s->rows, cap))) return st;
+    if ((st = alloc(w, d, &s->mat, cap))) return st;
+    if ((st = alloc(w, d, &s->ids, cap))) return st;
+    if ((st = alloc(w, d, &s->ids2, cap))) return st;
+    if ((st = alloc(w, d, &s->extra, cap))) return st;
+    if ((st = alloc(w, d, &s->la, (size_t)4 * cap))) return st;
+    if ((st = alloc(w, d, &s->lb, (size_t)4 * cap))) return st;
+    if ((st = alloc(w, d, &s->acc, (size_t)4 * cap))) return st;
+    if ((st = alloc(w, d, &s->pos, (size_t)4 * cap))) return st;
+    return DYN_OK;
+}
+
+uint32_t key_words(uint32_t n) {
+    uint32_t m = n > 0 ? n - 1 : 0;
+    uint32_t bits = m == 0 ? 0 : 32 - (uint32_t)__builtin_clz(m);
+    uint32_t words = (bits + 7) / 8;
+    return words < 1 ? 1 : (words > 4 ? 4 : words);
+}
+inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+inline uint32_t blocks_for(uint32_t n, uint32_t threads) {
+    uint32_t b = div_up(std::max<uint32_t>(n, 1), threads);
+    return std::min<uint32_t>(b, 148u * 16u);
+}
+
+void release_graphs(DeviceState* d) {
+    for (auto& e : d->exec) {
+        if (e) cudaGraphExecDestroy(e);
+        e = nullptr;
+    }
+    d->graph_dt = -1.0f;
+}
+
+// Allocates HBM for the current scene (capacities are the larger of declared and needed).
+dyn_status ensure_device(dyn_world* w) {
+    rebuild_rows(w);
+    uint32_t n = (uint32_t)w->states.size();
+    uint32_t k = (uint32_t)w->colliders.size();
+    std::vector<float> verts;
+    std::vector<dyn_shape_source_record> srcs = shape_sources(w, &verts);
+    uint32_t ns = (uint32_t)srcs.size(), nv = (uint32_t)(verts.size() / 4);
+    DeviceState* d = w->dev;
+    bool fits = d && n <= d->n_cap && k <= d->k_cap && ns <= d->src_cap && nv <= d->vert_cap;
+    if (!fits) {
+        if (d) destroy_device(w);
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(w, DYN_ERR_NO_DEVICE, "no CUDA device");
+        if (w->device < 0 || w->device >= count) return fail(w, DYN_ERR_NO_DEVICE, "CUDA device ordinal out of range");
+        DYN_CUDA(cudaSetDevice(w->device));
+        // the GJK/EPA frames of the narrowphase live in per-thread local memory
+        DYN_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 16384));
+        d = new DeviceState();
+        w->dev = d;
+        DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
+        d->stream = d->own_stream;
+        d->n_cap = std::max(n, w->capacity.bodies);
+        d->k_cap = std::max(k, w->capacity.colliders);
+        d->e_cap = 8u * std::max(d->k_cap, 1u);
+        d->p_cap = w->capacity.pairs ? w->capacity.pairs : 16u * std::max(d->k_cap, 64u);
+        d->c_cap = w->capacity.contacts ? w->capacity.contacts : 8u * std::max(d->k_cap, 64u);
+        d->src_cap = std::max(ns, 1u);
+        d->vert_cap = std::max(nv, 1u);
+        DeviceWorld& dw = d->dw;
+        dyn_status st;
+#define A(ptr, count) if ((st = alloc(w, d, &(ptr), (count)))) return st
+        uint32_t N = d->n_cap, K = d->k_cap, E = d->e_cap, P = d->p_cap, C = d->c_cap;
+        A(dw.hot, N);
+        A(dw.prev_pos, N);
+        A(dw.prev_rot, N);
+        A(dw.force, N);
+        A(dw.torque, N);
+        A(dw.ident, N);
+        A(dw.sleep_timer, N);
+        A(dw.damp, N);
+        A(dw.thresh, N);
+        A(dw.inert0, N);
+        A(dw.inert1, N);
+        A(dw.activity, N);
+        A(dw.motion, N);
+        A(dw.wake_flags, N);
+        A(dw.row_of_id, N);
+        A(dw.c_owner, K);
+        A(dw.c_kind, K);
+        A(dw.c_offset, K);
+        A(dw.c_lrot, K);
+        A(dw.c_half, K);
+        A(dw.c_mat, K);
+        A(dw.c_mat2, K);
+        A(dw.c_filter, K);
+        A(dw.c_scale, K);
+        A(d->sources, d->src_cap);
+        A(d->vertices, d->vert_cap);
+        A(dw.aabb, 2 * (size_t)K);
+        A(dw.c_level, K);
+        A(dw.entry_count, K);
+        A(dw.entry_offset, K);
+        A(dw.ekey, E);
+        A(dw.eval, E);
+        A(dw.ekey_alt, E);
+        A(dw.eval_alt, E);
+        A(dw.entries, 2 * (size_t)E);
+        A(dw.pmaj, P);
+        A(dw.pmin, P);
+        A(dw.pmaj_alt, P);
+        A(dw.pmin_alt, P);
+        A(dw.pair_slot, P);
+        A(dw.pair_flag, P);
+        A(dw.pair_rank, P);
+        A(dw.matched, C);
+        A(dw.parents, N);
+        A(dw.istate, N);
+        A(dw.live, N);
+        A(dw.solver_rows, N);
+        A(dw.vdelta, 8 * (size_t)N);
+        A(dw.pdelta, 8 * (size_t)N);
+        A(dw.contributions, N);
+        A(dw.resolution, N);
+        A(dw.counters, 64);
+        A(dw.ctl, CTL_COUNT);
+        A(d->hist, 8 * 256);
+        A(d->tile_counters, 16);
+        uint32_t max_tiles = std::max(div_up(std::max(E, P), kSortTile), 1u);
+        d->lookback_words = (size_t)8 * max_tiles * 256;
+        A(d->lookback, d->lookback_words);
+#undef A
+        if ((st = alloc_contacts(w, d, &dw.tmp, C))) return st;
+        if ((st = alloc_contacts(w, d, &dw.cur, C))) return st;
+        if ((st = alloc_contacts(w, d, &dw.arc, C))) return st;
+        dw.e_cap = E;
+        dw.p_cap = P;
+        dw.c_cap = C;
+        dw.sources = d->sources;
+        dw.vertices = d->vertices;
+    }
+    return DYN_OK;
+}
+
+// Converts the host rows to the device layout and uploads them.
+dyn_status upload_scene(dyn_world* w) {
+    dyn_status st = ensure_device(w);
+    if (st) return st;
+    DeviceState* d = w->dev;
+    DeviceWorld& dw = d->dw;
+    uint32_t n = (uint32_t)w->states.size(), k = (uint32_t)w->colliders.size();
+    dw.n = n;
+    dw.nd = w->dynamic_count;
+    dw.k = k;
+    dw.id_count = (uint32_t)w->row_of_id.size();
+    std::vector<BodyHot> hot(n);
+    std::vector<float4> prev_pos(n), prev_rot(n), force(n), torque(n), damp(n), inert0(n);
+    std::vector<uint4> ident(n);
+    std::vector<float> timer(n);
+    std::vector<float2> thresh(n), inert1(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const dyn_body_state_record& s = w->states[i];
+        const dyn_body_descriptor_record& c = w->descs[i];
+        BodyHot& h = hot[i];
+        h.pos = make_float4(s.position[0], s.position[1], s.position[2], c.inverse_mass);
+        h.rot = make_float4(s.orientation[0], s.orientation[1], s.orientation[2], s.orientation[3]);
+        h.vel = make_float4(s.velocity[0], s.velocity[1], s.velocity[2], 0.0f);
+        h.ang = make_float4(s.angular_velocity[0], s.angular_velocity[1], s.angular_velocity[2], 0.0f);
+        h.com = make_float4(c.com[0], c.com[1], c.com[2], 0.0f);
+        h.ii0 = make_float4(c.inverse_inertia[0], c.inverse_inertia[1], c.inverse_inertia[2], c.inverse_inertia[3]);
+        h.ii1 = make_float4(c.inverse_inertia[4], c.inverse_inertia[5], 0.0f, 0.0f);
+        h.aux = make_uint4(s.sleeping, c.flags, 0u, 0u);
+        prev_pos[i] = make_float4(s.prev_position[0], s.prev_position[1], s.prev_position[2], 0.0f);
+        prev_rot[i] = make_float4(s.prev_orientation[0], s.prev_orientation[1], s.prev_orientation[2], s.prev_orientation[3]);
+        force[i] = make_float4(s.force[0], s.force[1], s.force[2], 0.0f);
+        torque[i] = make_float4(s.torque[0], s.torque[1], s.torque[2], 0.0f);
+        ident[i] = make_uint4(s.body_id, s.generation, c.collision_group, c.collision_mask);
+        timer[i] = s.sleep_timer;
+        damp[i] = make_float4(c.linear_damping, c.angular_damping, c.gravity_scale, 0.0f);
+        thresh[i] = make_float2(c.sleep_velocity, c.sleep_angular_velocity);
+        inert0[i] = make_float4(c.inertia[0], c.inertia[1], c.inertia[2], c.inertia[3]);
+        inert1[i] = make_float2(c.inertia[4], c.inertia[5]);
+    }
+    std::vector<uint4> ckind(k);
+    std::vector<float4> coff(k), clrot(k), chalf(k), cmat(k), cmat2(k), cscale(k);
+    std::vector<uint2> cfilter(k);
+    for (uint32_t i = 0; i < k; ++i) {
+        const dyn_collider_record& c = w->colliders[i];
+        ckind[i] = make_uint4(c.kind, c.flags, c.source, 0u);
+        coff[i] = make_float4(c.local_offset[0], c.local_offset[1], c.local_offset[2], c.radius);
+        clrot[i] = make_float4(c.local_rotation[0], c.local_rotation[1], c.local_rotation[2], c.local_rotation[3]);
+        chalf[i] = make_float4(c.half_extents[0], c.half_extents[1], c.half_extents[2], c.half_height);
+        cmat[i] = make_float4(c.friction, c.restitution, c.rolling_friction, c.spin_friction);
+        cmat2[i] = make_float4(c.relaxation, c.damping_ratio, c.impact_force, 0.0f);
+        cfilter[i] = make_uint2(c.collision_group, c.collision_mask);
+        cscale[i] = make_float4(c.scale[0], c.scale[1], c.scale[2], 0.0f);
+    }
+    std::vector<float> verts;
+    std::vector<dyn_shape_source_record> srcs = shape_sources(w, &verts);
+    cudaStream_t s = d->stream;
+    // Host vectors live until the synchronisation at the end of this function.
+    DYN_CUDA(cudaMemcpyAsync(dw.hot, hot.data(), n * sizeof(BodyHot), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.prev_pos, prev_pos.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.prev_rot, prev_rot.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.force, force.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.torque, torque.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.ident, ident.data(), n * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.sleep_timer, timer.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.damp, damp.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.thresh, thresh.data(), n * sizeof(float2), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.inert0, inert0.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.inert1, inert1.data(), n * sizeof(float2), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.row_of_id, w->row_of_id.data(), w->row_of_id.size() * 4, cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemsetAsync(dw.wake_flags, 0, (size_t)d->n_cap * 4, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_owner, w->owners.data(), k * 4, cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_kind, ckind.data(), k * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_offset, coff.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_lrot, clrot.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_half, chalf.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_mat, cmat.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_mat2, cmat2.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_filter, cfilter.data(), k * sizeof(uint2), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.c_scale, cscale.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    if (!srcs.empty()) {
+        DYN_CUDA(cudaMemcpyAsync(d->sources, srcs.data(), srcs.size() * sizeof(dyn_shape_source_record), cudaMemcpyHostToDevice, s));
+        DYN_CUDA(cudaMemcpyAsync(d->vertices, verts.data(), verts.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    }
+    // a fresh scene has no archived contacts and no device status
+    DYN_CUDA(cudaMemsetAsync(dw.ctl, 0, CTL_COUNT * 4, s));
+    DYN_CUDA(cudaMemsetAsync(dw.counters, 0, 64 * 4, s));
+    DYN_CUDA(cudaStreamSynchronize(s));
+    d->parity = 0;
+    d->stepped = false;
+    release_graphs(d);
+    return DYN_OK;
+}
+
+dyn_status download_states(dyn_world* w, std::vector<dyn_body_state_record>* out) {
+    DeviceState* d = w->dev;
+    DeviceWorld& dw = d->dw;
+    uint32_t n = dw.n;
+    std::vector<BodyHot> hot(n);
+    std::vector<float4> prev_pos(n), prev_rot(n), force(n), torque(n);
+    std::vector<uint4> ident(n);
+    std::vector<float> timer(n);
+    cudaStream_t s = d->stream;
+    DYN_CUDA(cudaMemcpyAsync(hot.data(), dw.hot, n * sizeof(BodyHot), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaMemcpyAsync(prev_pos.data(), dw.prev_pos, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaMemcpyAsync(prev_rot.data(), dw.prev_rot, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaMemcpyAsync(force.data(), dw.force, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaMemcpyAsync(torque.data(), dw.torque, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaMemcpyAsync(ident.data(), dw.ident, n * sizeof(uint4), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaMemcpyAsync(timer.data(), dw.sleep_timer, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaStreamSynchronize(s));
+    out->resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        dyn_body_state_record& r = (*out)[i];
+        std::memset(&r, 0, sizeof(r));
+        const BodyHot& h = hot[i];
+        r.position[0] = h.pos.x;
+        r.position[1] = h.pos.y;
+        r.position[2] = h.pos.z;
+        r.prev_position[0] = prev_pos[i].x;
+        r.prev_position[1] = prev_pos[i].y;
+        r.prev_position[2] = prev_pos[i].z;
+        r.prev_orientation[0] = prev_rot[i].x;
+        r.prev_orientation[1] = prev_rot[i].y;
+        r.prev_orientation[2] = prev_rot[i].z;
+        r.prev_orientation[3] = prev_rot[i].w;
+        r.orientation[0] = h.rot.x;
+        r.orientation[1] = h.rot.y;
+        r.orientation[2] = h.rot.z;
+        r.orientation[3] = h.rot.w;
+        r.velocity[0] = h.vel.x;
+        r.velocity[1] = h.vel.y;
+        r.velocity[2] = h.vel.z;
+        r.angular_velocity[0] = h.ang.x;
+        r.angular_velocity[1] = h.ang.y;
+        r.angular_velocity[2] = h.ang.z;
+        r.force[0] = force[i].x;
+        r.force[1] = force[i].y;
+        r.force[2] = force[i].z;
+        r.torque[0] = torque[i].x;
+        r.torque[1] = torque[i].y;
+        r.torque[2] = torque[i].z;
+        r.body_id = ident[i].x;
+        r.generation = ident[i].y;
+        r.sleep_timer = timer[i];
+        r.sleeping = h.aux.x;
+    }
+    return DYN_OK;
+}
+
+// Stable LSD sort launches on `s` (see sort.cuh). Data ends in the primary buffers.
+void record_sort(DeviceState* d, cudaStream_t s, uint32_t* major, uint32_t* minor, uint32_t* val, uint32_t* major_alt,
+                 uint32_t* minor_alt, uint32_t* val_alt, const uint32_t* count_ptr, uint32_t n_fixed, uint32_t cap,
+                 uint32_t major_digits, uint32_t minor_digits) {
+    uint32_t passes = major_digits + minor_digits;
+    if (passes == 0) return;
+    uint32_t tiles = std::max(div_up(cap, kSortTile), 1u);
+    cudaMemsetAsync(d->hist, 0, passes * 256 * 4, s);
+    cudaMemsetAsync(d->tile_counters, 0, 16 * 4, s);
+    cudaMemsetAsync(d->lookback, 0, (size_t)passes * tiles * 256 * 4, s);
+    k_sort_histogram<<<std::min(div_up(cap, 256), 148u * 4u), 256, 0, s>>>(major, minor, count_ptr, n_fixed, cap,
+                                                                            (int)major_digits, (int)minor_digits, d->hist);
+    k_sort_offsets<<<1, 256, 0, s>>>(d->hist, (int)passes);
+    uint32_t* src_major = major;
+    uint32_t* src_minor = minor;
+    uint32_t* src_val = val;
+    uint32_t* dst_major = major_alt;
+    uint32_t* dst_minor = minor_alt;
+    uint32_t* dst_val = val_alt;
+    bool two = minor != nullptr;
+    for (uint32_t p = 0; p < passes; ++p) {
+        bool on_minor = p < minor_digits;
+        int shift = 8 * (int)(on_minor ? p : p - minor_digits);
+        uint32_t* key_in = on_minor ? src_minor : src_major;
+        uint32_t* key_out = on_minor ? dst_minor : dst_major;
+        uint32_t* oth_in = on_minor ? src_major : src_minor;
+        uint32_t* oth_out = on_minor ? dst_major : dst_minor;
+        uint32_t* lb = d->lookback + (size_t)p * tiles * 256;
+        uint32_t* status = d->dw.ctl + CTL_STATUS;
+        if (two && val) {
+            k_onesweep<true, true><<<tiles, kSortThreads, 0, s>>>(key_in, oth_in, src_val, key_out, oth_out, dst_val, count_ptr,
+                                                                   n_fixed, cap, shift, d->hist + p * 256, lb,
+                                                                   d->tile_counters + p, status);
+        } else if (two) {
+            k_onesweep<true, false><<<tiles, kSortThreads, 0, s>>>(key_in, oth_in, nullptr, key_out, oth_out, nullptr, count_ptr,
+                                                                    n_fixed, cap, shift, d->hist + p * 256, lb,
+                                                                    d->tile_counters + p, status);
+        } else if (val) {
+            k_onesweep<false, true><<<tiles, kSortThreads, 0, s>>>(key_in, nullptr, src_val, key_out, nullptr, dst_val, count_ptr,
+                                                                    n_fixed, cap, shift, d->hist + p * 256, lb,
+                                                                    d->tile_counters + p, status);
+        } else {
+            k_onesweep<false, false><<<tiles, kSortThreads, 0, s>>>(key_in, nullptr, nullptr, key_out, nullptr, nullptr,
+                                                                     count_ptr, n_fixed, cap, shift, d->hist + p * 256, lb,
+                                                                     d->tile_counters + p, status);
+        }
+        std::swap(src_major, dst_major);
+        std::swap(src_minor, dst_minor);
+        std::swap(src_val, dst_val);
+    }
+    if (passes % 2 == 1) {
+        // odd pass count: results sit in the alternate buffers
+        size_t bytes = (size_t)cap * 4;
+        cudaMemcpyAsync(major, src_major, bytes, cudaMemcpyDeviceToDevice, s);
+        if (two) cudaMemcpyAsync(minor, src_minor, bytes, cudaMemcpyDeviceToDevice, s);
+        if (val) cudaMemcpyAsync(val, src_val, bytes, cudaMemcpyDeviceToDevice, s);
+    }
+}
+
+void record_scan(DeviceState* d, cudaStream_t s, const uint32_t* in, uint32_t* out, const uint32_t* count_ptr,
+                 uint32_t n_fixed, uint32_t cap, uint32_t* total) {
+    uint32_t tiles = std::max(div_up(cap, kSortTile), 1u);
+    cudaMemsetAsync(d->tile_counters + 15, 0, 4, s);
+    cudaMemsetAsync(d->lookback, 0, (size_t)tiles * 4, s);
+    k_scan_exclusive<<<tiles, kSortThreads, 0, s>>>(in, out, count_ptr, n_fixed, cap, total, d->lookback, d->tile_counters + 15,
+                                                    d->dw.ctl + CTL_STATUS);
+}
+
+struct Marker {
+    DeviceState* d;
+    cudaStream_t s;
+    bool timed;
+    void operator()(uint32_t stage) {
+        if (!timed) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        d->events.push_back(e);
+        d->event_stage.push_back(stage);
+    }
+};
+
+// Issues one step's kernels on `s`. parity selects which contact set is current.
+void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
+    DeviceState* d = w->dev;
+    DeviceWorld dw = d->dw;
+    if (parity) std::swap(dw.cur, dw.arc);
+    const dyn_step_params p = d->params;
+    Marker mark{d, s, timed};
+    const uint32_t N = std::max(dw.n, 1u), K = std::max(dw.k, 1u), ND = std::max(dw.nd, 1u);
+    const uint32_t E = dw.e_cap, P = dw.p_cap, C = dw.c_cap;
+    mark(ST_BEGIN);
+    k_reset<<<1, 64, 0, s>>>(dw);
+    k_begin<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+    mark(ST_AABB);
+    k_aabb<<<blocks_for(K, 128), 128, 0, s>>>(dw, p);
+    mark(ST_ENTRIES);
+    k_entry_count<<<blocks_for(K, 256), 256, 0, s>>>(dw);
+    record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, std::max(dw.k, 1u), dw.ctl + CTL_ENTRIES);
+    k_entry_emit<<<blocks_for(K, 256), 256, 0, s>>>(dw);
+    mark(ST_ENTRY_SORT);
+    record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
+    mark(ST_PAIRS);
+    k_pairs<<<blocks_for(E, 256), 256, 0, s>>>(dw);
+    mark(ST_PAIR_SORT);
+    uint32_t words = key_words(std::max(dw.k, 1u));
+    record_sort(d, s, dw.pmaj, dw.pmin, nullptr, dw.pmaj_alt, dw.pmin_alt, nullptr, dw.counters + DYN_COUNTER_PAIRS, 0, P,
+                words, words);
+    mark(ST_NARROWPHASE);
+    k_narrowphase<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    mark(ST_COMPACT);
+    record_scan(d, s, dw.pair_flag, dw.pair_rank, dw.counters + DYN_COUNTER_PAIRS, 0, P, dw.ctl + CTL_VALID);
+    k_compact<<<blocks_for(P, 256), 256, 0, s>>>(dw);
+    mark(ST_IDENTITY);
+    k_relay<<<blocks_for(C, 128), 128, 0, s>>>(dw);
+    k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    mark(ST_ISLANDS);
+    k_island_link<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    uint32_t rounds = 32u - (uint32_t)__builtin_clz(std::max(dw.nd, 2u));
+    for (uint32_t r = 0; r < rounds; ++r) k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    k_island_aggregate<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    mark(ST_WAKE_LIVE);
+    k_wake_live<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    mark(ST_SOLVER_PREPARE);
+    k_solver_blocks<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    for (uint32_t sub = 0; sub < p.substeps; ++sub) {
+        mark(ST_INTEGRATE);
+        k_integrate<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+        if (sub == 0) {
+            mark(ST_WARM);
+            k_warm<<<blocks_for(C, 128), 128, 0, s>>>(dw);
+            k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+        }
+        mark(ST_VELOCITY);
+        for (uint32_t it = 0; it < p.solve_iterations; ++it) {
+            k_solve<<<blocks_for(C, 128), 128, 0, s>>>(dw, p);
+            k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+        }
+        mark(ST_ADVANCE);
+        k_advance<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+        mark(ST_POSITION);
+        for (uint32_t it = 0; it < p.position_iterations; ++it) {
+            k_position<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+            k_papply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+        }
+    }
+    mark(ST_SLEEP);
+    k_sleep<<<blocks_for(ND, 256), 256, 0, s>>>(dw, p);
+    mark(ST_COUNT);
+}
+
+dyn_status prepare_step(dyn_world* w, float dt) {
+    if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(w, DYN_ERR_INVALID, "a step timestep must be positive");
+    bool fresh = !w->dev || (w->rows_dirty && !w->raw_rows);
+    if (fresh && w->dev && w->dev->stepped) {
+        // bodies spawned after stepping: keep the simulated states of the existing bodies
+        std::vector<dyn_body_state_record> now;
+        dyn_status st = download_states(w, &now);
+        if (st) return st;
+        for (const dyn_body_state_record& s : now) {
+            if (s.body_id < w->spawn_states.size()) w->spawn_states[s.body_id] = s;
+        }
+    }
+    if (fresh) {
+        dyn_status st = upload_scene(w);
+        if (st) return st;
+    }
+    if (w->states.empty()) return fail(w, DYN_ERR_INVALID, "the world holds no bodies");
+    DeviceState* d = w->dev;
+    dyn_step_params p;
+    dyn_step_params_for(w, dt, &p);
+    if (d->graph_dt != dt) {
+        release_graphs(d);
+        d->params = p;
+        d->graph_dt = dt;
+    }
+    return DYN_OK;
+}
+
+}  // namespace
+
+void destroy_device(dyn_world* w) {
+    DeviceState* d = w->dev;
+    if (!d) return;
+    cudaSetDevice(w->device);
+    if (d->stream) cudaStreamSynchronize(d->stream);
+    release_graphs(d);
+    for (cudaEvent_t e : d->events) cudaEventDestroy(e);
+    for (void* p : d->allocs) cudaFree(p);
+    if (d->own_stream) cudaStreamDestroy(d->own_stream);
+    delete d;
+    w->dev = nullptr;
+}
+
+}  // namespace dyn
+
+using namespace dyn;
+
+extern "C" {
+
+DYN_API dyn_status dyn_world_create(const dyn_config* config, const dyn_capacity* capacity, int32_t device, dyn_world** out) {
+    if (!out) return DYN_ERR_INVALID;
+    *out = nullptr;
+    dyn_world* w = new dyn_world();
+    if (config) {
+        w->config = *config;
+    } else {
+        dyn_config_default(&w->config);
+    }
+    if (capacity) w->capacity = *capacity;
+    w->device = device;
+    const dyn_config& c = w->config;
+    if (c.substeps == 0 || c.solve_iterations == 0 || !(c.slop >= 0.0f) || !(c.contact_margin >= 0.0f)
+        || !(c.sleep_time > 0.0f) || c.friction_combine > 3 || c.restitution_combine > 3) {
+        delete w;
+        return DYN_ERR_INVALID;
+    }
+    *out = w;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_world_destroy(dyn_world* w) {
+    if (!w) return DYN_ERR_INVALID;
+    destroy_device(w);
+    delete w;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_world_set_stream(dyn_world* w, void* stream) {
+    if (!w) return DYN_ERR_INVALID;
+    if (!w->dev) {
+        dyn_status st = ensure_device(w);
+        if (st) return st;
+    }
+    w->dev->stream = stream ? static_cast<cudaStream_t>(stream) : w->dev->own_stream;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_upload_bodies(dyn_world* w, const dyn_body_state_record* states, const dyn_body_descriptor_record* descs,
+                                     uint32_t n, const dyn_collider_record* colliders, const uint32_t* owners, uint32_t k) {
+    if (!w || (n && (!states || !descs)) || (k && (!colliders || !owners)))
+        return fail(w, DYN_ERR_INVALID, "dyn_upload_bodies: null argument");
+    uint32_t dynamic = 0;
+    bool prefix = true;
+    for (uint32_t i = 0; i < n; ++i) {
+        bool dyn_row = (descs[i].flags & DYN_BODY_KINEMATIC) == 0u && descs[i].inverse_mass > 0.0f;
+        if (dyn_row) {
+            if (!prefix) return fail(w, DYN_ERR_INVALID, "dyn_upload_bodies: dynamic rows must come first");
+            ++dynamic;
+        } else {
+            prefix = false;
+        }
+    }
+    for (uint32_t i = 0; i < k; ++i) {
+        if (owners[i] != DYN_NO_BODY && owners[i] >= n) return fail(w, DYN_ERR_INVALID, "dyn_upload_bodies: owner out of range");
+        if (colliders[i].kind == DYN_SHAPE_HULL && colliders[i].source >= w->hulls.size())
+            return fail(w, DYN_ERR_INVALID, "dyn_upload_bodies: unknown hull source");
+    }
+    w->raw_rows = true;
+    w->rows_dirty = false;
+    w->states.assign(states, states + n);
+    w->descs.assign(descs, descs + n);
+    w->colliders.assign(colliders, colliders + k);
+    w->owners.assign(owners, owners + k);
+    w->dynamic_count = dynamic;
+    uint32_t max_id = 0;
+    for (uint32_t i = 0; i < n; ++i) max_id = std::max(max_id, states[i].body_id + 1);
+    w->row_of_id.assign(std::max(max_id, n), DYN_NO_BODY);
+    for (uint32_t i = 0; i < n; ++i) w->row_of_id[states[i].body_id] = i;
+    return upload_scene(w);
+}
+
+DYN_API dyn_status dyn_upload_states(dyn_world* w, const dyn_body_state_record* states, uint32_t n) {
+    if (!w || !states) return fail(w, DYN_ERR_INVALID, "dyn_upload_states: null argument");
+    rebuild_rows(w);
+    if (n != w->states.size()) return fail(w, DYN_ERR_INVALID, "dyn_upload_states: row count differs from the scene");
+    if (!w->dev) {
+        dyn_status st = upload_scene(w);
+        if (st) return st;
+    }
+    DeviceState* d = w->dev;
+    DeviceWorld& dw = d->dw;
+    cudaStream_t s = d->stream;
+    // Pose, velocities and sleep state land in the hot rows through a strided copy of each field.
+    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].pos, sizeof(BodyHot), states[0].position, sizeof(dyn_body_state_record), 12, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].rot, sizeof(BodyHot), states[0].orientation, sizeof(dyn_body_state_record), 16, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].vel, sizeof(BodyHot), states[0].velocity, sizeof(dyn_body_state_record), 12, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].ang, sizeof(BodyHot), states[0].angular_velocity, sizeof(dyn_body_state_record), 12,
+                               n, cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].aux.x, sizeof(BodyHot), &states[0].sleeping, sizeof(dyn_body_state_record), 4, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(dw.prev_pos, sizeof(float4), states[0].prev_position, sizeof(dyn_body_state_record), 12, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(dw.prev_rot, sizeof(float4), states[0].prev_orientation, sizeof(dyn_body_state_record), 16, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(dw.force, sizeof(float4), states[0].force, sizeof(dyn_body_state_record), 12, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(dw.torque, sizeof(float4), states[0].torque, sizeof(dyn_body_state_record), 12, n,
+                               cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpy2DAsync(dw.sleep_timer, sizeof(float), &states[0].sleep_timer, sizeof(dyn_body_state_record), 4, n,
+                               cudaMemcpyHostToDevice, s));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
+    if (!w) return DYN_ERR_INVALID;
+    dyn_status st = prepare_step(w, dt);
+    if (st) return st;
+    DeviceState* d = w->dev;
+    DYN_CUDA(cudaSetDevice(w->device));
+    uint32_t parity = d->parity;
+    if (w->timing) {
+        for (cudaEvent_t e : d->events) cudaEventDestroy(e);
+        d->events.clear();
+        d->event_stage.clear();
+        record_step(w, d->stream, parity, true);
+        DYN_CUDA(cudaGetLastError());
+    } else {
+        if (!d->exec[parity]) {
+            cudaGraph_t graph = nullptr;
+            cudaStream_t cap = d->own_stream;
+            DYN_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            record_step(w, cap, parity, false);
+            cudaError_t e = cudaStreamEndCapture(cap, &graph);
+            if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            size_t nodes = 0;
+            cudaGraphGetNodes(graph, nullptr, &nodes);
+            std::vector<cudaGraphNode_t> list(nodes);
+            cudaGraphGetNodes(graph, list.data(), &nodes);
+            uint32_t kernels = 0;
+            for (cudaGraphNode_t node : list) {
+                cudaGraphNodeType type;
+                if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernels;
+            }
+            d->graph_kernels = kernels;
+            e = cudaGraphInstantiate(&d->exec[parity], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        DYN_CUDA(cudaGraphLaunch(d->exec[parity], d->stream));
+    }
+    d->last_parity = parity;
+    d->parity ^= 1u;
+    d->stepped = true;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_sync(dyn_world* w) {
+    if (!w) return DYN_ERR_INVALID;
+    if (!w->dev) return DYN_OK;
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    uint32_t status = 0;
+    DYN_CUDA(cudaMemcpy(&status, w->dev->dw.ctl + CTL_STATUS, 4, cudaMemcpyDeviceToHost));
+    if (status) return fail(w, DYN_ERR_DEVICE_STATUS, "device status word " + std::to_string(status));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_device_status(dyn_world* w, uint32_t* status) {
+    if (!w || !status) return DYN_ERR_INVALID;
+    *status = 0;
+    if (!w->dev) return DYN_OK;
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    DYN_CUDA(cudaMemcpy(status, w->dev->dw.ctl + CTL_STATUS, 4, cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_download_states(dyn_world* w, dyn_body_state_record* out, uint32_t n) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    rebuild_rows(w);
+    if (!w->dev) {
+        if (n < w->states.size()) return DYN_ERR_INVALID;
+        std::memcpy(out, w->states.data(), w->states.size() * sizeof(*out));
+        return DYN_OK;
+    }
+    std::vector<dyn_body_state_record> states;
+    dyn_status st = download_states(w, &states);
+    if (st) return st;
+    if (n < states.size()) return fail(w, DYN_ERR_INVALID, "dyn_download_states: buffer too small");
+    std::memcpy(out, states.data(), states.size() * sizeof(*out));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_read_state(dyn_world* w, uint32_t body_id, dyn_body_state_record* out) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    rebuild_rows(w);
+    if (body_id >= w->row_of_id.size() || w->row_of_id[body_id] == DYN_NO_BODY) return fail(w, DYN_ERR_INVALID, "unknown body id");
+    uint32_t row = w->row_of_id[body_id];
+    if (!w->dev) {
+        *out = w->states[row];
+        return DYN_OK;
+    }
+    std::vector<dyn_body_state_record> states;
+    dyn_status st = download_states(w, &states);
+    if (st) return st;
+    *out = states[row];
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_read_counters(dyn_world* w, uint32_t* out, uint32_t n) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    uint32_t m = std::min<uint32_t>(n, DYN_COUNTER_DEVICE_COUNT);
+    if (!w->dev) {
+        std::memset(out, 0, m * 4);
+        return DYN_OK;
+    }
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    DYN_CUDA(cudaMemcpy(out, w->dev->dw.counters, m * 4, cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_debug_aabbs(dyn_world* w, dyn_aabb_record* out, uint32_t cap, uint32_t* count) {
+    if (!w || !w->dev) return DYN_ERR_INVALID;
+    DeviceWorld& dw = w->dev->dw;
+    if (count) *count = dw.k;
+    if (!out) return DYN_OK;
+    uint32_t m = std::min(cap, dw.k);
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    DYN_CUDA(cudaMemcpy(out, dw.aabb, m * sizeof(dyn_aabb_record), cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_debug_entries(dyn_world* w, uint32_t* keys, uint32_t* infos, uint32_t cap, uint32_t* count) {
+    if (!w || !w->dev) return DYN_ERR_INVALID;
+    DeviceWorld& dw = w->dev->dw;
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    uint32_t e = 0;
+    DYN_CUDA(cudaMemcpy(&e, dw.ctl + CTL_ENTRIES, 4, cudaMemcpyDeviceToHost));
+    e = std::min(e, dw.e_cap);
+    if (count) *count = e;
+    if (!keys) return DYN_OK;
+    uint32_t m = std::min(cap, e);
+    std::vector<uint32_t> order(m);
+    std::vector<float4> ent(2 * (size_t)e);
+    DYN_CUDA(cudaMemcpy(keys, dw.ekey, m * 4, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(order.data(), dw.eval, m * 4, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(ent.data(), dw.entries, 2 * (size_t)e * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (infos) {
+        for (uint32_t i = 0; i < m; ++i) {
+            float f = ent[2 * (size_t)order[i] + 1].w;
+            std::memcpy(&infos[i], &f, 4);
+        }
+    }
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_debug_pairs(dyn_world* w, uint32_t* major, uint32_t* minor, uint32_t cap, uint32_t* count) {
+    if (!w || !w->dev) return DYN_ERR_INVALID;
+    DeviceWorld& dw = w->dev->dw;
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    uint32_t p = 0;
+    DYN_CUDA(cudaMemcpy(&p, dw.counters + DYN_COUNTER_PAIRS, 4, cudaMemcpyDeviceToHost));
+    p = std::min(p, dw.p_cap);
+    if (count) *count = p;
+    if (!major) return DYN_OK;
+    uint32_t m = std::min(cap, p);
+    DYN_CUDA(cudaMemcpy(major, dw.pmaj, m * 4, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(minor, dw.pmin, m * 4, cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_debug_contacts(dyn_world* w, dyn_contact_record* out, uint32_t cap, uint32_t* count) {
+    if (!w || !w->dev) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    DeviceWorld dw = d->dw;
+    if (d->last_parity) std::swap(dw.cur, dw.arc);
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    uint32_t c = 0;
+    DYN_CUDA(cudaMemcpy(&c, dw.ctl + CTL_CONTACTS, 4, cudaMemcpyDeviceToHost));
+    if (!d->stepped) c = 0;
+    if (count) *count = c;
+    if (!out) return DYN_OK;
+    uint32_t m = std::min(cap, c);
+    uint32_t C = dw.c_cap;
+    std::vector<float4> normal(m), mat(m), extra(m), la(4 * (size_t)C), lb(4 * (size_t)C), acc(4 * (size_t)C), pos(4 * (size_t)C);
+    std::vector<uint4> rows(m), ids(m), ids2(m);
+    DYN_CUDA(cudaMemcpy(normal.data(), dw.cur.normal, m * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(mat.data(), dw.cur.mat, m * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(extra.data(), dw.cur.extra, m * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(rows.data(), dw.cur.rows, m * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(ids.data(), dw.cur.ids, m * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(ids2.data(), dw.cur.ids2, m * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(la.data(), dw.cur.la, 4 * (size_t)C * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(lb.data(), dw.cur.lb, 4 * (size_t)C * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(acc.data(), dw.cur.acc, 4 * (size_t)C * 16, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(pos.data(), dw.cur.pos, 4 * (size_t)C * 16, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < m; ++i) {
+        dyn_contact_record& r = out[i];
+        std::memset(&r, 0, sizeof(r));
+        r.a = ids[i].x;
+        r.b = ids[i].y;
+        r.point_count = rows[i].z & 0xFFu;
+        r.sensor = (rows[i].z >> 8) & 0xFFu;
+        r.first_body_id = ids[i].z;
+        r.second_body_id = ids[i].w;
+        r.first_generation = ids2[i].x;
+        r.second_generation = ids2[i].y;
+        r.normal[0] = normal[i].x;
+        r.normal[1] = normal[i].y;
+        r.normal[2] = normal[i].z;
+        r.events = rows[i].w;
+        r.surface = ids2[i].z;
+        r.triangle = ids2[i].w;
+        r.friction = normal[i].w;
+        r.restitution = extra[i].x;
+        r.rolling_friction = mat[i].x;
+        r.spin_friction = mat[i].y;
+        r.carried_normal = extra[i].y;
+        r.carried_tangent = extra[i].z;
+        r.relaxation = mat[i].z;
+        r.damping_ratio = mat[i].w;
+        for (uint32_t p = 0; p < r.point_count && p < 4; ++p) {
+            size_t o = (size_t)p * C + i;
+            dyn_manifold_point_record& q = r.points[p];
+            q.position[0] = pos[o].x;
+            q.position[1] = pos[o].y;
+            q.position[2] = pos[o].z;
+            q.depth = la[o].w;
+            q.local_a[0] = la[o].x;
+            q.local_a[1] = la[o].y;
+            q.local_a[2] = la[o].z;
+            q.local_b[0] = lb[o].x;
+            q.local_b[1] = lb[o].y;
+            q.local_b[2] = lb[o].z;
+            q.accumulated_normal = acc[o].x;
+            q.accumulated_tangent_1 = acc[o].y;
+            q.accumulated_tangent_2 = acc[o].z;
+            std::memcpy(&q.feature, &acc[o].w, 4);
+        }
+    }
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_debug_islands(dyn_world* w, uint32_t* out, uint32_t cap, uint32_t* count) {
+    if (!w || !w->dev) return DYN_ERR_INVALID;
+    DeviceWorld& dw = w->dev->dw;
+    if (count) *count = dw.nd;
+    if (!out) return DYN_OK;
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    DYN_CUDA(cudaMemcpy(out, dw.parents, std::min(cap, dw.nd) * 4, cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+DYN_API uint32_t dyn_step_kernel_count(const dyn_world* w) { return (w && w->dev) ? w->dev->graph_kernels : 0u; }
+
+DYN_API dyn_status dyn_set_timing(dyn_world* w, int32_t enabled) {
+    if (!w) return DYN_ERR_INVALID;
+    w->timing = enabled != 0;
+    return DYN_OK;
+}
+DYN_API uint32_t dyn_stage_count(void) { return ST_COUNT; }
+DYN_API const char* dyn_stage_name(uint32_t stage) { return stage < ST_COUNT ? kStageNames[stage] : ""; }
+DYN_API dyn_status dyn_stage_timings(dyn_world* w, float* ms, uint32_t n) {
+    if (!w || !ms || !w->dev) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    float acc[ST_COUNT] = {0};
+    for (size_t i = 0; i + 1 < d->events.size(); ++i) {
+        float t = 0.0f;
+        DYN_CUDA(cudaEventElapsedTime(&t, d->events[i], d->events[i + 1]));
+        uint32_t stage = d->event_stage[i];
+        if (stage < ST_COUNT) acc[stage] += t;
+    }
+    for (uint32_t i = 0; i < std::min<uint32_t>(n, ST_COUNT); ++i) ms[i] = acc[i];
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_radix_sort(dyn_world* w, uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
+                                  uint32_t major_digits, uint32_t minor_digits) {
+    if (!w || !major || major_digits > 4 || minor_digits > 4 || (minor_digits && !minor)) return DYN_ERR_INVALID;
+    if (n == 0 || major_digits + minor_digits == 0) return DYN_OK;
+    if (!w->dev) {
+        dyn_status st = ensure_device(w);
+        if (st) return st;
+    }
+    DeviceState* d = w->dev;
+    if (d->sort_alt_cap < n) {
+        for (uint32_t** p : {&d->sort_alt0, &d->sort_alt1, &d->sort_alt2}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        DYN_CUDA(cudaMalloc(&d->sort_alt0, (size_t)n * 4));
+        DYN_CUDA(cudaMalloc(&d->sort_alt1, (size_t)n * 4));
+        DYN_CUDA(cudaMalloc(&d->sort_alt2, (size_t)n * 4));
+        d->allocs.push_back(d->sort_alt0);
+        d->allocs.push_back(d->sort_alt1);
+        d->allocs.push_back(d->sort_alt2);
+        d->sort_alt_cap = n;
+    }
+    uint32_t tiles = div_up(n, kSortTile);
+    if ((size_t)(major_digits + minor_digits) * tiles * 256 > d->lookback_words) {
+        return fail(w, DYN_ERR_CAPACITY, "dyn_radix_sort: more keys than the world's sort scratch holds");
+    }
+    record_sort(d, d->stream, major, minor, payload, d->sort_alt0, minor ? d->sort_alt1 : nullptr,
+                payload ? d->sort_alt2 : nullptr, nullptr, n, n, major_digits, minor_digits);
+    DYN_CUDA(cudaGetLastError());
+    return DYN_OK;
+}
+
+}  // extern "C"

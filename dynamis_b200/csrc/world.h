@@ -1,0 +1,54 @@
+// world.h - host-side state of one world (private to libdynamis_cuda.so).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "dynamis_cuda.h"
+
+namespace dyn {
+
+struct HullSource {
+    std::vector<float> vertices;     // xyz triples, hull vertices in input order
+    std::vector<uint32_t> triangles; // outward triangles over `vertices`
+    float volume = 0.0f;
+    float centroid[3] = {0.0f, 0.0f, 0.0f};
+    float unit_second_moment[6] = {0, 0, 0, 0, 0, 0};
+};
+
+struct DeviceState;  // defined in world.cu
+
+}  // namespace dyn
+
+struct dyn_world {
+    dyn_config config{};
+    dyn_capacity capacity{};
+    int32_t device = 0;
+    std::string last_error;
+    // shape pool
+    std::vector<dyn::HullSource> hulls;
+    // scene in spawn order (body id = spawn index)
+    std::vector<dyn_body_state_record> spawn_states;
+    std::vector<dyn_body_descriptor_record> spawn_descs;
+    std::vector<dyn_collider_record> spawn_colliders;
+    std::vector<uint32_t> spawn_owner;  // body id of each collider
+    // scene as rows (dynamic rows first), rebuilt when the scene changes
+    bool rows_dirty = true;
+    bool raw_rows = false;  // scene came from dyn_upload_bodies
+    std::vector<dyn_body_state_record> states;
+    std::vector<dyn_body_descriptor_record> descs;
+    std::vector<dyn_collider_record> colliders;
+    std::vector<uint32_t> owners;
+    std::vector<uint32_t> row_of_id;
+    uint32_t dynamic_count = 0;
+    bool timing = false;
+    dyn::DeviceState* dev = nullptr;
+};
+
+namespace dyn {
+dyn_status fail(dyn_world* w, dyn_status status, const std::string& what);
+void rebuild_rows(dyn_world* w);
+std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vector<float>* vertices_xyzw);
+void destroy_device(dyn_world* w);
+}  // namespace dyn

@@ -1,0 +1,162 @@
+"""numpy views of the byte-exact Dynamis ABI records (include/dynamis_abi.h).
+
+Each dtype reproduces a WGSL storage layout of crates/dynamis-abi/abi/records.wgsl, so arrays of
+these records can be handed to the C ABI by pointer and compared field by field in tests.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+COUNTER_DEVICE_COUNT = 52
+COUNTERS = [
+    "ENTRIES", "RESTING_ENTRIES", "RESTING_LEVELS", "RESTING_REBUILD", "RESTING_SORT", "AWAKE_BASE",
+    "IMMOVABLE_ENTRIES", "IMMOVABLE_EMITTED", "IMMOVABLE_LEVELS", "ENTRY_BASE", "PAIRS", "GRID_LEVELS",
+    "CONTACTS", "ARCHIVED", "JOINTS", "EVENTS", "REFUSED_PAIRS", "REFUSED_EVENTS", "ENTRY_FAULTS",
+    "RESTING", "REFUSED_RESTING", "SLEPT", "WOKE", "ACTIVE", "WOKE_DEFERRED", "RESTING_GATHER",
+    "RESTING_INDEX", "RESTING_PENDING", "ISLANDS", "ISLAND_FAULTS", "BLOCKS", "SOLVER_ROWS",
+    "SOLVE_LINEAR_RESIDUAL", "SOLVE_ANGULAR_RESIDUAL", "COARSE_ACTIVE", "GRID_SCALE", "GRID_EXTENT",
+    "BREAKS", "PARTICLE_REACH", "COARSE_NEIGHBOURS", "LIVE", "LIVE_FAULTS", "ROW_FAULTS", "SOFT_ACTIVE",
+    "SOFT_SLEPT", "SOFT_WOKE", "REFUSED_CONTACTS", "STEP", "IMPACTS", "REFUSED_IMPACTS", "SOFT_EVENTS",
+    "REFUSED_SOFT_EVENTS",
+]
+COUNTER = {name: slot for slot, name in enumerate(COUNTERS)}
+
+SHAPE_SPHERE, SHAPE_CUBOID, SHAPE_CAPSULE, SHAPE_CYLINDER, SHAPE_HULL, SHAPE_PLANE = 1, 2, 3, 4, 5, 9
+NO_BODY = 0xFFFFFFFF
+NO_COLLISION_FILTER = 0xFFFFFFFF
+CONTACT_ANNOUNCED = 0x80000000
+
+
+def _dtype(fields, size):
+    names = [f[0] for f in fields]
+    formats = [f[1] for f in fields]
+    offsets = [f[2] for f in fields]
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": size})
+
+
+STEP_PARAMS = np.dtype([
+    ("gravity", "<f4", 4), ("dt", "<f4"), ("substep_dt", "<f4"), ("damping", "<f4"), ("angular_damping", "<f4"),
+    ("body_count", "<u4"), ("substeps", "<u4"), ("solve_iterations", "<u4"), ("constraint_count", "<u4"),
+    ("relaxation", "<f4"), ("slop", "<f4"), ("restitution_threshold", "<f4"), ("max_velocity", "<f4"),
+    ("max_angular_velocity", "<f4"), ("dynamic_count", "<u4"), ("sleep_velocity", "<f4"),
+    ("sleep_angular_velocity", "<f4"), ("sleep_time", "<f4"), ("friction_combine", "<u4"),
+    ("restitution_combine", "<u4"), ("position_iterations", "<u4"), ("contact_margin", "<f4"),
+    ("collider_count", "<u4"), ("soft_iterations", "<u4"), ("soft_substeps", "<u4"), ("particle_count", "<u4"),
+    ("element_count", "<u4"), ("soft_substep_dt", "<f4"), ("soft_body_count", "<u4"), ("attachment_count", "<u4"),
+    ("settle_velocity", "<f4"), ("observed_count", "<u4"), ("observed_joint_count", "<u4"),
+    ("character_count", "<u4"), ("vehicle_count", "<u4"), ("vehicle_wheel_count", "<u4"), ("wake_all", "<u4"),
+    ("field_count", "<u4"), ("_pad_tail", "<u4", 3),
+])
+
+
+
+def _fields(spec):
+    return [(name, (fmt, shape) if shape > 1 else fmt, off) for name, fmt, shape, off in spec]
+
+
+BODY_STATE = _dtype(_fields([
+    ("position", "<f4", 3, 0), ("prev_position", "<f4", 3, 16), ("prev_orientation", "<f4", 4, 32),
+    ("orientation", "<f4", 4, 48), ("velocity", "<f4", 3, 64), ("angular_velocity", "<f4", 3, 80),
+    ("force", "<f4", 3, 96), ("torque", "<f4", 3, 112), ("body_id", "<u4", 1, 128), ("generation", "<u4", 1, 132),
+    ("sleep_timer", "<f4", 1, 136), ("sleeping", "<u4", 1, 140),
+]), 144)
+
+BODY_DESCRIPTOR = _dtype(_fields([
+    ("inverse_mass", "<f4", 1, 0), ("linear_damping", "<f4", 1, 4), ("angular_damping", "<f4", 1, 8),
+    ("gravity_scale", "<f4", 1, 12), ("sleep_velocity", "<f4", 1, 16), ("sleep_angular_velocity", "<f4", 1, 20),
+    ("flags", "<u4", 1, 24), ("collision_group", "<u4", 1, 32), ("collision_mask", "<u4", 1, 36),
+    ("com", "<f4", 3, 48), ("inertia", "<f4", 6, 64), ("inverse_inertia", "<f4", 6, 88),
+]), 128)
+
+COLLIDER = _dtype(_fields([
+    ("slot", "<u4", 1, 0), ("kind", "<u4", 1, 4), ("flags", "<u4", 1, 8), ("radius", "<f4", 1, 12),
+    ("half_height", "<f4", 1, 16), ("relaxation", "<f4", 1, 20), ("damping_ratio", "<f4", 1, 24),
+    ("impact_force", "<f4", 1, 28), ("half_extents", "<f4", 3, 32), ("collision_group", "<u4", 1, 44),
+    ("local_offset", "<f4", 3, 48), ("collision_mask", "<u4", 1, 60), ("local_rotation", "<f4", 4, 64),
+    ("friction", "<f4", 1, 80), ("restitution", "<f4", 1, 84), ("source", "<u4", 1, 88),
+    ("rolling_friction", "<f4", 1, 92), ("scale", "<f4", 3, 96), ("spin_friction", "<f4", 1, 108),
+]), 112)
+
+SHAPE_SOURCE = _dtype(_fields([
+    ("kind", "<u4", 1, 0), ("vertex_offset", "<u4", 1, 4), ("vertex_count", "<u4", 1, 8),
+    ("triangle_offset", "<u4", 1, 12), ("node_offset", "<u4", 1, 16), ("node_count", "<u4", 1, 20),
+    ("local_min", "<f4", 3, 48), ("local_max", "<f4", 3, 64),
+]), 80)
+
+AABB = _dtype(_fields([("min", "<f4", 3, 0), ("max", "<f4", 3, 16)]), 32)
+
+MANIFOLD_POINT = _dtype(_fields([
+    ("position", "<f4", 3, 0), ("depth", "<f4", 1, 12), ("local_a", "<f4", 3, 16), ("local_b", "<f4", 3, 32),
+    ("accumulated_normal", "<f4", 1, 44), ("accumulated_tangent_1", "<f4", 1, 48),
+    ("accumulated_tangent_2", "<f4", 1, 52), ("feature", "<u4", 1, 56),
+]), 64)
+
+CONTACT = _dtype([
+    ("a", "<u4", 0), ("b", "<u4", 4), ("point_count", "<u4", 8), ("sensor", "<u4", 12),
+    ("first_body_id", "<u4", 16), ("second_body_id", "<u4", 20), ("first_generation", "<u4", 24),
+    ("second_generation", "<u4", 28), ("normal", ("<f4", 3), 32), ("events", "<u4", 44), ("surface", "<u4", 48),
+    ("triangle", "<u4", 52), ("friction", "<f4", 56), ("restitution", "<f4", 60), ("rolling_friction", "<f4", 64),
+    ("spin_friction", "<f4", 68), ("carried_normal", "<f4", 72), ("carried_tangent", "<f4", 76),
+    ("relaxation", "<f4", 80), ("damping_ratio", "<f4", 84), ("points", (MANIFOLD_POINT, 4), 96),
+], 352)
+
+# C ABI descriptors (include/dynamis_cuda.h)
+CONFIG = np.dtype([
+    ("gravity", "<f4", 3), ("damping", "<f4"), ("angular_damping", "<f4"), ("substeps", "<u4"),
+    ("solve_iterations", "<u4"), ("position_iterations", "<u4"), ("relaxation", "<f4"), ("slop", "<f4"),
+    ("contact_margin", "<f4"), ("restitution_threshold", "<f4"), ("max_velocity", "<f4"),
+    ("max_angular_velocity", "<f4"), ("sleep_velocity", "<f4"), ("sleep_angular_velocity", "<f4"),
+    ("sleep_time", "<f4"), ("friction_combine", "<u4"), ("restitution_combine", "<u4"),
+])
+CAPACITY = np.dtype([("bodies", "<u4"), ("colliders", "<u4"), ("pairs", "<u4"), ("contacts", "<u4")])
+COLLIDER_DESC = np.dtype([
+    ("shape", "<u4"), ("radius", "<f4"), ("half_height", "<f4"), ("half_extents", "<f4", 3), ("source", "<u4"),
+    ("offset", "<f4", 3), ("rotation", "<f4", 4), ("scale", "<f4", 3), ("friction", "<f4"),
+    ("restitution", "<f4"), ("rolling_friction", "<f4"), ("spin_friction", "<f4"), ("contact_frequency", "<f4"),
+    ("contact_damping_ratio", "<f4"), ("sensor", "<u4"), ("events", "<u4"), ("collision_group", "<u4"),
+    ("collision_mask", "<u4"), ("impact_force", "<f4"),
+])
+BODY_DESC = np.dtype([
+    ("position", "<f4", 3), ("orientation", "<f4", 4), ("velocity", "<f4", 3), ("angular_velocity", "<f4", 3),
+    ("mass", "<f4"), ("density", "<f4"), ("gravity_scale", "<f4"), ("linear_damping", "<f4"),
+    ("angular_damping", "<f4"), ("sleep_velocity", "<f4"), ("sleep_angular_velocity", "<f4"),
+    ("collision_group", "<u4"), ("collision_mask", "<u4"), ("kinematic", "<u4"), ("ccd", "<u4"),
+    ("collider_first", "<u4"), ("collider_count", "<u4"),
+])
+
+assert STEP_PARAMS.itemsize == 176 and BODY_STATE.itemsize == 144 and BODY_DESCRIPTOR.itemsize == 128
+assert COLLIDER.itemsize == 112 and SHAPE_SOURCE.itemsize == 80 and CONTACT.itemsize == 352
+assert MANIFOLD_POINT.itemsize == 64 and AABB.itemsize == 32
+
+
+def collider_defaults(n: int) -> np.ndarray:
+    """ColliderDesc::new defaults (crates/dynamis-model/src/collider.rs:52-70) for n colliders."""
+    c = np.zeros(n, COLLIDER_DESC)
+    c["shape"] = SHAPE_SPHERE
+    c["radius"] = 0.5
+    c["rotation"][:, 3] = 1.0
+    c["scale"] = 1.0
+    c["friction"] = 0.5
+    c["contact_frequency"] = np.inf
+    c["contact_damping_ratio"] = 1.0
+    c["collision_group"] = NO_COLLISION_FILTER
+    c["collision_mask"] = NO_COLLISION_FILTER
+    c["impact_force"] = np.inf
+    return c
+
+
+def body_defaults(n: int) -> np.ndarray:
+    """BodyDesc::new defaults (crates/dynamis-model/src/body.rs:174-194) for n bodies."""
+    b = np.zeros(n, BODY_DESC)
+    b["orientation"][:, 3] = 1.0
+    b["mass"] = 1.0
+    b["gravity_scale"] = 1.0
+    b["linear_damping"] = -1.0
+    b["angular_damping"] = -1.0
+    b["sleep_velocity"] = -1.0
+    b["sleep_angular_velocity"] = -1.0
+    b["collision_group"] = 1
+    b["collision_mask"] = 0xFFFFFFFF
+    b["collider_count"] = 1
+    b["collider_first"] = np.arange(n, dtype=np.uint32)
+    return b

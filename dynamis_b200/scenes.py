@@ -1,0 +1,209 @@
+"""Seeded synthetic scenes: the benchmark workloads and the small scenes the tests pin.
+
+The workloads restate the scenes the north-star benchmark names (lattices of boxes, spheres and
+hulls falling onto a ground plane); no dataset is involved. Every random draw comes from
+numpy.random.default_rng(seed), so a seed fixes a scene bit for bit.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import records as R
+
+
+@dataclass
+class Scene:
+    bodies: np.ndarray                      # BODY_DESC
+    colliders: np.ndarray                   # COLLIDER_DESC; hull colliders index `hulls`
+    hulls: list = field(default_factory=list)  # float32 (m, 3) point sets
+    name: str = "scene"
+
+    @property
+    def body_count(self) -> int:
+        return len(self.bodies)
+
+    def build(self, world) -> np.ndarray:
+        """Adds the hull sources and spawns every body into `world`; returns the body ids."""
+        colliders = self.colliders.copy()
+        if self.hulls:
+            sources = np.array([world.add_hull(points) for points in self.hulls], np.uint32)
+            is_hull = colliders["shape"] == R.SHAPE_HULL
+            colliders["source"][is_hull] = sources[colliders["source"][is_hull]]
+        return world.spawn(self.bodies, colliders)
+
+
+def yaw_quaternions(angles: np.ndarray) -> np.ndarray:
+    q = np.zeros((len(angles), 4), np.float64)
+    q[:, 1] = np.sin(angles / 2)
+    q[:, 3] = np.cos(angles / 2)
+    return q.astype(np.float32)
+
+
+def uniform_quaternions(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Uniformly distributed rotations (Shoemake, "Uniform random rotations", Graphics Gems III)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+    q = np.stack([a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2), b * np.sin(2 * np.pi * u3),
+                  b * np.cos(2 * np.pi * u3)], axis=1)
+    return q.astype(np.float32)
+
+
+def _ground(bodies: np.ndarray, colliders: np.ndarray, height: float = 0.0, friction: float = 0.5,
+            restitution: float = 0.0):
+    """Appends a static body carrying a ground plane (normal +y) at the given height."""
+    b = R.body_defaults(1)
+    b["position"][0] = (0.0, height, 0.0)
+    b["mass"] = 0.0
+    b["collider_first"] = len(colliders)
+    c = R.collider_defaults(1)
+    c["shape"] = R.SHAPE_PLANE
+    c["friction"] = friction
+    c["restitution"] = restitution
+    return np.concatenate([bodies, b]), np.concatenate([colliders, c])
+
+
+def falling_boxes(seed: int = 0, side: int = 10, spacing: float = 1.1) -> Scene:
+    """1,000 unit cubes (half-extent 0.5 m, density 1000) on a 10x10x10 lattice at 1.1 m spacing,
+    +-0.05 m position jitter and a random yaw each, at rest above a static ground plane at y = 0;
+    friction 0.5, restitution 0."""
+    rng = np.random.default_rng(seed)
+    n = side ** 3
+    i, j, k = np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij")
+    base = np.stack([(i.ravel() - (side - 1) / 2) * spacing, 0.6 + j.ravel() * spacing,
+                     (k.ravel() - (side - 1) / 2) * spacing], axis=1)
+    pos = base + rng.uniform(-0.05, 0.05, size=(n, 3))
+    bodies = R.body_defaults(n)
+    bodies["position"] = pos.astype(np.float32)
+    bodies["orientation"] = yaw_quaternions(rng.uniform(0.0, 2 * np.pi, n))
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(n)
+    colliders["shape"] = R.SHAPE_CUBOID
+    colliders["half_extents"] = 0.5
+    colliders["friction"] = 0.5
+    colliders["restitution"] = 0.0
+    bodies, colliders = _ground(bodies, colliders, 0.0, 0.5, 0.0)
+    return Scene(bodies, colliders, [], f"falling_boxes_{n}")
+
+
+def mixed_pile(side: int = 64, seed: int = 1, spacing: float = 1.3) -> Scene:
+    """side^3 bodies on a lattice at 1.3 m spacing with +-0.1 m jitter and uniform random
+    orientations: 50% boxes (half-extents U[0.2, 0.6] per axis), 30% spheres (radius U[0.2, 0.5]),
+    20% convex hulls (16-32 points uniform on the unit sphere, scaled U[0.3, 0.6]); density 1000,
+    friction 0.5, restitution 0.1, over a ground plane at y = 0. side = 64 gives 262,144 bodies."""
+    rng = np.random.default_rng(seed)
+    n = side ** 3
+    i, j, k = np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij")
+    base = np.stack([(i.ravel() - (side - 1) / 2) * spacing, 1.2 + j.ravel() * spacing,
+                     (k.ravel() - (side - 1) / 2) * spacing], axis=1)
+    pos = base + rng.uniform(-0.1, 0.1, size=(n, 3))
+    kind = rng.random(n)
+    shape = np.where(kind < 0.5, R.SHAPE_CUBOID, np.where(kind < 0.8, R.SHAPE_SPHERE, R.SHAPE_HULL)).astype(np.uint32)
+    bodies = R.body_defaults(n)
+    bodies["position"] = pos.astype(np.float32)
+    bodies["orientation"] = uniform_quaternions(rng, n)
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(n)
+    colliders["shape"] = shape
+    colliders["friction"] = 0.5
+    colliders["restitution"] = 0.1
+    boxes = shape == R.SHAPE_CUBOID
+    colliders["half_extents"][boxes] = rng.uniform(0.2, 0.6, size=(int(boxes.sum()), 3)).astype(np.float32)
+    spheres = shape == R.SHAPE_SPHERE
+    colliders["radius"][spheres] = rng.uniform(0.2, 0.5, size=int(spheres.sum())).astype(np.float32)
+    hull_rows = np.nonzero(shape == R.SHAPE_HULL)[0]
+    hulls = []
+    for index, row in enumerate(hull_rows):
+        m = int(rng.integers(16, 33))
+        d = rng.normal(size=(m, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        scale = rng.uniform(0.3, 0.6)
+        hulls.append((d * scale).astype(np.float32))
+        colliders["source"][row] = index
+        colliders["radius"][row] = 0.0
+    bodies, colliders = _ground(bodies, colliders, 0.0, 0.5, 0.1)
+    return Scene(bodies, colliders, hulls, f"mixed_pile_{n}")
+
+
+def sphere_row(count: int, radius: float = 0.5, gap: float = -0.05, height: float = 5.0, gravity: bool = False) -> Scene:
+    """`count` spheres in a row along x, neighbours overlapping by -gap (a 16-sphere chain has 15 pairs)."""
+    bodies = R.body_defaults(count)
+    bodies["position"][:, 0] = np.arange(count) * (2 * radius + gap)
+    bodies["position"][:, 1] = height
+    if not gravity:
+        bodies["gravity_scale"] = 0.0
+    colliders = R.collider_defaults(count)
+    colliders["radius"] = radius
+    return Scene(bodies, colliders, [], f"sphere_row_{count}")
+
+
+def crowd(count: int, seed: int = 3) -> Scene:
+    """`count` unit boxes resting on a wide floor box, none touching each other."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(np.sqrt(count)))
+    bodies = R.body_defaults(count)
+    idx = np.arange(count)
+    bodies["position"][:, 0] = (idx % side) * 3.0
+    bodies["position"][:, 2] = (idx // side) * 3.0
+    bodies["position"][:, 1] = 0.5
+    bodies["orientation"] = yaw_quaternions(rng.uniform(0, 2 * np.pi, count))
+    colliders = R.collider_defaults(count)
+    colliders["shape"] = R.SHAPE_CUBOID
+    colliders["half_extents"] = 0.5
+    floor = R.body_defaults(1)
+    floor["mass"] = 0.0
+    floor["position"][0] = (side * 1.5, -0.5, side * 1.5)
+    floor["collider_first"] = count
+    fc = R.collider_defaults(1)
+    fc["shape"] = R.SHAPE_CUBOID
+    fc["half_extents"] = (side * 2.0, 0.5, side * 2.0)
+    return Scene(np.concatenate([bodies, floor]), np.concatenate([colliders, fc]), [], f"crowd_{count}")
+
+
+def box_tower(levels: int = 8, half: float = 0.5, gap: float = 0.0) -> Scene:
+    """A single column of unit boxes resting on a ground plane."""
+    bodies = R.body_defaults(levels)
+    bodies["position"][:, 1] = half + np.arange(levels) * (2 * half + gap)
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(levels)
+    colliders["shape"] = R.SHAPE_CUBOID
+    colliders["half_extents"] = half
+    bodies, colliders = _ground(bodies, colliders)
+    return Scene(bodies, colliders, [], f"box_tower_{levels}")
+
+
+def random_mix(count: int, seed: int = 7, extent: float = 4.0, with_ground: bool = True) -> Scene:
+    """A small random heap of boxes, spheres, capsules and hulls in a cube of side `extent`,
+    overlapping freely (narrowphase coverage for every shape pair)."""
+    rng = np.random.default_rng(seed)
+    bodies = R.body_defaults(count)
+    bodies["position"] = rng.uniform(-extent / 2, extent / 2, size=(count, 3)).astype(np.float32)
+    bodies["position"][:, 1] += extent / 2 + 0.6
+    bodies["orientation"] = uniform_quaternions(rng, count)
+    bodies["velocity"] = rng.normal(0, 0.5, size=(count, 3)).astype(np.float32)
+    bodies["angular_velocity"] = rng.normal(0, 0.5, size=(count, 3)).astype(np.float32)
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(count)
+    kinds = rng.choice([R.SHAPE_CUBOID, R.SHAPE_SPHERE, R.SHAPE_CAPSULE, R.SHAPE_HULL], size=count)
+    colliders["shape"] = kinds
+    colliders["half_extents"] = rng.uniform(0.2, 0.6, size=(count, 3)).astype(np.float32)
+    colliders["radius"] = rng.uniform(0.2, 0.5, size=count).astype(np.float32)
+    colliders["half_height"] = rng.uniform(0.1, 0.4, size=count).astype(np.float32)
+    colliders["restitution"] = 0.1
+    hulls = []
+    for row in np.nonzero(kinds == R.SHAPE_HULL)[0]:
+        m = int(rng.integers(8, 33))
+        d = rng.normal(size=(m, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        hulls.append((d * rng.uniform(0.3, 0.6)).astype(np.float32))
+        colliders["source"][row] = len(hulls) - 1
+    if with_ground:
+        bodies, colliders = _ground(bodies, colliders, 0.0, 0.5, 0.1)
+    return Scene(bodies, colliders, hulls, f"random_mix_{count}")
+
+
+WORKLOADS = {
+    "falling_boxes_1000": lambda: falling_boxes(seed=0),
+    "mixed_pile_262144": lambda: mixed_pile(side=64, seed=1),
+}

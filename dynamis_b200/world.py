@@ -1,0 +1,204 @@
+"""World: the host-side mirror of dynamis-world's World over the C ABI.
+
+Method names follow crates/dynamis-world/src (World::new lib.rs:86, spawn body.rs:108,
+add_hull_from_mesh shape.rs:50, step step.rs:34, wait observation.rs:484, read_state body.rs:326,
+measured readback.rs:215, refusals readback.rs:226). Invalid input raises (the reference panics).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import records as R
+from ._native import DynamisError, check, lib, ptr
+
+
+def default_config() -> np.ndarray:
+    c = np.zeros(1, R.CONFIG)
+    lib.dyn_config_default(ptr(c))
+    return c
+
+
+class World:
+    """One simulated world on one GPU (crates/dynamis-world/src/lib.rs:64-109)."""
+
+    def __init__(self, config: np.ndarray | None = None, capacity: dict | None = None, device: int = 0, **overrides):
+        cfg = default_config() if config is None else np.array(config, R.CONFIG).reshape(1)
+        for key, value in overrides.items():
+            cfg[key] = value
+        cap = np.zeros(1, R.CAPACITY)
+        for key, value in (capacity or {}).items():
+            cap[key] = value
+        handle = ctypes.c_void_p()
+        check(lib.dyn_world_create(ptr(cfg), ptr(cap), int(device), ctypes.byref(handle)))
+        self._h = handle
+        self.config = cfg
+
+    def close(self) -> None:
+        if self._h:
+            lib.dyn_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, status: int) -> None:
+        check(status, self._h)
+
+    # ---- scene ----
+    def add_hull(self, points) -> int:
+        """World::add_hull_from_mesh: convex hull of the points becomes a shape source."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = ctypes.c_uint32()
+        self._check(lib.dyn_add_hull(self._h, ptr(pts), len(pts), ctypes.byref(out)))
+        return out.value
+
+    def hull_info(self, source: int) -> dict:
+        vc, tc, vol = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_float()
+        cen = np.zeros(3, np.float32)
+        self._check(lib.dyn_hull_info(self._h, source, ctypes.byref(vc), ctypes.byref(tc), ctypes.byref(vol), ptr(cen)))
+        return {"vertices": vc.value, "triangles": tc.value, "volume": vol.value, "centroid": cen}
+
+    def spawn(self, bodies: np.ndarray, colliders: np.ndarray) -> np.ndarray:
+        """World::spawn for every BODY_DESC row; returns the body ids."""
+        bodies = np.ascontiguousarray(bodies, R.BODY_DESC)
+        colliders = np.ascontiguousarray(colliders, R.COLLIDER_DESC)
+        ids = np.zeros(len(bodies), np.uint32)
+        self._check(lib.dyn_spawn_bodies(self._h, ptr(bodies), len(bodies), ptr(colliders), len(colliders), ptr(ids)))
+        return ids
+
+    def upload_bodies(self, states, descs, colliders, owners) -> None:
+        states = np.ascontiguousarray(states, R.BODY_STATE)
+        descs = np.ascontiguousarray(descs, R.BODY_DESCRIPTOR)
+        colliders = np.ascontiguousarray(colliders, R.COLLIDER)
+        owners = np.ascontiguousarray(owners, np.uint32)
+        self._check(lib.dyn_upload_bodies(self._h, ptr(states), ptr(descs), len(states), ptr(colliders), ptr(owners),
+                                          len(colliders)))
+
+    def upload_states(self, states: np.ndarray) -> None:
+        states = np.ascontiguousarray(states, R.BODY_STATE)
+        self._check(lib.dyn_upload_states(self._h, ptr(states), len(states)))
+
+    def sizes(self) -> dict:
+        vals = [ctypes.c_uint32() for _ in range(5)]
+        self._check(lib.dyn_scene_sizes(self._h, *[ctypes.byref(v) for v in vals]))
+        return dict(zip(["bodies", "dynamic", "colliders", "sources", "vertices"], [v.value for v in vals]))
+
+    def export_scene(self) -> dict:
+        """The scene as rows: the exact records the device receives."""
+        s = self.sizes()
+        states = np.zeros(s["bodies"], R.BODY_STATE)
+        descs = np.zeros(s["bodies"], R.BODY_DESCRIPTOR)
+        colliders = np.zeros(s["colliders"], R.COLLIDER)
+        owners = np.zeros(s["colliders"], np.uint32)
+        sources = np.zeros(s["sources"], R.SHAPE_SOURCE)
+        vertices = np.zeros((max(s["vertices"], 0), 4), np.float32)
+        self._check(lib.dyn_export_scene(self._h, ptr(states), ptr(descs), ptr(colliders), ptr(owners), ptr(sources),
+                                         ptr(vertices)))
+        return {"states": states, "descs": descs, "colliders": colliders, "owners": owners, "sources": sources,
+                "vertices": vertices, "dynamic": s["dynamic"]}
+
+    def step_params(self, dt: float) -> np.ndarray:
+        p = np.zeros(1, R.STEP_PARAMS)
+        self._check(lib.dyn_step_params_for(self._h, float(dt), ptr(p)))
+        return p
+
+    # ---- stepping ----
+    def step(self, dt: float) -> None:
+        """World::step: enqueues one step; returns without waiting."""
+        self._check(lib.dyn_step(self._h, float(dt)))
+
+    def wait(self) -> None:
+        """World::wait: blocks until queued steps finish; raises on a sticky device status."""
+        self._check(lib.dyn_sync(self._h))
+
+    def set_stream(self, cuda_stream: int | None) -> None:
+        self._check(lib.dyn_world_set_stream(self._h, cuda_stream))
+
+    # ---- readback ----
+    def read_states(self) -> np.ndarray:
+        """All body states in row order (dynamic rows first)."""
+        n = self.sizes()["bodies"]
+        out = np.zeros(n, R.BODY_STATE)
+        self._check(lib.dyn_download_states(self._h, ptr(out), n))
+        return out
+
+    def read_state(self, body_id: int) -> np.ndarray:
+        out = np.zeros(1, R.BODY_STATE)
+        self._check(lib.dyn_read_state(self._h, int(body_id), ptr(out)))
+        return out[0]
+
+    def measured(self) -> np.ndarray:
+        out = np.zeros(R.COUNTER_DEVICE_COUNT, np.uint32)
+        self._check(lib.dyn_read_counters(self._h, ptr(out), len(out)))
+        return out
+
+    def refusals(self) -> dict:
+        m = self.measured()
+        names = ["REFUSED_PAIRS", "REFUSED_CONTACTS", "ENTRY_FAULTS", "ISLAND_FAULTS", "LIVE_FAULTS"]
+        return {n: int(m[R.COUNTER[n]]) for n in names}
+
+    # ---- parity hooks (the last step's intermediate products) ----
+    def debug_aabbs(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_debug_aabbs(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, R.AABB)
+        self._check(lib.dyn_debug_aabbs(self._h, ptr(out), n.value, None))
+        return out
+
+    def debug_entries(self):
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_debug_entries(self._h, None, None, 0, ctypes.byref(n)))
+        keys = np.zeros(n.value, np.uint32)
+        infos = np.zeros(n.value, np.uint32)
+        self._check(lib.dyn_debug_entries(self._h, ptr(keys), ptr(infos), n.value, None))
+        return keys, infos
+
+    def debug_pairs(self):
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_debug_pairs(self._h, None, None, 0, ctypes.byref(n)))
+        major = np.zeros(n.value, np.uint32)
+        minor = np.zeros(n.value, np.uint32)
+        self._check(lib.dyn_debug_pairs(self._h, ptr(major), ptr(minor), n.value, None))
+        return major, minor
+
+    def debug_contacts(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_debug_contacts(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, R.CONTACT)
+        self._check(lib.dyn_debug_contacts(self._h, ptr(out), n.value, None))
+        return out
+
+    def debug_islands(self) -> np.ndarray:
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_debug_islands(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.uint32)
+        self._check(lib.dyn_debug_islands(self._h, ptr(out), n.value, None))
+        return out
+
+    # ---- timing ----
+    def step_kernel_count(self) -> int:
+        """Kernel launches per step (kernel nodes of the captured step graph)."""
+        return int(lib.dyn_step_kernel_count(self._h))
+
+    def set_timing(self, enabled: bool) -> None:
+        self._check(lib.dyn_set_timing(self._h, 1 if enabled else 0))
+
+    def stage_timings(self) -> dict:
+        n = lib.dyn_stage_count()
+        ms = np.zeros(n, np.float32)
+        self._check(lib.dyn_stage_timings(self._h, ptr(ms), n))
+        return {lib.dyn_stage_name(i).decode(): float(ms[i]) for i in range(n)}
+
+
+__all__ = ["World", "DynamisError", "default_config"]

@@ -1,0 +1,206 @@
+/*
+ * dynamis_cuda.h - C ABI of the B200 rigid-body step (libdynamis_cuda.so).
+ *
+ * This is the drop-in boundary for the reference's `dynamis-world` step path. Each entry point
+ * names the Rust API it replaces (paths relative to the reference project). Records crossing the
+ * boundary are the byte-exact ABI layouts of dynamis_abi.h. All memory is owned by the library
+ * behind the opaque world handle; every call returns a dyn_status (0 = ok) and never aborts.
+ * One world is used from one host thread at a time; distinct worlds are independent.
+ *
+ * Host-only calls (configuration, hulls, spawning, record export) work without a GPU; the device
+ * is touched on the first call that needs it (step, upload, download, debug reads).
+ */
+#ifndef DYNAMIS_CUDA_H
+#define DYNAMIS_CUDA_H
+
+#include <stdint.h>
+
+#include "dynamis_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DYN_API __attribute__((visibility("default")))
+#else
+#define DYN_API
+#endif
+
+typedef int32_t dyn_status;
+#define DYN_OK 0
+#define DYN_ERR_INVALID 1         /* argument or scene the reference would refuse (it panics) */
+#define DYN_ERR_CAPACITY 2        /* a declared capacity is too small for the scene */
+#define DYN_ERR_CUDA 3            /* a CUDA runtime call failed; see dyn_last_error */
+#define DYN_ERR_NO_DEVICE 4       /* no CUDA device, or the requested ordinal does not exist */
+#define DYN_ERR_DEVICE_STATUS 5   /* a kernel gave up a bounded wait; see dyn_device_status */
+#define DYN_ERR_DEGENERATE 6      /* a hull point set spans no volume */
+
+typedef struct dyn_world dyn_world;
+
+/* PhysicsConfig: crates/dynamis-model/src/config.rs:12-100 (defaults from dyn_config_default). */
+typedef struct dyn_config {
+    float gravity[3];
+    float damping;
+    float angular_damping;
+    uint32_t substeps;
+    uint32_t solve_iterations;
+    uint32_t position_iterations;
+    float relaxation;
+    float slop;
+    float contact_margin;
+    float restitution_threshold;
+    float max_velocity;
+    float max_angular_velocity;
+    float sleep_velocity;
+    float sleep_angular_velocity;
+    float sleep_time;
+    uint32_t friction_combine;    /* 0 multiply, 1 min, 2 max, 3 average (param.rs:160-167) */
+    uint32_t restitution_combine;
+} dyn_config;
+
+/* Stream capacities, fixed up front (the reference grows streams from lagged counters:
+ * crates/dynamis-broadphase/src/capacity.rs:27-78). Zero means "size from the scene". */
+typedef struct dyn_capacity {
+    uint32_t bodies;
+    uint32_t colliders;
+    uint32_t pairs;
+    uint32_t contacts;
+} dyn_capacity;
+
+/* ColliderDesc: crates/dynamis-model/src/collider.rs (one collider of a body). */
+typedef struct dyn_collider_desc {
+    uint32_t shape;          /* DYN_SHAPE_SPHERE, _CUBOID, _CAPSULE, _CYLINDER, _HULL, _PLANE */
+    float radius;            /* sphere, capsule, cylinder */
+    float half_height;       /* capsule, cylinder */
+    float half_extents[3];   /* cuboid */
+    uint32_t source;         /* hull source from dyn_add_hull */
+    float offset[3];
+    float rotation[4];
+    float scale[3];
+    float friction;          /* default 0.5 */
+    float restitution;       /* default 0 */
+    float rolling_friction;
+    float spin_friction;
+    float contact_frequency; /* +inf = hard contact (relaxation 0) */
+    float contact_damping_ratio; /* default 1 */
+    uint32_t sensor;
+    uint32_t events;         /* DYN_EVENT_MODE_* bits */
+    uint32_t collision_group; /* DYN_NO_COLLISION_FILTER = inherit the body's */
+    uint32_t collision_mask;
+    float impact_force;      /* +inf = none */
+} dyn_collider_desc;
+
+/* BodyDesc: crates/dynamis-model/src/body.rs:88-200. A body owns colliders
+ * [collider_first, collider_first + collider_count) of the collider array passed beside it. */
+typedef struct dyn_body_desc {
+    float position[3];
+    float orientation[4];
+    float velocity[3];
+    float angular_velocity[3];
+    float mass;              /* used when density <= 0; 0 makes a static body */
+    float density;           /* > 0: mass = density x solid volume */
+    float gravity_scale;     /* default 1 */
+    float linear_damping;    /* < 0 = the config's damping */
+    float angular_damping;   /* < 0 = the config's angular damping */
+    float sleep_velocity;    /* < 0 = the config's threshold */
+    float sleep_angular_velocity;
+    uint32_t collision_group; /* default 1 */
+    uint32_t collision_mask;  /* default all */
+    uint32_t kinematic;
+    uint32_t ccd;
+    uint32_t collider_first;
+    uint32_t collider_count;
+} dyn_body_desc;
+
+DYN_API uint32_t dyn_abi_version(void);
+DYN_API const char* dyn_status_string(dyn_status status);
+
+/* PhysicsConfig::default (config.rs:76-100), ColliderDesc::new and BodyDesc::new defaults. */
+DYN_API void dyn_config_default(dyn_config* out);
+DYN_API void dyn_collider_desc_default(dyn_collider_desc* out);
+DYN_API void dyn_body_desc_default(dyn_body_desc* out);
+
+/* World::new (crates/dynamis-world/src/lib.rs:86). device = CUDA ordinal used by device calls. */
+DYN_API dyn_status dyn_world_create(const dyn_config* config, const dyn_capacity* capacity, int32_t device,
+                                    dyn_world** out);
+DYN_API dyn_status dyn_world_destroy(dyn_world* world);
+/* Last error text of this world (empty when none). */
+DYN_API const char* dyn_last_error(const dyn_world* world);
+/* Run device work on a caller-owned cudaStream_t (NULL = the world's own stream). */
+DYN_API dyn_status dyn_world_set_stream(dyn_world* world, void* cuda_stream);
+
+/* World::add_hull_from_mesh (crates/dynamis-world/src/shape.rs:50; quickhull of
+ * crates/dynamis-hull/src/hull.rs:53-160 and solid integrals of solid.rs:62): the convex hull of
+ * n points (xyz triples) becomes a hull shape source. */
+DYN_API dyn_status dyn_add_hull(dyn_world* world, const float* xyz, uint32_t n, uint32_t* out_source);
+DYN_API dyn_status dyn_hull_info(const dyn_world* world, uint32_t source, uint32_t* vertex_count,
+                                 uint32_t* triangle_count, float* volume, float centroid[3]);
+
+/* World::spawn (crates/dynamis-world/src/body.rs:108-130) for n bodies at once: builds
+ * BodyStateRecord::initial, BodyDescriptorRecord::build (mass properties of
+ * crates/dynamis-model/src/mass.rs:155-212) and ColliderRecord::build. out_ids[i] = body id. */
+DYN_API dyn_status dyn_spawn_bodies(dyn_world* world, const dyn_body_desc* bodies, uint32_t n,
+                                    const dyn_collider_desc* colliders, uint32_t k, uint32_t* out_ids);
+
+/* Replaces the scene with ready-made ABI records (the Rust shim passes its bytemuck slices).
+ * Rows must hold the dynamic bodies first (the reference's row census); owners[i] is the body row
+ * of collider i. Shape sources come from dyn_add_hull on this world. */
+DYN_API dyn_status dyn_upload_bodies(dyn_world* world, const dyn_body_state_record* states,
+                                     const dyn_body_descriptor_record* descs, uint32_t n,
+                                     const dyn_collider_record* colliders, const uint32_t* owners, uint32_t k);
+/* Overwrites the n body states (row order) of the current scene. */
+DYN_API dyn_status dyn_upload_states(dyn_world* world, const dyn_body_state_record* states, uint32_t n);
+
+/* Host copy of the scene as rows: sizes, then records (any output pointer may be NULL). */
+DYN_API dyn_status dyn_scene_sizes(const dyn_world* world, uint32_t* bodies, uint32_t* dynamic_bodies,
+                                   uint32_t* colliders, uint32_t* sources, uint32_t* vertices);
+DYN_API dyn_status dyn_export_scene(const dyn_world* world, dyn_body_state_record* states,
+                                    dyn_body_descriptor_record* descs, dyn_collider_record* colliders,
+                                    uint32_t* owners, dyn_shape_source_record* sources, float* vertices_xyzw);
+/* StepParamsRecord::new (crates/dynamis-abi/src/param.rs:110-158) for this scene and dt. */
+DYN_API dyn_status dyn_step_params_for(const dyn_world* world, float dt, dyn_step_params* out);
+
+/* World::step (crates/dynamis-world/src/step.rs:34-39): enqueues one step (a CUDA graph launch)
+ * and returns without waiting, as the reference's submit does. */
+DYN_API dyn_status dyn_step(dyn_world* world, float dt);
+/* World::wait (observation.rs:484): blocks until queued steps finish; reports the sticky device
+ * status (DYN_ERR_DEVICE_STATUS when a kernel's bounded wait ran out). */
+DYN_API dyn_status dyn_sync(dyn_world* world);
+DYN_API dyn_status dyn_device_status(dyn_world* world, uint32_t* status);
+
+/* World::read_state (body.rs:326) for all rows, and one body by id. Synchronises. */
+DYN_API dyn_status dyn_download_states(dyn_world* world, dyn_body_state_record* out, uint32_t n);
+DYN_API dyn_status dyn_read_state(dyn_world* world, uint32_t body_id, dyn_body_state_record* out);
+/* World::measured (readback.rs:215): the device counters, slots of dynamis_abi.h's dyn_counter. */
+DYN_API dyn_status dyn_read_counters(dyn_world* world, uint32_t* out, uint32_t n);
+
+/* Parity hooks: the last step's intermediate products (synchronise). count = items available. */
+DYN_API dyn_status dyn_debug_aabbs(dyn_world* world, dyn_aabb_record* out, uint32_t cap, uint32_t* count);
+DYN_API dyn_status dyn_debug_entries(dyn_world* world, uint32_t* keys, uint32_t* infos, uint32_t cap, uint32_t* count);
+DYN_API dyn_status dyn_debug_pairs(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t cap, uint32_t* count);
+DYN_API dyn_status dyn_debug_contacts(dyn_world* world, dyn_contact_record* out, uint32_t cap, uint32_t* count);
+DYN_API dyn_status dyn_debug_islands(dyn_world* world, uint32_t* out, uint32_t cap, uint32_t* count);
+
+/* Per-stage timing (World::gpu_pass_timings, step.rs:187-190). With timing on, dyn_step runs the
+ * stages eagerly with CUDA events between them instead of the graph; dyn_stage_timings returns
+ * the last step's milliseconds per stage and their names. */
+DYN_API dyn_status dyn_set_timing(dyn_world* world, int32_t enabled);
+/* Kernel launches in one step (kernel nodes of the captured step graph; 0 before the first step). */
+DYN_API uint32_t dyn_step_kernel_count(const dyn_world* world);
+DYN_API uint32_t dyn_stage_count(void);
+DYN_API const char* dyn_stage_name(uint32_t stage);
+DYN_API dyn_status dyn_stage_timings(dyn_world* world, float* ms, uint32_t n);
+
+/* Standalone operator (crates/dynamis-sort/src/radix.rs:397 RadixSort::sort): stable LSD sort of
+ * n device-resident (major, minor) u32 keys with an optional u32 payload, minor_digits of the
+ * minor word then major_digits of the major word (8-bit digits). Pointers are device pointers;
+ * minor/payload may be NULL. Uses the world's stream and scratch. */
+DYN_API dyn_status dyn_radix_sort(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
+                                  uint32_t major_digits, uint32_t minor_digits);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* DYNAMIS_CUDA_H */

@@ -1,0 +1,1298 @@
+// oracle.cpp - CPU restatement of one Dynamis rigid-body step (World::step), the parity checker.
+//
+// TEST INFRASTRUCTURE ONLY. tests/ load the shared library built from this file (ctypes) to check
+// the CUDA product on identical inputs, and bench.py times it as the CPU baseline. The product
+// package never includes, links or loads it.
+//
+// Pass order follows crates/dynamis-rigid/src/lib.rs:119-153 and the record() functions of
+// apply_commands.rs:267-295, integrate.rs:90-107, emit_entries.rs:127-145,
+// crates/dynamis-broadphase/src/passes.rs:145-160, narrowphase.rs:110-133, islands.rs:237-258,
+// wake.rs, live.rs, solver.rs:76-95 and 304-333, commit.rs. Where the reference's output order
+// depends on atomics (entry slots, pair emission, live list, solver rows) the oracle takes
+// ascending order; parity is asserted on the order-independent results (sorted keys, sorted
+// pairs, contacts, island ids, body states).
+//
+// Scope notes (also in the design notes): the resting-region index (frozen grid entries and
+// contacts of sleeping bodies) is replaced by re-emitting every movable collider each step with
+// its awake bit, which yields the same candidate pairs for awake bodies; contact events are not
+// published (only the CONTACT_ANNOUNCED flag that gates warm starting is kept).
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "dynamis_abi.h"
+#include "oracle_geom.h"
+
+using namespace orc;
+
+namespace {
+
+// ---- grid: crates/dynamis-shader/shaders/grid_index.wgsl:28-287, core.wgsl:106-130 ----
+
+constexpr float kGridScaleLimit = 1e12f;
+
+struct I3 {
+    int32_t x, y, z;
+};
+struct GridCells {
+    I3 min, max;
+};
+
+inline float grid_extent_of(const Aabb& b) {
+    return fmaxw(fmaxw(b.max.x - b.min.x, b.max.y - b.min.y), b.max.z - b.min.z);
+}
+inline float grid_scale_of(const Aabb& b) {
+    float extent = grid_extent_of(b);
+    if (extent <= 0.0f) return 0.0f;
+    return clampw(1.0f / extent, 1.0f / kGridScaleLimit, kGridScaleLimit);
+}
+inline float grid_cell_size(uint32_t scale_bits, uint32_t extent_bits) {
+    float scale = u2f(scale_bits);
+    float extent = u2f(extent_bits);
+    float finest = scale > 0.0f ? 1.0f / scale : kGridScaleLimit;
+    return fmaxw(finest, extent * 9.31322574615478515625e-10f);  // exp2(-30)
+}
+inline int32_t f2i(float f) { return (int32_t)f; }  // values are already floored
+inline I3 floor_div(V3 v, float cs) {
+    return I3{f2i(std::floor(v.x / cs)), f2i(std::floor(v.y / cs)), f2i(std::floor(v.z / cs))};
+}
+inline GridCells grid_cells(const Aabb& box, float cs) { return GridCells{floor_div(box.min, cs), floor_div(box.max, cs)}; }
+inline void grid_cell_span(const GridCells& c, uint32_t span[3]) {
+    span[0] = (uint32_t)(c.max.x - c.min.x + 1);
+    span[1] = (uint32_t)(c.max.y - c.min.y + 1);
+    span[2] = (uint32_t)(c.max.z - c.min.z + 1);
+}
+inline uint32_t grid_cell_count(const GridCells& c) {
+    uint32_t s[3];
+    grid_cell_span(c, s);
+    return s[0] * s[1] * s[2];
+}
+inline I3 grid_cell_at(const GridCells& c, uint32_t ordinal) {
+    uint32_t s[3];
+    grid_cell_span(c, s);
+    uint32_t rows = s[1] * s[2];
+    return I3{c.min.x + (int32_t)(ordinal / rows), c.min.y + (int32_t)((ordinal / s[2]) % s[1]),
+              c.min.z + (int32_t)(ordinal % s[2])};
+}
+inline uint32_t grid_cell_offset(const GridCells& c, I3 coord) {
+    return (uint32_t)(coord.x - c.min.x) | ((uint32_t)(coord.y - c.min.y) << 1) | ((uint32_t)(coord.z - c.min.z) << 2);
+}
+inline uint32_t cell_hash(I3 c) {
+    uint32_t x = (uint32_t)c.x * 0x9E3779B9u;
+    uint32_t y = (uint32_t)c.y * 0x85EBCA77u;
+    uint32_t z = (uint32_t)c.z * 0xC2B2AE3Du;
+    return (x ^ y ^ z ^ (x << 7) ^ (y >> 3) ^ (z << 11)) & DYN_CELL_HASH_MASK;
+}
+inline uint32_t cell_key(uint32_t level, I3 c) { return (level << DYN_LEVEL_KEY_SHIFT) | cell_hash(c); }
+inline float level_cell_size(uint32_t level, float cs) { return cs * (float)(1u << level); }
+inline uint32_t shape_levels(const Aabb& box, float base) {
+    uint32_t level = 0;
+    for (;;) {
+        uint32_t s[3];
+        grid_cell_span(grid_cells(box, level_cell_size(level, base)), s);
+        uint32_t m = std::max(std::max(s[0], s[1]), s[2]);
+        if (m <= DYN_MAX_CELLS_PER_AXIS || level >= DYN_GRID_LEVEL_LIMIT) break;
+        level += 1;
+    }
+    return level;
+}
+inline bool i3eq(I3 a, I3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+inline bool aabb_overlaps(const Aabb& a, const Aabb& b) {
+    return a.min.x <= b.max.x && a.min.y <= b.max.y && a.min.z <= b.max.z && b.min.x <= a.max.x
+        && b.min.y <= a.max.y && b.min.z <= a.max.z;
+}
+
+// ---- LSD radix sort with 8-bit digits: crates/dynamis-sort/src/radix.rs:312-476 ----
+// Stable; the minor word's digits go first, then the major word's (radix.rs:312-317).
+void radix_sort_pairs(std::vector<uint32_t>& major, std::vector<uint32_t>& minor, std::vector<uint32_t>* payload,
+                      uint32_t major_words, uint32_t minor_words) {
+    size_t n = major.size();
+    std::vector<uint32_t> tmp_major(n), tmp_minor(n), tmp_payload(payload ? n : 0);
+    auto pass = [&](bool on_major, uint32_t digit) {
+        uint32_t count[256] = {0};
+        std::vector<uint32_t>& keys = on_major ? major : minor;
+        for (size_t i = 0; i < n; ++i) count[(keys[i] >> (8 * digit)) & 255u] += 1;
+        uint32_t offset[256];
+        uint32_t run = 0;
+        for (int d = 0; d < 256; ++d) {
+            offset[d] = run;
+            run += count[d];
+        }
+        for (size_t i = 0; i < n; ++i) {
+            uint32_t d = (keys[i] >> (8 * digit)) & 255u;
+            uint32_t dst = offset[d]++;
+            tmp_major[dst] = major[i];
+            tmp_minor[dst] = minor[i];
+            if (payload) tmp_payload[dst] = (*payload)[i];
+        }
+        major.swap(tmp_major);
+        minor.swap(tmp_minor);
+        if (payload) payload->swap(tmp_payload);
+    };
+    for (uint32_t d = 0; d < minor_words; ++d) pass(false, d);
+    for (uint32_t d = 0; d < major_words; ++d) pass(true, d);
+}
+// radix.rs:71-74: digits needed to hold values below n.
+uint32_t key_words(uint32_t n) {
+    uint32_t m = n > 0 ? n - 1 : 0;
+    uint32_t bits = m == 0 ? 0 : 32 - (uint32_t)__builtin_clz(m);
+    uint32_t words = (bits + 7) / 8;
+    return words < 1 ? 1 : (words > 4 ? 4 : words);
+}
+
+struct Entry {
+    Aabb box;
+    uint32_t group;
+    uint32_t info;
+};
+
+}  // namespace
+
+struct OracleWorld {
+    dyn_step_params params{};
+    Shapes shapes;
+    std::vector<dyn_shape_source_record> sources;
+    std::vector<V4> vertices;
+    std::vector<dyn_body_state_record> states;
+    std::vector<dyn_body_descriptor_record> descs;
+    std::vector<dyn_collider_record> colliders;
+    std::vector<uint32_t> owners;
+    std::vector<uint32_t> row_of_id;  // body_id -> row
+    uint32_t pair_capacity = 0;
+    uint32_t contact_capacity = 0;
+    // per-step products kept for inspection
+    uint32_t counters[DYN_COUNTER_DEVICE_COUNT] = {0};
+    std::vector<Aabb> aabbs;
+    std::vector<uint32_t> entry_keys, entry_order;
+    std::vector<Entry> entries;
+    std::vector<uint32_t> pair_major, pair_minor;
+    std::vector<dyn_contact_record> contacts, archive;
+    std::vector<uint32_t> contact_matched;
+    std::vector<uint32_t> island_parents, island_state;
+    std::vector<uint32_t> wake_flags, body_activity, body_motion;
+    std::vector<uint32_t> live;
+    std::vector<uint32_t> block_counts, blocks, solver_rows;
+    std::vector<float> target_speeds;
+    std::vector<V3> resolution;
+    std::vector<int32_t> velocity_deltas, position_deltas;
+    std::vector<uint32_t> contributions;
+    uint32_t solver_rounds = 0;
+};
+
+namespace {
+
+const uint32_t kPerStepCounters[] = {
+    DYN_COUNTER_ENTRIES, DYN_COUNTER_RESTING_REBUILD, DYN_COUNTER_RESTING_SORT, DYN_COUNTER_IMMOVABLE_EMITTED,
+    DYN_COUNTER_PAIRS, DYN_COUNTER_GRID_LEVELS, DYN_COUNTER_CONTACTS, DYN_COUNTER_JOINTS, DYN_COUNTER_EVENTS,
+    DYN_COUNTER_REFUSED_PAIRS, DYN_COUNTER_REFUSED_EVENTS, DYN_COUNTER_ENTRY_FAULTS, DYN_COUNTER_REFUSED_RESTING,
+    DYN_COUNTER_SLEPT, DYN_COUNTER_WOKE, DYN_COUNTER_ACTIVE, DYN_COUNTER_WOKE_DEFERRED, DYN_COUNTER_RESTING_GATHER,
+    DYN_COUNTER_ISLANDS, DYN_COUNTER_ISLAND_FAULTS, DYN_COUNTER_SOLVE_LINEAR_RESIDUAL,
+    DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL, DYN_COUNTER_COARSE_ACTIVE, DYN_COUNTER_GRID_SCALE, DYN_COUNTER_GRID_EXTENT,
+    DYN_COUNTER_BREAKS, DYN_COUNTER_PARTICLE_REACH, DYN_COUNTER_COARSE_NEIGHBOURS, DYN_COUNTER_LIVE,
+    DYN_COUNTER_LIVE_FAULTS, DYN_COUNTER_ROW_FAULTS, DYN_COUNTER_SOFT_ACTIVE, DYN_COUNTER_SOFT_SLEPT,
+    DYN_COUNTER_SOFT_WOKE, DYN_COUNTER_REFUSED_CONTACTS, DYN_COUNTER_IMPACTS, DYN_COUNTER_REFUSED_IMPACTS,
+    DYN_COUNTER_SOFT_EVENTS, DYN_COUNTER_REFUSED_SOFT_EVENTS};
+
+Body body_at(const OracleWorld& w, uint32_t row) { return load_body(w.states[row], w.descs[row]); }
+
+// core.wgsl:229-255
+bool body_is_active(const dyn_body_state_record& s, const dyn_body_descriptor_record& d) {
+    return body_moves_d(d.inverse_mass, d.flags) && s.sleeping == 0u;
+}
+bool body_is_moving(const dyn_body_state_record& s, const dyn_body_descriptor_record& d, const dyn_step_params& p) {
+    bool driven = body_moves_d(d.inverse_mass, d.flags) && !body_simulates_d(d.inverse_mass, d.flags);
+    if (driven && (!veq(rd3(s.velocity), splat3(0.0f)) || !veq(rd3(s.angular_velocity), splat3(0.0f)))) return true;
+    if (!body_simulates_d(d.inverse_mass, d.flags) || s.sleeping != 0u) return false;
+    float sleep_v = (d.flags & DYN_OVERRIDE_SLEEP_LINEAR) ? d.sleep_velocity : p.sleep_velocity;
+    float sleep_w = (d.flags & DYN_OVERRIDE_SLEEP_ANGULAR) ? d.sleep_angular_velocity : p.sleep_angular_velocity;
+    return length(rd3(s.velocity)) > sleep_v || length(rd3(s.angular_velocity)) > sleep_w;
+}
+
+// apply_commands.rs:267-295: reset_counters.wgsl, clear_inputs.wgsl, activity.wgsl
+void apply_commands(OracleWorld& w) {
+    for (uint32_t slot : kPerStepCounters) w.counters[slot] = 0;
+    uint32_t n = (uint32_t)w.states.size();
+    for (uint32_t i = 0; i < n; ++i) {
+        wr3(w.states[i].force, splat3(0.0f));
+        wr3(w.states[i].torque, splat3(0.0f));
+    }
+    w.body_activity.assign(n, 0);
+    w.body_motion.assign(n, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        bool awake = body_is_active(w.states[i], w.descs[i]);
+        w.body_activity[i] = awake ? 1u : 0u;
+        w.body_motion[i] = body_is_moving(w.states[i], w.descs[i], w.params) ? 1u : 0u;
+        if (awake) w.counters[DYN_COUNTER_ACTIVE] = 1;
+    }
+}
+
+// begin_step.wgsl:5-14 (dynamic rows); broadphase_aabb.wgsl:11-62 (colliders)
+void prepare(OracleWorld& w) {
+    for (uint32_t i = 0; i < w.params.dynamic_count; ++i) {
+        dyn_body_state_record& s = w.states[i];
+        if (s.sleeping != 0u) continue;
+        for (int k = 0; k < 3; ++k) s.prev_position[k] = s.position[k];
+        for (int k = 0; k < 4; ++k) s.prev_orientation[k] = s.orientation[k];
+    }
+    uint32_t k = (uint32_t)w.colliders.size();
+    w.aabbs.assign(k, Aabb{splat3(0.0f), splat3(0.0f)});
+    for (uint32_t i = 0; i < k; ++i) {
+        uint32_t owner = w.owners[i];
+        if (owner == DYN_NO_BODY) continue;
+        const dyn_body_state_record& s = w.states[owner];
+        const dyn_body_descriptor_record& d = w.descs[owner];
+        const dyn_collider_record& c = w.colliders[i];
+        WorldShape shape = world_collider(rd3(s.position), rd4(s.orientation), c);
+        Aabb tight = world_aabb_of(w.shapes, shape);
+        WorldShape upright = shape;
+        upright.rotation = V4{0.0f, 0.0f, 0.0f, 1.0f};
+        Aabb resolution = world_aabb_of(w.shapes, upright);
+        w.counters[DYN_COUNTER_GRID_SCALE] = std::max(w.counters[DYN_COUNTER_GRID_SCALE], f2u(grid_scale_of(resolution)));
+        w.counters[DYN_COUNTER_GRID_EXTENT] =
+            std::max(w.counters[DYN_COUNTER_GRID_EXTENT], f2u(fmaxw(grid_extent_of(resolution), 0.0f)));
+        Aabb swept = tight;
+        if (body_moves_d(d.inverse_mass, d.flags)) {
+            V3 travel = vabs(rd3(s.velocity) * w.params.dt);
+            float spin = length(rd3(s.angular_velocity) * w.params.dt);
+            Body b = load_body(s, d);
+            V3 center = rd3(s.position) + quat_rotate(rd4(s.orientation), rd3(c.local_offset));
+            float radius = length((tight.max - tight.min) * 0.5f) + length(center - body_com(b));
+            float reach_r = spin >= 3.141592653589793f ? 2.0f * radius : 2.0f * radius * osin(0.5f * spin);
+            V3 reach = splat3(w.params.contact_margin + reach_r);
+            swept.min = tight.min - travel - reach;
+            swept.max = tight.max + travel + reach;
+        }
+        w.aabbs[i] = swept;
+    }
+}
+
+float grid_base_cell(const OracleWorld& w) {
+    return grid_cell_size(w.counters[DYN_COUNTER_GRID_SCALE], w.counters[DYN_COUNTER_GRID_EXTENT]);
+}
+
+// immovable_entries.wgsl:8-29, collider_entries.wgsl:9-35, collider_emit.wgsl:6-63, then the
+// entry sort (broadphase/src/passes.rs:76-90: 4 digit passes over the cell key, payload = slot).
+void emit_entries(OracleWorld& w) {
+    float base = grid_base_cell(w);
+    w.counters[DYN_COUNTER_IMMOVABLE_LEVELS] = 0;
+    w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES] = 0;
+    std::vector<uint32_t> keys, order;
+    w.entries.clear();
+    uint32_t k = (uint32_t)w.colliders.size();
+    // slots in collider order (the reference takes them from an atomic counter, so any order is
+    // one of its possible layouts; the sorted keys do not depend on it).
+    {
+        for (uint32_t i = 0; i < k; ++i) {
+            uint32_t owner = w.owners[i];
+            if (owner == DYN_NO_BODY) continue;
+            const dyn_body_descriptor_record& d = w.descs[owner];
+            bool moves = body_moves_d(d.inverse_mass, d.flags);
+            bool awake = w.body_activity[owner] != 0u || w.wake_flags[owner] != 0u;
+            const Aabb& box = w.aabbs[i];
+            uint32_t level = shape_levels(box, base);
+            if (!moves) {
+                w.counters[DYN_COUNTER_IMMOVABLE_LEVELS] |= 1u << level;
+            } else {
+                w.counters[DYN_COUNTER_GRID_LEVELS] |= 1u << level;
+            }
+            GridCells cells = grid_cells(box, level_cell_size(level, base));
+            uint32_t count = grid_cell_count(cells);
+            uint32_t emitted = std::min(count, DYN_MAX_CELLS_PER_COLLIDER);
+            if (count > emitted) w.counters[DYN_COUNTER_ENTRY_FAULTS] += count - emitted;
+            if (level > 0u && awake) w.counters[DYN_COUNTER_COARSE_ACTIVE] += 1;
+            for (uint32_t ordinal = 0; ordinal < emitted; ++ordinal) {
+                I3 coord = grid_cell_at(cells, ordinal);
+                uint32_t offset = grid_cell_offset(cells, coord);
+                uint32_t info = i | (offset << DYN_ENTRY_CELL_SHIFT) | (DYN_ENTRY_KIND_COLLIDER << DYN_ENTRY_KIND_SHIFT);
+                if (moves && awake) info |= DYN_ENTRY_AWAKE;
+                if (moves) info |= DYN_ENTRY_MOBILE;
+                if (offset == 0u) info |= DYN_ENTRY_PRIMARY;
+                uint32_t slot = (uint32_t)w.entries.size();
+                w.entries.push_back(Entry{box, owner, info});
+                keys.push_back(cell_key(level, coord));
+                order.push_back(slot);
+                if (!moves) {
+                    w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES] += 1;
+                    w.counters[DYN_COUNTER_IMMOVABLE_EMITTED] += 1;
+                } else {
+                    w.counters[DYN_COUNTER_ENTRIES] += 1;
+                }
+            }
+        }
+    }
+    std::vector<uint32_t> zero(keys.size(), 0);
+    radix_sort_pairs(keys, zero, &order, 4, 0);
+    w.entry_keys = keys;
+    w.entry_order = order;
+}
+
+struct PairSink {
+    OracleWorld* w;
+    std::vector<uint32_t> major, minor;
+};
+
+// pair_emit.wgsl:3-31
+bool entry_awake(const OracleWorld& w, uint32_t node) {
+    const Entry& e = w.entries[node];
+    if ((e.info & DYN_ENTRY_MOBILE) == 0u) return w.wake_flags[e.group] != 0u;  // immovable region
+    return (e.info & DYN_ENTRY_AWAKE) != 0u;
+}
+void emit_pair(PairSink& sink, uint32_t first, uint32_t second) {
+    const Entry& a = sink.w->entries[first];
+    const Entry& b = sink.w->entries[second];
+    uint32_t ka = (a.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT;
+    uint32_t kb = (b.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT;
+    if (ka != DYN_ENTRY_KIND_COLLIDER || kb != DYN_ENTRY_KIND_COLLIDER) return;
+    if (first == second || a.group == b.group) return;
+    if ((a.info & DYN_ENTRY_MOBILE) == 0u && (b.info & DYN_ENTRY_MOBILE) == 0u) return;
+    uint32_t slot = sink.w->counters[DYN_COUNTER_PAIRS]++;
+    if (slot < sink.w->pair_capacity) {
+        uint32_t ia = a.info & DYN_ENTRY_INDEX_MASK;
+        uint32_t ib = b.info & DYN_ENTRY_INDEX_MASK;
+        sink.major.push_back(std::min(ia, ib));
+        sink.minor.push_back(std::max(ia, ib));
+    } else {
+        sink.w->counters[DYN_COUNTER_REFUSED_PAIRS] += 1;
+    }
+}
+I3 entry_cell(const Entry& e, float cs) {
+    uint32_t bits = (e.info & DYN_ENTRY_CELL_MASK) >> DYN_ENTRY_CELL_SHIFT;
+    I3 c = floor_div(e.box.min, cs);
+    return I3{c.x + (int32_t)(bits & 1u), c.y + (int32_t)((bits >> 1) & 1u), c.z + (int32_t)((bits >> 2) & 1u)};
+}
+I3 grid_overlap_cell(const Aabb& a, const Aabb& b, float cs) { return floor_div(vmax(a.min, b.min), cs); }
+void key_range(const OracleWorld& w, uint32_t key, uint32_t* first, uint32_t* last) {
+    auto lo = std::lower_bound(w.entry_keys.begin(), w.entry_keys.end(), key);
+    auto hi = std::upper_bound(w.entry_keys.begin(), w.entry_keys.end(), key);
+    *first = (uint32_t)(lo - w.entry_keys.begin());
+    *last = (uint32_t)(hi - w.entry_keys.begin());
+}
+
+// cell_pairs.wgsl:6-50 and level_links.wgsl:6-65, over one sorted entry array holding every
+// region; then the pair sort (narrowphase.rs:110-126: collider_slot_words digits per word).
+void broadphase(OracleWorld& w) {
+    PairSink sink{&w, {}, {}};
+    float grid = grid_base_cell(w);
+    uint32_t occupied = w.counters[DYN_COUNTER_GRID_LEVELS] | w.counters[DYN_COUNTER_RESTING_LEVELS]
+        | w.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
+    uint32_t live = (uint32_t)w.entry_keys.size();
+    // level_links first, then cell_pairs (passes.rs record order); the pair set is what matters.
+    for (uint32_t index = 0; index < live; ++index) {
+        uint32_t node = w.entry_order[index];
+        const Entry& e = w.entries[node];
+        if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
+        if ((e.info & DYN_ENTRY_PRIMARY) == 0u) continue;
+        bool awake = entry_awake(w, node);
+        if (!awake && w.counters[DYN_COUNTER_COARSE_ACTIVE] == 0u) continue;
+        uint32_t level = shape_levels(e.box, grid);
+        uint32_t coarser = occupied & ~((1u << std::min(level + 1u, 31u)) - 1u);
+        while (coarser != 0u) {
+            uint32_t link = 31u - (uint32_t)__builtin_clz(coarser);
+            coarser &= ~(1u << link);
+            float cs = level_cell_size(link, grid);
+            GridCells cells = grid_cells(e.box, cs);
+            uint32_t count = grid_cell_count(cells);
+            if ((long long)cells.max.x - cells.min.x > 3 || (long long)cells.max.y - cells.min.y > 3 ||
+                (long long)cells.max.z - cells.min.z > 3 || cells.max.x < cells.min.x || cells.max.y < cells.min.y ||
+                cells.max.z < cells.min.z) {
+                w.counters[DYN_COUNTER_ENTRY_FAULTS] += 1;  // non-finite box: same cut as the device
+                continue;
+            }
+            for (uint32_t ordinal = 0; ordinal < count; ++ordinal) {
+                I3 cell = grid_cell_at(cells, ordinal);
+                uint32_t first, last;
+                key_range(w, cell_key(link, cell), &first, &last);
+                for (uint32_t entry = first; entry < last; ++entry) {
+                    uint32_t other = w.entry_order[entry];
+                    if (other == node) continue;
+                    if (!awake && !entry_awake(w, other)) continue;
+                    const Entry& o = w.entries[other];
+                    if (!aabb_overlaps(e.box, o.box)) continue;
+                    if (!i3eq(entry_cell(o, cs), cell)) continue;
+                    if (!i3eq(grid_overlap_cell(e.box, o.box, cs), cell)) continue;
+                    emit_pair(sink, node, other);
+                }
+            }
+        }
+    }
+    for (uint32_t index = 0; index < live; ++index) {
+        uint32_t node = w.entry_order[index];
+        const Entry& e = w.entries[node];
+        if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
+        if (!entry_awake(w, node)) continue;
+        uint32_t level = shape_levels(e.box, grid);
+        float cs = level_cell_size(level, grid);
+        I3 cell = entry_cell(e, cs);
+        uint32_t first, last;
+        key_range(w, cell_key(level, cell), &first, &last);
+        for (uint32_t entry = first; entry < last; ++entry) {
+            if (entry == index) continue;
+            uint32_t other = w.entry_order[entry];
+            if (entry_awake(w, other) && entry < index) continue;
+            const Entry& o = w.entries[other];
+            if (!aabb_overlaps(e.box, o.box)) continue;
+            if (!i3eq(entry_cell(o, cs), cell)) continue;
+            if (!i3eq(grid_overlap_cell(e.box, o.box, cs), cell)) continue;
+            emit_pair(sink, node, other);
+        }
+    }
+    uint32_t words = key_words(std::max<uint32_t>((uint32_t)w.colliders.size(), 1u));
+    radix_sort_pairs(sink.major, sink.minor, nullptr, words, words);
+    w.pair_major = sink.major;
+    w.pair_minor = sink.minor;
+}
+
+// narrowphase.wgsl:518-685 for one pair; false when the pair answers no contact.
+bool narrowphase_pair(const OracleWorld& w, uint32_t first_slot, uint32_t second_slot, dyn_contact_record* out) {
+    uint32_t fb = w.owners[first_slot];
+    uint32_t sb = w.owners[second_slot];
+    if (fb == DYN_NO_BODY || sb == DYN_NO_BODY || fb == sb) return false;
+    Body first = body_at(w, fb);
+    Body second = body_at(w, sb);
+    if (!body_moves(first) && !body_moves(second)) return false;
+    const dyn_collider_record& fc = w.colliders[first_slot];
+    const dyn_collider_record& sc = w.colliders[second_slot];
+    if (fc.kind == DYN_SHAPE_NONE || sc.kind == DYN_SHAPE_NONE) return false;
+    uint32_t fg = fc.collision_group != DYN_NO_COLLISION_FILTER ? fc.collision_group : first.group;
+    uint32_t fm = fc.collision_mask != DYN_NO_COLLISION_FILTER ? fc.collision_mask : first.mask;
+    uint32_t sg = sc.collision_group != DYN_NO_COLLISION_FILTER ? sc.collision_group : second.group;
+    uint32_t sm = sc.collision_mask != DYN_NO_COLLISION_FILTER ? sc.collision_mask : second.mask;
+    if (!((fg & sm) != 0u && (sg & fm) != 0u)) return false;
+    // joined_pairs.wgsl: no joint filter without constraints.
+    bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
+    bool fw = shape_world_geometry(fc.kind);
+    bool sw = shape_world_geometry(sc.kind);
+    if (fw && sw) return false;
+    float margin = w.params.contact_margin;
+    if (body_has_ccd(first) || body_has_ccd(second)) {
+        margin = w.params.contact_margin + length(second.velocity - first.velocity) * w.params.dt;
+    }
+    Manifold m;
+    bool generated = false;
+    const Shapes& sh = w.shapes;
+    if (fw) {
+        if (fc.kind != DYN_SHAPE_PLANE) return false;  // meshes / heightfields not restated
+        WorldShape scene = world_collider(first.position, first.orientation, fc);
+        WorldShape ws = world_collider(second.position, second.orientation, sc);
+        m = plane_convex(sh, scene, ws, margin);
+        generated = m.point_count > 0u;
+    } else if (sw) {
+        if (sc.kind != DYN_SHAPE_PLANE) return false;
+        WorldShape scene = world_collider(second.position, second.orientation, sc);
+        WorldShape wf = world_collider(first.position, first.orientation, fc);
+        m = plane_convex(sh, scene, wf, margin);
+        m.normal = -m.normal;
+        mirror_features(&m);
+        generated = m.point_count > 0u;
+    } else if (scaled_shape(fc) || scaled_shape(sc) || !shape_analytic(fc.kind) || !shape_analytic(sc.kind)) {
+        WorldShape wf = world_collider(first.position, first.orientation, fc);
+        WorldShape ws = world_collider(second.position, second.orientation, sc);
+        ShapeHit hit = convex_hit(sh, wf, ws);
+        if (hit.distance <= margin) {
+            manifold_emit(&m, hit.normal);
+            generated = true;
+            if (!convex_pair_manifold(sh, wf, ws, hit.normal, &m)) manifold_from_hit(&m, hit, margin);
+        }
+    } else {
+        uint32_t a = fc.kind, b = sc.kind;
+        if (a == DYN_SHAPE_SPHERE && b == DYN_SHAPE_SPHERE) {
+            m = sphere_sphere(first, fc, second, sc, margin);
+        } else if (a == DYN_SHAPE_SPHERE && b == DYN_SHAPE_CUBOID) {
+            m = sphere_box(first, fc, second, sc, margin);
+        } else if (a == DYN_SHAPE_SPHERE && b == DYN_SHAPE_CAPSULE) {
+            m = sphere_capsule(first, fc, second, sc, margin);
+        } else if (a == DYN_SHAPE_CUBOID && b == DYN_SHAPE_SPHERE) {
+            m = sphere_box(second, sc, first, fc, margin);
+            m.normal = -m.normal;
+        } else if (a == DYN_SHAPE_CUBOID && b == DYN_SHAPE_CUBOID) {
+            m = box_box_sat(first, fc, second, sc, margin);
+        } else if (a == DYN_SHAPE_CAPSULE && b == DYN_SHAPE_SPHERE) {
+            m = sphere_capsule(second, sc, first, fc, margin);
+            m.normal = -m.normal;
+        } else if (a == DYN_SHAPE_CAPSULE && b == DYN_SHAPE_CAPSULE) {
+            m = capsule_capsule(first, fc, second, sc, margin);
+        } else {
+            WorldShape wf = world_collider(first.position, first.orientation, fc);
+            WorldShape ws = world_collider(second.position, second.orientation, sc);
+            ShapeHit hit = convex_hit(sh, wf, ws);
+            if (hit.distance <= margin) {
+                manifold_emit(&m, hit.normal);
+                if (!convex_pair_manifold(sh, wf, ws, hit.normal, &m)) manifold_from_hit(&m, hit, margin);
+            }
+        }
+        generated = true;
+    }
+    if (!generated || m.point_count == 0u) return false;
+    dyn_contact_record c;
+    std::memset(&c, 0, sizeof(c));
+    c.a = first_slot;
+    c.b = second_slot;
+    c.point_count = m.point_count;
+    c.sensor = sensor ? 1u : 0u;
+    c.first_body_id = first.body_id;
+    c.second_body_id = second.body_id;
+    c.first_generation = first.generation;
+    c.second_generation = second.generation;
+    wr3(c.normal, m.normal);
+    c.triangle = m.triangle;
+    c.surface = DYN_NO_SURFACE;
+    c.friction = material_combine(fc.friction, sc.friction, w.params.friction_combine);
+    c.restitution = material_combine(fc.restitution, sc.restitution, w.params.restitution_combine);
+    c.rolling_friction = fmaxw(fc.rolling_friction, sc.rolling_friction);
+    c.spin_friction = fmaxw(fc.spin_friction, sc.spin_friction);
+    c.relaxation = fc.relaxation + sc.relaxation;
+    c.damping_ratio = fmaxw(fc.damping_ratio, sc.damping_ratio);
+    c.events = (fc.flags & sc.flags) & (DYN_EVENT_MODE_BEGIN_END | DYN_EVENT_MODE_PERSIST);
+    for (uint32_t i = 0; i < m.point_count; ++i) {
+        dyn_manifold_point_record& p = c.points[i];
+        V3 point = m.points[i].position;
+        wr3(p.position, point);
+        p.depth = m.points[i].depth;
+        p.feature = m.points[i].feature;
+        wr3(p.local_a, quat_rotate(quat_conjugate(first.orientation), point - first.position));
+        wr3(p.local_b, quat_rotate(quat_conjugate(second.orientation), point - second.position));
+    }
+    *out = c;
+    return true;
+}
+
+// narrowphase pass + compact_scan/offsets/scatter.wgsl: contacts in pair order.
+void narrowphase(OracleWorld& w) {
+    w.contacts.clear();
+    size_t p = w.pair_major.size();
+    for (size_t i = 0; i < p; ++i) {
+        dyn_contact_record c;
+        if (!narrowphase_pair(w, w.pair_major[i], w.pair_minor[i], &c)) continue;
+        if (w.contacts.size() >= w.contact_capacity) {
+            w.counters[DYN_COUNTER_REFUSED_CONTACTS] += 1;
+            continue;
+        }
+        c.carried_normal = 0.0f;
+        c.carried_tangent = 0.0f;
+        w.contacts.push_back(c);
+    }
+    w.counters[DYN_COUNTER_CONTACTS] = (uint32_t)w.contacts.size();
+    w.contact_matched.assign(w.contacts.size(), 0);
+}
+
+// identity.wgsl:8-118
+bool contact_touches(const dyn_contact_record& c, float threshold) {
+    for (uint32_t i = 0; i < c.point_count; ++i) {
+        if (c.points[i].depth >= -threshold) return true;
+    }
+    return false;
+}
+bool contact_same_pair(const dyn_contact_record& h, const dyn_contact_record& c) {
+    bool same = h.first_body_id == c.first_body_id && h.first_generation == c.first_generation
+        && h.second_body_id == c.second_body_id && h.second_generation == c.second_generation && h.a == c.a
+        && h.b == c.b;
+    bool flipped = h.first_body_id == c.second_body_id && h.first_generation == c.second_generation
+        && h.second_body_id == c.first_body_id && h.second_generation == c.first_generation && h.a == c.b
+        && h.b == c.a;
+    return same || flipped;
+}
+float contact_normal_impulse(const dyn_contact_record& c) {
+    float total = 0.0f;
+    for (uint32_t i = 0; i < c.point_count; ++i) total = total + fmaxw(c.points[i].accumulated_normal, 0.0f);
+    return total;
+}
+float contact_tangent_impulse(const dyn_contact_record& c) {
+    float total = 0.0f;
+    for (uint32_t i = 0; i < c.point_count; ++i) {
+        const dyn_manifold_point_record& p = c.points[i];
+        total = total + std::sqrt(p.accumulated_tangent_1 * p.accumulated_tangent_1
+                                  + p.accumulated_tangent_2 * p.accumulated_tangent_2);
+    }
+    return total;
+}
+dyn_contact_record contact_relay_impulses(const dyn_contact_record& current, const dyn_contact_record& held) {
+    dyn_contact_record relayed = current;
+    bool taken[4] = {false, false, false, false};
+    for (uint32_t pi = 0; pi < current.point_count; ++pi) {
+        const dyn_manifold_point_record& point = relayed.points[pi];
+        uint32_t picked = DYN_NO_SLOT;
+        float picked_distance = 0.0f;
+        for (uint32_t hi = 0; hi < held.point_count; ++hi) {
+            if (taken[hi]) continue;
+            const dyn_manifold_point_record& hp = held.points[hi];
+            if (!(hp.feature == point.feature || hp.feature == feature_mirror(point.feature))) continue;
+            float distance = length(rd3(hp.local_a) - rd3(point.local_a)) + length(rd3(hp.local_b) - rd3(point.local_b));
+            if (picked == DYN_NO_SLOT || distance < picked_distance) {
+                picked = hi;
+                picked_distance = distance;
+            }
+        }
+        if (picked == DYN_NO_SLOT) continue;
+        taken[picked] = true;
+        relayed.points[pi].accumulated_normal = held.points[picked].accumulated_normal;
+        relayed.points[pi].accumulated_tangent_1 = held.points[picked].accumulated_tangent_1;
+        relayed.points[pi].accumulated_tangent_2 = held.points[picked].accumulated_tangent_2;
+    }
+    return relayed;
+}
+uint32_t resolve_row(const OracleWorld& w, uint32_t id, uint32_t generation) {
+    if (id >= w.row_of_id.size()) return DYN_NO_BODY;
+    uint32_t row = w.row_of_id[id];
+    if (row == DYN_NO_BODY || w.states[row].generation != generation) return DYN_NO_BODY;
+    return row;
+}
+
+// contact_relay.wgsl:34-71 and contact_begin.wgsl:41-71 (event publication left out)
+void relay_contacts(OracleWorld& w) {
+    uint32_t count = (uint32_t)w.contacts.size();
+    for (const dyn_contact_record& held : w.archive) {
+        uint32_t fr = resolve_row(w, held.first_body_id, held.first_generation);
+        uint32_t sr = resolve_row(w, held.second_body_id, held.second_generation);
+        if (fr == DYN_NO_BODY || sr == DYN_NO_BODY) continue;
+        uint32_t lo = 0, hi = count;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) / 2;
+            const dyn_contact_record& cand = w.contacts[mid];
+            if (cand.a < held.a || (cand.a == held.a && cand.b < held.b)) {
+                lo = mid + 1;
+            } else {
+                hi = mid;
+            }
+        }
+        if (!(lo < count && w.contacts[lo].a == held.a && w.contacts[lo].b == held.b)) continue;
+        dyn_contact_record current = w.contacts[lo];
+        if (!contact_same_pair(held, current)) continue;
+        if ((held.events & DYN_CONTACT_ANNOUNCED) == 0u) continue;
+        w.contact_matched[lo] = 1;
+        dyn_contact_record relayed = contact_relay_impulses(current, held);
+        relayed.carried_normal = contact_normal_impulse(relayed);
+        relayed.carried_tangent = contact_tangent_impulse(relayed);
+        relayed.events |= DYN_CONTACT_ANNOUNCED;
+        w.contacts[lo] = relayed;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        if (w.contact_matched[i] != 0u) continue;
+        if (contact_touches(w.contacts[i], w.params.slop)) w.contacts[i].events |= DYN_CONTACT_ANNOUNCED;
+    }
+}
+
+// island_link.wgsl:1-45
+uint32_t island_find(const OracleWorld& w, uint32_t node) {
+    uint32_t current = node;
+    uint32_t parent = w.island_parents[current];
+    while (parent != current) {
+        current = parent;
+        parent = w.island_parents[current];
+    }
+    return current;
+}
+void island_couple(OracleWorld& w, uint32_t first, uint32_t second) {
+    uint32_t dc = w.params.dynamic_count;
+    // carry_static_wake(first, second) then carry_static_wake(second, first)
+    if (second >= dc && w.wake_flags[second] != 0u) w.wake_flags[first] |= 1u;
+    if (first >= dc && w.wake_flags[first] != 0u) w.wake_flags[second] |= 1u;
+    if (first >= dc || second >= dc || first == second) return;
+    uint32_t a = island_find(w, first);
+    uint32_t b = island_find(w, second);
+    if (a == b) return;
+    uint32_t lower = std::min(a, b), higher = std::max(a, b);
+    w.island_parents[higher] = lower;
+}
+
+// islands.rs:237-258 BuildIslands.record
+void build_islands(OracleWorld& w) {
+    relay_contacts(w);
+    uint32_t dc = w.params.dynamic_count;
+    w.island_parents.resize(dc);
+    w.island_state.assign(dc, 0);
+    for (uint32_t i = 0; i < dc; ++i) w.island_parents[i] = i;
+    for (const dyn_contact_record& c : w.contacts) {
+        if (c.point_count == 0u || c.sensor == 1u || !contact_touches(c, w.params.slop)) continue;
+        island_couple(w, w.owners[c.a], w.owners[c.b]);
+    }
+    uint32_t rounds = 32 - (uint32_t)__builtin_clz(std::max(dc, 2u));  // ilog2(max(N,2)) + 1
+    for (uint32_t r = 0; r < rounds; ++r) {
+        std::vector<uint32_t> next(dc);
+        for (uint32_t i = 0; i < dc; ++i) {
+            uint32_t parent = w.island_parents[i];
+            next[i] = std::min(parent, w.island_parents[parent]);
+        }
+        w.island_parents.swap(next);
+    }
+    for (uint32_t i = 0; i < dc; ++i) {
+        if (w.wake_flags[i] == 0u && w.body_motion[i] == 0u) continue;
+        uint32_t root = w.island_parents[i];
+        w.island_state[root] = std::max(w.island_state[root], DYN_ISLAND_WAKE);
+    }
+    for (uint32_t i = 0; i < dc; ++i) {
+        if (w.island_parents[i] == i) w.counters[DYN_COUNTER_ISLANDS] += 1;
+    }
+}
+
+// island_wake.wgsl:10-22 and live.wgsl:8-18
+void wake_and_live(OracleWorld& w) {
+    uint32_t dc = w.params.dynamic_count;
+    for (uint32_t i = 0; i < dc; ++i) {
+        uint32_t root = w.island_parents[i];
+        dyn_body_state_record& s = w.states[i];
+        if (s.sleeping != 0u && (w.island_state[root] & DYN_ISLAND_WAKE) != 0u) {
+            w.counters[DYN_COUNTER_WOKE] += 1;
+            w.counters[DYN_COUNTER_WOKE_DEFERRED] += 1;
+            s.sleeping = 0;
+            s.sleep_timer = 0.0f;
+        }
+        w.wake_flags[i] = 0;
+    }
+    w.live.clear();
+    for (uint32_t i = 0; i < dc; ++i) {
+        if (body_is_active(w.states[i], w.descs[i])) w.live.push_back(i);
+    }
+    w.counters[DYN_COUNTER_LIVE] = (uint32_t)w.live.size();
+}
+
+// core.wgsl:6-12
+inline int32_t solver_word(float value, float scale) {
+    return (int32_t)clampw(value * scale, -2.0e9f, 2.0e9f);
+}
+inline float solver_value(int32_t word, float scale) { return (float)word / scale; }
+
+Body body_split(Body b, float scale) {
+    b.inverse_mass = b.inverse_mass * scale;
+    for (int i = 0; i < 6; ++i) b.inverse_inertia[i] = b.inverse_inertia[i] * scale;
+    return b;
+}
+inline bool contact_block_resolves(const dyn_contact_record& c) { return c.point_count > 0u && c.sensor == 0u; }
+
+// solver_reset.wgsl, solver_total.wgsl, solver_blocks.wgsl:24-48
+void solver_prepare(OracleWorld& w) {
+    uint32_t n = (uint32_t)w.states.size();
+    uint32_t c = (uint32_t)w.contacts.size();
+    w.block_counts.assign(n, 0);
+    w.resolution.assign(n, splat3(0.0f));
+    w.counters[DYN_COUNTER_BLOCKS] = c;
+    w.counters[DYN_COUNTER_SOLVER_ROWS] = 0;
+    w.blocks.assign(2 * (size_t)c, 0);
+    w.target_speeds.assign(4 * (size_t)c, 0.0f);
+    w.solver_rows.clear();
+    w.velocity_deltas.assign(8 * (size_t)n, 0);
+    w.position_deltas.assign(8 * (size_t)n, 0);
+    w.contributions.assign(n, 0);
+    for (uint32_t index = 0; index < c; ++index) {
+        const dyn_contact_record& contact = w.contacts[index];
+        uint32_t fb = w.owners[contact.a];
+        uint32_t sb = w.owners[contact.b];
+        w.blocks[2 * index] = fb;
+        w.blocks[2 * index + 1] = sb;
+        if (!contact_block_resolves(contact)) continue;
+        Body first = body_at(w, fb);
+        Body second = body_at(w, sb);
+        for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+            V3 position = rd3(contact.points[pi].position);
+            float speed = dot(relative_velocity(first, second, position, position), rd3(contact.normal));
+            float target = 0.0f;
+            if (contact.points[pi].depth < 0.0f) {
+                target = contact.points[pi].depth / w.params.dt;
+            } else if (speed < -w.params.restitution_threshold) {
+                target = -speed * contact.restitution;
+            }
+            w.target_speeds[4 * (size_t)index + pi] = target;
+        }
+        for (uint32_t row : {fb, sb}) {
+            if (w.block_counts[row]++ == 0u) {
+                w.solver_rows.push_back(row);
+                w.counters[DYN_COUNTER_SOLVER_ROWS] += 1;
+            }
+        }
+    }
+}
+
+void accumulate(std::vector<int32_t>& deltas, uint32_t row, V3 linear, V3 angular, float scale) {
+    int32_t* d = &deltas[8 * (size_t)row];
+    // i32 wrapping adds, as WGSL atomicAdd on u32 words
+    auto add = [](int32_t* word, int32_t v) { *word = (int32_t)((uint32_t)*word + (uint32_t)v); };
+    add(d + 0, solver_word(linear.x, scale));
+    add(d + 1, solver_word(linear.y, scale));
+    add(d + 2, solver_word(linear.z, scale));
+    add(d + 3, solver_word(angular.x, scale));
+    add(d + 4, solver_word(angular.y, scale));
+    add(d + 5, solver_word(angular.z, scale));
+}
+
+V3 manifold_arm(const Body& b, const dyn_manifold_point_record& p, bool first) {
+    return quat_rotate(b.orientation, first ? rd3(p.local_a) : rd3(p.local_b)) + b.position;
+}
+float point_momentum_mass(const Body& a, const Body& b, V3 pa, V3 pb, V3 axis) {
+    V3 ra = pa - body_com(a);
+    V3 rb = pb - body_com(b);
+    V3 rax = cross(ra, axis);
+    V3 rbx = cross(rb, axis);
+    return a.inverse_mass + b.inverse_mass + dot(rax, apply_inverse_inertia(a, rax))
+        + dot(rbx, apply_inverse_inertia(b, rbx));
+}
+void apply_pair_impulse(Body* a, Body* b, V3 pa, V3 pb, V3 impulse) {
+    a->velocity = a->velocity - impulse * a->inverse_mass;
+    a->angular_velocity = a->angular_velocity - apply_inverse_inertia(*a, cross(pa - body_com(*a), impulse));
+    b->velocity = b->velocity + impulse * b->inverse_mass;
+    b->angular_velocity = b->angular_velocity + apply_inverse_inertia(*b, cross(pb - body_com(*b), impulse));
+}
+struct Tangents {
+    V3 first, second;
+};
+Tangents make_tangents(V3 normal) {
+    V3 tangent = V3{1.0f, 0.0f, 0.0f};
+    if (std::fabs(normal.x) > 0.9f) tangent = V3{0.0f, 1.0f, 0.0f};
+    V3 t1 = normalize(cross(normal, tangent));
+    V3 t2 = cross(normal, t1);
+    return Tangents{t1, t2};
+}
+// core.wgsl:326-345
+float contact_normal_delta(const dyn_contact_record& c, float mass, float truth, float step, float goal, float depth,
+                           float speed, float accumulated) {
+    if (c.relaxation <= 0.0f) return (goal - speed) / mass;
+    float bias = fmaxw(depth / step, goal);
+    float drag = 2.0f * c.damping_ratio * c.relaxation / step;
+    float softness = c.relaxation * c.relaxation * truth / (step * step);
+    float prior = speed - accumulated * truth;
+    float wanted = (bias - (1.0f + drag) * prior) / (softness + (1.0f + drag) * truth);
+    return truth * (wanted - accumulated) / mass;
+}
+
+// solver_contact_block.wgsl:195-233
+void warm_contact_block(OracleWorld& w, uint32_t index) {
+    const dyn_contact_record& contact = w.contacts[index];
+    uint32_t fr = w.blocks[2 * index], sr = w.blocks[2 * index + 1];
+    if (!contact_block_resolves(contact)) {
+        accumulate(w.velocity_deltas, fr, splat3(0.0f), splat3(0.0f), DYN_SOLVER_VELOCITY_SCALE);
+        accumulate(w.velocity_deltas, sr, splat3(0.0f), splat3(0.0f), DYN_SOLVER_VELOCITY_SCALE);
+        return;
+    }
+    Body fl = body_at(w, fr), sl = body_at(w, sr);
+    Body first = body_is_inert(fl) ? body_frozen(fl) : fl;
+    Body second = body_is_inert(sl) ? body_frozen(sl) : sl;
+    V3 normal = rd3(contact.normal);
+    Tangents t = make_tangents(normal);
+    for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+        const dyn_manifold_point_record& p = contact.points[pi];
+        V3 af = manifold_arm(first, p, true);
+        V3 as = manifold_arm(second, p, false);
+        V3 impulse = normal * p.accumulated_normal + t.first * p.accumulated_tangent_1 + t.second * p.accumulated_tangent_2;
+        apply_pair_impulse(&first, &second, af, as, impulse);
+    }
+    accumulate(w.velocity_deltas, fr, first.velocity - fl.velocity, first.angular_velocity - fl.angular_velocity,
+               DYN_SOLVER_VELOCITY_SCALE);
+    accumulate(w.velocity_deltas, sr, second.velocity - sl.velocity, second.angular_velocity - sl.angular_velocity,
+               DYN_SOLVER_VELOCITY_SCALE);
+}
+
+// solver_contact_block.wgsl:6-193 and solver_block_solve.wgsl:39-94
+void solve_contact_block(OracleWorld& w, uint32_t index, bool residual) {
+    dyn_contact_record& stored = w.contacts[index];
+    const dyn_contact_record contact = stored;
+    uint32_t fr = w.blocks[2 * index], sr = w.blocks[2 * index + 1];
+    auto commit = [&](V3 da, V3 sa, V3 db, V3 sb) {
+        accumulate(w.velocity_deltas, fr, da, sa, DYN_SOLVER_VELOCITY_SCALE);
+        accumulate(w.velocity_deltas, sr, db, sb, DYN_SOLVER_VELOCITY_SCALE);
+        if (!residual) return;
+        uint32_t lin = (uint32_t)solver_word(fmaxw(length(da), length(db)), DYN_SOLVER_VELOCITY_SCALE);
+        uint32_t ang = (uint32_t)solver_word(fmaxw(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE);
+        w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL] = std::max(w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL], lin);
+        w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL] = std::max(w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL], ang);
+    };
+    V3 zero = splat3(0.0f);
+    if (!contact_block_resolves(contact)) {
+        commit(zero, zero, zero, zero);
+        return;
+    }
+    Body pf = body_at(w, fr), ps = body_at(w, sr);
+    Body split_f = body_split(pf, (float)std::max(w.block_counts[fr], 1u));
+    Body split_s = body_split(ps, (float)std::max(w.block_counts[sr], 1u));
+    if (body_is_inert(pf)) {
+        pf = body_frozen(pf);
+        split_f = body_frozen(split_f);
+    }
+    if (body_is_inert(ps)) {
+        ps = body_frozen(ps);
+        split_s = body_frozen(split_s);
+    }
+    if (body_is_inert(pf) && body_is_inert(ps)) {
+        commit(zero, zero, zero, zero);
+        return;
+    }
+    Body first = pf, second = ps;
+    V3 normal = rd3(contact.normal);
+    Tangents t = make_tangents(normal);
+    dyn_contact_record updated = contact;
+    V3 reach_f = zero, reach_s = zero;
+    for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+        reach_f = reach_f + (manifold_arm(pf, contact.points[pi], true) - body_com(pf));
+        reach_s = reach_s + (manifold_arm(ps, contact.points[pi], false) - body_com(ps));
+    }
+    float point_count = (float)std::max(contact.point_count, 1u);
+    float normal_total = 0.0f;
+    for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+        normal_total = normal_total + fmaxw(contact.points[pi].accumulated_normal, 0.0f);
+    }
+    V3 impulses[4] = {zero, zero, zero, zero};
+    for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+        const dyn_manifold_point_record& p = contact.points[pi];
+        V3 af = manifold_arm(pf, p, true);
+        V3 as = manifold_arm(ps, p, false);
+        float acc_n = p.accumulated_normal;
+        float acc_t1 = p.accumulated_tangent_1;
+        float acc_t2 = p.accumulated_tangent_2;
+        float normal_speed = dot(relative_velocity(pf, ps, af, as), normal);
+        // manifold_row_mass (solver_contact_block.wgsl:14-29)
+        V3 arm_f = cross(af - body_com(split_f), normal);
+        V3 arm_s = cross(as - body_com(split_s), normal);
+        float normal_mass = point_count * (split_f.inverse_mass + split_s.inverse_mass)
+            + dot(apply_inverse_inertia(split_f, cross(reach_f, normal)), arm_f)
+            + dot(apply_inverse_inertia(split_s, cross(reach_s, normal)), arm_s);
+        float normal_truth = point_momentum_mass(pf, ps, af, as, normal);
+        float delta = contact_normal_delta(contact, normal_mass, normal_truth, w.params.dt,
+                                           w.target_speeds[4 * (size_t)index + pi], p.depth, normal_speed, acc_n);
+        float next_normal = fmaxw(0.0f, acc_n + delta);
+        impulses[pi] = impulses[pi] + normal * (next_normal - acc_n);
+        acc_n = next_normal;
+        float friction_limit = contact.friction * acc_n;
+        float t1_mass = point_momentum_mass(split_f, split_s, af, as, t.first) * (float)std::max(contact.point_count, 1u);
+        float t1_speed = dot(relative_velocity(pf, ps, af, as), t.first);
+        float next_t1 = clampw(acc_t1 - t1_speed / t1_mass, -friction_limit, friction_limit);
+        impulses[pi] = impulses[pi] + t.first * (next_t1 - acc_t1);
+        acc_t1 = next_t1;
+        float t2_mass = point_momentum_mass(split_f, split_s, af, as, t.second) * (float)std::max(contact.point_count, 1u);
+        float t2_speed = dot(relative_velocity(pf, ps, af, as), t.second);
+        float remaining = std::sqrt(fmaxw(friction_limit * friction_limit - acc_t1 * acc_t1, 0.0f));
+        float next_t2 = clampw(acc_t2 - t2_speed / t2_mass, -remaining, remaining);
+        impulses[pi] = impulses[pi] + t.second * (next_t2 - acc_t2);
+        acc_t2 = next_t2;
+        updated.points[pi].accumulated_normal = acc_n;
+        updated.points[pi].accumulated_tangent_1 = acc_t1;
+        updated.points[pi].accumulated_tangent_2 = acc_t2;
+    }
+    for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+        V3 af = manifold_arm(pf, contact.points[pi], true);
+        V3 as = manifold_arm(ps, contact.points[pi], false);
+        apply_pair_impulse(&first, &second, af, as, impulses[pi]);
+    }
+    V3 rel_spin = second.angular_velocity - first.angular_velocity;
+    V3 planar_spin = rel_spin - normal * dot(rel_spin, normal);
+    float planar_len = length(planar_spin);
+    if (planar_len > 1e-6f) {
+        V3 axis = planar_spin / planar_len;
+        float mass = dot(axis, apply_inverse_inertia(split_f, axis)) + dot(axis, apply_inverse_inertia(split_s, axis));
+        if (mass > 0.0f) {
+            float limit = contact.rolling_friction * normal_total;
+            float applied = clampw(-planar_len / mass, -limit, limit);
+            first.angular_velocity = first.angular_velocity - apply_inverse_inertia(first, axis * applied);
+            second.angular_velocity = second.angular_velocity + apply_inverse_inertia(second, axis * applied);
+        }
+    }
+    float twist = dot(rel_spin, normal);
+    if (std::fabs(twist) > 1e-6f) {
+        float mass = dot(normal, apply_inverse_inertia(split_f, normal)) + dot(normal, apply_inverse_inertia(split_s, normal));
+        if (mass > 0.0f) {
+            float limit = contact.spin_friction * normal_total;
+            float applied = clampw(-twist / mass, -limit, limit);
+            first.angular_velocity = first.angular_velocity - apply_inverse_inertia(first, normal * applied);
+            second.angular_velocity = second.angular_velocity + apply_inverse_inertia(second, normal * applied);
+        }
+    }
+    stored = updated;
+    commit(first.velocity - pf.velocity, first.angular_velocity - pf.angular_velocity, second.velocity - ps.velocity,
+           second.angular_velocity - ps.angular_velocity);
+}
+
+// solver_block_apply.wgsl:7-29
+void block_apply(OracleWorld& w) {
+    if (!w.solver_rows.empty()) w.solver_rounds += 1;
+    for (uint32_t row : w.solver_rows) {
+        int32_t* d = &w.velocity_deltas[8 * (size_t)row];
+        V3 linear = V3{solver_value(d[0], DYN_SOLVER_VELOCITY_SCALE), solver_value(d[1], DYN_SOLVER_VELOCITY_SCALE),
+                       solver_value(d[2], DYN_SOLVER_VELOCITY_SCALE)};
+        V3 angular = V3{solver_value(d[3], DYN_SOLVER_VELOCITY_SCALE), solver_value(d[4], DYN_SOLVER_VELOCITY_SCALE),
+                        solver_value(d[5], DYN_SOLVER_VELOCITY_SCALE)};
+        for (int k = 0; k < 6; ++k) d[k] = 0;
+        if (veq(linear, splat3(0.0f)) && veq(angular, splat3(0.0f))) continue;
+        dyn_body_state_record& s = w.states[row];
+        wr3(s.velocity, rd3(s.velocity) + linear);
+        wr3(s.angular_velocity, rd3(s.angular_velocity) + angular);
+    }
+}
+
+// substep_integrate.wgsl:15-76 (no force fields)
+void substep_integrate(OracleWorld& w) {
+    w.solver_rounds = 0;
+    const dyn_step_params& p = w.params;
+    float h = p.substep_dt;
+    for (uint32_t row : w.live) {
+        const dyn_body_descriptor_record& d = w.descs[row];
+        if (!body_simulates_d(d.inverse_mass, d.flags)) continue;
+        dyn_body_state_record& s = w.states[row];
+        V4 q = rd4(s.orientation);
+        V3 acceleration = V3{p.gravity[0], p.gravity[1], p.gravity[2]} * d.gravity_scale + rd3(s.force) * d.inverse_mass;
+        V3 spin = rd3(s.angular_velocity);
+        V3 velocity = rd3(s.velocity) + acceleration * h;
+        // gyroscopic_spin
+        V3 gyro = spin;
+        const float* I = d.inertia;
+        bool isotropic = I[1] == 0.0f && I[2] == 0.0f && I[4] == 0.0f && I[0] == I[3] && I[3] == I[5];
+        if (!isotropic) {
+            V3 body_spin = quat_rotate(quat_conjugate(q), spin);
+            V3 momentum = symmetric_apply(I, body_spin);
+            if (!veq(cross(body_spin, momentum), splat3(0.0f))) {
+                V3 solved = momentum;
+                for (int it = 0; it < 4; ++it) {
+                    V3 midpoint = 0.5f * (momentum + solved);
+                    solved = rotate_about(-symmetric_apply(d.inverse_inertia, midpoint) * h, momentum);
+                }
+                gyro = quat_rotate(q, symmetric_apply(d.inverse_inertia, solved));
+            }
+        }
+        V3 angular = gyro + apply_inverse_inertia_of(d.inverse_inertia, q, rd3(s.torque) * h);
+        float speed = length(velocity);
+        if (speed > p.max_velocity) velocity = velocity * (p.max_velocity / speed);
+        float spin_speed = length(angular);
+        if (spin_speed > p.max_angular_velocity) angular = angular * (p.max_angular_velocity / spin_speed);
+        velocity = velocity / (1.0f + d.linear_damping * h);
+        angular = angular / (1.0f + d.angular_damping * h);
+        wr3(s.velocity, velocity);
+        wr3(s.angular_velocity, angular);
+    }
+}
+
+// substep_advance.wgsl:6-13
+void substep_advance(OracleWorld& w) {
+    float h = w.params.substep_dt;
+    for (uint32_t row : w.live) {
+        dyn_body_state_record& s = w.states[row];
+        wr3(s.position, rd3(s.position) + rd3(s.velocity) * h);
+        V3 av = rd3(s.angular_velocity);
+        V4 spin = V4{av.x, av.y, av.z, 0.0f};
+        V4 q = rd4(s.orientation);
+        wr4(s.orientation, normalize(q + 0.5f * h * quat_mul(spin, q)));
+    }
+}
+
+// position_correction.wgsl:5-46 + position_block.wgsl:11-33
+void position_block(OracleWorld& w) {
+    uint32_t c = (uint32_t)w.contacts.size();
+    for (uint32_t index = 0; index < c; ++index) {
+        const dyn_contact_record& contact = w.contacts[index];
+        if (!contact_block_resolves(contact) || contact.relaxation > 0.0f) continue;
+        uint32_t fr = w.blocks[2 * index], sr = w.blocks[2 * index + 1];
+        Body fl = body_at(w, fr), sl = body_at(w, sr);
+        Body first = body_is_inert(fl) ? body_frozen(fl) : fl;
+        Body second = body_is_inert(sl) ? body_frozen(sl) : sl;
+        V3 normal = rd3(contact.normal);
+        float resolved = dot(normal, w.resolution[sr] - w.resolution[fr]);
+        V3 total = splat3(0.0f);
+        uint32_t contributing = 0;
+        for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+            float error = fmaxw(contact.points[pi].depth - w.params.slop - resolved, 0.0f);
+            if (error <= 0.0f) continue;
+            float k = first.inverse_mass + second.inverse_mass;
+            if (k == 0.0f) continue;
+            total = total + normal * (w.params.relaxation * error / k);
+            contributing += 1;
+        }
+        if (contributing == 0u) continue;
+        V3 correction = total / (float)contributing;
+        V3 lin_f = -correction * first.inverse_mass;
+        V3 lin_s = correction * second.inverse_mass;
+        // correction.wgsl:18-31 pair_holds
+        bool holds = dot(lin_f, lin_f) > 0.0f || dot(lin_s, lin_s) > 0.0f;
+        if (!holds) continue;
+        w.contributions[fr] += 1;
+        w.contributions[sr] += 1;
+        accumulate(w.position_deltas, fr, lin_f, splat3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        accumulate(w.position_deltas, sr, lin_s, splat3(0.0f), DYN_SOLVER_POSITION_SCALE);
+    }
+}
+
+// position_apply.wgsl:12-27
+void position_apply(OracleWorld& w) {
+    for (uint32_t row : w.solver_rows) {
+        uint32_t contributing = w.contributions[row];
+        w.contributions[row] = 0;
+        int32_t* d = &w.position_deltas[8 * (size_t)row];
+        V3 linear = V3{solver_value(d[0], DYN_SOLVER_POSITION_SCALE), solver_value(d[1], DYN_SOLVER_POSITION_SCALE),
+                       solver_value(d[2], DYN_SOLVER_POSITION_SCALE)};
+        V3 angular = V3{solver_value(d[3], DYN_SOLVER_POSITION_SCALE), solver_value(d[4], DYN_SOLVER_POSITION_SCALE),
+                        solver_value(d[5], DYN_SOLVER_POSITION_SCALE)};
+        for (int k = 0; k < 6; ++k) d[k] = 0;
+        if (contributing == 0u) continue;
+        V3 applied_linear = linear / (float)contributing;
+        V3 applied_angular = angular / (float)contributing;
+        dyn_body_state_record& s = w.states[row];
+        wr3(s.position, rd3(s.position) + applied_linear);
+        V3 ha = applied_angular * 0.5f;
+        wr4(s.orientation, normalize(quat_mul(V4{ha.x, ha.y, ha.z, 1.0f}, rd4(s.orientation))));
+        w.resolution[row] = w.resolution[row] + applied_linear;
+    }
+}
+
+// solver.rs:304-333 SolveSubsteps.record (no joints)
+void solve_substeps(OracleWorld& w) {
+    uint32_t c = (uint32_t)w.contacts.size();
+    for (uint32_t substep = 0; substep < w.params.substeps; ++substep) {
+        substep_integrate(w);
+        if (substep == 0) {
+            for (uint32_t i = 0; i < c; ++i) warm_contact_block(w, i);
+            block_apply(w);
+        }
+        for (uint32_t it = 0; it < w.params.solve_iterations; ++it) {
+            bool residual = w.solver_rounds == w.params.solve_iterations;
+            for (uint32_t i = 0; i < c; ++i) solve_contact_block(w, i, residual);
+            block_apply(w);
+        }
+        substep_advance(w);
+        for (uint32_t it = 0; it < w.params.position_iterations; ++it) {
+            position_block(w);
+            position_apply(w);
+        }
+    }
+}
+
+// island_sleep.wgsl:10-29 (core.wgsl:218-227 freeze_body)
+void sleep(OracleWorld& w) {
+    for (uint32_t i = 0; i < w.params.dynamic_count; ++i) {
+        dyn_body_state_record& s = w.states[i];
+        if (s.sleeping != 0u || !body_simulates_d(w.descs[i].inverse_mass, w.descs[i].flags)) continue;
+        uint32_t root = w.island_parents[i];
+        bool disturbed = (w.island_state[root] & DYN_ISLAND_WAKE) != 0u || w.wake_flags[i] != 0u;
+        if (disturbed) {
+            s.sleep_timer = 0.0f;
+        } else {
+            s.sleep_timer = s.sleep_timer + w.params.dt;
+            if (s.sleep_timer >= w.params.sleep_time) {
+                wr3(s.velocity, splat3(0.0f));
+                wr3(s.angular_velocity, splat3(0.0f));
+                wr3(s.force, splat3(0.0f));
+                wr3(s.torque, splat3(0.0f));
+                for (int k = 0; k < 3; ++k) s.prev_position[k] = s.position[k];
+                for (int k = 0; k < 4; ++k) s.prev_orientation[k] = s.orientation[k];
+                s.sleep_timer = 0.0f;
+                s.sleeping = 1;
+                w.counters[DYN_COUNTER_SLEPT] += 1;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// ---- C API for ctypes (tests and bench only) ----
+extern "C" {
+
+OracleWorld* orc_world_create(const dyn_step_params* params, const dyn_body_state_record* states,
+                              const dyn_body_descriptor_record* descs, uint32_t n, const dyn_collider_record* colliders,
+                              const uint32_t* owners, uint32_t k, const dyn_shape_source_record* sources,
+                              uint32_t source_count, const float* vertices, uint32_t vertex_count,
+                              uint32_t pair_capacity, uint32_t contact_capacity) {
+    OracleWorld* w = new OracleWorld();
+    w->params = *params;
+    w->params.body_count = n;
+    w->params.collider_count = k;
+    w->states.assign(states, states + n);
+    w->descs.assign(descs, descs + n);
+    w->colliders.assign(colliders, colliders + k);
+    w->owners.assign(owners, owners + k);
+    w->sources.assign(sources, sources + source_count);
+    w->vertices.resize(vertex_count);
+    for (uint32_t i = 0; i < vertex_count; ++i) {
+        w->vertices[i] = V4{vertices[4 * i], vertices[4 * i + 1], vertices[4 * i + 2], vertices[4 * i + 3]};
+    }
+    w->shapes.sources = w->sources.data();
+    w->shapes.source_count = source_count;
+    w->shapes.vertices = w->vertices.data();
+    w->shapes.vertex_count = vertex_count;
+    uint32_t max_id = 0;
+    for (uint32_t i = 0; i < n; ++i) max_id = std::max(max_id, states[i].body_id + 1);
+    w->row_of_id.assign(max_id, DYN_NO_BODY);
+    for (uint32_t i = 0; i < n; ++i) w->row_of_id[states[i].body_id] = i;
+    w->pair_capacity = pair_capacity;
+    w->contact_capacity = contact_capacity;
+    w->wake_flags.assign(n, 0);
+    return w;
+}
+
+void orc_world_destroy(OracleWorld* w) { delete w; }
+
+void orc_step(OracleWorld* w, float dt) {
+    w->params.dt = dt;
+    w->params.substep_dt = dt / (float)w->params.substeps;
+    apply_commands(*w);
+    prepare(*w);
+    emit_entries(*w);
+    broadphase(*w);
+    narrowphase(*w);
+    build_islands(*w);
+    wake_and_live(*w);
+    solver_prepare(*w);
+    solve_substeps(*w);
+    sleep(*w);
+    w->archive = w->contacts;  // commit: contact_archive.wgsl + archive_count_sync.wgsl
+    w->counters[DYN_COUNTER_ARCHIVED] = (uint32_t)w->archive.size();
+    w->counters[DYN_COUNTER_STEP] += 1;
+}
+
+void orc_counters(const OracleWorld* w, uint32_t* out) {
+    for (uint32_t i = 0; i < DYN_COUNTER_DEVICE_COUNT; ++i) out[i] = w->counters[i];
+}
+uint32_t orc_states(const OracleWorld* w, dyn_body_state_record* out) {
+    if (out) std::memcpy(out, w->states.data(), w->states.size() * sizeof(dyn_body_state_record));
+    return (uint32_t)w->states.size();
+}
+uint32_t orc_aabbs(const OracleWorld* w, float* out) {
+    if (out) {
+        for (size_t i = 0; i < w->aabbs.size(); ++i) {
+            wr3(out + 8 * i, w->aabbs[i].min);
+            out[8 * i + 3] = 0.0f;
+            wr3(out + 8 * i + 4, w->aabbs[i].max);
+            out[8 * i + 7] = 0.0f;
+        }
+    }
+    return (uint32_t)w->aabbs.size();
+}
+uint32_t orc_entry_keys(const OracleWorld* w, uint32_t* keys, uint32_t* colliders) {
+    size_t e = w->entry_keys.size();
+    for (size_t i = 0; i < e && keys; ++i) {
+        keys[i] = w->entry_keys[i];
+        colliders[i] = w->entries[w->entry_order[i]].info;
+    }
+    return (uint32_t)e;
+}
+uint32_t orc_pairs(const OracleWorld* w, uint32_t* major, uint32_t* minor) {
+    size_t p = w->pair_major.size();
+    if (major) {
+        std::memcpy(major, w->pair_major.data(), p * 4);
+        std::memcpy(minor, w->pair_minor.data(), p * 4);
+    }
+    return (uint32_t)p;
+}
+uint32_t orc_contacts(const OracleWorld* w, dyn_contact_record* out) {
+    if (out) std::memcpy(out, w->contacts.data(), w->contacts.size() * sizeof(dyn_contact_record));
+    return (uint32_t)w->contacts.size();
+}
+uint32_t orc_islands(const OracleWorld* w, uint32_t* out) {
+    if (out) std::memcpy(out, w->island_parents.data(), w->island_parents.size() * 4);
+    return (uint32_t)w->island_parents.size();
+}
+
+// Known-answer hooks for the math and sort restatements.
+float orc_sin(float x) { return osin(x); }
+float orc_cos(float x) { return ocos(x); }
+float orc_atan2(float y, float x) { return oatan2(y, x); }
+uint32_t orc_key_words(uint32_t n) { return key_words(n); }
+void orc_radix_sort(uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n, uint32_t major_words,
+                    uint32_t minor_words) {
+    std::vector<uint32_t> a(major, major + n), b(minor, minor + n), c;
+    if (payload) c.assign(payload, payload + n);
+    radix_sort_pairs(a, b, payload ? &c : nullptr, major_words, minor_words);
+    std::memcpy(major, a.data(), n * 4);
+    std::memcpy(minor, b.data(), n * 4);
+    if (payload) std::memcpy(payload, c.data(), n * 4);
+}
+
+// One pair through the narrowphase restatement (bodies/colliders from the world).
+uint32_t orc_narrowphase_pair(const OracleWorld* w, uint32_t a, uint32_t b, dyn_contact_record* out) {
+    return narrowphase_pair(*w, a, b, out) ? 1u : 0u;
+}
+
+}  // extern "C"

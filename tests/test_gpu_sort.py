@@ -1,0 +1,65 @@
+"""The onesweep radix sort operator (dyn_radix_sort) against numpy's stable sort.
+
+Restates the behaviours crates/dynamis-sort/tests/gpu.rs pins: a stable sort carrying a payload,
+two-word keys, and lengths around the tile boundaries.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from dynamis_b200 import World
+from dynamis_b200._native import check, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_sort(world, major, minor, payload, major_digits, minor_digits):
+    dev = torch.device("cuda:0")
+    tm = torch.from_numpy(major.view(np.int32)).to(dev)
+    tn = torch.from_numpy(minor.view(np.int32)).to(dev) if minor is not None else None
+    tp = torch.from_numpy(payload.view(np.int32)).to(dev) if payload is not None else None
+    torch.cuda.synchronize()
+    check(lib.dyn_radix_sort(world._h, tm.data_ptr(), tn.data_ptr() if tn is not None else None,
+                             tp.data_ptr() if tp is not None else None, len(major), major_digits, minor_digits), world._h)
+    world.wait()
+    out = [tm.cpu().numpy().view(np.uint32)]
+    out.append(tn.cpu().numpy().view(np.uint32) if tn is not None else None)
+    out.append(tp.cpu().numpy().view(np.uint32) if tp is not None else None)
+    return out
+
+
+@pytest.fixture(scope="module")
+def world():
+    w = World(capacity={"bodies": 1, "colliders": 1, "pairs": 1 << 20})
+    from dynamis_b200 import scenes
+
+    scenes.sphere_row(2).build(w)
+    w.step(1 / 60)
+    w.wait()
+    yield w
+    w.close()
+
+
+@pytest.mark.parametrize("n", [1, 7, 255, 256, 257, 1000, 2047, 2048, 2049, 5000, 100000])
+def test_stable_with_payload(world, n):
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << 12, size=n, dtype=np.uint32)
+    payload = np.arange(n, dtype=np.uint32)
+    major, _, carried = gpu_sort(world, keys.copy(), None, payload.copy(), 4, 0)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(major, keys[order])
+    assert np.array_equal(carried, payload[order])
+
+
+def test_two_word_keys(world):
+    n = 300000
+    rng = np.random.default_rng(3)
+    major = rng.integers(0, 1 << 18, size=n, dtype=np.uint32)
+    minor = rng.integers(0, 1 << 18, size=n, dtype=np.uint32)
+    payload = np.arange(n, dtype=np.uint32)
+    smaj, smin, spay = gpu_sort(world, major.copy(), minor.copy(), payload.copy(), 3, 3)
+    order = np.lexsort((minor, major))
+    assert np.array_equal(smaj, major[order])
+    assert np.array_equal(smin, minor[order])
+    assert np.array_equal(spay, payload[order])
