@@ -33,6 +33,12 @@ sys.path.insert(0, str(ROOT))
 METRIC = "rigid body-steps/s at 256K bodies; batched-worlds & adjoint step/s vs plain"
 UNIT = "body-steps/s"
 DT = 1.0 / 60.0
+_T0 = time.perf_counter()
+
+
+def log(message: str) -> None:
+    """Progress on stderr (the JSON result is the only stdout line)."""
+    print(f"[bench {time.perf_counter() - _T0:8.1f}s] {message}", file=sys.stderr, flush=True)
 
 
 def peaks() -> dict:
@@ -136,11 +142,16 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     torch.cuda.set_device(local_rank)
     world, scene, build_s = build_world(args.workload, local_rank)
     bodies = world.sizes()["bodies"]
+    log(f"scene {args.workload}: {bodies} bodies built in {build_s:.1f}s")
     stream = torch.cuda.Stream(device=local_rank)
     world.set_stream(stream.cuda_stream)
-    for _ in range(args.setup):
+    for i in range(args.setup):
         world.step(DT)
+        if i % 20 == 19:
+            world.wait()
+            log(f"setup step {i + 1}/{args.setup}")
     world.wait()
+    log("setup done")
     for _ in range(args.warmup):
         world.step(DT)
     world.wait()
@@ -159,6 +170,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         end.synchronize()
     world.wait()
     ms = start.elapsed_time(end)
+    log(f"timed {args.steps} steps: {ms / args.steps:.3f} ms/step")
+    log("counts " + str({k: int(world.measured()[R.COUNTER[k]]) for k in ("ENTRIES", "PAIRS", "CONTACTS", "LIVE")}))
     if dist:
         t = torch.tensor([ms], device=f"cuda:{local_rank}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -175,6 +188,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     world.wait()
     stages = world.stage_timings()
     world.set_timing(False)
+    log("stages " + ", ".join(f"{k}={v:.3f}" for k, v in stages.items()))
     params = {"substeps": int(world.config["substeps"][0]), "solve_iterations": int(world.config["solve_iterations"][0]),
               "position_iterations": int(world.config["position_iterations"][0]),
               "pair_words": int(np.ceil(np.ceil(np.log2(max(counts["K"] - 1, 1) + 1)) / 8)) or 1}
@@ -198,8 +212,9 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         world.upload_states(states_in)
         world.step(DT)
         world._check(lib.dyn_download_states(world._h, ptr(states_out), bodies))
-        states_in[:] = states_out
+        states_in, states_out = states_out, states_in  # the result feeds the next step
     e2e_s = time.perf_counter() - t0
+    log(f"e2e {e2e_steps} steps: {e2e_s / e2e_steps * 1e3:.3f} ms/step")
     result = {
         "metric": METRIC, "value": bodies * args.steps * world_size / (ms * 1e-3), "unit": UNIT,
         "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -230,6 +245,7 @@ def cpu_baseline(world, budget_s: float = 20.0) -> dict:
     scene = world.export_scene()
     scene["states"] = world.read_states()
     oracle = OracleWorld(scene, world.step_params(DT))
+    log("cpu baseline: oracle world built")
     steps = 0
     t0 = time.perf_counter()
     while True:

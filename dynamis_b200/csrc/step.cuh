@@ -180,15 +180,24 @@ __global__ void k_entry_count(DeviceWorld w) {
             const BodyHot& h = w.hot[owner];
             bool mv = moves(h.pos.w, h.aux.y);
             bool awake = w.activity[owner] != 0u || w.wake_flags[owner] != 0u;
-            or_counter(&w.counters[mv ? DYN_COUNTER_GRID_LEVELS : DYN_COUNTER_IMMOVABLE_LEVELS], 1u << level);
+            // aggregated updates need one target per coalesced group: branch first
+            if (mv) {
+                or_counter(&w.counters[DYN_COUNTER_GRID_LEVELS], 1u << level);
+            } else {
+                or_counter(&w.counters[DYN_COUNTER_IMMOVABLE_LEVELS], 1u << level);
+            }
             float cs = level_size(level, base);
             I3 lo = floor_div(mn, cs), hi = floor_div(mx, cs);
             uint32_t count = (uint32_t)(hi.x - lo.x + 1) * (uint32_t)(hi.y - lo.y + 1) * (uint32_t)(hi.z - lo.z + 1);
             emitted = min(count, DYN_MAX_CELLS_PER_COLLIDER);
             if (count > emitted) add_counter(&w.counters[DYN_COUNTER_ENTRY_FAULTS], count - emitted);
             if (level > 0u && awake) add_counter(&w.counters[DYN_COUNTER_COARSE_ACTIVE], 1u);
-            add_counter(&w.counters[mv ? DYN_COUNTER_ENTRIES : DYN_COUNTER_IMMOVABLE_ENTRIES], emitted);
-            if (!mv) add_counter(&w.counters[DYN_COUNTER_IMMOVABLE_EMITTED], emitted);
+            if (mv) {
+                add_counter(&w.counters[DYN_COUNTER_ENTRIES], emitted);
+            } else {
+                add_counter(&w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES], emitted);
+                add_counter(&w.counters[DYN_COUNTER_IMMOVABLE_EMITTED], emitted);
+            }
         }
         w.entry_count[i] = emitted;
     }
@@ -752,8 +761,11 @@ __global__ void k_warm(DeviceWorld w) {
             f3 j = normal * acc.x + t1 * acc.y + t2 * acc.z;
             pair_impulse(&f, &s, af, as, j);
         }
-        accumulate(w.vdelta, r.x, f.velocity - fl.velocity, f.angular_velocity - fl.angular_velocity, DYN_SOLVER_VELOCITY_SCALE);
-        accumulate(w.vdelta, r.y, s.velocity - sl.velocity, s.angular_velocity - sl.angular_velocity, DYN_SOLVER_VELOCITY_SCALE);
+        // an inert (frozen) body's delta is exactly zero: its atomics would add nothing
+        if (!dbody_inert(fl))
+            accumulate(w.vdelta, r.x, f.velocity - fl.velocity, f.angular_velocity - fl.angular_velocity, DYN_SOLVER_VELOCITY_SCALE);
+        if (!dbody_inert(sl))
+            accumulate(w.vdelta, r.y, s.velocity - sl.velocity, s.angular_velocity - sl.angular_velocity, DYN_SOLVER_VELOCITY_SCALE);
     }
 }
 
@@ -870,8 +882,8 @@ __global__ void __launch_bounds__(128) k_solve(DeviceWorld w, dyn_step_params p)
         for (uint32_t pi = 0; pi < pc; ++pi) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
         f3 da = first.velocity - pf.velocity, sa = first.angular_velocity - pf.angular_velocity;
         f3 db = second.velocity - ps.velocity, sb = second.angular_velocity - ps.angular_velocity;
-        accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
-        accumulate(w.vdelta, r.y, db, sb, DYN_SOLVER_VELOCITY_SCALE);
+        if (!dbody_inert(pf)) accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
+        if (!dbody_inert(ps)) accumulate(w.vdelta, r.y, db, sb, DYN_SOLVER_VELOCITY_SCALE);
         if (residual) {
             max_counter(&w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL],
                         (uint32_t)solver_word(wmax(length(da), length(db)), DYN_SOLVER_VELOCITY_SCALE));
@@ -997,10 +1009,22 @@ __global__ void k_position(DeviceWorld w, dyn_step_params p) {
         f3 la = -correction * ima;
         f3 lb = correction * imb;
         if (!(dot(la, la) > 0.0f || dot(lb, lb) > 0.0f)) continue;
-        atomicAdd(&w.contributions[r.x], 1u);
-        atomicAdd(&w.contributions[r.y], 1u);
-        accumulate(w.pdelta, r.x, la, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
-        accumulate(w.pdelta, r.y, lb, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        // Both rows are marked as contributing (position_apply renormalises a contributed row's
+        // orientation). A moving row needs the exact count, which divides its summed delta; a
+        // frozen row's sum is zero, so only "contributed" matters there: every writer stores the
+        // same 1, without an atomic on the shared row of a static body.
+        if (ima > 0.0f) {
+            atomicAdd(&w.contributions[r.x], 1u);
+            accumulate(w.pdelta, r.x, la, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        } else if (w.contributions[r.x] == 0u) {
+            w.contributions[r.x] = 1u;
+        }
+        if (imb > 0.0f) {
+            atomicAdd(&w.contributions[r.y], 1u);
+            accumulate(w.pdelta, r.y, lb, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        } else if (w.contributions[r.y] == 0u) {
+            w.contributions[r.y] = 1u;
+        }
     }
 }
 
@@ -1063,6 +1087,45 @@ __global__ void k_sleep(DeviceWorld w, dyn_step_params p) {
             }
             w.sleep_timer[i] = t;
         }
+    }
+}
+
+// ---- ABI state records <-> device layout (one contiguous copy each way) ----
+__global__ void k_unpack_states(DeviceWorld w, const dyn_body_state_record* __restrict__ in, uint32_t n) {
+    GRID_STRIDE(i, n) {
+        const dyn_body_state_record& r = in[i];
+        BodyHot& h = w.hot[i];
+        h.pos = make_float4(r.position[0], r.position[1], r.position[2], h.pos.w);
+        h.rot = make_float4(r.orientation[0], r.orientation[1], r.orientation[2], r.orientation[3]);
+        h.vel = make_float4(r.velocity[0], r.velocity[1], r.velocity[2], 0.0f);
+        h.ang = make_float4(r.angular_velocity[0], r.angular_velocity[1], r.angular_velocity[2], 0.0f);
+        h.aux.x = r.sleeping;
+        w.prev_pos[i] = make_float4(r.prev_position[0], r.prev_position[1], r.prev_position[2], 0.0f);
+        w.prev_rot[i] = make_float4(r.prev_orientation[0], r.prev_orientation[1], r.prev_orientation[2], r.prev_orientation[3]);
+        w.force[i] = make_float4(r.force[0], r.force[1], r.force[2], 0.0f);
+        w.torque[i] = make_float4(r.torque[0], r.torque[1], r.torque[2], 0.0f);
+        w.sleep_timer[i] = r.sleep_timer;
+    }
+}
+__global__ void k_pack_states(DeviceWorld w, dyn_body_state_record* __restrict__ out, uint32_t n) {
+    GRID_STRIDE(i, n) {
+        const BodyHot& h = w.hot[i];
+        float4 pp = w.prev_pos[i], pr = w.prev_rot[i], f = w.force[i], t = w.torque[i];
+        uint4 id = w.ident[i];
+        dyn_body_state_record r;
+        r.position[0] = h.pos.x; r.position[1] = h.pos.y; r.position[2] = h.pos.z; r._pad0 = 0.0f;
+        r.prev_position[0] = pp.x; r.prev_position[1] = pp.y; r.prev_position[2] = pp.z; r._pad1 = 0.0f;
+        r.prev_orientation[0] = pr.x; r.prev_orientation[1] = pr.y; r.prev_orientation[2] = pr.z; r.prev_orientation[3] = pr.w;
+        r.orientation[0] = h.rot.x; r.orientation[1] = h.rot.y; r.orientation[2] = h.rot.z; r.orientation[3] = h.rot.w;
+        r.velocity[0] = h.vel.x; r.velocity[1] = h.vel.y; r.velocity[2] = h.vel.z; r._pad2 = 0.0f;
+        r.angular_velocity[0] = h.ang.x; r.angular_velocity[1] = h.ang.y; r.angular_velocity[2] = h.ang.z; r._pad3 = 0.0f;
+        r.force[0] = f.x; r.force[1] = f.y; r.force[2] = f.z; r._pad4 = 0.0f;
+        r.torque[0] = t.x; r.torque[1] = t.y; r.torque[2] = t.z; r._pad5 = 0.0f;
+        r.body_id = id.x;
+        r.generation = id.y;
+        r.sleep_timer = w.sleep_timer[i];
+        r.sleeping = h.aux.x;
+        out[i] = r;
     }
 }
 

@@ -60,12 +60,14 @@ struct DeviceState {
     uint32_t* sort_alt1 = nullptr;
     uint32_t* sort_alt2 = nullptr;
     uint32_t sort_alt_cap = 0;
+    dyn_body_state_record* staging = nullptr;  // n_cap ABI state records
     // graphs
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     float graph_dt = -1.0f;
     uint32_t parity = 0;  // which contact set is current for the next step
     uint32_t last_parity = 0;
     bool stepped = false;
+    bool uploaded = false;  // the current scene's records are on the device
     uint32_t graph_kernels = 0;  // kernel nodes in one step's graph
     dyn_step_params params{};
     // timing
@@ -149,7 +151,7 @@ dyn_status ensure_device(dyn_world* w) {
         d = new DeviceState();
         w->dev = d;
         DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
-        d->stream = d->own_stream;
+        d->stream = w->user_stream ? static_cast<cudaStream_t>(w->user_stream) : d->own_stream;
         d->n_cap = std::max(n, w->capacity.bodies);
         d->k_cap = std::max(k, w->capacity.colliders);
         d->e_cap = 8u * std::max(d->k_cap, 1u);
@@ -214,6 +216,7 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.resolution, N);
         A(dw.counters, 64);
         A(dw.ctl, CTL_COUNT);
+        A(d->staging, N);
         A(d->hist, 8 * 256);
         A(d->tile_counters, 16);
         uint32_t max_tiles = std::max(div_up(std::max(E, P), kSortTile), 1u);
@@ -321,63 +324,20 @@ dyn_status upload_scene(dyn_world* w) {
     DYN_CUDA(cudaStreamSynchronize(s));
     d->parity = 0;
     d->stepped = false;
+    d->uploaded = true;
     release_graphs(d);
     return DYN_OK;
 }
 
 dyn_status download_states(dyn_world* w, std::vector<dyn_body_state_record>* out) {
     DeviceState* d = w->dev;
-    DeviceWorld& dw = d->dw;
-    uint32_t n = dw.n;
-    std::vector<BodyHot> hot(n);
-    std::vector<float4> prev_pos(n), prev_rot(n), force(n), torque(n);
-    std::vector<uint4> ident(n);
-    std::vector<float> timer(n);
-    cudaStream_t s = d->stream;
-    DYN_CUDA(cudaMemcpyAsync(hot.data(), dw.hot, n * sizeof(BodyHot), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaMemcpyAsync(prev_pos.data(), dw.prev_pos, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaMemcpyAsync(prev_rot.data(), dw.prev_rot, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaMemcpyAsync(force.data(), dw.force, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaMemcpyAsync(torque.data(), dw.torque, n * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaMemcpyAsync(ident.data(), dw.ident, n * sizeof(uint4), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaMemcpyAsync(timer.data(), dw.sleep_timer, n * sizeof(float), cudaMemcpyDeviceToHost, s));
-    DYN_CUDA(cudaStreamSynchronize(s));
+    uint32_t n = d->dw.n;
     out->resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        dyn_body_state_record& r = (*out)[i];
-        std::memset(&r, 0, sizeof(r));
-        const BodyHot& h = hot[i];
-        r.position[0] = h.pos.x;
-        r.position[1] = h.pos.y;
-        r.position[2] = h.pos.z;
-        r.prev_position[0] = prev_pos[i].x;
-        r.prev_position[1] = prev_pos[i].y;
-        r.prev_position[2] = prev_pos[i].z;
-        r.prev_orientation[0] = prev_rot[i].x;
-        r.prev_orientation[1] = prev_rot[i].y;
-        r.prev_orientation[2] = prev_rot[i].z;
-        r.prev_orientation[3] = prev_rot[i].w;
-        r.orientation[0] = h.rot.x;
-        r.orientation[1] = h.rot.y;
-        r.orientation[2] = h.rot.z;
-        r.orientation[3] = h.rot.w;
-        r.velocity[0] = h.vel.x;
-        r.velocity[1] = h.vel.y;
-        r.velocity[2] = h.vel.z;
-        r.angular_velocity[0] = h.ang.x;
-        r.angular_velocity[1] = h.ang.y;
-        r.angular_velocity[2] = h.ang.z;
-        r.force[0] = force[i].x;
-        r.force[1] = force[i].y;
-        r.force[2] = force[i].z;
-        r.torque[0] = torque[i].x;
-        r.torque[1] = torque[i].y;
-        r.torque[2] = torque[i].z;
-        r.body_id = ident[i].x;
-        r.generation = ident[i].y;
-        r.sleep_timer = timer[i];
-        r.sleeping = h.aux.x;
-    }
+    k_pack_states<<<blocks_for(std::max(n, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, n);
+    DYN_CUDA(cudaGetLastError());
+    DYN_CUDA(cudaMemcpyAsync(out->data(), d->staging, (size_t)n * sizeof(dyn_body_state_record), cudaMemcpyDeviceToHost,
+                             d->stream));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
     return DYN_OK;
 }
 
@@ -534,7 +494,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
 
 dyn_status prepare_step(dyn_world* w, float dt) {
     if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(w, DYN_ERR_INVALID, "a step timestep must be positive");
-    bool fresh = !w->dev || (w->rows_dirty && !w->raw_rows);
+    bool fresh = !w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows);
     if (fresh && w->dev && w->dev->stepped) {
         // bodies spawned after stepping: keep the simulated states of the existing bodies
         std::vector<dyn_body_state_record> now;
@@ -615,6 +575,7 @@ DYN_API dyn_status dyn_world_set_stream(dyn_world* w, void* stream) {
         dyn_status st = ensure_device(w);
         if (st) return st;
     }
+    w->user_stream = stream;
     w->dev->stream = stream ? static_cast<cudaStream_t>(stream) : w->dev->own_stream;
     return DYN_OK;
 }
@@ -657,34 +618,16 @@ DYN_API dyn_status dyn_upload_states(dyn_world* w, const dyn_body_state_record* 
     if (!w || !states) return fail(w, DYN_ERR_INVALID, "dyn_upload_states: null argument");
     rebuild_rows(w);
     if (n != w->states.size()) return fail(w, DYN_ERR_INVALID, "dyn_upload_states: row count differs from the scene");
-    if (!w->dev) {
+    if (!w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows)) {
         dyn_status st = upload_scene(w);
         if (st) return st;
     }
     DeviceState* d = w->dev;
-    DeviceWorld& dw = d->dw;
-    cudaStream_t s = d->stream;
-    // Pose, velocities and sleep state land in the hot rows through a strided copy of each field.
-    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].pos, sizeof(BodyHot), states[0].position, sizeof(dyn_body_state_record), 12, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].rot, sizeof(BodyHot), states[0].orientation, sizeof(dyn_body_state_record), 16, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].vel, sizeof(BodyHot), states[0].velocity, sizeof(dyn_body_state_record), 12, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].ang, sizeof(BodyHot), states[0].angular_velocity, sizeof(dyn_body_state_record), 12,
-                               n, cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(&dw.hot[0].aux.x, sizeof(BodyHot), &states[0].sleeping, sizeof(dyn_body_state_record), 4, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(dw.prev_pos, sizeof(float4), states[0].prev_position, sizeof(dyn_body_state_record), 12, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(dw.prev_rot, sizeof(float4), states[0].prev_orientation, sizeof(dyn_body_state_record), 16, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(dw.force, sizeof(float4), states[0].force, sizeof(dyn_body_state_record), 12, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(dw.torque, sizeof(float4), states[0].torque, sizeof(dyn_body_state_record), 12, n,
-                               cudaMemcpyHostToDevice, s));
-    DYN_CUDA(cudaMemcpy2DAsync(dw.sleep_timer, sizeof(float), &states[0].sleep_timer, sizeof(dyn_body_state_record), 4, n,
-                               cudaMemcpyHostToDevice, s));
+    // one contiguous copy of the ABI records, then a kernel scatters them into the device layout
+    DYN_CUDA(cudaMemcpyAsync(d->staging, states, (size_t)n * sizeof(dyn_body_state_record), cudaMemcpyHostToDevice,
+                             d->stream));
+    k_unpack_states<<<blocks_for(std::max(n, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, n);
+    DYN_CUDA(cudaGetLastError());
     return DYN_OK;
 }
 
@@ -753,16 +696,19 @@ DYN_API dyn_status dyn_device_status(dyn_world* w, uint32_t* status) {
 DYN_API dyn_status dyn_download_states(dyn_world* w, dyn_body_state_record* out, uint32_t n) {
     if (!w || !out) return DYN_ERR_INVALID;
     rebuild_rows(w);
-    if (!w->dev) {
+    if (!w->dev || !w->dev->uploaded) {
         if (n < w->states.size()) return DYN_ERR_INVALID;
         std::memcpy(out, w->states.data(), w->states.size() * sizeof(*out));
         return DYN_OK;
     }
-    std::vector<dyn_body_state_record> states;
-    dyn_status st = download_states(w, &states);
-    if (st) return st;
-    if (n < states.size()) return fail(w, DYN_ERR_INVALID, "dyn_download_states: buffer too small");
-    std::memcpy(out, states.data(), states.size() * sizeof(*out));
+    DeviceState* d = w->dev;
+    uint32_t rows = d->dw.n;
+    if (n < rows) return fail(w, DYN_ERR_INVALID, "dyn_download_states: buffer too small");
+    k_pack_states<<<blocks_for(std::max(rows, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, rows);
+    DYN_CUDA(cudaGetLastError());
+    DYN_CUDA(cudaMemcpyAsync(out, d->staging, (size_t)rows * sizeof(dyn_body_state_record), cudaMemcpyDeviceToHost,
+                             d->stream));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
     return DYN_OK;
 }
 
@@ -771,7 +717,7 @@ DYN_API dyn_status dyn_read_state(dyn_world* w, uint32_t body_id, dyn_body_state
     rebuild_rows(w);
     if (body_id >= w->row_of_id.size() || w->row_of_id[body_id] == DYN_NO_BODY) return fail(w, DYN_ERR_INVALID, "unknown body id");
     uint32_t row = w->row_of_id[body_id];
-    if (!w->dev) {
+    if (!w->dev || !w->dev->uploaded) {
         *out = w->states[row];
         return DYN_OK;
     }

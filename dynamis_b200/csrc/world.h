@@ -43,6 +43,7 @@ struct dyn_world {
     std::vector<uint32_t> row_of_id;
     uint32_t dynamic_count = 0;
     bool timing = false;
+    void* user_stream = nullptr;  // caller's cudaStream_t (dyn_world_set_stream)
     dyn::DeviceState* dev = nullptr;
 };
 

@@ -205,5 +205,6 @@ def random_mix(count: int, seed: int = 7, extent: float = 4.0, with_ground: bool
 
 WORKLOADS = {
     "falling_boxes_1000": lambda: falling_boxes(seed=0),
+    "mixed_pile_32768": lambda: mixed_pile(side=32, seed=1),
     "mixed_pile_262144": lambda: mixed_pile(side=64, seed=1),
 }

@@ -1185,6 +1185,10 @@ OracleWorld* orc_world_create(const dyn_step_params* params, const dyn_body_stat
                               const uint32_t* owners, uint32_t k, const dyn_shape_source_record* sources,
                               uint32_t source_count, const float* vertices, uint32_t vertex_count,
                               uint32_t pair_capacity, uint32_t contact_capacity) {
+    for (uint32_t i = 0; i < k; ++i) {
+        if (owners[i] != DYN_NO_BODY && owners[i] >= n) return nullptr;  // records that do not fit together
+        if (colliders[i].kind == DYN_SHAPE_HULL && colliders[i].source >= source_count) return nullptr;
+    }
     OracleWorld* w = new OracleWorld();
     w->params = *params;
     w->params.body_count = n;

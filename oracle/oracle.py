@@ -63,6 +63,8 @@ class OracleWorld:
                                      self.n, _p(s["colliders"]), _p(s["owners"]), len(s["colliders"]),
                                      _p(s["sources"]), len(s["sources"]), _p(s["vertices"]), len(s["vertices"]),
                                      pair_capacity, contact_capacity)
+        if not self._h:
+            raise ValueError("oracle refused the scene: collider owners or hull sources out of range")
 
     def close(self):
         if self._h:

@@ -92,3 +92,34 @@ def test_sphere_chain_pairs():
 
 def test_box_tower_matches_oracle():
     run(scenes.box_tower(8), steps=5)
+
+
+def test_caller_stream_gives_the_same_step():
+    torch = pytest.importorskip("torch")
+    scene = scenes.random_mix(40, seed=8)
+    a = World()
+    scene.build(a)
+    b = World()
+    scene.build(b)
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)  # before the first step: the scene must still be uploaded
+    for _ in range(3):
+        a.step(DT)
+        b.step(DT)
+    a.wait()
+    b.wait()
+    assert a.measured()[R.COUNTER["PAIRS"]] > 0
+    assert np.array_equal(a.measured(), b.measured())
+    assert a.read_states().tobytes() == b.read_states().tobytes()
+
+
+def test_state_upload_download_round_trip():
+    world = World()
+    scenes.random_mix(20, seed=2).build(world)
+    world.step(DT)
+    states = world.read_states()
+    states["velocity"] += np.float32(0.25)
+    states["sleep_timer"] = np.float32(0.125)
+    world.upload_states(states)
+    back = world.read_states()
+    assert back.tobytes() == states.tobytes()
