@@ -50,6 +50,7 @@ enum Ctl : uint32_t {
     CTL_ROUNDS = 7,
     CTL_STATUS = 8,
     CTL_VALID = 9,
+    CTL_LIST0 = 10,  // narrowphase class lists (3 words)
     CTL_COUNT = 16
 };
 
@@ -106,6 +107,7 @@ struct DeviceWorld {
     uint32_t* pair_slot;
     uint32_t* pair_flag;
     uint32_t* pair_rank;
+    uint32_t* np_list;  // [3][p_cap] pair indices per narrowphase class
     ContactSet cur;
     ContactSet arc;
     uint32_t* matched;

@@ -754,10 +754,10 @@ struct EpaOut {
 // convex.wgsl:286-437. The polytope lives in the calling thread's local memory.
 __device__ EpaOut epa_tetrahedron(const DeviceWorld& w, const WShape& first, const WShape& second, const SPt* simplex) {
     f3 poly[64];
-    uint32_t fa[128], fb[128], fcv[128];
+    uint8_t fa[128], fb[128], fcv[128];  // polytope indices are below 64
     f3 fn[128];
-    uint32_t vis[128];
-    uint32_t na[64], nb[64], nc[64];
+    uint8_t vis[128];
+    uint8_t na[64], nb[64], nc[64];
     f3 nn[64];
     EpaOut invalid{false, mk3(0.0f, 1.0f, 0.0f), 0.0f};
     for (uint32_t i = 0; i < 4; ++i) poly[i] = simplex[i].w;
@@ -875,8 +875,11 @@ __device__ __forceinline__ float support_projection_depth(const DeviceWorld& w, 
     return dot(support(w, f, n) - support(w, s, -n), n);
 }
 // convex.wgsl:532-582
+// With stop_at_separation the probe returns as soon as one direction shows no overlap (depth <= 0):
+// the caller then only needs to know that the minimum is not positive, and the minimum over all
+// directions is unchanged whenever it is positive.
 __device__ EpaOut penetration_probe(const DeviceWorld& w, const WShape& first, const WShape& second, const SPt* simplex,
-                                    uint32_t count) {
+                                    uint32_t count, bool stop_at_separation = false) {
     EpaOut best{false, mk3(0.0f, 1.0f, 0.0f), 3.402823466e38f};
     f3 probed[16];
     uint32_t pc = 0;
@@ -897,6 +900,7 @@ __device__ EpaOut penetration_probe(const DeviceWorld& w, const WShape& first, c
             best.depth = depth;
             best.normal = normalize(probed[i]);
         }
+        if (stop_at_separation && depth <= 0.0f) break;
     }
     best.valid = best.depth < 3.402823466e38f;
     return best;
@@ -969,7 +973,7 @@ __device__ Hit convex_hit(const DeviceWorld& w, const WShape& first, const WShap
         cl = simplex_closest(s, count);
     }
     if (!rpen) {
-        EpaOut probe = penetration_probe(w, first, second, s, count);
+        EpaOut probe = penetration_probe(w, first, second, s, count, true);
         if (probe.depth > 0.0f) {
             f3 normal = probe.normal;
             if (dot(normal, second.center - first.center) < 0.0f) normal = -normal;
@@ -1032,18 +1036,25 @@ __device__ uint32_t ring_of(const DeviceWorld& w, const WShape& s, f3 direction,
     center = center / (float)count;
     f3 u = fabsf(n.x) > 0.9f ? normalize(cross(n, mk3(0.0f, 1.0f, 0.0f))) : normalize(cross(n, mk3(1.0f, 0.0f, 0.0f)));
     f3 v = cross(n, u);
+    // convex.wgsl:699-714 compares atan2 angles of the points currently at i and j; a point's
+    // angle does not depend on where it sits, so each is computed once and travels with it.
+    float angle[16];
+    for (uint32_t i = 0; i < count; ++i) {
+        f3 pa = pts[i] - center;
+        angle[i] = datan2(dot(pa, v), dot(pa, u));
+    }
     for (uint32_t i = 0; i < count; ++i) {
         for (uint32_t j = i + 1; j < count; ++j) {
-            f3 pa = pts[i] - center, pb = pts[j] - center;
-            float aa = datan2(dot(pa, v), dot(pa, u));
-            float ab = datan2(dot(pb, v), dot(pb, u));
-            if (ab < aa) {
+            if (angle[j] < angle[i]) {
                 f3 t = pts[i];
                 pts[i] = pts[j];
                 pts[j] = t;
                 uint32_t ti = ids[i];
                 ids[i] = ids[j];
                 ids[j] = ti;
+                float ta = angle[i];
+                angle[i] = angle[j];
+                angle[j] = ta;
             }
         }
     }

@@ -20,6 +20,7 @@ namespace dyn {
 
 namespace cg = cooperative_groups;
 
+// Aggregated append: every lane of the calling coalesced group must pass the same counter.
 __device__ __forceinline__ uint32_t append_slot(uint32_t* counter) {
     cg::coalesced_group g = cg::coalesced_threads();
     uint32_t base = 0;
@@ -384,18 +385,23 @@ __device__ __forceinline__ void write_contact(const ContactSet& s, uint32_t cap,
     }
 }
 
-__global__ void __launch_bounds__(128) k_narrowphase(DeviceWorld w, dyn_step_params p) {
+enum PairClass : uint32_t { PC_ANALYTIC = 0, PC_BOXES = 1, PC_CONVEX = 2, PC_COUNT = 3 };
+
+// narrowphase.wgsl:518-550 (filters) then the shape dispatch of :551-652, decided once per pair:
+// pairs that fail a filter are answered here; the rest go to one list per kernel class.
+__global__ void k_pair_class(DeviceWorld w) {
     const uint32_t pairs = min(w.counters[DYN_COUNTER_PAIRS], w.p_cap);
     GRID_STRIDE(index, pairs) {
         uint32_t fs = w.pmaj[index], ss = w.pmin[index];
-        uint32_t valid = 0u;
         uint32_t fr = w.c_owner[fs], sr = w.c_owner[ss];
+        int cls = -1;
         do {
             if (fr == DYN_NO_BODY || sr == DYN_NO_BODY || fr == sr) break;
-            DBody fb = load_dbody(w.hot, fr), sb = load_dbody(w.hot, sr);
-            if (!moves(fb.inverse_mass, fb.flags) && !moves(sb.inverse_mass, sb.flags)) break;
-            DColl fc = load_dcoll(w, fs), sc = load_dcoll(w, ss);
-            if (fc.kind == 0u || sc.kind == 0u) break;
+            const BodyHot& fh = w.hot[fr];
+            const BodyHot& sh = w.hot[sr];
+            if (!moves(fh.pos.w, fh.aux.y) && !moves(sh.pos.w, sh.aux.y)) break;
+            uint32_t fk = w.c_kind[fs].x, sk = w.c_kind[ss].x;
+            if (fk == 0u || sk == 0u) break;
             uint4 fi = w.ident[fr], si = w.ident[sr];
             uint2 ff = w.c_filter[fs], sf = w.c_filter[ss];
             uint32_t fg = ff.x != DYN_NO_COLLISION_FILTER ? ff.x : fi.z;
@@ -403,65 +409,104 @@ __global__ void __launch_bounds__(128) k_narrowphase(DeviceWorld w, dyn_step_par
             uint32_t sg = sf.x != DYN_NO_COLLISION_FILTER ? sf.x : si.z;
             uint32_t sm = sf.y != DYN_NO_COLLISION_FILTER ? sf.y : si.w;
             if (!((fg & sm) != 0u && (sg & fm) != 0u)) break;
-            bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
-            bool fw = shape_world_geometry(fc.kind), sw = shape_world_geometry(sc.kind);
+            bool fw = shape_world_geometry(fk), sw = shape_world_geometry(sk);
             if (fw && sw) break;
-            float margin = p.contact_margin;
-            if ((fb.flags & DYN_BODY_CCD) || (sb.flags & DYN_BODY_CCD)) {
-                margin = p.contact_margin + length(sb.velocity - fb.velocity) * p.dt;
-            }
-            Mani m;
-            m.count = 0;
-            m.normal = s3(0.0f);
-            if (fw) {
-                if (fc.kind != 9u) break;
-                m = plane_convex(w, world_shape(fb.position, fb.orientation, fc), world_shape(sb.position, sb.orientation, sc), margin);
-            } else if (sw) {
-                if (sc.kind != 9u) break;
-                m = plane_convex(w, world_shape(sb.position, sb.orientation, sc), world_shape(fb.position, fb.orientation, fc), margin);
-                m.normal = -m.normal;
-                for (uint32_t q = 0; q < m.count; ++q) m.p[q].feature = feature_mirror(m.p[q].feature);
-            } else if (!veq(fc.scale, s3(1.0f)) || !veq(sc.scale, s3(1.0f)) || !shape_analytic(fc.kind) || !shape_analytic(sc.kind)
-                       || (fc.kind == 2u && sc.kind == 3u) || (fc.kind == 3u && sc.kind == 2u)) {
-                WShape a = world_shape(fb.position, fb.orientation, fc);
-                WShape b = world_shape(sb.position, sb.orientation, sc);
-                Hit hit = convex_hit(w, a, b);
-                if (hit.distance <= margin) {
-                    mani_emit(&m, hit.normal);
-                    if (!convex_pair_manifold(w, a, b, hit.normal, &m)) {
-                        if (hit.distance <= margin) mani_push(&m, hit.point, -hit.distance, kFeatPoint);
-                    }
-                }
-            } else if (fc.kind == 1u && sc.kind == 1u) {
-                m = sphere_sphere(fb, fc, sb, sc, margin);
-            } else if (fc.kind == 1u && sc.kind == 2u) {
-                m = sphere_box(fb, fc, sb, sc, margin);
-            } else if (fc.kind == 1u && sc.kind == 3u) {
-                m = sphere_capsule(fb, fc, sb, sc, margin);
-            } else if (fc.kind == 2u && sc.kind == 1u) {
-                m = sphere_box(sb, sc, fb, fc, margin);
-                m.normal = -m.normal;
-            } else if (fc.kind == 2u && sc.kind == 2u) {
-                m = box_box_sat(fb, fc, sb, sc, margin);
-            } else if (fc.kind == 3u && sc.kind == 1u) {
-                m = sphere_capsule(sb, sc, fb, fc, margin);
-                m.normal = -m.normal;
-            } else {
-                m = capsule_capsule(fb, fc, sb, sc, margin);
-            }
-            if (m.count == 0u) break;
-            uint32_t slot = append_slot(&w.ctl[CTL_TMP]);
-            if (slot >= w.c_cap) {
-                add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
+            if (fw || sw) {
+                if ((fw ? fk : sk) != 9u) break;  // meshes and heightfields are outside this path
+                cls = PC_ANALYTIC;                // plane against a convex: one feature ring
                 break;
             }
-            write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs], w.c_mat[ss],
-                          w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine, p.restitution_combine);
+            bool unscaled = veq(xyz(w.c_scale[fs]), s3(1.0f)) && veq(xyz(w.c_scale[ss]), s3(1.0f));
+            if (!unscaled || !shape_analytic(fk) || !shape_analytic(sk) || (fk == 2u && sk == 3u) || (fk == 3u && sk == 2u)) {
+                cls = PC_CONVEX;
+            } else if (fk == 2u && sk == 2u) {
+                cls = PC_BOXES;
+            } else {
+                cls = PC_ANALYTIC;
+            }
+        } while (false);
+        if (cls < 0) {
+            w.pair_flag[index] = 0u;
+        } else if (cls == PC_ANALYTIC) {  // one branch per list: an aggregated append needs one target
+            w.np_list[append_slot(&w.ctl[CTL_LIST0 + PC_ANALYTIC])] = index;
+        } else if (cls == PC_BOXES) {
+            w.np_list[(size_t)PC_BOXES * w.p_cap + append_slot(&w.ctl[CTL_LIST0 + PC_BOXES])] = index;
+        } else {
+            w.np_list[(size_t)PC_CONVEX * w.p_cap + append_slot(&w.ctl[CTL_LIST0 + PC_CONVEX])] = index;
+        }
+    }
+}
+
+// One pair of a class list through its narrowphase kernel (the pair passed the filters).
+template <int kClass>
+__device__ __forceinline__ void narrow_pair(const DeviceWorld& w, const dyn_step_params& p, uint32_t index) {
+    uint32_t fs = w.pmaj[index], ss = w.pmin[index];
+    uint32_t fr = w.c_owner[fs], sr = w.c_owner[ss];
+    DBody fb = load_dbody(w.hot, fr), sb = load_dbody(w.hot, sr);
+    DColl fc = load_dcoll(w, fs), sc = load_dcoll(w, ss);
+    uint4 fi = w.ident[fr], si = w.ident[sr];
+    bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
+    float margin = p.contact_margin;
+    if ((fb.flags & DYN_BODY_CCD) || (sb.flags & DYN_BODY_CCD)) {
+        margin = p.contact_margin + length(sb.velocity - fb.velocity) * p.dt;
+    }
+    Mani m;
+    m.count = 0;
+    m.normal = s3(0.0f);
+    if (kClass == PC_ANALYTIC) {
+        if (fc.kind == 9u) {
+            m = plane_convex(w, world_shape(fb.position, fb.orientation, fc), world_shape(sb.position, sb.orientation, sc), margin);
+        } else if (sc.kind == 9u) {
+            m = plane_convex(w, world_shape(sb.position, sb.orientation, sc), world_shape(fb.position, fb.orientation, fc), margin);
+            m.normal = -m.normal;
+            for (uint32_t q = 0; q < m.count; ++q) m.p[q].feature = feature_mirror(m.p[q].feature);
+        } else if (fc.kind == 1u && sc.kind == 1u) {
+            m = sphere_sphere(fb, fc, sb, sc, margin);
+        } else if (fc.kind == 1u && sc.kind == 2u) {
+            m = sphere_box(fb, fc, sb, sc, margin);
+        } else if (fc.kind == 1u && sc.kind == 3u) {
+            m = sphere_capsule(fb, fc, sb, sc, margin);
+        } else if (fc.kind == 2u && sc.kind == 1u) {
+            m = sphere_box(sb, sc, fb, fc, margin);
+            m.normal = -m.normal;
+        } else if (fc.kind == 3u && sc.kind == 1u) {
+            m = sphere_capsule(sb, sc, fb, fc, margin);
+            m.normal = -m.normal;
+        } else {
+            m = capsule_capsule(fb, fc, sb, sc, margin);
+        }
+    } else if (kClass == PC_BOXES) {
+        m = box_box_sat(fb, fc, sb, sc, margin);
+    } else {
+        WShape a = world_shape(fb.position, fb.orientation, fc);
+        WShape b = world_shape(sb.position, sb.orientation, sc);
+        Hit hit = convex_hit(w, a, b);
+        if (hit.distance <= margin) {
+            mani_emit(&m, hit.normal);
+            if (!convex_pair_manifold(w, a, b, hit.normal, &m)) mani_push(&m, hit.point, -hit.distance, kFeatPoint);
+        }
+    }
+    uint32_t valid = 0u;
+    if (m.count > 0u) {
+        uint32_t slot = append_slot(&w.ctl[CTL_TMP]);
+        if (slot < w.c_cap) {
+            write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
+                          w.c_mat[ss], w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine,
+                          p.restitution_combine);
             w.pair_slot[index] = slot;
             valid = 1u;
-        } while (false);
-        w.pair_flag[index] = valid;
+        } else {
+            add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
+        }
     }
+    w.pair_flag[index] = valid;
+}
+
+template <int kClass>
+__global__ void __launch_bounds__(128) k_narrow_class(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = min(w.ctl[CTL_LIST0 + kClass], w.p_cap);
+    const uint32_t* list = w.np_list + (size_t)kClass * w.p_cap;
+    GRID_STRIDE(i, count) narrow_pair<kClass>(w, p, list[i]);
 }
 
 __device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi, const ContactSet& to, uint32_t ti, uint32_t cap) {
