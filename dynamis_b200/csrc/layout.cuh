@@ -51,6 +51,8 @@ enum Ctl : uint32_t {
     CTL_STATUS = 8,
     CTL_VALID = 9,
     CTL_LIST0 = 10,  // narrowphase class lists (3 words)
+    CTL_EPA = 13,    // penetrating convex pairs queued for EPA
+    CTL_HITS = 14,   // convex pairs queued for the manifold
     CTL_COUNT = 16
 };
 
@@ -108,6 +110,10 @@ struct DeviceWorld {
     uint32_t* pair_flag;
     uint32_t* pair_rank;
     uint32_t* np_list;  // [3][p_cap] pair indices per narrowphase class
+    uint32_t* epa_list;      // pair indices of penetrating convex pairs
+    float4* epa_simplex;     // [4][slot]: the GJK simplex (w.xyz) EPA starts from
+    uint32_t* hit_list;      // pair indices of convex hits
+    float4* hit_data;        // [2][slot]: point.xyz + distance, normal.xyz
     ContactSet cur;
     ContactSet arc;
     uint32_t* matched;

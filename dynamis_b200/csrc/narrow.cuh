@@ -999,6 +999,366 @@ __device__ Hit convex_hit(const DeviceWorld& w, const WShape& first, const WShap
     return result;
 }
 
+// ---- the convex path in three phases (results identical to convex_hit) ----
+//
+// Phase 1, one thread per pair: GJK (convex.wgsl:464-521) and, for separated shapes, the
+// penetration probe that may still report overlap (convex.wgsl:588-600). Phase 2, one warp per
+// penetrating pair: EPA (convex.wgsl:286-437) with the polytope in shared memory and its face
+// loops spread over the lanes, then the acceptance test and probe fallback (convex.wgsl:602-617).
+// Phase 3, one thread per hit: the feature-ring manifold.
+
+struct GjkOut {
+    bool pen;
+    uint32_t count;
+    float dist;
+    f3 pa, pb, normal;
+    SPt s[4];
+};
+
+__device__ GjkOut gjk_phase(const DeviceWorld& w, const WShape& first, const WShape& second) {
+    GjkOut o;
+    o.count = 0;
+    o.dist = 0.0f;
+    o.pa = first.center;
+    o.pb = second.center;
+    o.normal = sign_normalize(second.center - first.center);
+    o.pen = false;
+    f3 dir = second.center - first.center;
+    if (length(dir) < 1e-8f) dir = mk3(1.0f, 0.0f, 0.0f);
+    o.s[0] = support_pair(w, first, second, dir);
+    o.count = 1;
+    SRes cl = simplex_closest(o.s, o.count);
+    float tiny = 1e-4f * wmin(shape_scale(first), shape_scale(second));
+    for (uint32_t iter = 0; iter < 24u; ++iter) {
+        if (cl.pen || length(cl.v) < tiny) {
+            while (o.count < 4u) {
+                f3 d = simplex_expand_dir(o.s, o.count);
+                o.s[o.count] = support_pair(w, first, second, d);
+                o.count += 1;
+            }
+            o.pen = true;
+            o.dist = 0.0f;
+            o.pa = cl.pa;
+            o.pb = cl.pb;
+            break;
+        }
+        SPt sp = support_pair(w, first, second, -cl.v);
+        if (dot(sp.w, -cl.v) <= dot(cl.v, -cl.v) + 1e-4f * wmax(1.0f, dot(cl.v, cl.v))) {
+            o.dist = length(cl.v);
+            o.pa = cl.pa;
+            o.pb = cl.pb;
+            if (o.dist > 1e-6f) o.normal = sign_normalize(cl.pb - cl.pa);
+            break;
+        }
+        SPt kept[4];
+        uint32_t kc = 0;
+        for (uint32_t i = 0; i < 4; ++i) {
+            if (cl.lam[i] > 1e-6f) kept[kc++] = o.s[i];
+        }
+        if (kc == 0u) {
+            kept[0] = o.s[0];
+            kc = 1;
+        }
+        for (uint32_t i = 0; i < kc; ++i) o.s[i] = kept[i];
+        o.count = kc;
+        float span = shape_scale(second);
+        float tol = (1e-5f * span) * (1e-5f * span);
+        bool holds = false;
+        for (uint32_t i = 0; i < o.count; ++i) {
+            f3 off = o.s[i].w - sp.w;
+            if (dot(off, off) <= tol) holds = true;
+        }
+        if (holds) {
+            o.dist = length(cl.v);
+            o.pa = cl.pa;
+            o.pb = cl.pb;
+            if (o.dist > 1e-6f) o.normal = sign_normalize(cl.pb - cl.pa);
+            break;
+        }
+        o.s[o.count] = sp;
+        o.count += 1;
+        cl = simplex_closest(o.s, o.count);
+    }
+    return o;
+}
+
+// convex.wgsl:588-600 for a separated GJK result.
+__device__ Hit separated_hit(const DeviceWorld& w, const WShape& first, const WShape& second, const GjkOut& g) {
+    EpaOut probe = penetration_probe(w, first, second, g.s, g.count, true);
+    if (probe.depth > 0.0f) {
+        f3 normal = probe.normal;
+        if (dot(normal, second.center - first.center) < 0.0f) normal = -normal;
+        return Hit{-probe.depth, (g.pa + g.pb) * 0.5f, normal};
+    }
+    if (g.dist > 0.0f) return Hit{g.dist, (g.pa + g.pb) * 0.5f, g.normal};
+    return Hit{3.402823466e38f, s3(0.0f), s3(0.0f)};
+}
+
+// ---- warp-cooperative pieces ----
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+
+// support_local over a hull with the warp's lanes striding the vertices; the reduction keeps the
+// sequential scan's choice: the largest dot product, the lowest index among equal ones.
+__device__ __forceinline__ f3 warp_support_local(const DeviceWorld& w, const WShape& s, f3 d) {
+    if (s.kind != 5u) return support_local(w, s, d);
+    const dyn_shape_source_record& src = w.sources[s.source];
+    const float4* verts = w.vertices + src.vertex_offset;
+    const uint32_t lane = threadIdx.x & 31u;
+    float best = -3.402823466e38f;
+    uint32_t bi = 0xFFFFFFFFu;
+    for (uint32_t i = lane; i < src.vertex_count; i += 32u) {
+        float sd = dot(xyz(__ldg(verts + i)), d);
+        if (sd > best) {
+            best = sd;
+            bi = i;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        float ob = __shfl_xor_sync(kFull, best, off);
+        uint32_t oi = __shfl_xor_sync(kFull, bi, off);
+        if (oi != 0xFFFFFFFFu && (bi == 0xFFFFFFFFu || ob > best || (ob == best && oi < bi))) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    return bi == 0xFFFFFFFFu ? s3(0.0f) : xyz(__ldg(verts + bi));
+}
+__device__ __forceinline__ f3 warp_support(const DeviceWorld& w, const WShape& s, f3 direction) {
+    f3 local_d = quat_rotate(quat_conj(s.rotation), direction);
+    f3 local = warp_support_local(w, s, local_d * s.scale);
+    return s.center + quat_rotate(s.rotation, local * s.scale);
+}
+
+struct EpaWarpShared {
+    float4 poly[64];
+    float4 fn[128];      // face normal.xyz, packed (a | b << 8 | c << 16) bits in w
+    float4 nn[64];
+    uint8_t vis[128];
+    uint8_t visflag[128];
+};
+
+__device__ __forceinline__ float4 pack_face(f3 n, uint32_t a, uint32_t b, uint32_t c) {
+    return make_float4(n.x, n.y, n.z, __uint_as_float(a | (b << 8) | (c << 16)));
+}
+__device__ __forceinline__ void unpack_face(float4 f, uint32_t* a, uint32_t* b, uint32_t* c) {
+    uint32_t bits = __float_as_uint(f.w);
+    *a = bits & 255u;
+    *b = (bits >> 8) & 255u;
+    *c = (bits >> 16) & 255u;
+}
+
+// (min distance, lowest index) over faces whose normal is longer than 0.5: the first minimum of
+// convex.wgsl:344-352, identical on every lane.
+__device__ __forceinline__ void warp_best_face(const EpaWarpShared& m, uint32_t fcount, float* best_dist, uint32_t* best_face) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float bd = 3.402823466e38f;
+    uint32_t bi = 0u;
+    bool any = false;
+    for (uint32_t j = lane; j < fcount; j += 32u) {
+        float4 f = m.fn[j];
+        uint32_t a, b, c;
+        unpack_face(f, &a, &b, &c);
+        f3 n = xyz(f);
+        float dist = dot(n, xyz(m.poly[a]));
+        if (dist < bd && length(n) > 0.5f) {
+            bd = dist;
+            bi = j;
+            any = true;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        float od = __shfl_xor_sync(kFull, bd, off);
+        uint32_t oi = __shfl_xor_sync(kFull, bi, off);
+        bool oa = __shfl_xor_sync(kFull, any, off);
+        if (oa && (!any || od < bd || (od == bd && oi < bi))) {
+            bd = od;
+            bi = oi;
+            any = true;
+        }
+    }
+    *best_dist = bd;
+    *best_face = any ? bi : 0u;
+}
+
+// convex.wgsl:286-437 on one warp. All lanes return the same result.
+__device__ EpaOut warp_epa(const DeviceWorld& w, const WShape& first, const WShape& second, const f3* simplex, EpaWarpShared& m) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    EpaOut invalid{false, mk3(0.0f, 1.0f, 0.0f), 0.0f};
+    if (lane < 4u) m.poly[lane] = mk4(simplex[lane], 0.0f);
+    __syncwarp();
+    const uint32_t tet[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 3, 2}};
+    bool bad = false;
+    if (lane < 4u) {
+        uint32_t a = tet[lane][0], b = tet[lane][1], c = tet[lane][2];
+        f3 pa = xyz(m.poly[a]), pb = xyz(m.poly[b]), pc = xyz(m.poly[c]);
+        f3 normal = cross(pb - pa, pc - pa);
+        float ln = length(normal);
+        if (ln < 1e-10f) {
+            bad = true;
+        } else {
+            f3 unit = normal / ln;
+            f3 centroid = (pa + pb + pc) * (1.0f / 3.0f);
+            m.fn[lane] = pack_face(dot(unit, centroid) > 0.0f ? -unit : unit, a, b, c);
+        }
+    }
+    if (__any_sync(kFull, bad)) return invalid;
+    __syncwarp();
+    uint32_t fcount = 4, vc = 4;
+    float bd = 0.0f;
+    uint32_t bf = 0;
+    for (uint32_t iter = 0; iter < 32u; ++iter) {
+        warp_best_face(m, fcount, &bd, &bf);
+        f3 n = xyz(m.fn[bf]);
+        f3 probe = warp_support(w, first, n) - warp_support(w, second, -n);
+        float gain = dot(probe, n) - bd;
+        if (gain < 1e-4f) break;
+        if (vc >= 64u) break;
+        __syncwarp();
+        if (lane == 0u) m.poly[vc] = mk4(probe, 0.0f);
+        vc += 1;
+        // visible faces in index order
+        uint32_t vcount = 0;
+        for (uint32_t base = 0; base < fcount; base += 32u) {
+            uint32_t j = base + lane;
+            bool v = false;
+            if (j < fcount) {
+                float4 f = m.fn[j];
+                uint32_t a, b, c;
+                unpack_face(f, &a, &b, &c);
+                v = dot(xyz(f), probe - xyz(m.poly[a])) > 1e-6f;
+                m.visflag[j] = v ? 1u : 0u;
+            }
+            uint32_t mask = __ballot_sync(kFull, v);
+            if (v) m.vis[vcount + __popc(mask & lt)] = (uint8_t)j;
+            vcount += __popc(mask);
+        }
+        __syncwarp();
+        // horizon edges become new faces, in (visible face, edge) order, at most 64
+        uint32_t ncount = 0;
+        const uint32_t apex = vc - 1u;
+        for (uint32_t base = 0; base < 3u * vcount; base += 32u) {
+            uint32_t t = base + lane;
+            bool keep = false;
+            float4 face = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (t < 3u * vcount) {
+                uint32_t i = t / 3u, e = t % 3u;
+                uint32_t a, b, c;
+                unpack_face(m.fn[m.vis[i]], &a, &b, &c);
+                uint32_t start = e == 0u ? a : (e == 1u ? b : c);
+                uint32_t end = e == 0u ? b : (e == 1u ? c : a);
+                bool shared = false;
+                for (uint32_t jj = 0; jj < vcount; ++jj) {
+                    if (jj == i) continue;
+                    uint32_t oa, ob, oc;
+                    unpack_face(m.fn[m.vis[jj]], &oa, &ob, &oc);
+                    if ((oa == end && ob == start) || (ob == end && oc == start) || (oc == end && oa == start)) shared = true;
+                }
+                if (!shared) {
+                    f3 pap = xyz(m.poly[apex]), ps = xyz(m.poly[start]), pe = xyz(m.poly[end]);
+                    f3 normal = cross(pe - pap, ps - pap);
+                    float ln = length(normal);
+                    if (ln > 1e-10f) {
+                        f3 unit = normal / ln;
+                        f3 centroid = (pap + ps + pe) * (1.0f / 3.0f);
+                        face = pack_face(dot(unit, centroid) > 0.0f ? -unit : unit, apex, start, end);
+                        keep = true;
+                    }
+                }
+            }
+            uint32_t mask = __ballot_sync(kFull, keep);
+            uint32_t rank = ncount + __popc(mask & lt);
+            if (keep && rank < 64u) m.nn[rank] = face;
+            ncount = min(ncount + (uint32_t)__popc(mask), 64u);
+        }
+        __syncwarp();
+        // drop the visible faces, keeping order
+        uint32_t write = 0;
+        for (uint32_t base = 0; base < fcount; base += 32u) {
+            uint32_t j = base + lane;
+            bool keepf = j < fcount && m.visflag[j] == 0u;
+            float4 f = j < fcount ? m.fn[j] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            uint32_t mask = __ballot_sync(kFull, keepf);
+            __syncwarp();
+            if (keepf) m.fn[write + __popc(mask & lt)] = f;
+            write += __popc(mask);
+            __syncwarp();
+        }
+        fcount = write;
+        if (fcount + ncount > 128u) break;
+        for (uint32_t t = lane; t < ncount; t += 32u) m.fn[fcount + t] = m.nn[t];
+        fcount += ncount;
+        __syncwarp();
+    }
+    __syncwarp();
+    float fd = 3.402823466e38f;
+    uint32_t ff = bf;
+    {
+        float d2;
+        uint32_t f2;
+        warp_best_face(m, fcount, &d2, &f2);
+        fd = d2;
+        if (d2 < 3.402823466e38f) ff = f2;
+    }
+    EpaOut r;
+    r.valid = fd < 3.402823466e38f;
+    r.normal = xyz(m.fn[ff < 128u ? ff : 0u]);
+    r.depth = fd;
+    return r;
+}
+
+__device__ __forceinline__ float warp_projection_depth(const DeviceWorld& w, const WShape& f, const WShape& s, f3 direction) {
+    f3 n = normalize(direction);
+    return dot(warp_support(w, f, n) - warp_support(w, s, -n), n);
+}
+
+// convex.wgsl:602-617 after a penetrating GJK (one warp, every lane returns the same hit).
+__device__ Hit warp_penetrating_hit(const DeviceWorld& w, const WShape& first, const WShape& second, const f3* simplex,
+                                    EpaWarpShared& m) {
+    EpaOut epa = warp_epa(w, first, second, simplex, m);
+    Hit result;
+    bool accept = epa.valid && epa.depth > 0.0f && epa.depth < 3.402823466e38f && length(epa.normal) > 0.5f;
+    if (accept) {
+        accept = epa.depth < warp_projection_depth(w, first, second, epa.normal) + 0.1f * wmin(shape_scale(first), shape_scale(second));
+    }
+    if (accept) {
+        f3 pa = warp_support(w, first, epa.normal);
+        f3 pb = warp_support(w, second, -epa.normal);
+        result = Hit{-epa.depth, (pa + pb) * 0.5f, epa.normal};
+    } else {
+        // convex_penetration_probe over the four-point simplex, centre direction and six axes
+        f3 probed[16];
+        uint32_t pc = 0;
+        for (uint32_t i = 0; i < 4; ++i)
+            for (uint32_t j = i + 1; j < 4; ++j)
+                for (uint32_t k = j + 1; k < 4; ++k) {
+                    f3 normal = cross(simplex[j] - simplex[i], simplex[k] - simplex[i]);
+                    if (length(normal) > 1e-8f && pc < 16u) probed[pc++] = normal;
+                }
+        f3 cdir = second.center - first.center;
+        if (length(cdir) > 1e-8f && pc < 16u) probed[pc++] = cdir;
+        const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        for (uint32_t i = 0; i < 6; ++i)
+            if (pc < 16u) probed[pc++] = mk3(ax[i][0], ax[i][1], ax[i][2]);
+        float best_depth = 3.402823466e38f;
+        f3 best_normal = mk3(0.0f, 1.0f, 0.0f);
+        for (uint32_t i = 0; i < pc; ++i) {
+            float depth = warp_projection_depth(w, first, second, probed[i]);
+            if (depth < best_depth) {
+                best_depth = depth;
+                best_normal = normalize(probed[i]);
+            }
+        }
+        f3 pa = warp_support(w, first, best_normal);
+        f3 pb = warp_support(w, second, -best_normal);
+        result = Hit{-best_depth, (pa + pb) * 0.5f, best_normal};
+    }
+    if (dot(result.normal, second.center - first.center) < 0.0f) result.normal = -result.normal;
+    return result;
+}
+
 // ---- features (convex.wgsl:639-900) ----
 __device__ uint32_t box_feature_ring(const WShape& s, f3 direction, f3* out, uint32_t* ids, uint32_t* face) {
     f3 axes[3] = {quat_rotate(s.rotation, mk3(1.0f, 0.0f, 0.0f)), quat_rotate(s.rotation, mk3(0.0f, 1.0f, 0.0f)),

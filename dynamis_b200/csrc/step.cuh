@@ -502,6 +502,114 @@ __device__ __forceinline__ void narrow_pair(const DeviceWorld& w, const dyn_step
     w.pair_flag[index] = valid;
 }
 
+// ---- the convex class in three phases ----
+__device__ __forceinline__ float pair_margin(const dyn_step_params& p, const DBody& fb, const DBody& sb) {
+    if ((fb.flags & DYN_BODY_CCD) || (sb.flags & DYN_BODY_CCD)) return p.contact_margin + length(sb.velocity - fb.velocity) * p.dt;
+    return p.contact_margin;
+}
+__device__ __forceinline__ void convex_shapes(const DeviceWorld& w, uint32_t index, WShape* a, WShape* b, DBody* fb, DBody* sb) {
+    uint32_t fs = w.pmaj[index], ss = w.pmin[index];
+    *fb = load_dbody(w.hot, w.c_owner[fs]);
+    *sb = load_dbody(w.hot, w.c_owner[ss]);
+    DColl fc = load_dcoll(w, fs), sc = load_dcoll(w, ss);
+    *a = world_shape(fb->position, fb->orientation, fc);
+    *b = world_shape(sb->position, sb->orientation, sc);
+}
+__device__ __forceinline__ void push_hit(const DeviceWorld& w, uint32_t index, const Hit& hit) {
+    uint32_t slot = append_slot(&w.ctl[CTL_HITS]);
+    w.hit_list[slot] = index;
+    w.hit_data[2 * (size_t)slot] = mk4(hit.point, hit.distance);
+    w.hit_data[2 * (size_t)slot + 1] = mk4(hit.normal, 0.0f);
+}
+
+// Phase 1: GJK per pair; separated pairs are answered here (probe), penetrating ones queue for EPA.
+__global__ void __launch_bounds__(128) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = min(w.ctl[CTL_LIST0 + PC_CONVEX], w.p_cap);
+    const uint32_t* list = w.np_list + (size_t)PC_CONVEX * w.p_cap;
+    GRID_STRIDE(i, count) {
+        uint32_t index = list[i];
+        WShape a, b;
+        DBody fb, sb;
+        convex_shapes(w, index, &a, &b, &fb, &sb);
+        GjkOut g = gjk_phase(w, a, b);
+        if (g.pen) {
+            uint32_t slot = append_slot(&w.ctl[CTL_EPA]);
+            w.epa_list[slot] = index;
+            for (uint32_t k = 0; k < 4; ++k) w.epa_simplex[4 * (size_t)slot + k] = mk4(g.s[k].w, 0.0f);
+            continue;
+        }
+        Hit hit = separated_hit(w, a, b, g);
+        if (hit.distance <= pair_margin(p, fb, sb)) {
+            push_hit(w, index, hit);
+        } else {
+            w.pair_flag[index] = 0u;
+        }
+    }
+}
+
+// Phase 2: one warp per penetrating pair.
+constexpr int kEpaWarpsPerBlock = 4;
+__global__ void __launch_bounds__(32 * kEpaWarpsPerBlock) k_convex_epa(DeviceWorld w, dyn_step_params p) {
+    __shared__ EpaWarpShared shared[kEpaWarpsPerBlock];
+    const uint32_t count = min(w.ctl[CTL_EPA], w.p_cap);
+    const uint32_t warp = threadIdx.x >> 5;
+    EpaWarpShared& m = shared[warp];
+    for (uint32_t e = blockIdx.x * kEpaWarpsPerBlock + warp; e < count; e += gridDim.x * kEpaWarpsPerBlock) {
+        uint32_t index = w.epa_list[e];
+        WShape a, b;
+        DBody fb, sb;
+        convex_shapes(w, index, &a, &b, &fb, &sb);
+        f3 simplex[4];
+        for (uint32_t k = 0; k < 4; ++k) simplex[k] = xyz(w.epa_simplex[4 * (size_t)e + k]);
+        Hit hit = warp_penetrating_hit(w, a, b, simplex, m);
+        if ((threadIdx.x & 31u) == 0u) {
+            if (hit.distance <= pair_margin(p, fb, sb)) {
+                push_hit(w, index, hit);
+            } else {
+                w.pair_flag[index] = 0u;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Phase 3: the feature-ring manifold for every hit (convex_pair_manifold, else manifold_from_hit).
+__global__ void __launch_bounds__(128) k_convex_manifold(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = min(w.ctl[CTL_HITS], w.p_cap);
+    GRID_STRIDE(i, count) {
+        uint32_t index = w.hit_list[i];
+        float4 h0 = w.hit_data[2 * (size_t)i], h1 = w.hit_data[2 * (size_t)i + 1];
+        uint32_t fs = w.pmaj[index], ss = w.pmin[index];
+        uint32_t fr = w.c_owner[fs], sr = w.c_owner[ss];
+        DBody fb = load_dbody(w.hot, fr), sb = load_dbody(w.hot, sr);
+        DColl fc = load_dcoll(w, fs), sc = load_dcoll(w, ss);
+        WShape a = world_shape(fb.position, fb.orientation, fc);
+        WShape b = world_shape(sb.position, sb.orientation, sc);
+        float margin = pair_margin(p, fb, sb);
+        Mani m;
+        mani_emit(&m, xyz(h1));
+        if (!convex_pair_manifold(w, a, b, xyz(h1), &m)) {
+            if (h0.w <= margin) mani_push(&m, xyz(h0), -h0.w, kFeatPoint);
+        }
+        uint32_t valid = 0u;
+        if (m.count > 0u) {
+            uint32_t slot = append_slot(&w.ctl[CTL_TMP]);
+            if (slot < w.c_cap) {
+                uint4 fi = w.ident[fr], si = w.ident[sr];
+                bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
+                write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
+                              w.c_mat[ss], w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine,
+                              p.restitution_combine);
+                w.pair_slot[index] = slot;
+                valid = 1u;
+            } else {
+                add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
+            }
+        }
+        w.pair_flag[index] = valid;
+    }
+}
+
 template <int kClass>
 __global__ void __launch_bounds__(128) k_narrow_class(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = min(w.ctl[CTL_LIST0 + kClass], w.p_cap);

@@ -206,6 +206,10 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.pair_flag, P);
         A(dw.pair_rank, P);
         A(dw.np_list, 3 * (size_t)P);
+        A(dw.epa_list, P);
+        A(dw.epa_simplex, 4 * (size_t)P);
+        A(dw.hit_list, P);
+        A(dw.hit_data, 2 * (size_t)P);
         A(dw.matched, C);
         A(dw.parents, N);
         A(dw.istate, N);
@@ -454,7 +458,9 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
     k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
-    k_narrow_class<PC_CONVEX><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    k_convex_gjk<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
+    k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     mark(ST_COMPACT);
     record_scan(d, s, dw.pair_flag, dw.pair_rank, dw.counters + DYN_COUNTER_PAIRS, 0, P, dw.ctl + CTL_VALID);
     k_compact<<<blocks_for(P, 256), 256, 0, s>>>(dw);

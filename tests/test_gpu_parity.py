@@ -123,3 +123,9 @@ def test_state_upload_download_round_trip():
     world.upload_states(states)
     back = world.read_states()
     assert back.tobytes() == states.tobytes()
+
+
+def test_forming_pile_matches_oracle_every_step():
+    """45 steps of a 1,000-body mixed pile: bodies land and rest, so penetrating hull contacts
+    (EPA), warm-started impulses and sleeping all occur; every step is compared."""
+    run(scenes.mixed_pile(side=10, seed=4), steps=45)
