@@ -38,7 +38,7 @@ __device__ __forceinline__ void store_relaxed(uint32_t* p, uint32_t v) {
 
 // Counts digit occurrences for every pass of the sort in one read. hist: passes x 256 words.
 // Digit pass p reads word (p < minor_digits ? minor : major), byte (p or p - minor_digits).
-__global__ void k_sort_histogram(const uint32_t* __restrict__ major, const uint32_t* __restrict__ minor,
+static __global__ void k_sort_histogram(const uint32_t* __restrict__ major, const uint32_t* __restrict__ minor,
                                  const uint32_t* __restrict__ count_ptr, uint32_t n_fixed, uint32_t cap,
                                  int major_digits, int minor_digits, uint32_t* __restrict__ hist) {
     __shared__ uint32_t local[8][256];
@@ -63,7 +63,7 @@ __global__ void k_sort_histogram(const uint32_t* __restrict__ major, const uint3
 }
 
 // Exclusive scan of each pass's 256 digit counts, in place (one block of 256 threads).
-__global__ void k_sort_offsets(uint32_t* hist, int passes) {
+static __global__ void k_sort_offsets(uint32_t* hist, int passes) {
     __shared__ uint32_t buf[256];
     for (int p = 0; p < passes; ++p) {
         uint32_t v = hist[p * 256 + threadIdx.x];
@@ -82,7 +82,7 @@ __global__ void k_sort_offsets(uint32_t* hist, int passes) {
 
 // One digit pass. The sorted word is `key` (major or minor per pass); `other` rides along.
 template <bool kTwoWords, bool kPayload>
-__global__ void __launch_bounds__(kSortThreads)
+static __global__ void __launch_bounds__(kSortThreads)
     k_onesweep(const uint32_t* __restrict__ key_in, const uint32_t* __restrict__ other_in,
                const uint32_t* __restrict__ val_in, uint32_t* __restrict__ key_out, uint32_t* __restrict__ other_out,
                uint32_t* __restrict__ val_out, const uint32_t* __restrict__ count_ptr, uint32_t n_fixed, uint32_t cap,
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kSortThreads)
 
 // Single-pass exclusive scan of u32 values (decoupled look-back over 2048-value tiles).
 // Writes out[i] = sum(in[0..i)) and, from the last tile, *total = sum(in[0..n)).
-__global__ void __launch_bounds__(kSortThreads)
+static __global__ void __launch_bounds__(kSortThreads)
     k_scan_exclusive(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint32_t* __restrict__ count_ptr,
                      uint32_t n_fixed, uint32_t cap, uint32_t* __restrict__ total, uint32_t* __restrict__ lookback,
                      uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status) {

@@ -536,13 +536,18 @@ void destroy_device(dyn_world* w) {
     DeviceState* d = w->dev;
     if (!d) return;
     cudaSetDevice(w->device);
-    if (d->stream) cudaStreamSynchronize(d->stream);
+    // the caller's stream may already be gone: wait for the whole device instead
+    cudaDeviceSynchronize();
     release_graphs(d);
     for (cudaEvent_t e : d->events) cudaEventDestroy(e);
     for (void* p : d->allocs) cudaFree(p);
+    for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
+        if (p) cudaFree(p);
+    }
     if (d->own_stream) cudaStreamDestroy(d->own_stream);
     delete d;
     w->dev = nullptr;
+    cudaGetLastError();  // nothing from tear-down may surface in a later, unrelated call
 }
 
 }  // namespace dyn
@@ -920,12 +925,11 @@ DYN_API dyn_status dyn_radix_sort(dyn_world* w, uint32_t* major, uint32_t* minor
             if (*p) cudaFree(*p);
             *p = nullptr;
         }
+        d->sort_alt_cap = 0;
+        // owned here (freed on growth and in destroy_device), not in the world's allocation list
         DYN_CUDA(cudaMalloc(&d->sort_alt0, (size_t)n * 4));
         DYN_CUDA(cudaMalloc(&d->sort_alt1, (size_t)n * 4));
         DYN_CUDA(cudaMalloc(&d->sort_alt2, (size_t)n * 4));
-        d->allocs.push_back(d->sort_alt0);
-        d->allocs.push_back(d->sort_alt1);
-        d->allocs.push_back(d->sort_alt2);
         d->sort_alt_cap = n;
     }
     uint32_t tiles = div_up(n, kSortTile);

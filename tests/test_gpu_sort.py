@@ -63,3 +63,27 @@ def test_two_word_keys(world):
     assert np.array_equal(smaj, major[order])
     assert np.array_equal(smin, minor[order])
     assert np.array_equal(spay, payload[order])
+
+
+def test_growing_sort_scratch_then_closing_leaves_no_latched_error():
+    """Sorting ever larger arrays regrows the world's sort scratch; closing the world afterwards
+    must not free anything twice, and the next world's calls must see no stale CUDA error."""
+    from dynamis_b200 import scenes
+
+    w = World(capacity={"pairs": 1 << 20})
+    scenes.sphere_row(2).build(w)
+    w.step(1 / 60)
+    w.wait()
+    for n in (10, 1000, 100000):
+        keys = np.arange(n, 0, -1, dtype=np.uint32)
+        out, _, _ = gpu_sort(w, keys.copy(), None, None, 4, 0)
+        assert np.array_equal(out, np.sort(keys))
+    w.close()
+    w2 = World(capacity={"pairs": 1 << 20})
+    scenes.sphere_row(2).build(w2)
+    w2.step(1 / 60)
+    w2.wait()
+    keys = np.arange(5000, 0, -1, dtype=np.uint32)
+    out, _, _ = gpu_sort(w2, keys.copy(), None, None, 4, 0)
+    assert np.array_equal(out, np.sort(keys))
+    w2.close()
