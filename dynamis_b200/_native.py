@@ -53,6 +53,7 @@ SIGNATURES = {
     "dyn_stage_name": (ctypes.c_char_p, [U32]),
     "dyn_stage_timings": (I32, [P, P, U32]),
     "dyn_radix_sort": (I32, [P, P, P, P, U32, U32, U32]),
+    "dyn_radix_sort_static": (I32, [P, P, P, U32, U32, U32, P]),
 }
 
 

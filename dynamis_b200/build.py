@@ -56,6 +56,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     world_cu = CSRC / "world.cu"
     scene_cpp = CSRC / "scene.cpp"
     world_o = BUILD / "world.o"
+    static_cu = CSRC / "static_sort.cu"
+    static_o = BUILD / "static_sort.o"
     scene_o = BUILD / "scene.o"
     nvcc = _nvcc()
     flags = list(NVCC_FLAGS)
@@ -63,10 +65,12 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
         flags += ["-Xptxas", "-v"]
     if _stale(world_o, [world_cu, *headers]) or ptxas_info:
         _run([nvcc, *ARCH, *flags, "-I", str(INCLUDE), "-c", str(world_cu), "-o", str(world_o)])
+    if _stale(static_o, [static_cu, *headers]):
+        _run([nvcc, *ARCH, *flags, "-I", str(INCLUDE), "-c", str(static_cu), "-o", str(static_o)])
     if _stale(scene_o, [scene_cpp, *headers]):
         _run(["g++", *CXX_FLAGS, "-I", str(INCLUDE), "-c", str(scene_cpp), "-o", str(scene_o)])
-    if _stale(LIBRARY, [world_o, scene_o]):
-        _run([nvcc, *ARCH, "-shared", "-o", str(LIBRARY), str(world_o), str(scene_o)])
+    if _stale(LIBRARY, [world_o, static_o, scene_o]):
+        _run([nvcc, *ARCH, "-shared", "-o", str(LIBRARY), str(world_o), str(static_o), str(scene_o)])
     if verbose:
         print(f"built {LIBRARY}")
     return LIBRARY

@@ -199,6 +199,20 @@ DYN_API dyn_status dyn_stage_timings(dyn_world* world, float* ms, uint32_t n);
 DYN_API dyn_status dyn_radix_sort(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
                                   uint32_t major_digits, uint32_t minor_digits);
 
+/* No counterpart in the reference. The same stable LSD sort as dyn_radix_sort for callers that
+ * cannot allocate device memory (an external pool that forbids out-of-band allocations, or a path
+ * where cudaMalloc / cudaFree would synchronise the device): it needs no world and allocates
+ * nothing. Its scratch is one file-scope device array sized for DYN_STATIC_SORT_MAX_KEYS keys
+ * (about 4.2 MB, held by every GPU that loads the library until exit); larger n returns
+ * DYN_ERR_CAPACITY. Keys and payload are device pointers, sorted in place on cuda_stream (NULL =
+ * the legacy default stream); the call is asynchronous. All calls on a device share the array,
+ * so calls that overlap on the GPU race and must be serialised by the caller. The first call on
+ * a device (with that device current) looks up the array's address; make it before any stream
+ * capture. */
+#define DYN_STATIC_SORT_MAX_KEYS 262144u
+DYN_API dyn_status dyn_radix_sort_static(uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
+                                         uint32_t major_digits, uint32_t minor_digits, void* cuda_stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
