@@ -68,7 +68,7 @@ class DynamisError(RuntimeError):
 def _load() -> ctypes.CDLL:
     if not LIBRARY.exists():
         raise ImportError(
-            f"{LIBRARY} is missing: build it with `python -m dynamis_b200.build` (nvcc, sm_100a); "
+            f"{LIBRARY} is missing: build it with `python dynamis_b200/build.py` (nvcc, sm_100a); "
             "there is no CPU fallback")
     lib = ctypes.CDLL(str(LIBRARY))
     for name, (restype, argtypes) in SIGNATURES.items():

@@ -87,3 +87,34 @@ def test_growing_sort_scratch_then_closing_leaves_no_latched_error():
     out, _, _ = gpu_sort(w2, keys.copy(), None, None, 4, 0)
     assert np.array_equal(out, np.sort(keys))
     w2.close()
+
+
+def test_known_answers_of_the_reference_sort_tests(world):
+    """The cases of crates/dynamis-sort/tests/gpu.rs:192-275 from tests/golden/sort_known_answers.json."""
+    import hashlib
+    import json
+    from pathlib import Path
+
+    from test_golden import xorshift_keys
+
+    cases = json.loads((Path(__file__).resolve().parent / "golden" / "sort_known_answers.json").read_text())
+    ten = cases["ten_keys"]
+    keys = np.array(ten["keys"], np.uint32)
+    major, _, payload = gpu_sort(world, keys, None, np.arange(len(keys), dtype=np.uint32), ten["major_digits"], 0)
+    assert major.tolist() == ten["sorted"] and payload.tolist() == ten["payload"]
+    mm = cases["major_above_minor"]
+    major, minor, payload = gpu_sort(world, np.array(mm["major"], np.uint32), np.array(mm["minor"], np.uint32),
+                                     np.arange(len(mm["major"]), dtype=np.uint32), mm["major_digits"], mm["minor_digits"])
+    assert major.tolist() == mm["sorted_major"] and minor.tolist() == mm["sorted_minor"]
+    assert payload.tolist() == mm["payload"]
+    wide = cases["wide_two_word"]
+    major = xorshift_keys(wide["length"], wide["major_salt"])
+    minor = xorshift_keys(wide["length"], wide["minor_salt"])
+    smaj, smin, pay = gpu_sort(world, major, minor, np.arange(wide["length"], dtype=np.uint32), wide["major_digits"],
+                               wide["minor_digits"])
+
+    def digest(a):
+        return hashlib.sha256(np.ascontiguousarray(a, np.uint32).tobytes()).hexdigest()
+
+    assert digest(smaj) == wide["sorted_major_sha256"] and digest(smin) == wide["sorted_minor_sha256"]
+    assert digest(pay) == wide["payload_sha256"]
