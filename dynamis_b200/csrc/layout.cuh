@@ -53,6 +53,7 @@ enum Ctl : uint32_t {
     CTL_LIST0 = 10,  // narrowphase class lists (3 words)
     CTL_EPA = 13,    // penetrating convex pairs queued for EPA
     CTL_HITS = 14,   // convex pairs queued for the manifold
+    CTL_CELL_OVERFLOW = 15,  // the cell table could not place a run: lookups fall back to searching
     CTL_COUNT = 16
 };
 
@@ -100,6 +101,8 @@ struct DeviceWorld {
     uint32_t* ekey_alt;
     uint32_t* eval_alt;
     float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits
+    uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
+    uint32_t cell_bits;
     uint32_t* pmaj;
     uint32_t* pmin;
     uint32_t* pmaj_alt;

@@ -1009,14 +1009,23 @@ __device__ Hit convex_hit(const DeviceWorld& w, const WShape& first, const WShap
 
 struct GjkOut {
     bool pen;
+    bool rejected;  // the centre-axis gap already exceeds the caller's margin: no contact
     uint32_t count;
     float dist;
     f3 pa, pb, normal;
     SPt s[4];
 };
 
-__device__ GjkOut gjk_phase(const DeviceWorld& w, const WShape& first, const WShape& second) {
+// With reject_gap > 0, a pair whose gap along the centre axis exceeds reject_gap returns at once
+// with `rejected` set. That answer equals the full path's: the first support point is taken along
+// that axis, a gap g along any unit axis bounds the true distance from below, GJK's reported
+// distance (the closest point of a simplex inside the Minkowski difference) is at least the true
+// distance, and the penetration probe includes the centre axis, whose depth is -g < 0. So the full
+// path reports either a distance >= g or no hit, and the caller discards both when g exceeds its
+// margin; reject_gap carries a tolerance above the margin for the rounding of the dot products.
+__device__ GjkOut gjk_phase(const DeviceWorld& w, const WShape& first, const WShape& second, float reject_gap = -1.0f) {
     GjkOut o;
+    o.rejected = false;
     o.count = 0;
     o.dist = 0.0f;
     o.pa = first.center;
@@ -1027,6 +1036,10 @@ __device__ GjkOut gjk_phase(const DeviceWorld& w, const WShape& first, const WSh
     if (length(dir) < 1e-8f) dir = mk3(1.0f, 0.0f, 0.0f);
     o.s[0] = support_pair(w, first, second, dir);
     o.count = 1;
+    if (reject_gap > 0.0f && dot(o.s[0].w, dir) < -reject_gap * length(dir)) {
+        o.rejected = true;
+        return o;
+    }
     SRes cl = simplex_closest(o.s, o.count);
     float tiny = 1e-4f * wmin(shape_scale(first), shape_scale(second));
     for (uint32_t iter = 0; iter < 24u; ++iter) {

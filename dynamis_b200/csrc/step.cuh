@@ -287,6 +287,66 @@ __device__ __forceinline__ uint32_t lower_bound(const uint32_t* keys, uint32_t n
     return lo;
 }
 
+// ---- cell table: cell key -> first index of its run in the sorted entries ----
+// An open-addressing table rebuilt every step after the entry sort, sized to twice the live entry
+// count (a power of two, at most 1 << cell_bits), so the coarse-level walk of k_pairs finds a cell
+// in one or two probes instead of a binary search over all entries. Key 0xFFFFFFFF marks an empty
+// slot; no cell key reaches it (levels stop at DYN_GRID_LEVEL_LIMIT). If an insert ever fails its
+// bounded probe, CTL_CELL_OVERFLOW is set and every lookup of that step searches the sorted keys
+// instead, so the pairs found never depend on the table.
+constexpr uint32_t kCellEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kCellProbeLimit = 1024u;
+__device__ __forceinline__ uint32_t cell_table_bits(const DeviceWorld& w, uint32_t live) {
+    uint32_t bits = 10u;
+    while (bits < w.cell_bits && (1u << bits) < 2u * live) ++bits;
+    return bits;
+}
+__device__ __forceinline__ uint32_t cell_slot(uint32_t key, uint32_t bits) { return (key * 0x9E3779B1u) >> (32u - bits); }
+
+__global__ void k_cell_clear(DeviceWorld w) {
+    const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
+    const uint32_t slots = 1u << cell_table_bits(w, live);
+    GRID_STRIDE(i, slots) w.cell_table[i] = make_uint2(kCellEmpty, 0u);
+}
+
+__global__ void k_cell_insert(DeviceWorld w) {
+    const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
+    const uint32_t bits = cell_table_bits(w, live);
+    const uint32_t mask = (1u << bits) - 1u;
+    GRID_STRIDE(i, live) {
+        uint32_t key = w.ekey[i];
+        if (i > 0u && w.ekey[i - 1u] == key) continue;
+        uint32_t slot = cell_slot(key, bits);
+        bool placed = false;
+        for (uint32_t probe = 0; probe < kCellProbeLimit; ++probe) {
+            if (atomicCAS(&w.cell_table[slot].x, kCellEmpty, key) == kCellEmpty) {
+                w.cell_table[slot].y = i;
+                placed = true;
+                break;
+            }
+            slot = (slot + 1u) & mask;
+        }
+        if (!placed) atomicOr(&w.ctl[CTL_CELL_OVERFLOW], 1u);
+    }
+}
+
+// First index of the run of `key` in the sorted entries, or `live` when no entry has it.
+__device__ __forceinline__ uint32_t cell_find(const DeviceWorld& w, uint32_t live, uint32_t bits, bool overflow, uint32_t key) {
+    if (overflow) {
+        uint32_t j = lower_bound(w.ekey, live, key);
+        return (j < live && __ldg(w.ekey + j) == key) ? j : live;
+    }
+    const uint32_t mask = (1u << bits) - 1u;
+    uint32_t slot = cell_slot(key, bits);
+    for (uint32_t probe = 0; probe < kCellProbeLimit; ++probe) {
+        uint2 e = __ldg(w.cell_table + slot);
+        if (e.x == key) return e.y;
+        if (e.x == kCellEmpty) return live;
+        slot = (slot + 1u) & mask;
+    }
+    return live;
+}
+
 // One thread per sorted entry: coarse-level links of a primary entry, then same-cell mates.
 __global__ void k_pairs(DeviceWorld w) {
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
@@ -294,6 +354,8 @@ __global__ void k_pairs(DeviceWorld w) {
     const uint32_t occupied =
         w.counters[DYN_COUNTER_GRID_LEVELS] | w.counters[DYN_COUNTER_RESTING_LEVELS] | w.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
     const bool coarse_active = w.counters[DYN_COUNTER_COARSE_ACTIVE] != 0u;
+    const uint32_t bits = cell_table_bits(w, live);
+    const bool overflow = w.ctl[CTL_CELL_OVERFLOW] != 0u;
     GRID_STRIDE(index, live) {
         uint32_t node = w.eval[index];
         GEntry e = load_entry(w, node);
@@ -319,7 +381,7 @@ __global__ void k_pairs(DeviceWorld w) {
                         for (int z = lo.z; z <= hi.z; ++z) {
                             I3 cell = I3{x, y, z};
                             uint32_t key = cell_key(link, cell);
-                            uint32_t j = lower_bound(w.ekey, live, key);
+                            uint32_t j = cell_find(w, live, bits, overflow, key);
                             for (; j < live && __ldg(w.ekey + j) == key; ++j) {
                                 uint32_t other = w.eval[j];
                                 if (other == node) continue;
@@ -522,6 +584,10 @@ __device__ __forceinline__ void push_hit(const DeviceWorld& w, uint32_t index, c
     w.hit_data[2 * (size_t)slot + 1] = mk4(hit.normal, 0.0f);
 }
 
+// Slack above the contact margin before a pair is rejected on its centre-axis gap alone: well above
+// the rounding of support points at world coordinates of a few hundred metres (~1e-5 m).
+constexpr float kRejectTolerance = 1e-3f;
+
 // Phase 1: GJK per pair; separated pairs are answered here (probe), penetrating ones queue for EPA.
 __global__ void __launch_bounds__(128) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = min(w.ctl[CTL_LIST0 + PC_CONVEX], w.p_cap);
@@ -531,7 +597,11 @@ __global__ void __launch_bounds__(128) k_convex_gjk(DeviceWorld w, dyn_step_para
         WShape a, b;
         DBody fb, sb;
         convex_shapes(w, index, &a, &b, &fb, &sb);
-        GjkOut g = gjk_phase(w, a, b);
+        GjkOut g = gjk_phase(w, a, b, pair_margin(p, fb, sb) + kRejectTolerance);
+        if (g.rejected) {
+            w.pair_flag[index] = 0u;
+            continue;
+        }
         if (g.pen) {
             uint32_t slot = append_slot(&w.ctl[CTL_EPA]);
             w.epa_list[slot] = index;
@@ -752,12 +822,19 @@ __global__ void k_contact_begin(DeviceWorld w, dyn_step_params p) {
 }
 
 // ---- islands (island_link*.wgsl, island_flatten.wgsl, island_aggregate.wgsl, island_count.wgsl) ----
+// Union-find over the dynamic rows, hooking the higher root under the lower one, so each island's
+// root is its smallest row. Parents are read with ld.global.cg: the L2 copy every CAS acts on (an L1
+// copy could stay stale for the whole kernel). Finding halves the path: a non-root row's parent
+// entry only ever moves to one of its own ancestors, and roots change only through the CAS, so the
+// plain store of the grandparent never undoes a hook.
 __device__ __forceinline__ uint32_t island_find(const DeviceWorld& w, uint32_t node) {
     uint32_t current = node;
-    uint32_t parent = atomicAdd(&w.parents[current], 0u);
+    uint32_t parent = __ldcg(w.parents + current);
     for (uint32_t guard = 0; parent != current && guard < w.nd; ++guard) {
-        current = parent;
-        parent = atomicAdd(&w.parents[current], 0u);
+        uint32_t grand = __ldcg(w.parents + parent);
+        if (grand != parent) w.parents[current] = grand;
+        current = grand;
+        parent = __ldcg(w.parents + current);
     }
     return current;
 }
@@ -788,12 +865,19 @@ __global__ void k_island_link(DeviceWorld w, dyn_step_params p) {
         if (!joined) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
     }
 }
+// island_flatten.wgsl:4-8 repeated ilog2(max(N,2))+1 times leaves every row pointing at its root
+// (pointer jumping doubles the reach each round and a chain is at most N long); one pass that
+// follows each chain to its root gives that same array. Roots no longer change here, and rows
+// rewritten concurrently only ever point further up their own chain.
 __global__ void k_island_flatten(DeviceWorld w) {
     GRID_STRIDE(i, w.nd) {
-        volatile uint32_t* par = w.parents;
-        uint32_t parent = par[i];
-        uint32_t grand = par[parent];
-        par[i] = min(parent, grand);
+        uint32_t root = i;
+        uint32_t parent = __ldcg(w.parents + root);
+        for (uint32_t guard = 0; parent != root && guard < w.nd; ++guard) {
+            root = parent;
+            parent = __ldcg(w.parents + root);
+        }
+        w.parents[i] = root;
     }
 }
 __global__ void k_island_aggregate(DeviceWorld w) {

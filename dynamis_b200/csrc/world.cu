@@ -198,6 +198,9 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.ekey_alt, E);
         A(dw.eval_alt, E);
         A(dw.entries, 2 * (size_t)E);
+        dw.cell_bits = 10u;
+        while (dw.cell_bits < 31u && ((size_t)1 << dw.cell_bits) < 2 * (size_t)E) ++dw.cell_bits;
+        A(dw.cell_table, (size_t)1 << dw.cell_bits);
         A(dw.pmaj, P);
         A(dw.pmin, P);
         A(dw.pmaj_alt, P);
@@ -449,6 +452,8 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_ENTRY_SORT);
     record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
     mark(ST_PAIRS);
+    k_cell_clear<<<blocks_for(1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
+    k_cell_insert<<<blocks_for(E, 256), 256, 0, s>>>(dw);
     k_pairs<<<blocks_for(E, 256), 256, 0, s>>>(dw);
     mark(ST_PAIR_SORT);
     uint32_t words = key_words(std::max(dw.k, 1u));
@@ -469,8 +474,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
     mark(ST_ISLANDS);
     k_island_link<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
-    uint32_t rounds = 32u - (uint32_t)__builtin_clz(std::max(dw.nd, 2u));
-    for (uint32_t r = 0; r < rounds; ++r) k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     k_island_aggregate<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
     k_wake_live<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
