@@ -54,7 +54,8 @@ enum Ctl : uint32_t {
     CTL_EPA = 13,    // penetrating convex pairs queued for EPA
     CTL_HITS = 14,   // convex pairs queued for the manifold
     CTL_CELL_OVERFLOW = 15,  // the cell table could not place a run: lookups fall back to searching
-    CTL_COUNT = 16
+    CTL_GJK_NEXT = 16,       // next convex pair ticket of the GJK kernel
+    CTL_COUNT = 32
 };
 
 struct DeviceWorld {

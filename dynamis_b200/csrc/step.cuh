@@ -588,31 +588,196 @@ __device__ __forceinline__ void push_hit(const DeviceWorld& w, uint32_t index, c
 // the rounding of support points at world coordinates of a few hundred metres (~1e-5 m).
 constexpr float kRejectTolerance = 1e-3f;
 
-// Phase 1: GJK per pair; separated pairs are answered here (probe), penetrating ones queue for EPA.
+// Phase 1: GJK per pair (convex.wgsl:464-521) and, for separated shapes, the penetration probe
+// (convex.wgsl:532-582, 588-600); penetrating pairs queue for EPA.
+//
+// The work of one pair is a sequence of support-pair evaluations: the first along the centre axis,
+// one per GJK iteration along -v, up to three that grow a penetrating simplex to a tetrahedron, and
+// one per probe direction. Each lane runs its pair as a state machine that makes exactly one
+// support-pair evaluation per trip of the loop below, and a lane whose pair is done takes the next
+// pair from the convex list through a shared ticket. So the lanes of a warp keep evaluating
+// supports together instead of waiting for the warp's slowest pair, whatever their pairs' iteration
+// counts. Each state does the same arithmetic, in the same order, as gjk_phase followed by
+// separated_hit (narrow.cuh); only the interleaving of pairs on a lane changes.
+enum GjkState : uint32_t { GS_IDLE = 0, GS_FIRST = 1, GS_ITER = 2, GS_EXPAND = 3, GS_PROBE = 4 };
+// simplex triples in the probe's order (i < j < k ascending), one per bit of GjkLane::triples
+__constant__ uint8_t kProbeTriple[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+constexpr uint32_t kProbeCentre = 4u, kProbeAxes = 5u, kProbeEnd = 11u;
+
+struct GjkLane {
+    uint32_t state, index, count, iter, probe, triples;
+    float tiny, margin, dist, best;
+    f3 pa, pb, normal, best_normal;
+    SPt s[4];
+    SRes cl;
+    WShape a, b;
+};
+
+__device__ __forceinline__ f3 probe_direction(const GjkLane& L, uint32_t k) {
+    const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    if (k < kProbeCentre) {
+        const f3 wi = L.s[kProbeTriple[k][0]].w, wj = L.s[kProbeTriple[k][1]].w, wk = L.s[kProbeTriple[k][2]].w;
+        return normalize(cross(wj - wi, wk - wi));
+    }
+    if (k == kProbeCentre) return normalize(L.b.center - L.a.center);
+    const uint32_t x = k - kProbeAxes;
+    return normalize(mk3(ax[x][0], ax[x][1], ax[x][2]));
+}
+// The first probe position at or after k that the probe would test.
+__device__ __forceinline__ uint32_t probe_next(const GjkLane& L, uint32_t k) {
+    for (; k < kProbeCentre; ++k)
+        if (L.triples & (1u << k)) return k;
+    if (k == kProbeCentre && length(L.b.center - L.a.center) <= 1e-8f) ++k;
+    return k;
+}
+// penetration_probe's direction list over the final simplex: triples whose normal is not degenerate.
+__device__ __forceinline__ void probe_begin(GjkLane& L) {
+    L.triples = 0u;
+    const uint32_t ntri = L.count == 3u ? 1u : (L.count == 4u ? 4u : 0u);
+    for (uint32_t t = 0; t < ntri; ++t) {
+        const f3 wi = L.s[kProbeTriple[t][0]].w, wj = L.s[kProbeTriple[t][1]].w, wk = L.s[kProbeTriple[t][2]].w;
+        if (length(cross(wj - wi, wk - wi)) > 1e-8f) L.triples |= 1u << t;
+    }
+    L.best = 3.402823466e38f;
+    L.best_normal = mk3(0.0f, 1.0f, 0.0f);
+    L.probe = probe_next(L, 0u);
+    L.state = GS_PROBE;
+}
+// A penetrating pair with its tetrahedron complete goes to the EPA queue.
+__device__ __forceinline__ void gjk_to_epa(const DeviceWorld& w, GjkLane& L) {
+    const uint32_t slot = append_slot(&w.ctl[CTL_EPA]);
+    w.epa_list[slot] = L.index;
+    for (uint32_t k = 0; k < 4; ++k) w.epa_simplex[4 * (size_t)slot + k] = mk4(L.s[k].w, 0.0f);
+    L.state = GS_IDLE;
+}
+// The loop head of gjk_phase: terminate, grow a penetrating simplex, or take another iteration.
+__device__ __forceinline__ void gjk_head(const DeviceWorld& w, GjkLane& L) {
+    if (L.iter >= 24u) {
+        probe_begin(L);
+    } else if (L.cl.pen || length(L.cl.v) < L.tiny) {
+        if (L.count < 4u) {
+            L.state = GS_EXPAND;
+        } else {
+            gjk_to_epa(w, L);
+        }
+    } else {
+        L.state = GS_ITER;
+    }
+}
+__device__ __forceinline__ void gjk_separated(GjkLane& L) {
+    L.dist = length(L.cl.v);
+    L.pa = L.cl.pa;
+    L.pb = L.cl.pb;
+    if (L.dist > 1e-6f) L.normal = sign_normalize(L.cl.pb - L.cl.pa);
+    probe_begin(L);
+}
+
 __global__ void __launch_bounds__(128) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = min(w.ctl[CTL_LIST0 + PC_CONVEX], w.p_cap);
     const uint32_t* list = w.np_list + (size_t)PC_CONVEX * w.p_cap;
-    GRID_STRIDE(i, count) {
-        uint32_t index = list[i];
-        WShape a, b;
-        DBody fb, sb;
-        convex_shapes(w, index, &a, &b, &fb, &sb);
-        GjkOut g = gjk_phase(w, a, b, pair_margin(p, fb, sb) + kRejectTolerance);
-        if (g.rejected) {
-            w.pair_flag[index] = 0u;
-            continue;
+    GjkLane L;
+    L.state = GS_IDLE;
+    for (;;) {
+        if (L.state == GS_IDLE) {
+            const uint32_t ticket = append_slot(&w.ctl[CTL_GJK_NEXT]);
+            if (ticket >= count) break;
+            L.index = list[ticket];
+            DBody fb, sb;
+            convex_shapes(w, L.index, &L.a, &L.b, &fb, &sb);
+            L.margin = pair_margin(p, fb, sb);
+            L.count = 0u;
+            L.dist = 0.0f;
+            L.pa = L.a.center;
+            L.pb = L.b.center;
+            L.normal = sign_normalize(L.b.center - L.a.center);
+            L.state = GS_FIRST;
         }
-        if (g.pen) {
-            uint32_t slot = append_slot(&w.ctl[CTL_EPA]);
-            w.epa_list[slot] = index;
-            for (uint32_t k = 0; k < 4; ++k) w.epa_simplex[4 * (size_t)slot + k] = mk4(g.s[k].w, 0.0f);
-            continue;
-        }
-        Hit hit = separated_hit(w, a, b, g);
-        if (hit.distance <= pair_margin(p, fb, sb)) {
-            push_hit(w, index, hit);
+        f3 d;
+        if (L.state == GS_FIRST) {
+            d = L.b.center - L.a.center;
+            if (length(d) < 1e-8f) d = mk3(1.0f, 0.0f, 0.0f);
+        } else if (L.state == GS_ITER) {
+            d = -L.cl.v;
+        } else if (L.state == GS_EXPAND) {
+            d = simplex_expand_dir(L.s, L.count);
         } else {
-            w.pair_flag[index] = 0u;
+            d = probe_direction(L, L.probe);
+        }
+        const SPt sp = support_pair(w, L.a, L.b, d);
+        if (L.state == GS_FIRST) {
+            L.s[0] = sp;
+            L.count = 1u;
+            // the exact centre-axis rejection of gjk_phase
+            if (dot(sp.w, d) < -(L.margin + kRejectTolerance) * length(d)) {
+                w.pair_flag[L.index] = 0u;
+                L.state = GS_IDLE;
+                continue;
+            }
+            L.cl = simplex_closest(L.s, L.count);
+            L.tiny = 1e-4f * wmin(shape_scale(L.a), shape_scale(L.b));
+            L.iter = 0u;
+            gjk_head(w, L);
+        } else if (L.state == GS_ITER) {
+            const f3 v = L.cl.v;
+            if (dot(sp.w, -v) <= dot(v, -v) + 1e-4f * wmax(1.0f, dot(v, v))) {
+                gjk_separated(L);
+                continue;
+            }
+            SPt kept[4];
+            uint32_t kc = 0;
+            for (uint32_t i = 0; i < 4; ++i) {
+                if (L.cl.lam[i] > 1e-6f) kept[kc++] = L.s[i];
+            }
+            if (kc == 0u) {
+                kept[0] = L.s[0];
+                kc = 1;
+            }
+            for (uint32_t i = 0; i < kc; ++i) L.s[i] = kept[i];
+            L.count = kc;
+            const float span = shape_scale(L.b);
+            const float tol = (1e-5f * span) * (1e-5f * span);
+            bool holds = false;
+            for (uint32_t i = 0; i < L.count; ++i) {
+                const f3 off = L.s[i].w - sp.w;
+                if (dot(off, off) <= tol) holds = true;
+            }
+            if (holds) {
+                gjk_separated(L);
+                continue;
+            }
+            L.s[L.count] = sp;
+            L.count += 1u;
+            L.cl = simplex_closest(L.s, L.count);
+            L.iter += 1u;
+            gjk_head(w, L);
+        } else if (L.state == GS_EXPAND) {
+            L.s[L.count] = sp;
+            L.count += 1u;
+            if (L.count == 4u) gjk_to_epa(w, L);
+        } else {
+            const float depth = dot(sp.w, d);
+            if (depth < L.best) {
+                L.best = depth;
+                L.best_normal = d;
+            }
+            L.probe = depth <= 0.0f ? kProbeEnd : probe_next(L, L.probe + 1u);
+            if (L.probe >= kProbeEnd) {
+                // separated_hit, then the margin test of the caller
+                Hit hit{3.402823466e38f, s3(0.0f), s3(0.0f)};
+                if (L.best > 0.0f) {
+                    f3 normal = L.best_normal;
+                    if (dot(normal, L.b.center - L.a.center) < 0.0f) normal = -normal;
+                    hit = Hit{-L.best, (L.pa + L.pb) * 0.5f, normal};
+                } else if (L.dist > 0.0f) {
+                    hit = Hit{L.dist, (L.pa + L.pb) * 0.5f, L.normal};
+                }
+                if (hit.distance <= L.margin) {
+                    push_hit(w, L.index, hit);
+                } else {
+                    w.pair_flag[L.index] = 0u;
+                }
+                L.state = GS_IDLE;
+            }
         }
     }
 }

@@ -463,7 +463,8 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
     k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
-    k_convex_gjk<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    // persistent: lanes draw pairs from a ticket, so four blocks per SM keep every SM busy
+    k_convex_gjk<<<148u * 4u, 128, 0, s>>>(dw, p);
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     mark(ST_COMPACT);
