@@ -214,6 +214,10 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         world._check(lib.dyn_download_states(world._h, ptr(states_out), bodies))
         states_in, states_out = states_out, states_in  # the result feeds the next step
     e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
     log(f"e2e {e2e_steps} steps: {e2e_s / e2e_steps * 1e3:.3f} ms/step")
     result = {
         "metric": METRIC, "value": bodies * args.steps * world_size / (ms * 1e-3), "unit": UNIT,
@@ -223,7 +227,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                    "parallelism": f"replicas{world_size}" if world_size > 1 else "single-world",
                    "l2": "working set > 126 MB L2 (no flush between steps)", "counts_last_step": counts,
                    "scene_build_s": round(build_s, 2)},
-        "e2e": {"value": bodies * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bodies * R.BODY_STATE.itemsize,
+        "e2e": {"value": bodies * e2e_steps * world_size / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bodies * R.BODY_STATE.itemsize,
                 "d2h_bytes_per_step": bodies * R.BODY_STATE.itemsize},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk["source"],

@@ -38,6 +38,16 @@ struct ContactSet {
     float4* pos;     // position.xyz, 0
 };
 
+// Pose-only terms of the contact blocks, rebuilt once per substep (point slot p of contact i at
+// [p * cap + i], like ContactSet).
+struct SolverRows {
+    float4* arm_a;     // contact point - first body's world centre of mass, normal effective mass
+    float4* arm_b;     // contact point - second body's world centre of mass, unsplit normal mass
+    float2* masses;    // tangent-1 and tangent-2 effective masses
+    float4* tangent1;  // [cap] tangent 1, twist mass
+    float4* tangent2;  // [cap] tangent 2, 0
+};
+
 // Control words (device-side counts the graph's kernels read instead of host values).
 enum Ctl : uint32_t {
     CTL_ENTRIES = 0,
@@ -120,6 +130,7 @@ struct DeviceWorld {
     float4* hit_data;        // [2][slot]: point.xyz + distance, normal.xyz
     ContactSet cur;
     ContactSet arc;
+    SolverRows srows;
     uint32_t* matched;
     // islands, live list, solver
     uint32_t* parents;

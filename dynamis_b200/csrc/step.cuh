@@ -1141,27 +1141,113 @@ __device__ __forceinline__ DBody split_body(DBody b, float s) {
     return b;
 }
 
+// ---- pose-only terms of each contact block, once per substep ----
+// Between integrate and advance no pose changes, so the contact arms, the effective masses along
+// the normal and both tangents and the twist mass are the same in the warm start and in every
+// velocity iteration of a substep. k_solve_prepare computes them once per substep with the very
+// expressions solver_contact_block.wgsl:24-80 uses (stored floats reload bit for bit), and k_warm
+// and k_solve read them. arm_a/arm_b hold a contact point minus the body's world centre of mass,
+// the operand that point_velocity and the impulse torques take.
+__device__ __forceinline__ f3 point_velocity_arm(const DBody& b, f3 arm_from_com) {
+    return b.velocity + cross(b.angular_velocity, arm_from_com);
+}
+__device__ __forceinline__ void pair_impulse_arms(DBody* a, DBody* b, f3 ra, f3 rb, f3 j) {
+    a->velocity = a->velocity - j * a->inverse_mass;
+    a->angular_velocity = a->angular_velocity - dbody_iinv(*a, cross(ra, j));
+    b->velocity = b->velocity + j * b->inverse_mass;
+    b->angular_velocity = b->angular_velocity + dbody_iinv(*b, cross(rb, j));
+}
+__device__ __forceinline__ float momentum_mass_arms(const DBody& a, const DBody& b, f3 ra, f3 rb, f3 axis) {
+    f3 rax = cross(ra, axis), rbx = cross(rb, axis);
+    return a.inverse_mass + b.inverse_mass + dot(rax, dbody_iinv(a, rax)) + dot(rbx, dbody_iinv(b, rbx));
+}
+// The two bodies of a contact as the block sees them: the bodies, their mass-split copies, and the
+// frozen (massless) form of an inert one.
+struct BlockBodies {
+    DBody pf, ps, sf, ss;
+};
+__device__ __forceinline__ BlockBodies block_bodies(const DeviceWorld& w, uint4 r) {
+    BlockBodies b;
+    b.pf = load_dbody(w.hot, r.x);
+    b.ps = load_dbody(w.hot, r.y);
+    b.sf = split_body(b.pf, (float)max(w.hot[r.x].aux.z, 1u));
+    b.ss = split_body(b.ps, (float)max(w.hot[r.y].aux.z, 1u));
+    if (dbody_inert(b.pf)) {
+        b.pf = dbody_frozen(b.pf);
+        b.sf = dbody_frozen(b.sf);
+    }
+    if (dbody_inert(b.ps)) {
+        b.ps = dbody_frozen(b.ps);
+        b.ss = dbody_frozen(b.ss);
+    }
+    return b;
+}
+
+__global__ void k_solve_prepare(DeviceWorld w) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const uint32_t cap = w.c_cap;
+    const SolverRows& sr = w.srows;
+    GRID_STRIDE(i, count) {
+        uint4 r = w.cur.rows[i];
+        if (!resolves(r)) continue;
+        const BlockBodies b = block_bodies(w, r);
+        if (dbody_inert(b.pf) && dbody_inert(b.ps)) continue;
+        f3 normal = xyz(w.cur.normal[i]);
+        f3 t1, t2;
+        make_tangents(normal, &t1, &t2);
+        uint32_t pc = r.z & 0xFFu;
+        f3 ra[4], rb[4];
+        f3 reach_f = s3(0.0f), reach_s = s3(0.0f);
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            size_t o = (size_t)pi * cap + i;
+            f3 af = arm(b.pf, xyz(w.cur.la[o]));
+            f3 as = arm(b.ps, xyz(w.cur.lb[o]));
+            ra[pi] = af - dbody_com(b.pf);
+            rb[pi] = as - dbody_com(b.ps);
+            reach_f = reach_f + ra[pi];
+            reach_s = reach_s + rb[pi];
+        }
+        float count_f = (float)max(pc, 1u);
+        f3 spread_f = dbody_iinv(b.sf, cross(reach_f, normal));
+        f3 spread_s = dbody_iinv(b.ss, cross(reach_s, normal));
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            size_t o = (size_t)pi * cap + i;
+            f3 arm_f = cross(ra[pi], normal);
+            f3 arm_s = cross(rb[pi], normal);
+            float normal_mass = count_f * (b.sf.inverse_mass + b.ss.inverse_mass) + dot(spread_f, arm_f) + dot(spread_s, arm_s);
+            float truth = momentum_mass_arms(b.pf, b.ps, ra[pi], rb[pi], normal);
+            float t1_mass = momentum_mass_arms(b.sf, b.ss, ra[pi], rb[pi], t1) * count_f;
+            float t2_mass = momentum_mass_arms(b.sf, b.ss, ra[pi], rb[pi], t2) * count_f;
+            sr.arm_a[o] = mk4(ra[pi], normal_mass);
+            sr.arm_b[o] = mk4(rb[pi], truth);
+            sr.masses[o] = make_float2(t1_mass, t2_mass);
+        }
+        float twist_mass = dot(normal, dbody_iinv(b.sf, normal)) + dot(normal, dbody_iinv(b.ss, normal));
+        sr.tangent1[i] = mk4(t1, twist_mass);
+        sr.tangent2[i] = mk4(t2, 0.0f);
+    }
+}
+
 // solver_contact_block.wgsl:195-233
 __global__ void k_warm(DeviceWorld w) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     const uint32_t cap = w.c_cap;
+    const SolverRows& sr = w.srows;
     GRID_STRIDE(i, count) {
         uint4 r = w.cur.rows[i];
         if (!resolves(r)) continue;  // zero deltas change nothing
         DBody fl = load_dbody(w.hot, r.x), sl = load_dbody(w.hot, r.y);
         DBody f = dbody_inert(fl) ? dbody_frozen(fl) : fl;
         DBody s = dbody_inert(sl) ? dbody_frozen(sl) : sl;
+        if (dbody_inert(fl) && dbody_inert(sl)) continue;  // no rows were prepared; both deltas are zero
         f3 normal = xyz(w.cur.normal[i]);
-        f3 t1, t2;
-        make_tangents(normal, &t1, &t2);
+        f3 t1 = xyz(sr.tangent1[i]), t2 = xyz(sr.tangent2[i]);
         uint32_t pc = r.z & 0xFFu;
         for (uint32_t pi = 0; pi < pc; ++pi) {
             size_t o = (size_t)pi * cap + i;
-            f3 af = arm(f, xyz(w.cur.la[o]));
-            f3 as = arm(s, xyz(w.cur.lb[o]));
             float4 acc = w.cur.acc[o];
             f3 j = normal * acc.x + t1 * acc.y + t2 * acc.z;
-            pair_impulse(&f, &s, af, as, j);
+            pair_impulse_arms(&f, &s, xyz(sr.arm_a[o]), xyz(sr.arm_b[o]), j);
         }
         // an inert (frozen) body's delta is exactly zero: its atomics would add nothing
         if (!dbody_inert(fl))
@@ -1171,150 +1257,134 @@ __global__ void k_warm(DeviceWorld w) {
     }
 }
 
-// solver_contact_block.wgsl:6-193 (Jacobi block with mass splitting)
-__global__ void __launch_bounds__(128) k_solve(DeviceWorld w, dyn_step_params p) {
-    const uint32_t count = w.ctl[CTL_CONTACTS];
+// solver_contact_block.wgsl:6-193 (Jacobi block with mass splitting); the pose-only terms come
+// from k_solve_prepare.
+__device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step_params& p, uint32_t i, bool residual) {
     const uint32_t cap = w.c_cap;
-    const bool residual = w.ctl[CTL_ROUNDS] == p.solve_iterations;
-    GRID_STRIDE(i, count) {
-        uint4 r = w.cur.rows[i];
-        if (!resolves(r)) continue;
-        DBody pf = load_dbody(w.hot, r.x), ps = load_dbody(w.hot, r.y);
-        DBody sf = split_body(pf, (float)max(w.hot[r.x].aux.z, 1u));
-        DBody ss = split_body(ps, (float)max(w.hot[r.y].aux.z, 1u));
-        if (dbody_inert(pf)) {
-            pf = dbody_frozen(pf);
-            sf = dbody_frozen(sf);
+    const SolverRows& sr = w.srows;
+    uint4 r = w.cur.rows[i];
+    if (!resolves(r)) return;
+    const BlockBodies b = block_bodies(w, r);
+    const DBody& pf = b.pf;
+    const DBody& ps = b.ps;
+    if (dbody_inert(pf) && dbody_inert(ps)) return;
+    DBody first = pf, second = ps;
+    float4 nf = w.cur.normal[i];
+    f3 normal = xyz(nf);
+    float friction = nf.w;
+    float4 mat = w.cur.mat[i];
+    float4 tw1 = sr.tangent1[i];
+    f3 t1 = xyz(tw1), t2 = xyz(sr.tangent2[i]);
+    float twist_mass = tw1.w;
+    uint32_t pc = r.z & 0xFFu;
+    f3 ra[4], rb[4];
+    float4 acc[4];
+    float normal_total = 0.0f;
+    for (uint32_t pi = 0; pi < pc; ++pi) {
+        size_t o = (size_t)pi * cap + i;
+        acc[pi] = w.cur.acc[o];
+        normal_total = normal_total + wmax(acc[pi].x, 0.0f);
+    }
+    f3 impulses[4];
+    for (uint32_t pi = 0; pi < pc; ++pi) {
+        size_t o = (size_t)pi * cap + i;
+        float4 a4 = sr.arm_a[o], b4 = sr.arm_b[o];
+        float2 m2 = sr.masses[o];
+        ra[pi] = xyz(a4);
+        rb[pi] = xyz(b4);
+        float normal_mass = a4.w, truth = b4.w;
+        float depth = w.cur.la[o].w, target = w.cur.lb[o].w;
+        float an = acc[pi].x, at1 = acc[pi].y, at2 = acc[pi].z;
+        f3 rel = point_velocity_arm(ps, rb[pi]) - point_velocity_arm(pf, ra[pi]);
+        float normal_speed = dot(rel, normal);
+        float delta;
+        if (mat.z <= 0.0f) {
+            delta = (target - normal_speed) / normal_mass;
+        } else {
+            float bias = wmax(depth / p.dt, target);
+            float drag = 2.0f * mat.w * mat.z / p.dt;
+            float softness = mat.z * mat.z * truth / (p.dt * p.dt);
+            float prior = normal_speed - an * truth;
+            float wanted = (bias - (1.0f + drag) * prior) / (softness + (1.0f + drag) * truth);
+            delta = truth * (wanted - an) / normal_mass;
         }
-        if (dbody_inert(ps)) {
-            ps = dbody_frozen(ps);
-            ss = dbody_frozen(ss);
-        }
-        if (dbody_inert(pf) && dbody_inert(ps)) continue;
-        DBody first = pf, second = ps;
-        float4 nf = w.cur.normal[i];
-        f3 normal = xyz(nf);
-        float friction = nf.w;
-        float4 mat = w.cur.mat[i];
-        f3 t1, t2;
-        make_tangents(normal, &t1, &t2);
-        uint32_t pc = r.z & 0xFFu;
-        f3 la[4], lb[4], af[4], as[4];
-        float4 acc[4];
-        float depth[4], target[4];
-        f3 reach_f = s3(0.0f), reach_s = s3(0.0f);
-        float normal_total = 0.0f;
-        for (uint32_t pi = 0; pi < pc; ++pi) {
-            size_t o = (size_t)pi * cap + i;
-            float4 a4 = w.cur.la[o], b4 = w.cur.lb[o];
-            la[pi] = xyz(a4);
-            lb[pi] = xyz(b4);
-            depth[pi] = a4.w;
-            target[pi] = b4.w;
-            acc[pi] = w.cur.acc[o];
-            af[pi] = arm(pf, la[pi]);
-            as[pi] = arm(ps, lb[pi]);
-            reach_f = reach_f + (af[pi] - dbody_com(pf));
-            reach_s = reach_s + (as[pi] - dbody_com(ps));
-        }
-        for (uint32_t pi = 0; pi < pc; ++pi) normal_total = normal_total + wmax(acc[pi].x, 0.0f);
-        float count_f = (float)max(pc, 1u);
-        f3 impulses[4];
-        for (uint32_t pi = 0; pi < pc; ++pi) {
-            float an = acc[pi].x, at1 = acc[pi].y, at2 = acc[pi].z;
-            f3 rel = relative_velocity(pf, ps, af[pi], as[pi]);
-            float normal_speed = dot(rel, normal);
-            f3 arm_f = cross(af[pi] - dbody_com(sf), normal);
-            f3 arm_s = cross(as[pi] - dbody_com(ss), normal);
-            float normal_mass = count_f * (sf.inverse_mass + ss.inverse_mass) + dot(dbody_iinv(sf, cross(reach_f, normal)), arm_f)
-                + dot(dbody_iinv(ss, cross(reach_s, normal)), arm_s);
-            float truth = momentum_mass(pf, ps, af[pi], as[pi], normal);
-            float delta;
-            if (mat.z <= 0.0f) {
-                delta = (target[pi] - normal_speed) / normal_mass;
-            } else {
-                float bias = wmax(depth[pi] / p.dt, target[pi]);
-                float drag = 2.0f * mat.w * mat.z / p.dt;
-                float softness = mat.z * mat.z * truth / (p.dt * p.dt);
-                float prior = normal_speed - an * truth;
-                float wanted = (bias - (1.0f + drag) * prior) / (softness + (1.0f + drag) * truth);
-                delta = truth * (wanted - an) / normal_mass;
-            }
-            float next_n = wmax(0.0f, an + delta);
-            impulses[pi] = s3(0.0f) + normal * (next_n - an);
-            an = next_n;
-            float limit = friction * an;
-            float t1_mass = momentum_mass(sf, ss, af[pi], as[pi], t1) * count_f;
-            float t1_speed = dot(relative_velocity(pf, ps, af[pi], as[pi]), t1);
-            float next_t1 = wclamp(at1 - t1_speed / t1_mass, -limit, limit);
-            impulses[pi] = impulses[pi] + t1 * (next_t1 - at1);
-            at1 = next_t1;
-            float t2_mass = momentum_mass(sf, ss, af[pi], as[pi], t2) * count_f;
-            float t2_speed = dot(relative_velocity(pf, ps, af[pi], as[pi]), t2);
-            float remaining = sqrtf(wmax(limit * limit - at1 * at1, 0.0f));
-            float next_t2 = wclamp(at2 - t2_speed / t2_mass, -remaining, remaining);
-            impulses[pi] = impulses[pi] + t2 * (next_t2 - at2);
-            at2 = next_t2;
-            acc[pi] = make_float4(an, at1, at2, acc[pi].w);
-        }
-        for (uint32_t pi = 0; pi < pc; ++pi) pair_impulse(&first, &second, af[pi], as[pi], impulses[pi]);
-        f3 rel_spin = second.angular_velocity - first.angular_velocity;
-        f3 planar = rel_spin - normal * dot(rel_spin, normal);
-        float planar_len = length(planar);
-        if (planar_len > 1e-6f) {
-            f3 axis = planar / planar_len;
-            float mass = dot(axis, dbody_iinv(sf, axis)) + dot(axis, dbody_iinv(ss, axis));
-            if (mass > 0.0f) {
-                float limit = mat.x * normal_total;
-                float applied = wclamp(-planar_len / mass, -limit, limit);
-                first.angular_velocity = first.angular_velocity - dbody_iinv(first, axis * applied);
-                second.angular_velocity = second.angular_velocity + dbody_iinv(second, axis * applied);
-            }
-        }
-        float twist = dot(rel_spin, normal);
-        if (fabsf(twist) > 1e-6f) {
-            float mass = dot(normal, dbody_iinv(sf, normal)) + dot(normal, dbody_iinv(ss, normal));
-            if (mass > 0.0f) {
-                float limit = mat.y * normal_total;
-                float applied = wclamp(-twist / mass, -limit, limit);
-                first.angular_velocity = first.angular_velocity - dbody_iinv(first, normal * applied);
-                second.angular_velocity = second.angular_velocity + dbody_iinv(second, normal * applied);
-            }
-        }
-        for (uint32_t pi = 0; pi < pc; ++pi) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
-        f3 da = first.velocity - pf.velocity, sa = first.angular_velocity - pf.angular_velocity;
-        f3 db = second.velocity - ps.velocity, sb = second.angular_velocity - ps.angular_velocity;
-        if (!dbody_inert(pf)) accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
-        if (!dbody_inert(ps)) accumulate(w.vdelta, r.y, db, sb, DYN_SOLVER_VELOCITY_SCALE);
-        if (residual) {
-            max_counter(&w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL],
-                        (uint32_t)solver_word(wmax(length(da), length(db)), DYN_SOLVER_VELOCITY_SCALE));
-            max_counter(&w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL],
-                        (uint32_t)solver_word(wmax(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE));
+        float next_n = wmax(0.0f, an + delta);
+        impulses[pi] = s3(0.0f) + normal * (next_n - an);
+        an = next_n;
+        float limit = friction * an;
+        float t1_speed = dot(rel, t1);
+        float next_t1 = wclamp(at1 - t1_speed / m2.x, -limit, limit);
+        impulses[pi] = impulses[pi] + t1 * (next_t1 - at1);
+        at1 = next_t1;
+        float t2_speed = dot(rel, t2);
+        float remaining = sqrtf(wmax(limit * limit - at1 * at1, 0.0f));
+        float next_t2 = wclamp(at2 - t2_speed / m2.y, -remaining, remaining);
+        impulses[pi] = impulses[pi] + t2 * (next_t2 - at2);
+        at2 = next_t2;
+        acc[pi] = make_float4(an, at1, at2, acc[pi].w);
+    }
+    for (uint32_t pi = 0; pi < pc; ++pi) pair_impulse_arms(&first, &second, ra[pi], rb[pi], impulses[pi]);
+    f3 rel_spin = second.angular_velocity - first.angular_velocity;
+    f3 planar = rel_spin - normal * dot(rel_spin, normal);
+    float planar_len = length(planar);
+    if (planar_len > 1e-6f) {
+        f3 axis = planar / planar_len;
+        float mass = dot(axis, dbody_iinv(b.sf, axis)) + dot(axis, dbody_iinv(b.ss, axis));
+        if (mass > 0.0f) {
+            float limit = mat.x * normal_total;
+            float applied = wclamp(-planar_len / mass, -limit, limit);
+            first.angular_velocity = first.angular_velocity - dbody_iinv(first, axis * applied);
+            second.angular_velocity = second.angular_velocity + dbody_iinv(second, axis * applied);
         }
     }
+    float twist = dot(rel_spin, normal);
+    if (fabsf(twist) > 1e-6f) {
+        if (twist_mass > 0.0f) {
+            float limit = mat.y * normal_total;
+            float applied = wclamp(-twist / twist_mass, -limit, limit);
+            first.angular_velocity = first.angular_velocity - dbody_iinv(first, normal * applied);
+            second.angular_velocity = second.angular_velocity + dbody_iinv(second, normal * applied);
+        }
+    }
+    for (uint32_t pi = 0; pi < pc; ++pi) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
+    f3 da = first.velocity - pf.velocity, sa = first.angular_velocity - pf.angular_velocity;
+    f3 db = second.velocity - ps.velocity, sb = second.angular_velocity - ps.angular_velocity;
+    if (!dbody_inert(pf)) accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
+    if (!dbody_inert(ps)) accumulate(w.vdelta, r.y, db, sb, DYN_SOLVER_VELOCITY_SCALE);
+    if (residual) {
+        max_counter(&w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL],
+                    (uint32_t)solver_word(wmax(length(da), length(db)), DYN_SOLVER_VELOCITY_SCALE));
+        max_counter(&w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL],
+                    (uint32_t)solver_word(wmax(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE));
+    }
+}
+__global__ void __launch_bounds__(128) k_solve(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const bool residual = w.ctl[CTL_ROUNDS] == p.solve_iterations;
+    GRID_STRIDE(i, count) solve_block(w, p, i, residual);
 }
 
 // solver_block_apply.wgsl:7-29
+__device__ __forceinline__ void apply_velocity_row(const DeviceWorld& w, uint32_t i) {
+    uint32_t row = w.solver_rows[i];
+    int4* d = reinterpret_cast<int4*>(w.vdelta + 8u * row);
+    int4 a = d[0], b = d[1];
+    d[0] = make_int4(0, 0, 0, 0);
+    d[1] = make_int4(0, 0, 0, 0);
+    f3 lin = mk3((float)a.x / DYN_SOLVER_VELOCITY_SCALE, (float)a.y / DYN_SOLVER_VELOCITY_SCALE,
+                 (float)a.z / DYN_SOLVER_VELOCITY_SCALE);
+    f3 ang = mk3((float)a.w / DYN_SOLVER_VELOCITY_SCALE, (float)b.x / DYN_SOLVER_VELOCITY_SCALE,
+                 (float)b.y / DYN_SOLVER_VELOCITY_SCALE);
+    if (is_zero3(lin) && is_zero3(ang)) return;
+    BodyHot& h = w.hot[row];
+    float4 v = h.vel, av = h.ang;
+    h.vel = make_float4(v.x + lin.x, v.y + lin.y, v.z + lin.z, v.w);
+    h.ang = make_float4(av.x + ang.x, av.y + ang.y, av.z + ang.z, av.w);
+}
 __global__ void k_vapply(DeviceWorld w) {
     const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
     if (blockIdx.x == 0 && threadIdx.x == 0 && rows > 0u) w.ctl[CTL_ROUNDS] += 1u;
-    GRID_STRIDE(i, rows) {
-        uint32_t row = w.solver_rows[i];
-        int4* d = reinterpret_cast<int4*>(w.vdelta + 8u * row);
-        int4 a = d[0], b = d[1];
-        d[0] = make_int4(0, 0, 0, 0);
-        d[1] = make_int4(0, 0, 0, 0);
-        f3 lin = mk3((float)a.x / DYN_SOLVER_VELOCITY_SCALE, (float)a.y / DYN_SOLVER_VELOCITY_SCALE,
-                     (float)a.z / DYN_SOLVER_VELOCITY_SCALE);
-        f3 ang = mk3((float)a.w / DYN_SOLVER_VELOCITY_SCALE, (float)b.x / DYN_SOLVER_VELOCITY_SCALE,
-                     (float)b.y / DYN_SOLVER_VELOCITY_SCALE);
-        if (is_zero3(lin) && is_zero3(ang)) continue;
-        BodyHot& h = w.hot[row];
-        float4 v = h.vel, av = h.ang;
-        h.vel = make_float4(v.x + lin.x, v.y + lin.y, v.z + lin.z, v.w);
-        h.ang = make_float4(av.x + ang.x, av.y + ang.y, av.z + ang.z, av.w);
-    }
+    GRID_STRIDE(i, rows) apply_velocity_row(w, i);
 }
 
 // substep_integrate.wgsl:15-76 (no force fields)
@@ -1381,81 +1451,83 @@ __global__ void k_advance(DeviceWorld w, dyn_step_params p) {
 }
 
 // position_correction.wgsl:5-46 with position_block.wgsl:11-33
+__device__ __forceinline__ void position_block(const DeviceWorld& w, const dyn_step_params& p, uint32_t i) {
+    const uint32_t cap = w.c_cap;
+    uint4 r = w.cur.rows[i];
+    if (!resolves(r)) return;
+    float4 mat = w.cur.mat[i];
+    if (mat.z > 0.0f) return;
+    const BodyHot& ha = w.hot[r.x];
+    const BodyHot& hb = w.hot[r.y];
+    float ima = (!simulates(ha.pos.w, ha.aux.y) || ha.aux.x != 0u) ? 0.0f : ha.pos.w;
+    float imb = (!simulates(hb.pos.w, hb.aux.y) || hb.aux.x != 0u) ? 0.0f : hb.pos.w;
+    f3 normal = xyz(w.cur.normal[i]);
+    float resolved = dot(normal, xyz(w.resolution[r.y]) - xyz(w.resolution[r.x]));
+    f3 total = s3(0.0f);
+    uint32_t contributing = 0;
+    uint32_t pc = r.z & 0xFFu;
+    for (uint32_t pi = 0; pi < pc; ++pi) {
+        float error = wmax(w.cur.la[(size_t)pi * cap + i].w - p.slop - resolved, 0.0f);
+        if (error <= 0.0f) continue;
+        float k = ima + imb;
+        if (k == 0.0f) continue;
+        total = total + normal * (p.relaxation * error / k);
+        contributing += 1;
+    }
+    if (contributing == 0u) return;
+    f3 correction = total / (float)contributing;
+    f3 la = -correction * ima;
+    f3 lb = correction * imb;
+    if (!(dot(la, la) > 0.0f || dot(lb, lb) > 0.0f)) return;
+    // Both rows are marked as contributing (position_apply renormalises a contributed row's
+    // orientation). A moving row needs the exact count, which divides its summed delta; a
+    // frozen row's sum is zero, so only "contributed" matters there: every writer stores the
+    // same 1, without an atomic on the shared row of a static body.
+    if (ima > 0.0f) {
+        atomicAdd(&w.contributions[r.x], 1u);
+        accumulate(w.pdelta, r.x, la, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+    } else if (w.contributions[r.x] == 0u) {
+        w.contributions[r.x] = 1u;
+    }
+    if (imb > 0.0f) {
+        atomicAdd(&w.contributions[r.y], 1u);
+        accumulate(w.pdelta, r.y, lb, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+    } else if (w.contributions[r.y] == 0u) {
+        w.contributions[r.y] = 1u;
+    }
+}
 __global__ void k_position(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
-    const uint32_t cap = w.c_cap;
-    GRID_STRIDE(i, count) {
-        uint4 r = w.cur.rows[i];
-        if (!resolves(r)) continue;
-        float4 mat = w.cur.mat[i];
-        if (mat.z > 0.0f) continue;
-        const BodyHot& ha = w.hot[r.x];
-        const BodyHot& hb = w.hot[r.y];
-        float ima = (!simulates(ha.pos.w, ha.aux.y) || ha.aux.x != 0u) ? 0.0f : ha.pos.w;
-        float imb = (!simulates(hb.pos.w, hb.aux.y) || hb.aux.x != 0u) ? 0.0f : hb.pos.w;
-        f3 normal = xyz(w.cur.normal[i]);
-        float resolved = dot(normal, xyz(w.resolution[r.y]) - xyz(w.resolution[r.x]));
-        f3 total = s3(0.0f);
-        uint32_t contributing = 0;
-        uint32_t pc = r.z & 0xFFu;
-        for (uint32_t pi = 0; pi < pc; ++pi) {
-            float error = wmax(w.cur.la[(size_t)pi * cap + i].w - p.slop - resolved, 0.0f);
-            if (error <= 0.0f) continue;
-            float k = ima + imb;
-            if (k == 0.0f) continue;
-            total = total + normal * (p.relaxation * error / k);
-            contributing += 1;
-        }
-        if (contributing == 0u) continue;
-        f3 correction = total / (float)contributing;
-        f3 la = -correction * ima;
-        f3 lb = correction * imb;
-        if (!(dot(la, la) > 0.0f || dot(lb, lb) > 0.0f)) continue;
-        // Both rows are marked as contributing (position_apply renormalises a contributed row's
-        // orientation). A moving row needs the exact count, which divides its summed delta; a
-        // frozen row's sum is zero, so only "contributed" matters there: every writer stores the
-        // same 1, without an atomic on the shared row of a static body.
-        if (ima > 0.0f) {
-            atomicAdd(&w.contributions[r.x], 1u);
-            accumulate(w.pdelta, r.x, la, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
-        } else if (w.contributions[r.x] == 0u) {
-            w.contributions[r.x] = 1u;
-        }
-        if (imb > 0.0f) {
-            atomicAdd(&w.contributions[r.y], 1u);
-            accumulate(w.pdelta, r.y, lb, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
-        } else if (w.contributions[r.y] == 0u) {
-            w.contributions[r.y] = 1u;
-        }
-    }
+    GRID_STRIDE(i, count) position_block(w, p, i);
 }
 
 // position_apply.wgsl:12-27
+__device__ __forceinline__ void apply_position_row(const DeviceWorld& w, uint32_t i) {
+    uint32_t row = w.solver_rows[i];
+    uint32_t contributing = w.contributions[row];
+    w.contributions[row] = 0u;
+    int4* d = reinterpret_cast<int4*>(w.pdelta + 8u * row);
+    int4 a = d[0], b = d[1];
+    d[0] = make_int4(0, 0, 0, 0);
+    d[1] = make_int4(0, 0, 0, 0);
+    if (contributing == 0u) return;
+    f3 lin = mk3((float)a.x / DYN_SOLVER_POSITION_SCALE, (float)a.y / DYN_SOLVER_POSITION_SCALE,
+                 (float)a.z / DYN_SOLVER_POSITION_SCALE);
+    f3 ang = mk3((float)a.w / DYN_SOLVER_POSITION_SCALE, (float)b.x / DYN_SOLVER_POSITION_SCALE,
+                 (float)b.y / DYN_SOLVER_POSITION_SCALE);
+    f3 al = lin / (float)contributing;
+    f3 aa = ang / (float)contributing;
+    BodyHot& h = w.hot[row];
+    f3 pos = xyz(h.pos) + al;
+    h.pos = mk4(pos, h.pos.w);
+    f3 ha = aa * 0.5f;
+    h.rot = normalize4(quat_mul(make_float4(ha.x, ha.y, ha.z, 1.0f), h.rot));
+    float4 res = w.resolution[row];
+    w.resolution[row] = make_float4(res.x + al.x, res.y + al.y, res.z + al.z, 0.0f);
+}
 __global__ void k_papply(DeviceWorld w) {
     const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
-    GRID_STRIDE(i, rows) {
-        uint32_t row = w.solver_rows[i];
-        uint32_t contributing = w.contributions[row];
-        w.contributions[row] = 0u;
-        int4* d = reinterpret_cast<int4*>(w.pdelta + 8u * row);
-        int4 a = d[0], b = d[1];
-        d[0] = make_int4(0, 0, 0, 0);
-        d[1] = make_int4(0, 0, 0, 0);
-        if (contributing == 0u) continue;
-        f3 lin = mk3((float)a.x / DYN_SOLVER_POSITION_SCALE, (float)a.y / DYN_SOLVER_POSITION_SCALE,
-                     (float)a.z / DYN_SOLVER_POSITION_SCALE);
-        f3 ang = mk3((float)a.w / DYN_SOLVER_POSITION_SCALE, (float)b.x / DYN_SOLVER_POSITION_SCALE,
-                     (float)b.y / DYN_SOLVER_POSITION_SCALE);
-        f3 al = lin / (float)contributing;
-        f3 aa = ang / (float)contributing;
-        BodyHot& h = w.hot[row];
-        f3 pos = xyz(h.pos) + al;
-        h.pos = mk4(pos, h.pos.w);
-        f3 ha = aa * 0.5f;
-        h.rot = normalize4(quat_mul(make_float4(ha.x, ha.y, ha.z, 1.0f), h.rot));
-        float4 res = w.resolution[row];
-        w.resolution[row] = make_float4(res.x + al.x, res.y + al.y, res.z + al.z, 0.0f);
-    }
+    GRID_STRIDE(i, rows) apply_position_row(w, i);
 }
 
 // island_sleep.wgsl:10-29, then commit (contact_archive + archive_count_sync).

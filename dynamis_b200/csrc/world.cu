@@ -214,6 +214,11 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.hit_list, P);
         A(dw.hit_data, 2 * (size_t)P);
         A(dw.matched, C);
+        A(dw.srows.arm_a, 4 * (size_t)C);
+        A(dw.srows.arm_b, 4 * (size_t)C);
+        A(dw.srows.masses, 4 * (size_t)C);
+        A(dw.srows.tangent1, C);
+        A(dw.srows.tangent2, C);
         A(dw.parents, N);
         A(dw.istate, N);
         A(dw.live, N);
@@ -484,6 +489,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     for (uint32_t sub = 0; sub < p.substeps; ++sub) {
         mark(ST_INTEGRATE);
         k_integrate<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+        k_solve_prepare<<<blocks_for(C, 128), 128, 0, s>>>(dw);
         if (sub == 0) {
             mark(ST_WARM);
             k_warm<<<blocks_for(C, 128), 128, 0, s>>>(dw);
