@@ -92,6 +92,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+# DRAM bytes the narrowphase stage moved per candidate pair, measured with ncu on the formed
+# 32,768-body pile (profiles/narrowphase_traffic_mixed_pile_32768.md); the full-size workload is too
+# large for a multi-metric capture, and the traffic grows with the pair count.
+NARROWPHASE_DRAM_BYTES_PER_PAIR = 328.0
+
+
 def stage_bytes(stage: str, m: dict, params: dict) -> float:
     """Algorithmic (compulsory) HBM bytes of one launch of a stage's kernel pair, from the counts
     of the same step: K colliders, E entries, P pairs, C contacts, R solver rows, L live bodies."""
@@ -230,7 +236,9 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         "e2e": {"value": bodies * e2e_steps * world_size / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bodies * R.BODY_STATE.itemsize,
                 "d2h_bytes_per_step": bodies * R.BODY_STATE.itemsize},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk["source"],
+                     "frac": achieved / pk["hbm_gbs"],
+                     "traffic": NARROWPHASE_DRAM_BYTES_PER_PAIR * counts["P"] if dominant == "narrowphase" else None,
+                     "peak_source": pk["source"],
                      "algorithmic_bytes_per_launch": algo, "ms_per_launch": per_launch_ms},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "gpu_launches": launches_per_step * args.steps,
