@@ -141,6 +141,20 @@ struct DeviceWorld {
     int32_t* pdelta;  // [8n]
     uint32_t* contributions;
     float4* resolution;
+    // constraints (ball joints) and their solve order
+    uint32_t jcount;
+    uint32_t jgroup_count;
+    uint32_t jfilter_count;
+    uint4* jmeta;       // kind, flags, first row, second row
+    float4* janchor_a;  // anchor in the first body's frame, break force
+    float4* janchor_b;  // anchor in the second body's frame, break torque
+    dyn_constraint_runtime_record* jruntime;
+    uint32_t* jrows;    // joints layer by layer
+    uint2* jlayers;     // (first entry of jrows, count)
+    uint2* jcomps;      // (first layer, layer count)
+    uint4* jgroups;     // warp groups: first component, components, lanes each, deepest stack
+    uint2* jfilter;     // sorted (lower row, higher row) of the joints that disable collisions
+    uint32_t* jfilter_joint;
     // counters (reference slots) and control words
     uint32_t* counters;
     uint32_t* ctl;

@@ -390,6 +390,190 @@ std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vect
     return out;
 }
 
+
+// ---- joint solve order (crates/dynamis-world/src/schedule.rs:105-296) ----
+namespace {
+uint32_t plan_find(std::vector<uint32_t>& roots, uint32_t row) {
+    while (roots[row] != row) {
+        roots[row] = roots[roots[row]];
+        row = roots[row];
+    }
+    return row;
+}
+}  // namespace
+
+void plan_joints(const std::vector<uint32_t>& first, const std::vector<uint32_t>& second, uint32_t body_rows,
+                 uint32_t dynamic_count, JointPlan* plan) {
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    const uint32_t joints = (uint32_t)first.size();
+    plan->rows.clear();
+    plan->layers.clear();
+    plan->components.clear();
+    plan->groups.clear();
+    if (joints == 0) return;
+    // components by union of the two ends; a row that does not simulate anchors its component
+    std::vector<uint8_t> anchor(body_rows, 0);
+    std::vector<uint32_t> roots(body_rows);
+    for (uint32_t i = 0; i < body_rows; ++i) roots[i] = i;
+    for (uint32_t j = 0; j < joints; ++j) {
+        uint32_t a = first[j], b = second[j];
+        if (a >= dynamic_count) anchor[a] = 1;
+        if (b >= dynamic_count) anchor[b] = 1;
+        uint32_t ra = plan_find(roots, a), rb = plan_find(roots, b);
+        uint32_t root = std::min(ra, rb);
+        roots[ra] = root;
+        roots[rb] = root;
+    }
+    std::vector<uint32_t> root_of(joints);
+    for (uint32_t j = 0; j < joints; ++j) root_of[j] = plan_find(roots, first[j]);
+    std::vector<uint8_t> anchored(body_rows, 0);
+    std::vector<uint32_t> head_of(body_rows, kNone);
+    for (uint32_t j = 0; j < joints; ++j) {
+        uint32_t r = root_of[j];
+        anchored[r] |= (uint8_t)(anchor[first[j]] | anchor[second[j]]);
+        head_of[r] = std::min(head_of[r], std::min(first[j], second[j]));
+    }
+    std::vector<std::vector<uint32_t>> adjacency(body_rows);
+    for (uint32_t j = 0; j < joints; ++j) {
+        adjacency[first[j]].push_back(second[j]);
+        adjacency[second[j]].push_back(first[j]);
+    }
+    // depth: breadth-first from the anchors, then from the head of each unanchored component
+    std::vector<uint32_t> depth(body_rows, kNone);
+    std::vector<uint32_t> frontier;
+    for (uint32_t b = 0; b < body_rows; ++b) {
+        if (anchor[b]) {
+            depth[b] = 0;
+            frontier.push_back(b);
+        }
+    }
+    for (uint32_t r = 0; r < body_rows; ++r) {
+        if (head_of[r] != kNone && !anchored[r]) {
+            depth[head_of[r]] = 0;
+            frontier.push_back(head_of[r]);
+        }
+    }
+    for (size_t cursor = 0; cursor < frontier.size(); ++cursor) {
+        uint32_t b = frontier[cursor];
+        for (uint32_t nb : adjacency[b]) {
+            if (depth[nb] == kNone) {
+                depth[nb] = depth[b] + 1;
+                frontier.push_back(nb);
+            }
+        }
+    }
+    // joints in order of depth, component, row; each takes the layer after its ends' last layers
+    std::vector<uint32_t> settled(joints);
+    for (uint32_t j = 0; j < joints; ++j) settled[j] = j;
+    auto depth_key = [&](uint32_t j) { return std::max(depth[first[j]], depth[second[j]]); };
+    std::sort(settled.begin(), settled.end(), [&](uint32_t x, uint32_t y) {
+        uint32_t dx = depth_key(x), dy = depth_key(y);
+        if (dx != dy) return dx < dy;
+        if (root_of[x] != root_of[y]) return root_of[x] < root_of[y];
+        return x < y;
+    });
+    std::vector<uint32_t> held_layer(body_rows, 0);
+    struct Held {
+        uint32_t root, layer, row;
+    };
+    std::vector<Held> held;
+    held.reserve(joints);
+    for (uint32_t j : settled) {
+        uint32_t layer = std::max(held_layer[first[j]], held_layer[second[j]]) + 1;
+        held_layer[first[j]] = layer;
+        held_layer[second[j]] = layer;
+        held.push_back(Held{root_of[j], layer, j});
+    }
+    std::sort(held.begin(), held.end(), [](const Held& x, const Held& y) {
+        if (x.root != y.root) return x.root < y.root;
+        if (x.layer != y.layer) return x.layer < y.layer;
+        return x.row < y.row;
+    });
+    struct Comp {
+        uint32_t first_layer, layers, first_row, head, lanes;
+    };
+    std::vector<uint32_t> rows, layers;
+    std::vector<Comp> comps;
+    size_t index = 0;
+    while (index < held.size()) {
+        uint32_t root = held[index].root;
+        Comp c{(uint32_t)(layers.size() / 2), 0, (uint32_t)rows.size(), kNone, 0};
+        uint32_t widest = 0;
+        while (index < held.size() && held[index].root == root) {
+            uint32_t layer = held[index].layer;
+            size_t start = rows.size();
+            while (index < held.size() && held[index].root == root && held[index].layer == layer) {
+                uint32_t j = held[index].row;
+                c.head = std::min(c.head, std::min(first[j], second[j]));
+                rows.push_back(j);
+                ++index;
+            }
+            uint32_t count = (uint32_t)(rows.size() - start);
+            widest = std::max(widest, count);
+            layers.push_back((uint32_t)start);
+            layers.push_back(count);
+            c.layers += 1;
+        }
+        uint32_t lanes = 1;
+        while (lanes < widest) lanes <<= 1;
+        c.lanes = std::min(lanes, 64u);  // JOINT_BATCH_LANES
+        comps.push_back(c);
+    }
+    std::stable_sort(comps.begin(), comps.end(), [](const Comp& x, const Comp& y) {
+        if (x.lanes != y.lanes) return x.lanes > y.lanes;
+        if (x.layers != y.layers) return x.layers > y.layers;
+        return x.head < y.head;
+    });
+    for (const Comp& c : comps) {
+        plan->components.push_back((uint32_t)(plan->layers.size() / 2));
+        plan->components.push_back(c.layers);
+        uint32_t cursor = c.first_row;
+        for (uint32_t l = c.first_layer; l < c.first_layer + c.layers; ++l) {
+            uint32_t count = layers[2 * l + 1];
+            plan->layers.push_back((uint32_t)plan->rows.size());
+            plan->layers.push_back(count);
+            plan->rows.insert(plan->rows.end(), rows.begin() + cursor, rows.begin() + cursor + count);
+            cursor += count;
+        }
+    }
+    // device packing (not the reference's workgroup packing: results do not depend on it, since
+    // components share no body): consecutive components of equal lane width fill 32-lane warps
+    uint32_t c = 0;
+    while (c < (uint32_t)comps.size()) {
+        uint32_t lanes = std::min(comps[c].lanes, 32u);
+        uint32_t span = comps[c].layers;
+        uint32_t taken = 1;
+        while (c + taken < (uint32_t)comps.size() && (taken + 1) * lanes <= 32u && std::min(comps[c + taken].lanes, 32u) == lanes) {
+            span = std::max(span, comps[c + taken].layers);
+            ++taken;
+        }
+        plan->groups.push_back(c);
+        plan->groups.push_back(taken);
+        plan->groups.push_back(lanes);
+        plan->groups.push_back(span);
+        c += taken;
+    }
+}
+
+dyn_status rebuild_joints(dyn_world* w) {
+    rebuild_rows(w);
+    const uint32_t m = (uint32_t)w->joint_descs.size();
+    const uint32_t n = (uint32_t)w->states.size();
+    w->joint_rows.resize(m);
+    std::vector<uint32_t> first(m), second(m);
+    for (uint32_t j = 0; j < m; ++j) {
+        const dyn_constraint_descriptor_record& d = w->joint_descs[j];
+        uint32_t a = d.first_body_id < w->row_of_id.size() ? w->row_of_id[d.first_body_id] : DYN_NO_BODY;
+        uint32_t b = d.second_body_id < w->row_of_id.size() ? w->row_of_id[d.second_body_id] : DYN_NO_BODY;
+        if (a == DYN_NO_BODY || b == DYN_NO_BODY || a >= n || b >= n)
+            return fail(w, DYN_ERR_INVALID, "a joint must join two live bodies");
+        w->joint_rows[j] = dyn_constraint_rows_record{a, b};
+        first[j] = a;
+        second[j] = b;
+    }
+    plan_joints(first, second, n, w->dynamic_count, &w->joint_plan);
+    return DYN_OK;
+}
 }  // namespace dyn
 
 using namespace dyn;
@@ -734,10 +918,108 @@ DYN_API dyn_status dyn_step_params_for(const dyn_world* cw, float dt, dyn_step_p
     out->position_iterations = c.position_iterations;
     out->contact_margin = c.contact_margin;
     out->collider_count = (uint32_t)w->colliders.size();
+    out->constraint_count = (uint32_t)w->joint_descs.size();
     out->soft_iterations = 1;
     out->soft_substeps = 4;
     out->soft_substep_dt = dt / 4.0f;
     out->settle_velocity = 1.0e-4f;
+    return DYN_OK;
+}
+
+// ---- constraints (ball joints) ----
+namespace {
+dyn_status add_constraint_record(dyn_world* w, const dyn_constraint_descriptor_record& r) {
+    const uint32_t supported = DYN_CONSTRAINT_DISABLE_COLLISIONS | DYN_CONSTRAINT_WARM_START | DYN_CONSTRAINT_HAS_BREAK;
+    if (r.kind != DYN_CONSTRAINT_BALL) return fail(w, DYN_ERR_INVALID, "only ball joints are on this path");
+    if (r.flags & ~supported) return fail(w, DYN_ERR_INVALID, "ball joint limits and swing cones are not on this path");
+    uint32_t ids = (uint32_t)std::max(w->spawn_states.size(), w->row_of_id.size());
+    if (r.first_body_id >= ids || r.second_body_id >= ids) return fail(w, DYN_ERR_INVALID, "a joint must join two live bodies");
+    if (r.first_body_id == r.second_body_id) return fail(w, DYN_ERR_INVALID, "a joint must join two different bodies");
+    for (int i = 0; i < 3; ++i) {
+        if (!std::isfinite(r.anchor_a[i]) || !std::isfinite(r.anchor_b[i])) return fail(w, DYN_ERR_INVALID, "joint anchors must be finite");
+    }
+    w->joint_descs.push_back(r);
+    dyn_constraint_runtime_record rt;
+    std::memset(&rt, 0, sizeof(rt));
+    rt.constraint_id = (uint32_t)w->joint_descs.size() - 1u;  // ConstraintRuntimeRecord::fresh
+    w->joint_runtime.push_back(rt);
+    w->joints_dirty = true;
+    return DYN_OK;
+}
+}  // namespace
+
+DYN_API dyn_status dyn_add_ball_joint(dyn_world* w, uint32_t first_body, uint32_t second_body, const float* anchor_a,
+                                      const float* anchor_b, uint32_t* out_id) {
+    if (!w || !anchor_a || !anchor_b) return fail(w, DYN_ERR_INVALID, "dyn_add_ball_joint: null argument");
+    // ConstraintDesc::ball with the defaults of ConstraintDesc::VACANT, packed as
+    // ConstraintDescriptorRecord::build does (crates/dynamis-abi/src/constraint.rs:109-141)
+    dyn_constraint_descriptor_record r;
+    std::memset(&r, 0, sizeof(r));
+    r.kind = DYN_CONSTRAINT_BALL;
+    r.first_body_id = first_body;
+    r.second_body_id = second_body;
+    r.flags = DYN_CONSTRAINT_DISABLE_COLLISIONS | DYN_CONSTRAINT_WARM_START;
+    for (int i = 0; i < 3; ++i) {
+        r.anchor_a[i] = anchor_a[i];
+        r.anchor_b[i] = anchor_b[i];
+    }
+    r.axis_a[1] = 1.0f;
+    r.swing_a = 3.14159265358979323846f;
+    r.swing_b = 3.14159265358979323846f;
+    r.gear_ratio = 1.0f;
+    dyn_status st = add_constraint_record(w, r);
+    if (st) return st;
+    if (out_id) *out_id = (uint32_t)w->joint_descs.size() - 1u;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_add_constraints(dyn_world* w, const dyn_constraint_descriptor_record* records, uint32_t m,
+                                       uint32_t* out_first_id) {
+    if (!w || (m && !records)) return fail(w, DYN_ERR_INVALID, "dyn_add_constraints: null argument");
+    size_t before = w->joint_descs.size();
+    for (uint32_t i = 0; i < m; ++i) {
+        dyn_status st = add_constraint_record(w, records[i]);
+        if (st) {  // all or nothing
+            w->joint_descs.resize(before);
+            w->joint_runtime.resize(before);
+            return st;
+        }
+    }
+    if (out_first_id) *out_first_id = (uint32_t)before;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_constraint_count(const dyn_world* w, uint32_t* count) {
+    if (!w || !count) return DYN_ERR_INVALID;
+    *count = (uint32_t)w->joint_descs.size();
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_joint_plan(const dyn_world* cw, uint32_t* rows, uint32_t* layers, uint32_t* components,
+                                  uint32_t* layer_count, uint32_t* component_count) {
+    if (!cw) return DYN_ERR_INVALID;
+    dyn_world* w = const_cast<dyn_world*>(cw);
+    dyn_status st = rebuild_joints(w);
+    if (st) return st;
+    const JointPlan& p = w->joint_plan;
+    if (rows) std::memcpy(rows, p.rows.data(), p.rows.size() * 4);
+    if (layers) std::memcpy(layers, p.layers.data(), p.layers.size() * 4);
+    if (components) std::memcpy(components, p.components.data(), p.components.size() * 4);
+    if (layer_count) *layer_count = (uint32_t)(p.layers.size() / 2);
+    if (component_count) *component_count = (uint32_t)(p.components.size() / 2);
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_export_constraints(const dyn_world* cw, dyn_constraint_descriptor_record* descs,
+                                          dyn_constraint_rows_record* rows, dyn_constraint_runtime_record* runtime) {
+    if (!cw) return DYN_ERR_INVALID;
+    dyn_world* w = const_cast<dyn_world*>(cw);
+    dyn_status st = rebuild_joints(w);
+    if (st) return st;
+    size_t m = w->joint_descs.size();
+    if (descs) std::memcpy(descs, w->joint_descs.data(), m * sizeof(*descs));
+    if (rows) std::memcpy(rows, w->joint_rows.data(), m * sizeof(*rows));
+    if (runtime) std::memcpy(runtime, w->joint_runtime.data(), m * sizeof(*runtime));
     return DYN_OK;
 }
 

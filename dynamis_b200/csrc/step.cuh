@@ -451,6 +451,30 @@ enum PairClass : uint32_t { PC_ANALYTIC = 0, PC_BOXES = 1, PC_CONVEX = 2, PC_COU
 
 // narrowphase.wgsl:518-550 (filters) then the shape dispatch of :551-652, decided once per pair:
 // pairs that fail a filter are answered here; the rest go to one list per kernel class.
+// joined_pairs.wgsl: is there an unbroken joint between these rows that disables their collisions?
+// jfilter is sorted by (lower row, higher row); several joints may join one pair.
+__device__ __forceinline__ bool joined_by_joint(const DeviceWorld& w, uint32_t ra, uint32_t rb) {
+    const uint32_t count = w.jfilter_count;
+    if (count == 0u) return false;
+    const uint32_t a = min(ra, rb), b = max(ra, rb);
+    uint32_t lo = 0, hi = count;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint2 e = w.jfilter[mid];
+        if (e.x < a || (e.x == a && e.y < b)) {
+            lo = mid + 1u;
+        } else {
+            hi = mid;
+        }
+    }
+    for (; lo < count; ++lo) {
+        const uint2 e = w.jfilter[lo];
+        if (e.x != a || e.y != b) break;
+        if (w.jruntime[w.jfilter_joint[lo]].broken == 0u) return true;
+    }
+    return false;
+}
+
 __global__ void k_pair_class(DeviceWorld w) {
     const uint32_t pairs = min(w.counters[DYN_COUNTER_PAIRS], w.p_cap);
     GRID_STRIDE(index, pairs) {
@@ -471,6 +495,7 @@ __global__ void k_pair_class(DeviceWorld w) {
             uint32_t sg = sf.x != DYN_NO_COLLISION_FILTER ? sf.x : si.z;
             uint32_t sm = sf.y != DYN_NO_COLLISION_FILTER ? sf.y : si.w;
             if (!((fg & sm) != 0u && (sg & fm) != 0u)) break;
+            if (joined_by_joint(w, fr, sr)) break;
             bool fw = shape_world_geometry(fk), sw = shape_world_geometry(sk);
             if (fw && sw) break;
             if (fw || sw) {
@@ -1003,31 +1028,28 @@ __device__ __forceinline__ uint32_t island_find(const DeviceWorld& w, uint32_t n
     }
     return current;
 }
+// island_couple (island_link.wgsl:3-45): a static row carries its wake flag to the other row, and
+// two dynamic rows join one island. Returns false when the bounded union gave up.
+__device__ __forceinline__ bool island_couple(const DeviceWorld& w, uint32_t first, uint32_t second) {
+    uint32_t dc = w.nd;
+    if (second >= dc && w.wake_flags[second] != 0u) atomicOr(&w.wake_flags[first], 1u);
+    if (first >= dc && w.wake_flags[first] != 0u) atomicOr(&w.wake_flags[second], 1u);
+    if (first >= dc || second >= dc || first == second) return true;
+    for (uint32_t attempt = 0; attempt < 256u; ++attempt) {
+        uint32_t a = island_find(w, first), b = island_find(w, second);
+        if (a == b) return true;
+        uint32_t lower = min(a, b), higher = max(a, b);
+        if (atomicCAS(&w.parents[higher], higher, lower) == higher) return true;
+    }
+    return false;
+}
 __global__ void k_island_link(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     GRID_STRIDE(i, count) {
         uint4 r = w.cur.rows[i];
         uint32_t pc = r.z & 0xFFu, sensor = (r.z >> 8) & 0xFFu;
         if (pc == 0u || sensor == 1u || !touches(w.cur, i, w.c_cap, p.slop)) continue;
-        uint32_t first = r.x, second = r.y;
-        uint32_t dc = w.nd;
-        if (second >= dc && w.wake_flags[second] != 0u) atomicOr(&w.wake_flags[first], 1u);
-        if (first >= dc && w.wake_flags[first] != 0u) atomicOr(&w.wake_flags[second], 1u);
-        if (first >= dc || second >= dc || first == second) continue;
-        bool joined = false;
-        for (uint32_t attempt = 0; attempt < 256u; ++attempt) {
-            uint32_t a = island_find(w, first), b = island_find(w, second);
-            if (a == b) {
-                joined = true;
-                break;
-            }
-            uint32_t lower = min(a, b), higher = max(a, b);
-            if (atomicCAS(&w.parents[higher], higher, lower) == higher) {
-                joined = true;
-                break;
-            }
-        }
-        if (!joined) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
+        if (!island_couple(w, r.x, r.y)) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
     }
 }
 // island_flatten.wgsl:4-8 repeated ilog2(max(N,2))+1 times leaves every row pointing at its root

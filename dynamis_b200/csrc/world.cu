@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "joints.cuh"
 #include "step.cuh"
 #include "world.h"
 
@@ -61,6 +62,7 @@ struct DeviceState {
     uint32_t* sort_alt2 = nullptr;
     uint32_t sort_alt_cap = 0;
     dyn_body_state_record* staging = nullptr;  // n_cap ABI state records
+    std::vector<void*> joint_allocs;  // constraint buffers, rebuilt whenever the constraint set changes
     // graphs
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     float graph_dt = -1.0f;
@@ -249,6 +251,95 @@ dyn_status ensure_device(dyn_world* w) {
 }
 
 // Converts the host rows to the device layout and uploads them.
+// The device's constraint runtime (accumulated impulses, reactions, broken flags) back into the
+// host copy, so that re-uploading the scene or the constraint set keeps what the steps built.
+dyn_status save_joint_runtime(dyn_world* w) {
+    DeviceState* d = w->dev;
+    if (!d || !d->stepped || d->dw.jcount == 0) return DYN_OK;
+    uint32_t m = std::min<uint32_t>(d->dw.jcount, (uint32_t)w->joint_runtime.size());
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    DYN_CUDA(cudaMemcpy(w->joint_runtime.data(), d->dw.jruntime, (size_t)m * sizeof(dyn_constraint_runtime_record),
+                        cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+// Constraint descriptors, runtime, solve order and collision filter onto the device.
+dyn_status upload_joints(dyn_world* w) {
+    dyn_status st = rebuild_joints(w);
+    if (st) return st;
+    DeviceState* d = w->dev;
+    DeviceWorld& dw = d->dw;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    for (void* p : d->joint_allocs) cudaFree(p);
+    d->joint_allocs.clear();
+    dw.jcount = dw.jgroup_count = dw.jfilter_count = 0;
+    release_graphs(d);
+    w->joints_dirty = false;
+    const uint32_t m = (uint32_t)w->joint_descs.size();
+    if (m == 0) return DYN_OK;
+    const JointPlan& plan = w->joint_plan;
+    std::vector<uint4> meta(m);
+    std::vector<float4> anchor_a(m), anchor_b(m);
+    struct Filter {
+        uint32_t a, b, joint;
+    };
+    std::vector<Filter> filter;
+    for (uint32_t j = 0; j < m; ++j) {
+        const dyn_constraint_descriptor_record& c = w->joint_descs[j];
+        const dyn_constraint_rows_record& r = w->joint_rows[j];
+        meta[j] = make_uint4(c.kind, c.flags, r.first_row, r.second_row);
+        anchor_a[j] = make_float4(c.anchor_a[0], c.anchor_a[1], c.anchor_a[2], c.break_force);
+        anchor_b[j] = make_float4(c.anchor_b[0], c.anchor_b[1], c.anchor_b[2], c.break_torque);
+        if (c.flags & DYN_CONSTRAINT_DISABLE_COLLISIONS)
+            filter.push_back(Filter{std::min(r.first_row, r.second_row), std::max(r.first_row, r.second_row), j});
+    }
+    std::sort(filter.begin(), filter.end(), [](const Filter& x, const Filter& y) {
+        return x.a != y.a ? x.a < y.a : (x.b != y.b ? x.b < y.b : x.joint < y.joint);
+    });
+    std::vector<uint2> fpairs(filter.size());
+    std::vector<uint32_t> fjoint(filter.size());
+    for (size_t i = 0; i < filter.size(); ++i) {
+        fpairs[i] = make_uint2(filter[i].a, filter[i].b);
+        fjoint[i] = filter[i].joint;
+    }
+    auto grab = [&](void** ptr, size_t bytes) -> dyn_status {
+        DYN_CUDA(cudaMalloc(ptr, std::max<size_t>(bytes, 16)));
+        d->joint_allocs.push_back(*ptr);
+        return DYN_OK;
+    };
+#define JA(field, bytes) if ((st = grab(reinterpret_cast<void**>(&dw.field), (bytes)))) return st
+    JA(jmeta, m * sizeof(uint4));
+    JA(janchor_a, m * sizeof(float4));
+    JA(janchor_b, m * sizeof(float4));
+    JA(jruntime, m * sizeof(dyn_constraint_runtime_record));
+    JA(jrows, plan.rows.size() * 4);
+    JA(jlayers, plan.layers.size() * 4);
+    JA(jcomps, plan.components.size() * 4);
+    JA(jgroups, plan.groups.size() * 4);
+    JA(jfilter, fpairs.size() * sizeof(uint2));
+    JA(jfilter_joint, fjoint.size() * 4);
+#undef JA
+    cudaStream_t s = d->stream;
+    DYN_CUDA(cudaMemcpyAsync(dw.jmeta, meta.data(), m * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.janchor_a, anchor_a.data(), m * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.janchor_b, anchor_b.data(), m * sizeof(float4), cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.jruntime, w->joint_runtime.data(), m * sizeof(dyn_constraint_runtime_record),
+                             cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.jrows, plan.rows.data(), plan.rows.size() * 4, cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.jlayers, plan.layers.data(), plan.layers.size() * 4, cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.jcomps, plan.components.data(), plan.components.size() * 4, cudaMemcpyHostToDevice, s));
+    DYN_CUDA(cudaMemcpyAsync(dw.jgroups, plan.groups.data(), plan.groups.size() * 4, cudaMemcpyHostToDevice, s));
+    if (!fpairs.empty()) {
+        DYN_CUDA(cudaMemcpyAsync(dw.jfilter, fpairs.data(), fpairs.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+        DYN_CUDA(cudaMemcpyAsync(dw.jfilter_joint, fjoint.data(), fjoint.size() * 4, cudaMemcpyHostToDevice, s));
+    }
+    DYN_CUDA(cudaStreamSynchronize(s));
+    dw.jcount = m;
+    dw.jgroup_count = (uint32_t)(plan.groups.size() / 4);
+    dw.jfilter_count = (uint32_t)fpairs.size();
+    return DYN_OK;
+}
+
 dyn_status upload_scene(dyn_world* w) {
     dyn_status st = ensure_device(w);
     if (st) return st;
@@ -335,6 +426,7 @@ dyn_status upload_scene(dyn_world* w) {
     DYN_CUDA(cudaMemsetAsync(dw.ctl, 0, CTL_COUNT * 4, s));
     DYN_CUDA(cudaMemsetAsync(dw.counters, 0, 64 * 4, s));
     DYN_CUDA(cudaStreamSynchronize(s));
+    if ((st = upload_joints(w))) return st;
     d->parity = 0;
     d->stepped = false;
     d->uploaded = true;
@@ -445,8 +537,10 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     Marker mark{d, s, timed};
     const uint32_t N = std::max(dw.n, 1u), K = std::max(dw.k, 1u), ND = std::max(dw.nd, 1u);
     const uint32_t E = dw.e_cap, P = dw.p_cap, C = dw.c_cap;
+    const uint32_t joint_blocks = div_up(dw.jgroup_count, 4u);  // four warp groups per 128-thread block
     mark(ST_BEGIN);
     k_reset<<<1, 64, 0, s>>>(dw);
+    if (dw.jcount) k_joint_count<<<blocks_for(std::max(dw.jfilter_count, 1u), 256), 256, 0, s>>>(dw);
     k_begin<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
     mark(ST_AABB);
     k_aabb<<<blocks_for(K, 128), 128, 0, s>>>(dw, p);
@@ -480,6 +574,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
     mark(ST_ISLANDS);
     k_island_link<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    if (dw.jcount) k_island_link_joints<<<blocks_for(dw.jcount, 256), 256, 0, s>>>(dw);
     k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     k_island_aggregate<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
@@ -492,11 +587,13 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         k_solve_prepare<<<blocks_for(C, 128), 128, 0, s>>>(dw);
         if (sub == 0) {
             mark(ST_WARM);
+            if (joint_blocks) k_joints<JP_WARM><<<joint_blocks, 128, 0, s>>>(dw, p);
             k_warm<<<blocks_for(C, 128), 128, 0, s>>>(dw);
             k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_VELOCITY);
         for (uint32_t it = 0; it < p.solve_iterations; ++it) {
+            if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 128, 0, s>>>(dw, p);
             k_solve<<<blocks_for(C, 128), 128, 0, s>>>(dw, p);
             k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
         }
@@ -504,6 +601,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         k_advance<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
         mark(ST_POSITION);
         for (uint32_t it = 0; it < p.position_iterations; ++it) {
+            if (joint_blocks) k_joints<JP_POSITION><<<joint_blocks, 128, 0, s>>>(dw, p);
             k_position<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
             k_papply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
         }
@@ -516,6 +614,10 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
 dyn_status prepare_step(dyn_world* w, float dt) {
     if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(w, DYN_ERR_INVALID, "a step timestep must be positive");
     bool fresh = !w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows);
+    if (fresh || w->joints_dirty) {
+        dyn_status st = save_joint_runtime(w);
+        if (st) return st;
+    }
     if (fresh && w->dev && w->dev->stepped) {
         // bodies spawned after stepping: keep the simulated states of the existing bodies
         std::vector<dyn_body_state_record> now;
@@ -527,6 +629,9 @@ dyn_status prepare_step(dyn_world* w, float dt) {
     }
     if (fresh) {
         dyn_status st = upload_scene(w);
+        if (st) return st;
+    } else if (w->joints_dirty) {
+        dyn_status st = upload_joints(w);
         if (st) return st;
     }
     if (w->states.empty()) return fail(w, DYN_ERR_INVALID, "the world holds no bodies");
@@ -552,6 +657,7 @@ void destroy_device(dyn_world* w) {
     release_graphs(d);
     for (cudaEvent_t e : d->events) cudaEventDestroy(e);
     for (void* p : d->allocs) cudaFree(p);
+    for (void* p : d->joint_allocs) cudaFree(p);
     for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
         if (p) cudaFree(p);
     }
@@ -707,6 +813,19 @@ DYN_API dyn_status dyn_sync(dyn_world* w) {
     uint32_t status = 0;
     DYN_CUDA(cudaMemcpy(&status, w->dev->dw.ctl + CTL_STATUS, 4, cudaMemcpyDeviceToHost));
     if (status) return fail(w, DYN_ERR_DEVICE_STATUS, "device status word " + std::to_string(status));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_read_constraints(dyn_world* w, dyn_constraint_runtime_record* out, uint32_t m) {
+    if (!w || (m && !out)) return fail(w, DYN_ERR_INVALID, "dyn_read_constraints: null argument");
+    if (m != w->joint_descs.size()) return fail(w, DYN_ERR_INVALID, "dyn_read_constraints: count differs from the constraints");
+    DeviceState* d = w->dev;
+    if (d && d->uploaded && !w->joints_dirty && d->dw.jcount == m && m) {
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        DYN_CUDA(cudaMemcpy(out, d->dw.jruntime, (size_t)m * sizeof(*out), cudaMemcpyDeviceToHost));
+        return DYN_OK;
+    }
+    if (m) std::memcpy(out, w->joint_runtime.data(), (size_t)m * sizeof(*out));
     return DYN_OK;
 }
 

@@ -17,6 +17,19 @@ struct HullSource {
     float unit_second_moment[6] = {0, 0, 0, 0, 0, 0};
 };
 
+// The joint solve order of schedule.rs:105-296 over body rows: `rows` lists joint indices layer by
+// layer, `layers` holds (first entry of `rows`, count) pairs, `components` holds (first layer,
+// layer count) pairs in the planner's component order, and `groups` packs components into 32-lane
+// warps for the device: (first component, component count, lanes per component, deepest stack).
+struct JointPlan {
+    std::vector<uint32_t> rows;
+    std::vector<uint32_t> layers;
+    std::vector<uint32_t> components;
+    std::vector<uint32_t> groups;
+};
+void plan_joints(const std::vector<uint32_t>& first, const std::vector<uint32_t>& second, uint32_t body_rows,
+                 uint32_t dynamic_count, JointPlan* plan);
+
 struct DeviceState;  // defined in world.cu
 
 }  // namespace dyn
@@ -42,6 +55,12 @@ struct dyn_world {
     std::vector<uint32_t> owners;
     std::vector<uint32_t> row_of_id;
     uint32_t dynamic_count = 0;
+    // constraints in creation order (constraint id = index); rows and plan derived with the rows
+    std::vector<dyn_constraint_descriptor_record> joint_descs;
+    std::vector<dyn_constraint_runtime_record> joint_runtime;  // initial runtime records
+    std::vector<dyn_constraint_rows_record> joint_rows;
+    dyn::JointPlan joint_plan;
+    bool joints_dirty = false;  // the device's joint buffers and plan are out of date
     bool timing = false;
     void* user_stream = nullptr;  // caller's cudaStream_t (dyn_world_set_stream)
     dyn::DeviceState* dev = nullptr;
@@ -50,6 +69,7 @@ struct dyn_world {
 namespace dyn {
 dyn_status fail(dyn_world* w, dyn_status status, const std::string& what);
 void rebuild_rows(dyn_world* w);
+dyn_status rebuild_joints(dyn_world* w);
 std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vector<float>* vertices_xyzw);
 void destroy_device(dyn_world* w);
 }  // namespace dyn

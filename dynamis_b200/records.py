@@ -100,6 +100,24 @@ CONTACT = _dtype([
     ("relaxation", "<f4", 80), ("damping_ratio", "<f4", 84), ("points", (MANIFOLD_POINT, 4), 96),
 ], 352)
 
+# records.wgsl:355-416 (the fields this path uses; the rest of the 400 bytes are kept as raw padding)
+CONSTRAINT_DESCRIPTOR = _dtype(_fields([
+    ("kind", "<u4", 1, 0), ("first_body_id", "<u4", 1, 4), ("second_body_id", "<u4", 1, 8), ("flags", "<u4", 1, 12),
+    ("anchor_a", "<f4", 3, 16), ("anchor_b", "<f4", 3, 32), ("axis_a", "<f4", 3, 48), ("axis_b", "<f4", 3, 64),
+    ("distance", "<f4", 1, 80), ("limit_min", "<f4", 1, 84), ("limit_max", "<f4", 1, 88), ("swing_a", "<f4", 1, 92),
+    ("swing_b", "<f4", 1, 96), ("break_force", "<f4", 1, 116), ("break_torque", "<f4", 1, 120),
+    ("gear_ratio", "<f4", 1, 124),
+]), 400)
+CONSTRAINT_ROWS = _dtype(_fields([("first_row", "<u4", 1, 0), ("second_row", "<u4", 1, 4)]), 8)
+# records.wgsl:418-426 with ConstraintReaction :445-454
+CONSTRAINT_RUNTIME = _dtype(_fields([
+    ("linear_first", "<f4", 3, 0), ("angular_first", "<f4", 3, 16), ("linear_second", "<f4", 3, 32),
+    ("angular_second", "<f4", 3, 48), ("reference", "<f4", 4, 64), ("accumulated", "<f4", 16, 80),
+    ("broken", "<u4", 1, 144), ("constraint_id", "<u4", 1, 148), ("generation", "<u4", 1, 152),
+]), 160)
+CONSTRAINT_BALL = 0
+CONSTRAINT_DISABLE_COLLISIONS, CONSTRAINT_HAS_BREAK, CONSTRAINT_WARM_START = 1, 32, 64
+
 # C ABI descriptors (include/dynamis_cuda.h)
 CONFIG = np.dtype([
     ("gravity", "<f4", 3), ("damping", "<f4"), ("angular_damping", "<f4"), ("substeps", "<u4"),
@@ -127,6 +145,7 @@ BODY_DESC = np.dtype([
 assert STEP_PARAMS.itemsize == 176 and BODY_STATE.itemsize == 144 and BODY_DESCRIPTOR.itemsize == 128
 assert COLLIDER.itemsize == 112 and SHAPE_SOURCE.itemsize == 80 and CONTACT.itemsize == 352
 assert MANIFOLD_POINT.itemsize == 64 and AABB.itemsize == 32
+assert CONSTRAINT_DESCRIPTOR.itemsize == 400 and CONSTRAINT_ROWS.itemsize == 8 and CONSTRAINT_RUNTIME.itemsize == 160
 
 
 def collider_defaults(n: int) -> np.ndarray:

@@ -13,12 +13,17 @@ import numpy as np
 from . import records as R
 
 
+# a ball joint between two bodies of a scene (indices into Scene.bodies), anchors in body frames
+JOINT = np.dtype([("first", "<u4"), ("second", "<u4"), ("anchor_a", "<f4", 3), ("anchor_b", "<f4", 3)])
+
+
 @dataclass
 class Scene:
     bodies: np.ndarray                      # BODY_DESC
     colliders: np.ndarray                   # COLLIDER_DESC; hull colliders index `hulls`
     hulls: list = field(default_factory=list)  # float32 (m, 3) point sets
     name: str = "scene"
+    joints: np.ndarray | None = None        # JOINT rows: ball joints added after the bodies
 
     @property
     def body_count(self) -> int:
@@ -31,7 +36,11 @@ class Scene:
             sources = np.array([world.add_hull(points) for points in self.hulls], np.uint32)
             is_hull = colliders["shape"] == R.SHAPE_HULL
             colliders["source"][is_hull] = sources[colliders["source"][is_hull]]
-        return world.spawn(self.bodies, colliders)
+        ids = world.spawn(self.bodies, colliders)
+        if self.joints is not None:
+            for jt in self.joints:
+                world.add_ball_joint(int(ids[jt["first"]]), int(ids[jt["second"]]), jt["anchor_a"], jt["anchor_b"])
+        return ids
 
 
 def yaw_quaternions(angles: np.ndarray) -> np.ndarray:
@@ -203,8 +212,52 @@ def random_mix(count: int, seed: int = 7, extent: float = 4.0, with_ground: bool
     return Scene(bodies, colliders, hulls, f"random_mix_{count}")
 
 
+def hanging_chains(chains_x: int = 64, chains_z: int = 64, links: int = 32, seed: int = 2, spacing: float = 1.5,
+                   ground: float = -10.0, spin: float = 0.5) -> Scene:
+    """chains_x x chains_z chains of `links` boxes (half-extents 0.1 x 0.25 x 0.1 m, density 1000)
+    joined end to end by ball joints (anchors at +-0.25 m on y), each hanging from a static anchor
+    body on a grid at `spacing` metres and y = 0; every box starts with an angular velocity drawn
+    from N(0, spin) rad/s per axis, and the chains swing into each other and onto a ground plane at
+    y = `ground`. 64 x 64 x 32 gives 131,072 boxes and 131,072 joints."""
+    rng = np.random.default_rng(seed)
+    chains = chains_x * chains_z
+    n = chains * links
+    ci, ck = np.meshgrid(np.arange(chains_x), np.arange(chains_z), indexing="ij")
+    top = np.stack([(ci.ravel() - (chains_x - 1) / 2) * spacing, np.zeros(chains),
+                    (ck.ravel() - (chains_z - 1) / 2) * spacing], axis=1)
+    link = np.arange(links)
+    pos = top[:, None, :] + np.stack([np.zeros(links), -0.25 - 0.5 * link, np.zeros(links)], axis=1)[None, :, :]
+    bodies = R.body_defaults(n)
+    bodies["position"] = pos.reshape(n, 3).astype(np.float32)
+    bodies["angular_velocity"] = rng.normal(0.0, spin, size=(n, 3)).astype(np.float32)
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(n)
+    colliders["shape"] = R.SHAPE_CUBOID
+    colliders["half_extents"] = (0.1, 0.25, 0.1)
+    colliders["friction"] = 0.5
+    anchors = R.body_defaults(chains)
+    anchors["position"] = top.astype(np.float32)
+    anchors["mass"] = 0.0
+    anchors["collider_first"] = n + np.arange(chains)
+    anchor_colliders = R.collider_defaults(chains)
+    anchor_colliders["radius"] = 0.05
+    bodies = np.concatenate([bodies, anchors])
+    colliders = np.concatenate([colliders, anchor_colliders])
+    joints = np.zeros(n, JOINT)
+    chain = np.repeat(np.arange(chains), links)
+    k = np.tile(link, chains)
+    joints["first"] = np.where(k == 0, n + chain, np.arange(n) - 1)
+    joints["second"] = np.arange(n)
+    joints["anchor_a"] = np.where((k == 0)[:, None], np.zeros(3), np.array([0.0, -0.25, 0.0]))
+    joints["anchor_b"] = (0.0, 0.25, 0.0)
+    bodies, colliders = _ground(bodies, colliders, ground, 0.5, 0.0)
+    return Scene(bodies, colliders, [], f"hanging_chains_{n}", joints)
+
+
 WORKLOADS = {
     "falling_boxes_1000": lambda: falling_boxes(seed=0),
     "mixed_pile_32768": lambda: mixed_pile(side=32, seed=1),
     "mixed_pile_262144": lambda: mixed_pile(side=64, seed=1),
+    "hanging_chains_8192": lambda: hanging_chains(16, 16, 32),
+    "hanging_chains_131072": lambda: hanging_chains(64, 64, 32),
 }

@@ -105,8 +105,52 @@ class World:
         vertices = np.zeros((max(s["vertices"], 0), 4), np.float32)
         self._check(lib.dyn_export_scene(self._h, ptr(states), ptr(descs), ptr(colliders), ptr(owners), ptr(sources),
                                          ptr(vertices)))
-        return {"states": states, "descs": descs, "colliders": colliders, "owners": owners, "sources": sources,
-                "vertices": vertices, "dynamic": s["dynamic"]}
+        scene = {"states": states, "descs": descs, "colliders": colliders, "owners": owners, "sources": sources,
+                 "vertices": vertices, "dynamic": s["dynamic"]}
+        m = self.constraint_count()
+        if m:
+            jd, jr, jt = np.zeros(m, R.CONSTRAINT_DESCRIPTOR), np.zeros(m, R.CONSTRAINT_ROWS), np.zeros(m, R.CONSTRAINT_RUNTIME)
+            self._check(lib.dyn_export_constraints(self._h, ptr(jd), ptr(jr), ptr(jt)))
+            scene.update(constraint_descs=jd, constraint_rows=jr, constraint_runtime=jt)
+        return scene
+
+    # ---- constraints ----
+    def add_ball_joint(self, first_body: int, second_body: int, anchor_a, anchor_b) -> int:
+        """World::add_constraint(first, second, ConstraintDesc::ball(anchor_a, anchor_b)); returns the id."""
+        a = np.ascontiguousarray(anchor_a, np.float32)
+        b = np.ascontiguousarray(anchor_b, np.float32)
+        out = ctypes.c_uint32()
+        self._check(lib.dyn_add_ball_joint(self._h, int(first_body), int(second_body), ptr(a), ptr(b), ctypes.byref(out)))
+        return out.value
+
+    def add_constraints(self, records: np.ndarray) -> int:
+        """Appends ConstraintDescriptorRecords; returns the id of the first."""
+        records = np.ascontiguousarray(records, R.CONSTRAINT_DESCRIPTOR)
+        out = ctypes.c_uint32()
+        self._check(lib.dyn_add_constraints(self._h, ptr(records), len(records), ctypes.byref(out)))
+        return out.value
+
+    def constraint_count(self) -> int:
+        out = ctypes.c_uint32()
+        self._check(lib.dyn_constraint_count(self._h, ctypes.byref(out)))
+        return out.value
+
+    def read_constraints(self) -> np.ndarray:
+        """ConstraintRuntimeRecords after the last step (accumulated impulses, reactions, broken)."""
+        m = self.constraint_count()
+        out = np.zeros(m, R.CONSTRAINT_RUNTIME)
+        self._check(lib.dyn_read_constraints(self._h, ptr(out), m))
+        return out
+
+    def joint_plan(self) -> dict:
+        """The joint solve order: rows, (first, count) layers and (first layer, count) components."""
+        nl, nc = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(lib.dyn_joint_plan(self._h, None, None, None, ctypes.byref(nl), ctypes.byref(nc)))
+        rows = np.zeros(self.constraint_count(), np.uint32)
+        layers = np.zeros((nl.value, 2), np.uint32)
+        comps = np.zeros((nc.value, 2), np.uint32)
+        self._check(lib.dyn_joint_plan(self._h, ptr(rows), ptr(layers), ptr(comps), None, None))
+        return {"rows": rows, "layers": layers, "components": comps}
 
     def step_params(self, dt: float) -> np.ndarray:
         p = np.zeros(1, R.STEP_PARAMS)

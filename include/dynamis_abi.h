@@ -66,8 +66,24 @@ extern "C" {
 #define DYN_LEVEL_KEY_SHIFT 27u
 #define DYN_CELL_HASH_MASK 0x07FFFFFFu
 #define DYN_GRID_LEVEL_LIMIT 30u
+/* constraint kinds and flags: crates/dynamis-abi/src/constant.rs:88-103 */
 #define DYN_CONSTRAINT_BALL 0u
+#define DYN_CONSTRAINT_DISTANCE 1u
+#define DYN_CONSTRAINT_REVOLUTE 2u
+#define DYN_CONSTRAINT_PRISMATIC 3u
+#define DYN_CONSTRAINT_FIXED 4u
+#define DYN_CONSTRAINT_GEAR 5u
+#define DYN_CONSTRAINT_PULLEY 6u
+#define DYN_CONSTRAINT_CONE 7u
+#define DYN_CONSTRAINT_SIXDOF 8u
 #define DYN_CONSTRAINT_DISABLE_COLLISIONS 1u
+#define DYN_CONSTRAINT_HAS_LIMIT 2u
+#define DYN_CONSTRAINT_HAS_MOTOR 4u
+#define DYN_CONSTRAINT_IS_SPRING 8u
+#define DYN_CONSTRAINT_HAS_SWING 16u
+#define DYN_CONSTRAINT_HAS_BREAK 32u
+#define DYN_CONSTRAINT_WARM_START 64u
+#define DYN_CONSTRAINT_ACCUMULATOR_SLOTS 16u
 #define DYN_NO_BODY 0xFFFFFFFFu
 #define DYN_NO_SLOT 0xFFFFFFFFu
 #define DYN_NO_SURFACE 0xFFFFFFFFu
@@ -376,6 +392,29 @@ typedef struct dyn_constraint_rows_record {
     uint32_t second_row;
 } dyn_constraint_rows_record;
 
+/* records.wgsl:445-454 (64 bytes) */
+typedef struct dyn_constraint_reaction_record {
+    float linear_first[3];
+    float _pad_linear_first;
+    float angular_first[3];
+    float _pad_angular_first;
+    float linear_second[3];
+    float _pad_linear_second;
+    float angular_second[3];
+    float _pad_angular_second;
+} dyn_constraint_reaction_record;
+
+/* records.wgsl:418-426 (160 bytes) */
+typedef struct dyn_constraint_runtime_record {
+    dyn_constraint_reaction_record reaction;
+    float reference[4];
+    float accumulated[DYN_CONSTRAINT_ACCUMULATOR_SLOTS];
+    uint32_t broken;
+    uint32_t constraint_id;
+    uint32_t generation;
+    uint32_t _pad0;
+} dyn_constraint_runtime_record;
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
@@ -420,5 +459,11 @@ DYN_ABI_ASSERT(offsetof(dyn_contact_record, damping_ratio) == 84, "Contact.dampi
 DYN_ABI_ASSERT(offsetof(dyn_contact_record, points) == 96, "Contact.points @96");
 DYN_ABI_ASSERT(sizeof(dyn_constraint_descriptor_record) == 400, "ConstraintDescriptor is 400 bytes");
 DYN_ABI_ASSERT(sizeof(dyn_constraint_rows_record) == 8, "ConstraintRows is 8 bytes");
+DYN_ABI_ASSERT(sizeof(dyn_constraint_reaction_record) == 64, "ConstraintReaction is 64 bytes");
+DYN_ABI_ASSERT(sizeof(dyn_constraint_runtime_record) == 160, "ConstraintRuntime is 160 bytes");
+DYN_ABI_ASSERT(offsetof(dyn_constraint_runtime_record, accumulated) == 80, "ConstraintRuntime.accumulated @80");
+DYN_ABI_ASSERT(offsetof(dyn_constraint_runtime_record, broken) == 144, "ConstraintRuntime.broken @144");
+DYN_ABI_ASSERT(offsetof(dyn_constraint_descriptor_record, axis_a) == 48, "ConstraintDescriptor.axis_a @48");
+DYN_ABI_ASSERT(offsetof(dyn_constraint_descriptor_record, break_force) == 116, "ConstraintDescriptor.break_force @116");
 
 #endif /* DYNAMIS_ABI_H */

@@ -199,6 +199,32 @@ DYN_API dyn_status dyn_stage_timings(dyn_world* world, float* ms, uint32_t n);
 DYN_API dyn_status dyn_radix_sort(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
                                   uint32_t major_digits, uint32_t minor_digits);
 
+/* ---- constraints: ball joints (row a11 of the path) ----
+ * World::add_constraint(first, second, ConstraintDesc::ball(anchor_a, anchor_b))
+ * (crates/dynamis-world/src/constraint.rs:121, crates/dynamis-model/src/constraint.rs:568): a ball joint
+ * between two bodies by id, anchors in each body's frame, with the reference's defaults (collisions
+ * between the two bodies disabled, warm start on, axis +y). *out_id is the constraint id (creation
+ * order). The joint takes effect at the next dyn_step. */
+DYN_API dyn_status dyn_add_ball_joint(dyn_world* world, uint32_t first_body, uint32_t second_body, const float* anchor_a,
+                                      const float* anchor_b, uint32_t* out_id);
+/* ConstraintDescriptorRecords as dynamis-abi builds them (src/constraint.rs:109), appended in order
+ * (all or nothing). On this path: DYN_CONSTRAINT_BALL with DISABLE_COLLISIONS, WARM_START and
+ * HAS_BREAK; limits, swing cones and the other kinds return DYN_ERR_INVALID. */
+DYN_API dyn_status dyn_add_constraints(dyn_world* world, const dyn_constraint_descriptor_record* records, uint32_t m,
+                                       uint32_t* out_first_id);
+DYN_API dyn_status dyn_constraint_count(const dyn_world* world, uint32_t* count);
+/* The constraint runtime stream after the last step (accumulated impulses, reaction, broken), in
+ * constraint order; m must equal dyn_constraint_count. */
+DYN_API dyn_status dyn_read_constraints(dyn_world* world, dyn_constraint_runtime_record* out, uint32_t m);
+/* Descriptors, body rows and initial runtime records of every constraint, for a checker. */
+DYN_API dyn_status dyn_export_constraints(const dyn_world* world, dyn_constraint_descriptor_record* descs,
+                                          dyn_constraint_rows_record* rows, dyn_constraint_runtime_record* runtime);
+/* The joint solve order (crates/dynamis-world/src/schedule.rs:105-296): joint rows layer by layer,
+ * (first row, count) per layer and (first layer, layer count) per component, in the planner's
+ * component order. Any output may be NULL; sizes come back in *layer_count / *component_count. */
+DYN_API dyn_status dyn_joint_plan(const dyn_world* world, uint32_t* rows, uint32_t* layers, uint32_t* components,
+                                  uint32_t* layer_count, uint32_t* component_count);
+
 /* No counterpart in the reference. The same stable LSD sort as dyn_radix_sort for callers that
  * cannot allocate device memory (an external pool that forbids out-of-band allocations, or a path
  * where cudaMalloc / cudaFree would synchronise the device): it needs no world and allocates

@@ -21,6 +21,8 @@
 // its awake bit, which yields the same candidate pairs for awake bodies; contact events are not
 // published (only the CONTACT_ANNOUNCED flag that gates warm starting is kept).
 #include <algorithm>
+#include <cstring>
+#include <array>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -182,6 +184,11 @@ struct OracleWorld {
     std::vector<int32_t> velocity_deltas, position_deltas;
     std::vector<uint32_t> contributions;
     uint32_t solver_rounds = 0;
+    // constraints (ball joints) and their solve order (schedule.rs:105-296)
+    std::vector<dyn_constraint_descriptor_record> joint_descs;
+    std::vector<dyn_constraint_rows_record> joint_rows;
+    std::vector<dyn_constraint_runtime_record> joint_runtime;
+    std::vector<uint32_t> plan_rows, plan_layers, plan_components;
 };
 
 namespace {
@@ -215,7 +222,13 @@ bool body_is_moving(const dyn_body_state_record& s, const dyn_body_descriptor_re
 
 // apply_commands.rs:267-295: reset_counters.wgsl, clear_inputs.wgsl, activity.wgsl
 void apply_commands(OracleWorld& w) {
+    // joint_filter.wgsl: the jointed pairs filtered this step
+    uint32_t jointed = 0;
+    for (size_t j = 0; j < w.joint_descs.size(); ++j) {
+        if (w.joint_runtime[j].broken == 0u && (w.joint_descs[j].flags & DYN_CONSTRAINT_DISABLE_COLLISIONS)) ++jointed;
+    }
     for (uint32_t slot : kPerStepCounters) w.counters[slot] = 0;
+    w.counters[DYN_COUNTER_JOINTS] = jointed;
     uint32_t n = (uint32_t)w.states.size();
     for (uint32_t i = 0; i < n; ++i) {
         wr3(w.states[i].force, splat3(0.0f));
@@ -448,6 +461,19 @@ void broadphase(OracleWorld& w) {
 }
 
 // narrowphase.wgsl:518-685 for one pair; false when the pair answers no contact.
+// joint_filter.wgsl:9-24 then joined_pairs.wgsl: an unbroken joint with collisions disabled between
+// the two rows. The reference rebuilds the sorted list every step; a scan of the joints is the same test.
+bool joined_by_joint(const OracleWorld& w, uint32_t first_row, uint32_t second_row) {
+    uint32_t a = std::min(first_row, second_row), b = std::max(first_row, second_row);
+    for (size_t j = 0; j < w.joint_descs.size(); ++j) {
+        if (w.joint_runtime[j].broken != 0u) continue;
+        if ((w.joint_descs[j].flags & DYN_CONSTRAINT_DISABLE_COLLISIONS) == 0u) continue;
+        const dyn_constraint_rows_record& r = w.joint_rows[j];
+        if (std::min(r.first_row, r.second_row) == a && std::max(r.first_row, r.second_row) == b) return true;
+    }
+    return false;
+}
+
 bool narrowphase_pair(const OracleWorld& w, uint32_t first_slot, uint32_t second_slot, dyn_contact_record* out) {
     uint32_t fb = w.owners[first_slot];
     uint32_t sb = w.owners[second_slot];
@@ -463,7 +489,7 @@ bool narrowphase_pair(const OracleWorld& w, uint32_t first_slot, uint32_t second
     uint32_t sg = sc.collision_group != DYN_NO_COLLISION_FILTER ? sc.collision_group : second.group;
     uint32_t sm = sc.collision_mask != DYN_NO_COLLISION_FILTER ? sc.collision_mask : second.mask;
     if (!((fg & sm) != 0u && (sg & fm) != 0u)) return false;
-    // joined_pairs.wgsl: no joint filter without constraints.
+    if (joined_by_joint(w, fb, sb)) return false;
     bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
     bool fw = shape_world_geometry(fc.kind);
     bool sw = shape_world_geometry(sc.kind);
@@ -709,6 +735,11 @@ void build_islands(OracleWorld& w) {
     for (const dyn_contact_record& c : w.contacts) {
         if (c.point_count == 0u || c.sensor == 1u || !contact_touches(c, w.params.slop)) continue;
         island_couple(w, w.owners[c.a], w.owners[c.b]);
+    }
+    // island_link_constraints.wgsl
+    for (size_t j = 0; j < w.joint_descs.size(); ++j) {
+        if (w.joint_runtime[j].broken != 0u) continue;
+        island_couple(w, w.joint_rows[j].first_row, w.joint_rows[j].second_row);
     }
     uint32_t rounds = 32 - (uint32_t)__builtin_clz(std::max(dc, 2u));  // ilog2(max(N,2)) + 1
     for (uint32_t r = 0; r < rounds; ++r) {
@@ -1131,22 +1162,318 @@ void position_apply(OracleWorld& w) {
     }
 }
 
-// solver.rs:304-333 SolveSubsteps.record (no joints)
+
+// ---- ball joints (joint_velocity.wgsl, joint_solve.wgsl, joint_position.wgsl, joint_correction.wgsl) ----
+
+// schedule.rs:105-296 solve_order: components, layers, and the component order of the plan.
+uint32_t plan_root(std::vector<uint32_t>& roots, uint32_t row) {
+    while (roots[row] != row) {
+        roots[row] = roots[roots[row]];
+        row = roots[row];
+    }
+    return row;
+}
+void plan_joint_order(OracleWorld& w) {
+    const uint32_t none = 0xFFFFFFFFu;
+    const uint32_t joints = (uint32_t)w.joint_descs.size();
+    const uint32_t rows_n = (uint32_t)w.states.size();
+    w.plan_rows.clear();
+    w.plan_layers.clear();
+    w.plan_components.clear();
+    if (joints == 0) return;
+    std::vector<uint32_t> a(joints), b(joints);
+    for (uint32_t j = 0; j < joints; ++j) {
+        a[j] = w.joint_rows[j].first_row;
+        b[j] = w.joint_rows[j].second_row;
+    }
+    std::vector<bool> anchor(rows_n, false);
+    std::vector<uint32_t> roots(rows_n);
+    for (uint32_t i = 0; i < rows_n; ++i) roots[i] = i;
+    for (uint32_t j = 0; j < joints; ++j) {
+        if (!body_simulates_d(w.descs[a[j]].inverse_mass, w.descs[a[j]].flags)) anchor[a[j]] = true;
+        if (!body_simulates_d(w.descs[b[j]].inverse_mass, w.descs[b[j]].flags)) anchor[b[j]] = true;
+        uint32_t fr = plan_root(roots, a[j]), sr = plan_root(roots, b[j]);
+        uint32_t root = std::min(fr, sr);
+        roots[fr] = root;
+        roots[sr] = root;
+    }
+    std::vector<uint32_t> roots_of(joints);
+    for (uint32_t j = 0; j < joints; ++j) roots_of[j] = plan_root(roots, a[j]);
+    std::vector<bool> anchored(rows_n, false);
+    std::vector<uint32_t> head_of(rows_n, none);
+    for (uint32_t j = 0; j < joints; ++j) {
+        uint32_t root = roots_of[j];
+        if (anchor[a[j]] || anchor[b[j]]) anchored[root] = true;
+        head_of[root] = std::min(head_of[root], std::min(a[j], b[j]));
+    }
+    std::vector<std::vector<uint32_t>> adjacency(rows_n);
+    for (uint32_t j = 0; j < joints; ++j) {
+        adjacency[a[j]].push_back(b[j]);
+        adjacency[b[j]].push_back(a[j]);
+    }
+    std::vector<uint32_t> depth(rows_n, none), frontier;
+    for (uint32_t body = 0; body < rows_n; ++body) {
+        if (anchor[body]) {
+            depth[body] = 0;
+            frontier.push_back(body);
+        }
+    }
+    for (uint32_t root = 0; root < rows_n; ++root) {
+        if (head_of[root] != none && !anchored[root]) {
+            depth[head_of[root]] = 0;
+            frontier.push_back(head_of[root]);
+        }
+    }
+    for (size_t cursor = 0; cursor < frontier.size(); ++cursor) {
+        uint32_t body = frontier[cursor];
+        for (uint32_t neighbor : adjacency[body]) {
+            if (depth[neighbor] == none) {
+                depth[neighbor] = depth[body] + 1;
+                frontier.push_back(neighbor);
+            }
+        }
+    }
+    struct Key {
+        uint32_t depth, root, row;
+    };
+    std::vector<Key> settled(joints);
+    for (uint32_t j = 0; j < joints; ++j) settled[j] = Key{std::max(depth[a[j]], depth[b[j]]), roots_of[j], j};
+    std::sort(settled.begin(), settled.end(), [](const Key& x, const Key& y) {
+        return x.depth != y.depth ? x.depth < y.depth : (x.root != y.root ? x.root < y.root : x.row < y.row);
+    });
+    std::vector<uint32_t> held_layer(rows_n, 0);
+    std::vector<std::array<uint32_t, 3>> held;  // (root, layer, row)
+    for (const Key& k : settled) {
+        uint32_t layer = std::max(held_layer[a[k.row]], held_layer[b[k.row]]) + 1;
+        held_layer[a[k.row]] = layer;
+        held_layer[b[k.row]] = layer;
+        held.push_back({roots_of[k.row], layer, k.row});
+    }
+    std::sort(held.begin(), held.end());
+    struct Component {
+        uint32_t first_layer, layers, first_row, head, lanes;
+    };
+    std::vector<uint32_t> rows, layers;
+    std::vector<Component> components;
+    size_t index = 0;
+    while (index < held.size()) {
+        uint32_t root = held[index][0];
+        Component c{(uint32_t)(layers.size() / 2), 0, (uint32_t)rows.size(), none, 0};
+        uint32_t lanes = 0;
+        while (index < held.size() && held[index][0] == root) {
+            uint32_t layer = held[index][1];
+            size_t first = rows.size();
+            while (index < held.size() && held[index][0] == root && held[index][1] == layer) {
+                uint32_t row = held[index][2];
+                c.head = std::min(c.head, std::min(a[row], b[row]));
+                rows.push_back(row);
+                ++index;
+            }
+            uint32_t count = (uint32_t)(rows.size() - first);
+            lanes = std::max(lanes, count);
+            layers.push_back((uint32_t)first);
+            layers.push_back(count);
+            c.layers += 1;
+        }
+        uint32_t p2 = 1;
+        while (p2 < lanes) p2 <<= 1;
+        c.lanes = std::min(std::max(p2, 1u), 64u);
+        components.push_back(c);
+    }
+    std::stable_sort(components.begin(), components.end(), [](const Component& x, const Component& y) {
+        if (x.lanes != y.lanes) return x.lanes > y.lanes;
+        if (x.layers != y.layers) return x.layers > y.layers;
+        return x.head < y.head;
+    });
+    for (const Component& c : components) {
+        w.plan_components.push_back((uint32_t)(w.plan_layers.size() / 2));
+        w.plan_components.push_back(c.layers);
+        uint32_t cursor = c.first_row;
+        for (uint32_t layer = c.first_layer; layer < c.first_layer + c.layers; ++layer) {
+            uint32_t count = layers[2 * layer + 1];
+            w.plan_layers.push_back((uint32_t)w.plan_rows.size());
+            w.plan_layers.push_back(count);
+            for (uint32_t i = 0; i < count; ++i) w.plan_rows.push_back(rows[cursor + i]);
+            cursor += count;
+        }
+    }
+}
+
+V3 world_axis(uint32_t i) { return V3{i == 0 ? 1.0f : 0.0f, i == 1 ? 1.0f : 0.0f, i == 2 ? 1.0f : 0.0f}; }
+V3 constraint_anchor(const Body& b, V3 local) { return b.position + quat_rotate(b.orientation, local); }
+void store_velocity(OracleWorld& w, uint32_t row, const Body& b) {
+    wr3(w.states[row].velocity, b.velocity);
+    wr3(w.states[row].angular_velocity, b.angular_velocity);
+}
+
+// joint_solve.wgsl:803-832 warm_joint (ball rows of warm_constraint_rows :754-766)
+void joint_warm(OracleWorld& w, uint32_t j) {
+    const dyn_constraint_runtime_record& rt = w.joint_runtime[j];
+    if (rt.broken != 0u) return;
+    const dyn_constraint_descriptor_record& c = w.joint_descs[j];
+    const dyn_constraint_rows_record& r = w.joint_rows[j];
+    Body first_loaded = body_at(w, r.first_row), second_loaded = body_at(w, r.second_row);
+    Body first = body_is_inert(first_loaded) ? body_frozen(first_loaded) : first_loaded;
+    Body second = body_is_inert(second_loaded) ? body_frozen(second_loaded) : second_loaded;
+    if (c.flags & DYN_CONSTRAINT_WARM_START) {
+        V3 anchor_a = constraint_anchor(first, rd3(c.anchor_a));
+        V3 anchor_b = constraint_anchor(second, rd3(c.anchor_b));
+        for (uint32_t i = 0; i < 3; ++i) apply_pair_impulse(&first, &second, anchor_a, anchor_b, world_axis(i) * rt.accumulated[i]);
+    }
+    store_velocity(w, r.first_row, first);
+    store_velocity(w, r.second_row, second);
+}
+
+// joint_solve.wgsl:236-267, 419-430 solve_joint for a ball joint; solve_point_row :96-128
+void joint_solve(OracleWorld& w, uint32_t j, bool residual) {
+    dyn_constraint_runtime_record& rt = w.joint_runtime[j];
+    const dyn_constraint_descriptor_record& c = w.joint_descs[j];
+    const dyn_constraint_rows_record& r = w.joint_rows[j];
+    float accumulated[DYN_CONSTRAINT_ACCUMULATOR_SLOTS];
+    for (uint32_t i = 0; i < DYN_CONSTRAINT_ACCUMULATOR_SLOTS; ++i)
+        accumulated[i] = (c.flags & DYN_CONSTRAINT_WARM_START) ? rt.accumulated[i] : 0.0f;
+    if (rt.broken != 0u) return;
+    Body first_loaded = body_at(w, r.first_row), second_loaded = body_at(w, r.second_row);
+    if (body_is_inert(first_loaded) && body_is_inert(second_loaded)) return;
+    Body first = body_is_inert(first_loaded) ? body_frozen(first_loaded) : first_loaded;
+    Body second = body_is_inert(second_loaded) ? body_frozen(second_loaded) : second_loaded;
+    const Body mass_first = first, mass_second = second;
+    V3 anchor_a = constraint_anchor(first, rd3(c.anchor_a));
+    V3 anchor_b = constraint_anchor(second, rd3(c.anchor_b));
+    V3 linear_first{0, 0, 0}, angular_first{0, 0, 0}, linear_second{0, 0, 0}, angular_second{0, 0, 0};
+    for (uint32_t i = 0; i < 3; ++i) {
+        V3 axis = world_axis(i);
+        float k = point_momentum_mass(mass_first, mass_second, anchor_a, anchor_b, axis);
+        if (k > 0.0f) {
+            Body row_first = first, row_second = second;
+            V3 velocity = relative_velocity(first, second, anchor_a, anchor_b);
+            float jacobian_speed = dot(velocity, axis);
+            float next = accumulated[i] - jacobian_speed / k;
+            float applied = next - accumulated[i];
+            apply_pair_impulse(&first, &second, anchor_a, anchor_b, axis * applied);
+            accumulated[i] = next;
+            V3 impulse = axis * accumulated[i];
+            linear_first = linear_first + (-impulse);
+            linear_second = linear_second + impulse;
+            angular_first = angular_first + cross(anchor_a - body_com(row_first), -impulse);
+            angular_second = angular_second + cross(anchor_b - body_com(row_second), impulse);
+        }
+    }
+    if (c.flags & DYN_CONSTRAINT_HAS_BREAK) {
+        float force = length(linear_second) / w.params.dt;
+        float torque = length(angular_second) / w.params.dt;
+        if ((c.break_force > 0.0f && force > c.break_force) || (c.break_torque > 0.0f && torque > c.break_torque)) rt.broken = 1u;
+    }
+    for (uint32_t i = 0; i < DYN_CONSTRAINT_ACCUMULATOR_SLOTS; ++i) rt.accumulated[i] = accumulated[i];
+    std::memset(&rt.reaction, 0, sizeof(rt.reaction));
+    wr3(rt.reaction.linear_first, linear_first);
+    wr3(rt.reaction.angular_first, angular_first);
+    wr3(rt.reaction.linear_second, linear_second);
+    wr3(rt.reaction.angular_second, angular_second);
+    store_velocity(w, r.first_row, first);
+    store_velocity(w, r.second_row, second);
+    if (!residual) return;
+    uint32_t lin = (uint32_t)solver_word(fmaxw(length(first.velocity - first_loaded.velocity),
+                                               length(second.velocity - second_loaded.velocity)),
+                                         DYN_SOLVER_VELOCITY_SCALE);
+    uint32_t ang = (uint32_t)solver_word(fmaxw(length(first.angular_velocity - first_loaded.angular_velocity),
+                                               length(second.angular_velocity - second_loaded.angular_velocity)),
+                                         DYN_SOLVER_VELOCITY_SCALE);
+    w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL] = std::max(w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL], lin);
+    w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL] = std::max(w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL], ang);
+}
+
+// joint_position.wgsl:18-36 project over joint_correction.wgsl:5-27, 85-90 (ball: three point rows)
+void apply_correction(Body* b, V3 linear, V3 angular) {
+    b->position = b->position + linear;
+    V3 half = angular * 0.5f;
+    b->orientation = normalize(quat_mul(V4{half.x, half.y, half.z, 1.0f}, b->orientation));
+}
+void joint_project(OracleWorld& w, uint32_t j) {
+    const dyn_constraint_descriptor_record& c = w.joint_descs[j];
+    const dyn_constraint_rows_record& r = w.joint_rows[j];
+    if (w.joint_runtime[j].broken != 0u) return;
+    Body first_loaded = body_at(w, r.first_row), second_loaded = body_at(w, r.second_row);
+    Body first = body_is_inert(first_loaded) ? body_frozen(first_loaded) : first_loaded;
+    Body second = body_is_inert(second_loaded) ? body_frozen(second_loaded) : second_loaded;
+    const float scale = w.params.relaxation;
+    V3 zero{0.0f, 0.0f, 0.0f};
+    V3 total_first = zero, total_first_angular = zero, total_second = zero, total_second_angular = zero;
+    for (uint32_t i = 0; i < 3; ++i) {
+        V3 axis = world_axis(i);
+        V3 point_a = constraint_anchor(first, rd3(c.anchor_a));
+        V3 point_b = constraint_anchor(second, rd3(c.anchor_b));
+        V3 linear_first = zero, linear_second = zero;
+        float k = first.inverse_mass + second.inverse_mass;  // linear_momentum_mass
+        if (k > 0.0f) {
+            float magnitude = scale * (dot(point_b - point_a, axis) - 0.0f) / k;
+            linear_first = axis * (magnitude * first.inverse_mass);
+            linear_second = axis * (-magnitude * second.inverse_mass);
+        }
+        apply_correction(&first, linear_first, zero);
+        apply_correction(&second, linear_second, zero);
+        total_first = total_first + linear_first;
+        total_first_angular = total_first_angular + zero;
+        total_second = total_second + linear_second;
+        total_second_angular = total_second_angular + zero;
+    }
+    bool holds = dot(total_first, total_first) > 0.0f || dot(total_first_angular, total_first_angular) > 0.0f ||
+                 dot(total_second, total_second) > 0.0f || dot(total_second_angular, total_second_angular) > 0.0f;
+    if (!holds) return;
+    dyn_body_state_record& sa = w.states[r.first_row];
+    dyn_body_state_record& sb = w.states[r.second_row];
+    Body fa = load_body(sa, w.descs[r.first_row]), fb = load_body(sb, w.descs[r.second_row]);
+    apply_correction(&fa, total_first, total_first_angular);
+    apply_correction(&fb, total_second, total_second_angular);
+    wr3(sa.position, fa.position);
+    wr4(sa.orientation, fa.orientation);
+    wr3(sb.position, fb.position);
+    wr4(sb.orientation, fb.orientation);
+    w.resolution[r.first_row] = w.resolution[r.first_row] + total_first;
+    w.resolution[r.second_row] = w.resolution[r.second_row] + total_second;
+}
+
+// joint_velocity.wgsl:24-54 / joint_position.wgsl:30-61: every component, a forward and a backward
+// sweep over its layers. Components and the joints of a layer touch disjoint bodies, so visiting
+// them in sequence gives what the parallel lanes give.
+enum class JointWalk { Warm, Solve, Project };
+void walk_joints(OracleWorld& w, JointWalk mode, bool residual) {
+    for (size_t c = 0; c + 1 < w.plan_components.size(); c += 2) {
+        uint32_t offset = w.plan_components[c], count = w.plan_components[c + 1];
+        for (uint32_t sweep = 0; sweep < 2; ++sweep) {
+            for (uint32_t step = 0; step < count; ++step) {
+                uint32_t layer = sweep == 0 ? offset + step : offset + count - 1 - step;
+                uint32_t first = w.plan_layers[2 * layer], n = w.plan_layers[2 * layer + 1];
+                for (uint32_t i = 0; i < n; ++i) {
+                    uint32_t j = w.plan_rows[first + i];
+                    if (mode == JointWalk::Warm) joint_warm(w, j);
+                    else if (mode == JointWalk::Solve) joint_solve(w, j, residual);
+                    else joint_project(w, j);
+                }
+            }
+        }
+    }
+}
+
+// solver.rs:304-333 SolveSubsteps.record
 void solve_substeps(OracleWorld& w) {
     uint32_t c = (uint32_t)w.contacts.size();
     for (uint32_t substep = 0; substep < w.params.substeps; ++substep) {
         substep_integrate(w);
         if (substep == 0) {
+            walk_joints(w, JointWalk::Warm, false);
             for (uint32_t i = 0; i < c; ++i) warm_contact_block(w, i);
             block_apply(w);
         }
         for (uint32_t it = 0; it < w.params.solve_iterations; ++it) {
             bool residual = w.solver_rounds == w.params.solve_iterations;
+            walk_joints(w, JointWalk::Solve, residual);
             for (uint32_t i = 0; i < c; ++i) solve_contact_block(w, i, residual);
             block_apply(w);
         }
         substep_advance(w);
         for (uint32_t it = 0; it < w.params.position_iterations; ++it) {
+            walk_joints(w, JointWalk::Project, false);
             position_block(w);
             position_apply(w);
         }
@@ -1221,6 +1548,39 @@ OracleWorld* orc_world_create(const dyn_step_params* params, const dyn_body_stat
 }
 
 void orc_world_destroy(OracleWorld* w) { delete w; }
+
+// Constraints in row order with their body rows and runtime records; plans the solve order.
+// Returns 0 when a row is out of range or a kind other than the ball joint appears.
+uint32_t orc_set_constraints(OracleWorld* w, const dyn_constraint_descriptor_record* descs,
+                             const dyn_constraint_rows_record* rows, const dyn_constraint_runtime_record* runtime,
+                             uint32_t m) {
+    uint32_t n = (uint32_t)w->states.size();
+    for (uint32_t j = 0; j < m; ++j) {
+        if (rows[j].first_row >= n || rows[j].second_row >= n || descs[j].kind != DYN_CONSTRAINT_BALL) return 0;
+    }
+    w->joint_descs.assign(descs, descs + m);
+    w->joint_rows.assign(rows, rows + m);
+    w->joint_runtime.assign(runtime, runtime + m);
+    plan_joint_order(*w);
+    w->params.constraint_count = m;
+    return 1;
+}
+
+uint32_t orc_constraints(const OracleWorld* w, dyn_constraint_runtime_record* out) {
+    if (out) std::memcpy(out, w->joint_runtime.data(), w->joint_runtime.size() * sizeof(*out));
+    return (uint32_t)w->joint_runtime.size();
+}
+
+void orc_joint_plan(const OracleWorld* w, uint32_t* rows, uint32_t* layers, uint32_t* components, uint32_t* sizes) {
+    if (rows) std::memcpy(rows, w->plan_rows.data(), w->plan_rows.size() * 4);
+    if (layers) std::memcpy(layers, w->plan_layers.data(), w->plan_layers.size() * 4);
+    if (components) std::memcpy(components, w->plan_components.data(), w->plan_components.size() * 4);
+    if (sizes) {
+        sizes[0] = (uint32_t)w->plan_rows.size();
+        sizes[1] = (uint32_t)(w->plan_layers.size() / 2);
+        sizes[2] = (uint32_t)(w->plan_components.size() / 2);
+    }
+}
 
 void orc_step(OracleWorld* w, float dt) {
     w->params.dt = dt;

@@ -44,6 +44,11 @@ def lib() -> ctypes.CDLL:
         _lib.orc_radix_sort.argtypes = [P, P, P, U32, U32, U32]
         _lib.orc_narrowphase_pair.restype = U32
         _lib.orc_narrowphase_pair.argtypes = [P, U32, U32, P]
+        _lib.orc_set_constraints.restype = U32
+        _lib.orc_set_constraints.argtypes = [P, P, P, P, U32]
+        _lib.orc_constraints.restype = U32
+        _lib.orc_constraints.argtypes = [P, P]
+        _lib.orc_joint_plan.argtypes = [P, P, P, P, P]
     return _lib
 
 
@@ -65,6 +70,11 @@ class OracleWorld:
                                      pair_capacity, contact_capacity)
         if not self._h:
             raise ValueError("oracle refused the scene: collider owners or hull sources out of range")
+        if "constraint_descs" in s:
+            m = len(s["constraint_descs"])
+            if not L.orc_set_constraints(self._h, _p(s["constraint_descs"]), _p(s["constraint_rows"]),
+                                         _p(s["constraint_runtime"]), m):
+                raise ValueError("oracle refused the constraints: rows out of range or a kind other than ball")
 
     def close(self):
         if self._h:
@@ -115,6 +125,21 @@ class OracleWorld:
         out = np.zeros(n, R.CONTACT)
         lib().orc_contacts(self._h, _p(out))
         return out
+
+    def constraints(self) -> np.ndarray:
+        n = lib().orc_constraints(self._h, None)
+        out = np.zeros(n, R.CONSTRAINT_RUNTIME)
+        lib().orc_constraints(self._h, _p(out))
+        return out
+
+    def joint_plan(self) -> dict:
+        sizes = np.zeros(3, np.uint32)
+        lib().orc_joint_plan(self._h, None, None, None, _p(sizes))
+        rows = np.zeros(sizes[0], np.uint32)
+        layers = np.zeros((sizes[1], 2), np.uint32)
+        comps = np.zeros((sizes[2], 2), np.uint32)
+        lib().orc_joint_plan(self._h, _p(rows), _p(layers), _p(comps), None)
+        return {"rows": rows, "layers": layers, "components": comps}
 
     def islands(self) -> np.ndarray:
         n = lib().orc_islands(self._h, None)
