@@ -33,6 +33,12 @@ sys.path.insert(0, str(ROOT))
 METRIC = "rigid body-steps/s at 256K bodies; batched-worlds & adjoint step/s vs plain"
 UNIT = "body-steps/s"
 DT = 1.0 / 60.0
+WORKLOAD_DT = {"hanging_chains_8192": 1.0 / 120.0, "hanging_chains_131072": 1.0 / 120.0}
+
+
+def dt_of(workload: str) -> float:
+    """The timestep the workload's scene is specified at (1/120 s for the joint chains)."""
+    return WORKLOAD_DT.get(workload, DT)
 _T0 = time.perf_counter()
 
 
@@ -102,10 +108,14 @@ def stage_bytes(stage: str, m: dict, params: dict) -> float:
     """Algorithmic (compulsory) HBM bytes of one launch of a stage's kernel pair, from the counts
     of the same step: K colliders, E entries, P pairs, C contacts, R solver rows, L live bodies."""
     K, E, P, C, R_, L = m["K"], m["E"], m["P"], m["C"], m["R"], m["L"]
-    if stage == "velocity":     # one Jacobi iteration: solve over contacts + apply over rows
-        return 472.0 * C + 72.0 * R_
+    J = m.get("J", 0)
+    # a ball joint per sweep (two sweeps per pass): 112 B of descriptor, two 92 B bodies read and
+    # their velocities (or poses) written back, 12 B of accumulated impulse
+    joint = 2 * (112.0 + 2 * 92.0 + 2 * 24.0 + 12.0) * J
+    if stage == "velocity":     # one Jacobi iteration: joints, solve over contacts + apply over rows
+        return 472.0 * C + 72.0 * R_ + joint
     if stage == "position":     # one position iteration
-        return 200.0 * C + 64.0 * R_
+        return 200.0 * C + 64.0 * R_ + joint
     if stage == "narrowphase":
         return 596.0 * P
     if stage == "aabb":
@@ -146,6 +156,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     from dynamis_b200 import records as R
 
     torch.cuda.set_device(local_rank)
+    DT = dt_of(args.workload)
     world, scene, build_s = build_world(args.workload, local_rank)
     bodies = world.sizes()["bodies"]
     log(f"scene {args.workload}: {bodies} bodies built in {build_s:.1f}s")
@@ -186,7 +197,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     m = world.measured()
     counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
               "P": int(m[R.COUNTER["PAIRS"]]), "C": int(m[R.COUNTER["CONTACTS"]]), "R": int(m[R.COUNTER["SOLVER_ROWS"]]),
-              "L": int(m[R.COUNTER["LIVE"]])}
+              "L": int(m[R.COUNTER["LIVE"]]), "J": world.constraint_count()}
     launches_per_step = world.step_kernel_count()
     # per-stage breakdown: one more step run eagerly with CUDA events between stages
     world.set_timing(True)
@@ -245,23 +256,23 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         "clocks": clocks.summary(),
     }
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget)
+        result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
     world.close()
     return result
 
 
-def cpu_baseline(world, budget_s: float = 20.0) -> dict:
+def cpu_baseline(world, budget_s: float = 20.0, dt: float = DT) -> dict:
     """The oracle (CPU restatement, one thread) stepping the same world state."""
     from oracle.oracle import OracleWorld
 
     scene = world.export_scene()
     scene["states"] = world.read_states()
-    oracle = OracleWorld(scene, world.step_params(DT))
+    oracle = OracleWorld(scene, world.step_params(dt))
     log("cpu baseline: oracle world built")
     steps = 0
     t0 = time.perf_counter()
     while True:
-        oracle.step(DT)
+        oracle.step(dt)
         steps += 1
         if time.perf_counter() - t0 > budget_s / 2 or steps >= 3:
             break
@@ -275,6 +286,7 @@ def run_reference(args) -> dict:
     """The reference arm: the CPU restatement of the step on the host, all it can use (one thread)."""
     from dynamis_b200 import World
 
+    DT = dt_of(args.workload)
     world, scene, _ = build_world(args.workload, 0)
     state_note = "initial lattice state"
     try:
@@ -287,7 +299,7 @@ def run_reference(args) -> dict:
             state_note = f"state after {args.setup + args.warmup} steps (input prepared on the GPU, untimed)"
     except Exception:
         pass
-    base = cpu_baseline(world, budget_s=args.cpu_budget)
+    base = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
     base["sample"] += f"; {state_note}"
     world.close()
     return {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,

@@ -167,7 +167,7 @@ __device__ __forceinline__ void joint_project(const DeviceWorld& w, const dyn_st
 
 // One warp per group of components (joint_velocity.wgsl:24-54 with a warp for a workgroup).
 template <int kPass>
-__global__ void __launch_bounds__(128) k_joints(DeviceWorld w, dyn_step_params p) {
+__global__ void __launch_bounds__(32) k_joints(DeviceWorld w, dyn_step_params p) {
     const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (group >= w.jgroup_count) return;  // warp-uniform
     const uint32_t lane = threadIdx.x & 31u;

@@ -537,13 +537,18 @@ void plan_joints(const std::vector<uint32_t>& first, const std::vector<uint32_t>
         }
     }
     // device packing (not the reference's workgroup packing: results do not depend on it, since
-    // components share no body): consecutive components of equal lane width fill 32-lane warps
+    // components share no body): consecutive components of equal lane width share a 32-lane warp,
+    // at most kComponentsPerWarp of them. A component is a chain of dependent solves, so a pass
+    // takes (layers x latency of one solve); spreading components over more warps gives each SM
+    // several warps to interleave instead of one warp holding 32 chains.
+    constexpr uint32_t kComponentsPerWarp = 8;
     uint32_t c = 0;
     while (c < (uint32_t)comps.size()) {
         uint32_t lanes = std::min(comps[c].lanes, 32u);
         uint32_t span = comps[c].layers;
         uint32_t taken = 1;
-        while (c + taken < (uint32_t)comps.size() && (taken + 1) * lanes <= 32u && std::min(comps[c + taken].lanes, 32u) == lanes) {
+        while (c + taken < (uint32_t)comps.size() && taken < kComponentsPerWarp && (taken + 1) * lanes <= 32u &&
+               std::min(comps[c + taken].lanes, 32u) == lanes) {
             span = std::max(span, comps[c + taken].layers);
             ++taken;
         }

@@ -537,7 +537,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     Marker mark{d, s, timed};
     const uint32_t N = std::max(dw.n, 1u), K = std::max(dw.k, 1u), ND = std::max(dw.nd, 1u);
     const uint32_t E = dw.e_cap, P = dw.p_cap, C = dw.c_cap;
-    const uint32_t joint_blocks = div_up(dw.jgroup_count, 4u);  // four warp groups per 128-thread block
+    const uint32_t joint_blocks = dw.jgroup_count;  // one warp group per 32-thread block
     mark(ST_BEGIN);
     k_reset<<<1, 64, 0, s>>>(dw);
     if (dw.jcount) k_joint_count<<<blocks_for(std::max(dw.jfilter_count, 1u), 256), 256, 0, s>>>(dw);
@@ -587,13 +587,13 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         k_solve_prepare<<<blocks_for(C, 128), 128, 0, s>>>(dw);
         if (sub == 0) {
             mark(ST_WARM);
-            if (joint_blocks) k_joints<JP_WARM><<<joint_blocks, 128, 0, s>>>(dw, p);
+            if (joint_blocks) k_joints<JP_WARM><<<joint_blocks, 32, 0, s>>>(dw, p);
             k_warm<<<blocks_for(C, 128), 128, 0, s>>>(dw);
             k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_VELOCITY);
         for (uint32_t it = 0; it < p.solve_iterations; ++it) {
-            if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 128, 0, s>>>(dw, p);
+            if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 32, 0, s>>>(dw, p);
             k_solve<<<blocks_for(C, 128), 128, 0, s>>>(dw, p);
             k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
         }
@@ -601,7 +601,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         k_advance<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
         mark(ST_POSITION);
         for (uint32_t it = 0; it < p.position_iterations; ++it) {
-            if (joint_blocks) k_joints<JP_POSITION><<<joint_blocks, 128, 0, s>>>(dw, p);
+            if (joint_blocks) k_joints<JP_POSITION><<<joint_blocks, 32, 0, s>>>(dw, p);
             k_position<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
             k_papply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
         }

@@ -37,10 +37,27 @@ class Scene:
             is_hull = colliders["shape"] == R.SHAPE_HULL
             colliders["source"][is_hull] = sources[colliders["source"][is_hull]]
         ids = world.spawn(self.bodies, colliders)
-        if self.joints is not None:
-            for jt in self.joints:
-                world.add_ball_joint(int(ids[jt["first"]]), int(ids[jt["second"]]), jt["anchor_a"], jt["anchor_b"])
+        if self.joints is not None and len(self.joints):
+            world.add_constraints(ball_joint_records(ids[self.joints["first"]], ids[self.joints["second"]],
+                                                     self.joints["anchor_a"], self.joints["anchor_b"]))
         return ids
+
+
+def ball_joint_records(first_ids, second_ids, anchor_a, anchor_b) -> np.ndarray:
+    """ConstraintDescriptorRecords of ConstraintDesc::ball joints with the reference's defaults
+    (collisions disabled between the pair, warm start, axis +y), as dyn_add_ball_joint builds them."""
+    rec = np.zeros(len(first_ids), R.CONSTRAINT_DESCRIPTOR)
+    rec["kind"] = R.CONSTRAINT_BALL
+    rec["first_body_id"] = first_ids
+    rec["second_body_id"] = second_ids
+    rec["flags"] = R.CONSTRAINT_DISABLE_COLLISIONS | R.CONSTRAINT_WARM_START
+    rec["anchor_a"] = anchor_a
+    rec["anchor_b"] = anchor_b
+    rec["axis_a"] = (0.0, 1.0, 0.0)
+    rec["swing_a"] = np.float32(np.pi)
+    rec["swing_b"] = np.float32(np.pi)
+    rec["gear_ratio"] = 1.0
+    return rec
 
 
 def yaw_quaternions(angles: np.ndarray) -> np.ndarray:
