@@ -255,10 +255,51 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
     }
+    if args.workload.startswith("batched_worlds_"):
+        result["batch"] = loop_baseline(args, DT, ms / args.steps, local_rank)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
     world.close()
     return result
+
+
+def loop_baseline(args, dt: float, batch_ms: float, device: int, sample_every: int = 16) -> dict:
+    """The same worlds as a loop of plain single-world steps (one World, one graph launch each), timed
+    on a sample of every `sample_every`-th world after the same setup steps, on one stream."""
+    import torch
+
+    from dynamis_b200 import World, scenes
+
+    worlds = int(args.workload.rsplit("_", 1)[1])
+    parts = scenes.batched_world_parts(worlds)
+    sample = parts[::sample_every]
+    stream = torch.cuda.Stream(device=device)
+    loop = []
+    for part in sample:
+        w = World(device=device)
+        part.build(w)
+        w.set_stream(stream.cuda_stream)
+        loop.append(w)
+    for _ in range(args.setup + args.warmup):
+        for w in loop:
+            w.step(dt)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        for w in loop:
+            w.step(dt)
+    end.record(stream)
+    end.synchronize()
+    sample_ms = start.elapsed_time(end) / args.steps
+    for w in loop:
+        w.close()
+    estimate = sample_ms * len(parts) / len(sample)
+    log(f"loop of {len(sample)} sampled worlds: {sample_ms:.3f} ms/step; all {len(parts)}: ~{estimate:.1f} ms/step")
+    return {"worlds": len(parts), "batch_ms_per_step": batch_ms,
+            "loop": {"sample_worlds": len(sample), "sample": f"every {sample_every}th world, same setup steps",
+                     "ms_per_step_sample": sample_ms, "ms_per_step_estimate": estimate},
+            "speedup_vs_loop": estimate / batch_ms}
 
 
 def cpu_baseline(world, budget_s: float = 20.0, dt: float = DT) -> dict:

@@ -90,6 +90,7 @@ struct DeviceWorld {
     uint32_t* wake_flags;
     uint32_t* row_of_id;
     uint32_t id_count;
+    uint32_t* body_world;  // sub-world of each row (all 0 outside a batch)
     // colliders
     uint32_t* c_owner;
     uint4* c_kind;     // kind, flags, source, 0

@@ -357,6 +357,10 @@ void rebuild_rows(dyn_world* w) {
         w->descs[r] = w->spawn_descs[order[r]];
         w->row_of_id[order[r]] = r;
     }
+    w->body_world.assign(n, 0u);
+    for (uint32_t r = 0; r < n; ++r) {
+        if (order[r] < w->world_of_id.size()) w->body_world[r] = w->world_of_id[order[r]];
+    }
     w->colliders = w->spawn_colliders;
     w->owners.resize(w->spawn_owner.size());
     for (size_t i = 0; i < w->spawn_owner.size(); ++i) w->owners[i] = w->row_of_id[w->spawn_owner[i]];
@@ -572,6 +576,8 @@ dyn_status rebuild_joints(dyn_world* w) {
         uint32_t b = d.second_body_id < w->row_of_id.size() ? w->row_of_id[d.second_body_id] : DYN_NO_BODY;
         if (a == DYN_NO_BODY || b == DYN_NO_BODY || a >= n || b >= n)
             return fail(w, DYN_ERR_INVALID, "a joint must join two live bodies");
+        if (a < w->body_world.size() && b < w->body_world.size() && w->body_world[a] != w->body_world[b])
+            return fail(w, DYN_ERR_INVALID, "a joint must not join bodies of different sub-worlds");
         w->joint_rows[j] = dyn_constraint_rows_record{a, b};
         first[j] = a;
         second[j] = b;
@@ -991,6 +997,34 @@ DYN_API dyn_status dyn_add_constraints(dyn_world* w, const dyn_constraint_descri
         }
     }
     if (out_first_id) *out_first_id = (uint32_t)before;
+    return DYN_OK;
+}
+
+// ---- batched worlds ----
+DYN_API dyn_status dyn_set_body_worlds(dyn_world* w, const uint32_t* world_of_body, uint32_t n) {
+    if (!w || (n && !world_of_body)) return fail(w, DYN_ERR_INVALID, "dyn_set_body_worlds: null argument");
+    uint32_t ids = (uint32_t)std::max(w->spawn_states.size(), w->row_of_id.size());
+    if (n != ids) return fail(w, DYN_ERR_INVALID, "dyn_set_body_worlds: one sub-world per body id");
+    w->world_of_id.assign(world_of_body, world_of_body + n);
+    if (w->raw_rows) {
+        w->body_world.assign(w->states.size(), 0u);
+        for (size_t r = 0; r < w->states.size(); ++r) {
+            uint32_t id = w->states[r].body_id;
+            if (id < n) w->body_world[r] = world_of_body[id];
+        }
+    } else {
+        w->rows_dirty = true;
+    }
+    w->joints_dirty = true;
+    if (w->dev) w->scene_dirty = true;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_export_body_worlds(const dyn_world* cw, uint32_t* rows_out) {
+    if (!cw || !rows_out) return DYN_ERR_INVALID;
+    dyn_world* w = const_cast<dyn_world*>(cw);
+    rebuild_rows(w);
+    for (size_t r = 0; r < w->states.size(); ++r) rows_out[r] = r < w->body_world.size() ? w->body_world[r] : 0u;
     return DYN_OK;
 }
 

@@ -154,6 +154,14 @@ __device__ __forceinline__ uint32_t cell_hash(I3 c) {
     return (x ^ y ^ z ^ (x << 7) ^ (y >> 3) ^ (z << 11)) & DYN_CELL_HASH_MASK;
 }
 __device__ __forceinline__ uint32_t cell_key(uint32_t level, I3 c) { return (level << DYN_LEVEL_KEY_SHIFT) | cell_hash(c); }
+// Batched worlds: the sub-world of a row is mixed into its cells' hash, so the grids of different
+// sub-worlds share no cell (up to hash collisions, which the pair test rejects). World 0 mixes in
+// nothing, so a single world's keys are the reference's. The odd multiplier keeps distinct worlds
+// distinct modulo the 27-bit hash.
+__device__ __forceinline__ uint32_t world_mix(uint32_t world) { return world * 0x2545F491u; }
+__device__ __forceinline__ uint32_t cell_key_in(uint32_t level, I3 c, uint32_t world) {
+    return (level << DYN_LEVEL_KEY_SHIFT) | ((cell_hash(c) ^ world_mix(world)) & DYN_CELL_HASH_MASK);
+}
 __device__ __forceinline__ uint32_t shape_levels(f3 mn, f3 mx, float base) {
     uint32_t level = 0;
     for (;;) {
@@ -222,6 +230,7 @@ __global__ void k_entry_emit(DeviceWorld w) {
         const BodyHot& h = w.hot[owner];
         bool mv = moves(h.pos.w, h.aux.y);
         bool awake = w.activity[owner] != 0u || w.wake_flags[owner] != 0u;
+        const uint32_t world = w.body_world[owner];
         for (uint32_t ordinal = 0; ordinal < emitted; ++ordinal) {
             I3 c = I3{lo.x + (int)(ordinal / rows), lo.y + (int)((ordinal / sz) % sy), lo.z + (int)(ordinal % sz)};
             uint32_t offset = (uint32_t)(c.x - lo.x) | ((uint32_t)(c.y - lo.y) << 1) | ((uint32_t)(c.z - lo.z) << 2);
@@ -230,7 +239,7 @@ __global__ void k_entry_emit(DeviceWorld w) {
             if (mv) info |= DYN_ENTRY_MOBILE;
             if (offset == 0u) info |= DYN_ENTRY_PRIMARY;
             uint32_t slot = first + ordinal;
-            w.ekey[slot] = cell_key(level, c);
+            w.ekey[slot] = cell_key_in(level, c, world);
             w.eval[slot] = slot;
             w.entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(owner));
             w.entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(info));
@@ -268,6 +277,7 @@ __device__ __forceinline__ void emit_pair(const DeviceWorld& w, const GEntry& a,
     if (((b.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) return;
     if (same_node || a.group == b.group) return;
     if ((a.info & DYN_ENTRY_MOBILE) == 0u && (b.info & DYN_ENTRY_MOBILE) == 0u) return;
+    if (w.body_world[a.group] != w.body_world[b.group]) return;  // different sub-worlds of a batch
     uint32_t slot = append_slot(&w.counters[DYN_COUNTER_PAIRS]);
     if (slot < w.p_cap) {
         uint32_t ia = a.info & DYN_ENTRY_INDEX_MASK, ib = b.info & DYN_ENTRY_INDEX_MASK;
@@ -363,6 +373,7 @@ __global__ void k_pairs(DeviceWorld w) {
         bool awake = entry_awake(w, e);
         uint32_t level = w.c_level[e.info & DYN_ENTRY_INDEX_MASK];
         if ((e.info & DYN_ENTRY_PRIMARY) != 0u && (awake || coarse_active)) {
+            const uint32_t world = w.body_world[e.group];
             uint32_t coarser = occupied & ~((1u << min(level + 1u, 31u)) - 1u);
             while (coarser != 0u) {
                 uint32_t link = 31u - __clz(coarser);
@@ -380,7 +391,7 @@ __global__ void k_pairs(DeviceWorld w) {
                     for (int y = lo.y; y <= hi.y; ++y)
                         for (int z = lo.z; z <= hi.z; ++z) {
                             I3 cell = I3{x, y, z};
-                            uint32_t key = cell_key(link, cell);
+                            uint32_t key = cell_key_in(link, cell, world);
                             uint32_t j = cell_find(w, live, bits, overflow, key);
                             for (; j < live && __ldg(w.ekey + j) == key; ++j) {
                                 uint32_t other = w.eval[j];

@@ -180,6 +180,7 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.motion, N);
         A(dw.wake_flags, N);
         A(dw.row_of_id, N);
+        A(dw.body_world, N);
         A(dw.c_owner, K);
         A(dw.c_kind, K);
         A(dw.c_offset, K);
@@ -408,6 +409,9 @@ dyn_status upload_scene(dyn_world* w) {
     DYN_CUDA(cudaMemcpyAsync(dw.inert0, inert0.data(), n * sizeof(float4), cudaMemcpyHostToDevice, s));
     DYN_CUDA(cudaMemcpyAsync(dw.inert1, inert1.data(), n * sizeof(float2), cudaMemcpyHostToDevice, s));
     DYN_CUDA(cudaMemcpyAsync(dw.row_of_id, w->row_of_id.data(), w->row_of_id.size() * 4, cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> body_world(n, 0u);
+    for (uint32_t i = 0; i < n && i < w->body_world.size(); ++i) body_world[i] = w->body_world[i];
+    DYN_CUDA(cudaMemcpyAsync(dw.body_world, body_world.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
     DYN_CUDA(cudaMemsetAsync(dw.wake_flags, 0, (size_t)d->n_cap * 4, s));
     DYN_CUDA(cudaMemcpyAsync(dw.c_owner, w->owners.data(), k * 4, cudaMemcpyHostToDevice, s));
     DYN_CUDA(cudaMemcpyAsync(dw.c_kind, ckind.data(), k * sizeof(uint4), cudaMemcpyHostToDevice, s));
@@ -427,6 +431,7 @@ dyn_status upload_scene(dyn_world* w) {
     DYN_CUDA(cudaMemsetAsync(dw.counters, 0, 64 * 4, s));
     DYN_CUDA(cudaStreamSynchronize(s));
     if ((st = upload_joints(w))) return st;
+    w->scene_dirty = false;
     d->parity = 0;
     d->stepped = false;
     d->uploaded = true;
@@ -613,7 +618,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
 
 dyn_status prepare_step(dyn_world* w, float dt) {
     if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(w, DYN_ERR_INVALID, "a step timestep must be positive");
-    bool fresh = !w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows);
+    bool fresh = !w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows) || w->scene_dirty;
     if (fresh || w->joints_dirty) {
         dyn_status st = save_joint_runtime(w);
         if (st) return st;
@@ -743,6 +748,10 @@ DYN_API dyn_status dyn_upload_bodies(dyn_world* w, const dyn_body_state_record* 
     for (uint32_t i = 0; i < n; ++i) max_id = std::max(max_id, states[i].body_id + 1);
     w->row_of_id.assign(std::max(max_id, n), DYN_NO_BODY);
     for (uint32_t i = 0; i < n; ++i) w->row_of_id[states[i].body_id] = i;
+    w->body_world.assign(n, 0u);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (states[i].body_id < w->world_of_id.size()) w->body_world[i] = w->world_of_id[states[i].body_id];
+    }
     return upload_scene(w);
 }
 
@@ -750,7 +759,7 @@ DYN_API dyn_status dyn_upload_states(dyn_world* w, const dyn_body_state_record* 
     if (!w || !states) return fail(w, DYN_ERR_INVALID, "dyn_upload_states: null argument");
     rebuild_rows(w);
     if (n != w->states.size()) return fail(w, DYN_ERR_INVALID, "dyn_upload_states: row count differs from the scene");
-    if (!w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows)) {
+    if (!w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows) || w->scene_dirty) {
         dyn_status st = upload_scene(w);
         if (st) return st;
     }

@@ -55,12 +55,16 @@ struct dyn_world {
     std::vector<uint32_t> owners;
     std::vector<uint32_t> row_of_id;
     uint32_t dynamic_count = 0;
+    // batched worlds: the sub-world of every body by id (empty: one world) and of every row
+    std::vector<uint32_t> world_of_id;
+    std::vector<uint32_t> body_world;
     // constraints in creation order (constraint id = index); rows and plan derived with the rows
     std::vector<dyn_constraint_descriptor_record> joint_descs;
     std::vector<dyn_constraint_runtime_record> joint_runtime;  // initial runtime records
     std::vector<dyn_constraint_rows_record> joint_rows;
     dyn::JointPlan joint_plan;
     bool joints_dirty = false;  // the device's joint buffers and plan are out of date
+    bool scene_dirty = false;   // the device's scene is out of date although the rows are current
     bool timing = false;
     void* user_stream = nullptr;  // caller's cudaStream_t (dyn_world_set_stream)
     dyn::DeviceState* dev = nullptr;

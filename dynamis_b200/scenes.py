@@ -24,6 +24,7 @@ class Scene:
     hulls: list = field(default_factory=list)  # float32 (m, 3) point sets
     name: str = "scene"
     joints: np.ndarray | None = None        # JOINT rows: ball joints added after the bodies
+    worlds: np.ndarray | None = None        # sub-world of every body (a batch of independent worlds)
 
     @property
     def body_count(self) -> int:
@@ -37,6 +38,10 @@ class Scene:
             is_hull = colliders["shape"] == R.SHAPE_HULL
             colliders["source"][is_hull] = sources[colliders["source"][is_hull]]
         ids = world.spawn(self.bodies, colliders)
+        if self.worlds is not None:
+            by_id = np.zeros(int(ids.max()) + 1, np.uint32)
+            by_id[ids] = self.worlds
+            world.set_body_worlds(by_id)
         if self.joints is not None and len(self.joints):
             world.add_constraints(ball_joint_records(ids[self.joints["first"]], ids[self.joints["second"]],
                                                      self.joints["anchor_a"], self.joints["anchor_b"]))
@@ -271,10 +276,71 @@ def hanging_chains(chains_x: int = 64, chains_z: int = 64, links: int = 32, seed
     return Scene(bodies, colliders, [], f"hanging_chains_{n}", joints)
 
 
+def batch(parts: list) -> Scene:
+    """Independent scenes as sub-worlds of one batch: body i of part w is in sub-world w."""
+    bodies, colliders, hulls, joints, worlds = [], [], [], [], []
+    body_base = collider_base = 0
+    for index, part in enumerate(parts):
+        b = part.bodies.copy()
+        c = part.colliders.copy()
+        b["collider_first"] += collider_base
+        hull = c["shape"] == R.SHAPE_HULL
+        c["source"][hull] += len(hulls)
+        hulls.extend(part.hulls)
+        if part.joints is not None:
+            j = part.joints.copy()
+            j["first"] += body_base
+            j["second"] += body_base
+            joints.append(j)
+        bodies.append(b)
+        colliders.append(c)
+        worlds.append(np.full(len(b), index, np.uint32))
+        body_base += len(b)
+        collider_base += len(c)
+    return Scene(np.concatenate(bodies), np.concatenate(colliders), hulls, f"batch_{len(parts)}",
+                 np.concatenate(joints) if joints else None, np.concatenate(worlds))
+
+
+def box_lattice(count: int, seed: int, spacing: float = 1.1) -> Scene:
+    """`count` unit cubes (falling_boxes' shape mix and distributions) on the smallest cubic lattice
+    that holds them, above their own ground plane."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(count ** (1.0 / 3.0) - 1e-9))
+    idx = np.arange(count)
+    i, j, k = idx % side, (idx // side) % side, idx // (side * side)
+    base = np.stack([(i - (side - 1) / 2) * spacing, 0.6 + j * spacing, (k - (side - 1) / 2) * spacing], axis=1)
+    bodies = R.body_defaults(count)
+    bodies["position"] = (base + rng.uniform(-0.05, 0.05, size=(count, 3))).astype(np.float32)
+    bodies["orientation"] = yaw_quaternions(rng.uniform(0.0, 2 * np.pi, count))
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(count)
+    colliders["shape"] = R.SHAPE_CUBOID
+    colliders["half_extents"] = 0.5
+    colliders["friction"] = 0.5
+    colliders["restitution"] = 0.0
+    bodies, colliders = _ground(bodies, colliders, 0.0, 0.5, 0.0)
+    return Scene(bodies, colliders, [], f"box_lattice_{count}")
+
+
+def batched_world_parts(worlds: int = 4096, seed: int = 4, smallest: int = 16, largest: int = 2048) -> list:
+    """`worlds` independent box lattices, each on its own ground plane, whose body counts are drawn
+    log-uniform in [smallest, largest]."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(smallest), np.log(largest), worlds)).astype(np.int64)
+    return [box_lattice(int(n), seed * 100003 + w) for w, n in enumerate(counts)]
+
+
+def batched_worlds(worlds: int = 4096, seed: int = 4) -> Scene:
+    """batched_world_parts as one batch (one sub-world each); 4,096 worlds hold about 1.76M bodies."""
+    return batch(batched_world_parts(worlds, seed))
+
+
 WORKLOADS = {
     "falling_boxes_1000": lambda: falling_boxes(seed=0),
     "mixed_pile_32768": lambda: mixed_pile(side=32, seed=1),
     "mixed_pile_262144": lambda: mixed_pile(side=64, seed=1),
     "hanging_chains_8192": lambda: hanging_chains(16, 16, 32),
     "hanging_chains_131072": lambda: hanging_chains(64, 64, 32),
+    "batched_worlds_256": lambda: batched_worlds(256),
+    "batched_worlds_4096": lambda: batched_worlds(4096),
 }

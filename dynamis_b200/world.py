@@ -107,12 +107,22 @@ class World:
                                          ptr(vertices)))
         scene = {"states": states, "descs": descs, "colliders": colliders, "owners": owners, "sources": sources,
                  "vertices": vertices, "dynamic": s["dynamic"]}
+        body_world = np.zeros(s["bodies"], np.uint32)
+        self._check(lib.dyn_export_body_worlds(self._h, ptr(body_world)))
+        if body_world.any():
+            scene["body_world"] = body_world
         m = self.constraint_count()
         if m:
             jd, jr, jt = np.zeros(m, R.CONSTRAINT_DESCRIPTOR), np.zeros(m, R.CONSTRAINT_ROWS), np.zeros(m, R.CONSTRAINT_RUNTIME)
             self._check(lib.dyn_export_constraints(self._h, ptr(jd), ptr(jr), ptr(jt)))
             scene.update(constraint_descs=jd, constraint_rows=jr, constraint_runtime=jt)
         return scene
+
+    # ---- batched worlds ----
+    def set_body_worlds(self, world_of_body) -> None:
+        """Puts every body (indexed by body id) in a sub-world; sub-worlds never interact."""
+        arr = np.ascontiguousarray(world_of_body, np.uint32)
+        self._check(lib.dyn_set_body_worlds(self._h, ptr(arr), len(arr)))
 
     # ---- constraints ----
     def add_ball_joint(self, first_body: int, second_body: int, anchor_a, anchor_b) -> int:

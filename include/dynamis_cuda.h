@@ -199,6 +199,16 @@ DYN_API dyn_status dyn_stage_timings(dyn_world* world, float* ms, uint32_t n);
 DYN_API dyn_status dyn_radix_sort(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
                                   uint32_t major_digits, uint32_t minor_digits);
 
+/* ---- batched worlds ----
+ * Thousands of independent worlds stepped by one dyn_step: every body id gets a sub-world
+ * (world_of_body[id], n = the number of bodies spawned or uploaded), and bodies of different
+ * sub-worlds never pair, contact or join an island, so each sub-world steps exactly as it would
+ * alone. Sub-world 0 is the default. No counterpart in the reference, which steps one world per
+ * World::step; this is the batched-worlds configuration of the benchmark. */
+DYN_API dyn_status dyn_set_body_worlds(dyn_world* world, const uint32_t* world_of_body, uint32_t n);
+/* The sub-world of every row (dyn_export_scene's row order), for a checker. */
+DYN_API dyn_status dyn_export_body_worlds(const dyn_world* world, uint32_t* rows_out);
+
 /* ---- constraints: ball joints (row a11 of the path) ----
  * World::add_constraint(first, second, ConstraintDesc::ball(anchor_a, anchor_b))
  * (crates/dynamis-world/src/constraint.rs:121, crates/dynamis-model/src/constraint.rs:568): a ball joint

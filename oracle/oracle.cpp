@@ -91,6 +91,11 @@ inline uint32_t cell_hash(I3 c) {
     return (x ^ y ^ z ^ (x << 7) ^ (y >> 3) ^ (z << 11)) & DYN_CELL_HASH_MASK;
 }
 inline uint32_t cell_key(uint32_t level, I3 c) { return (level << DYN_LEVEL_KEY_SHIFT) | cell_hash(c); }
+// Batched worlds (no counterpart in the reference): a row's sub-world is mixed into its cells'
+// hash; sub-world 0 leaves the key unchanged.
+inline uint32_t cell_key_in(uint32_t level, I3 c, uint32_t world) {
+    return (level << DYN_LEVEL_KEY_SHIFT) | ((cell_hash(c) ^ (world * 0x2545F491u)) & DYN_CELL_HASH_MASK);
+}
 inline float level_cell_size(uint32_t level, float cs) { return cs * (float)(1u << level); }
 inline uint32_t shape_levels(const Aabb& box, float base) {
     uint32_t level = 0;
@@ -189,6 +194,8 @@ struct OracleWorld {
     std::vector<dyn_constraint_rows_record> joint_rows;
     std::vector<dyn_constraint_runtime_record> joint_runtime;
     std::vector<uint32_t> plan_rows, plan_layers, plan_components;
+    std::vector<uint32_t> body_world;  // sub-world of every row (empty: one world)
+    uint32_t world_of(uint32_t row) const { return body_world.empty() ? 0u : body_world[row]; }
 };
 
 namespace {
@@ -327,7 +334,7 @@ void emit_entries(OracleWorld& w) {
                 if (offset == 0u) info |= DYN_ENTRY_PRIMARY;
                 uint32_t slot = (uint32_t)w.entries.size();
                 w.entries.push_back(Entry{box, owner, info});
-                keys.push_back(cell_key(level, coord));
+                keys.push_back(cell_key_in(level, coord, w.world_of(owner)));
                 order.push_back(slot);
                 if (!moves) {
                     w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES] += 1;
@@ -363,6 +370,7 @@ void emit_pair(PairSink& sink, uint32_t first, uint32_t second) {
     if (ka != DYN_ENTRY_KIND_COLLIDER || kb != DYN_ENTRY_KIND_COLLIDER) return;
     if (first == second || a.group == b.group) return;
     if ((a.info & DYN_ENTRY_MOBILE) == 0u && (b.info & DYN_ENTRY_MOBILE) == 0u) return;
+    if (sink.w->world_of(a.group) != sink.w->world_of(b.group)) return;
     uint32_t slot = sink.w->counters[DYN_COUNTER_PAIRS]++;
     if (slot < sink.w->pair_capacity) {
         uint32_t ia = a.info & DYN_ENTRY_INDEX_MASK;
@@ -419,7 +427,7 @@ void broadphase(OracleWorld& w) {
             for (uint32_t ordinal = 0; ordinal < count; ++ordinal) {
                 I3 cell = grid_cell_at(cells, ordinal);
                 uint32_t first, last;
-                key_range(w, cell_key(link, cell), &first, &last);
+                key_range(w, cell_key_in(link, cell, w.world_of(e.group)), &first, &last);
                 for (uint32_t entry = first; entry < last; ++entry) {
                     uint32_t other = w.entry_order[entry];
                     if (other == node) continue;
@@ -442,7 +450,7 @@ void broadphase(OracleWorld& w) {
         float cs = level_cell_size(level, grid);
         I3 cell = entry_cell(e, cs);
         uint32_t first, last;
-        key_range(w, cell_key(level, cell), &first, &last);
+        key_range(w, cell_key_in(level, cell, w.world_of(e.group)), &first, &last);
         for (uint32_t entry = first; entry < last; ++entry) {
             if (entry == index) continue;
             uint32_t other = w.entry_order[entry];
@@ -1564,6 +1572,10 @@ uint32_t orc_set_constraints(OracleWorld* w, const dyn_constraint_descriptor_rec
     plan_joint_order(*w);
     w->params.constraint_count = m;
     return 1;
+}
+
+void orc_set_body_worlds(OracleWorld* w, const uint32_t* rows, uint32_t n) {
+    w->body_world.assign(rows, rows + n);
 }
 
 uint32_t orc_constraints(const OracleWorld* w, dyn_constraint_runtime_record* out) {

@@ -49,6 +49,7 @@ def lib() -> ctypes.CDLL:
         _lib.orc_constraints.restype = U32
         _lib.orc_constraints.argtypes = [P, P]
         _lib.orc_joint_plan.argtypes = [P, P, P, P, P]
+        _lib.orc_set_body_worlds.argtypes = [P, P, U32]
     return _lib
 
 
@@ -70,6 +71,8 @@ class OracleWorld:
                                      pair_capacity, contact_capacity)
         if not self._h:
             raise ValueError("oracle refused the scene: collider owners or hull sources out of range")
+        if "body_world" in s:
+            L.orc_set_body_worlds(self._h, _p(s["body_world"]), len(s["body_world"]))
         if "constraint_descs" in s:
             m = len(s["constraint_descs"])
             if not L.orc_set_constraints(self._h, _p(s["constraint_descs"]), _p(s["constraint_rows"]),
