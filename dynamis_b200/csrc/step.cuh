@@ -357,8 +357,11 @@ __device__ __forceinline__ uint32_t cell_find(const DeviceWorld& w, uint32_t liv
     return live;
 }
 
-// One thread per sorted entry: coarse-level links of a primary entry, then same-cell mates.
-__global__ void k_pairs(DeviceWorld w) {
+// Pair emission in two kernels whose warps each do one kind of work: the coarse-level links of
+// every collider's primary entry (level_links.wgsl:6-65; one thread per collider, whose primary entry
+// is its first emitted slot), and the same-cell mates of every sorted entry (cell_pairs.wgsl:6-50).
+// The pair set does not depend on which kernel emits a pair first: the list is sorted afterwards.
+__global__ void k_pairs_coarse(DeviceWorld w) {
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
     const float grid = base_cell(w);
     const uint32_t occupied =
@@ -366,47 +369,60 @@ __global__ void k_pairs(DeviceWorld w) {
     const bool coarse_active = w.counters[DYN_COUNTER_COARSE_ACTIVE] != 0u;
     const uint32_t bits = cell_table_bits(w, live);
     const bool overflow = w.ctl[CTL_CELL_OVERFLOW] != 0u;
+    GRID_STRIDE(i, w.k) {
+        if (w.entry_count[i] == 0u) continue;
+        const uint32_t node = w.entry_offset[i];
+        if (node >= live) continue;
+        GEntry e = load_entry(w, node);
+        if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
+        if ((e.info & DYN_ENTRY_PRIMARY) == 0u) continue;
+        const bool awake = entry_awake(w, e);
+        if (!(awake || coarse_active)) continue;
+        const uint32_t level = w.c_level[e.info & DYN_ENTRY_INDEX_MASK];
+        const uint32_t world = w.body_world[e.group];
+        uint32_t coarser = occupied & ~((1u << min(level + 1u, 31u)) - 1u);
+        while (coarser != 0u) {
+            uint32_t link = 31u - __clz(coarser);
+            coarser &= ~(1u << link);
+            float cs = level_size(link, grid);
+            I3 lo = floor_div(e.mn, cs), hi = floor_div(e.mx, cs);
+            // A box spans at most two cells per axis at any level coarser than its own; a wider
+            // span only comes from a non-finite box, whose walk is cut short and counted.
+            if ((long long)hi.x - lo.x > 3 || (long long)hi.y - lo.y > 3 || (long long)hi.z - lo.z > 3 || hi.x < lo.x ||
+                hi.y < lo.y || hi.z < lo.z) {
+                add_counter(&w.counters[DYN_COUNTER_ENTRY_FAULTS], 1u);
+                continue;
+            }
+            for (int x = lo.x; x <= hi.x; ++x)
+                for (int y = lo.y; y <= hi.y; ++y)
+                    for (int z = lo.z; z <= hi.z; ++z) {
+                        I3 cell = I3{x, y, z};
+                        uint32_t key = cell_key_in(link, cell, world);
+                        uint32_t j = cell_find(w, live, bits, overflow, key);
+                        for (; j < live && __ldg(w.ekey + j) == key; ++j) {
+                            uint32_t other = w.eval[j];
+                            if (other == node) continue;
+                            GEntry o = load_entry(w, other);
+                            if (!awake && !entry_awake(w, o)) continue;
+                            if (!overlaps(e, o)) continue;
+                            if (!same_cell(entry_cell(o, cs), cell)) continue;
+                            if (!overlap_cell_is(e, o, cs, cell)) continue;
+                            emit_pair(w, e, o, false);
+                        }
+                    }
+        }
+    }
+}
+
+__global__ void k_pairs_cell(DeviceWorld w) {
+    const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
+    const float grid = base_cell(w);
     GRID_STRIDE(index, live) {
         uint32_t node = w.eval[index];
         GEntry e = load_entry(w, node);
         if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
-        bool awake = entry_awake(w, e);
+        if (!entry_awake(w, e)) continue;
         uint32_t level = w.c_level[e.info & DYN_ENTRY_INDEX_MASK];
-        if ((e.info & DYN_ENTRY_PRIMARY) != 0u && (awake || coarse_active)) {
-            const uint32_t world = w.body_world[e.group];
-            uint32_t coarser = occupied & ~((1u << min(level + 1u, 31u)) - 1u);
-            while (coarser != 0u) {
-                uint32_t link = 31u - __clz(coarser);
-                coarser &= ~(1u << link);
-                float cs = level_size(link, grid);
-                I3 lo = floor_div(e.mn, cs), hi = floor_div(e.mx, cs);
-                // A box spans at most two cells per axis at any level coarser than its own; a
-                // wider span only comes from a non-finite box, whose walk is cut short and counted.
-                if ((long long)hi.x - lo.x > 3 || (long long)hi.y - lo.y > 3 || (long long)hi.z - lo.z > 3 || hi.x < lo.x ||
-                    hi.y < lo.y || hi.z < lo.z) {
-                    add_counter(&w.counters[DYN_COUNTER_ENTRY_FAULTS], 1u);
-                    continue;
-                }
-                for (int x = lo.x; x <= hi.x; ++x)
-                    for (int y = lo.y; y <= hi.y; ++y)
-                        for (int z = lo.z; z <= hi.z; ++z) {
-                            I3 cell = I3{x, y, z};
-                            uint32_t key = cell_key_in(link, cell, world);
-                            uint32_t j = cell_find(w, live, bits, overflow, key);
-                            for (; j < live && __ldg(w.ekey + j) == key; ++j) {
-                                uint32_t other = w.eval[j];
-                                if (other == node) continue;
-                                GEntry o = load_entry(w, other);
-                                if (!awake && !entry_awake(w, o)) continue;
-                                if (!overlaps(e, o)) continue;
-                                if (!same_cell(entry_cell(o, cs), cell)) continue;
-                                if (!overlap_cell_is(e, o, cs, cell)) continue;
-                                emit_pair(w, e, o, false);
-                            }
-                        }
-            }
-        }
-        if (!awake) continue;
         float cs = level_size(level, grid);
         I3 cell = entry_cell(e, cs);
         uint32_t key = __ldg(w.ekey + index);

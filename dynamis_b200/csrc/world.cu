@@ -558,7 +558,8 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_PAIRS);
     k_cell_clear<<<blocks_for(1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
     k_cell_insert<<<blocks_for(E, 256), 256, 0, s>>>(dw);
-    k_pairs<<<blocks_for(E, 256), 256, 0, s>>>(dw);
+    k_pairs_coarse<<<blocks_for(K, 128), 128, 0, s>>>(dw);
+    k_pairs_cell<<<blocks_for(E, 256), 256, 0, s>>>(dw);
     mark(ST_PAIR_SORT);
     uint32_t words = key_words(std::max(dw.k, 1u));
     record_sort(d, s, dw.pmaj, dw.pmin, nullptr, dw.pmaj_alt, dw.pmin_alt, nullptr, dw.counters + DYN_COUNTER_PAIRS, 0, P,
@@ -567,8 +568,8 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
     k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
-    // persistent: lanes draw pairs from a ticket, so four blocks per SM keep every SM busy
-    k_convex_gjk<<<148u * 4u, 128, 0, s>>>(dw, p);
+    // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
+    k_convex_gjk<<<148u * 6u, 128, 0, s>>>(dw, p);
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     mark(ST_COMPACT);
