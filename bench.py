@@ -189,10 +189,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     ms = start.elapsed_time(end)
     log(f"timed {args.steps} steps: {ms / args.steps:.3f} ms/step")
     log("counts " + str({k: int(world.measured()[R.COUNTER[k]]) for k in ("ENTRIES", "PAIRS", "CONTACTS", "LIVE")}))
+    ms = max_over_ranks(ms, dist, f"cuda:{local_rank}")
     if dist:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     m = world.measured()
     counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
@@ -231,20 +229,17 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         world._check(lib.dyn_download_states(world._h, ptr(states_out), bodies))
         states_in, states_out = states_out, states_in  # the result feeds the next step
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
     log(f"e2e {e2e_steps} steps: {e2e_s / e2e_steps * 1e3:.3f} ms/step")
     result = {
-        "metric": METRIC, "value": bodies * args.steps * world_size / (ms * 1e-3), "unit": UNIT,
+        "metric": METRIC, "value": whole_job_rate(bodies * args.steps, world_size, ms * 1e-3), "unit": UNIT,
         "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "bodies": bodies, "setup_steps": args.setup, "dt": DT,
                    "parallelism": f"replicas{world_size}" if world_size > 1 else "single-world",
                    "l2": "working set > 126 MB L2 (no flush between steps)", "counts_last_step": counts,
                    "scene_build_s": round(build_s, 2)},
-        "e2e": {"value": bodies * e2e_steps * world_size / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bodies * R.BODY_STATE.itemsize,
+        "e2e": {"value": whole_job_rate(bodies * e2e_steps, world_size, e2e_s), "unit": UNIT, "h2d_bytes_per_step": bodies * R.BODY_STATE.itemsize,
                 "d2h_bytes_per_step": bodies * R.BODY_STATE.itemsize},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"],
@@ -261,6 +256,22 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
     world.close()
     return result
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of every rank's value: a replicated job ends when its slowest replica does."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world_size: int, seconds: float) -> float:
+    """Units all ranks processed per second of the slowest rank."""
+    return units_per_rank * world_size / seconds
 
 
 def loop_baseline(args, dt: float, batch_ms: float, device: int, sample_every: int = 16) -> dict:
