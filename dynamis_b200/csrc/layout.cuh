@@ -43,7 +43,7 @@ struct ContactSet {
 struct SolverRows {
     float4* arm_a;     // contact point - first body's world centre of mass, normal effective mass
     float4* arm_b;     // contact point - second body's world centre of mass, unsplit normal mass
-    float2* masses;    // tangent-1 and tangent-2 effective masses
+    float4* masses;    // tangent-1 and tangent-2 effective masses, depth, target speed
     float4* tangent1;  // [cap] tangent 1, twist mass
     float4* tangent2;  // [cap] tangent 2, 0
 };

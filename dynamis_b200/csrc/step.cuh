@@ -1269,7 +1269,7 @@ __global__ void k_solve_prepare(DeviceWorld w) {
             float t2_mass = momentum_mass_arms(b.sf, b.ss, ra[pi], rb[pi], t2) * count_f;
             sr.arm_a[o] = mk4(ra[pi], normal_mass);
             sr.arm_b[o] = mk4(rb[pi], truth);
-            sr.masses[o] = make_float2(t1_mass, t2_mass);
+            sr.masses[o] = make_float4(t1_mass, t2_mass, w.cur.la[o].w, w.cur.lb[o].w);
         }
         float twist_mass = dot(normal, dbody_iinv(b.sf, normal)) + dot(normal, dbody_iinv(b.ss, normal));
         sr.tangent1[i] = mk4(t1, twist_mass);
@@ -1338,11 +1338,11 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
     for (uint32_t pi = 0; pi < pc; ++pi) {
         size_t o = (size_t)pi * cap + i;
         float4 a4 = sr.arm_a[o], b4 = sr.arm_b[o];
-        float2 m2 = sr.masses[o];
+        float4 m2 = sr.masses[o];
         ra[pi] = xyz(a4);
         rb[pi] = xyz(b4);
         float normal_mass = a4.w, truth = b4.w;
-        float depth = w.cur.la[o].w, target = w.cur.lb[o].w;
+        float depth = m2.z, target = m2.w;
         float an = acc[pi].x, at1 = acc[pi].y, at2 = acc[pi].z;
         f3 rel = point_velocity_arm(ps, rb[pi]) - point_velocity_arm(pf, ra[pi]);
         float normal_speed = dot(rel, normal);
