@@ -660,10 +660,16 @@ struct GjkLane {
     uint32_t state, index, count, iter, probe, triples;
     float tiny, margin, dist, best;
     f3 pa, pb, normal, best_normal;
-    SPt s[4];
+    SPt* s;  // the simplex (4 points), in this lane's slice of shared memory
     SRes cl;
     WShape a, b;
 };
+// Each lane's simplex lives in shared memory at an odd word stride (37 words for 36 used), so the
+// lanes of a warp reading the same point land in different banks; held in the lane's registers it
+// would be indexed by the simplex size and spill to local memory.
+constexpr uint32_t kGjkThreads = 128;
+constexpr uint32_t kSimplexStride = 37;
+static_assert(sizeof(SPt) * 4 <= kSimplexStride * sizeof(float), "a lane's simplex fits its slice");
 
 __device__ __forceinline__ f3 probe_direction(const GjkLane& L, uint32_t k) {
     const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
@@ -724,10 +730,12 @@ __device__ __forceinline__ void gjk_separated(GjkLane& L) {
     probe_begin(L);
 }
 
-__global__ void __launch_bounds__(128) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
+__global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
+    __shared__ float simplex_slices[kGjkThreads * kSimplexStride];
     const uint32_t count = min(w.ctl[CTL_LIST0 + PC_CONVEX], w.p_cap);
     const uint32_t* list = w.np_list + (size_t)PC_CONVEX * w.p_cap;
     GjkLane L;
+    L.s = reinterpret_cast<SPt*>(simplex_slices + threadIdx.x * kSimplexStride);
     L.state = GS_IDLE;
     for (;;) {
         if (L.state == GS_IDLE) {
@@ -775,16 +783,15 @@ __global__ void __launch_bounds__(128) k_convex_gjk(DeviceWorld w, dyn_step_para
                 gjk_separated(L);
                 continue;
             }
-            SPt kept[4];
+            // simplex_reduce: keep the points with weight, in order (a stable in-place compaction)
             uint32_t kc = 0;
             for (uint32_t i = 0; i < 4; ++i) {
-                if (L.cl.lam[i] > 1e-6f) kept[kc++] = L.s[i];
+                if (L.cl.lam[i] > 1e-6f) {
+                    if (kc != i) L.s[kc] = L.s[i];
+                    ++kc;
+                }
             }
-            if (kc == 0u) {
-                kept[0] = L.s[0];
-                kc = 1;
-            }
-            for (uint32_t i = 0; i < kc; ++i) L.s[i] = kept[i];
+            if (kc == 0u) kc = 1;  // no weight: keep the first point
             L.count = kc;
             const float span = shape_scale(L.b);
             const float tol = (1e-5f * span) * (1e-5f * span);
