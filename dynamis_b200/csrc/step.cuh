@@ -1336,13 +1336,15 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
     f3 ra[4], rb[4];
     float4 acc[4];
     float normal_total = 0.0f;
-    for (uint32_t pi = 0; pi < pc; ++pi) {
+    #pragma unroll
+    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) {
         size_t o = (size_t)pi * cap + i;
         acc[pi] = w.cur.acc[o];
         normal_total = normal_total + wmax(acc[pi].x, 0.0f);
     }
     f3 impulses[4];
-    for (uint32_t pi = 0; pi < pc; ++pi) {
+    #pragma unroll
+    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) {
         size_t o = (size_t)pi * cap + i;
         float4 a4 = sr.arm_a[o], b4 = sr.arm_b[o];
         float4 m2 = sr.masses[o];
@@ -1379,7 +1381,8 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
         at2 = next_t2;
         acc[pi] = make_float4(an, at1, at2, acc[pi].w);
     }
-    for (uint32_t pi = 0; pi < pc; ++pi) pair_impulse_arms(&first, &second, ra[pi], rb[pi], impulses[pi]);
+    #pragma unroll
+    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) pair_impulse_arms(&first, &second, ra[pi], rb[pi], impulses[pi]);
     f3 rel_spin = second.angular_velocity - first.angular_velocity;
     f3 planar = rel_spin - normal * dot(rel_spin, normal);
     float planar_len = length(planar);
@@ -1402,7 +1405,8 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
             second.angular_velocity = second.angular_velocity + dbody_iinv(second, normal * applied);
         }
     }
-    for (uint32_t pi = 0; pi < pc; ++pi) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
+    #pragma unroll
+    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
     f3 da = first.velocity - pf.velocity, sa = first.angular_velocity - pf.angular_velocity;
     f3 db = second.velocity - ps.velocity, sb = second.angular_velocity - ps.angular_velocity;
     if (!dbody_inert(pf)) accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
@@ -1414,7 +1418,7 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
                     (uint32_t)solver_word(wmax(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE));
     }
 }
-__global__ void __launch_bounds__(128) k_solve(DeviceWorld w, dyn_step_params p) {
+__global__ void __launch_bounds__(128, 4) k_solve(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     const bool residual = w.ctl[CTL_ROUNDS] == p.solve_iterations;
     GRID_STRIDE(i, count) solve_block(w, p, i, residual);
