@@ -101,7 +101,7 @@ class ClockSampler:
 # DRAM bytes the narrowphase stage moved per candidate pair, measured with ncu on the formed
 # 32,768-body pile (profiles/narrowphase_traffic_mixed_pile_32768.md); the full-size workload is too
 # large for a multi-metric capture, and the traffic grows with the pair count.
-NARROWPHASE_DRAM_BYTES_PER_PAIR = 328.0
+NARROWPHASE_DRAM_BYTES_PER_PAIR = 250.0
 
 
 def stage_bytes(stage: str, m: dict, params: dict) -> float:
