@@ -55,6 +55,7 @@ SIGNATURES = {
     "dyn_radix_sort": (I32, [P, P, P, P, U32, U32, U32]),
     "dyn_radix_sort_static": (I32, [P, P, P, U32, U32, U32, P]),
     "dyn_set_body_worlds": (I32, [P, P, U32]),
+    "dyn_edit_bodies": (I32, [P, P, P, U32]),
     "dyn_export_body_worlds": (I32, [P, P]),
     "dyn_add_ball_joint": (I32, [P, U32, U32, P, P, PU32]),
     "dyn_add_constraints": (I32, [P, P, U32, PU32]),

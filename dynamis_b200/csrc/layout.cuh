@@ -156,6 +156,10 @@ struct DeviceWorld {
     uint4* jgroups;     // warp groups: first component, components, lanes each, deepest stack
     uint2* jfilter;     // sorted (lower row, higher row) of the joints that disable collisions
     uint32_t* jfilter_joint;
+    // queued body edits of this step (runs of one row each; *edit_count runs)
+    const dyn_body_edit_record* edits;
+    const uint4* edit_runs;
+    uint32_t* edit_count;
     // counters (reference slots) and control words
     uint32_t* counters;
     uint32_t* ctl;

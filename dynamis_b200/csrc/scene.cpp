@@ -1000,6 +1000,19 @@ DYN_API dyn_status dyn_add_constraints(dyn_world* w, const dyn_constraint_descri
     return DYN_OK;
 }
 
+// ---- body commands ----
+DYN_API dyn_status dyn_edit_bodies(dyn_world* w, const uint32_t* body_ids, const dyn_body_edit_record* edits, uint32_t n) {
+    if (!w || (n && (!body_ids || !edits))) return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: null argument");
+    uint32_t ids = (uint32_t)std::max(w->spawn_states.size(), w->row_of_id.size());
+    for (uint32_t i = 0; i < n; ++i) {
+        if (body_ids[i] >= ids) return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: unknown body id");
+        if (edits[i].kind > DYN_EDIT_ANGULAR_IMPULSE) return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: unknown edit kind");
+    }
+    w->edit_ids.insert(w->edit_ids.end(), body_ids, body_ids + n);
+    w->edits.insert(w->edits.end(), edits, edits + n);
+    return DYN_OK;
+}
+
 // ---- batched worlds ----
 DYN_API dyn_status dyn_set_body_worlds(dyn_world* w, const uint32_t* world_of_body, uint32_t n) {
     if (!w || (n && !world_of_body)) return fail(w, DYN_ERR_INVALID, "dyn_set_body_worlds: null argument");

@@ -60,10 +60,126 @@ __global__ void k_reset(DeviceWorld w) {
 // clear_inputs.wgsl, activity.wgsl (all rows); begin_step.wgsl, island_init.wgsl (dynamic rows);
 // solver_reset.wgsl (all rows). Folding them into one pass changes nothing: none of them reads
 // what another writes.
-__global__ void k_begin(DeviceWorld w, dyn_step_params p) {
+// clear_inputs.wgsl on its own, for steps that apply body edits between it and the rest.
+__global__ void k_clear_inputs(DeviceWorld w) {
     GRID_STRIDE(i, w.n) {
         w.force[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         w.torque[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// body_edits.wgsl: the queued commands of one body row, in order, after the inputs are cleared and
+// before anything reads the rows.
+__device__ __forceinline__ void edit_disturbs(const DeviceWorld& w, uint32_t row, uint32_t* sleeping, float* timer, bool disturbed) {
+    if (*sleeping != 0u) {
+        atomicAdd(&w.counters[DYN_COUNTER_WOKE], 1u);
+        atomicOr(&w.wake_flags[row], 1u);
+    } else if (disturbed) {
+        atomicOr(&w.wake_flags[row], 1u);
+    }
+    *sleeping = 0u;
+    *timer = 0.0f;
+}
+__global__ void k_body_edits(DeviceWorld w) {
+    const uint32_t runs = *w.edit_count;
+    GRID_STRIDE(r, runs) {
+        const uint4 run = w.edit_runs[r];
+        const uint32_t row = run.x;
+        if (row >= w.n || run.z == 0u) continue;
+        BodyHot& h = w.hot[row];
+        f3 position = xyz(h.pos), velocity = xyz(h.vel), angular = xyz(h.ang);
+        float4 orientation = h.rot;
+        f3 prev_position = xyz(w.prev_pos[row]);
+        float4 prev_orientation = w.prev_rot[row];
+        f3 force = xyz(w.force[row]), torque = xyz(w.torque[row]);
+        uint32_t sleeping = h.aux.x;
+        float timer = w.sleep_timer[row];
+        const float im = h.pos.w;
+        const uint32_t flags = h.aux.y;
+        const f3 com_local = xyz(h.com);
+        const float4 ii0 = h.ii0;
+        const float2 ii1 = make_float2(h.ii1.x, h.ii1.y);
+        for (uint32_t k = 0; k < run.z; ++k) {
+            const dyn_body_edit_record& e = w.edits[run.y + k];
+            const f3 ev = mk3(e.state.velocity[0], e.state.velocity[1], e.state.velocity[2]);
+            const f3 ep = mk3(e.state.position[0], e.state.position[1], e.state.position[2]);
+            if (e.kind == DYN_EDIT_PATCH) {
+                if (e.mask & DYN_PATCH_POSITION) {
+                    position = ep;
+                    prev_position = ep;
+                }
+                if (e.mask & DYN_PATCH_ORIENTATION) {
+                    orientation = make_float4(e.state.orientation[0], e.state.orientation[1], e.state.orientation[2],
+                                              e.state.orientation[3]);
+                    prev_orientation = orientation;
+                }
+                if (e.mask & DYN_PATCH_VELOCITY) velocity = ev;
+                if (e.mask & DYN_PATCH_ANGULAR_VELOCITY)
+                    angular = mk3(e.state.angular_velocity[0], e.state.angular_velocity[1], e.state.angular_velocity[2]);
+                const bool teleport = (e.mask & (DYN_PATCH_POSITION | DYN_PATCH_ORIENTATION)) != 0u;
+                edit_disturbs(w, row, &sleeping, &timer, teleport || !simulates(im, flags));
+            } else if (e.kind == DYN_EDIT_FORCE) {
+                force = force + mk3(e.state.force[0], e.state.force[1], e.state.force[2]);
+                edit_disturbs(w, row, &sleeping, &timer, false);
+            } else if (e.kind == DYN_EDIT_FORCE_AT_POINT) {
+                const f3 f = mk3(e.state.force[0], e.state.force[1], e.state.force[2]);
+                force = force + f;
+                torque = torque + cross(ep - (position + quat_rotate(orientation, com_local)), f);
+                edit_disturbs(w, row, &sleeping, &timer, false);
+            } else if (e.kind == DYN_EDIT_TORQUE) {
+                torque = torque + mk3(e.state.torque[0], e.state.torque[1], e.state.torque[2]);
+                edit_disturbs(w, row, &sleeping, &timer, false);
+            } else if (e.kind == DYN_EDIT_IMPULSE) {
+                velocity = velocity + ev * im;
+                edit_disturbs(w, row, &sleeping, &timer, false);
+            } else if (e.kind == DYN_EDIT_IMPULSE_AT_POINT) {
+                velocity = velocity + ev * im;
+                const f3 lever = ep - (position + quat_rotate(orientation, com_local));
+                angular = angular + inv_inertia_world(ii0, ii1, orientation, cross(lever, ev));
+                edit_disturbs(w, row, &sleeping, &timer, false);
+            } else if (e.kind == DYN_EDIT_ANGULAR_IMPULSE) {
+                angular = angular + inv_inertia_world(ii0, ii1, orientation,
+                                                      mk3(e.state.angular_velocity[0], e.state.angular_velocity[1],
+                                                          e.state.angular_velocity[2]));
+                edit_disturbs(w, row, &sleeping, &timer, false);
+            } else if (e.kind == DYN_EDIT_SLEEP) {
+                if (sleeping == 0u) atomicAdd(&w.counters[DYN_COUNTER_SLEPT], 1u);
+                velocity = s3(0.0f);  // freeze_body (core.wgsl:218-227)
+                angular = s3(0.0f);
+                force = s3(0.0f);
+                torque = s3(0.0f);
+                prev_position = position;
+                prev_orientation = orientation;
+                timer = 0.0f;
+                sleeping = 1u;
+                atomicExch(&w.wake_flags[row], 0u);
+            } else if (e.kind == DYN_EDIT_WAKE) {
+                if (sleeping != 0u) atomicAdd(&w.counters[DYN_COUNTER_WOKE], 1u);
+                timer = 0.0f;
+                sleeping = 0u;
+                atomicOr(&w.wake_flags[row], 1u);
+            }
+        }
+        h.pos = mk4(position, im);
+        h.rot = orientation;
+        h.vel = mk4(velocity, 0.0f);
+        h.ang = mk4(angular, 0.0f);
+        h.aux.x = sleeping;
+        w.prev_pos[row] = mk4(prev_position, 0.0f);
+        w.prev_rot[row] = prev_orientation;
+        w.force[row] = mk4(force, 0.0f);
+        w.torque[row] = mk4(torque, 0.0f);
+        w.sleep_timer[row] = timer;
+    }
+}
+
+template <bool kClearInputs>
+__global__ void k_begin(DeviceWorld w, dyn_step_params p) {
+    GRID_STRIDE(i, w.n) {
+        if (kClearInputs) {
+            w.force[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            w.torque[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
         BodyHot& h = w.hot[i];
         float im = h.pos.w;
         uint32_t flags = h.aux.y;

@@ -63,6 +63,13 @@ struct DeviceState {
     uint32_t sort_alt_cap = 0;
     dyn_body_state_record* staging = nullptr;  // n_cap ABI state records
     std::vector<void*> joint_allocs;  // constraint buffers, rebuilt whenever the constraint set changes
+    // body edits: once a world has taken edits its step graph runs k_clear_inputs, k_body_edits and
+    // k_begin<false>; before that, k_begin<true> alone
+    bool edit_graphs = false;
+    bool edits_pending_on_device = false;  // *edit_count is non-zero
+    dyn_body_edit_record* edit_buffer = nullptr;
+    uint4* edit_run_buffer = nullptr;
+    uint32_t edit_capacity = 0;
     // graphs
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     float graph_dt = -1.0f;
@@ -181,6 +188,7 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.wake_flags, N);
         A(dw.row_of_id, N);
         A(dw.body_world, N);
+        A(dw.edit_count, 1);
         A(dw.c_owner, K);
         A(dw.c_kind, K);
         A(dw.c_offset, K);
@@ -546,7 +554,13 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_BEGIN);
     k_reset<<<1, 64, 0, s>>>(dw);
     if (dw.jcount) k_joint_count<<<blocks_for(std::max(dw.jfilter_count, 1u), 256), 256, 0, s>>>(dw);
-    k_begin<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+    if (d->edit_graphs) {
+        k_clear_inputs<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+        k_body_edits<<<blocks_for(std::max(d->edit_capacity, 1u), 128), 128, 0, s>>>(dw);
+        k_begin<false><<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+    } else {
+        k_begin<true><<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+    }
     mark(ST_AABB);
     k_aabb<<<blocks_for(K, 128), 128, 0, s>>>(dw, p);
     mark(ST_ENTRIES);
@@ -617,6 +631,81 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_COUNT);
 }
 
+// The queued body edits as runs of one row each (command order within a row, rows in order of
+// their first edit, as command.rs:157-176 compiles them), onto the device for the next step.
+dyn_status upload_edits(dyn_world* w) {
+    DeviceState* d = w->dev;
+    DeviceWorld& dw = d->dw;
+    const uint32_t n = (uint32_t)w->edits.size();
+    if (n == 0) {
+        if (d->edits_pending_on_device) {
+            DYN_CUDA(cudaMemsetAsync(dw.edit_count, 0, 4, d->stream));
+            d->edits_pending_on_device = false;
+        }
+        return DYN_OK;
+    }
+    std::vector<uint32_t> order;  // edit indices grouped by row
+    std::vector<uint4> runs;
+    {
+        std::vector<uint32_t> rows(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t id = w->edit_ids[i];
+            rows[i] = id < w->row_of_id.size() ? w->row_of_id[id] : DYN_NO_BODY;
+        }
+        std::vector<uint32_t> run_of_row;  // row -> run index + 1
+        std::vector<std::vector<uint32_t>> members;
+        std::vector<uint32_t> run_rows;
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t row = rows[i];
+            if (row == DYN_NO_BODY || row >= w->states.size()) continue;
+            if (run_of_row.size() <= row) run_of_row.resize(row + 1, 0u);
+            if (run_of_row[row] == 0u) {
+                members.emplace_back();
+                run_rows.push_back(row);
+                run_of_row[row] = (uint32_t)members.size();
+            }
+            members[run_of_row[row] - 1].push_back(i);
+        }
+        for (size_t r = 0; r < members.size(); ++r) {
+            runs.push_back(make_uint4(run_rows[r], (uint32_t)order.size(), (uint32_t)members[r].size(), 0u));
+            order.insert(order.end(), members[r].begin(), members[r].end());
+        }
+    }
+    std::vector<dyn_body_edit_record> grouped(order.size());
+    for (size_t i = 0; i < order.size(); ++i) grouped[i] = w->edits[order[i]];
+    w->edits.clear();
+    w->edit_ids.clear();
+    const uint32_t need = std::max((uint32_t)grouped.size(), (uint32_t)runs.size());
+    if (need > d->edit_capacity || !d->edit_graphs) {
+        uint32_t cap = std::max(need, std::max(2 * d->edit_capacity, 256u));
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        if (d->edit_buffer) cudaFree(d->edit_buffer);
+        if (d->edit_run_buffer) cudaFree(d->edit_run_buffer);
+        d->edit_buffer = nullptr;
+        d->edit_run_buffer = nullptr;
+        DYN_CUDA(cudaMalloc(&d->edit_buffer, (size_t)cap * sizeof(dyn_body_edit_record)));
+        DYN_CUDA(cudaMalloc(&d->edit_run_buffer, (size_t)cap * sizeof(uint4)));
+        d->edit_capacity = cap;
+        dw.edits = d->edit_buffer;
+        dw.edit_runs = d->edit_run_buffer;
+        d->edit_graphs = true;
+        release_graphs(d);  // the step graph gains the edit kernels and the new buffers
+    }
+    uint32_t count = (uint32_t)runs.size();
+    if (!grouped.empty()) {
+        DYN_CUDA(cudaMemcpyAsync(d->edit_buffer, grouped.data(), grouped.size() * sizeof(dyn_body_edit_record),
+                                 cudaMemcpyHostToDevice, d->stream));
+    }
+    if (count) {
+        DYN_CUDA(cudaMemcpyAsync(d->edit_run_buffer, runs.data(), runs.size() * sizeof(uint4), cudaMemcpyHostToDevice,
+                                 d->stream));
+    }
+    DYN_CUDA(cudaMemcpyAsync(dw.edit_count, &count, 4, cudaMemcpyHostToDevice, d->stream));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));  // the host vectors above go out of scope
+    d->edits_pending_on_device = count != 0;
+    return DYN_OK;
+}
+
 dyn_status prepare_step(dyn_world* w, float dt) {
     if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(w, DYN_ERR_INVALID, "a step timestep must be positive");
     bool fresh = !w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows) || w->scene_dirty;
@@ -642,6 +731,7 @@ dyn_status prepare_step(dyn_world* w, float dt) {
     }
     if (w->states.empty()) return fail(w, DYN_ERR_INVALID, "the world holds no bodies");
     DeviceState* d = w->dev;
+    if (dyn_status st = upload_edits(w)) return st;
     dyn_step_params p;
     dyn_step_params_for(w, dt, &p);
     if (d->graph_dt != dt) {
@@ -664,6 +754,8 @@ void destroy_device(dyn_world* w) {
     for (cudaEvent_t e : d->events) cudaEventDestroy(e);
     for (void* p : d->allocs) cudaFree(p);
     for (void* p : d->joint_allocs) cudaFree(p);
+    if (d->edit_buffer) cudaFree(d->edit_buffer);
+    if (d->edit_run_buffer) cudaFree(d->edit_run_buffer);
     for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
         if (p) cudaFree(p);
     }

@@ -65,6 +65,9 @@ struct dyn_world {
     dyn::JointPlan joint_plan;
     bool joints_dirty = false;  // the device's joint buffers and plan are out of date
     bool scene_dirty = false;   // the device's scene is out of date although the rows are current
+    // body commands queued for the next step (body id, edit), in the order given
+    std::vector<uint32_t> edit_ids;
+    std::vector<dyn_body_edit_record> edits;
     bool timing = false;
     void* user_stream = nullptr;  // caller's cudaStream_t (dyn_world_set_stream)
     dyn::DeviceState* dev = nullptr;

@@ -116,6 +116,12 @@ CONSTRAINT_RUNTIME = _dtype(_fields([
     ("broken", "<u4", 1, 144), ("constraint_id", "<u4", 1, 148), ("generation", "<u4", 1, 152),
 ]), 160)
 CONSTRAINT_BALL = 0
+# records.wgsl BodyEdit: a command kind, a patch mask and the state it carries (160 bytes)
+BODY_EDIT = np.dtype({"names": ["kind", "mask", "state"], "formats": ["<u4", "<u4", BODY_STATE],
+                      "offsets": [0, 4, 16], "itemsize": 160})
+EDIT_PATCH, EDIT_FORCE, EDIT_TORQUE, EDIT_IMPULSE, EDIT_SLEEP, EDIT_WAKE = 0, 1, 2, 3, 4, 5
+EDIT_FORCE_AT_POINT, EDIT_IMPULSE_AT_POINT, EDIT_ANGULAR_IMPULSE = 6, 7, 8
+PATCH_POSITION, PATCH_VELOCITY, PATCH_ORIENTATION, PATCH_ANGULAR_VELOCITY = 1, 2, 4, 8
 CONSTRAINT_DISABLE_COLLISIONS, CONSTRAINT_HAS_BREAK, CONSTRAINT_WARM_START = 1, 32, 64
 
 # C ABI descriptors (include/dynamis_cuda.h)
@@ -179,3 +185,18 @@ def body_defaults(n: int) -> np.ndarray:
     b["collider_count"] = 1
     b["collider_first"] = np.arange(n, dtype=np.uint32)
     return b
+
+
+def body_edit(kind: int, mask: int = 0, position=None, orientation=None, velocity=None, angular_velocity=None,
+              force=None, torque=None) -> np.ndarray:
+    """One BodyEdit record (command.rs BodyCommand::edit): `velocity` carries an impulse, `position`
+    a point of application or a patched position, `angular_velocity` an angular impulse."""
+    e = np.zeros(1, BODY_EDIT)
+    e["kind"], e["mask"] = kind, mask
+    st = e["state"]
+    for name, value in (("position", position), ("orientation", orientation), ("velocity", velocity),
+                        ("angular_velocity", angular_velocity), ("force", force), ("torque", torque)):
+        if value is not None:
+            st[name] = value
+    e["state"] = st
+    return e

@@ -124,6 +124,35 @@ class World:
         arr = np.ascontiguousarray(world_of_body, np.uint32)
         self._check(lib.dyn_set_body_worlds(self._h, ptr(arr), len(arr)))
 
+    # ---- body commands ----
+    def edit_bodies(self, body_ids, edits: np.ndarray) -> None:
+        """Queues BodyEdit records (records.BODY_EDIT) for the next step, one per body id; a body's
+        commands run in the order given, after the step clears the applied forces."""
+        ids = np.ascontiguousarray(body_ids, np.uint32)
+        recs = np.ascontiguousarray(edits, R.BODY_EDIT)
+        if len(ids) != len(recs):
+            raise ValueError("one body id per edit")
+        self._check(lib.dyn_edit_bodies(self._h, ptr(ids), ptr(recs), len(ids)))
+
+    def apply_force(self, body_id: int, force) -> None:
+        self.edit_bodies([body_id], R.body_edit(R.EDIT_FORCE, force=force))
+
+    def apply_impulse(self, body_id: int, impulse, point=None) -> None:
+        if point is None:
+            self.edit_bodies([body_id], R.body_edit(R.EDIT_IMPULSE, velocity=impulse))
+        else:
+            self.edit_bodies([body_id], R.body_edit(R.EDIT_IMPULSE_AT_POINT, velocity=impulse, position=point))
+
+    def teleport(self, body_id: int, position=None, orientation=None) -> None:
+        mask = (R.PATCH_POSITION if position is not None else 0) | (R.PATCH_ORIENTATION if orientation is not None else 0)
+        self.edit_bodies([body_id], R.body_edit(R.EDIT_PATCH, mask=mask, position=position, orientation=orientation))
+
+    def sleep_body(self, body_id: int) -> None:
+        self.edit_bodies([body_id], R.body_edit(R.EDIT_SLEEP))
+
+    def wake_body(self, body_id: int) -> None:
+        self.edit_bodies([body_id], R.body_edit(R.EDIT_WAKE))
+
     # ---- constraints ----
     def add_ball_joint(self, first_body: int, second_body: int, anchor_a, anchor_b) -> int:
         """World::add_constraint(first, second, ConstraintDesc::ball(anchor_a, anchor_b)); returns the id."""

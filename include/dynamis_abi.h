@@ -66,6 +66,20 @@ extern "C" {
 #define DYN_LEVEL_KEY_SHIFT 27u
 #define DYN_CELL_HASH_MASK 0x07FFFFFFu
 #define DYN_GRID_LEVEL_LIMIT 30u
+/* body edit kinds and patch masks: crates/dynamis-abi/src/constant.rs:6-18 */
+#define DYN_EDIT_PATCH 0u
+#define DYN_EDIT_FORCE 1u
+#define DYN_EDIT_TORQUE 2u
+#define DYN_EDIT_IMPULSE 3u
+#define DYN_EDIT_SLEEP 4u
+#define DYN_EDIT_WAKE 5u
+#define DYN_EDIT_FORCE_AT_POINT 6u
+#define DYN_EDIT_IMPULSE_AT_POINT 7u
+#define DYN_EDIT_ANGULAR_IMPULSE 8u
+#define DYN_PATCH_POSITION 1u
+#define DYN_PATCH_VELOCITY 2u
+#define DYN_PATCH_ORIENTATION 4u
+#define DYN_PATCH_ANGULAR_VELOCITY 8u
 /* constraint kinds and flags: crates/dynamis-abi/src/constant.rs:88-103 */
 #define DYN_CONSTRAINT_BALL 0u
 #define DYN_CONSTRAINT_DISTANCE 1u
@@ -386,6 +400,23 @@ typedef struct dyn_constraint_descriptor_record {
     float angular_motor_force[4];
 } dyn_constraint_descriptor_record;
 
+/* records.wgsl:193-199 (160 bytes): one command for one body, applied at the next step */
+typedef struct dyn_body_edit_record {
+    uint32_t kind;  /* DYN_EDIT_* */
+    uint32_t mask;  /* DYN_PATCH_* for DYN_EDIT_PATCH */
+    uint32_t _pad0;
+    uint32_t _pad1;
+    dyn_body_state_record state;  /* the values the edit carries (see body_edits.wgsl) */
+} dyn_body_edit_record;
+
+/* records.wgsl:201-206 (16 bytes): the edits [first, first + len) of one row */
+typedef struct dyn_body_edit_run_record {
+    uint32_t row;
+    uint32_t first;
+    uint32_t len;
+    uint32_t _pad;
+} dyn_body_edit_run_record;
+
 /* records.wgsl:440-443 (8 bytes) */
 typedef struct dyn_constraint_rows_record {
     uint32_t first_row;
@@ -460,6 +491,9 @@ DYN_ABI_ASSERT(offsetof(dyn_contact_record, points) == 96, "Contact.points @96")
 DYN_ABI_ASSERT(sizeof(dyn_constraint_descriptor_record) == 400, "ConstraintDescriptor is 400 bytes");
 DYN_ABI_ASSERT(sizeof(dyn_constraint_rows_record) == 8, "ConstraintRows is 8 bytes");
 DYN_ABI_ASSERT(sizeof(dyn_constraint_reaction_record) == 64, "ConstraintReaction is 64 bytes");
+DYN_ABI_ASSERT(sizeof(dyn_body_edit_record) == 160, "BodyEdit is 160 bytes");
+DYN_ABI_ASSERT(offsetof(dyn_body_edit_record, state) == 16, "BodyEdit.state @16");
+DYN_ABI_ASSERT(sizeof(dyn_body_edit_run_record) == 16, "BodyEditRun is 16 bytes");
 DYN_ABI_ASSERT(sizeof(dyn_constraint_runtime_record) == 160, "ConstraintRuntime is 160 bytes");
 DYN_ABI_ASSERT(offsetof(dyn_constraint_runtime_record, accumulated) == 80, "ConstraintRuntime.accumulated @80");
 DYN_ABI_ASSERT(offsetof(dyn_constraint_runtime_record, broken) == 144, "ConstraintRuntime.broken @144");

@@ -199,6 +199,14 @@ DYN_API dyn_status dyn_stage_timings(dyn_world* world, float* ms, uint32_t n);
 DYN_API dyn_status dyn_radix_sort(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
                                   uint32_t major_digits, uint32_t minor_digits);
 
+/* ---- body commands ----
+ * World's body commands (set_position / set_velocity / apply_force / apply_impulse / sleep / wake ...,
+ * compiled to BodyEditRecords by crates/dynamis-world/src/command.rs:129-184): edits[i] applies to
+ * the body with id body_ids[i]. Edits queue on the host and run at the start of the next dyn_step,
+ * after the step clears forces and before anything reads the bodies (body_edits.wgsl), in the order
+ * given for each body. */
+DYN_API dyn_status dyn_edit_bodies(dyn_world* world, const uint32_t* body_ids, const dyn_body_edit_record* edits, uint32_t n);
+
 /* ---- batched worlds ----
  * Thousands of independent worlds stepped by one dyn_step: every body id gets a sub-world
  * (world_of_body[id], n = the number of bodies spawned or uploaded), and bodies of different

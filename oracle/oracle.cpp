@@ -195,6 +195,8 @@ struct OracleWorld {
     std::vector<dyn_constraint_runtime_record> joint_runtime;
     std::vector<uint32_t> plan_rows, plan_layers, plan_components;
     std::vector<uint32_t> body_world;  // sub-world of every row (empty: one world)
+    // body commands queued for the next step: (row, edit), in command order
+    std::vector<std::pair<uint32_t, dyn_body_edit_record>> edits;
     uint32_t world_of(uint32_t row) const { return body_world.empty() ? 0u : body_world[row]; }
 };
 
@@ -227,7 +229,85 @@ bool body_is_moving(const dyn_body_state_record& s, const dyn_body_descriptor_re
     return length(rd3(s.velocity)) > sleep_v || length(rd3(s.angular_velocity)) > sleep_w;
 }
 
-// apply_commands.rs:267-295: reset_counters.wgsl, clear_inputs.wgsl, activity.wgsl
+// body_edits.wgsl:11-21 (mark_disturbed)
+void edit_disturbs(OracleWorld& w, uint32_t row, dyn_body_state_record& s, bool disturbed) {
+    if (s.sleeping != 0u) {
+        w.counters[DYN_COUNTER_WOKE] += 1;
+        w.wake_flags[row] = 1u;
+    } else if (disturbed) {
+        w.wake_flags[row] = 1u;
+    }
+    s.sleeping = 0u;
+    s.sleep_timer = 0.0f;
+}
+
+// body_edits.wgsl:35-103: every queued command of a row, in order. Rows run one after another
+// here; on the device one thread takes each row's run (command.rs:157-176 groups them).
+void apply_edits(OracleWorld& w) {
+    for (const auto& [row, e] : w.edits) {
+        if (row >= w.states.size()) continue;
+        dyn_body_state_record& s = w.states[row];
+        const dyn_body_descriptor_record& d = w.descs[row];
+        const V3 ev = rd3(e.state.velocity), ep = rd3(e.state.position);
+        if (e.kind == DYN_EDIT_PATCH) {
+            if (e.mask & DYN_PATCH_POSITION) {
+                wr3(s.position, ep);
+                wr3(s.prev_position, ep);
+            }
+            if (e.mask & DYN_PATCH_ORIENTATION) {
+                for (int k = 0; k < 4; ++k) s.orientation[k] = s.prev_orientation[k] = e.state.orientation[k];
+            }
+            if (e.mask & DYN_PATCH_VELOCITY) wr3(s.velocity, ev);
+            if (e.mask & DYN_PATCH_ANGULAR_VELOCITY) wr3(s.angular_velocity, rd3(e.state.angular_velocity));
+            bool teleport = (e.mask & (DYN_PATCH_POSITION | DYN_PATCH_ORIENTATION)) != 0u;
+            edit_disturbs(w, row, s, teleport || !body_simulates_d(d.inverse_mass, d.flags));
+        } else if (e.kind == DYN_EDIT_FORCE) {
+            wr3(s.force, rd3(s.force) + rd3(e.state.force));
+            edit_disturbs(w, row, s, false);
+        } else if (e.kind == DYN_EDIT_FORCE_AT_POINT) {
+            V3 f = rd3(e.state.force);
+            wr3(s.force, rd3(s.force) + f);
+            wr3(s.torque, rd3(s.torque) + cross(ep - body_com(load_body(s, d)), f));
+            edit_disturbs(w, row, s, false);
+        } else if (e.kind == DYN_EDIT_TORQUE) {
+            wr3(s.torque, rd3(s.torque) + rd3(e.state.torque));
+            edit_disturbs(w, row, s, false);
+        } else if (e.kind == DYN_EDIT_IMPULSE) {
+            wr3(s.velocity, rd3(s.velocity) + ev * d.inverse_mass);
+            edit_disturbs(w, row, s, false);
+        } else if (e.kind == DYN_EDIT_IMPULSE_AT_POINT) {  // apply_impulse_at, body_edits.wgsl:23-33
+            wr3(s.velocity, rd3(s.velocity) + ev * d.inverse_mass);
+            Body b = load_body(s, d);
+            V3 lever = ep - body_com(b);
+            wr3(s.angular_velocity, rd3(s.angular_velocity) + apply_inverse_inertia(b, cross(lever, ev)));
+            edit_disturbs(w, row, s, false);
+        } else if (e.kind == DYN_EDIT_ANGULAR_IMPULSE) {
+            Body b = load_body(s, d);
+            wr3(s.angular_velocity, rd3(s.angular_velocity) + apply_inverse_inertia(b, rd3(e.state.angular_velocity)));
+            edit_disturbs(w, row, s, false);
+        } else if (e.kind == DYN_EDIT_SLEEP) {
+            if (s.sleeping == 0u) w.counters[DYN_COUNTER_SLEPT] += 1;
+            // freeze_body, core.wgsl:218-227
+            wr3(s.velocity, splat3(0.0f));
+            wr3(s.angular_velocity, splat3(0.0f));
+            wr3(s.force, splat3(0.0f));
+            wr3(s.torque, splat3(0.0f));
+            for (int k = 0; k < 3; ++k) s.prev_position[k] = s.position[k];
+            for (int k = 0; k < 4; ++k) s.prev_orientation[k] = s.orientation[k];
+            s.sleep_timer = 0.0f;
+            s.sleeping = 1u;
+            w.wake_flags[row] = 0u;
+        } else if (e.kind == DYN_EDIT_WAKE) {
+            if (s.sleeping != 0u) w.counters[DYN_COUNTER_WOKE] += 1;
+            s.sleep_timer = 0.0f;
+            s.sleeping = 0u;
+            w.wake_flags[row] = 1u;
+        }
+    }
+    w.edits.clear();
+}
+
+// apply_commands.rs:267-295: reset_counters.wgsl, clear_inputs.wgsl, body_edits.wgsl, activity.wgsl
 void apply_commands(OracleWorld& w) {
     // joint_filter.wgsl: the jointed pairs filtered this step
     uint32_t jointed = 0;
@@ -241,6 +321,7 @@ void apply_commands(OracleWorld& w) {
         wr3(w.states[i].force, splat3(0.0f));
         wr3(w.states[i].torque, splat3(0.0f));
     }
+    apply_edits(w);
     w.body_activity.assign(n, 0);
     w.body_motion.assign(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
@@ -1572,6 +1653,11 @@ uint32_t orc_set_constraints(OracleWorld* w, const dyn_constraint_descriptor_rec
     plan_joint_order(*w);
     w->params.constraint_count = m;
     return 1;
+}
+
+// Queues body commands for the next step by row (the caller maps body ids to rows).
+void orc_queue_edits(OracleWorld* w, const uint32_t* rows, const dyn_body_edit_record* edits, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i) w->edits.emplace_back(rows[i], edits[i]);
 }
 
 void orc_set_body_worlds(OracleWorld* w, const uint32_t* rows, uint32_t n) {

@@ -50,6 +50,7 @@ def lib() -> ctypes.CDLL:
         _lib.orc_constraints.argtypes = [P, P]
         _lib.orc_joint_plan.argtypes = [P, P, P, P, P]
         _lib.orc_set_body_worlds.argtypes = [P, P, U32]
+        _lib.orc_queue_edits.argtypes = [P, P, P, U32]
     return _lib
 
 
@@ -92,6 +93,14 @@ class OracleWorld:
 
     def step(self, dt: float) -> None:
         lib().orc_step(self._h, float(dt))
+
+    def edit_bodies(self, body_ids, edits: np.ndarray) -> None:
+        """Queues BodyEdit records for the next step (body ids mapped to this world's rows)."""
+        ids = np.asarray(body_ids, np.int64)
+        row_of = {int(b): r for r, b in enumerate(self.states()["body_id"])}
+        rows = np.array([row_of.get(int(i), R.NO_BODY) for i in ids], np.uint32)
+        recs = np.ascontiguousarray(edits, R.BODY_EDIT)
+        lib().orc_queue_edits(self._h, _p(rows), _p(recs), len(rows))
 
     def counters(self) -> np.ndarray:
         out = np.zeros(R.COUNTER_DEVICE_COUNT, np.uint32)
