@@ -314,13 +314,15 @@ def loop_baseline(args, dt: float, batch_ms: float, device: int, sample_every: i
 
 
 def cpu_baseline(world, budget_s: float = 20.0, dt: float = DT) -> dict:
-    """The oracle (CPU restatement, one thread) stepping the same world state."""
-    from oracle.oracle import OracleWorld
+    """The oracle (CPU restatement) stepping the same world state on every host thread, then one
+    more step on a single thread."""
+    from oracle import oracle as orc
 
     scene = world.export_scene()
     scene["states"] = world.read_states()
-    oracle = OracleWorld(scene, world.step_params(dt))
-    log("cpu baseline: oracle world built")
+    oracle = orc.OracleWorld(scene, world.step_params(dt))
+    cores = orc.threads()
+    log(f"cpu baseline: oracle world built; {cores} threads")
     steps = 0
     t0 = time.perf_counter()
     while True:
@@ -328,14 +330,24 @@ def cpu_baseline(world, budget_s: float = 20.0, dt: float = DT) -> dict:
         steps += 1
         if time.perf_counter() - t0 > budget_s / 2 or steps >= 3:
             break
-    dt = time.perf_counter() - t0
+    elapsed = time.perf_counter() - t0
     n = len(scene["states"])
-    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{steps} step(s) of the full {n}-body world from the GPU run's current state, one thread"}
+    single = None
+    if budget_s > 0:
+        orc.set_threads(1)
+        t1 = time.perf_counter()
+        oracle.step(dt)
+        single = n / (time.perf_counter() - t1)
+        orc.set_threads(cores)
+    oracle.close()
+    return {"value": n * steps / elapsed, "unit": UNIT, "cores": cores, "kind": "port",
+            "single_thread_value": single,
+            "sample": f"{steps} step(s) of the full {n}-body world from its current state on "
+                      f"{cores} threads (OpenMP), then 1 step on one thread (single_thread_value)"}
 
 
 def run_reference(args) -> dict:
-    """The reference arm: the CPU restatement of the step on the host, all it can use (one thread)."""
+    """The reference arm: the CPU restatement of the step on the host, on every host thread."""
     from dynamis_b200 import World
 
     DT = dt_of(args.workload)

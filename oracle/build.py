@@ -23,7 +23,7 @@ def build(verbose: bool = False) -> Path:
     newest = max(p.stat().st_mtime for p in SOURCES + HEADERS)
     if LIBRARY.exists() and LIBRARY.stat().st_mtime >= newest:
         return LIBRARY
-    cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+    cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
            "-I", str(ROOT / "include"), *map(str, SOURCES), "-o", str(LIBRARY)]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:

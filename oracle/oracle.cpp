@@ -20,6 +20,12 @@
 // contacts of sleeping bodies) is replaced by re-emitting every movable collider each step with
 // its awake bit, which yields the same candidate pairs for awake bodies; contact events are not
 // published (only the CONTACT_ANNOUNCED flag that gates warm starting is kept).
+//
+// Threads: the loops the reference runs as data-parallel passes (AABBs, pair emission, the
+// narrowphase, the contact solve and position blocks, integration, the applies) run on every host
+// thread through OpenMP. Each shared write is an integer atomic (the fixed-point deltas, counters)
+// or goes into per-block lists joined in index order, so every result, bit for bit, is the same for
+// any thread count, including one.
 #include <algorithm>
 #include <cstring>
 #include <array>
@@ -29,6 +35,26 @@
 
 #include "dynamis_abi.h"
 #include "oracle_geom.h"
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+inline void atomic_add_u32(uint32_t* p, uint32_t v) { __atomic_fetch_add(p, v, __ATOMIC_RELAXED); }
+inline void atomic_max_u32(uint32_t* p, uint32_t v) {
+    uint32_t cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+    while (cur < v && !__atomic_compare_exchange_n(p, &cur, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+    }
+}
+// Runs fn(first, last, block) over [0, n) in blocks of `block` items on every thread.
+template <typename F>
+void parallel_blocks(size_t n, size_t block, F&& fn) {
+    const long long blocks = (long long)((n + block - 1) / block);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long b = 0; b < blocks; ++b) {
+        size_t first = (size_t)b * block;
+        fn(first, std::min(n, first + block), (size_t)b);
+    }
+}
 
 using namespace orc;
 
@@ -334,6 +360,7 @@ void apply_commands(OracleWorld& w) {
 
 // begin_step.wgsl:5-14 (dynamic rows); broadphase_aabb.wgsl:11-62 (colliders)
 void prepare(OracleWorld& w) {
+#pragma omp parallel for schedule(static)
     for (uint32_t i = 0; i < w.params.dynamic_count; ++i) {
         dyn_body_state_record& s = w.states[i];
         if (s.sleeping != 0u) continue;
@@ -342,6 +369,7 @@ void prepare(OracleWorld& w) {
     }
     uint32_t k = (uint32_t)w.colliders.size();
     w.aabbs.assign(k, Aabb{splat3(0.0f), splat3(0.0f)});
+#pragma omp parallel for schedule(static)
     for (uint32_t i = 0; i < k; ++i) {
         uint32_t owner = w.owners[i];
         if (owner == DYN_NO_BODY) continue;
@@ -353,9 +381,8 @@ void prepare(OracleWorld& w) {
         WorldShape upright = shape;
         upright.rotation = V4{0.0f, 0.0f, 0.0f, 1.0f};
         Aabb resolution = world_aabb_of(w.shapes, upright);
-        w.counters[DYN_COUNTER_GRID_SCALE] = std::max(w.counters[DYN_COUNTER_GRID_SCALE], f2u(grid_scale_of(resolution)));
-        w.counters[DYN_COUNTER_GRID_EXTENT] =
-            std::max(w.counters[DYN_COUNTER_GRID_EXTENT], f2u(fmaxw(grid_extent_of(resolution), 0.0f)));
+        atomic_max_u32(&w.counters[DYN_COUNTER_GRID_SCALE], f2u(grid_scale_of(resolution)));
+        atomic_max_u32(&w.counters[DYN_COUNTER_GRID_EXTENT], f2u(fmaxw(grid_extent_of(resolution), 0.0f)));
         Aabb swept = tight;
         if (body_moves_d(d.inverse_mass, d.flags)) {
             V3 travel = vabs(rd3(s.velocity) * w.params.dt);
@@ -433,7 +460,7 @@ void emit_entries(OracleWorld& w) {
 }
 
 struct PairSink {
-    OracleWorld* w;
+    const OracleWorld* w;
     std::vector<uint32_t> major, minor;
 };
 
@@ -452,15 +479,11 @@ void emit_pair(PairSink& sink, uint32_t first, uint32_t second) {
     if (first == second || a.group == b.group) return;
     if ((a.info & DYN_ENTRY_MOBILE) == 0u && (b.info & DYN_ENTRY_MOBILE) == 0u) return;
     if (sink.w->world_of(a.group) != sink.w->world_of(b.group)) return;
-    uint32_t slot = sink.w->counters[DYN_COUNTER_PAIRS]++;
-    if (slot < sink.w->pair_capacity) {
-        uint32_t ia = a.info & DYN_ENTRY_INDEX_MASK;
-        uint32_t ib = b.info & DYN_ENTRY_INDEX_MASK;
-        sink.major.push_back(std::min(ia, ib));
-        sink.minor.push_back(std::max(ia, ib));
-    } else {
-        sink.w->counters[DYN_COUNTER_REFUSED_PAIRS] += 1;
-    }
+    // the pair's slot (and the capacity cut) is taken when the blocks are joined in order
+    uint32_t ia = a.info & DYN_ENTRY_INDEX_MASK;
+    uint32_t ib = b.info & DYN_ENTRY_INDEX_MASK;
+    sink.major.push_back(std::min(ia, ib));
+    sink.minor.push_back(std::max(ia, ib));
 }
 I3 entry_cell(const Entry& e, float cs) {
     uint32_t bits = (e.info & DYN_ENTRY_CELL_MASK) >> DYN_ENTRY_CELL_SHIFT;
@@ -478,75 +501,99 @@ void key_range(const OracleWorld& w, uint32_t key, uint32_t* first, uint32_t* la
 // cell_pairs.wgsl:6-50 and level_links.wgsl:6-65, over one sorted entry array holding every
 // region; then the pair sort (narrowphase.rs:110-126: collider_slot_words digits per word).
 void broadphase(OracleWorld& w) {
-    PairSink sink{&w, {}, {}};
     float grid = grid_base_cell(w);
     uint32_t occupied = w.counters[DYN_COUNTER_GRID_LEVELS] | w.counters[DYN_COUNTER_RESTING_LEVELS]
         | w.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
     uint32_t live = (uint32_t)w.entry_keys.size();
+    const size_t kBlock = 2048;
+    const size_t blocks = (live + kBlock - 1) / kBlock;
+    std::vector<PairSink> links(blocks, PairSink{&w, {}, {}}), cells(blocks, PairSink{&w, {}, {}});
     // level_links first, then cell_pairs (passes.rs record order); the pair set is what matters.
-    for (uint32_t index = 0; index < live; ++index) {
-        uint32_t node = w.entry_order[index];
-        const Entry& e = w.entries[node];
-        if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
-        if ((e.info & DYN_ENTRY_PRIMARY) == 0u) continue;
-        bool awake = entry_awake(w, node);
-        if (!awake && w.counters[DYN_COUNTER_COARSE_ACTIVE] == 0u) continue;
-        uint32_t level = shape_levels(e.box, grid);
-        uint32_t coarser = occupied & ~((1u << std::min(level + 1u, 31u)) - 1u);
-        while (coarser != 0u) {
-            uint32_t link = 31u - (uint32_t)__builtin_clz(coarser);
-            coarser &= ~(1u << link);
-            float cs = level_cell_size(link, grid);
-            GridCells cells = grid_cells(e.box, cs);
-            uint32_t count = grid_cell_count(cells);
-            if ((long long)cells.max.x - cells.min.x > 3 || (long long)cells.max.y - cells.min.y > 3 ||
-                (long long)cells.max.z - cells.min.z > 3 || cells.max.x < cells.min.x || cells.max.y < cells.min.y ||
-                cells.max.z < cells.min.z) {
-                w.counters[DYN_COUNTER_ENTRY_FAULTS] += 1;  // non-finite box: same cut as the device
-                continue;
-            }
-            for (uint32_t ordinal = 0; ordinal < count; ++ordinal) {
-                I3 cell = grid_cell_at(cells, ordinal);
-                uint32_t first, last;
-                key_range(w, cell_key_in(link, cell, w.world_of(e.group)), &first, &last);
-                for (uint32_t entry = first; entry < last; ++entry) {
-                    uint32_t other = w.entry_order[entry];
-                    if (other == node) continue;
-                    if (!awake && !entry_awake(w, other)) continue;
-                    const Entry& o = w.entries[other];
-                    if (!aabb_overlaps(e.box, o.box)) continue;
-                    if (!i3eq(entry_cell(o, cs), cell)) continue;
-                    if (!i3eq(grid_overlap_cell(e.box, o.box, cs), cell)) continue;
-                    emit_pair(sink, node, other);
+    parallel_blocks(live, kBlock, [&](size_t begin, size_t end, size_t b) {
+        PairSink& sink = links[b];
+        for (uint32_t index = (uint32_t)begin; index < (uint32_t)end; ++index) {
+            uint32_t node = w.entry_order[index];
+            const Entry& e = w.entries[node];
+            if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
+            if ((e.info & DYN_ENTRY_PRIMARY) == 0u) continue;
+            bool awake = entry_awake(w, node);
+            if (!awake && w.counters[DYN_COUNTER_COARSE_ACTIVE] == 0u) continue;
+            uint32_t level = shape_levels(e.box, grid);
+            uint32_t coarser = occupied & ~((1u << std::min(level + 1u, 31u)) - 1u);
+            while (coarser != 0u) {
+                uint32_t link = 31u - (uint32_t)__builtin_clz(coarser);
+                coarser &= ~(1u << link);
+                float cs = level_cell_size(link, grid);
+                GridCells gc = grid_cells(e.box, cs);
+                uint32_t count = grid_cell_count(gc);
+                if ((long long)gc.max.x - gc.min.x > 3 || (long long)gc.max.y - gc.min.y > 3 ||
+                    (long long)gc.max.z - gc.min.z > 3 || gc.max.x < gc.min.x || gc.max.y < gc.min.y ||
+                    gc.max.z < gc.min.z) {
+                    atomic_add_u32(&w.counters[DYN_COUNTER_ENTRY_FAULTS], 1u);  // non-finite box: same cut as the device
+                    continue;
+                }
+                for (uint32_t ordinal = 0; ordinal < count; ++ordinal) {
+                    I3 cell = grid_cell_at(gc, ordinal);
+                    uint32_t first, last;
+                    key_range(w, cell_key_in(link, cell, w.world_of(e.group)), &first, &last);
+                    for (uint32_t entry = first; entry < last; ++entry) {
+                        uint32_t other = w.entry_order[entry];
+                        if (other == node) continue;
+                        if (!awake && !entry_awake(w, other)) continue;
+                        const Entry& o = w.entries[other];
+                        if (!aabb_overlaps(e.box, o.box)) continue;
+                        if (!i3eq(entry_cell(o, cs), cell)) continue;
+                        if (!i3eq(grid_overlap_cell(e.box, o.box, cs), cell)) continue;
+                        emit_pair(sink, node, other);
+                    }
                 }
             }
         }
-    }
-    for (uint32_t index = 0; index < live; ++index) {
-        uint32_t node = w.entry_order[index];
-        const Entry& e = w.entries[node];
-        if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
-        if (!entry_awake(w, node)) continue;
-        uint32_t level = shape_levels(e.box, grid);
-        float cs = level_cell_size(level, grid);
-        I3 cell = entry_cell(e, cs);
-        uint32_t first, last;
-        key_range(w, cell_key_in(level, cell, w.world_of(e.group)), &first, &last);
-        for (uint32_t entry = first; entry < last; ++entry) {
-            if (entry == index) continue;
-            uint32_t other = w.entry_order[entry];
-            if (entry_awake(w, other) && entry < index) continue;
-            const Entry& o = w.entries[other];
-            if (!aabb_overlaps(e.box, o.box)) continue;
-            if (!i3eq(entry_cell(o, cs), cell)) continue;
-            if (!i3eq(grid_overlap_cell(e.box, o.box, cs), cell)) continue;
-            emit_pair(sink, node, other);
+    });
+    parallel_blocks(live, kBlock, [&](size_t begin, size_t end, size_t b) {
+        PairSink& sink = cells[b];
+        for (uint32_t index = (uint32_t)begin; index < (uint32_t)end; ++index) {
+            uint32_t node = w.entry_order[index];
+            const Entry& e = w.entries[node];
+            if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
+            if (!entry_awake(w, node)) continue;
+            uint32_t level = shape_levels(e.box, grid);
+            float cs = level_cell_size(level, grid);
+            I3 cell = entry_cell(e, cs);
+            uint32_t first, last;
+            key_range(w, cell_key_in(level, cell, w.world_of(e.group)), &first, &last);
+            for (uint32_t entry = first; entry < last; ++entry) {
+                if (entry == index) continue;
+                uint32_t other = w.entry_order[entry];
+                if (entry_awake(w, other) && entry < index) continue;
+                const Entry& o = w.entries[other];
+                if (!aabb_overlaps(e.box, o.box)) continue;
+                if (!i3eq(entry_cell(o, cs), cell)) continue;
+                if (!i3eq(grid_overlap_cell(e.box, o.box, cs), cell)) continue;
+                emit_pair(sink, node, other);
+            }
+        }
+    });
+    // pair_emit.wgsl's slot counter: pairs beyond the capacity are refused, in emission order
+    std::vector<uint32_t> major, minor;
+    uint64_t emitted = 0;
+    for (const std::vector<PairSink>* part : {&links, &cells}) {
+        for (const PairSink& sink : *part) {
+            for (size_t i = 0; i < sink.major.size(); ++i, ++emitted) {
+                if (emitted >= w.pair_capacity) continue;
+                major.push_back(sink.major[i]);
+                minor.push_back(sink.minor[i]);
+            }
         }
     }
+    w.counters[DYN_COUNTER_PAIRS] = (uint32_t)emitted;
+    w.counters[DYN_COUNTER_REFUSED_PAIRS] = (uint32_t)(emitted - major.size());
+    links.clear();
+    cells.clear();
     uint32_t words = key_words(std::max<uint32_t>((uint32_t)w.colliders.size(), 1u));
-    radix_sort_pairs(sink.major, sink.minor, nullptr, words, words);
-    w.pair_major = sink.major;
-    w.pair_minor = sink.minor;
+    radix_sort_pairs(major, minor, nullptr, words, words);
+    w.pair_major = std::move(major);
+    w.pair_minor = std::move(minor);
 }
 
 // narrowphase.wgsl:518-685 for one pair; false when the pair answers no contact.
@@ -679,17 +726,31 @@ bool narrowphase_pair(const OracleWorld& w, uint32_t first_slot, uint32_t second
 // narrowphase pass + compact_scan/offsets/scatter.wgsl: contacts in pair order.
 void narrowphase(OracleWorld& w) {
     w.contacts.clear();
-    size_t p = w.pair_major.size();
-    for (size_t i = 0; i < p; ++i) {
-        dyn_contact_record c;
-        if (!narrowphase_pair(w, w.pair_major[i], w.pair_minor[i], &c)) continue;
-        if (w.contacts.size() >= w.contact_capacity) {
-            w.counters[DYN_COUNTER_REFUSED_CONTACTS] += 1;
-            continue;
+    const size_t p = w.pair_major.size();
+    // pairs in blocks on every thread; the blocks' contacts are joined in pair order
+    const size_t kBlock = 1024, kSpan = 64 * kBlock;
+    std::vector<std::vector<dyn_contact_record>> found;
+    for (size_t span = 0; span < p; span += kSpan) {
+        const size_t n = std::min(kSpan, p - span);
+        found.assign((n + kBlock - 1) / kBlock, {});
+        parallel_blocks(n, kBlock, [&](size_t begin, size_t end, size_t b) {
+            for (size_t i = span + begin; i < span + end; ++i) {
+                dyn_contact_record c;
+                if (!narrowphase_pair(w, w.pair_major[i], w.pair_minor[i], &c)) continue;
+                c.carried_normal = 0.0f;
+                c.carried_tangent = 0.0f;
+                found[b].push_back(c);
+            }
+        });
+        for (const std::vector<dyn_contact_record>& block : found) {
+            for (const dyn_contact_record& c : block) {
+                if (w.contacts.size() >= w.contact_capacity) {
+                    w.counters[DYN_COUNTER_REFUSED_CONTACTS] += 1;
+                    continue;
+                }
+                w.contacts.push_back(c);
+            }
         }
-        c.carried_normal = 0.0f;
-        c.carried_tangent = 0.0f;
-        w.contacts.push_back(c);
     }
     w.counters[DYN_COUNTER_CONTACTS] = (uint32_t)w.contacts.size();
     w.contact_matched.assign(w.contacts.size(), 0);
@@ -929,7 +990,7 @@ void solver_prepare(OracleWorld& w) {
 void accumulate(std::vector<int32_t>& deltas, uint32_t row, V3 linear, V3 angular, float scale) {
     int32_t* d = &deltas[8 * (size_t)row];
     // i32 wrapping adds, as WGSL atomicAdd on u32 words
-    auto add = [](int32_t* word, int32_t v) { *word = (int32_t)((uint32_t)*word + (uint32_t)v); };
+    auto add = [](int32_t* word, int32_t v) { atomic_add_u32(reinterpret_cast<uint32_t*>(word), (uint32_t)v); };
     add(d + 0, solver_word(linear.x, scale));
     add(d + 1, solver_word(linear.y, scale));
     add(d + 2, solver_word(linear.z, scale));
@@ -1015,8 +1076,8 @@ void solve_contact_block(OracleWorld& w, uint32_t index, bool residual) {
         if (!residual) return;
         uint32_t lin = (uint32_t)solver_word(fmaxw(length(da), length(db)), DYN_SOLVER_VELOCITY_SCALE);
         uint32_t ang = (uint32_t)solver_word(fmaxw(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE);
-        w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL] = std::max(w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL], lin);
-        w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL] = std::max(w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL], ang);
+        atomic_max_u32(&w.counters[DYN_COUNTER_SOLVE_LINEAR_RESIDUAL], lin);
+        atomic_max_u32(&w.counters[DYN_COUNTER_SOLVE_ANGULAR_RESIDUAL], ang);
     };
     V3 zero = splat3(0.0f);
     if (!contact_block_resolves(contact)) {
@@ -1125,7 +1186,10 @@ void solve_contact_block(OracleWorld& w, uint32_t index, bool residual) {
 // solver_block_apply.wgsl:7-29
 void block_apply(OracleWorld& w) {
     if (!w.solver_rows.empty()) w.solver_rounds += 1;
-    for (uint32_t row : w.solver_rows) {
+    const size_t rows = w.solver_rows.size();
+#pragma omp parallel for schedule(static)
+    for (size_t r = 0; r < rows; ++r) {
+        const uint32_t row = w.solver_rows[r];
         int32_t* d = &w.velocity_deltas[8 * (size_t)row];
         V3 linear = V3{solver_value(d[0], DYN_SOLVER_VELOCITY_SCALE), solver_value(d[1], DYN_SOLVER_VELOCITY_SCALE),
                        solver_value(d[2], DYN_SOLVER_VELOCITY_SCALE)};
@@ -1134,6 +1198,7 @@ void block_apply(OracleWorld& w) {
         for (int k = 0; k < 6; ++k) d[k] = 0;
         if (veq(linear, splat3(0.0f)) && veq(angular, splat3(0.0f))) continue;
         dyn_body_state_record& s = w.states[row];
+        // (rows are distinct: each solver row is claimed once)
         wr3(s.velocity, rd3(s.velocity) + linear);
         wr3(s.angular_velocity, rd3(s.angular_velocity) + angular);
     }
@@ -1144,7 +1209,10 @@ void substep_integrate(OracleWorld& w) {
     w.solver_rounds = 0;
     const dyn_step_params& p = w.params;
     float h = p.substep_dt;
-    for (uint32_t row : w.live) {
+    const size_t live = w.live.size();
+#pragma omp parallel for schedule(static)
+    for (size_t r = 0; r < live; ++r) {
+        const uint32_t row = w.live[r];
         const dyn_body_descriptor_record& d = w.descs[row];
         if (!body_simulates_d(d.inverse_mass, d.flags)) continue;
         dyn_body_state_record& s = w.states[row];
@@ -1183,8 +1251,10 @@ void substep_integrate(OracleWorld& w) {
 // substep_advance.wgsl:6-13
 void substep_advance(OracleWorld& w) {
     float h = w.params.substep_dt;
-    for (uint32_t row : w.live) {
-        dyn_body_state_record& s = w.states[row];
+    const size_t live = w.live.size();
+#pragma omp parallel for schedule(static)
+    for (size_t r = 0; r < live; ++r) {
+        dyn_body_state_record& s = w.states[w.live[r]];
         wr3(s.position, rd3(s.position) + rd3(s.velocity) * h);
         V3 av = rd3(s.angular_velocity);
         V4 spin = V4{av.x, av.y, av.z, 0.0f};
@@ -1196,6 +1266,7 @@ void substep_advance(OracleWorld& w) {
 // position_correction.wgsl:5-46 + position_block.wgsl:11-33
 void position_block(OracleWorld& w) {
     uint32_t c = (uint32_t)w.contacts.size();
+#pragma omp parallel for schedule(dynamic, 256)
     for (uint32_t index = 0; index < c; ++index) {
         const dyn_contact_record& contact = w.contacts[index];
         if (!contact_block_resolves(contact) || contact.relaxation > 0.0f) continue;
@@ -1222,8 +1293,8 @@ void position_block(OracleWorld& w) {
         // correction.wgsl:18-31 pair_holds
         bool holds = dot(lin_f, lin_f) > 0.0f || dot(lin_s, lin_s) > 0.0f;
         if (!holds) continue;
-        w.contributions[fr] += 1;
-        w.contributions[sr] += 1;
+        atomic_add_u32(&w.contributions[fr], 1u);
+        atomic_add_u32(&w.contributions[sr], 1u);
         accumulate(w.position_deltas, fr, lin_f, splat3(0.0f), DYN_SOLVER_POSITION_SCALE);
         accumulate(w.position_deltas, sr, lin_s, splat3(0.0f), DYN_SOLVER_POSITION_SCALE);
     }
@@ -1231,7 +1302,10 @@ void position_block(OracleWorld& w) {
 
 // position_apply.wgsl:12-27
 void position_apply(OracleWorld& w) {
-    for (uint32_t row : w.solver_rows) {
+    const size_t rows = w.solver_rows.size();
+#pragma omp parallel for schedule(static)
+    for (size_t r = 0; r < rows; ++r) {
+        const uint32_t row = w.solver_rows[r];
         uint32_t contributing = w.contributions[row];
         w.contributions[row] = 0;
         int32_t* d = &w.position_deltas[8 * (size_t)row];
@@ -1551,12 +1625,14 @@ void solve_substeps(OracleWorld& w) {
         substep_integrate(w);
         if (substep == 0) {
             walk_joints(w, JointWalk::Warm, false);
+#pragma omp parallel for schedule(dynamic, 256)
             for (uint32_t i = 0; i < c; ++i) warm_contact_block(w, i);
             block_apply(w);
         }
         for (uint32_t it = 0; it < w.params.solve_iterations; ++it) {
             bool residual = w.solver_rounds == w.params.solve_iterations;
             walk_joints(w, JointWalk::Solve, residual);
+#pragma omp parallel for schedule(dynamic, 256)
             for (uint32_t i = 0; i < c; ++i) solve_contact_block(w, i, residual);
             block_apply(w);
         }
@@ -1742,6 +1818,22 @@ uint32_t orc_islands(const OracleWorld* w, uint32_t* out) {
 }
 
 // Known-answer hooks for the math and sort restatements.
+// Host threads for the parallel loops (results do not depend on the count).
+uint32_t orc_threads(void) {
+#ifdef _OPENMP
+    return (uint32_t)omp_get_max_threads();
+#else
+    return 1u;
+#endif
+}
+void orc_set_threads(uint32_t n) {
+#ifdef _OPENMP
+    omp_set_num_threads((int)std::max(n, 1u));
+#else
+    (void)n;
+#endif
+}
+
 float orc_sin(float x) { return osin(x); }
 float orc_cos(float x) { return ocos(x); }
 float orc_atan2(float y, float x) { return oatan2(y, x); }

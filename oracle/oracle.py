@@ -51,6 +51,8 @@ def lib() -> ctypes.CDLL:
         _lib.orc_joint_plan.argtypes = [P, P, P, P, P]
         _lib.orc_set_body_worlds.argtypes = [P, P, U32]
         _lib.orc_queue_edits.argtypes = [P, P, P, U32]
+        _lib.orc_threads.restype = U32
+        _lib.orc_set_threads.argtypes = [U32]
     return _lib
 
 
@@ -163,6 +165,16 @@ class OracleWorld:
 def oracle_from_world(world, dt: float, **capacity) -> OracleWorld:
     """An oracle world holding exactly the records `world` uploads to the device."""
     return OracleWorld(world.export_scene(), world.step_params(dt), **capacity)
+
+
+def threads() -> int:
+    """Host threads the oracle's parallel loops use."""
+    return int(lib().orc_threads())
+
+
+def set_threads(n: int) -> None:
+    """Sets the oracle's host thread count (its results are the same for any count)."""
+    lib().orc_set_threads(max(int(n), 1))
 
 
 def radix_sort(major, minor=None, payload=None, major_digits=4, minor_digits=0):

@@ -11,6 +11,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+from dynamis_b200 import records as R
 from oracle import oracle as O
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -96,3 +97,28 @@ def test_oracle_reproduces_the_step_fixture(step_golden):
         assert np.array_equal(oracle.counters(), step_golden[f"s{s}_counters"]), f"step {s}: counters"
     oracle.close()
     world.close()
+
+
+def test_the_oracle_steps_alike_on_one_thread_and_on_many():
+    """The oracle's parallel loops join their results in index order and sum integers only, so a
+    step is bit-identical for any thread count."""
+    from dynamis_b200 import World, scenes
+
+    default = O.threads()
+    results = []
+    try:
+        for n in (1, 4):
+            O.set_threads(n)
+            w = World()
+            scenes.mixed_pile(side=6, seed=2).build(w)
+            o = O.oracle_from_world(w, 1.0 / 60.0)
+            for _ in range(25):
+                o.step(1.0 / 60.0)
+            results.append((o.states(), o.contacts(), o.counters()))
+            o.close()
+            w.close()
+    finally:
+        O.set_threads(default)
+    (s1, c1, k1), (s4, c4, k4) = results
+    assert k1[R.COUNTER["CONTACTS"]] > 0
+    assert s1.tobytes() == s4.tobytes() and c1.tobytes() == c4.tobytes() and np.array_equal(k1, k4)
