@@ -124,12 +124,10 @@ def stage_bytes(stage: str, m: dict, params: dict) -> float:
         return 40.0 * E
     if stage == "entry_sort":
         return 16.0 * E * 4
-    if stage == "pair_sort":
-        return 16.0 * P * 2 * params["pair_words"]
     if stage == "pairs":
         return 40.0 * E + 8.0 * P
-    if stage == "compact":
-        return 4.0 * P + 2 * 352.0 * C
+    if stage == "compact":   # contact keys (12 B), their sort (2 x 12 B a pass), the 352 B gather
+        return 12.0 * C + 24.0 * C * 2 * params["contact_words"] + 2 * 352.0 * C
     if stage == "integrate":
         return 152.0 * L
     return 0.0
@@ -206,7 +204,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     log("stages " + ", ".join(f"{k}={v:.3f}" for k, v in stages.items()))
     params = {"substeps": int(world.config["substeps"][0]), "solve_iterations": int(world.config["solve_iterations"][0]),
               "position_iterations": int(world.config["position_iterations"][0]),
-              "pair_words": int(np.ceil(np.ceil(np.log2(max(counts["K"] - 1, 1) + 1)) / 8)) or 1}
+              "contact_words": int(np.ceil(np.ceil(np.log2(max(counts["K"] - 1, 1) + 1)) / 8)) or 1}
     dominant = max(stages, key=stages.get)
     launches = LAUNCHES.get(dominant, lambda p: 1)(params)
     per_launch_ms = stages[dominant] / launches

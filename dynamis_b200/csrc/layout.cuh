@@ -53,13 +53,12 @@ enum Ctl : uint32_t {
     CTL_ENTRIES = 0,
     CTL_PAIRS = 1,
     CTL_CONTACTS = 2,
-    CTL_TMP = 3,
+    CTL_APPENDED = 3,  // contacts the narrowphase appended (stored ones: the first c_cap)
     CTL_LIVE = 4,
     CTL_SOLVER_ROWS = 5,
     CTL_ARCHIVED = 6,
     CTL_ROUNDS = 7,
     CTL_STATUS = 8,
-    CTL_VALID = 9,
     CTL_LIST0 = 10,  // narrowphase class lists (3 words)
     CTL_EPA = 13,    // penetrating convex pairs queued for EPA
     CTL_HITS = 14,   // convex pairs queued for the manifold
@@ -115,22 +114,23 @@ struct DeviceWorld {
     float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits
     uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
     uint32_t cell_bits;
-    uint32_t* pmaj;
+    uint32_t* pmaj;  // candidate pairs in emission order (lower, higher collider slot)
     uint32_t* pmin;
-    uint32_t* pmaj_alt;
-    uint32_t* pmin_alt;
-    // narrowphase staging and compaction
+    // narrowphase, its staging set (append order) and the compaction into pair order
     ContactSet tmp;
-    uint32_t* pair_slot;
-    uint32_t* pair_flag;
-    uint32_t* pair_rank;
+    uint32_t* cmaj;  // [c_cap] staged contacts' (lower, higher) collider slot, then sorted
+    uint32_t* cmin;
+    uint32_t* cval;  // staged contact of each sorted key
+    uint32_t* cmaj_alt;
+    uint32_t* cmin_alt;
+    uint32_t* cval_alt;
     uint32_t* np_list;  // [3][p_cap] pair indices per narrowphase class
     uint32_t* epa_list;      // pair indices of penetrating convex pairs
     float4* epa_simplex;     // [4][slot]: the GJK simplex (w.xyz) EPA starts from
     uint32_t* hit_list;      // pair indices of convex hits
     float4* hit_data;        // [2][slot]: point.xyz + distance, normal.xyz
-    ContactSet cur;
-    ContactSet arc;
+    ContactSet cur;  // this step's contacts in sorted pair order
+    ContactSet arc;  // last step's
     SolverRows srows;
     uint32_t* matched;
     // islands, live list, solver

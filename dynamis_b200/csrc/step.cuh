@@ -477,7 +477,12 @@ __device__ __forceinline__ uint32_t cell_find(const DeviceWorld& w, uint32_t liv
 // every collider's primary entry (level_links.wgsl:6-65; one thread per collider, whose primary entry
 // is its first emitted slot), and the same-cell mates of every sorted entry (cell_pairs.wgsl:6-50).
 // The pair set does not depend on which kernel emits a pair first: the list is sorted afterwards.
-__global__ void k_pairs_coarse(DeviceWorld w) {
+//
+// The coarse links spread over gridDim.y: thread (i, y) walks collider i's cells at the occupied
+// levels whose rank among the occupied levels is y, y + gridDim.y, ... (the walk of one collider is
+// a chain of dependent lookups; splitting it by level shortens the chain a thread waits through).
+constexpr uint32_t kCoarseLevelSlices = 4u;
+__global__ void __launch_bounds__(128) k_pairs_coarse(DeviceWorld w) {
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
     const float grid = base_cell(w);
     const uint32_t occupied =
@@ -496,10 +501,13 @@ __global__ void k_pairs_coarse(DeviceWorld w) {
         if (!(awake || coarse_active)) continue;
         const uint32_t level = w.c_level[e.info & DYN_ENTRY_INDEX_MASK];
         const uint32_t world = w.body_world[e.group];
-        uint32_t coarser = occupied & ~((1u << min(level + 1u, 31u)) - 1u);
-        while (coarser != 0u) {
-            uint32_t link = 31u - __clz(coarser);
-            coarser &= ~(1u << link);
+        const uint32_t coarser = occupied & ~((1u << min(level + 1u, 31u)) - 1u);
+        // the levels of this slice: every gridDim.y-th set bit of `coarser`, from the lowest
+        uint32_t rest = coarser;
+        for (uint32_t skip = 0; skip < blockIdx.y && rest != 0u; ++skip) rest &= rest - 1u;
+        while (rest != 0u) {
+            const uint32_t link = (uint32_t)__ffs(rest) - 1u;
+            for (uint32_t skip = 0; skip < gridDim.y && rest != 0u; ++skip) rest &= rest - 1u;
             float cs = level_size(link, grid);
             I3 lo = floor_div(e.mn, cs), hi = floor_div(e.mx, cs);
             // A box spans at most two cells per axis at any level coarser than its own; a wider
@@ -656,7 +664,7 @@ __global__ void k_pair_class(DeviceWorld w) {
             }
         } while (false);
         if (cls < 0) {
-            w.pair_flag[index] = 0u;
+            continue;  // answered here: no contact
         } else if (cls == PC_ANALYTIC) {  // one branch per list: an aggregated append needs one target
             w.np_list[append_slot(&w.ctl[CTL_LIST0 + PC_ANALYTIC])] = index;
         } else if (cls == PC_BOXES) {
@@ -716,20 +724,16 @@ __device__ __forceinline__ void narrow_pair(const DeviceWorld& w, const dyn_step
             if (!convex_pair_manifold(w, a, b, hit.normal, &m)) mani_push(&m, hit.point, -hit.distance, kFeatPoint);
         }
     }
-    uint32_t valid = 0u;
     if (m.count > 0u) {
-        uint32_t slot = append_slot(&w.ctl[CTL_TMP]);
+        uint32_t slot = append_slot(&w.ctl[CTL_APPENDED]);
         if (slot < w.c_cap) {
             write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
                           w.c_mat[ss], w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine,
                           p.restitution_combine);
-            w.pair_slot[index] = slot;
-            valid = 1u;
         } else {
             add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
         }
     }
-    w.pair_flag[index] = valid;
 }
 
 // ---- the convex class in three phases ----
@@ -885,7 +889,6 @@ __global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dy
             L.count = 1u;
             // the exact centre-axis rejection of gjk_phase
             if (dot(sp.w, d) < -(L.margin + kRejectTolerance) * length(d)) {
-                w.pair_flag[L.index] = 0u;
                 L.state = GS_IDLE;
                 continue;
             }
@@ -946,11 +949,7 @@ __global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dy
                 } else if (L.dist > 0.0f) {
                     hit = Hit{L.dist, (L.pa + L.pb) * 0.5f, L.normal};
                 }
-                if (hit.distance <= L.margin) {
-                    push_hit(w, L.index, hit);
-                } else {
-                    w.pair_flag[L.index] = 0u;
-                }
+                if (hit.distance <= L.margin) push_hit(w, L.index, hit);
                 L.state = GS_IDLE;
             }
         }
@@ -973,11 +972,7 @@ __global__ void __launch_bounds__(32 * kEpaWarpsPerBlock) k_convex_epa(DeviceWor
         for (uint32_t k = 0; k < 4; ++k) simplex[k] = xyz(w.epa_simplex[4 * (size_t)e + k]);
         Hit hit = warp_penetrating_hit(w, a, b, simplex, m);
         if ((threadIdx.x & 31u) == 0u) {
-            if (hit.distance <= pair_margin(p, fb, sb)) {
-                push_hit(w, index, hit);
-            } else {
-                w.pair_flag[index] = 0u;
-            }
+            if (hit.distance <= pair_margin(p, fb, sb)) push_hit(w, index, hit);
         }
         __syncwarp();
     }
@@ -1001,22 +996,18 @@ __global__ void __launch_bounds__(128) k_convex_manifold(DeviceWorld w, dyn_step
         if (!convex_pair_manifold(w, a, b, xyz(h1), &m)) {
             if (h0.w <= margin) mani_push(&m, xyz(h0), -h0.w, kFeatPoint);
         }
-        uint32_t valid = 0u;
         if (m.count > 0u) {
-            uint32_t slot = append_slot(&w.ctl[CTL_TMP]);
+            uint32_t slot = append_slot(&w.ctl[CTL_APPENDED]);
             if (slot < w.c_cap) {
                 uint4 fi = w.ident[fr], si = w.ident[sr];
                 bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
                 write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
                               w.c_mat[ss], w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine,
                               p.restitution_combine);
-                w.pair_slot[index] = slot;
-                valid = 1u;
             } else {
                 add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
             }
         }
-        w.pair_flag[index] = valid;
     }
 }
 
@@ -1027,6 +1018,27 @@ __global__ void __launch_bounds__(128) k_narrow_class(DeviceWorld w, dyn_step_pa
     GRID_STRIDE(i, count) narrow_pair<kClass>(w, p, list[i]);
 }
 
+// ---- compaction (compact_scan.wgsl, compact_offsets.wgsl, compact_scatter.wgsl) ----
+// The reference sorts all candidate pairs and compacts the narrowphase output in pair order. Here
+// the pairs stay in emission order; the narrowphase appends its contacts to a staging set, and the
+// stored contacts alone are sorted by (lower, higher) collider slot and gathered. Each pair yields at
+// most one contact, so the contacts come out in the reference's order, for a sort of C keys instead
+// of P. When more contacts arrive than the capacity holds, which ones were stored depends on
+// completion order (the counts stay exact).
+__global__ void k_contact_keys(DeviceWorld w) {
+    const uint32_t c = min(w.ctl[CTL_APPENDED], w.c_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.counters[DYN_COUNTER_CONTACTS] = c;
+        w.ctl[CTL_CONTACTS] = c;
+        w.counters[DYN_COUNTER_BLOCKS] = c;
+    }
+    GRID_STRIDE(i, c) {
+        const uint4 ids = w.tmp.ids[i];
+        w.cmaj[i] = ids.x;
+        w.cmin[i] = ids.y;
+        w.cval[i] = i;
+    }
+}
 __device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi, const ContactSet& to, uint32_t ti, uint32_t cap) {
     uint4 rows = from.rows[fi];
     to.normal[ti] = from.normal[fi];
@@ -1034,8 +1046,7 @@ __device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi
     to.mat[ti] = from.mat[fi];
     to.ids[ti] = from.ids[fi];
     to.ids2[ti] = from.ids2[fi];
-    float4 ex = from.extra[fi];
-    to.extra[ti] = make_float4(ex.x, 0.0f, 0.0f, 0.0f);
+    to.extra[ti] = from.extra[fi];
     uint32_t count = rows.z & 0xFFu;
     for (uint32_t p = 0; p < count; ++p) {
         size_t f = (size_t)p * cap + fi, t = (size_t)p * cap + ti;
@@ -1045,26 +1056,11 @@ __device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi
         to.pos[t] = from.pos[f];
     }
 }
-
-// compact_scatter.wgsl:12-27 (ranks from the pair-flag scan): contacts in sorted pair order.
-__global__ void k_compact(DeviceWorld w) {
-    const uint32_t pairs = min(w.counters[DYN_COUNTER_PAIRS], w.p_cap);
-    const uint32_t valid = w.ctl[CTL_VALID];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        uint32_t c = min(valid, w.c_cap);
-        w.counters[DYN_COUNTER_CONTACTS] = valid;
-        w.ctl[CTL_CONTACTS] = c;
-        w.counters[DYN_COUNTER_BLOCKS] = c;
-    }
-    GRID_STRIDE(index, pairs) {
-        if (w.pair_flag[index] == 0u) continue;
-        uint32_t dst = w.pair_rank[index];
-        if (dst >= w.c_cap) {
-            add_counter(&w.counters[DYN_COUNTER_REFUSED_CONTACTS], 1u);
-            continue;
-        }
-        copy_contact(w.tmp, w.pair_slot[index], w.cur, dst, w.c_cap);
-        w.matched[dst] = 0u;
+__global__ void k_contact_gather(DeviceWorld w) {
+    const uint32_t c = w.ctl[CTL_CONTACTS];
+    GRID_STRIDE(i, c) {
+        copy_contact(w.tmp, w.cval[i], w.cur, i, w.c_cap);
+        w.matched[i] = 0u;
     }
 }
 
@@ -1288,6 +1284,14 @@ __device__ __forceinline__ void accumulate(int32_t* deltas, uint32_t row, f3 lin
     atomicAdd(d + 3, solver_word(ang.x, scale));
     atomicAdd(d + 4, solver_word(ang.y, scale));
     atomicAdd(d + 5, solver_word(ang.z, scale));
+}
+// The linear words alone: position corrections carry no angular part, and adding a zero word
+// changes nothing, so the three angular atomics are left out.
+__device__ __forceinline__ void accumulate_linear(int32_t* deltas, uint32_t row, f3 lin, float scale) {
+    int32_t* d = deltas + 8u * row;
+    atomicAdd(d + 0, solver_word(lin.x, scale));
+    atomicAdd(d + 1, solver_word(lin.y, scale));
+    atomicAdd(d + 2, solver_word(lin.z, scale));
 }
 __device__ __forceinline__ void make_tangents(f3 n, f3* t1, f3* t2) {
     f3 t = fabsf(n.x) > 0.9f ? mk3(0.0f, 1.0f, 0.0f) : mk3(1.0f, 0.0f, 0.0f);
@@ -1661,13 +1665,13 @@ __device__ __forceinline__ void position_block(const DeviceWorld& w, const dyn_s
     // same 1, without an atomic on the shared row of a static body.
     if (ima > 0.0f) {
         atomicAdd(&w.contributions[r.x], 1u);
-        accumulate(w.pdelta, r.x, la, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        accumulate_linear(w.pdelta, r.x, la, DYN_SOLVER_POSITION_SCALE);
     } else if (w.contributions[r.x] == 0u) {
         w.contributions[r.x] = 1u;
     }
     if (imb > 0.0f) {
         atomicAdd(&w.contributions[r.y], 1u);
-        accumulate(w.pdelta, r.y, lb, s3(0.0f), DYN_SOLVER_POSITION_SCALE);
+        accumulate_linear(w.pdelta, r.y, lb, DYN_SOLVER_POSITION_SCALE);
     } else if (w.contributions[r.y] == 0u) {
         w.contributions[r.y] = 1u;
     }

@@ -23,7 +23,6 @@ enum Stage : uint32_t {
     ST_ENTRIES,
     ST_ENTRY_SORT,
     ST_PAIRS,
-    ST_PAIR_SORT,
     ST_NARROWPHASE,
     ST_COMPACT,
     ST_IDENTITY,
@@ -39,7 +38,7 @@ enum Stage : uint32_t {
     ST_COUNT
 };
 static const char* kStageNames[ST_COUNT] = {"begin",       "aabb",     "entries",   "entry_sort",     "pairs",
-                                            "pair_sort",   "narrowphase", "compact", "identity",       "islands",
+                                            "narrowphase", "compact",  "identity",       "islands",
                                             "wake_live",   "solver_prepare", "integrate", "warm_start", "velocity",
                                             "advance",     "position", "sleep"};
 
@@ -214,11 +213,12 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.cell_table, (size_t)1 << dw.cell_bits);
         A(dw.pmaj, P);
         A(dw.pmin, P);
-        A(dw.pmaj_alt, P);
-        A(dw.pmin_alt, P);
-        A(dw.pair_slot, P);
-        A(dw.pair_flag, P);
-        A(dw.pair_rank, P);
+        A(dw.cmaj, C);
+        A(dw.cmin, C);
+        A(dw.cval, C);
+        A(dw.cmaj_alt, C);
+        A(dw.cmin_alt, C);
+        A(dw.cval_alt, C);
         A(dw.np_list, 3 * (size_t)P);
         A(dw.epa_list, P);
         A(dw.epa_simplex, 4 * (size_t)P);
@@ -572,12 +572,9 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_PAIRS);
     k_cell_clear<<<blocks_for(1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
     k_cell_insert<<<blocks_for(E, 256), 256, 0, s>>>(dw);
-    k_pairs_coarse<<<blocks_for(K, 128), 128, 0, s>>>(dw);
+    k_pairs_coarse<<<dim3(blocks_for(K, 128), kCoarseLevelSlices), 128, 0, s>>>(dw);
     k_pairs_cell<<<blocks_for(E, 256), 256, 0, s>>>(dw);
-    mark(ST_PAIR_SORT);
-    uint32_t words = key_words(std::max(dw.k, 1u));
-    record_sort(d, s, dw.pmaj, dw.pmin, nullptr, dw.pmaj_alt, dw.pmin_alt, nullptr, dw.counters + DYN_COUNTER_PAIRS, 0, P,
-                words, words);
+    // the candidate pairs stay in emission order; the contacts are sorted into pair order below
     mark(ST_NARROWPHASE);
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
     k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
@@ -587,8 +584,11 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     mark(ST_COMPACT);
-    record_scan(d, s, dw.pair_flag, dw.pair_rank, dw.counters + DYN_COUNTER_PAIRS, 0, P, dw.ctl + CTL_VALID);
-    k_compact<<<blocks_for(P, 256), 256, 0, s>>>(dw);
+    k_contact_keys<<<blocks_for(C, 256), 256, 0, s>>>(dw);
+    const uint32_t words = key_words(std::max(dw.k, 1u));
+    record_sort(d, s, dw.cmaj, dw.cmin, dw.cval, dw.cmaj_alt, dw.cmin_alt, dw.cval_alt, dw.ctl + CTL_CONTACTS, 0, C, words,
+                words);
+    k_contact_gather<<<blocks_for(C, 128), 128, 0, s>>>(dw);
     mark(ST_IDENTITY);
     k_relay<<<blocks_for(C, 128), 128, 0, s>>>(dw);
     k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
@@ -1031,9 +1031,18 @@ DYN_API dyn_status dyn_debug_pairs(dyn_world* w, uint32_t* major, uint32_t* mino
     p = std::min(p, dw.p_cap);
     if (count) *count = p;
     if (!major) return DYN_OK;
+    // the device keeps the pairs in emission order; the readback sorts them (the reference's order)
+    std::vector<uint32_t> maj(p), mnr(p);
+    DYN_CUDA(cudaMemcpy(maj.data(), dw.pmaj, (size_t)p * 4, cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(mnr.data(), dw.pmin, (size_t)p * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> keys(p);
+    for (uint32_t i = 0; i < p; ++i) keys[i] = ((uint64_t)maj[i] << 32) | mnr[i];
+    std::sort(keys.begin(), keys.end());
     uint32_t m = std::min(cap, p);
-    DYN_CUDA(cudaMemcpy(major, dw.pmaj, m * 4, cudaMemcpyDeviceToHost));
-    DYN_CUDA(cudaMemcpy(minor, dw.pmin, m * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < m; ++i) {
+        major[i] = (uint32_t)(keys[i] >> 32);
+        minor[i] = (uint32_t)keys[i];
+    }
     return DYN_OK;
 }
 
@@ -1048,10 +1057,13 @@ DYN_API dyn_status dyn_debug_contacts(dyn_world* w, dyn_contact_record* out, uin
     if (!d->stepped) c = 0;
     if (count) *count = c;
     if (!out) return DYN_OK;
-    uint32_t m = std::min(cap, c);
+    // the device keeps the contacts in the order the narrowphase appended them; the readback sorts
+    // them by collider pair (the reference's compacted order)
+    uint32_t m = c;
     uint32_t C = dw.c_cap;
     std::vector<float4> normal(m), mat(m), extra(m), la(4 * (size_t)C), lb(4 * (size_t)C), acc(4 * (size_t)C), pos(4 * (size_t)C);
     std::vector<uint4> rows(m), ids(m), ids2(m);
+    std::vector<dyn_contact_record> all(m);
     DYN_CUDA(cudaMemcpy(normal.data(), dw.cur.normal, m * 16, cudaMemcpyDeviceToHost));
     DYN_CUDA(cudaMemcpy(mat.data(), dw.cur.mat, m * 16, cudaMemcpyDeviceToHost));
     DYN_CUDA(cudaMemcpy(extra.data(), dw.cur.extra, m * 16, cudaMemcpyDeviceToHost));
@@ -1063,7 +1075,7 @@ DYN_API dyn_status dyn_debug_contacts(dyn_world* w, dyn_contact_record* out, uin
     DYN_CUDA(cudaMemcpy(acc.data(), dw.cur.acc, 4 * (size_t)C * 16, cudaMemcpyDeviceToHost));
     DYN_CUDA(cudaMemcpy(pos.data(), dw.cur.pos, 4 * (size_t)C * 16, cudaMemcpyDeviceToHost));
     for (uint32_t i = 0; i < m; ++i) {
-        dyn_contact_record& r = out[i];
+        dyn_contact_record& r = all[i];
         std::memset(&r, 0, sizeof(r));
         r.a = ids[i].x;
         r.b = ids[i].y;
@@ -1106,6 +1118,10 @@ DYN_API dyn_status dyn_debug_contacts(dyn_world* w, dyn_contact_record* out, uin
             std::memcpy(&q.feature, &acc[o].w, 4);
         }
     }
+    std::sort(all.begin(), all.end(), [](const dyn_contact_record& x, const dyn_contact_record& y) {
+        return x.a < y.a || (x.a == y.a && x.b < y.b);
+    });
+    std::memcpy(out, all.data(), (size_t)std::min(cap, c) * sizeof(dyn_contact_record));
     return DYN_OK;
 }
 
