@@ -557,15 +557,14 @@ __device__ Mani box_box_sat(const DBody& fb, const DColl& fc, const DBody& sb, c
 
 // ---- convex support maps (convex.wgsl:1-91) ----
 __device__ f3 support_local(const DeviceWorld& w, const WShape& s, f3 d) {
-    f3 n = normalize(d);
-    if (s.kind == 1u) return n * s.radius;
+    if (s.kind == 1u) return normalize(d) * s.radius;
     if (s.kind == 2u) {
         f3 signs = mk3(d.x > 0.0f ? 1.0f : -1.0f, d.y > 0.0f ? 1.0f : -1.0f, d.z > 0.0f ? 1.0f : -1.0f);
         return signs * s.half_extents;
     }
     if (s.kind == 3u) {
         f3 tip = mk3(0.0f, 1.0f, 0.0f) * s.half_height * (d.y > 0.0f ? 1.0f : -1.0f);
-        return tip + n * s.radius;
+        return tip + normalize(d) * s.radius;
     }
     if (s.kind == 4u) {
         f3 base = mk3(0.0f, 1.0f, 0.0f) * s.half_height * (d.y > 0.0f ? 1.0f : -1.0f);
@@ -575,11 +574,23 @@ __device__ f3 support_local(const DeviceWorld& w, const WShape& s, f3 d) {
     }
     const dyn_shape_source_record& src = w.sources[s.source];
     const float4* verts = w.vertices + src.vertex_offset;
+    const uint32_t count = src.vertex_count;
     float best_dot = -3.402823466e38f;
     f3 best = s3(0.0f);
-    for (uint32_t i = 0; i < src.vertex_count; ++i) {
-        f3 v = xyz(__ldg(verts + i));
-        float sd = dot(v, d);
+    // four loads in flight, then the same comparisons in index order as the one-at-a-time scan
+    uint32_t i = 0;
+    for (; i + 4u <= count; i += 4u) {
+        const f3 v0 = xyz(__ldg(verts + i)), v1 = xyz(__ldg(verts + i + 1u));
+        const f3 v2 = xyz(__ldg(verts + i + 2u)), v3 = xyz(__ldg(verts + i + 3u));
+        const float s0 = dot(v0, d), s1 = dot(v1, d), s2 = dot(v2, d), s3_ = dot(v3, d);
+        if (s0 > best_dot) { best_dot = s0; best = v0; }
+        if (s1 > best_dot) { best_dot = s1; best = v1; }
+        if (s2 > best_dot) { best_dot = s2; best = v2; }
+        if (s3_ > best_dot) { best_dot = s3_; best = v3; }
+    }
+    for (; i < count; ++i) {
+        const f3 v = xyz(__ldg(verts + i));
+        const float sd = dot(v, d);
         if (sd > best_dot) {
             best_dot = sd;
             best = v;

@@ -1175,11 +1175,14 @@ __device__ __forceinline__ uint32_t island_find(const DeviceWorld& w, uint32_t n
     return current;
 }
 // island_couple (island_link.wgsl:3-45): a static row carries its wake flag to the other row, and
-// two dynamic rows join one island. Returns false when the bounded union gave up.
-__device__ __forceinline__ bool island_couple(const DeviceWorld& w, uint32_t first, uint32_t second) {
+// two dynamic rows join one island. The union returns false when its bounded retries gave up.
+__device__ __forceinline__ void island_carry(const DeviceWorld& w, uint32_t first, uint32_t second) {
     uint32_t dc = w.nd;
     if (second >= dc && w.wake_flags[second] != 0u) atomicOr(&w.wake_flags[first], 1u);
     if (first >= dc && w.wake_flags[first] != 0u) atomicOr(&w.wake_flags[second], 1u);
+}
+__device__ __forceinline__ bool island_union(const DeviceWorld& w, uint32_t first, uint32_t second) {
+    uint32_t dc = w.nd;
     if (first >= dc || second >= dc || first == second) return true;
     for (uint32_t attempt = 0; attempt < 256u; ++attempt) {
         uint32_t a = island_find(w, first), b = island_find(w, second);
@@ -1189,13 +1192,31 @@ __device__ __forceinline__ bool island_couple(const DeviceWorld& w, uint32_t fir
     }
     return false;
 }
+__device__ __forceinline__ bool island_couple(const DeviceWorld& w, uint32_t first, uint32_t second) {
+    island_carry(w, first, second);
+    return island_union(w, first, second);
+}
+// The contacts join islands in two passes with a flatten between (the sampling idea of Afforest,
+// Sutton et al. 2018): first only the first contact of each collider's run in the sorted list,
+// which already ties most of a pile together; after the flatten every row points at its root, so
+// a later contact whose rows share a parent is skipped without a find. Which contact hooks which
+// root does not change the islands, and each island's root stays its smallest row.
+template <bool kSample>
 __global__ void k_island_link(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     GRID_STRIDE(i, count) {
         uint4 r = w.cur.rows[i];
         uint32_t pc = r.z & 0xFFu, sensor = (r.z >> 8) & 0xFFu;
         if (pc == 0u || sensor == 1u || !touches(w.cur, i, w.c_cap, p.slop)) continue;
-        if (!island_couple(w, r.x, r.y)) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
+        const bool first_of_run = i == 0u || w.cur.ids[i - 1u].x != w.cur.ids[i].x;
+        if (kSample) {
+            island_carry(w, r.x, r.y);
+            if (!first_of_run) continue;
+        } else {
+            if (first_of_run) continue;
+            if (r.x < w.nd && r.y < w.nd && __ldcg(w.parents + r.x) == __ldcg(w.parents + r.y)) continue;
+        }
+        if (!island_union(w, r.x, r.y)) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
     }
 }
 // island_flatten.wgsl:4-8 repeated ilog2(max(N,2))+1 times leaves every row pointing at its root
@@ -1218,6 +1239,8 @@ __global__ void k_island_aggregate(DeviceWorld w) {
         uint32_t root = w.parents[i];
         if (root == i) add_counter(&w.counters[DYN_COUNTER_ISLANDS], 1u);
         if (w.wake_flags[i] == 0u && w.motion[i] == 0u) continue;
+        // a large island's rows all aim at one word: once it holds the mark, the max is a no-op
+        if (__ldcg(w.istate + root) >= DYN_ISLAND_WAKE) continue;
         atomicMax(&w.istate[root], DYN_ISLAND_WAKE);
     }
 }

@@ -593,7 +593,9 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_relay<<<blocks_for(C, 128), 128, 0, s>>>(dw);
     k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
     mark(ST_ISLANDS);
-    k_island_link<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    k_island_link<true><<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    k_island_link<false><<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
     if (dw.jcount) k_island_link_joints<<<blocks_for(dw.jcount, 256), 256, 0, s>>>(dw);
     k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     k_island_aggregate<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
