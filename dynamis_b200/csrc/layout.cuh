@@ -137,7 +137,9 @@ struct DeviceWorld {
     uint32_t* parents;
     uint32_t* istate;
     uint32_t* live;
-    uint32_t* solver_rows;
+    uint32_t* solver_rows;  // rows with a contact block, ascending
+    uint32_t* row_flag;     // [n] 1 for a row with a contact block
+    uint32_t* row_offset;   // [n] its place in solver_rows
     int32_t* vdelta;  // [8n]
     int32_t* pdelta;  // [8n]
     uint32_t* contributions;

@@ -211,6 +211,7 @@ __global__ void k_begin(DeviceWorld w, dyn_step_params p) {
             w.istate[i] = 0u;
         }
         h.aux.z = 0u;
+        w.row_flag[i] = 0u;
         w.resolution[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
@@ -1292,10 +1293,18 @@ __global__ void k_solver_blocks(DeviceWorld w, dyn_step_params p) {
             float4 lb = w.cur.lb[o];
             w.cur.lb[o] = make_float4(lb.x, lb.y, lb.z, target);
         }
-        if (atomicAdd(&w.hot[r.x].aux.z, 1u) == 0u) w.solver_rows[append_slot(&w.ctl[CTL_SOLVER_ROWS])] = r.x;
-        if (atomicAdd(&w.hot[r.y].aux.z, 1u) == 0u) w.solver_rows[append_slot(&w.ctl[CTL_SOLVER_ROWS])] = r.y;
+        if (atomicAdd(&w.hot[r.x].aux.z, 1u) == 0u) w.row_flag[r.x] = 1u;
+        if (atomicAdd(&w.hot[r.y].aux.z, 1u) == 0u) w.row_flag[r.y] = 1u;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[DYN_COUNTER_BLOCKS] = count;
+}
+// The claimed rows in ascending order (scanned flags): the applies then walk the body rows in
+// memory order instead of claim order. The set of rows is the reference's; their order changes
+// nothing, each row being applied on its own.
+__global__ void k_solver_row_list(DeviceWorld w) {
+    GRID_STRIDE(i, w.n) {
+        if (w.row_flag[i] != 0u) w.solver_rows[w.row_offset[i]] = i;
+    }
 }
 
 __device__ __forceinline__ int32_t solver_word(float value, float scale) { return (int32_t)wclamp(value * scale, -2.0e9f, 2.0e9f); }

@@ -234,6 +234,8 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.istate, N);
         A(dw.live, N);
         A(dw.solver_rows, N);
+        A(dw.row_flag, N);
+        A(dw.row_offset, N);
         A(dw.vdelta, 8 * (size_t)N);
         A(dw.pdelta, 8 * (size_t)N);
         A(dw.contributions, N);
@@ -603,6 +605,8 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_wake_live<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     mark(ST_SOLVER_PREPARE);
     k_solver_blocks<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    record_scan(d, s, dw.row_flag, dw.row_offset, nullptr, std::max(dw.n, 1u), N, dw.ctl + CTL_SOLVER_ROWS);
+    k_solver_row_list<<<blocks_for(N, 256), 256, 0, s>>>(dw);
     for (uint32_t sub = 0; sub < p.substeps; ++sub) {
         mark(ST_INTEGRATE);
         k_integrate<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
