@@ -1121,6 +1121,22 @@ __device__ Hit separated_hit(const DeviceWorld& w, const WShape& first, const WS
 // ---- warp-cooperative pieces ----
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
+// An unsigned key that orders floats above -FLT_MAX as the floats compare: -0 and +0 share a key
+// (they compare equal), and NaN, -inf and -FLT_MAX (never above the scans' -FLT_MAX start) get 0.
+__device__ __forceinline__ uint32_t order_key(float x) {
+    if (!(x > -3.402823466e38f)) return 0u;
+    const uint32_t b = __float_as_uint(x == 0.0f ? 0.0f : x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+// The lane holding the first maximum of a warp-wide scan: the largest key, then the lowest index
+// among the lanes that hold it (each lane holds the first index of its own maximum). Returns
+// 0xFFFFFFFF when no lane holds a candidate.
+__device__ __forceinline__ uint32_t warp_first_max(uint32_t key, uint32_t index) {
+    const uint32_t top = __reduce_max_sync(kFull, key);
+    if (top == 0u) return 0xFFFFFFFFu;
+    return __reduce_min_sync(kFull, key == top ? index : 0xFFFFFFFFu);
+}
+
 // support_local over a hull with the warp's lanes striding the vertices; the reduction keeps the
 // sequential scan's choice: the largest dot product, the lowest index among equal ones.
 __device__ __forceinline__ f3 warp_support_local(const DeviceWorld& w, const WShape& s, f3 d) {
@@ -1137,15 +1153,7 @@ __device__ __forceinline__ f3 warp_support_local(const DeviceWorld& w, const WSh
             bi = i;
         }
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        float ob = __shfl_xor_sync(kFull, best, off);
-        uint32_t oi = __shfl_xor_sync(kFull, bi, off);
-        if (oi != 0xFFFFFFFFu && (bi == 0xFFFFFFFFu || ob > best || (ob == best && oi < bi))) {
-            best = ob;
-            bi = oi;
-        }
-    }
+    bi = warp_first_max(bi == 0xFFFFFFFFu ? 0u : order_key(best), bi);
     return bi == 0xFFFFFFFFu ? s3(0.0f) : xyz(__ldg(verts + bi));
 }
 __device__ __forceinline__ f3 warp_support(const DeviceWorld& w, const WShape& s, f3 direction) {
@@ -1191,19 +1199,15 @@ __device__ __forceinline__ void warp_best_face(const EpaWarpShared& m, uint32_t 
             any = true;
         }
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        float od = __shfl_xor_sync(kFull, bd, off);
-        uint32_t oi = __shfl_xor_sync(kFull, bi, off);
-        bool oa = __shfl_xor_sync(kFull, any, off);
-        if (oa && (!any || od < bd || (od == bd && oi < bi))) {
-            bd = od;
-            bi = oi;
-            any = true;
-        }
+    // the first minimum: the first maximum of the negated distances (negation is exact)
+    const uint32_t first = warp_first_max(any ? order_key(-bd) : 0u, any ? bi : 0xFFFFFFFFu);
+    if (first == 0xFFFFFFFFu) {
+        *best_dist = 3.402823466e38f;
+        *best_face = 0u;
+        return;
     }
-    *best_dist = bd;
-    *best_face = any ? bi : 0u;
+    *best_dist = __shfl_sync(kFull, bd, first & 31u);  // face j lives on lane j % 32
+    *best_face = first;
 }
 
 // convex.wgsl:286-437 on one warp. All lanes return the same result.
@@ -1352,7 +1356,9 @@ __device__ Hit warp_penetrating_hit(const DeviceWorld& w, const WShape& first, c
         f3 pb = warp_support(w, second, -epa.normal);
         result = Hit{-epa.depth, (pa + pb) * 0.5f, epa.normal};
     } else {
-        // convex_penetration_probe over the four-point simplex, centre direction and six axes
+        // convex_penetration_probe over the four-point simplex, centre direction and six axes: each
+        // direction's projection depth on its own lane (the lane scans the vertices itself), then
+        // the first minimum in direction order, as the sequential loop keeps it
         f3 probed[16];
         uint32_t pc = 0;
         for (uint32_t i = 0; i < 4; ++i)
@@ -1366,15 +1372,18 @@ __device__ Hit warp_penetrating_hit(const DeviceWorld& w, const WShape& first, c
         const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
         for (uint32_t i = 0; i < 6; ++i)
             if (pc < 16u) probed[pc++] = mk3(ax[i][0], ax[i][1], ax[i][2]);
+        const uint32_t lane = threadIdx.x & 31u;
+        const float mine = lane < pc ? support_projection_depth(w, first, second, probed[lane]) : 3.402823466e38f;
         float best_depth = 3.402823466e38f;
-        f3 best_normal = mk3(0.0f, 1.0f, 0.0f);
+        uint32_t best_i = pc;
         for (uint32_t i = 0; i < pc; ++i) {
-            float depth = warp_projection_depth(w, first, second, probed[i]);
+            const float depth = __shfl_sync(kFull, mine, i);
             if (depth < best_depth) {
                 best_depth = depth;
-                best_normal = normalize(probed[i]);
+                best_i = i;
             }
         }
+        const f3 best_normal = best_i < pc ? normalize(probed[best_i]) : mk3(0.0f, 1.0f, 0.0f);
         f3 pa = warp_support(w, first, best_normal);
         f3 pb = warp_support(w, second, -best_normal);
         result = Hit{-best_depth, (pa + pb) * 0.5f, best_normal};
