@@ -1485,27 +1485,23 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
     f3 t1 = xyz(tw1), t2 = xyz(sr.tangent2[i]);
     float twist_mass = tw1.w;
     uint32_t pc = r.z & 0xFFu;
-    f3 ra[4], rb[4];
-    float4 acc[4];
+    // One point at a time: every point's impulse is computed from the velocities the block started
+    // with (pf, ps), so applying each to first/second as soon as it is known gives the same sums,
+    // in the same order, as applying all four after the loop; the old normal accumulators are summed
+    // in point order as they are read. Only one point's data is live at a time.
     float normal_total = 0.0f;
     #pragma unroll
     for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) {
         size_t o = (size_t)pi * cap + i;
-        acc[pi] = w.cur.acc[o];
-        normal_total = normal_total + wmax(acc[pi].x, 0.0f);
-    }
-    f3 impulses[4];
-    #pragma unroll
-    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) {
-        size_t o = (size_t)pi * cap + i;
+        float4 acc = w.cur.acc[o];
+        normal_total = normal_total + wmax(acc.x, 0.0f);
         float4 a4 = sr.arm_a[o], b4 = sr.arm_b[o];
         float4 m2 = sr.masses[o];
-        ra[pi] = xyz(a4);
-        rb[pi] = xyz(b4);
+        const f3 ra = xyz(a4), rb = xyz(b4);
         float normal_mass = a4.w, truth = b4.w;
         float depth = m2.z, target = m2.w;
-        float an = acc[pi].x, at1 = acc[pi].y, at2 = acc[pi].z;
-        f3 rel = point_velocity_arm(ps, rb[pi]) - point_velocity_arm(pf, ra[pi]);
+        float an = acc.x, at1 = acc.y, at2 = acc.z;
+        f3 rel = point_velocity_arm(ps, rb) - point_velocity_arm(pf, ra);
         float normal_speed = dot(rel, normal);
         float delta;
         if (mat.z <= 0.0f) {
@@ -1519,22 +1515,21 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
             delta = truth * (wanted - an) / normal_mass;
         }
         float next_n = wmax(0.0f, an + delta);
-        impulses[pi] = s3(0.0f) + normal * (next_n - an);
+        f3 impulse = s3(0.0f) + normal * (next_n - an);
         an = next_n;
         float limit = friction * an;
         float t1_speed = dot(rel, t1);
         float next_t1 = wclamp(at1 - t1_speed / m2.x, -limit, limit);
-        impulses[pi] = impulses[pi] + t1 * (next_t1 - at1);
+        impulse = impulse + t1 * (next_t1 - at1);
         at1 = next_t1;
         float t2_speed = dot(rel, t2);
         float remaining = sqrtf(wmax(limit * limit - at1 * at1, 0.0f));
         float next_t2 = wclamp(at2 - t2_speed / m2.y, -remaining, remaining);
-        impulses[pi] = impulses[pi] + t2 * (next_t2 - at2);
+        impulse = impulse + t2 * (next_t2 - at2);
         at2 = next_t2;
-        acc[pi] = make_float4(an, at1, at2, acc[pi].w);
+        w.cur.acc[o] = make_float4(an, at1, at2, acc.w);
+        pair_impulse_arms(&first, &second, ra, rb, impulse);
     }
-    #pragma unroll
-    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) pair_impulse_arms(&first, &second, ra[pi], rb[pi], impulses[pi]);
     f3 rel_spin = second.angular_velocity - first.angular_velocity;
     f3 planar = rel_spin - normal * dot(rel_spin, normal);
     float planar_len = length(planar);
@@ -1557,8 +1552,6 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
             second.angular_velocity = second.angular_velocity + dbody_iinv(second, normal * applied);
         }
     }
-    #pragma unroll
-    for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) w.cur.acc[(size_t)pi * cap + i] = acc[pi];
     f3 da = first.velocity - pf.velocity, sa = first.angular_velocity - pf.angular_velocity;
     f3 db = second.velocity - ps.velocity, sb = second.angular_velocity - ps.angular_velocity;
     if (!dbody_inert(pf)) accumulate(w.vdelta, r.x, da, sa, DYN_SOLVER_VELOCITY_SCALE);
