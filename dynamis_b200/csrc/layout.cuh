@@ -64,6 +64,7 @@ enum Ctl : uint32_t {
     CTL_HITS = 14,   // convex pairs queued for the manifold
     CTL_CELL_OVERFLOW = 15,  // the cell table could not place a run: lookups fall back to searching
     CTL_GJK_NEXT = 16,       // next convex pair ticket of the GJK kernel
+    CTL_GJK_PAIRS = 17,      // convex pairs past the centre-axis rejection
     CTL_COUNT = 32
 };
 
@@ -124,7 +125,7 @@ struct DeviceWorld {
     uint32_t* cmaj_alt;
     uint32_t* cmin_alt;
     uint32_t* cval_alt;
-    uint32_t* np_list;  // [3][p_cap] pair indices per narrowphase class
+    uint32_t* np_list;  // [4][p_cap] pair indices per narrowphase class, then the GJK's convex pairs
     uint32_t* epa_list;      // pair indices of penetrating convex pairs
     float4* epa_simplex;     // [4][slot]: the GJK simplex (w.xyz) EPA starts from
     uint32_t* hit_list;      // pair indices of convex hits

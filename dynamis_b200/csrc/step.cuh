@@ -851,10 +851,32 @@ __device__ __forceinline__ void gjk_separated(GjkLane& L) {
     probe_begin(L);
 }
 
-__global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
-    __shared__ float simplex_slices[kGjkThreads * kSimplexStride];
+// The centre-axis rejection of gjk_phase for every convex pair, ahead of the state machine: one
+// support-pair evaluation per pair with the arithmetic of the state machine's first trip, one thread
+// per pair. In a pile about nine convex pairs in ten stop here; the rest go on to k_convex_gjk,
+// whose first trip repeats the same test and passes.
+__global__ void __launch_bounds__(128) k_convex_reject(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = min(w.ctl[CTL_LIST0 + PC_CONVEX], w.p_cap);
     const uint32_t* list = w.np_list + (size_t)PC_CONVEX * w.p_cap;
+    uint32_t* gjk_pairs = w.np_list + (size_t)PC_COUNT * w.p_cap;
+    GRID_STRIDE(i, count) {
+        const uint32_t index = list[i];
+        WShape a, b;
+        DBody fb, sb;
+        convex_shapes(w, index, &a, &b, &fb, &sb);
+        const float margin = pair_margin(p, fb, sb);
+        f3 d = b.center - a.center;
+        if (length(d) < 1e-8f) d = mk3(1.0f, 0.0f, 0.0f);
+        const SPt sp = support_pair(w, a, b, d);
+        if (dot(sp.w, d) < -(margin + kRejectTolerance) * length(d)) continue;
+        gjk_pairs[append_slot(&w.ctl[CTL_GJK_PAIRS])] = index;
+    }
+}
+
+__global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dyn_step_params p) {
+    __shared__ float simplex_slices[kGjkThreads * kSimplexStride];
+    const uint32_t count = min(w.ctl[CTL_GJK_PAIRS], w.p_cap);
+    const uint32_t* list = w.np_list + (size_t)PC_COUNT * w.p_cap;
     GjkLane L;
     L.s = reinterpret_cast<SPt*>(simplex_slices + threadIdx.x * kSimplexStride);
     L.state = GS_IDLE;

@@ -219,7 +219,7 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.cmaj_alt, C);
         A(dw.cmin_alt, C);
         A(dw.cval_alt, C);
-        A(dw.np_list, 3 * (size_t)P);
+        A(dw.np_list, (PC_COUNT + 1) * (size_t)P);
         A(dw.epa_list, P);
         A(dw.epa_simplex, 4 * (size_t)P);
         A(dw.hit_list, P);
@@ -581,6 +581,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
     k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    k_convex_reject<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
     k_convex_gjk<<<148u * 6u, 128, 0, s>>>(dw, p);
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
