@@ -65,6 +65,7 @@ enum Ctl : uint32_t {
     CTL_CELL_OVERFLOW = 15,  // the cell table could not place a run: lookups fall back to searching
     CTL_GJK_NEXT = 16,       // next convex pair ticket of the GJK kernel
     CTL_GJK_PAIRS = 17,      // convex pairs past the centre-axis rejection
+    CTL_PROBES = 18,         // separated convex pairs queued for the penetration probe
     CTL_COUNT = 32
 };
 
@@ -128,6 +129,8 @@ struct DeviceWorld {
     uint32_t* np_list;  // [4][p_cap] pair indices per narrowphase class, then the GJK's convex pairs
     uint32_t* epa_list;      // pair indices of penetrating convex pairs
     float4* epa_simplex;     // [4][slot]: the GJK simplex (w.xyz) EPA starts from
+    uint32_t* probe_list;    // pair indices of separated convex pairs
+    float4* probe_data;      // [6][slot]: their simplex, point count, distance, closest points, normal
     uint32_t* hit_list;      // pair indices of convex hits
     float4* hit_data;        // [2][slot]: point.xyz + distance, normal.xyz
     ContactSet cur;  // this step's contacts in sorted pair order

@@ -772,15 +772,15 @@ constexpr float kRejectTolerance = 1e-3f;
 // supports together instead of waiting for the warp's slowest pair, whatever their pairs' iteration
 // counts. Each state does the same arithmetic, in the same order, as gjk_phase followed by
 // separated_hit (narrow.cuh); only the interleaving of pairs on a lane changes.
-enum GjkState : uint32_t { GS_IDLE = 0, GS_FIRST = 1, GS_ITER = 2, GS_EXPAND = 3, GS_PROBE = 4 };
+enum GjkState : uint32_t { GS_IDLE = 0, GS_FIRST = 1, GS_ITER = 2, GS_EXPAND = 3 };
 // simplex triples in the probe's order (i < j < k ascending), one per bit of GjkLane::triples
 __constant__ uint8_t kProbeTriple[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
 constexpr uint32_t kProbeCentre = 4u, kProbeAxes = 5u, kProbeEnd = 11u;
 
 struct GjkLane {
-    uint32_t state, index, count, iter, probe, triples;
-    float tiny, margin, dist, best;
-    f3 pa, pb, normal, best_normal;
+    uint32_t state, index, count, iter;
+    float tiny, margin, dist;
+    f3 pa, pb, normal;
     SPt* s;  // the simplex (4 points), in this lane's slice of shared memory
     SRes cl;
     WShape a, b;
@@ -792,35 +792,19 @@ constexpr uint32_t kGjkThreads = 128;
 constexpr uint32_t kSimplexStride = 37;
 static_assert(sizeof(SPt) * 4 <= kSimplexStride * sizeof(float), "a lane's simplex fits its slice");
 
-__device__ __forceinline__ f3 probe_direction(const GjkLane& L, uint32_t k) {
-    const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-    if (k < kProbeCentre) {
-        const f3 wi = L.s[kProbeTriple[k][0]].w, wj = L.s[kProbeTriple[k][1]].w, wk = L.s[kProbeTriple[k][2]].w;
-        return normalize(cross(wj - wi, wk - wi));
-    }
-    if (k == kProbeCentre) return normalize(L.b.center - L.a.center);
-    const uint32_t x = k - kProbeAxes;
-    return normalize(mk3(ax[x][0], ax[x][1], ax[x][2]));
-}
-// The first probe position at or after k that the probe would test.
-__device__ __forceinline__ uint32_t probe_next(const GjkLane& L, uint32_t k) {
-    for (; k < kProbeCentre; ++k)
-        if (L.triples & (1u << k)) return k;
-    if (k == kProbeCentre && length(L.b.center - L.a.center) <= 1e-8f) ++k;
-    return k;
-}
-// penetration_probe's direction list over the final simplex: triples whose normal is not degenerate.
-__device__ __forceinline__ void probe_begin(GjkLane& L) {
-    L.triples = 0u;
-    const uint32_t ntri = L.count == 3u ? 1u : (L.count == 4u ? 4u : 0u);
-    for (uint32_t t = 0; t < ntri; ++t) {
-        const f3 wi = L.s[kProbeTriple[t][0]].w, wj = L.s[kProbeTriple[t][1]].w, wk = L.s[kProbeTriple[t][2]].w;
-        if (length(cross(wj - wi, wk - wi)) > 1e-8f) L.triples |= 1u << t;
-    }
-    L.best = 3.402823466e38f;
-    L.best_normal = mk3(0.0f, 1.0f, 0.0f);
-    L.probe = probe_next(L, 0u);
-    L.state = GS_PROBE;
+// A pair that GJK leaves separated, or that runs out of iterations, goes to the penetration probe's
+// queue with its simplex, its closest points and its normal (k_convex_probe).
+__device__ __forceinline__ void gjk_to_probe(const DeviceWorld& w, GjkLane& L) {
+    const uint32_t slot = append_slot(&w.ctl[CTL_PROBES]);
+    w.probe_list[slot] = L.index;
+    float4* q = w.probe_data + 6 * (size_t)slot;
+    q[0] = mk4(L.s[0].w, __uint_as_float(L.count));
+    q[1] = mk4(L.count > 1u ? L.s[1].w : s3(0.0f), L.dist);
+    q[2] = mk4(L.count > 2u ? L.s[2].w : s3(0.0f), L.pa.x);
+    q[3] = mk4(L.count > 3u ? L.s[3].w : s3(0.0f), L.pa.y);
+    q[4] = mk4(L.pb, L.pa.z);
+    q[5] = mk4(L.normal, 0.0f);
+    L.state = GS_IDLE;
 }
 // A penetrating pair with its tetrahedron complete goes to the EPA queue.
 __device__ __forceinline__ void gjk_to_epa(const DeviceWorld& w, GjkLane& L) {
@@ -832,7 +816,7 @@ __device__ __forceinline__ void gjk_to_epa(const DeviceWorld& w, GjkLane& L) {
 // The loop head of gjk_phase: terminate, grow a penetrating simplex, or take another iteration.
 __device__ __forceinline__ void gjk_head(const DeviceWorld& w, GjkLane& L) {
     if (L.iter >= 24u) {
-        probe_begin(L);
+        gjk_to_probe(w, L);
     } else if (L.cl.pen || length(L.cl.v) < L.tiny) {
         if (L.count < 4u) {
             L.state = GS_EXPAND;
@@ -843,12 +827,12 @@ __device__ __forceinline__ void gjk_head(const DeviceWorld& w, GjkLane& L) {
         L.state = GS_ITER;
     }
 }
-__device__ __forceinline__ void gjk_separated(GjkLane& L) {
+__device__ __forceinline__ void gjk_separated(const DeviceWorld& w, GjkLane& L) {
     L.dist = length(L.cl.v);
     L.pa = L.cl.pa;
     L.pb = L.cl.pb;
     if (L.dist > 1e-6f) L.normal = sign_normalize(L.cl.pb - L.cl.pa);
-    probe_begin(L);
+    gjk_to_probe(w, L);
 }
 
 // The centre-axis rejection of gjk_phase for every convex pair, ahead of the state machine: one
@@ -901,10 +885,8 @@ __global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dy
             if (length(d) < 1e-8f) d = mk3(1.0f, 0.0f, 0.0f);
         } else if (L.state == GS_ITER) {
             d = -L.cl.v;
-        } else if (L.state == GS_EXPAND) {
-            d = simplex_expand_dir(L.s, L.count);
         } else {
-            d = probe_direction(L, L.probe);
+            d = simplex_expand_dir(L.s, L.count);
         }
         const SPt sp = support_pair(w, L.a, L.b, d);
         if (L.state == GS_FIRST) {
@@ -922,7 +904,7 @@ __global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dy
         } else if (L.state == GS_ITER) {
             const f3 v = L.cl.v;
             if (dot(sp.w, -v) <= dot(v, -v) + 1e-4f * wmax(1.0f, dot(v, v))) {
-                gjk_separated(L);
+                gjk_separated(w, L);
                 continue;
             }
             // simplex_reduce: keep the points with weight, in order (a stable in-place compaction)
@@ -943,7 +925,7 @@ __global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dy
                 if (dot(off, off) <= tol) holds = true;
             }
             if (holds) {
-                gjk_separated(L);
+                gjk_separated(w, L);
                 continue;
             }
             L.s[L.count] = sp;
@@ -951,31 +933,72 @@ __global__ void __launch_bounds__(kGjkThreads, 6) k_convex_gjk(DeviceWorld w, dy
             L.cl = simplex_closest(L.s, L.count);
             L.iter += 1u;
             gjk_head(w, L);
-        } else if (L.state == GS_EXPAND) {
+        } else {
             L.s[L.count] = sp;
             L.count += 1u;
             if (L.count == 4u) gjk_to_epa(w, L);
-        } else {
-            const float depth = dot(sp.w, d);
-            if (depth < L.best) {
-                L.best = depth;
-                L.best_normal = d;
-            }
-            L.probe = depth <= 0.0f ? kProbeEnd : probe_next(L, L.probe + 1u);
-            if (L.probe >= kProbeEnd) {
-                // separated_hit, then the margin test of the caller
-                Hit hit{3.402823466e38f, s3(0.0f), s3(0.0f)};
-                if (L.best > 0.0f) {
-                    f3 normal = L.best_normal;
-                    if (dot(normal, L.b.center - L.a.center) < 0.0f) normal = -normal;
-                    hit = Hit{-L.best, (L.pa + L.pb) * 0.5f, normal};
-                } else if (L.dist > 0.0f) {
-                    hit = Hit{L.dist, (L.pa + L.pb) * 0.5f, L.normal};
-                }
-                if (hit.distance <= L.margin) push_hit(w, L.index, hit);
-                L.state = GS_IDLE;
-            }
         }
+    }
+}
+
+// convex.wgsl:532-582 (penetration_probe) then separated_hit (:588-600) for the pairs GJK left
+// separated: the simplex triples, the centre axis and the six axes in order, stopping at the first
+// direction with no overlap (the minimum is then not positive, which is all separated_hit asks);
+// when every direction overlaps, the first minimum gives the penetration. One thread per pair.
+__global__ void __launch_bounds__(128) k_convex_probe(DeviceWorld w, dyn_step_params p) {
+    const uint32_t count = min(w.ctl[CTL_PROBES], w.p_cap);
+    GRID_STRIDE(i, count) {
+        const uint32_t index = w.probe_list[i];
+        const float4* q = w.probe_data + 6 * (size_t)i;
+        const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5];
+        const f3 sw[4] = {xyz(q0), xyz(q1), xyz(q2), xyz(q3)};
+        const uint32_t n = __float_as_uint(q0.w);
+        const float dist = q1.w;
+        const f3 pa = mk3(q2.w, q3.w, q4.w), pb = xyz(q4), normal = xyz(q5);
+        WShape a, b;
+        DBody fb, sb;
+        convex_shapes(w, index, &a, &b, &fb, &sb);
+        const float margin = pair_margin(p, fb, sb);
+        uint32_t triples = 0u;
+        const uint32_t ntri = n == 3u ? 1u : (n == 4u ? 4u : 0u);
+        for (uint32_t t = 0; t < ntri; ++t) {
+            const f3 wi = sw[kProbeTriple[t][0]], wj = sw[kProbeTriple[t][1]], wk = sw[kProbeTriple[t][2]];
+            if (length(cross(wj - wi, wk - wi)) > 1e-8f) triples |= 1u << t;
+        }
+        const bool centre = !(length(b.center - a.center) <= 1e-8f);
+        const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        float best = 3.402823466e38f;
+        f3 best_normal = mk3(0.0f, 1.0f, 0.0f);
+        for (uint32_t k = 0; k < kProbeEnd; ++k) {
+            f3 d;
+            if (k < kProbeCentre) {
+                if (!(triples & (1u << k))) continue;
+                const f3 wi = sw[kProbeTriple[k][0]], wj = sw[kProbeTriple[k][1]], wk = sw[kProbeTriple[k][2]];
+                d = normalize(cross(wj - wi, wk - wi));
+            } else if (k == kProbeCentre) {
+                if (!centre) continue;
+                d = normalize(b.center - a.center);
+            } else {
+                const uint32_t x = k - kProbeAxes;
+                d = normalize(mk3(ax[x][0], ax[x][1], ax[x][2]));
+            }
+            const SPt sp = support_pair(w, a, b, d);
+            const float depth = dot(sp.w, d);
+            if (depth < best) {
+                best = depth;
+                best_normal = d;
+            }
+            if (depth <= 0.0f) break;
+        }
+        Hit hit{3.402823466e38f, s3(0.0f), s3(0.0f)};
+        if (best > 0.0f) {
+            f3 nrm = best_normal;
+            if (dot(nrm, b.center - a.center) < 0.0f) nrm = -nrm;
+            hit = Hit{-best, (pa + pb) * 0.5f, nrm};
+        } else if (dist > 0.0f) {
+            hit = Hit{dist, (pa + pb) * 0.5f, normal};
+        }
+        if (hit.distance <= margin) push_hit(w, index, hit);
     }
 }
 

@@ -222,6 +222,8 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.np_list, (PC_COUNT + 1) * (size_t)P);
         A(dw.epa_list, P);
         A(dw.epa_simplex, 4 * (size_t)P);
+        A(dw.probe_list, P);
+        A(dw.probe_data, 6 * (size_t)P);
         A(dw.hit_list, P);
         A(dw.hit_data, 2 * (size_t)P);
         A(dw.matched, C);
@@ -584,6 +586,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_convex_reject<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
     k_convex_gjk<<<148u * 6u, 128, 0, s>>>(dw, p);
+    k_convex_probe<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     mark(ST_COMPACT);
