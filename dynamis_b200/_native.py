@@ -56,6 +56,12 @@ SIGNATURES = {
     "dyn_radix_sort_static": (I32, [P, P, P, U32, U32, U32, P]),
     "dyn_set_body_worlds": (I32, [P, P, U32]),
     "dyn_edit_bodies": (I32, [P, P, P, U32]),
+    "dyn_remove_bodies": (I32, [P, P, U32]),
+    "dyn_observe_bodies": (I32, [P, P, U32]),
+    "dyn_stop_observing": (I32, [P]),
+    "dyn_poll": (I32, [P]),
+    "dyn_try_state": (I32, [P, U32, P, P]),
+    "dyn_try_counters": (I32, [P, P, U32, P]),
     "dyn_export_body_worlds": (I32, [P, P]),
     "dyn_add_ball_joint": (I32, [P, U32, U32, P, P, PU32]),
     "dyn_add_constraints": (I32, [P, P, U32, PU32]),

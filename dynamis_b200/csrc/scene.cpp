@@ -337,21 +337,23 @@ bool inertia_inverse(const float in[6], float out[6]) {
 
 void rebuild_rows(dyn_world* w) {
     if (w->raw_rows || !w->rows_dirty) return;
-    uint32_t n = (uint32_t)w->spawn_states.size();
+    const uint32_t ids = (uint32_t)w->spawn_states.size();
+    w->removed.resize(ids, 0u);
     std::vector<uint32_t> order;
-    order.reserve(n);
-    for (uint32_t i = 0; i < n; ++i) {
+    order.reserve(ids);
+    for (uint32_t i = 0; i < ids; ++i) {
         const dyn_body_descriptor_record& d = w->spawn_descs[i];
-        if ((d.flags & DYN_BODY_KINEMATIC) == 0u && d.inverse_mass > 0.0f) order.push_back(i);
+        if (!w->removed[i] && (d.flags & DYN_BODY_KINEMATIC) == 0u && d.inverse_mass > 0.0f) order.push_back(i);
     }
     w->dynamic_count = (uint32_t)order.size();
-    for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t i = 0; i < ids; ++i) {
         const dyn_body_descriptor_record& d = w->spawn_descs[i];
-        if (!((d.flags & DYN_BODY_KINEMATIC) == 0u && d.inverse_mass > 0.0f)) order.push_back(i);
+        if (!w->removed[i] && !((d.flags & DYN_BODY_KINEMATIC) == 0u && d.inverse_mass > 0.0f)) order.push_back(i);
     }
+    const uint32_t n = (uint32_t)order.size();
     w->states.resize(n);
     w->descs.resize(n);
-    w->row_of_id.assign(n, DYN_NO_BODY);
+    w->row_of_id.assign(ids, DYN_NO_BODY);
     for (uint32_t r = 0; r < n; ++r) {
         w->states[r] = w->spawn_states[order[r]];
         w->descs[r] = w->spawn_descs[order[r]];
@@ -361,10 +363,15 @@ void rebuild_rows(dyn_world* w) {
     for (uint32_t r = 0; r < n; ++r) {
         if (order[r] < w->world_of_id.size()) w->body_world[r] = w->world_of_id[order[r]];
     }
-    w->colliders = w->spawn_colliders;
-    w->owners.resize(w->spawn_owner.size());
-    for (size_t i = 0; i < w->spawn_owner.size(); ++i) w->owners[i] = w->row_of_id[w->spawn_owner[i]];
+    w->colliders.clear();
+    w->owners.clear();
+    for (size_t i = 0; i < w->spawn_owner.size(); ++i) {
+        if (w->removed[w->spawn_owner[i]]) continue;
+        w->colliders.push_back(w->spawn_colliders[i]);
+        w->owners.push_back(w->row_of_id[w->spawn_owner[i]]);
+    }
     w->rows_dirty = false;
+    w->scene_dirty = true;  // whoever rebuilt the rows (an export, a read), the device needs them
 }
 
 std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vector<float>* verts) {
@@ -602,6 +609,7 @@ DYN_API const char* dyn_status_string(dyn_status s) {
         case DYN_ERR_NO_DEVICE: return "no CUDA device";
         case DYN_ERR_DEVICE_STATUS: return "device gave up a bounded wait";
         case DYN_ERR_DEGENERATE: return "degenerate hull";
+        case DYN_NOT_READY: return "no observation completed yet";
         default: return "unknown status";
     }
 }
@@ -1005,11 +1013,35 @@ DYN_API dyn_status dyn_edit_bodies(dyn_world* w, const uint32_t* body_ids, const
     if (!w || (n && (!body_ids || !edits))) return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: null argument");
     uint32_t ids = (uint32_t)std::max(w->spawn_states.size(), w->row_of_id.size());
     for (uint32_t i = 0; i < n; ++i) {
-        if (body_ids[i] >= ids) return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: unknown body id");
+        if (body_ids[i] >= ids || (body_ids[i] < w->removed.size() && w->removed[body_ids[i]]))
+            return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: unknown body id");
         if (edits[i].kind > DYN_EDIT_ANGULAR_IMPULSE) return fail(w, DYN_ERR_INVALID, "dyn_edit_bodies: unknown edit kind");
     }
     w->edit_ids.insert(w->edit_ids.end(), body_ids, body_ids + n);
     w->edits.insert(w->edits.end(), edits, edits + n);
+    return DYN_OK;
+}
+
+// ---- removal ----
+DYN_API dyn_status dyn_remove_bodies(dyn_world* w, const uint32_t* body_ids, uint32_t n) {
+    if (!w || (n && !body_ids)) return fail(w, DYN_ERR_INVALID, "dyn_remove_bodies: null argument");
+    if (w->raw_rows) return fail(w, DYN_ERR_INVALID, "dyn_remove_bodies: scene was replaced by dyn_upload_bodies");
+    const uint32_t ids = (uint32_t)w->spawn_states.size();
+    w->removed.resize(ids, 0u);
+    std::vector<uint8_t> gone(ids, 0u);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t id = body_ids[i];
+        if (id >= ids || w->removed[id] || gone[id]) return fail(w, DYN_ERR_INVALID, "dyn_remove_bodies: unknown or repeated body id");
+        gone[id] = 1u;
+    }
+    // World::remove asserts the body is unreferenced (body.rs:132-134): a constraint still names it
+    for (const dyn_constraint_descriptor_record& c : w->joint_descs) {
+        if ((c.first_body_id < ids && gone[c.first_body_id]) || (c.second_body_id < ids && gone[c.second_body_id]))
+            return fail(w, DYN_ERR_INVALID, "dyn_remove_bodies: a constraint still references the body");
+    }
+    if (dyn_status st = sync_spawn_states(w)) return st;  // the other bodies keep their simulated states
+    for (uint32_t i = 0; i < n; ++i) w->removed[body_ids[i]] = 1u;
+    w->rows_dirty = true;
     return DYN_OK;
 }
 

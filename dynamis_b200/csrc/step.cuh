@@ -1831,25 +1831,34 @@ __global__ void k_unpack_states(DeviceWorld w, const dyn_body_state_record* __re
         w.sleep_timer[i] = r.sleep_timer;
     }
 }
+__device__ __forceinline__ void pack_state(const DeviceWorld& w, uint32_t i, dyn_body_state_record* __restrict__ dst) {
+    const BodyHot& h = w.hot[i];
+    float4 pp = w.prev_pos[i], pr = w.prev_rot[i], f = w.force[i], t = w.torque[i];
+    uint4 id = w.ident[i];
+    dyn_body_state_record r;
+    r.position[0] = h.pos.x; r.position[1] = h.pos.y; r.position[2] = h.pos.z; r._pad0 = 0.0f;
+    r.prev_position[0] = pp.x; r.prev_position[1] = pp.y; r.prev_position[2] = pp.z; r._pad1 = 0.0f;
+    r.prev_orientation[0] = pr.x; r.prev_orientation[1] = pr.y; r.prev_orientation[2] = pr.z; r.prev_orientation[3] = pr.w;
+    r.orientation[0] = h.rot.x; r.orientation[1] = h.rot.y; r.orientation[2] = h.rot.z; r.orientation[3] = h.rot.w;
+    r.velocity[0] = h.vel.x; r.velocity[1] = h.vel.y; r.velocity[2] = h.vel.z; r._pad2 = 0.0f;
+    r.angular_velocity[0] = h.ang.x; r.angular_velocity[1] = h.ang.y; r.angular_velocity[2] = h.ang.z; r._pad3 = 0.0f;
+    r.force[0] = f.x; r.force[1] = f.y; r.force[2] = f.z; r._pad4 = 0.0f;
+    r.torque[0] = t.x; r.torque[1] = t.y; r.torque[2] = t.z; r._pad5 = 0.0f;
+    r.body_id = id.x;
+    r.generation = id.y;
+    r.sleep_timer = w.sleep_timer[i];
+    r.sleeping = h.aux.x;
+    *dst = r;
+}
 __global__ void k_pack_states(DeviceWorld w, dyn_body_state_record* __restrict__ out, uint32_t n) {
-    GRID_STRIDE(i, n) {
-        const BodyHot& h = w.hot[i];
-        float4 pp = w.prev_pos[i], pr = w.prev_rot[i], f = w.force[i], t = w.torque[i];
-        uint4 id = w.ident[i];
-        dyn_body_state_record r;
-        r.position[0] = h.pos.x; r.position[1] = h.pos.y; r.position[2] = h.pos.z; r._pad0 = 0.0f;
-        r.prev_position[0] = pp.x; r.prev_position[1] = pp.y; r.prev_position[2] = pp.z; r._pad1 = 0.0f;
-        r.prev_orientation[0] = pr.x; r.prev_orientation[1] = pr.y; r.prev_orientation[2] = pr.z; r.prev_orientation[3] = pr.w;
-        r.orientation[0] = h.rot.x; r.orientation[1] = h.rot.y; r.orientation[2] = h.rot.z; r.orientation[3] = h.rot.w;
-        r.velocity[0] = h.vel.x; r.velocity[1] = h.vel.y; r.velocity[2] = h.vel.z; r._pad2 = 0.0f;
-        r.angular_velocity[0] = h.ang.x; r.angular_velocity[1] = h.ang.y; r.angular_velocity[2] = h.ang.z; r._pad3 = 0.0f;
-        r.force[0] = f.x; r.force[1] = f.y; r.force[2] = f.z; r._pad4 = 0.0f;
-        r.torque[0] = t.x; r.torque[1] = t.y; r.torque[2] = t.z; r._pad5 = 0.0f;
-        r.body_id = id.x;
-        r.generation = id.y;
-        r.sleep_timer = w.sleep_timer[i];
-        r.sleeping = h.aux.x;
-        out[i] = r;
+    GRID_STRIDE(i, n) pack_state(w, i, out + i);
+}
+// The state records of the listed rows, in list order (the observation ring's copies).
+__global__ void k_pack_rows(DeviceWorld w, const uint32_t* __restrict__ rows, dyn_body_state_record* __restrict__ out,
+                            uint32_t m) {
+    GRID_STRIDE(i, m) {
+        const uint32_t row = rows[i];
+        if (row < w.n) pack_state(w, row, out + i);
     }
 }
 

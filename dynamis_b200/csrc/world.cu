@@ -48,6 +48,7 @@ struct DeviceState {
     DeviceWorld dw{};
     std::vector<void*> allocs;
     uint32_t n_cap = 0, k_cap = 0, e_cap = 0, p_cap = 0, c_cap = 0;
+    uint32_t id_cap = 0;  // body ids the row_of_id table holds (ids of removed bodies are not reused)
     uint32_t src_cap = 0, vert_cap = 0;
     dyn_shape_source_record* sources = nullptr;
     float4* vertices = nullptr;
@@ -146,8 +147,9 @@ dyn_status ensure_device(dyn_world* w) {
     std::vector<float> verts;
     std::vector<dyn_shape_source_record> srcs = shape_sources(w, &verts);
     uint32_t ns = (uint32_t)srcs.size(), nv = (uint32_t)(verts.size() / 4);
+    const uint32_t ids = (uint32_t)w->row_of_id.size();
     DeviceState* d = w->dev;
-    bool fits = d && n <= d->n_cap && k <= d->k_cap && ns <= d->src_cap && nv <= d->vert_cap;
+    bool fits = d && n <= d->n_cap && k <= d->k_cap && ns <= d->src_cap && nv <= d->vert_cap && ids <= d->id_cap;
     if (!fits) {
         if (d) destroy_device(w);
         int count = 0;
@@ -185,7 +187,8 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.activity, N);
         A(dw.motion, N);
         A(dw.wake_flags, N);
-        A(dw.row_of_id, N);
+        d->id_cap = std::max(N, ids + ids / 2);  // room for spawns after removals
+        A(dw.row_of_id, d->id_cap);
         A(dw.body_world, N);
         A(dw.edit_count, 1);
         A(dw.c_owner, K);
@@ -723,14 +726,10 @@ dyn_status prepare_step(dyn_world* w, float dt) {
         dyn_status st = save_joint_runtime(w);
         if (st) return st;
     }
-    if (fresh && w->dev && w->dev->stepped) {
-        // bodies spawned after stepping: keep the simulated states of the existing bodies
-        std::vector<dyn_body_state_record> now;
-        dyn_status st = download_states(w, &now);
+    if (fresh) {
+        // bodies spawned or removed after stepping: keep the simulated states of the others
+        dyn_status st = sync_spawn_states(w);
         if (st) return st;
-        for (const dyn_body_state_record& s : now) {
-            if (s.body_id < w->spawn_states.size()) w->spawn_states[s.body_id] = s;
-        }
     }
     if (fresh) {
         dyn_status st = upload_scene(w);
@@ -753,6 +752,122 @@ dyn_status prepare_step(dyn_world* w, float dt) {
 }
 
 }  // namespace
+
+// ---- observation ring ----
+void release_observer(dyn_world* w) {
+    Observer& o = w->observer;
+    for (ObservationSlot& s : o.slots) {
+        if (s.done) cudaEventSynchronize(static_cast<cudaEvent_t>(s.done));
+        if (s.states) cudaFreeHost(s.states);
+        if (s.counters) cudaFreeHost(s.counters);
+        if (s.done) cudaEventDestroy(static_cast<cudaEvent_t>(s.done));
+        s = ObservationSlot();
+    }
+    if (o.rows) cudaFree(o.rows);
+    o.rows = nullptr;
+    o.rows_capacity = 0;
+    o.latest = -1;
+}
+// World::poll: every slot whose copies have completed becomes readable; the newest is the latest.
+void observer_poll(dyn_world* w) {
+    Observer& o = w->observer;
+    for (uint32_t i = 0; i < kObservationSlots; ++i) {
+        ObservationSlot& s = o.slots[i];
+        if (!s.pending) continue;
+        cudaError_t e = cudaEventQuery(static_cast<cudaEvent_t>(s.done));
+        if (e == cudaErrorNotReady) continue;
+        cudaGetLastError();
+        s.pending = false;
+        s.ready = e == cudaSuccess;
+        if (s.ready && (o.latest < 0 || s.step > o.slots[o.latest].step)) o.latest = (int)i;
+    }
+}
+// After a step: copy the observed records and the counters into a slot other than the latest
+// (which a reader may be copying from): a completed one if there is one, else the oldest still in
+// flight, whose copy this newer one supersedes (the copies are ordered on the stream, so the new one
+// lands after it; the host never reads a slot in flight).
+dyn_status observe_after_step(dyn_world* w) {
+    Observer& o = w->observer;
+    DeviceState* d = w->dev;
+    observer_poll(w);
+    int pick = -1;
+    for (uint32_t k = 0; k < kObservationSlots; ++k) {
+        if (!o.slots[k].pending && (int)k != o.latest) {
+            pick = (int)k;
+            break;
+        }
+    }
+    if (pick < 0) {
+        for (uint32_t k = 0; k < kObservationSlots; ++k) {
+            if ((int)k == o.latest) continue;
+            if (pick < 0 || o.slots[k].step < o.slots[pick].step) pick = (int)k;
+        }
+        o.superseded += 1;
+    }
+    ObservationSlot& s = o.slots[pick];
+    s.ids.clear();
+    s.index_of_id.clear();
+    if (o.all) {
+        s.ids.reserve(w->states.size());
+        for (const dyn_body_state_record& r : w->states) s.ids.push_back(r.body_id);
+    } else {
+        for (uint32_t id : o.ids) {
+            if (id < w->row_of_id.size() && w->row_of_id[id] != DYN_NO_BODY) s.ids.push_back(id);
+        }
+    }
+    const uint32_t m = (uint32_t)s.ids.size();
+    if (m > s.capacity) {
+        if (s.states) cudaFreeHost(s.states);
+        s.states = nullptr;
+        s.capacity = 0;
+        DYN_CUDA(cudaHostAlloc(&s.states, (size_t)std::max(m, 1u) * sizeof(dyn_body_state_record), cudaHostAllocDefault));
+        s.capacity = std::max(m, 1u);
+    }
+    if (!s.counters) DYN_CUDA(cudaHostAlloc(&s.counters, 64 * sizeof(uint32_t), cudaHostAllocDefault));
+    if (!s.done) {
+        cudaEvent_t e;
+        DYN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        s.done = e;
+    }
+    if (m > 0) {
+        if (o.all) {
+            k_pack_states<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, d->staging, m);
+        } else {
+            if (m > o.rows_capacity) {
+                if (o.rows) cudaFree(o.rows);
+                o.rows = nullptr;
+                o.rows_capacity = 0;
+                DYN_CUDA(cudaMalloc(&o.rows, (size_t)m * 4));
+                o.rows_capacity = m;
+            }
+            std::vector<uint32_t> rows(m);
+            for (uint32_t i = 0; i < m; ++i) rows[i] = w->row_of_id[s.ids[i]];
+            DYN_CUDA(cudaMemcpyAsync(o.rows, rows.data(), (size_t)m * 4, cudaMemcpyHostToDevice, d->stream));
+            DYN_CUDA(cudaStreamSynchronize(d->stream));  // the host row list goes out of scope
+            k_pack_rows<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, static_cast<uint32_t*>(o.rows), d->staging, m);
+        }
+        DYN_CUDA(cudaGetLastError());
+        DYN_CUDA(cudaMemcpyAsync(s.states, d->staging, (size_t)m * sizeof(dyn_body_state_record), cudaMemcpyDeviceToHost,
+                                 d->stream));
+    }
+    DYN_CUDA(cudaMemcpyAsync(s.counters, d->dw.counters, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
+    DYN_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(s.done), d->stream));
+    s.step = w->steps_taken;
+    s.pending = true;
+    s.ready = false;
+    return DYN_OK;
+}
+
+dyn_status sync_spawn_states(dyn_world* w) {
+    if (!w->dev || !w->dev->stepped || w->raw_rows) return DYN_OK;
+    std::vector<dyn_body_state_record> now;
+    dyn_status st = download_states(w, &now);
+    if (st) return st;
+    for (const dyn_body_state_record& s : now) {
+        if (s.body_id < w->spawn_states.size()) w->spawn_states[s.body_id] = s;
+    }
+    return DYN_OK;
+}
 
 void destroy_device(dyn_world* w) {
     DeviceState* d = w->dev;
@@ -804,6 +919,8 @@ DYN_API dyn_status dyn_world_create(const dyn_config* config, const dyn_capacity
 
 DYN_API dyn_status dyn_world_destroy(dyn_world* w) {
     if (!w) return DYN_ERR_INVALID;
+    if (w->dev) cudaSetDevice(w->device);
+    release_observer(w);
     destroy_device(w);
     delete w;
     return DYN_OK;
@@ -915,6 +1032,72 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
     d->last_parity = parity;
     d->parity ^= 1u;
     d->stepped = true;
+    w->steps_taken += 1;
+    if (w->observer.active) return observe_after_step(w);
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_observe_bodies(dyn_world* w, const uint32_t* body_ids, uint32_t n) {
+    if (!w || (n && !body_ids)) return fail(w, DYN_ERR_INVALID, "dyn_observe_bodies: null argument");
+    Observer& o = w->observer;
+    if (!body_ids) {
+        o.all = true;
+        o.ids.clear();
+    } else {
+        const uint32_t ids = (uint32_t)std::max(w->spawn_states.size(), w->row_of_id.size());
+        for (uint32_t i = 0; i < n; ++i) {
+            if (body_ids[i] >= ids) return fail(w, DYN_ERR_INVALID, "dyn_observe_bodies: unknown body id");
+        }
+        if (o.all) o.ids.clear();
+        o.all = false;
+        o.ids.insert(o.ids.end(), body_ids, body_ids + n);
+        std::sort(o.ids.begin(), o.ids.end());
+        o.ids.erase(std::unique(o.ids.begin(), o.ids.end()), o.ids.end());
+    }
+    o.active = true;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_stop_observing(dyn_world* w) {
+    if (!w) return DYN_ERR_INVALID;
+    w->observer.active = false;
+    w->observer.all = false;
+    w->observer.ids.clear();
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_poll(dyn_world* w) {
+    if (!w) return DYN_ERR_INVALID;
+    observer_poll(w);
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_try_state(dyn_world* w, uint32_t body_id, dyn_body_state_record* out, uint64_t* step) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    observer_poll(w);
+    Observer& o = w->observer;
+    if (o.latest < 0) return DYN_NOT_READY;
+    ObservationSlot& s = o.slots[o.latest];
+    if (s.index_of_id.empty() && !s.ids.empty()) {
+        uint32_t top = *std::max_element(s.ids.begin(), s.ids.end());
+        s.index_of_id.assign((size_t)top + 1, DYN_NO_BODY);
+        for (uint32_t i = 0; i < (uint32_t)s.ids.size(); ++i) s.index_of_id[s.ids[i]] = i;
+    }
+    if (body_id >= s.index_of_id.size() || s.index_of_id[body_id] == DYN_NO_BODY)
+        return fail(w, DYN_ERR_INVALID, "dyn_try_state: the body is not in the latest observation");
+    *out = static_cast<const dyn_body_state_record*>(s.states)[s.index_of_id[body_id]];
+    if (step) *step = s.step;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_try_counters(dyn_world* w, uint32_t* out, uint32_t n, uint64_t* step) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    observer_poll(w);
+    Observer& o = w->observer;
+    if (o.latest < 0) return DYN_NOT_READY;
+    const ObservationSlot& s = o.slots[o.latest];
+    std::memcpy(out, s.counters, (size_t)std::min<uint32_t>(n, DYN_COUNTER_DEVICE_COUNT) * 4);
+    if (step) *step = s.step;
     return DYN_OK;
 }
 

@@ -32,6 +32,30 @@ void plan_joints(const std::vector<uint32_t>& first, const std::vector<uint32_t>
 
 struct DeviceState;  // defined in world.cu
 
+// The observation ring (observation.rs, dynamis-gpu/src/readback.rs:158-173): after each step the
+// observed bodies' state records and the counters are copied on the world's stream into one of a
+// few pinned host slots; reads take the newest slot whose copy has completed and never wait.
+constexpr uint32_t kObservationSlots = 4;
+struct ObservationSlot {
+    void* states = nullptr;    // pinned dyn_body_state_record[capacity]
+    void* counters = nullptr;  // pinned uint32_t[64]
+    uint32_t capacity = 0;
+    void* done = nullptr;      // cudaEvent_t recorded after the copies
+    std::vector<uint32_t> ids; // body id of each copied record
+    std::vector<uint32_t> index_of_id;  // built on the first read
+    uint64_t step = 0;
+    bool pending = false, ready = false;
+};
+struct Observer {
+    bool active = false, all = false;
+    std::vector<uint32_t> ids;  // the observed bodies (when not all)
+    ObservationSlot slots[kObservationSlots];
+    int latest = -1;            // newest completed slot
+    void* rows = nullptr;       // device copy of the observed rows
+    uint32_t rows_capacity = 0;
+    uint64_t superseded = 0;    // copies replaced by a newer one before they completed
+};
+
 }  // namespace dyn
 
 struct dyn_world {
@@ -46,6 +70,7 @@ struct dyn_world {
     std::vector<dyn_body_descriptor_record> spawn_descs;
     std::vector<dyn_collider_record> spawn_colliders;
     std::vector<uint32_t> spawn_owner;  // body id of each collider
+    std::vector<uint8_t> removed;       // by body id: removed from the world (ids are not reused)
     // scene as rows (dynamic rows first), rebuilt when the scene changes
     bool rows_dirty = true;
     bool raw_rows = false;  // scene came from dyn_upload_bodies
@@ -70,6 +95,8 @@ struct dyn_world {
     std::vector<dyn_body_edit_record> edits;
     bool timing = false;
     void* user_stream = nullptr;  // caller's cudaStream_t (dyn_world_set_stream)
+    uint64_t steps_taken = 0;     // dyn_step calls since creation
+    dyn::Observer observer;
     dyn::DeviceState* dev = nullptr;
 };
 
@@ -77,6 +104,8 @@ namespace dyn {
 dyn_status fail(dyn_world* w, dyn_status status, const std::string& what);
 void rebuild_rows(dyn_world* w);
 dyn_status rebuild_joints(dyn_world* w);
+// Copies the device's current body states into the spawn-order store (a no-op before the first step).
+dyn_status sync_spawn_states(dyn_world* w);
 std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vector<float>* vertices_xyzw);
 void destroy_device(dyn_world* w);
 }  // namespace dyn

@@ -13,6 +13,8 @@ import numpy as np
 from . import records as R
 from ._native import DynamisError, check, lib, ptr
 
+NOT_READY = 7  # DYN_NOT_READY: no observation has completed yet
+
 
 def default_config() -> np.ndarray:
     c = np.zeros(1, R.CONFIG)
@@ -123,6 +125,46 @@ class World:
         """Puts every body (indexed by body id) in a sub-world; sub-worlds never interact."""
         arr = np.ascontiguousarray(world_of_body, np.uint32)
         self._check(lib.dyn_set_body_worlds(self._h, ptr(arr), len(arr)))
+
+    # ---- lagged observations ----
+    def observe_bodies(self, body_ids=None) -> None:
+        """World::observe_bodies (or observe_all_bodies when body_ids is None)."""
+        if body_ids is None:
+            self._check(lib.dyn_observe_bodies(self._h, None, 0))
+        else:
+            ids = np.ascontiguousarray(body_ids, np.uint32)
+            self._check(lib.dyn_observe_bodies(self._h, ptr(ids), len(ids)))
+
+    def stop_observing(self) -> None:
+        self._check(lib.dyn_stop_observing(self._h))
+
+    def poll(self) -> None:
+        self._check(lib.dyn_poll(self._h))
+
+    def try_state(self, body_id: int):
+        """World::try_state: (state record, step it was taken after) from the newest completed
+        observation, or None while none has completed. Never waits for the GPU."""
+        out = np.zeros(1, R.BODY_STATE)
+        step = ctypes.c_uint64()
+        status = lib.dyn_try_state(self._h, int(body_id), ptr(out), ctypes.byref(step))
+        if status == NOT_READY:
+            return None
+        self._check(status)
+        return out[0], step.value
+
+    def try_counters(self):
+        out = np.zeros(R.COUNTER_DEVICE_COUNT, np.uint32)
+        step = ctypes.c_uint64()
+        status = lib.dyn_try_counters(self._h, ptr(out), len(out), ctypes.byref(step))
+        if status == NOT_READY:
+            return None
+        self._check(status)
+        return out, step.value
+
+    def remove_bodies(self, body_ids) -> None:
+        """World::remove for each id: the bodies leave the world at the next step."""
+        ids = np.ascontiguousarray(body_ids, np.uint32)
+        self._check(lib.dyn_remove_bodies(self._h, ptr(ids), len(ids)))
 
     # ---- body commands ----
     def edit_bodies(self, body_ids, edits: np.ndarray) -> None:

@@ -35,6 +35,7 @@ typedef int32_t dyn_status;
 #define DYN_ERR_NO_DEVICE 4       /* no CUDA device, or the requested ordinal does not exist */
 #define DYN_ERR_DEVICE_STATUS 5   /* a kernel gave up a bounded wait; see dyn_device_status */
 #define DYN_ERR_DEGENERATE 6      /* a hull point set spans no volume */
+#define DYN_NOT_READY 7           /* no observation has completed yet (dyn_try_state, dyn_try_counters) */
 
 typedef struct dyn_world dyn_world;
 
@@ -205,6 +206,31 @@ DYN_API dyn_status dyn_radix_sort(dyn_world* world, uint32_t* major, uint32_t* m
  * the body with id body_ids[i]. Edits queue on the host and run at the start of the next dyn_step,
  * after the step clears forces and before anything reads the bodies (body_edits.wgsl), in the order
  * given for each body. */
+/* Lagged observations (World::observe_bodies / observe_all_bodies / stop_observing_all_bodies / poll /
+ * try_state, crates/dynamis-world/src/observation.rs:480-516; the counter ring of
+ * dynamis-gpu/src/readback.rs:158-173). While observing, every dyn_step also copies, on the world's
+ * stream, the observed bodies' state records and the counters into one of four pinned host slots.
+ * dyn_try_state and dyn_try_counters read the newest slot whose copy has completed, with the step
+ * number it was taken after, and never wait for the GPU: DYN_NOT_READY until a first copy
+ * completes. When every slot is still in flight, a step's copy replaces the oldest one (the newest
+ * observation wins); nothing waits.
+ * body_ids == NULL observes every body (bodies spawned later included); otherwise the ids are added
+ * to the observed set. */
+DYN_API dyn_status dyn_observe_bodies(dyn_world* world, const uint32_t* body_ids, uint32_t n);
+DYN_API dyn_status dyn_stop_observing(dyn_world* world);
+DYN_API dyn_status dyn_poll(dyn_world* world);
+DYN_API dyn_status dyn_try_state(dyn_world* world, uint32_t body_id, dyn_body_state_record* out, uint64_t* step);
+DYN_API dyn_status dyn_try_counters(dyn_world* world, uint32_t* out, uint32_t n, uint64_t* step);
+
+/* World::remove (crates/dynamis-world/src/body.rs:132-155) for n bodies at once. The bodies and
+ * their colliders leave the world at the next dyn_step; the other bodies keep their simulated
+ * states (the device's states are read back first), and body ids are not reused. Refused with
+ * DYN_ERR_INVALID when an id is unknown, repeated or already removed, or while a constraint still
+ * names the body (the reference asserts the body is unreferenced), and for worlds whose scene came
+ * from dyn_upload_bodies. A removal re-uploads the scene, so the next step starts without
+ * archived contacts (no warm start for that one step). */
+DYN_API dyn_status dyn_remove_bodies(dyn_world* world, const uint32_t* body_ids, uint32_t n);
+
 DYN_API dyn_status dyn_edit_bodies(dyn_world* world, const uint32_t* body_ids, const dyn_body_edit_record* edits, uint32_t n);
 
 /* ---- batched worlds ----

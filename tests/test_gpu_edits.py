@@ -113,3 +113,45 @@ def test_a_sleep_command_matches_the_oracle_counts():
     assert w.measured()[R.COUNTER["SLEPT"]] == o.counters()[R.COUNTER["SLEPT"]] >= 1
     o.close()
     w.close()
+
+
+def test_bodies_removed_after_stepping_match_the_oracle():
+    """A pile steps on the GPU, loses some bodies (several of them in contact), and steps on: the
+    rest keep their simulated states and match the oracle built from the world after the removal."""
+    w = World()
+    ids = scenes.random_mix(24, seed=14).build(w)
+    for _ in range(20):
+        w.step(DT)
+    w.wait()
+    gone = np.asarray(ids[2:8], np.uint32)
+    before = {int(s["body_id"]): s for s in w.read_states()}
+    w.remove_bodies(gone)
+    o = oracle_from_world(w, DT)
+    kept = o.states()
+    for s in kept:  # the oracle starts from the GPU's states of the remaining bodies
+        assert np.array_equal(s["position"], before[int(s["body_id"])]["position"])
+    for step in range(30):
+        w.step(DT)
+        o.step(DT)
+        w.wait()
+        compare_step(w, o, step)
+    assert not set(int(i) for i in w.read_states()["body_id"]) & set(int(i) for i in gone)
+    o.close()
+    w.close()
+
+
+def test_bodies_spawned_after_a_removal_match_the_oracle():
+    w = World()
+    ids = scenes.random_mix(16, seed=15).build(w)
+    for _ in range(10):
+        w.step(DT)
+    w.remove_bodies(ids[:3])
+    scenes.sphere_row(3, height=6.0, gravity=True).build(w)
+    o = oracle_from_world(w, DT)
+    for step in range(25):
+        w.step(DT)
+        o.step(DT)
+        w.wait()
+        compare_step(w, o, step)
+    o.close()
+    w.close()
