@@ -74,6 +74,7 @@ struct DeviceWorld {
     uint32_t nd;  // dynamic rows (rows [0, nd))
     uint32_t k;   // colliders
     uint32_t e_cap, p_cap, c_cap;
+    uint32_t n_cap;  // body rows the per-row buffers hold
     // bodies
     BodyHot* hot;
     float4* prev_pos;
@@ -148,6 +149,11 @@ struct DeviceWorld {
     int32_t* pdelta;  // [8n]
     uint32_t* contributions;
     float4* resolution;
+    // the position pass with its apply folded into the next iteration (worlds without joints)
+    int4* pd3;              // [3][n_cap] rotating linear position deltas (x, y, z, 0)
+    uint32_t* cnt3;         // [3][n_cap] rotating contribution counts
+    float4* resolution_alt; // [n_cap] the resolution of odd iterations
+    uint32_t* cowner;       // [c_cap] bit 0 / bit 1: the contact claimed its first / second row
     // constraints (ball joints) and their solve order
     uint32_t jcount;
     uint32_t jgroup_count;

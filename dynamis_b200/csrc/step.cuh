@@ -1319,7 +1319,10 @@ __global__ void k_solver_blocks(DeviceWorld w, dyn_step_params p) {
     const uint32_t cap = w.c_cap;
     GRID_STRIDE(i, count) {
         uint4 r = w.cur.rows[i];
-        if (!resolves(r)) continue;
+        if (!resolves(r)) {
+            w.cowner[i] = 0u;
+            continue;
+        }
         DBody fb = load_dbody(w.hot, r.x), sb = load_dbody(w.hot, r.y);
         f3 normal = xyz(w.cur.normal[i]);
         float restitution = w.cur.extra[i].x;
@@ -1338,8 +1341,16 @@ __global__ void k_solver_blocks(DeviceWorld w, dyn_step_params p) {
             float4 lb = w.cur.lb[o];
             w.cur.lb[o] = make_float4(lb.x, lb.y, lb.z, target);
         }
-        if (atomicAdd(&w.hot[r.x].aux.z, 1u) == 0u) w.row_flag[r.x] = 1u;
-        if (atomicAdd(&w.hot[r.y].aux.z, 1u) == 0u) w.row_flag[r.y] = 1u;
+        uint32_t own = 0u;
+        if (atomicAdd(&w.hot[r.x].aux.z, 1u) == 0u) {
+            w.row_flag[r.x] = 1u;
+            own |= 1u;
+        }
+        if (atomicAdd(&w.hot[r.y].aux.z, 1u) == 0u) {
+            w.row_flag[r.y] = 1u;
+            own |= 2u;
+        }
+        w.cowner[i] = own;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[DYN_COUNTER_BLOCKS] = count;
 }
@@ -1778,6 +1789,156 @@ __device__ __forceinline__ void apply_position_row(const DeviceWorld& w, uint32_
 __global__ void k_papply(DeviceWorld w) {
     const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
     GRID_STRIDE(i, rows) apply_position_row(w, i);
+}
+
+// ---- the position pass with its apply folded into the next iteration (worlds without joints) ----
+// Iteration k of a substep's position loop needs each row's resolution after iteration k-1's
+// correction: the row's summed delta over its contribution count, as position_apply.wgsl:12-27
+// forms it. Every contact forms it where it reads it, from iteration k-1's delta words; the row's
+// owner (the contact that claimed the row in k_solver_blocks) also stores it and moves the row's
+// pose. Three delta buffers rotate: k-1's are read, k's are summed into, k+1's are cleared by the
+// owners (nothing reads or writes them during iteration k). The integers and the float operations
+// are k_papply's, so poses and resolutions come out bit for bit as with the separate apply, one
+// launch per iteration fewer; k_papply_last applies the last iteration. Joint passes move bodies
+// between the contact iterations, so worlds with joints keep the separate apply.
+struct RowCorrection {
+    f3 al;
+    uint32_t contributing;
+};
+__device__ __forceinline__ RowCorrection row_correction(const int4* __restrict__ pd, const uint32_t* __restrict__ cnt, uint32_t row) {
+    RowCorrection c;
+    c.contributing = cnt[row];
+    c.al = s3(0.0f);
+    if (c.contributing != 0u) {
+        const int4 a = pd[row];
+        const f3 lin = mk3((float)a.x / DYN_SOLVER_POSITION_SCALE, (float)a.y / DYN_SOLVER_POSITION_SCALE,
+                           (float)a.z / DYN_SOLVER_POSITION_SCALE);
+        c.al = lin / (float)c.contributing;
+    }
+    return c;
+}
+__device__ __forceinline__ float4 corrected(float4 res, const RowCorrection& c) {
+    if (c.contributing == 0u) return res;
+    return make_float4(res.x + c.al.x, res.y + c.al.y, res.z + c.al.z, 0.0f);
+}
+// apply_position_row's pose update: a pure translation, and the orientation renormalised
+__device__ __forceinline__ void move_row(const DeviceWorld& w, uint32_t row, const RowCorrection& c) {
+    if (c.contributing == 0u) return;
+    const f3 aa = s3(0.0f) / (float)c.contributing;
+    BodyHot& h = w.hot[row];
+    const f3 pos = xyz(h.pos) + c.al;
+    h.pos = mk4(pos, h.pos.w);
+    const f3 ha = aa * 0.5f;
+    h.rot = normalize4(quat_mul(make_float4(ha.x, ha.y, ha.z, 1.0f), h.rot));
+}
+__device__ __forceinline__ void position_block_rows(const DeviceWorld& w, const dyn_step_params& p, uint32_t i, uint4 r,
+                                                    float4 res_a, float4 res_b, int4* __restrict__ pd,
+                                                    uint32_t* __restrict__ cnt) {
+    const uint32_t cap = w.c_cap;
+    if (!resolves(r)) return;
+    float4 mat = w.cur.mat[i];
+    if (mat.z > 0.0f) return;
+    const BodyHot& ha = w.hot[r.x];
+    const BodyHot& hb = w.hot[r.y];
+    float ima = (!simulates(ha.pos.w, ha.aux.y) || ha.aux.x != 0u) ? 0.0f : ha.pos.w;
+    float imb = (!simulates(hb.pos.w, hb.aux.y) || hb.aux.x != 0u) ? 0.0f : hb.pos.w;
+    f3 normal = xyz(w.cur.normal[i]);
+    float resolved = dot(normal, xyz(res_b) - xyz(res_a));
+    f3 total = s3(0.0f);
+    uint32_t contributing = 0;
+    uint32_t pc = r.z & 0xFFu;
+    for (uint32_t pi = 0; pi < pc; ++pi) {
+        float error = wmax(w.cur.la[(size_t)pi * cap + i].w - p.slop - resolved, 0.0f);
+        if (error <= 0.0f) continue;
+        float k = ima + imb;
+        if (k == 0.0f) continue;
+        total = total + normal * (p.relaxation * error / k);
+        contributing += 1;
+    }
+    if (contributing == 0u) return;
+    f3 correction = total / (float)contributing;
+    f3 la = -correction * ima;
+    f3 lb = correction * imb;
+    if (!(dot(la, la) > 0.0f || dot(lb, lb) > 0.0f)) return;
+    int32_t* da = reinterpret_cast<int32_t*>(pd + r.x);
+    int32_t* db = reinterpret_cast<int32_t*>(pd + r.y);
+    if (ima > 0.0f) {
+        atomicAdd(&cnt[r.x], 1u);
+        atomicAdd(da + 0, solver_word(la.x, DYN_SOLVER_POSITION_SCALE));
+        atomicAdd(da + 1, solver_word(la.y, DYN_SOLVER_POSITION_SCALE));
+        atomicAdd(da + 2, solver_word(la.z, DYN_SOLVER_POSITION_SCALE));
+    } else if (cnt[r.x] == 0u) {
+        cnt[r.x] = 1u;
+    }
+    if (imb > 0.0f) {
+        atomicAdd(&cnt[r.y], 1u);
+        atomicAdd(db + 0, solver_word(lb.x, DYN_SOLVER_POSITION_SCALE));
+        atomicAdd(db + 1, solver_word(lb.y, DYN_SOLVER_POSITION_SCALE));
+        atomicAdd(db + 2, solver_word(lb.z, DYN_SOLVER_POSITION_SCALE));
+    } else if (cnt[r.y] == 0u) {
+        cnt[r.y] = 1u;
+    }
+}
+template <bool kFirst>
+__global__ void k_position_fused(DeviceWorld w, dyn_step_params p, uint32_t k) {
+    const uint32_t count = w.ctl[CTL_CONTACTS];
+    const size_t n = w.n_cap;
+    const int4* pd_prev = w.pd3 + ((k + 2u) % 3u) * n;
+    int4* pd_cur = w.pd3 + (k % 3u) * n;
+    int4* pd_next = w.pd3 + ((k + 1u) % 3u) * n;
+    const uint32_t* cnt_prev = w.cnt3 + ((k + 2u) % 3u) * n;
+    uint32_t* cnt_cur = w.cnt3 + (k % 3u) * n;
+    uint32_t* cnt_next = w.cnt3 + ((k + 1u) % 3u) * n;
+    const float4* res_prev = ((k + 1u) & 1u) ? w.resolution_alt : w.resolution;
+    float4* res_cur = (k & 1u) ? w.resolution_alt : w.resolution;
+    GRID_STRIDE(i, count) {
+        const uint4 r = w.cur.rows[i];
+        float4 res_a, res_b;
+        if (kFirst) {
+            res_a = w.resolution[r.x];
+            res_b = w.resolution[r.y];
+        } else {
+            const RowCorrection ca = row_correction(pd_prev, cnt_prev, r.x);
+            const RowCorrection cb = row_correction(pd_prev, cnt_prev, r.y);
+            res_a = corrected(res_prev[r.x], ca);
+            res_b = corrected(res_prev[r.y], cb);
+            const uint32_t own = w.cowner[i];
+            if (own & 1u) {
+                res_cur[r.x] = res_a;
+                move_row(w, r.x, ca);
+                pd_next[r.x] = make_int4(0, 0, 0, 0);
+                cnt_next[r.x] = 0u;
+            }
+            if (own & 2u) {
+                res_cur[r.y] = res_b;
+                move_row(w, r.y, cb);
+                pd_next[r.y] = make_int4(0, 0, 0, 0);
+                cnt_next[r.y] = 0u;
+            }
+        }
+        position_block_rows(w, p, i, r, res_a, res_b, pd_cur, cnt_cur);
+    }
+}
+// The last iteration's correction of every solver row, into the resolution every later pass reads;
+// the three delta buffers are left cleared for the next substep.
+__global__ void k_papply_last(DeviceWorld w, uint32_t iterations) {
+    const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
+    const size_t n = w.n_cap;
+    const uint32_t last = iterations - 1u;
+    const int4* pd_last = w.pd3 + (last % 3u) * n;
+    const uint32_t* cnt_last = w.cnt3 + (last % 3u) * n;
+    const float4* res_last = (last & 1u) ? w.resolution_alt : w.resolution;
+    GRID_STRIDE(i, rows) {
+        const uint32_t row = w.solver_rows[i];
+        const RowCorrection c = row_correction(pd_last, cnt_last, row);
+        const float4 res = corrected(res_last[row], c);
+        w.resolution[row] = res;
+        move_row(w, row, c);
+        for (uint32_t b = 0; b < 3u; ++b) {
+            w.pd3[b * n + row] = make_int4(0, 0, 0, 0);
+            w.cnt3[b * n + row] = 0u;
+        }
+    }
 }
 
 // island_sleep.wgsl:10-29, then commit (contact_archive + archive_count_sync).

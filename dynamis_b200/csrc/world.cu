@@ -245,6 +245,10 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.pdelta, 8 * (size_t)N);
         A(dw.contributions, N);
         A(dw.resolution, N);
+        A(dw.pd3, 3 * (size_t)N);
+        A(dw.cnt3, 3 * (size_t)N);
+        A(dw.resolution_alt, N);
+        A(dw.cowner, C);
         A(dw.counters, 64);
         A(dw.ctl, CTL_COUNT);
         A(d->staging, N);
@@ -258,6 +262,7 @@ dyn_status ensure_device(dyn_world* w) {
         if ((st = alloc_contacts(w, d, &dw.cur, C))) return st;
         if ((st = alloc_contacts(w, d, &dw.arc, C))) return st;
         dw.e_cap = E;
+        dw.n_cap = N;
         dw.p_cap = P;
         dw.c_cap = C;
         dw.sources = d->sources;
@@ -633,10 +638,22 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         mark(ST_ADVANCE);
         k_advance<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
         mark(ST_POSITION);
-        for (uint32_t it = 0; it < p.position_iterations; ++it) {
-            if (joint_blocks) k_joints<JP_POSITION><<<joint_blocks, 32, 0, s>>>(dw, p);
-            k_position<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
-            k_papply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+        if (joint_blocks == 0u) {
+            // each iteration applies the one before it; one apply after the last
+            for (uint32_t it = 0; it < p.position_iterations; ++it) {
+                if (it == 0u) {
+                    k_position_fused<true><<<blocks_for(C, 256), 256, 0, s>>>(dw, p, it);
+                } else {
+                    k_position_fused<false><<<blocks_for(C, 256), 256, 0, s>>>(dw, p, it);
+                }
+            }
+            if (p.position_iterations > 0u) k_papply_last<<<blocks_for(N, 256), 256, 0, s>>>(dw, p.position_iterations);
+        } else {
+            for (uint32_t it = 0; it < p.position_iterations; ++it) {
+                k_joints<JP_POSITION><<<joint_blocks, 32, 0, s>>>(dw, p);
+                k_position<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+                k_papply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+            }
         }
     }
     mark(ST_SLEEP);
