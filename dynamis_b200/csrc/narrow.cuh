@@ -461,6 +461,10 @@ __device__ Mani box_box_sat(const DBody& fb, const DColl& fc, const DBody& sb, c
             face_on_right = true;
         }
     }
+    // No contact whatever the edge axes give: an edge axis wins only when its depth is below the face
+    // depth (edge_depth <= edge_depth + 1e-3 * extent < face_depth, rounding being monotone), and
+    // either depth at or below -margin answers no contact below. So the nine edge axes are skipped.
+    if (face_depth <= -margin) return m;
     float edge_depth = 1e30f;
     f3 edge_axis = face_axis;
     uint32_t efa = 0, esa = 0;
@@ -1669,12 +1673,18 @@ __device__ bool convex_pair_manifold(const DeviceWorld& w, const WShape& first, 
     return true;
 }
 // narrowphase.wgsl:485-512
+// Slack below -margin before a plane pair is answered from the convex's deepest point alone: far
+// above the rounding of the feature points at world coordinates of a few hundred metres.
+constexpr float kPlaneRejectTolerance = 1e-3f;
 __device__ Mani plane_convex(const DeviceWorld& w, const WShape& plane, const WShape& convex, float margin) {
     Mani m;
     f3 n = quat_rotate(plane.rotation, mk3(0.0f, 1.0f, 0.0f));
     float side = dot(convex.center - plane.center, n);
     f3 facing = side < 0.0f ? -n : n;
     mani_emit(&m, facing);
+    // Every feature point below is a point of the convex, so none is deeper than its support point
+    // along -facing: when that one is clear of the margin by more than rounding, no point is kept.
+    if (dot(plane.center - support(w, convex, -facing), facing) < -(margin + kPlaneRejectTolerance)) return m;
     f3 pts[8];
     uint32_t ids[8];
     uint32_t feature = 0;
