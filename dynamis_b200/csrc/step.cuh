@@ -2014,12 +2014,18 @@ __device__ __forceinline__ void pack_state(const DeviceWorld& w, uint32_t i, dyn
 __global__ void k_pack_states(DeviceWorld w, dyn_body_state_record* __restrict__ out, uint32_t n) {
     GRID_STRIDE(i, n) pack_state(w, i, out + i);
 }
-// The state records of the listed rows, in list order (the observation ring's copies).
-__global__ void k_pack_rows(DeviceWorld w, const uint32_t* __restrict__ rows, dyn_body_state_record* __restrict__ out,
-                            uint32_t m) {
+// The state records of the listed bodies, in list order (the observation ring's copies); a body
+// that is not in the world gets a record with body_id DYN_NO_BODY.
+__global__ void k_pack_ids(DeviceWorld w, const uint32_t* __restrict__ ids, dyn_body_state_record* __restrict__ out,
+                           uint32_t m) {
     GRID_STRIDE(i, m) {
-        const uint32_t row = rows[i];
-        if (row < w.n) pack_state(w, row, out + i);
+        const uint32_t id = ids[i];
+        const uint32_t row = id < w.id_count ? w.row_of_id[id] : DYN_NO_BODY;
+        if (row < w.n) {
+            pack_state(w, row, out + i);
+        } else {
+            out[i].body_id = DYN_NO_BODY;
+        }
     }
 }
 

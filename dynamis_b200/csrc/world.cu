@@ -780,9 +780,10 @@ void release_observer(dyn_world* w) {
         if (s.done) cudaEventDestroy(static_cast<cudaEvent_t>(s.done));
         s = ObservationSlot();
     }
-    if (o.rows) cudaFree(o.rows);
-    o.rows = nullptr;
-    o.rows_capacity = 0;
+    if (o.ids_dev) cudaFree(o.ids_dev);
+    o.ids_dev = nullptr;
+    o.ids_dev_capacity = 0;
+    o.ids_dirty = true;
     o.latest = -1;
 }
 // World::poll: every slot whose copies have completed becomes readable; the newest is the latest.
@@ -822,17 +823,20 @@ dyn_status observe_after_step(dyn_world* w) {
         o.superseded += 1;
     }
     ObservationSlot& s = o.slots[pick];
-    s.ids.clear();
     s.index_of_id.clear();
-    if (o.all) {
-        s.ids.reserve(w->states.size());
-        for (const dyn_body_state_record& r : w->states) s.ids.push_back(r.body_id);
-    } else {
-        for (uint32_t id : o.ids) {
-            if (id < w->row_of_id.size() && w->row_of_id[id] != DYN_NO_BODY) s.ids.push_back(id);
+    const uint32_t m = o.all ? (uint32_t)w->states.size() : (uint32_t)o.ids.size();
+    if (!o.all && o.ids_dirty) {
+        // the observed set changed (dyn_observe_bodies): one synchronous upload, then none per step
+        if (m > o.ids_dev_capacity) {
+            if (o.ids_dev) cudaFree(o.ids_dev);
+            o.ids_dev = nullptr;
+            o.ids_dev_capacity = 0;
+            DYN_CUDA(cudaMalloc(&o.ids_dev, (size_t)std::max(m, 1u) * 4));
+            o.ids_dev_capacity = std::max(m, 1u);
         }
+        if (m > 0) DYN_CUDA(cudaMemcpy(o.ids_dev, o.ids.data(), (size_t)m * 4, cudaMemcpyHostToDevice));
+        o.ids_dirty = false;
     }
-    const uint32_t m = (uint32_t)s.ids.size();
     if (m > s.capacity) {
         if (s.states) cudaFreeHost(s.states);
         s.states = nullptr;
@@ -850,18 +854,8 @@ dyn_status observe_after_step(dyn_world* w) {
         if (o.all) {
             k_pack_states<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, d->staging, m);
         } else {
-            if (m > o.rows_capacity) {
-                if (o.rows) cudaFree(o.rows);
-                o.rows = nullptr;
-                o.rows_capacity = 0;
-                DYN_CUDA(cudaMalloc(&o.rows, (size_t)m * 4));
-                o.rows_capacity = m;
-            }
-            std::vector<uint32_t> rows(m);
-            for (uint32_t i = 0; i < m; ++i) rows[i] = w->row_of_id[s.ids[i]];
-            DYN_CUDA(cudaMemcpyAsync(o.rows, rows.data(), (size_t)m * 4, cudaMemcpyHostToDevice, d->stream));
-            DYN_CUDA(cudaStreamSynchronize(d->stream));  // the host row list goes out of scope
-            k_pack_rows<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, static_cast<uint32_t*>(o.rows), d->staging, m);
+            k_pack_ids<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, static_cast<const uint32_t*>(o.ids_dev),
+                                                                 d->staging, m);
         }
         DYN_CUDA(cudaGetLastError());
         DYN_CUDA(cudaMemcpyAsync(s.states, d->staging, (size_t)m * sizeof(dyn_body_state_record), cudaMemcpyDeviceToHost,
@@ -869,6 +863,7 @@ dyn_status observe_after_step(dyn_world* w) {
     }
     DYN_CUDA(cudaMemcpyAsync(s.counters, d->dw.counters, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, d->stream));
     DYN_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(s.done), d->stream));
+    s.count = m;
     s.step = w->steps_taken;
     s.pending = true;
     s.ready = false;
@@ -1070,6 +1065,7 @@ DYN_API dyn_status dyn_observe_bodies(dyn_world* w, const uint32_t* body_ids, ui
         o.ids.insert(o.ids.end(), body_ids, body_ids + n);
         std::sort(o.ids.begin(), o.ids.end());
         o.ids.erase(std::unique(o.ids.begin(), o.ids.end()), o.ids.end());
+        o.ids_dirty = true;
     }
     o.active = true;
     return DYN_OK;
@@ -1095,14 +1091,20 @@ DYN_API dyn_status dyn_try_state(dyn_world* w, uint32_t body_id, dyn_body_state_
     Observer& o = w->observer;
     if (o.latest < 0) return DYN_NOT_READY;
     ObservationSlot& s = o.slots[o.latest];
-    if (s.index_of_id.empty() && !s.ids.empty()) {
-        uint32_t top = *std::max_element(s.ids.begin(), s.ids.end());
+    const dyn_body_state_record* records = static_cast<const dyn_body_state_record*>(s.states);
+    if (s.index_of_id.empty() && s.count > 0) {
+        uint32_t top = 0;
+        for (uint32_t i = 0; i < s.count; ++i) {
+            if (records[i].body_id != DYN_NO_BODY) top = std::max(top, records[i].body_id);
+        }
         s.index_of_id.assign((size_t)top + 1, DYN_NO_BODY);
-        for (uint32_t i = 0; i < (uint32_t)s.ids.size(); ++i) s.index_of_id[s.ids[i]] = i;
+        for (uint32_t i = 0; i < s.count; ++i) {
+            if (records[i].body_id != DYN_NO_BODY) s.index_of_id[records[i].body_id] = i;
+        }
     }
     if (body_id >= s.index_of_id.size() || s.index_of_id[body_id] == DYN_NO_BODY)
         return fail(w, DYN_ERR_INVALID, "dyn_try_state: the body is not in the latest observation");
-    *out = static_cast<const dyn_body_state_record*>(s.states)[s.index_of_id[body_id]];
+    *out = records[s.index_of_id[body_id]];
     if (step) *step = s.step;
     return DYN_OK;
 }

@@ -40,9 +40,9 @@ struct ObservationSlot {
     void* states = nullptr;    // pinned dyn_body_state_record[capacity]
     void* counters = nullptr;  // pinned uint32_t[64]
     uint32_t capacity = 0;
+    uint32_t count = 0;        // records copied
     void* done = nullptr;      // cudaEvent_t recorded after the copies
-    std::vector<uint32_t> ids; // body id of each copied record
-    std::vector<uint32_t> index_of_id;  // built on the first read
+    std::vector<uint32_t> index_of_id;  // body id -> record, built from the records on the first read
     uint64_t step = 0;
     bool pending = false, ready = false;
 };
@@ -51,8 +51,9 @@ struct Observer {
     std::vector<uint32_t> ids;  // the observed bodies (when not all)
     ObservationSlot slots[kObservationSlots];
     int latest = -1;            // newest completed slot
-    void* rows = nullptr;       // device copy of the observed rows
-    uint32_t rows_capacity = 0;
+    void* ids_dev = nullptr;    // device copy of ids, resolved to rows on the device at each copy
+    uint32_t ids_dev_capacity = 0;
+    bool ids_dirty = false;     // ids changed since the device copy was made
     uint64_t superseded = 0;    // copies replaced by a newer one before they completed
 };
 
