@@ -44,6 +44,10 @@ static const char* kStageNames[ST_COUNT] = {"begin",       "aabb",     "entries"
 
 struct DeviceState {
     cudaStream_t own_stream = nullptr;
+    // a second stream the captured step forks onto for kernels independent of the main line
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t fork_events[2] = {nullptr, nullptr};
+    cudaEvent_t join_events[2] = {nullptr, nullptr};
     cudaStream_t stream = nullptr;
     DeviceWorld dw{};
     std::vector<void*> allocs;
@@ -161,6 +165,11 @@ dyn_status ensure_device(dyn_world* w) {
         d = new DeviceState();
         w->dev = d;
         DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
+        DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream, cudaStreamNonBlocking));
+        for (uint32_t i = 0; i < 2; ++i) {
+            DYN_CUDA(cudaEventCreateWithFlags(&d->fork_events[i], cudaEventDisableTiming));
+            DYN_CUDA(cudaEventCreateWithFlags(&d->join_events[i], cudaEventDisableTiming));
+        }
         d->stream = w->user_stream ? static_cast<cudaStream_t>(w->user_stream) : d->own_stream;
         d->n_cap = std::max(n, w->capacity.bodies);
         d->k_cap = std::max(k, w->capacity.colliders);
@@ -584,19 +593,39 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_PAIRS);
     k_cell_clear<<<blocks_for(1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
     k_cell_insert<<<blocks_for(E, 256), 256, 0, s>>>(dw);
+    // Independent kernels run as parallel branches of the captured graph (a fork onto the side
+    // stream and a join back): the coarse links beside the same-cell scan, the analytic classes
+    // beside the convex chain. They only share append counters, and every product they feed is
+    // sorted or order-independent. The eager timed path keeps one stream, so stage times stay apart.
+    const bool branches = !timed;
+    cudaStream_t side = branches ? d->side_stream : s;
+    auto fork = [&](uint32_t k) {
+        if (!branches) return;
+        cudaEventRecord(d->fork_events[k], s);
+        cudaStreamWaitEvent(side, d->fork_events[k], 0);
+    };
+    auto join = [&](uint32_t k) {
+        if (!branches) return;
+        cudaEventRecord(d->join_events[k], side);
+        cudaStreamWaitEvent(s, d->join_events[k], 0);
+    };
+    fork(0);
     k_pairs_coarse<<<dim3(blocks_for(K, 128), kCoarseLevelSlices), 128, 0, s>>>(dw);
-    k_pairs_cell<<<blocks_for(E, 256), 256, 0, s>>>(dw);
+    k_pairs_cell<<<blocks_for(E, 256), 256, 0, side>>>(dw);
+    join(0);
     // the candidate pairs stay in emission order; the contacts are sorted into pair order below
     mark(ST_NARROWPHASE);
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
-    k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
-    k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    fork(1);
+    k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, side>>>(dw, p);
+    k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, side>>>(dw, p);
     k_convex_reject<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
     k_convex_gjk<<<148u * 6u, 128, 0, s>>>(dw, p);
     k_convex_probe<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    join(1);
     mark(ST_COMPACT);
     k_contact_keys<<<blocks_for(C, 256), 256, 0, s>>>(dw);
     const uint32_t words = key_words(std::max(dw.k, 1u));
@@ -896,6 +925,11 @@ void destroy_device(dyn_world* w) {
     for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
         if (p) cudaFree(p);
     }
+    for (uint32_t i = 0; i < 2; ++i) {
+        if (d->fork_events[i]) cudaEventDestroy(d->fork_events[i]);
+        if (d->join_events[i]) cudaEventDestroy(d->join_events[i]);
+    }
+    if (d->side_stream) cudaStreamDestroy(d->side_stream);
     if (d->own_stream) cudaStreamDestroy(d->own_stream);
     delete d;
     w->dev = nullptr;
