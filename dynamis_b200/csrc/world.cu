@@ -46,8 +46,9 @@ struct DeviceState {
     cudaStream_t own_stream = nullptr;
     // a second stream the captured step forks onto for kernels independent of the main line
     cudaStream_t side_stream = nullptr;
-    cudaEvent_t fork_events[2] = {nullptr, nullptr};
-    cudaEvent_t join_events[2] = {nullptr, nullptr};
+    cudaStream_t side_stream2 = nullptr;
+    cudaEvent_t fork_events[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t join_events[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t stream = nullptr;
     DeviceWorld dw{};
     std::vector<void*> allocs;
@@ -166,7 +167,8 @@ dyn_status ensure_device(dyn_world* w) {
         w->dev = d;
         DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream, cudaStreamNonBlocking));
-        for (uint32_t i = 0; i < 2; ++i) {
+        DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream2, cudaStreamNonBlocking));
+        for (uint32_t i = 0; i < 4; ++i) {
             DYN_CUDA(cudaEventCreateWithFlags(&d->fork_events[i], cudaEventDisableTiming));
             DYN_CUDA(cudaEventCreateWithFlags(&d->join_events[i], cudaEventDisableTiming));
         }
@@ -599,39 +601,51 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     // sorted or order-independent. The eager timed path keeps one stream, so stage times stay apart.
     const bool branches = !timed;
     cudaStream_t side = branches ? d->side_stream : s;
-    auto fork = [&](uint32_t k) {
+    cudaStream_t side2 = branches ? d->side_stream2 : s;
+    auto fork = [&](uint32_t k, cudaStream_t to) {
         if (!branches) return;
         cudaEventRecord(d->fork_events[k], s);
-        cudaStreamWaitEvent(side, d->fork_events[k], 0);
+        cudaStreamWaitEvent(to, d->fork_events[k], 0);
     };
-    auto join = [&](uint32_t k) {
+    auto join = [&](uint32_t k, cudaStream_t from) {
         if (!branches) return;
-        cudaEventRecord(d->join_events[k], side);
+        cudaEventRecord(d->join_events[k], from);
         cudaStreamWaitEvent(s, d->join_events[k], 0);
     };
-    fork(0);
+    fork(0, side);
     k_pairs_coarse<<<dim3(blocks_for(K, 128), kCoarseLevelSlices), 128, 0, s>>>(dw);
     k_pairs_cell<<<blocks_for(E, 256), 256, 0, side>>>(dw);
-    join(0);
+    join(0, side);
     // the candidate pairs stay in emission order; the contacts are sorted into pair order below
     mark(ST_NARROWPHASE);
     k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
-    fork(1);
+    fork(1, side);
     k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, side>>>(dw, p);
     k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, side>>>(dw, p);
     k_convex_reject<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
     // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
     k_convex_gjk<<<148u * 6u, 128, 0, s>>>(dw, p);
-    k_convex_probe<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    // separated pairs (probe) and penetrating ones (EPA) are disjoint queues
+    fork(3, side2);
+    k_convex_probe<<<blocks_for(P, 128), 128, 0, side2>>>(dw, p);
     k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
+    join(3, side2);
     k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
-    join(1);
+    join(1, side);
     mark(ST_COMPACT);
     k_contact_keys<<<blocks_for(C, 256), 256, 0, s>>>(dw);
     const uint32_t words = key_words(std::max(dw.k, 1u));
     record_sort(d, s, dw.cmaj, dw.cmin, dw.cval, dw.cmaj_alt, dw.cmin_alt, dw.cval_alt, dw.ctl + CTL_CONTACTS, 0, C, words,
                 words);
     k_contact_gather<<<blocks_for(C, 128), 128, 0, s>>>(dw);
+    // the solver blocks (target speeds, row claims) beside the identity, islands and wake passes:
+    // neither reads what the other writes (the relay rewrites only the w word of a contact's rows
+    // and the carried impulses; waking clears sleep flags the row claims do not look at)
+    mark(ST_SOLVER_PREPARE);
+    fork(2, side);
+    k_solver_blocks<<<blocks_for(C, 256), 256, 0, side>>>(dw, p);
+    record_scan(d, side, dw.row_flag, dw.row_offset, nullptr, std::max(dw.n, 1u), N, dw.ctl + CTL_SOLVER_ROWS);
+    k_solver_row_list<<<blocks_for(N, 256), 256, 0, side>>>(dw);
     mark(ST_IDENTITY);
     k_relay<<<blocks_for(C, 128), 128, 0, s>>>(dw);
     k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
@@ -644,10 +658,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     k_island_aggregate<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
     k_wake_live<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
-    mark(ST_SOLVER_PREPARE);
-    k_solver_blocks<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
-    record_scan(d, s, dw.row_flag, dw.row_offset, nullptr, std::max(dw.n, 1u), N, dw.ctl + CTL_SOLVER_ROWS);
-    k_solver_row_list<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+    join(2, side);
     for (uint32_t sub = 0; sub < p.substeps; ++sub) {
         mark(ST_INTEGRATE);
         k_integrate<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
@@ -925,11 +936,12 @@ void destroy_device(dyn_world* w) {
     for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
         if (p) cudaFree(p);
     }
-    for (uint32_t i = 0; i < 2; ++i) {
+    for (uint32_t i = 0; i < 4; ++i) {
         if (d->fork_events[i]) cudaEventDestroy(d->fork_events[i]);
         if (d->join_events[i]) cudaEventDestroy(d->join_events[i]);
     }
     if (d->side_stream) cudaStreamDestroy(d->side_stream);
+    if (d->side_stream2) cudaStreamDestroy(d->side_stream2);
     if (d->own_stream) cudaStreamDestroy(d->own_stream);
     delete d;
     w->dev = nullptr;
