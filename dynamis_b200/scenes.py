@@ -1,7 +1,7 @@
 """Seeded synthetic scenes: the benchmark workloads and the small scenes the tests pin.
 
-The workloads restate the scenes the north-star benchmark names (lattices of boxes, spheres and
-hulls falling onto a ground plane); no dataset is involved. Every random draw comes from
+The workloads are the benchmark scenes of this path (lattices of boxes, spheres and hulls falling
+onto a ground plane, hanging chains, batches of small worlds); no dataset is involved. Every random draw comes from
 numpy.random.default_rng(seed), so a seed fixes a scene bit for bit.
 """
 from __future__ import annotations
