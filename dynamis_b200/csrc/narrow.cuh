@@ -1125,6 +1125,38 @@ __device__ Hit separated_hit(const DeviceWorld& w, const WShape& first, const WS
 // ---- warp-cooperative pieces ----
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
+// A group of G consecutive lanes of a warp (G = 32: the whole warp) working on one pair: its lane
+// numbers, its member mask, and the warp intrinsics restricted to it.
+template <uint32_t G>
+struct Lanes {
+    static_assert(G == 32u || G == 16u || G == 8u, "a lane group is a power-of-two part of a warp");
+    uint32_t lane, base, mask;
+    __device__ __forceinline__ Lanes() {
+        const uint32_t l = threadIdx.x & 31u;
+        lane = l & (G - 1u);
+        base = l - lane;
+        if constexpr (G == 32u) {
+            mask = kFull;
+        } else {
+            mask = ((1u << G) - 1u) << base;
+        }
+    }
+    __device__ __forceinline__ uint32_t ballot(bool p) const {
+        const uint32_t b = __ballot_sync(mask, p) >> base;
+        if constexpr (G == 32u) {
+            return b;
+        } else {
+            return b & ((1u << G) - 1u);
+        }
+    }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+    __device__ __forceinline__ bool any(bool p) const { return __any_sync(mask, p); }
+    __device__ __forceinline__ uint32_t max(uint32_t v) const { return __reduce_max_sync(mask, v); }
+    __device__ __forceinline__ uint32_t min(uint32_t v) const { return __reduce_min_sync(mask, v); }
+    template <class T>
+    __device__ __forceinline__ T shfl(T v, uint32_t src) const { return __shfl_sync(mask, v, (int)src, (int)G); }
+};
+
 // An unsigned key that orders floats above -FLT_MAX as the floats compare: -0 and +0 share a key
 // (they compare equal), and NaN, -inf and -FLT_MAX (never above the scans' -FLT_MAX start) get 0.
 __device__ __forceinline__ uint32_t order_key(float x) {
@@ -1132,37 +1164,39 @@ __device__ __forceinline__ uint32_t order_key(float x) {
     const uint32_t b = __float_as_uint(x == 0.0f ? 0.0f : x);
     return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
-// The lane holding the first maximum of a warp-wide scan: the largest key, then the lowest index
-// among the lanes that hold it (each lane holds the first index of its own maximum). Returns
-// 0xFFFFFFFF when no lane holds a candidate.
-__device__ __forceinline__ uint32_t warp_first_max(uint32_t key, uint32_t index) {
-    const uint32_t top = __reduce_max_sync(kFull, key);
+// The first maximum of a group-wide scan: the largest key, then the lowest index among the lanes
+// that hold it (each lane holds the first index of its own maximum). Returns 0xFFFFFFFF when no
+// lane holds a candidate.
+template <uint32_t G>
+__device__ __forceinline__ uint32_t warp_first_max(const Lanes<G>& L, uint32_t key, uint32_t index) {
+    const uint32_t top = L.max(key);
     if (top == 0u) return 0xFFFFFFFFu;
-    return __reduce_min_sync(kFull, key == top ? index : 0xFFFFFFFFu);
+    return L.min(key == top ? index : 0xFFFFFFFFu);
 }
 
 // support_local over a hull with the warp's lanes striding the vertices; the reduction keeps the
 // sequential scan's choice: the largest dot product, the lowest index among equal ones.
-__device__ __forceinline__ f3 warp_support_local(const DeviceWorld& w, const WShape& s, f3 d) {
+template <uint32_t G>
+__device__ __forceinline__ f3 warp_support_local(const Lanes<G>& L, const DeviceWorld& w, const WShape& s, f3 d) {
     if (s.kind != 5u) return support_local(w, s, d);
     const dyn_shape_source_record& src = w.sources[s.source];
     const float4* verts = w.vertices + src.vertex_offset;
-    const uint32_t lane = threadIdx.x & 31u;
     float best = -3.402823466e38f;
     uint32_t bi = 0xFFFFFFFFu;
-    for (uint32_t i = lane; i < src.vertex_count; i += 32u) {
+    for (uint32_t i = L.lane; i < src.vertex_count; i += G) {
         float sd = dot(xyz(__ldg(verts + i)), d);
         if (sd > best) {
             best = sd;
             bi = i;
         }
     }
-    bi = warp_first_max(bi == 0xFFFFFFFFu ? 0u : order_key(best), bi);
+    bi = warp_first_max(L, bi == 0xFFFFFFFFu ? 0u : order_key(best), bi);
     return bi == 0xFFFFFFFFu ? s3(0.0f) : xyz(__ldg(verts + bi));
 }
-__device__ __forceinline__ f3 warp_support(const DeviceWorld& w, const WShape& s, f3 direction) {
+template <uint32_t G>
+__device__ __forceinline__ f3 warp_support(const Lanes<G>& L, const DeviceWorld& w, const WShape& s, f3 direction) {
     f3 local_d = quat_rotate(quat_conj(s.rotation), direction);
-    f3 local = warp_support_local(w, s, local_d * s.scale);
+    f3 local = warp_support_local(L, w, s, local_d * s.scale);
     return s.center + quat_rotate(s.rotation, local * s.scale);
 }
 
@@ -1186,12 +1220,13 @@ __device__ __forceinline__ void unpack_face(float4 f, uint32_t* a, uint32_t* b, 
 
 // (min distance, lowest index) over faces whose normal is longer than 0.5: the first minimum of
 // convex.wgsl:344-352, identical on every lane.
-__device__ __forceinline__ void warp_best_face(const EpaWarpShared& m, uint32_t fcount, float* best_dist, uint32_t* best_face) {
-    const uint32_t lane = threadIdx.x & 31u;
+template <uint32_t G>
+__device__ __forceinline__ void warp_best_face(const Lanes<G>& L, const EpaWarpShared& m, uint32_t fcount, float* best_dist,
+                                               uint32_t* best_face) {
     float bd = 3.402823466e38f;
     uint32_t bi = 0u;
     bool any = false;
-    for (uint32_t j = lane; j < fcount; j += 32u) {
+    for (uint32_t j = L.lane; j < fcount; j += G) {
         float4 f = m.fn[j];
         uint32_t a, b, c;
         unpack_face(f, &a, &b, &c);
@@ -1204,23 +1239,25 @@ __device__ __forceinline__ void warp_best_face(const EpaWarpShared& m, uint32_t 
         }
     }
     // the first minimum: the first maximum of the negated distances (negation is exact)
-    const uint32_t first = warp_first_max(any ? order_key(-bd) : 0u, any ? bi : 0xFFFFFFFFu);
+    const uint32_t first = warp_first_max(L, any ? order_key(-bd) : 0u, any ? bi : 0xFFFFFFFFu);
     if (first == 0xFFFFFFFFu) {
         *best_dist = 3.402823466e38f;
         *best_face = 0u;
         return;
     }
-    *best_dist = __shfl_sync(kFull, bd, first & 31u);  // face j lives on lane j % 32
+    *best_dist = L.shfl(bd, first & (G - 1u));  // face j lives on lane j % G
     *best_face = first;
 }
 
 // convex.wgsl:286-437 on one warp. All lanes return the same result.
-__device__ EpaOut warp_epa(const DeviceWorld& w, const WShape& first, const WShape& second, const f3* simplex, EpaWarpShared& m) {
-    const uint32_t lane = threadIdx.x & 31u;
+template <uint32_t G>
+__device__ EpaOut warp_epa(const Lanes<G>& L, const DeviceWorld& w, const WShape& first, const WShape& second,
+                           const f3* simplex, EpaWarpShared& m) {
+    const uint32_t lane = L.lane;
     const uint32_t lt = (1u << lane) - 1u;
     EpaOut invalid{false, mk3(0.0f, 1.0f, 0.0f), 0.0f};
     if (lane < 4u) m.poly[lane] = mk4(simplex[lane], 0.0f);
-    __syncwarp();
+    L.sync();
     const uint32_t tet[4][3] = {{0, 1, 2}, {0, 2, 3}, {0, 3, 1}, {1, 3, 2}};
     bool bad = false;
     if (lane < 4u) {
@@ -1236,24 +1273,24 @@ __device__ EpaOut warp_epa(const DeviceWorld& w, const WShape& first, const WSha
             m.fn[lane] = pack_face(dot(unit, centroid) > 0.0f ? -unit : unit, a, b, c);
         }
     }
-    if (__any_sync(kFull, bad)) return invalid;
-    __syncwarp();
+    if (L.any(bad)) return invalid;
+    L.sync();
     uint32_t fcount = 4, vc = 4;
     float bd = 0.0f;
     uint32_t bf = 0;
     for (uint32_t iter = 0; iter < 32u; ++iter) {
-        warp_best_face(m, fcount, &bd, &bf);
+        warp_best_face(L, m, fcount, &bd, &bf);
         f3 n = xyz(m.fn[bf]);
-        f3 probe = warp_support(w, first, n) - warp_support(w, second, -n);
+        f3 probe = warp_support(L, w, first, n) - warp_support(L, w, second, -n);
         float gain = dot(probe, n) - bd;
         if (gain < 1e-4f) break;
         if (vc >= 64u) break;
-        __syncwarp();
+        L.sync();
         if (lane == 0u) m.poly[vc] = mk4(probe, 0.0f);
         vc += 1;
         // visible faces in index order
         uint32_t vcount = 0;
-        for (uint32_t base = 0; base < fcount; base += 32u) {
+        for (uint32_t base = 0; base < fcount; base += G) {
             uint32_t j = base + lane;
             bool v = false;
             if (j < fcount) {
@@ -1263,15 +1300,15 @@ __device__ EpaOut warp_epa(const DeviceWorld& w, const WShape& first, const WSha
                 v = dot(xyz(f), probe - xyz(m.poly[a])) > 1e-6f;
                 m.visflag[j] = v ? 1u : 0u;
             }
-            uint32_t mask = __ballot_sync(kFull, v);
+            uint32_t mask = L.ballot(v);
             if (v) m.vis[vcount + __popc(mask & lt)] = (uint8_t)j;
             vcount += __popc(mask);
         }
-        __syncwarp();
+        L.sync();
         // horizon edges become new faces, in (visible face, edge) order, at most 64
         uint32_t ncount = 0;
         const uint32_t apex = vc - 1u;
-        for (uint32_t base = 0; base < 3u * vcount; base += 32u) {
+        for (uint32_t base = 0; base < 3u * vcount; base += G) {
             uint32_t t = base + lane;
             bool keep = false;
             float4 face = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1300,37 +1337,37 @@ __device__ EpaOut warp_epa(const DeviceWorld& w, const WShape& first, const WSha
                     }
                 }
             }
-            uint32_t mask = __ballot_sync(kFull, keep);
+            uint32_t mask = L.ballot(keep);
             uint32_t rank = ncount + __popc(mask & lt);
             if (keep && rank < 64u) m.nn[rank] = face;
             ncount = min(ncount + (uint32_t)__popc(mask), 64u);
         }
-        __syncwarp();
+        L.sync();
         // drop the visible faces, keeping order
         uint32_t write = 0;
-        for (uint32_t base = 0; base < fcount; base += 32u) {
+        for (uint32_t base = 0; base < fcount; base += G) {
             uint32_t j = base + lane;
             bool keepf = j < fcount && m.visflag[j] == 0u;
             float4 f = j < fcount ? m.fn[j] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            uint32_t mask = __ballot_sync(kFull, keepf);
-            __syncwarp();
+            uint32_t mask = L.ballot(keepf);
+            L.sync();
             if (keepf) m.fn[write + __popc(mask & lt)] = f;
             write += __popc(mask);
-            __syncwarp();
+            L.sync();
         }
         fcount = write;
         if (fcount + ncount > 128u) break;
-        for (uint32_t t = lane; t < ncount; t += 32u) m.fn[fcount + t] = m.nn[t];
+        for (uint32_t t = lane; t < ncount; t += G) m.fn[fcount + t] = m.nn[t];
         fcount += ncount;
-        __syncwarp();
+        L.sync();
     }
-    __syncwarp();
+    L.sync();
     float fd = 3.402823466e38f;
     uint32_t ff = bf;
     {
         float d2;
         uint32_t f2;
-        warp_best_face(m, fcount, &d2, &f2);
+        warp_best_face(L, m, fcount, &d2, &f2);
         fd = d2;
         if (d2 < 3.402823466e38f) ff = f2;
     }
@@ -1341,23 +1378,26 @@ __device__ EpaOut warp_epa(const DeviceWorld& w, const WShape& first, const WSha
     return r;
 }
 
-__device__ __forceinline__ float warp_projection_depth(const DeviceWorld& w, const WShape& f, const WShape& s, f3 direction) {
+template <uint32_t G>
+__device__ __forceinline__ float warp_projection_depth(const Lanes<G>& L, const DeviceWorld& w, const WShape& f, const WShape& s,
+                                                       f3 direction) {
     f3 n = normalize(direction);
-    return dot(warp_support(w, f, n) - warp_support(w, s, -n), n);
+    return dot(warp_support(L, w, f, n) - warp_support(L, w, s, -n), n);
 }
 
 // convex.wgsl:602-617 after a penetrating GJK (one warp, every lane returns the same hit).
-__device__ Hit warp_penetrating_hit(const DeviceWorld& w, const WShape& first, const WShape& second, const f3* simplex,
-                                    EpaWarpShared& m) {
-    EpaOut epa = warp_epa(w, first, second, simplex, m);
+template <uint32_t G>
+__device__ Hit warp_penetrating_hit(const Lanes<G>& L, const DeviceWorld& w, const WShape& first, const WShape& second,
+                                    const f3* simplex, EpaWarpShared& m) {
+    EpaOut epa = warp_epa(L, w, first, second, simplex, m);
     Hit result;
     bool accept = epa.valid && epa.depth > 0.0f && epa.depth < 3.402823466e38f && length(epa.normal) > 0.5f;
     if (accept) {
-        accept = epa.depth < warp_projection_depth(w, first, second, epa.normal) + 0.1f * wmin(shape_scale(first), shape_scale(second));
+        accept = epa.depth < warp_projection_depth(L, w, first, second, epa.normal) + 0.1f * wmin(shape_scale(first), shape_scale(second));
     }
     if (accept) {
-        f3 pa = warp_support(w, first, epa.normal);
-        f3 pb = warp_support(w, second, -epa.normal);
+        f3 pa = warp_support(L, w, first, epa.normal);
+        f3 pb = warp_support(L, w, second, -epa.normal);
         result = Hit{-epa.depth, (pa + pb) * 0.5f, epa.normal};
     } else {
         // convex_penetration_probe over the four-point simplex, centre direction and six axes: each
@@ -1376,20 +1416,20 @@ __device__ Hit warp_penetrating_hit(const DeviceWorld& w, const WShape& first, c
         const float ax[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
         for (uint32_t i = 0; i < 6; ++i)
             if (pc < 16u) probed[pc++] = mk3(ax[i][0], ax[i][1], ax[i][2]);
-        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t lane = L.lane;  // pc <= 11 < G: one direction per lane
         const float mine = lane < pc ? support_projection_depth(w, first, second, probed[lane]) : 3.402823466e38f;
         float best_depth = 3.402823466e38f;
         uint32_t best_i = pc;
         for (uint32_t i = 0; i < pc; ++i) {
-            const float depth = __shfl_sync(kFull, mine, i);
+            const float depth = L.shfl(mine, i);
             if (depth < best_depth) {
                 best_depth = depth;
                 best_i = i;
             }
         }
         const f3 best_normal = best_i < pc ? normalize(probed[best_i]) : mk3(0.0f, 1.0f, 0.0f);
-        f3 pa = warp_support(w, first, best_normal);
-        f3 pb = warp_support(w, second, -best_normal);
+        f3 pa = warp_support(L, w, first, best_normal);
+        f3 pb = warp_support(L, w, second, -best_normal);
         result = Hit{-best_depth, (pa + pb) * 0.5f, best_normal};
     }
     if (dot(result.normal, second.center - first.center) < 0.0f) result.normal = -result.normal;

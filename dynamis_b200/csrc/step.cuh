@@ -1002,25 +1002,30 @@ __global__ void __launch_bounds__(128) k_convex_probe(DeviceWorld w, dyn_step_pa
     }
 }
 
-// Phase 2: one warp per penetrating pair.
+// Phase 2: one lane group (half a warp) per penetrating pair: the polytopes of this path hold a few
+// dozen faces, which sixteen lanes cover in one or two strides, so two pairs share each warp's
+// instructions.
 constexpr int kEpaWarpsPerBlock = 4;
+constexpr uint32_t kEpaLanes = 16;
+constexpr uint32_t kEpaGroupsPerBlock = kEpaWarpsPerBlock * (32u / kEpaLanes);
 __global__ void __launch_bounds__(32 * kEpaWarpsPerBlock) k_convex_epa(DeviceWorld w, dyn_step_params p) {
-    __shared__ EpaWarpShared shared[kEpaWarpsPerBlock];
+    __shared__ EpaWarpShared shared[kEpaGroupsPerBlock];
     const uint32_t count = min(w.ctl[CTL_EPA], w.p_cap);
-    const uint32_t warp = threadIdx.x >> 5;
-    EpaWarpShared& m = shared[warp];
-    for (uint32_t e = blockIdx.x * kEpaWarpsPerBlock + warp; e < count; e += gridDim.x * kEpaWarpsPerBlock) {
+    const Lanes<kEpaLanes> L;
+    const uint32_t group = threadIdx.x / kEpaLanes;
+    EpaWarpShared& m = shared[group];
+    for (uint32_t e = blockIdx.x * kEpaGroupsPerBlock + group; e < count; e += gridDim.x * kEpaGroupsPerBlock) {
         uint32_t index = w.epa_list[e];
         WShape a, b;
         DBody fb, sb;
         convex_shapes(w, index, &a, &b, &fb, &sb);
         f3 simplex[4];
         for (uint32_t k = 0; k < 4; ++k) simplex[k] = xyz(w.epa_simplex[4 * (size_t)e + k]);
-        Hit hit = warp_penetrating_hit(w, a, b, simplex, m);
-        if ((threadIdx.x & 31u) == 0u) {
+        Hit hit = warp_penetrating_hit(L, w, a, b, simplex, m);
+        if (L.lane == 0u) {
             if (hit.distance <= pair_margin(p, fb, sb)) push_hit(w, index, hit);
         }
-        __syncwarp();
+        L.sync();
     }
 }
 
