@@ -107,6 +107,7 @@ struct DeviceWorld {
     const float4* vertices;
     // broadphase
     float4* aabb;  // [2k]: min.xyz, max.xyz
+    uint4* c_class;  // [k] per step: owner row, collision group, collision mask, kind | moves << 8 | unscaled << 9
     uint32_t* c_level;
     uint32_t* entry_count;
     uint32_t* entry_offset;

@@ -222,9 +222,20 @@ __device__ __forceinline__ float grid_extent_of(f3 mn, f3 mx) { return wmax(wmax
 __global__ void k_aabb(DeviceWorld w, dyn_step_params p) {
     GRID_STRIDE(i, w.k) {
         uint32_t owner = w.c_owner[i];
-        if (owner == DYN_NO_BODY) continue;
+        if (owner == DYN_NO_BODY) {
+            w.c_class[i] = make_uint4(DYN_NO_BODY, 0u, 0u, 0u);
+            continue;
+        }
         DBody b = load_dbody(w.hot, owner);
         DColl c = load_dcoll(w, i);
+        {  // what k_pair_class asks of this collider, in one record (nothing it reads changes before it runs)
+            const uint4 id = w.ident[owner];
+            const uint2 f = w.c_filter[i];
+            const bool unscaled = veq(c.scale, s3(1.0f));
+            w.c_class[i] = make_uint4(owner, f.x != DYN_NO_COLLISION_FILTER ? f.x : id.z,
+                                      f.y != DYN_NO_COLLISION_FILTER ? f.y : id.w,
+                                      c.kind | (moves(b.inverse_mass, b.flags) ? 0x100u : 0u) | (unscaled ? 0x200u : 0u));
+        }
         WShape s = world_shape(b.position, b.orientation, c);
         DAabb tight = world_aabb(w, s);
         WShape up = s;
@@ -630,23 +641,14 @@ __device__ __forceinline__ bool joined_by_joint(const DeviceWorld& w, uint32_t r
 __global__ void k_pair_class(DeviceWorld w) {
     const uint32_t pairs = min(w.counters[DYN_COUNTER_PAIRS], w.p_cap);
     GRID_STRIDE(index, pairs) {
-        uint32_t fs = w.pmaj[index], ss = w.pmin[index];
-        uint32_t fr = w.c_owner[fs], sr = w.c_owner[ss];
+        const uint4 f = w.c_class[w.pmaj[index]], s = w.c_class[w.pmin[index]];
+        const uint32_t fr = f.x, sr = s.x, fk = f.w & 0xffu, sk = s.w & 0xffu;
         int cls = -1;
         do {
             if (fr == DYN_NO_BODY || sr == DYN_NO_BODY || fr == sr) break;
-            const BodyHot& fh = w.hot[fr];
-            const BodyHot& sh = w.hot[sr];
-            if (!moves(fh.pos.w, fh.aux.y) && !moves(sh.pos.w, sh.aux.y)) break;
-            uint32_t fk = w.c_kind[fs].x, sk = w.c_kind[ss].x;
+            if (((f.w | s.w) & 0x100u) == 0u) break;  // neither body moves
             if (fk == 0u || sk == 0u) break;
-            uint4 fi = w.ident[fr], si = w.ident[sr];
-            uint2 ff = w.c_filter[fs], sf = w.c_filter[ss];
-            uint32_t fg = ff.x != DYN_NO_COLLISION_FILTER ? ff.x : fi.z;
-            uint32_t fm = ff.y != DYN_NO_COLLISION_FILTER ? ff.y : fi.w;
-            uint32_t sg = sf.x != DYN_NO_COLLISION_FILTER ? sf.x : si.z;
-            uint32_t sm = sf.y != DYN_NO_COLLISION_FILTER ? sf.y : si.w;
-            if (!((fg & sm) != 0u && (sg & fm) != 0u)) break;
+            if (!((f.y & s.z) != 0u && (s.y & f.z) != 0u)) break;
             if (joined_by_joint(w, fr, sr)) break;
             bool fw = shape_world_geometry(fk), sw = shape_world_geometry(sk);
             if (fw && sw) break;
@@ -655,7 +657,7 @@ __global__ void k_pair_class(DeviceWorld w) {
                 cls = PC_ANALYTIC;                // plane against a convex: one feature ring
                 break;
             }
-            bool unscaled = veq(xyz(w.c_scale[fs]), s3(1.0f)) && veq(xyz(w.c_scale[ss]), s3(1.0f));
+            bool unscaled = (f.w & s.w & 0x200u) != 0u;
             if (!unscaled || !shape_analytic(fk) || !shape_analytic(sk) || (fk == 2u && sk == 3u) || (fk == 3u && sk == 2u)) {
                 cls = PC_CONVEX;
             } else if (fk == 2u && sk == 2u) {

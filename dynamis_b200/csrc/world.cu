@@ -214,6 +214,7 @@ dyn_status ensure_device(dyn_world* w) {
         A(d->sources, d->src_cap);
         A(d->vertices, d->vert_cap);
         A(dw.aabb, 2 * (size_t)K);
+        A(dw.c_class, K);
         A(dw.c_level, K);
         A(dw.entry_count, K);
         A(dw.entry_offset, K);
