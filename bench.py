@@ -193,7 +193,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     m = world.measured()
     counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
               "P": int(m[R.COUNTER["PAIRS"]]), "C": int(m[R.COUNTER["CONTACTS"]]), "R": int(m[R.COUNTER["SOLVER_ROWS"]]),
-              "L": int(m[R.COUNTER["LIVE"]]), "J": world.constraint_count()}
+              "L": int(m[R.COUNTER["LIVE"]]), "J": world.constraint_count(),
+              "refused_pairs": int(m[R.COUNTER["REFUSED_PAIRS"]]), "pair_stream": world.stream_capacity()["pairs"]}
     launches_per_step = world.step_kernel_count()
     # per-stage breakdown: one more step run eagerly with CUDA events between stages
     world.set_timing(True)

@@ -33,6 +33,7 @@ SIGNATURES = {
     "dyn_spawn_bodies": (I32, [P, P, U32, P, U32, P]),
     "dyn_upload_bodies": (I32, [P, P, P, U32, P, P, U32]),
     "dyn_upload_states": (I32, [P, P, U32]),
+    "dyn_stream_capacity": (I32, [P, PU32, PU32]),
     "dyn_scene_sizes": (I32, [P, PU32, PU32, PU32, PU32, PU32]),
     "dyn_export_scene": (I32, [P, P, P, P, P, P, P]),
     "dyn_step_params_for": (I32, [P, F32, P]),

@@ -118,6 +118,7 @@ struct DeviceWorld {
     float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits
     uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
     uint32_t cell_bits;
+    uint32_t* spill;  // host-mapped: [0] unused, [1] pairs attempted, [2] pairs refused (left by a refusing step)
     uint32_t* pmaj;  // candidate pairs in emission order (lower, higher collider slot)
     uint32_t* pmin;
     // narrowphase, its staging set (append order) and the compaction into pair order

@@ -1956,6 +1956,14 @@ __global__ void k_sleep(DeviceWorld w, dyn_step_params p) {
         w.counters[DYN_COUNTER_LIVE] = w.ctl[CTL_LIVE];
         w.counters[DYN_COUNTER_SOLVER_ROWS] = w.ctl[CTL_SOLVER_ROWS];
         w.counters[DYN_COUNTER_STEP] += 1u;
+        // the host reads the pair demand (the largest since it last looked) and any refusal, and
+        // widens the pair stream before a later step
+        if (w.spill != nullptr) {
+            const uint32_t refused = w.counters[DYN_COUNTER_REFUSED_PAIRS];
+            const uint32_t demand = w.counters[DYN_COUNTER_PAIRS];
+            if (demand > w.spill[1]) w.spill[1] = demand;
+            if (refused != 0u) w.spill[2] = refused;
+        }
     }
     GRID_STRIDE(i, w.nd) {
         BodyHot& h = w.hot[i];

@@ -52,6 +52,7 @@ struct DeviceState {
     cudaStream_t stream = nullptr;
     DeviceWorld dw{};
     std::vector<void*> allocs;
+    uint32_t* spill_host = nullptr;  // host-mapped mailbox of refused pairs (DeviceWorld::spill)
     uint32_t n_cap = 0, k_cap = 0, e_cap = 0, p_cap = 0, c_cap = 0;
     uint32_t id_cap = 0;  // body ids the row_of_id table holds (ids of removed bodies are not reused)
     uint32_t src_cap = 0, vert_cap = 0;
@@ -173,6 +174,9 @@ dyn_status ensure_device(dyn_world* w) {
             DYN_CUDA(cudaEventCreateWithFlags(&d->join_events[i], cudaEventDisableTiming));
         }
         d->stream = w->user_stream ? static_cast<cudaStream_t>(w->user_stream) : d->own_stream;
+        DYN_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&d->spill_host), 4 * sizeof(uint32_t), cudaHostAllocMapped));
+        std::memset(d->spill_host, 0, 4 * sizeof(uint32_t));
+        DYN_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d->dw.spill), d->spill_host, 0));
         d->n_cap = std::max(n, w->capacity.bodies);
         d->k_cap = std::max(k, w->capacity.colliders);
         d->e_cap = 8u * std::max(d->k_cap, 1u);
@@ -931,6 +935,7 @@ void destroy_device(dyn_world* w) {
     release_graphs(d);
     for (cudaEvent_t e : d->events) cudaEventDestroy(e);
     for (void* p : d->allocs) cudaFree(p);
+    if (d->spill_host) cudaFreeHost(d->spill_host);
     for (void* p : d->joint_allocs) cudaFree(p);
     if (d->edit_buffer) cudaFree(d->edit_buffer);
     if (d->edit_run_buffer) cudaFree(d->edit_run_buffer);
@@ -1051,12 +1056,81 @@ DYN_API dyn_status dyn_upload_states(dyn_world* w, const dyn_body_state_record* 
     return DYN_OK;
 }
 
+// The pair stream widens after a step that refused pairs, as the reference widens its streams
+// after a spill (crates/dynamis-broadphase/src/capacity.rs:27-80 plans the pair stream from the
+// measured pair count; crates/dynamis-world/tests/suite/capacity.rs:142-187: within a few steps
+// the step stops refusing). Every step's last kernel leaves the pair demand and any refusal in
+// host-mapped memory, and each dyn_step reads them without waiting. Steps are queued ahead of the
+// device without bound, so a refusal can be seen many steps after it happened; the stream
+// therefore also widens as soon as the demand passes half of it, which keeps a growing pile from
+// reaching the limit before the host sees it. The new size is grown() of
+// crates/dynamis-domain/src/capacity.rs:15-23 applied to twice the demand: at least twice the
+// stream. The pair buffers are per-step scratch: nothing in them outlives a step, so they are
+// replaced, not copied. If the wider buffers cannot be had, the stream keeps its size and the
+// refusals stay counted.
+constexpr uint64_t kMaxPairCapacity = 1ull << 27;
+dyn_status widen_pair_stream(dyn_world* w) {
+    DeviceState* d = w->dev;
+    volatile uint32_t* mail = d->spill_host;
+    if (!mail || d->p_cap >= kMaxPairCapacity) return DYN_OK;
+    if (mail[2] == 0u && mail[1] <= d->p_cap / 2) return DYN_OK;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));  // no step in flight writes the mailbox or the buffers
+    const uint64_t demand = mail[1];
+    mail[1] = 0u;
+    mail[2] = 0u;
+    uint64_t want = std::max<uint64_t>(2ull * demand, 2ull * d->p_cap);
+    want = std::min<uint64_t>((want + 1023u) & ~1023ull, kMaxPairCapacity);
+    if (want <= d->p_cap) return DYN_OK;
+    const size_t P = (size_t)want;
+    DeviceWorld& dw = d->dw;
+    struct Buffer {
+        void** slot;
+        size_t bytes;
+        void* fresh;
+    };
+    Buffer list[] = {{reinterpret_cast<void**>(&dw.pmaj), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.pmin), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.np_list), (PC_COUNT + 1) * P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.epa_list), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.epa_simplex), 4 * P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.probe_list), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.probe_data), 6 * P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.hit_list), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.hit_data), 2 * P * sizeof(float4), nullptr}};
+    for (Buffer& b : list) {
+        if (cudaMalloc(&b.fresh, b.bytes) != cudaSuccess) {
+            for (Buffer& f : list) if (f.fresh) cudaFree(f.fresh);
+            (void)cudaGetLastError();  // out of memory: keep the stream, keep counting refusals
+            return DYN_OK;
+        }
+    }
+    for (Buffer& b : list) {
+        auto it = std::find(d->allocs.begin(), d->allocs.end(), *b.slot);
+        if (it != d->allocs.end()) d->allocs.erase(it);
+        DYN_CUDA(cudaFree(*b.slot));
+        DYN_CUDA(cudaMemsetAsync(b.fresh, 0, b.bytes, d->stream));
+        d->allocs.push_back(b.fresh);
+        *b.slot = b.fresh;
+    }
+    d->p_cap = dw.p_cap = (uint32_t)P;
+    release_graphs(d);  // the graphs hold the old buffers and capacity
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_stream_capacity(const dyn_world* w, uint32_t* pairs, uint32_t* contacts) {
+    if (!w || !pairs || !contacts) return DYN_ERR_INVALID;
+    *pairs = w->dev ? w->dev->p_cap : 0u;
+    *contacts = w->dev ? w->dev->c_cap : 0u;
+    return DYN_OK;
+}
+
 DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
     if (!w) return DYN_ERR_INVALID;
     dyn_status st = prepare_step(w, dt);
     if (st) return st;
     DeviceState* d = w->dev;
     DYN_CUDA(cudaSetDevice(w->device));
+    if ((st = widen_pair_stream(w))) return st;
     uint32_t parity = d->parity;
     if (w->timing) {
         for (cudaEvent_t e : d->events) cudaEventDestroy(e);

@@ -91,6 +91,13 @@ class World:
         states = np.ascontiguousarray(states, R.BODY_STATE)
         self._check(lib.dyn_upload_states(self._h, ptr(states), len(states)))
 
+    def stream_capacity(self) -> dict:
+        """The device's pair and contact stream capacities (World::stream_capacity); 0 before the first
+        step. The pair stream widens by itself after a step that refused pairs."""
+        pairs, contacts = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(lib.dyn_stream_capacity(self._h, ctypes.byref(pairs), ctypes.byref(contacts)))
+        return {"pairs": pairs.value, "contacts": contacts.value}
+
     def sizes(self) -> dict:
         vals = [ctypes.c_uint32() for _ in range(5)]
         self._check(lib.dyn_scene_sizes(self._h, *[ctypes.byref(v) for v in vals]))

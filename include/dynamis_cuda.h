@@ -153,6 +153,13 @@ DYN_API dyn_status dyn_upload_bodies(dyn_world* world, const dyn_body_state_reco
 /* Overwrites the n body states (row order) of the current scene. */
 DYN_API dyn_status dyn_upload_states(dyn_world* world, const dyn_body_state_record* states, uint32_t n);
 
+/* The device's pair and contact stream capacities (0 before the first step). The pair stream
+ * widens by itself, before a later dyn_step, once a step refused pairs or needed more than half of
+ * it: to twice the demand, at least twice its size (replaces World::stream_capacity,
+ * crates/dynamis-world/src/lib.rs:132, and the widening of
+ * crates/dynamis-broadphase/src/capacity.rs:27-80). */
+DYN_API dyn_status dyn_stream_capacity(const dyn_world* world, uint32_t* pairs, uint32_t* contacts);
+
 /* Host copy of the scene as rows: sizes, then records (any output pointer may be NULL). */
 DYN_API dyn_status dyn_scene_sizes(const dyn_world* world, uint32_t* bodies, uint32_t* dynamic_bodies,
                                    uint32_t* colliders, uint32_t* sources, uint32_t* vertices);
