@@ -138,11 +138,19 @@ LAUNCHES = {"velocity": lambda p: p["substeps"] * p["solve_iterations"],
             "integrate": lambda p: p["substeps"]}
 
 
+# Pair slots reserved per collider (World(capacity=...), the reference's kept reservation,
+# crates/dynamis-world/tests/suite/capacity.rs:228: a reservation serves a whole scene without a second
+# allocation). The formed mixed pile asks for up to ~18 pairs per collider in the timed steps; the
+# stream widens by itself past half of its size, so 48 keeps a widening (a wait for the queued steps,
+# new buffers and a new step graph) out of the timed region. Smaller streams are covered by the tests.
+PAIR_SLOTS_PER_COLLIDER = 48
+
+
 def build_world(workload: str, device: int):
     from dynamis_b200 import World, scenes
 
     scene = scenes.WORKLOADS[workload]()
-    world = World(device=device)
+    world = World(device=device, capacity={"pairs": PAIR_SLOTS_PER_COLLIDER * (len(scene.colliders) + 1)})
     t0 = time.perf_counter()
     scene.build(world)
     return world, scene, time.perf_counter() - t0
@@ -194,7 +202,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
               "P": int(m[R.COUNTER["PAIRS"]]), "C": int(m[R.COUNTER["CONTACTS"]]), "R": int(m[R.COUNTER["SOLVER_ROWS"]]),
               "L": int(m[R.COUNTER["LIVE"]]), "J": world.constraint_count(),
-              "refused_pairs": int(m[R.COUNTER["REFUSED_PAIRS"]]), "pair_stream": world.stream_capacity()["pairs"]}
+              "refused_pairs": int(m[R.COUNTER["REFUSED_PAIRS"]]), "pair_stream": world.stream_capacity()["pairs"],
+              "pair_stream_reserved": PAIR_SLOTS_PER_COLLIDER * (len(scene.colliders) + 1)}
     launches_per_step = world.step_kernel_count()
     # per-stage breakdown: one more step run eagerly with CUDA events between stages
     world.set_timing(True)

@@ -49,6 +49,11 @@ struct DeviceState {
     cudaStream_t side_stream2 = nullptr;
     cudaEvent_t fork_events[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t join_events[4] = {nullptr, nullptr, nullptr, nullptr};
+    // the last kStepsInFlight steps' completion events: dyn_step waits for the oldest before it
+    // queues another, so what the device reports (the pair demand) is at most that many steps old
+    cudaEvent_t inflight[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool inflight_used[4] = {false, false, false, false};
+    uint32_t inflight_next = 0;
     cudaStream_t stream = nullptr;
     DeviceWorld dw{};
     std::vector<void*> allocs;
@@ -172,6 +177,7 @@ dyn_status ensure_device(dyn_world* w) {
         for (uint32_t i = 0; i < 4; ++i) {
             DYN_CUDA(cudaEventCreateWithFlags(&d->fork_events[i], cudaEventDisableTiming));
             DYN_CUDA(cudaEventCreateWithFlags(&d->join_events[i], cudaEventDisableTiming));
+            DYN_CUDA(cudaEventCreateWithFlags(&d->inflight[i], cudaEventDisableTiming));
         }
         d->stream = w->user_stream ? static_cast<cudaStream_t>(w->user_stream) : d->own_stream;
         DYN_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&d->spill_host), 4 * sizeof(uint32_t), cudaHostAllocMapped));
@@ -945,6 +951,7 @@ void destroy_device(dyn_world* w) {
     for (uint32_t i = 0; i < 4; ++i) {
         if (d->fork_events[i]) cudaEventDestroy(d->fork_events[i]);
         if (d->join_events[i]) cudaEventDestroy(d->join_events[i]);
+        if (d->inflight[i]) cudaEventDestroy(d->inflight[i]);
     }
     if (d->side_stream) cudaStreamDestroy(d->side_stream);
     if (d->side_stream2) cudaStreamDestroy(d->side_stream2);
@@ -1060,15 +1067,16 @@ DYN_API dyn_status dyn_upload_states(dyn_world* w, const dyn_body_state_record* 
 // after a spill (crates/dynamis-broadphase/src/capacity.rs:27-80 plans the pair stream from the
 // measured pair count; crates/dynamis-world/tests/suite/capacity.rs:142-187: within a few steps
 // the step stops refusing). Every step's last kernel leaves the pair demand and any refusal in
-// host-mapped memory, and each dyn_step reads them without waiting. Steps are queued ahead of the
-// device without bound, so a refusal can be seen many steps after it happened; the stream
-// therefore also widens as soon as the demand passes half of it, which keeps a growing pile from
-// reaching the limit before the host sees it. The new size is grown() of
+// host-mapped memory, and each dyn_step reads them without waiting. Up to kStepsInFlight steps
+// are queued ahead of the device, so a refusal is seen up to that many steps after it happened;
+// the stream therefore also widens as soon as the demand passes half of it, which keeps a growing
+// pile from reaching the limit before the host sees it. The new size is grown() of
 // crates/dynamis-domain/src/capacity.rs:15-23 applied to twice the demand: at least twice the
 // stream. The pair buffers are per-step scratch: nothing in them outlives a step, so they are
 // replaced, not copied. If the wider buffers cannot be had, the stream keeps its size and the
 // refusals stay counted.
 constexpr uint64_t kMaxPairCapacity = 1ull << 27;
+constexpr uint32_t kStepsInFlight = 4u;
 dyn_status widen_pair_stream(dyn_world* w) {
     DeviceState* d = w->dev;
     volatile uint32_t* mail = d->spill_host;
@@ -1130,6 +1138,8 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
     if (st) return st;
     DeviceState* d = w->dev;
     DYN_CUDA(cudaSetDevice(w->device));
+    const uint32_t slot = d->inflight_next;
+    if (d->inflight_used[slot]) DYN_CUDA(cudaEventSynchronize(d->inflight[slot]));
     if ((st = widen_pair_stream(w))) return st;
     uint32_t parity = d->parity;
     if (w->timing) {
@@ -1162,6 +1172,9 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
         }
         DYN_CUDA(cudaGraphLaunch(d->exec[parity], d->stream));
     }
+    DYN_CUDA(cudaEventRecord(d->inflight[slot], d->stream));
+    d->inflight_used[slot] = true;
+    d->inflight_next = (slot + 1u) % kStepsInFlight;
     d->last_parity = parity;
     d->parity ^= 1u;
     d->stepped = true;

@@ -79,3 +79,24 @@ def test_one_full_size_step_matches_the_oracle(formed_pile):
     assert np.array_equal(islands[islands], islands)
     assert np.all(islands <= np.arange(len(islands)))
     world.close()
+
+
+def test_worlds_stay_bit_identical_through_the_pair_stream_widening():
+    """150 steps: the pile's pair demand passes half the first pair stream and the stream widens on
+    both worlds; their states still agree bit for bit, and the last step refused no pair."""
+    finals = []
+    for _ in range(2):
+        w = World()
+        scenes.WORKLOADS["mixed_pile_262144"]().build(w)
+        first = None
+        for step in range(150):
+            w.step(DT)
+            if step == 0:
+                w.wait()
+                first = w.stream_capacity()["pairs"]
+        w.wait()
+        assert w.stream_capacity()["pairs"] > first, "the pile's demand must widen the pair stream"
+        assert w.measured()[R.COUNTER["REFUSED_PAIRS"]] == 0
+        finals.append(w.read_states().tobytes())
+        w.close()
+    assert finals[0] == finals[1]
