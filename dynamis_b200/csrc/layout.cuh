@@ -66,6 +66,7 @@ enum Ctl : uint32_t {
     CTL_GJK_NEXT = 16,       // next convex pair ticket of the GJK kernel
     CTL_GJK_PAIRS = 17,      // convex pairs past the centre-axis rejection
     CTL_PROBES = 18,         // separated convex pairs queued for the penetration probe
+    CTL_EPA_NEXT = 19,       // next penetrating pair ticket of the EPA kernel
     CTL_COUNT = 32
 };
 

@@ -1016,7 +1016,11 @@ __global__ void __launch_bounds__(32 * kEpaWarpsPerBlock) k_convex_epa(DeviceWor
     const Lanes<kEpaLanes> L;
     const uint32_t group = threadIdx.x / kEpaLanes;
     EpaWarpShared& m = shared[group];
-    for (uint32_t e = blockIdx.x * kEpaGroupsPerBlock + group; e < count; e += gridDim.x * kEpaGroupsPerBlock) {
+    for (;;) {  // each lane group takes the next pair from a shared ticket: pairs differ in cost
+        uint32_t e = 0u;
+        if (L.lane == 0u) e = atomicAdd(&w.ctl[CTL_EPA_NEXT], 1u);
+        e = L.shfl(e, 0u);
+        if (e >= count) break;
         uint32_t index = w.epa_list[e];
         WShape a, b;
         DBody fb, sb;
@@ -1064,8 +1068,10 @@ __global__ void __launch_bounds__(128) k_convex_manifold(DeviceWorld w, dyn_step
     }
 }
 
+// Four blocks per SM: the analytic class then holds 128 registers (a few spilled) instead of 168,
+// which measured faster than the three blocks its registers allow otherwise.
 template <int kClass>
-__global__ void __launch_bounds__(128) k_narrow_class(DeviceWorld w, dyn_step_params p) {
+__global__ void __launch_bounds__(128, 4) k_narrow_class(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = min(w.ctl[CTL_LIST0 + kClass], w.p_cap);
     const uint32_t* list = w.np_list + (size_t)kClass * w.p_cap;
     GRID_STRIDE(i, count) narrow_pair<kClass>(w, p, list[i]);
