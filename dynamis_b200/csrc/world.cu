@@ -693,9 +693,9 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
             // each iteration applies the one before it; one apply after the last
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 if (it == 0u) {
-                    k_position_fused<true><<<blocks_for(C, 256), 256, 0, s>>>(dw, p, it);
+                    k_position_fused<true><<<blocks_for(C, 128), 128, 0, s>>>(dw, p, it);
                 } else {
-                    k_position_fused<false><<<blocks_for(C, 256), 256, 0, s>>>(dw, p, it);
+                    k_position_fused<false><<<blocks_for(C, 128), 128, 0, s>>>(dw, p, it);
                 }
             }
             if (p.position_iterations > 0u) k_papply_last<<<blocks_for(N, 256), 256, 0, s>>>(dw, p.position_iterations);
