@@ -99,8 +99,8 @@ class ClockSampler:
 
 
 # DRAM bytes the narrowphase stage moved per candidate pair, measured with ncu on the formed
-# 32,768-body pile (profiles/narrowphase_traffic_mixed_pile_32768.md); the full-size workload is too
-# large for a multi-metric capture, and the traffic grows with the pair count.
+# 32,768-body pile; the full-size workload is too large for a multi-metric capture, and the traffic
+# grows with the pair count.
 NARROWPHASE_DRAM_BYTES_PER_PAIR = 250.0
 
 
@@ -202,7 +202,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
               "P": int(m[R.COUNTER["PAIRS"]]), "C": int(m[R.COUNTER["CONTACTS"]]), "R": int(m[R.COUNTER["SOLVER_ROWS"]]),
               "L": int(m[R.COUNTER["LIVE"]]), "J": world.constraint_count(),
-              "refused_pairs": int(m[R.COUNTER["REFUSED_PAIRS"]]), "pair_stream": world.stream_capacity()["pairs"],
+              "refused_pairs": int(m[R.COUNTER["REFUSED_PAIRS"]]),
+              "refused_contacts": int(m[R.COUNTER["REFUSED_CONTACTS"]]), "pair_stream": world.stream_capacity()["pairs"],
               "pair_stream_reserved": PAIR_SLOTS_PER_COLLIDER * (len(scene.colliders) + 1)}
     launches_per_step = world.step_kernel_count()
     # per-stage breakdown: one more step run eagerly with CUDA events between stages

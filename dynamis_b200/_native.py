@@ -55,6 +55,9 @@ SIGNATURES = {
     "dyn_stage_timings": (I32, [P, P, U32]),
     "dyn_radix_sort": (I32, [P, P, P, P, U32, U32, U32]),
     "dyn_radix_sort_static": (I32, [P, P, P, U32, U32, U32, P]),
+    "dyn_radix_sort_static_status": (I32, [P, PU32]),
+    "dyn_clear_device_status": (I32, [P]),
+    "dyn_debug_sort_fault": (I32, [P, U32, U32]),
     "dyn_set_body_worlds": (I32, [P, P, U32]),
     "dyn_edit_bodies": (I32, [P, P, P, U32]),
     "dyn_remove_bodies": (I32, [P, P, U32]),

@@ -10,11 +10,14 @@
 //     counts, and resolves its global digit prefix by decoupled look-back over earlier tiles;
 //   * keys are staged in shared memory in digit order so the global scatter is coalesced runs.
 // Tiles are claimed from an atomic counter, so a tile only waits on tiles already running.
-// Every look-back wait is bounded; a wait that runs out sets DYN_STATUS_LOOKBACK_TIMEOUT in the
-// world's status word and the pass finishes without trapping.
+// Every look-back wait is bounded (spin_limit polls per thread, kLookbackSpinLimit unless a caller
+// lowers it); a wait that runs out sets DYN_STATUS_LOOKBACK_TIMEOUT in the status word it is given
+// and the pass finishes without trapping.
 #pragma once
 
 #include <cstdint>
+
+#include "dynamis_cuda.h"
 
 namespace dyn {
 
@@ -26,8 +29,7 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
 
-constexpr uint32_t DYN_STATUS_LOOKBACK_TIMEOUT = 1u << 0;
-constexpr uint32_t DYN_STATUS_ISLAND_HOOKS = 1u << 1;
+// DYN_STATUS_* bits: dynamis_cuda.h
 
 __device__ __forceinline__ uint32_t load_relaxed(const uint32_t* p) {
     return *reinterpret_cast<const volatile uint32_t*>(p);
@@ -87,7 +89,7 @@ static __global__ void __launch_bounds__(kSortThreads)
                const uint32_t* __restrict__ val_in, uint32_t* __restrict__ key_out, uint32_t* __restrict__ other_out,
                uint32_t* __restrict__ val_out, const uint32_t* __restrict__ count_ptr, uint32_t n_fixed, uint32_t cap,
                int shift, const uint32_t* __restrict__ digit_base, uint32_t* __restrict__ lookback,
-               uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status) {
+               uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status, uint32_t spin_limit) {
     constexpr int kWarps = kSortThreads / 32;
     __shared__ uint32_t warp_hist[kWarps][256];
     __shared__ uint32_t tile_start[256];
@@ -155,7 +157,7 @@ static __global__ void __launch_bounds__(kSortThreads)
             uint32_t word = load_relaxed(lookback + (size_t)t * 256u + d);
             uint32_t flag = word & ~kValueMask;
             if (flag == 0u) {
-                if (++spins > kLookbackSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(status, DYN_STATUS_LOOKBACK_TIMEOUT);
                     break;
                 }
@@ -207,7 +209,7 @@ static __global__ void __launch_bounds__(kSortThreads)
 static __global__ void __launch_bounds__(kSortThreads)
     k_scan_exclusive(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint32_t* __restrict__ count_ptr,
                      uint32_t n_fixed, uint32_t cap, uint32_t* __restrict__ total, uint32_t* __restrict__ lookback,
-                     uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status) {
+                     uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status, uint32_t spin_limit) {
     __shared__ uint32_t tile_id;
     __shared__ uint32_t warp_sums[kSortThreads / 32];
     __shared__ uint32_t tile_exclusive;
@@ -260,7 +262,7 @@ static __global__ void __launch_bounds__(kSortThreads)
                     uint32_t word = load_relaxed(&lookback[t]);
                     uint32_t flag = word & ~kValueMask;
                     if (flag == 0u) {
-                        if (++spins > kLookbackSpinLimit) {
+                        if (++spins > spin_limit) {
                             atomicOr(status, DYN_STATUS_LOOKBACK_TIMEOUT);
                             break;
                         }

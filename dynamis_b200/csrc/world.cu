@@ -72,6 +72,11 @@ struct DeviceState {
     uint32_t* sort_alt1 = nullptr;
     uint32_t* sort_alt2 = nullptr;
     uint32_t sort_alt_cap = 0;
+    // test hook (dyn_debug_sort_fault): the next dyn_radix_sort starts each digit pass's tile
+    // ticket at sort_fault_skip (tiles below it never run) and polls at most sort_fault_limit times
+    bool sort_fault_armed = false;
+    uint32_t sort_fault_skip = 0;
+    uint32_t sort_fault_limit = kLookbackSpinLimit;
     dyn_body_state_record* staging = nullptr;  // n_cap ABI state records
     std::vector<void*> joint_allocs;  // constraint buffers, rebuilt whenever the constraint set changes
     // body edits: once a world has taken edits its step graph runs k_clear_inputs, k_body_edits and
@@ -89,6 +94,7 @@ struct DeviceState {
     bool stepped = false;
     bool uploaded = false;  // the current scene's records are on the device
     uint32_t graph_kernels = 0;  // kernel nodes in one step's graph
+    uint32_t sms = 148;          // multiprocessors of the device (read when the device state is made)
     dyn_step_params params{};
     // timing
     std::vector<cudaEvent_t> events;
@@ -137,9 +143,10 @@ uint32_t key_words(uint32_t n) {
     return words < 1 ? 1 : (words > 4 ? 4 : words);
 }
 inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
-inline uint32_t blocks_for(uint32_t n, uint32_t threads) {
+// Grid-stride launches: enough blocks for n threads, at most 16 blocks per SM of the device.
+inline uint32_t blocks_for(const DeviceState* d, uint32_t n, uint32_t threads) {
     uint32_t b = div_up(std::max<uint32_t>(n, 1), threads);
-    return std::min<uint32_t>(b, 148u * 16u);
+    return std::min<uint32_t>(b, d->sms * 16u);
 }
 
 void release_graphs(DeviceState* d) {
@@ -171,6 +178,9 @@ dyn_status ensure_device(dyn_world* w) {
         DYN_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 16384));
         d = new DeviceState();
         w->dev = d;
+        int sm_count = 0;
+        DYN_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, w->device));
+        d->sms = (uint32_t)std::max(sm_count, 1);
         DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream2, cudaStreamNonBlocking));
@@ -485,7 +495,7 @@ dyn_status download_states(dyn_world* w, std::vector<dyn_body_state_record>* out
     DeviceState* d = w->dev;
     uint32_t n = d->dw.n;
     out->resize(n);
-    k_pack_states<<<blocks_for(std::max(n, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, n);
+    k_pack_states<<<blocks_for(d, std::max(n, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, n);
     DYN_CUDA(cudaGetLastError());
     DYN_CUDA(cudaMemcpyAsync(out->data(), d->staging, (size_t)n * sizeof(dyn_body_state_record), cudaMemcpyDeviceToHost,
                              d->stream));
@@ -496,14 +506,22 @@ dyn_status download_states(dyn_world* w, std::vector<dyn_body_state_record>* out
 // Stable LSD sort launches on `s` (see sort.cuh). Data ends in the primary buffers.
 void record_sort(DeviceState* d, cudaStream_t s, uint32_t* major, uint32_t* minor, uint32_t* val, uint32_t* major_alt,
                  uint32_t* minor_alt, uint32_t* val_alt, const uint32_t* count_ptr, uint32_t n_fixed, uint32_t cap,
-                 uint32_t major_digits, uint32_t minor_digits) {
+                 uint32_t major_digits, uint32_t minor_digits, uint32_t spin_limit = kLookbackSpinLimit,
+                 uint32_t first_ticket = 0) {
     uint32_t passes = major_digits + minor_digits;
     if (passes == 0) return;
     uint32_t tiles = std::max(div_up(cap, kSortTile), 1u);
     cudaMemsetAsync(d->hist, 0, passes * 256 * 4, s);
     cudaMemsetAsync(d->tile_counters, 0, 16 * 4, s);
+    if (first_ticket) {
+        // test hook only: every pass's tickets start above tile 0, so the tiles after it wait on a
+        // look-back word nothing writes until their bounded polls run out
+        static uint32_t tickets[8];
+        for (uint32_t& t : tickets) t = first_ticket;
+        cudaMemcpyAsync(d->tile_counters, tickets, sizeof(tickets), cudaMemcpyHostToDevice, s);
+    }
     cudaMemsetAsync(d->lookback, 0, (size_t)passes * tiles * 256 * 4, s);
-    k_sort_histogram<<<std::min(div_up(cap, 256), 148u * 4u), 256, 0, s>>>(major, minor, count_ptr, n_fixed, cap,
+    k_sort_histogram<<<std::min(div_up(cap, 256), d->sms * 4u), 256, 0, s>>>(major, minor, count_ptr, n_fixed, cap,
                                                                             (int)major_digits, (int)minor_digits, d->hist);
     k_sort_offsets<<<1, 256, 0, s>>>(d->hist, (int)passes);
     uint32_t* src_major = major;
@@ -525,19 +543,19 @@ void record_sort(DeviceState* d, cudaStream_t s, uint32_t* major, uint32_t* mino
         if (two && val) {
             k_onesweep<true, true><<<tiles, kSortThreads, 0, s>>>(key_in, oth_in, src_val, key_out, oth_out, dst_val, count_ptr,
                                                                    n_fixed, cap, shift, d->hist + p * 256, lb,
-                                                                   d->tile_counters + p, status);
+                                                                   d->tile_counters + p, status, spin_limit);
         } else if (two) {
             k_onesweep<true, false><<<tiles, kSortThreads, 0, s>>>(key_in, oth_in, nullptr, key_out, oth_out, nullptr, count_ptr,
                                                                     n_fixed, cap, shift, d->hist + p * 256, lb,
-                                                                    d->tile_counters + p, status);
+                                                                    d->tile_counters + p, status, spin_limit);
         } else if (val) {
             k_onesweep<false, true><<<tiles, kSortThreads, 0, s>>>(key_in, nullptr, src_val, key_out, nullptr, dst_val, count_ptr,
                                                                     n_fixed, cap, shift, d->hist + p * 256, lb,
-                                                                    d->tile_counters + p, status);
+                                                                    d->tile_counters + p, status, spin_limit);
         } else {
             k_onesweep<false, false><<<tiles, kSortThreads, 0, s>>>(key_in, nullptr, nullptr, key_out, nullptr, nullptr,
                                                                      count_ptr, n_fixed, cap, shift, d->hist + p * 256, lb,
-                                                                     d->tile_counters + p, status);
+                                                                     d->tile_counters + p, status, spin_limit);
         }
         std::swap(src_major, dst_major);
         std::swap(src_minor, dst_minor);
@@ -558,7 +576,7 @@ void record_scan(DeviceState* d, cudaStream_t s, const uint32_t* in, uint32_t* o
     cudaMemsetAsync(d->tile_counters + 15, 0, 4, s);
     cudaMemsetAsync(d->lookback, 0, (size_t)tiles * 4, s);
     k_scan_exclusive<<<tiles, kSortThreads, 0, s>>>(in, out, count_ptr, n_fixed, cap, total, d->lookback, d->tile_counters + 15,
-                                                    d->dw.ctl + CTL_STATUS);
+                                                    d->dw.ctl + CTL_STATUS, kLookbackSpinLimit);
 }
 
 struct Marker {
@@ -587,25 +605,25 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     const uint32_t joint_blocks = dw.jgroup_count;  // one warp group per 32-thread block
     mark(ST_BEGIN);
     k_reset<<<1, 64, 0, s>>>(dw);
-    if (dw.jcount) k_joint_count<<<blocks_for(std::max(dw.jfilter_count, 1u), 256), 256, 0, s>>>(dw);
+    if (dw.jcount) k_joint_count<<<blocks_for(d, std::max(dw.jfilter_count, 1u), 256), 256, 0, s>>>(dw);
     if (d->edit_graphs) {
-        k_clear_inputs<<<blocks_for(N, 256), 256, 0, s>>>(dw);
-        k_body_edits<<<blocks_for(std::max(d->edit_capacity, 1u), 128), 128, 0, s>>>(dw);
-        k_begin<false><<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+        k_clear_inputs<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
+        k_body_edits<<<blocks_for(d, std::max(d->edit_capacity, 1u), 128), 128, 0, s>>>(dw);
+        k_begin<false><<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
     } else {
-        k_begin<true><<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+        k_begin<true><<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
     }
     mark(ST_AABB);
-    k_aabb<<<blocks_for(K, 128), 128, 0, s>>>(dw, p);
+    k_aabb<<<blocks_for(d, K, 128), 128, 0, s>>>(dw, p);
     mark(ST_ENTRIES);
-    k_entry_count<<<blocks_for(K, 256), 256, 0, s>>>(dw);
+    k_entry_count<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, std::max(dw.k, 1u), dw.ctl + CTL_ENTRIES);
-    k_entry_emit<<<blocks_for(K, 256), 256, 0, s>>>(dw);
+    k_entry_emit<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     mark(ST_ENTRY_SORT);
     record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
     mark(ST_PAIRS);
-    k_cell_clear<<<blocks_for(1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
-    k_cell_insert<<<blocks_for(E, 256), 256, 0, s>>>(dw);
+    k_cell_clear<<<blocks_for(d, 1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
+    k_cell_insert<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);
     // Independent kernels run as parallel branches of the captured graph (a fork onto the side
     // stream and a join back): the coarse links beside the same-cell scan, the analytic classes
     // beside the convex chain. They only share append counters, and every product they feed is
@@ -624,91 +642,91 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         cudaStreamWaitEvent(s, d->join_events[k], 0);
     };
     fork(0, side);
-    k_pairs_coarse<<<dim3(blocks_for(K, 128), kCoarseLevelSlices), 128, 0, s>>>(dw);
-    k_pairs_cell<<<blocks_for(E, 256), 256, 0, side>>>(dw);
+    k_pairs_coarse<<<dim3(blocks_for(d, K, 128), kCoarseLevelSlices), 128, 0, s>>>(dw);
+    k_pairs_cell<<<blocks_for(d, E, 256), 256, 0, side>>>(dw);
     join(0, side);
     // the candidate pairs stay in emission order; the contacts are sorted into pair order below
     mark(ST_NARROWPHASE);
-    k_pair_class<<<blocks_for(P, 256), 256, 0, s>>>(dw);
+    k_pair_class<<<blocks_for(d, P, 256), 256, 0, s>>>(dw);
     fork(1, side);
-    k_narrow_class<PC_ANALYTIC><<<blocks_for(P, 128), 128, 0, side>>>(dw, p);
-    k_narrow_class<PC_BOXES><<<blocks_for(P, 128), 128, 0, side>>>(dw, p);
-    k_convex_reject<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    k_narrow_class<PC_ANALYTIC><<<blocks_for(d, P, 128), 128, 0, side>>>(dw, p);
+    k_narrow_class<PC_BOXES><<<blocks_for(d, P, 128), 128, 0, side>>>(dw, p);
+    k_convex_reject<<<blocks_for(d, P, 128), 128, 0, s>>>(dw, p);
     // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
-    k_convex_gjk<<<148u * 6u, 128, 0, s>>>(dw, p);
+    k_convex_gjk<<<d->sms * 6u, 128, 0, s>>>(dw, p);
     // separated pairs (probe) and penetrating ones (EPA) are disjoint queues
     fork(3, side2);
-    k_convex_probe<<<blocks_for(P, 128), 128, 0, side2>>>(dw, p);
-    k_convex_epa<<<148u * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
+    k_convex_probe<<<blocks_for(d, P, 128), 128, 0, side2>>>(dw, p);
+    k_convex_epa<<<d->sms * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     join(3, side2);
-    k_convex_manifold<<<blocks_for(P, 128), 128, 0, s>>>(dw, p);
+    k_convex_manifold<<<blocks_for(d, P, 128), 128, 0, s>>>(dw, p);
     join(1, side);
     mark(ST_COMPACT);
-    k_contact_keys<<<blocks_for(C, 256), 256, 0, s>>>(dw);
+    k_contact_keys<<<blocks_for(d, C, 256), 256, 0, s>>>(dw);
     const uint32_t words = key_words(std::max(dw.k, 1u));
     record_sort(d, s, dw.cmaj, dw.cmin, dw.cval, dw.cmaj_alt, dw.cmin_alt, dw.cval_alt, dw.ctl + CTL_CONTACTS, 0, C, words,
                 words);
-    k_contact_gather<<<blocks_for(C, 128), 128, 0, s>>>(dw);
+    k_contact_gather<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
     // the solver blocks (target speeds, row claims) beside the identity, islands and wake passes:
     // neither reads what the other writes (the relay rewrites only the w word of a contact's rows
     // and the carried impulses; waking clears sleep flags the row claims do not look at)
     mark(ST_SOLVER_PREPARE);
     fork(2, side);
-    k_solver_blocks<<<blocks_for(C, 256), 256, 0, side>>>(dw, p);
+    k_solver_blocks<<<blocks_for(d, C, 256), 256, 0, side>>>(dw, p);
     record_scan(d, side, dw.row_flag, dw.row_offset, nullptr, std::max(dw.n, 1u), N, dw.ctl + CTL_SOLVER_ROWS);
-    k_solver_row_list<<<blocks_for(N, 256), 256, 0, side>>>(dw);
+    k_solver_row_list<<<blocks_for(d, N, 256), 256, 0, side>>>(dw);
     mark(ST_IDENTITY);
-    k_relay<<<blocks_for(C, 128), 128, 0, s>>>(dw);
-    k_contact_begin<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
+    k_relay<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
+    k_contact_begin<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
     mark(ST_ISLANDS);
-    k_island_link<true><<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
-    k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
-    k_island_link<false><<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
-    if (dw.jcount) k_island_link_joints<<<blocks_for(dw.jcount, 256), 256, 0, s>>>(dw);
-    k_island_flatten<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
-    k_island_aggregate<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    k_island_link<true><<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
+    k_island_flatten<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
+    k_island_link<false><<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
+    if (dw.jcount) k_island_link_joints<<<blocks_for(d, dw.jcount, 256), 256, 0, s>>>(dw);
+    k_island_flatten<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
+    k_island_aggregate<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
-    k_wake_live<<<blocks_for(ND, 256), 256, 0, s>>>(dw);
+    k_wake_live<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     join(2, side);
     for (uint32_t sub = 0; sub < p.substeps; ++sub) {
         mark(ST_INTEGRATE);
-        k_integrate<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
-        k_solve_prepare<<<blocks_for(C, 128), 128, 0, s>>>(dw);
+        k_integrate<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
+        k_solve_prepare<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
         if (sub == 0) {
             mark(ST_WARM);
             if (joint_blocks) k_joints<JP_WARM><<<joint_blocks, 32, 0, s>>>(dw, p);
-            k_warm<<<blocks_for(C, 128), 128, 0, s>>>(dw);
-            k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+            k_warm<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
+            k_vapply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_VELOCITY);
         for (uint32_t it = 0; it < p.solve_iterations; ++it) {
             if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 32, 0, s>>>(dw, p);
-            k_solve<<<blocks_for(C, 128), 128, 0, s>>>(dw, p);
-            k_vapply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+            k_solve<<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p);
+            k_vapply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_ADVANCE);
-        k_advance<<<blocks_for(N, 256), 256, 0, s>>>(dw, p);
+        k_advance<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
         mark(ST_POSITION);
         if (joint_blocks == 0u) {
             // each iteration applies the one before it; one apply after the last
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 if (it == 0u) {
-                    k_position_fused<true><<<blocks_for(C, 128), 128, 0, s>>>(dw, p, it);
+                    k_position_fused<true><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it);
                 } else {
-                    k_position_fused<false><<<blocks_for(C, 128), 128, 0, s>>>(dw, p, it);
+                    k_position_fused<false><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it);
                 }
             }
-            if (p.position_iterations > 0u) k_papply_last<<<blocks_for(N, 256), 256, 0, s>>>(dw, p.position_iterations);
+            if (p.position_iterations > 0u) k_papply_last<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p.position_iterations);
         } else {
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 k_joints<JP_POSITION><<<joint_blocks, 32, 0, s>>>(dw, p);
-                k_position<<<blocks_for(C, 256), 256, 0, s>>>(dw, p);
-                k_papply<<<blocks_for(N, 256), 256, 0, s>>>(dw);
+                k_position<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
+                k_papply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
             }
         }
     }
     mark(ST_SLEEP);
-    k_sleep<<<blocks_for(ND, 256), 256, 0, s>>>(dw, p);
+    k_sleep<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw, p);
     mark(ST_COUNT);
 }
 
@@ -903,9 +921,9 @@ dyn_status observe_after_step(dyn_world* w) {
     }
     if (m > 0) {
         if (o.all) {
-            k_pack_states<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, d->staging, m);
+            k_pack_states<<<blocks_for(d, m, 256), 256, 0, d->stream>>>(d->dw, d->staging, m);
         } else {
-            k_pack_ids<<<blocks_for(m, 256), 256, 0, d->stream>>>(d->dw, static_cast<const uint32_t*>(o.ids_dev),
+            k_pack_ids<<<blocks_for(d, m, 256), 256, 0, d->stream>>>(d->dw, static_cast<const uint32_t*>(o.ids_dev),
                                                                  d->staging, m);
         }
         DYN_CUDA(cudaGetLastError());
@@ -1058,7 +1076,7 @@ DYN_API dyn_status dyn_upload_states(dyn_world* w, const dyn_body_state_record* 
     // one contiguous copy of the ABI records, then a kernel scatters them into the device layout
     DYN_CUDA(cudaMemcpyAsync(d->staging, states, (size_t)n * sizeof(dyn_body_state_record), cudaMemcpyHostToDevice,
                              d->stream));
-    k_unpack_states<<<blocks_for(std::max(n, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, n);
+    k_unpack_states<<<blocks_for(d, std::max(n, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, n);
     DYN_CUDA(cudaGetLastError());
     return DYN_OK;
 }
@@ -1297,7 +1315,7 @@ DYN_API dyn_status dyn_download_states(dyn_world* w, dyn_body_state_record* out,
     DeviceState* d = w->dev;
     uint32_t rows = d->dw.n;
     if (n < rows) return fail(w, DYN_ERR_INVALID, "dyn_download_states: buffer too small");
-    k_pack_states<<<blocks_for(std::max(rows, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, rows);
+    k_pack_states<<<blocks_for(d, std::max(rows, 1u), 256), 256, 0, d->stream>>>(d->dw, d->staging, rows);
     DYN_CUDA(cudaGetLastError());
     DYN_CUDA(cudaMemcpyAsync(out, d->staging, (size_t)rows * sizeof(dyn_body_state_record), cudaMemcpyDeviceToHost,
                              d->stream));
@@ -1530,9 +1548,34 @@ DYN_API dyn_status dyn_radix_sort(dyn_world* w, uint32_t* major, uint32_t* minor
     if ((size_t)(major_digits + minor_digits) * tiles * 256 > d->lookback_words) {
         return fail(w, DYN_ERR_CAPACITY, "dyn_radix_sort: more keys than the world's sort scratch holds");
     }
+    const uint32_t limit = d->sort_fault_armed ? d->sort_fault_limit : kLookbackSpinLimit;
+    const uint32_t first_ticket = d->sort_fault_armed ? d->sort_fault_skip : 0u;
+    d->sort_fault_armed = false;
     record_sort(d, d->stream, major, minor, payload, d->sort_alt0, minor ? d->sort_alt1 : nullptr,
-                payload ? d->sort_alt2 : nullptr, nullptr, n, n, major_digits, minor_digits);
+                payload ? d->sort_alt2 : nullptr, nullptr, n, n, major_digits, minor_digits, limit, first_ticket);
     DYN_CUDA(cudaGetLastError());
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_debug_sort_fault(dyn_world* w, uint32_t skipped_tiles, uint32_t spin_limit) {
+    if (!w) return static_sort_fault(skipped_tiles, spin_limit);
+    if (spin_limit == 0u || skipped_tiles > 1u) return fail(w, DYN_ERR_INVALID, "dyn_debug_sort_fault: spin_limit must be > 0, skipped_tiles 0 or 1");
+    if (!w->dev) {
+        dyn_status st = ensure_device(w);
+        if (st) return st;
+    }
+    w->dev->sort_fault_armed = true;
+    w->dev->sort_fault_skip = skipped_tiles;
+    w->dev->sort_fault_limit = spin_limit;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_clear_device_status(dyn_world* w) {
+    if (!w) return DYN_ERR_INVALID;
+    if (!w->dev) return DYN_OK;
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+    DYN_CUDA(cudaMemsetAsync(w->dev->dw.ctl + CTL_STATUS, 0, 4, w->dev->stream));
+    DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
     return DYN_OK;
 }
 

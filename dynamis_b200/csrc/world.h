@@ -109,4 +109,6 @@ dyn_status rebuild_joints(dyn_world* w);
 dyn_status sync_spawn_states(dyn_world* w);
 std::vector<dyn_shape_source_record> shape_sources(const dyn_world* w, std::vector<float>* vertices_xyzw);
 void destroy_device(dyn_world* w);
+// Arms the next dyn_radix_sort_static call with a fault (static_sort.cu; dyn_debug_sort_fault).
+dyn_status static_sort_fault(uint32_t skipped_tiles, uint32_t spin_limit);
 }  // namespace dyn

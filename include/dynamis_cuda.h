@@ -289,6 +289,29 @@ DYN_API dyn_status dyn_joint_plan(const dyn_world* world, uint32_t* rows, uint32
 #define DYN_STATIC_SORT_MAX_KEYS 262144u
 DYN_API dyn_status dyn_radix_sort_static(uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_t n,
                                          uint32_t major_digits, uint32_t minor_digits, void* cuda_stream);
+/* No counterpart in the reference. The status word of the latest dyn_radix_sort_static call on the
+ * current device, read after cuda_stream's work: *out = 0 and DYN_OK when every look-back wait
+ * completed; otherwise the DYN_STATUS_* bits (DYN_STATUS_LOOKBACK_TIMEOUT: a wait ran out and the
+ * output is not sorted) and DYN_ERR_DEVICE_STATUS. The next dyn_radix_sort_static call clears it.
+ * Allocates nothing. */
+DYN_API dyn_status dyn_radix_sort_static_status(void* cuda_stream, uint32_t* out);
+
+/* Device status bits (dyn_device_status, dyn_radix_sort_static_status). */
+#define DYN_STATUS_LOOKBACK_TIMEOUT 1u   /* a sort or scan look-back wait ran out of polls */
+#define DYN_STATUS_ISLAND_HOOKS 2u
+
+/* Clears the world's sticky device status word (dyn_sync keeps reporting it until this call or a
+ * new scene upload). Synchronises the world's stream. No counterpart in the reference, which has
+ * no device status word. */
+DYN_API dyn_status dyn_clear_device_status(dyn_world* world);
+
+/* Test hook, no counterpart in the reference: the next dyn_radix_sort on `world` (world NULL: the
+ * next dyn_radix_sort_static call) starts every digit pass's tile tickets at skipped_tiles (0 or 1;
+ * with 1 the first tile never runs, so the look-back words the other tiles wait on are never
+ * published) and gives each look-back wait at most spin_limit polls. Every wait then ends within
+ * the limit with DYN_STATUS_LOOKBACK_TIMEOUT set and the output unsorted; every write stays inside
+ * the caller's n keys. One call only; later sorts use the normal limit (2^22 polls). */
+DYN_API dyn_status dyn_debug_sort_fault(dyn_world* world, uint32_t skipped_tiles, uint32_t spin_limit);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -3,6 +3,8 @@
 Restates the behaviours crates/dynamis-sort/tests/gpu.rs pins: a stable sort carrying a payload,
 two-word keys, and lengths around the tile boundaries.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -118,3 +120,32 @@ def test_known_answers_of_the_reference_sort_tests(world):
 
     assert digest(smaj) == wide["sorted_major_sha256"] and digest(smin) == wide["sorted_minor_sha256"]
     assert digest(pay) == wide["payload_sha256"]
+
+
+def test_a_lookback_wait_that_runs_out_is_reported_and_cleared(world):
+    """The bounded look-back wait, made to run out on purpose: the first tile of every digit pass is
+    never run (its ticket is skipped), so the later tiles poll for a word nothing writes until their
+    limit of 1,000 polls is spent. Every write stays within the n keys. dyn_sync must then report
+    DYN_ERR_DEVICE_STATUS with the timeout bit, and after the status is cleared a normal sort and a
+    normal step succeed."""
+    from dynamis_b200._native import DynamisError
+
+    rng = np.random.default_rng(5)
+    n = 5 * 2048 + 17  # six tiles: five of them wait on the missing first one
+    keys = rng.integers(0, 1 << 30, size=n, dtype=np.uint32)
+    check(lib.dyn_debug_sort_fault(world._h, 1, 1000), world._h)
+    tm = torch.from_numpy(keys.view(np.int32)).to("cuda:0")
+    torch.cuda.synchronize()
+    check(lib.dyn_radix_sort(world._h, tm.data_ptr(), None, None, n, 4, 0), world._h)
+    assert lib.dyn_sync(world._h) == 5  # DYN_ERR_DEVICE_STATUS
+    status = ctypes.c_uint32(0)
+    check(lib.dyn_device_status(world._h, ctypes.byref(status)), world._h)
+    assert status.value & 1  # DYN_STATUS_LOOKBACK_TIMEOUT
+    with pytest.raises(DynamisError):
+        world.wait()
+    check(lib.dyn_clear_device_status(world._h), world._h)
+    world.wait()
+    got = gpu_sort(world, keys, None, None, 4, 0)[0]
+    assert np.array_equal(got, np.sort(keys))
+    world.step(1 / 60)
+    world.wait()

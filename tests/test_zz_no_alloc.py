@@ -87,3 +87,51 @@ def test_requests_above_the_capacity_are_refused():
     keys = torch.zeros(MAX_KEYS + 1, dtype=torch.int32, device="cuda:0")
     status = lib.dyn_radix_sort_static(keys.data_ptr(), None, None, MAX_KEYS + 1, 4, 0, None)
     assert status == 2  # DYN_ERR_CAPACITY
+
+
+@pytest.mark.parametrize("with_minor,with_payload,major_digits,minor_digits", [
+    (True, False, 2, 2),    # two words, no payload
+    (False, False, 3, 0),   # one word, no payload, odd pass count
+    (True, True, 0, 3),     # minor digits only (the major word rides along), odd pass count
+    (True, False, 0, 2),    # minor digits only, no payload
+])
+def test_every_kernel_variant_matches_the_allocating_sort(world, with_minor, with_payload, major_digits, minor_digits):
+    rng = np.random.default_rng(17 + 4 * major_digits + minor_digits)
+    n = 40961
+    major = rng.integers(0, 1 << 24, size=n, dtype=np.uint32)
+    minor = rng.integers(0, 1 << 24, size=n, dtype=np.uint32) if with_minor else None
+    payload = np.arange(n, dtype=np.uint32)[::-1].copy() if with_payload else None
+    want = sort_with_world(world, major, minor, payload, major_digits, minor_digits)
+    got = sort_static(major, minor, payload, major_digits, minor_digits)
+    for w_, g_ in zip(want, got):
+        assert (w_ is None and g_ is None) or np.array_equal(w_, g_)
+    mask_major = (1 << (8 * major_digits)) - 1
+    mask_minor = (1 << (8 * minor_digits)) - 1
+    keys = [minor & mask_minor] if with_minor else []
+    order = np.lexsort(keys + [major & mask_major])  # stable on the sorted digits only
+    assert np.array_equal(got[0], major[order])
+    if with_minor:
+        assert np.array_equal(got[1], minor[order])
+    if with_payload:
+        assert np.array_equal(got[2], payload[order])
+
+
+def test_the_status_of_a_call_is_readable_after_it():
+    """A look-back wait made to run out (the first tile's ticket skipped, 1,000 polls) is reported by
+    dyn_radix_sort_static_status; the next call clears it."""
+    import ctypes
+
+    rng = np.random.default_rng(23)
+    n = 4 * 2048 + 5
+    keys = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    stream = torch.cuda.current_stream()
+    status = ctypes.c_uint32(7)
+    sort_static(keys, None, None, 4, 0)
+    assert lib.dyn_radix_sort_static_status(stream.cuda_stream, ctypes.byref(status)) == 0 and status.value == 0
+    assert lib.dyn_debug_sort_fault(None, 1, 1000) == 0
+    sort_static(keys, None, None, 4, 0)
+    assert lib.dyn_radix_sort_static_status(stream.cuda_stream, ctypes.byref(status)) == 5  # DYN_ERR_DEVICE_STATUS
+    assert status.value & 1  # DYN_STATUS_LOOKBACK_TIMEOUT
+    got = sort_static(keys, None, None, 4, 0)[0]
+    assert lib.dyn_radix_sort_static_status(stream.cuda_stream, ctypes.byref(status)) == 0 and status.value == 0
+    assert np.array_equal(got, np.sort(keys))
