@@ -335,6 +335,57 @@ def batched_worlds(worlds: int = 4096, seed: int = 4) -> Scene:
     return batch(batched_world_parts(worlds, seed))
 
 
+def tower_world(seed: int, levels: int = 8, footprint: int = 4, distance: float = 4.0, box_mass: float = 1.0,
+                friction: float = 0.5) -> Scene:
+    """An `levels`-high tower of unit boxes (half-extent 0.5 m) on a `footprint` x `footprint` base,
+    standing on a ground plane, and a sphere of radius 0.5 m resting on the ground `distance` metres
+    from the tower's axis, on a heading drawn from U(-0.2, 0.2) rad about -x. Every collider has the
+    given friction; boxes and sphere the given mass. The sphere is the last body before the plane."""
+    rng = np.random.default_rng(seed)
+    n = levels * footprint * footprint
+    i, k, j = np.meshgrid(np.arange(footprint), np.arange(footprint), np.arange(levels), indexing="ij")
+    pos = np.stack([i.ravel() - (footprint - 1) / 2, 0.5 + j.ravel(), k.ravel() - (footprint - 1) / 2], axis=1)
+    order = np.lexsort((pos[:, 2], pos[:, 0], pos[:, 1]))  # level by level
+    bodies = R.body_defaults(n + 1)
+    bodies["position"][:n] = pos[order].astype(np.float32)
+    heading = rng.uniform(-0.2, 0.2)
+    bodies["position"][n] = (-distance * np.cos(heading), 0.5, -distance * np.sin(heading))
+    bodies["mass"] = box_mass
+    bodies["collider_first"] = np.arange(n + 1)
+    colliders = R.collider_defaults(n + 1)
+    colliders["shape"][:n] = R.SHAPE_CUBOID
+    colliders["half_extents"][:n] = 0.5
+    colliders["shape"][n] = R.SHAPE_SPHERE
+    colliders["radius"][n] = 0.5
+    colliders["friction"] = friction
+    colliders["restitution"] = 0.0
+    bodies, colliders = _ground(bodies, colliders, 0.0, friction, 0.0)
+    return Scene(bodies, colliders, [], f"tower_{n}")
+
+
+def sphere_launch(scene_seed: int, speed_range=(3.0, 8.0)) -> tuple:
+    """The sphere's launch of tower_world(scene_seed): a speed drawn from U(3, 8) m/s along the
+    heading from the sphere to the tower's axis."""
+    rng = np.random.default_rng(scene_seed + 7919)
+    speed = rng.uniform(*speed_range)
+    return speed
+
+
+def differentiable_towers(worlds: int = 256, seed: int = 5, levels: int = 8, footprint: int = 4) -> Scene:
+    """`worlds` tower worlds (tower_world) as one batch: per-body masses drawn from U(0.5, 2) kg and a
+    per-world friction from U(0.3, 0.8), every collider of a world (its plane included) at the
+    world's friction."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for w in range(worlds):
+        part = tower_world(seed * 1000003 + w, levels, footprint, friction=float(rng.uniform(0.3, 0.8)))
+        part.bodies["mass"][:-1] = rng.uniform(0.5, 2.0, len(part.bodies) - 1).astype(np.float32)
+        parts.append(part)
+    scene = batch(parts)
+    scene.name = f"differentiable_towers_{worlds}"
+    return scene
+
+
 WORKLOADS = {
     "falling_boxes_1000": lambda: falling_boxes(seed=0),
     "mixed_pile_32768": lambda: mixed_pile(side=32, seed=1),

@@ -14,7 +14,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 OUT = HERE / "_build"
 LIBRARY = OUT / "liboracle.so"
-SOURCES = [HERE / "oracle.cpp"]
+SOURCES = [HERE / "oracle.cpp", HERE / "adjoint64.cpp"]
 HEADERS = [HERE / "oracle_math.h", HERE / "oracle_geom.h", ROOT / "include" / "dynamis_abi.h"]
 
 

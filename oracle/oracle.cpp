@@ -205,6 +205,11 @@ struct OracleWorld {
     std::vector<Entry> entries;
     std::vector<uint32_t> pair_major, pair_minor;
     std::vector<dyn_contact_record> contacts, archive;
+    // the contacts as the substeps receive them (after the relay of accumulated impulses and the
+    // target speeds), and for each of their points the archived point it was relayed from
+    // (4 x held contact + held point, or -1): the frozen contact set of a differentiable step
+    std::vector<dyn_contact_record> solve_contacts;
+    std::vector<int32_t> relay_source;
     std::vector<uint32_t> contact_matched;
     std::vector<uint32_t> island_parents, island_state;
     std::vector<uint32_t> wake_flags, body_activity, body_motion;
@@ -786,7 +791,8 @@ float contact_tangent_impulse(const dyn_contact_record& c) {
     }
     return total;
 }
-dyn_contact_record contact_relay_impulses(const dyn_contact_record& current, const dyn_contact_record& held) {
+dyn_contact_record contact_relay_impulses(const dyn_contact_record& current, const dyn_contact_record& held,
+                                          int32_t* source = nullptr, int32_t held_index = 0) {
     dyn_contact_record relayed = current;
     bool taken[4] = {false, false, false, false};
     for (uint32_t pi = 0; pi < current.point_count; ++pi) {
@@ -805,6 +811,7 @@ dyn_contact_record contact_relay_impulses(const dyn_contact_record& current, con
         }
         if (picked == DYN_NO_SLOT) continue;
         taken[picked] = true;
+        if (source) source[pi] = 4 * held_index + (int32_t)picked;
         relayed.points[pi].accumulated_normal = held.points[picked].accumulated_normal;
         relayed.points[pi].accumulated_tangent_1 = held.points[picked].accumulated_tangent_1;
         relayed.points[pi].accumulated_tangent_2 = held.points[picked].accumulated_tangent_2;
@@ -821,7 +828,9 @@ uint32_t resolve_row(const OracleWorld& w, uint32_t id, uint32_t generation) {
 // contact_relay.wgsl:34-71 and contact_begin.wgsl:41-71 (event publication left out)
 void relay_contacts(OracleWorld& w) {
     uint32_t count = (uint32_t)w.contacts.size();
-    for (const dyn_contact_record& held : w.archive) {
+    w.relay_source.assign(4 * (size_t)count, -1);
+    for (size_t held_index = 0; held_index < w.archive.size(); ++held_index) {
+        const dyn_contact_record& held = w.archive[held_index];
         uint32_t fr = resolve_row(w, held.first_body_id, held.first_generation);
         uint32_t sr = resolve_row(w, held.second_body_id, held.second_generation);
         if (fr == DYN_NO_BODY || sr == DYN_NO_BODY) continue;
@@ -840,7 +849,7 @@ void relay_contacts(OracleWorld& w) {
         if (!contact_same_pair(held, current)) continue;
         if ((held.events & DYN_CONTACT_ANNOUNCED) == 0u) continue;
         w.contact_matched[lo] = 1;
-        dyn_contact_record relayed = contact_relay_impulses(current, held);
+        dyn_contact_record relayed = contact_relay_impulses(current, held, &w.relay_source[4 * (size_t)lo], (int32_t)held_index);
         relayed.carried_normal = contact_normal_impulse(relayed);
         relayed.carried_tangent = contact_tangent_impulse(relayed);
         relayed.events |= DYN_CONTACT_ANNOUNCED;
@@ -1767,6 +1776,7 @@ void orc_step(OracleWorld* w, float dt) {
     build_islands(*w);
     wake_and_live(*w);
     solver_prepare(*w);
+    w->solve_contacts = w->contacts;
     solve_substeps(*w);
     sleep(*w);
     w->archive = w->contacts;  // commit: contact_archive.wgsl + archive_count_sync.wgsl
@@ -1811,6 +1821,16 @@ uint32_t orc_pairs(const OracleWorld* w, uint32_t* major, uint32_t* minor) {
 uint32_t orc_contacts(const OracleWorld* w, dyn_contact_record* out) {
     if (out) std::memcpy(out, w->contacts.data(), w->contacts.size() * sizeof(dyn_contact_record));
     return (uint32_t)w->contacts.size();
+}
+// The last step's frozen contact set: the contacts as its substeps received them (accumulated
+// impulses after the relay), their target speeds (4 per contact) and relay sources (4 per contact:
+// 4 x archived contact + archived point, -1 when not relayed). Returns the contact count.
+uint32_t orc_solve_contacts(const OracleWorld* w, dyn_contact_record* out, float* targets, int32_t* sources) {
+    const size_t c = w->solve_contacts.size();
+    if (out) std::copy(w->solve_contacts.begin(), w->solve_contacts.end(), out);
+    if (targets) std::copy(w->target_speeds.begin(), w->target_speeds.begin() + 4 * c, targets);
+    if (sources) std::copy(w->relay_source.begin(), w->relay_source.begin() + 4 * c, sources);
+    return (uint32_t)c;
 }
 uint32_t orc_islands(const OracleWorld* w, uint32_t* out) {
     if (out) std::memcpy(out, w->island_parents.data(), w->island_parents.size() * 4);
