@@ -58,6 +58,14 @@ SIGNATURES = {
     "dyn_radix_sort_static_status": (I32, [P, PU32]),
     "dyn_clear_device_status": (I32, [P]),
     "dyn_debug_sort_fault": (I32, [P, U32, U32]),
+    "dyn_tape_begin": (I32, [P, U32]),
+    "dyn_tape_end": (I32, [P]),
+    "dyn_tape_steps": (I32, [P, PU32, PU32]),
+    "dyn_step_backward": (I32, [P, P, P, U32]),
+    "dyn_backward": (I32, [P, P, P, U32, U32]),
+    "dyn_param_grads": (I32, [P, P, P, U32, P, U32]),
+    "dyn_set_mass_properties": (I32, [P, P, P, U32]),
+    "dyn_set_friction": (I32, [P, P, U32]),
     "dyn_set_body_worlds": (I32, [P, P, U32]),
     "dyn_edit_bodies": (I32, [P, P, P, U32]),
     "dyn_remove_bodies": (I32, [P, P, U32]),

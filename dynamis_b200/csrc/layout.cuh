@@ -178,6 +178,10 @@ struct DeviceWorld {
     // counters (reference slots) and control words
     uint32_t* counters;
     uint32_t* ctl;
+    // a taped step (differentiation): where k_relay records each point's relay source
+    // ([slot][4 c_cap], the slot read from *tape_slot); null outside taped steps
+    uint32_t* tape_relay;
+    const uint32_t* tape_slot;
 };
 
 }  // namespace dyn

@@ -1191,6 +1191,7 @@ __global__ void k_relay(DeviceWorld w) {
             float4 nacc = cacc;
             if (picked != DYN_NO_SLOT) {
                 taken[picked] = true;
+                if (w.tape_relay) w.tape_relay[(size_t)(*w.tape_slot) * 4u * cap + co] = picked * cap + h;
                 float4 hacc = w.arc.acc[(size_t)picked * cap + h];
                 nacc = make_float4(hacc.x, hacc.y, hacc.z, cacc.w);
                 w.cur.acc[co] = nacc;

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "joints.cuh"
 #include "step.cuh"
 #include "world.h"
@@ -41,6 +42,35 @@ static const char* kStageNames[ST_COUNT] = {"begin",       "aabb",     "entries"
                                             "narrowphase", "compact",  "identity",       "islands",
                                             "wake_live",   "solver_prepare", "integrate", "warm_start", "velocity",
                                             "advance",     "position", "sleep"};
+
+// A recorded trajectory for the adjoint (dyn_tape_begin ... dyn_tape_end): checkpoints on the
+// device, the taped segment and the gradient buffers.
+struct Checkpoint {
+    std::vector<void*> bufs;  // device copies, in the order save_checkpoint lists them
+    uint32_t parity = 0;
+};
+struct TapeHost {
+    bool active = false;
+    uint32_t interval = 10;
+    uint32_t recorded = 0;  // steps recorded since dyn_tape_begin
+    uint32_t reversed = 0;  // of those, the last ones already reversed
+    float dt = 0.0f;        // every recorded step's timestep
+    std::vector<Checkpoint> checkpoints;  // checkpoint j: the world before recorded step j * interval
+    Checkpoint end;                       // the world after the last recorded step (kept from the first backward on)
+    bool have_end = false;
+    std::vector<std::vector<uint32_t>> edit_ids;  // each recorded step's queued edits, replayed with it
+    std::vector<std::vector<dyn_body_edit_record>> edits;
+    int32_t segment = -1;  // the segment whose steps the tape slots hold
+    TapeView view{};
+    std::vector<void*> tape_allocs;
+    AdjView adj{};
+    std::vector<void*> adj_allocs;
+    dyn_body_grad* grad_staging = nullptr;  // [n_cap] ABI gradient records
+    uint32_t* patch_rows = nullptr;         // [n_cap] rows and masks of a step's PATCH edits
+    uint32_t* patch_masks = nullptr;
+    cudaGraphExec_t taped[2] = {nullptr, nullptr};
+    cudaGraphExec_t back = nullptr;
+};
 
 struct DeviceState {
     cudaStream_t own_stream = nullptr;
@@ -100,6 +130,7 @@ struct DeviceState {
     std::vector<cudaEvent_t> events;
     std::vector<uint32_t> event_stage;
     float stage_ms[ST_COUNT] = {0};
+    TapeHost tape;
 };
 
 namespace {
@@ -154,6 +185,12 @@ void release_graphs(DeviceState* d) {
         if (e) cudaGraphExecDestroy(e);
         e = nullptr;
     }
+    for (auto& e : d->tape.taped) {
+        if (e) cudaGraphExecDestroy(e);
+        e = nullptr;
+    }
+    if (d->tape.back) cudaGraphExecDestroy(d->tape.back);
+    d->tape.back = nullptr;
     d->graph_dt = -1.0f;
 }
 
@@ -593,11 +630,17 @@ struct Marker {
     }
 };
 
-// Issues one step's kernels on `s`. parity selects which contact set is current.
-void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
+// Issues one step's kernels on `s`. parity selects which contact set is current. With a tape the
+// step also snapshots what its adjoint needs into the tape's current slot (adjoint.cuh) and runs
+// the position passes with their separate apply, which k_position_fused matches bit for bit.
+void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, const TapeView* tape = nullptr) {
     DeviceState* d = w->dev;
     DeviceWorld dw = d->dw;
     if (parity) std::swap(dw.cur, dw.arc);
+    if (tape) {
+        dw.tape_relay = tape->relay;
+        dw.tape_slot = tape->slot;
+    }
     const dyn_step_params p = d->params;
     Marker mark{d, s, timed};
     const uint32_t N = std::max(dw.n, 1u), K = std::max(dw.k, 1u), ND = std::max(dw.nd, 1u);
@@ -676,6 +719,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     record_scan(d, side, dw.row_flag, dw.row_offset, nullptr, std::max(dw.n, 1u), N, dw.ctl + CTL_SOLVER_ROWS);
     k_solver_row_list<<<blocks_for(d, N, 256), 256, 0, side>>>(dw);
     mark(ST_IDENTITY);
+    if (tape) k_tape_clear_relay<<<blocks_for(d, 4 * C, 256), 256, 0, s>>>(*tape);
     k_relay<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
     k_contact_begin<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
     mark(ST_ISLANDS);
@@ -688,8 +732,10 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     mark(ST_WAKE_LIVE);
     k_wake_live<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     join(2, side);
+    if (tape) k_tape_contacts<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, *tape);
     for (uint32_t sub = 0; sub < p.substeps; ++sub) {
         mark(ST_INTEGRATE);
+        if (tape) k_tape_hot<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, *tape, sub);
         k_integrate<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
         k_solve_prepare<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
         if (sub == 0) {
@@ -701,13 +747,20 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
         mark(ST_VELOCITY);
         for (uint32_t it = 0; it < p.solve_iterations; ++it) {
             if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 32, 0, s>>>(dw, p);
+            if (tape) k_tape_iteration<<<blocks_for(d, std::max(N, C), 256), 256, 0, s>>>(dw, *tape, sub, it);
             k_solve<<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p);
             k_vapply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_ADVANCE);
         k_advance<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
         mark(ST_POSITION);
-        if (joint_blocks == 0u) {
+        if (tape) {
+            for (uint32_t it = 0; it < p.position_iterations; ++it) {
+                k_position<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
+                k_tape_position<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, *tape, sub, it);
+                k_papply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
+            }
+        } else if (joint_blocks == 0u) {
             // each iteration applies the one before it; one apply after the last
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 if (it == 0u) {
@@ -727,6 +780,10 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed) {
     }
     mark(ST_SLEEP);
     k_sleep<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw, p);
+    if (tape) {
+        k_tape_hot<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, *tape, p.substeps);
+        k_tape_advance<<<1, 32, 0, s>>>(*tape);
+    }
     mark(ST_COUNT);
 }
 
@@ -1150,8 +1207,11 @@ DYN_API dyn_status dyn_stream_capacity(const dyn_world* w, uint32_t* pairs, uint
     return DYN_OK;
 }
 
-DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
-    if (!w) return DYN_ERR_INVALID;
+}  // extern "C"
+
+// One step on the world's stream: the step graph, or with `taped` the taped graph that also
+// snapshots the step into the tape's current slot (a segment replayed for dyn_step_backward).
+static dyn_status step_once(dyn_world* w, float dt, bool taped) {
     dyn_status st = prepare_step(w, dt);
     if (st) return st;
     DeviceState* d = w->dev;
@@ -1160,18 +1220,20 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
     if (d->inflight_used[slot]) DYN_CUDA(cudaEventSynchronize(d->inflight[slot]));
     if ((st = widen_pair_stream(w))) return st;
     uint32_t parity = d->parity;
+    const TapeView* tape = taped ? &d->tape.view : nullptr;
     if (w->timing) {
         for (cudaEvent_t e : d->events) cudaEventDestroy(e);
         d->events.clear();
         d->event_stage.clear();
-        record_step(w, d->stream, parity, true);
+        record_step(w, d->stream, parity, true, tape);
         DYN_CUDA(cudaGetLastError());
     } else {
-        if (!d->exec[parity]) {
+        cudaGraphExec_t* exec = taped ? &d->tape.taped[parity] : &d->exec[parity];
+        if (!*exec) {
             cudaGraph_t graph = nullptr;
             cudaStream_t cap = d->own_stream;
             DYN_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-            record_step(w, cap, parity, false);
+            record_step(w, cap, parity, false, tape);
             cudaError_t e = cudaStreamEndCapture(cap, &graph);
             if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
             size_t nodes = 0;
@@ -1183,12 +1245,12 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
                 cudaGraphNodeType type;
                 if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernels;
             }
-            d->graph_kernels = kernels;
-            e = cudaGraphInstantiate(&d->exec[parity], graph, 0);
+            if (!taped) d->graph_kernels = kernels;
+            e = cudaGraphInstantiate(exec, graph, 0);
             cudaGraphDestroy(graph);
             if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         }
-        DYN_CUDA(cudaGraphLaunch(d->exec[parity], d->stream));
+        DYN_CUDA(cudaGraphLaunch(*exec, d->stream));
     }
     DYN_CUDA(cudaEventRecord(d->inflight[slot], d->stream));
     d->inflight_used[slot] = true;
@@ -1196,8 +1258,497 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
     d->last_parity = parity;
     d->parity ^= 1u;
     d->stepped = true;
+    return DYN_OK;
+}
+
+// ---- differentiation: checkpoints, the taped segment, the reverse graph ----
+// What a step reads that an earlier step wrote: the body rows and cold body fields, the contact set
+// the next step archives from (which of the two sets that is follows the parity), the counters and
+// control words.
+struct CheckpointPart {
+    void* ptr;
+    size_t bytes;
+};
+static std::vector<CheckpointPart> checkpoint_parts(DeviceState* d) {
+    DeviceWorld& dw = d->dw;
+    const size_t N = d->n_cap, C = d->c_cap;
+    ContactSet& arc = d->parity == 0u ? dw.arc : dw.cur;
+    return {{dw.hot, N * sizeof(BodyHot)},        {dw.prev_pos, N * sizeof(float4)}, {dw.prev_rot, N * sizeof(float4)},
+            {dw.force, N * sizeof(float4)},       {dw.torque, N * sizeof(float4)},   {dw.sleep_timer, N * sizeof(float)},
+            {dw.wake_flags, N * sizeof(uint32_t)}, {dw.counters, 64 * sizeof(uint32_t)}, {dw.ctl, CTL_COUNT * sizeof(uint32_t)},
+            {arc.normal, C * sizeof(float4)},     {arc.rows, C * sizeof(uint4)},     {arc.mat, C * sizeof(float4)},
+            {arc.ids, C * sizeof(uint4)},         {arc.ids2, C * sizeof(uint4)},     {arc.extra, C * sizeof(float4)},
+            {arc.la, 4 * C * sizeof(float4)},     {arc.lb, 4 * C * sizeof(float4)},  {arc.acc, 4 * C * sizeof(float4)},
+            {arc.pos, 4 * C * sizeof(float4)}};
+}
+static void free_checkpoint(Checkpoint* c) {
+    for (void* p : c->bufs) cudaFree(p);
+    c->bufs.clear();
+}
+static dyn_status save_checkpoint(dyn_world* w, Checkpoint* c) {
+    DeviceState* d = w->dev;
+    free_checkpoint(c);
+    for (const CheckpointPart& part : checkpoint_parts(d)) {
+        void* p = nullptr;
+        DYN_CUDA(cudaMalloc(&p, part.bytes));
+        c->bufs.push_back(p);
+        DYN_CUDA(cudaMemcpyAsync(p, part.ptr, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
+    }
+    c->parity = d->parity;
+    return DYN_OK;
+}
+static dyn_status restore_checkpoint(dyn_world* w, const Checkpoint& c) {
+    DeviceState* d = w->dev;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    d->parity = c.parity;  // before listing the parts: the archived set follows the parity
+    std::vector<CheckpointPart> parts = checkpoint_parts(d);
+    for (size_t i = 0; i < parts.size() && i < c.bufs.size(); ++i)
+        DYN_CUDA(cudaMemcpyAsync(parts[i].ptr, c.bufs[i], parts[i].bytes, cudaMemcpyDeviceToDevice, d->stream));
+    return DYN_OK;
+}
+static void free_tape_buffers(TapeHost& t) {
+    for (void* p : t.tape_allocs) cudaFree(p);
+    t.tape_allocs.clear();
+    t.view = TapeView{};
+    t.segment = -1;
+}
+static void free_adjoint(TapeHost& t) {
+    for (void* p : t.adj_allocs) cudaFree(p);
+    t.adj_allocs.clear();
+    t.adj = AdjView{};
+    t.grad_staging = nullptr;
+    t.patch_rows = t.patch_masks = nullptr;
+}
+static void release_tape(DeviceState* d) {
+    TapeHost& t = d->tape;
+    for (auto& e : t.taped) {
+        if (e) cudaGraphExecDestroy(e);
+        e = nullptr;
+    }
+    if (t.back) cudaGraphExecDestroy(t.back);
+    t.back = nullptr;
+    for (Checkpoint& c : t.checkpoints) free_checkpoint(&c);
+    t.checkpoints.clear();
+    free_checkpoint(&t.end);
+    t.have_end = false;
+    free_tape_buffers(t);
+    free_adjoint(t);
+    t.edit_ids.clear();
+    t.edits.clear();
+    t.active = false;
+    t.recorded = t.reversed = 0;
+}
+template <typename T>
+static dyn_status tape_alloc(dyn_world* w, std::vector<void*>& list, T** out, size_t count) {
+    void* p = nullptr;
+    DYN_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    DYN_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), w->dev->stream));
+    list.push_back(p);
+    *out = static_cast<T*>(p);
+    return DYN_OK;
+}
+static dyn_status alloc_tape_buffers(dyn_world* w) {
+    DeviceState* d = w->dev;
+    TapeHost& t = d->tape;
+    if (!t.tape_allocs.empty()) return DYN_OK;
+    const dyn_step_params& p = d->params;
+    TapeView& v = t.view;
+    v.steps = t.interval;
+    v.substeps = p.substeps;
+    v.iterations = p.solve_iterations;
+    v.piterations = p.position_iterations;
+    v.n = d->n_cap;
+    v.c = d->c_cap;
+    const size_t S = v.steps, N = v.n, C = v.c, K = v.substeps;
+    dyn_status st;
+#define TA(field, count) if ((st = tape_alloc(w, t.tape_allocs, &v.field, (count)))) return st
+    TA(slot, 1);
+    TA(counts, S);
+    TA(rows, S * C);
+    TA(normal, S * C);
+    TA(mat, S * C);
+    TA(ids, S * C);
+    TA(extra, S * C);
+    TA(la, S * 4 * C);
+    TA(lb, S * 4 * C);
+    TA(pos, S * 4 * C);
+    TA(relay, S * 4 * C);
+    TA(acc, S * K * v.iterations * 4 * C);
+    TA(hot, S * (K + 1) * N);
+    TA(vel, S * K * v.iterations * 2 * N);
+    TA(res, S * K * v.piterations * N);
+    TA(cnt, S * K * v.piterations * N);
+#undef TA
+    return DYN_OK;
+}
+static dyn_status alloc_adjoint(dyn_world* w) {
+    DeviceState* d = w->dev;
+    TapeHost& t = d->tape;
+    if (!t.adj_allocs.empty()) return DYN_OK;
+    const size_t N = d->n_cap, C = d->c_cap, K = d->k_cap;
+    AdjView& a = t.adj;
+    dyn_status st;
+#define AA(ptr, count) if ((st = tape_alloc(w, t.adj_allocs, &(ptr), (count)))) return st
+    AA(a.gx, N);
+    AA(a.gq, N);
+    AA(a.gv, N);
+    AA(a.gw, N);
+    AA(a.gv_acc, N);
+    AA(a.gw_acc, N);
+    AA(a.gres, N);
+    AA(a.gres_acc, N);
+    AA(a.gsum, N);
+    AA(a.g_im, N);
+    AA(a.g_scale, N);
+    AA(a.g_friction, K);
+    AA(a.gacc[0], 4 * C);
+    AA(a.gacc[1], 4 * C);
+    AA(a.acc_flip, 1);
+    AA(a.g_ra, 4 * C);
+    AA(a.g_rb, 4 * C);
+    AA(a.g_m, 4 * C);
+    AA(a.g_pt, 4 * C);
+    AA(a.g_param, C);
+    AA(a.g_mu, C);
+    AA(t.grad_staging, N);
+    AA(t.patch_rows, N);
+    AA(t.patch_masks, N);
+#undef AA
+    a.status = d->dw.ctl + CTL_STATUS;
+    return DYN_OK;
+}
+
+// The reverse of one step (adjoint.cuh), on `s`.
+static void record_backward_step(dyn_world* w, cudaStream_t s) {
+    DeviceState* d = w->dev;
+    const TapeView& t = d->tape.view;
+    const AdjView& a = d->tape.adj;
+    const dyn_step_params p = d->params;
+    const uint32_t n = std::max(d->dw.n, 1u);
+    const uint32_t C = d->c_cap;
+    const uint32_t rows_grid = blocks_for(d, n, 256), contact_grid = blocks_for(d, C, 128);
+    k_adj_begin<<<1, 32, 0, s>>>(t, a);
+    k_adj_clear<<<blocks_for(d, std::max(4 * C, n), 256), 256, 0, s>>>(t, a, n);
+    for (int32_t k = (int32_t)p.substeps - 1; k >= 0; --k) {
+        const uint32_t P = p.position_iterations;
+        if (P > 0) {
+            k_adj_prow<<<rows_grid, 256, 0, s>>>(t, a, n, (uint32_t)k, P - 1, false, true);
+            for (int32_t it = (int32_t)P - 1; it >= 0; --it) {
+                k_adj_pcontact<<<contact_grid, 128, 0, s>>>(t, a, p, (uint32_t)k, (uint32_t)it);
+                k_adj_prow<<<rows_grid, 256, 0, s>>>(t, a, n, (uint32_t)k, it > 0 ? (uint32_t)(it - 1) : 0u, true, it > 0);
+            }
+        }
+        k_adj_advance<<<rows_grid, 256, 0, s>>>(t, a, n, p, (uint32_t)k);
+        for (int32_t it = (int32_t)p.solve_iterations - 1; it >= 0; --it) {
+            k_adj_solve<<<contact_grid, 128, 0, s>>>(t, a, p, (uint32_t)k, (uint32_t)it);
+            k_adj_vmerge<<<rows_grid, 256, 0, s>>>(a, n);
+        }
+        if (k == 0) k_adj_warm<<<contact_grid, 128, 0, s>>>(t, a);
+        k_adj_prepare<<<contact_grid, 128, 0, s>>>(t, a, (uint32_t)k);
+        k_adj_integrate<<<rows_grid, 256, 0, s>>>(d->dw, t, a, p, (uint32_t)k);
+    }
+    k_adj_start<<<contact_grid, 128, 0, s>>>(d->dw, t, a, p);
+    k_adj_end<<<1, 32, 0, s>>>(a);
+}
+
+// Steps the recorded steps of segment `seg` again from its checkpoint, taped.
+static dyn_status materialize_segment(dyn_world* w, int32_t seg) {
+    DeviceState* d = w->dev;
+    TapeHost& t = d->tape;
+    if (t.segment == seg) return DYN_OK;
+    dyn_status st = alloc_tape_buffers(w);
+    if (st) return st;
+    if ((st = restore_checkpoint(w, t.checkpoints[(size_t)seg]))) return st;
+    DYN_CUDA(cudaMemsetAsync(t.view.slot, 0, sizeof(uint32_t), d->stream));
+    const uint32_t first = (uint32_t)seg * t.interval;
+    const uint32_t last = std::min(t.recorded, first + t.interval);
+    for (uint32_t j = first; j < last; ++j) {
+        w->edit_ids = t.edit_ids[j];
+        w->edits = t.edits[j];
+        if ((st = step_once(w, t.dt, true))) return st;
+    }
+    t.segment = seg;
+    return DYN_OK;
+}
+
+// The rows and PATCH masks of recorded step j's edits, onto the device; returns how many.
+static dyn_status upload_patches(dyn_world* w, uint32_t j, uint32_t* count) {
+    DeviceState* d = w->dev;
+    TapeHost& t = d->tape;
+    std::vector<uint32_t> rows, masks;
+    for (size_t e = 0; e < t.edits[j].size(); ++e) {
+        const uint32_t id = t.edit_ids[j][e];
+        const uint32_t row = id < w->row_of_id.size() ? w->row_of_id[id] : DYN_NO_BODY;
+        if (row == DYN_NO_BODY || row >= d->dw.n) continue;
+        rows.push_back(row);
+        masks.push_back(t.edits[j][e].mask);
+    }
+    *count = (uint32_t)rows.size();
+    if (rows.empty()) return DYN_OK;
+    DYN_CUDA(cudaMemcpyAsync(t.patch_rows, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    DYN_CUDA(cudaMemcpyAsync(t.patch_masks, masks.data(), masks.size() * 4, cudaMemcpyHostToDevice, d->stream));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    return DYN_OK;
+}
+
+static dyn_status backward_steps(dyn_world* w, const dyn_body_grad* grad_in, dyn_body_grad* grad_out, uint32_t n,
+                                 uint32_t steps) {
+    if (!w || !grad_in || !grad_out) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    if (!d || !d->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_step_backward: no tape is recording (dyn_tape_begin)");
+    TapeHost& t = d->tape;
+    if (n != d->dw.n) return fail(w, DYN_ERR_INVALID, "dyn_step_backward: n differs from the world's body rows");
+    if (steps == 0 || steps > t.recorded - t.reversed)
+        return fail(w, DYN_ERR_INVALID, "dyn_step_backward: fewer recorded steps are left to reverse");
+    DYN_CUDA(cudaSetDevice(w->device));
+    dyn_status st;
+    if (!t.have_end) {
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        if ((st = save_checkpoint(w, &t.end))) return st;
+        t.have_end = true;
+    }
+    if ((st = alloc_adjoint(w))) return st;
+    DYN_CUDA(cudaMemcpyAsync(t.grad_staging, grad_in, (size_t)n * sizeof(dyn_body_grad), cudaMemcpyHostToDevice, d->stream));
+    k_grad_unpack<<<blocks_for(d, n, 256), 256, 0, d->stream>>>(t.adj, t.grad_staging, n);
+    DYN_CUDA(cudaGetLastError());
+    for (uint32_t k = 0; k < steps; ++k) {
+        const uint32_t step = t.recorded - t.reversed - 1u;
+        if (k > 0) {
+            // the step after this one replaced some fields by edits: no gradient reaches past them
+            uint32_t m = 0;
+            if ((st = upload_patches(w, step + 1u, &m))) return st;
+            if (m) k_adj_patch<<<blocks_for(d, m, 256), 256, 0, d->stream>>>(t.adj, t.patch_rows, t.patch_masks, m);
+        }
+        const int32_t seg = (int32_t)(step / t.interval);
+        if ((st = materialize_segment(w, seg))) return st;
+        if (!t.back) {
+            alloc_tape_buffers(w);
+            cudaGraph_t graph = nullptr;
+            cudaStream_t cap = d->own_stream;
+            DYN_CUDA(cudaStreamSynchronize(d->stream));
+            DYN_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            record_backward_step(w, cap);
+            cudaError_t e = cudaStreamEndCapture(cap, &graph);
+            if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("backward graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&t.back, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("backward graph instantiate: ") + cudaGetErrorString(e));
+        }
+        DYN_CUDA(cudaGraphLaunch(t.back, d->stream));
+        t.reversed += 1u;
+        if (step % t.interval == 0u) t.segment = -1;  // the segment's slots are all consumed
+    }
+    k_grad_pack<<<blocks_for(d, n, 256), 256, 0, d->stream>>>(t.adj, t.grad_staging, n);
+    DYN_CUDA(cudaGetLastError());
+    DYN_CUDA(cudaMemcpyAsync(grad_out, t.grad_staging, (size_t)n * sizeof(dyn_body_grad), cudaMemcpyDeviceToHost, d->stream));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    return DYN_OK;
+}
+
+extern "C" {
+
+DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
+    if (!w) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    const bool recording = d && d->tape.active;
+    if (recording) {
+        TapeHost& t = d->tape;
+        if (t.reversed > 0) return fail(w, DYN_ERR_INVALID, "dyn_step: the tape is being reversed (dyn_tape_end first)");
+        if (t.recorded > 0 && dt != t.dt) return fail(w, DYN_ERR_INVALID, "dyn_step: every recorded step takes one timestep");
+        for (const dyn_body_edit_record& e : w->edits) {
+            if (e.kind != DYN_EDIT_PATCH) return fail(w, DYN_ERR_INVALID, "dyn_step: only PATCH edits while recording");
+        }
+        if (w->rows_dirty && !w->raw_rows) return fail(w, DYN_ERR_INVALID, "dyn_step: the scene changed while recording");
+        if (t.recorded > 0 && t.recorded % t.interval == 0u) {
+            t.checkpoints.emplace_back();
+            dyn_status st = save_checkpoint(w, &t.checkpoints.back());
+            if (st) return st;
+        }
+        t.edit_ids.push_back(w->edit_ids);
+        t.edits.push_back(w->edits);
+        t.dt = dt;
+    }
+    dyn_status st = step_once(w, dt, false);
+    if (st) return st;
+    if (recording) w->dev->tape.recorded += 1u;
     w->steps_taken += 1;
     if (w->observer.active) return observe_after_step(w);
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_tape_begin(dyn_world* w, uint32_t checkpoint_interval) {
+    if (!w || checkpoint_interval == 0) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: the checkpoint interval must be > 0");
+    if (std::isfinite(w->config.sleep_time)) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: sleeping must be off (sleep_time = inf)");
+    if (!w->joint_descs.empty()) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: constraints are not differentiated");
+    rebuild_rows(w);
+    for (uint32_t i = 0; i < w->dynamic_count && i < w->descs.size(); ++i) {
+        const float* ii = w->descs[i].inverse_inertia;
+        if (w->descs[i].inverse_mass > 0.0f && !(ii[1] == 0.0f && ii[2] == 0.0f && ii[4] == 0.0f && ii[0] == ii[3] && ii[3] == ii[5]))
+            return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: a dynamic body's inverse inertia is not isotropic");
+    }
+    bool fresh = !w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows) || w->scene_dirty;
+    if (fresh) {
+        dyn_status st = upload_scene(w);
+        if (st) return st;
+    }
+    DeviceState* d = w->dev;
+    DYN_CUDA(cudaSetDevice(w->device));
+    release_tape(d);
+    TapeHost& t = d->tape;
+    t.interval = checkpoint_interval;
+    t.active = true;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    t.checkpoints.emplace_back();
+    dyn_status st = save_checkpoint(w, &t.checkpoints.back());
+    if (st) {
+        release_tape(d);
+        return st;
+    }
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_tape_end(dyn_world* w) {
+    if (!w) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    if (!d || !d->tape.active) return DYN_OK;
+    DYN_CUDA(cudaSetDevice(w->device));
+    if (d->tape.have_end) {
+        dyn_status st = restore_checkpoint(w, d->tape.end);
+        if (st) return st;
+    }
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    release_tape(d);
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_tape_steps(const dyn_world* w, uint32_t* recorded, uint32_t* reversed) {
+    if (!w) return DYN_ERR_INVALID;
+    const bool on = w->dev && w->dev->tape.active;
+    if (recorded) *recorded = on ? w->dev->tape.recorded : 0u;
+    if (reversed) *reversed = on ? w->dev->tape.reversed : 0u;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_step_backward(dyn_world* w, const dyn_body_grad* grad_in, dyn_body_grad* grad_out, uint32_t n) {
+    return backward_steps(w, grad_in, grad_out, n, 1u);
+}
+
+DYN_API dyn_status dyn_backward(dyn_world* w, const dyn_body_grad* grad_in, dyn_body_grad* grad_out, uint32_t n, uint32_t steps) {
+    return backward_steps(w, grad_in, grad_out, n, steps);
+}
+
+DYN_API dyn_status dyn_set_mass_properties(dyn_world* w, const float* inverse_mass, const float* inverse_inertia, uint32_t n) {
+    if (!w || !inverse_mass || !inverse_inertia) return fail(w, DYN_ERR_INVALID, "dyn_set_mass_properties: null argument");
+    if (w->dev && w->dev->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_set_mass_properties: a tape is recording");
+    rebuild_rows(w);
+    if (n != w->descs.size()) return fail(w, DYN_ERR_INVALID, "dyn_set_mass_properties: n differs from the body rows");
+    for (uint32_t r = 0; r < n; ++r) {
+        const bool dynamic = r < w->dynamic_count;
+        if (!std::isfinite(inverse_mass[r]) || (dynamic != (inverse_mass[r] > 0.0f)))
+            return fail(w, DYN_ERR_INVALID, "dyn_set_mass_properties: a row would change between dynamic and static");
+        for (int k = 0; k < 6; ++k) {
+            if (!std::isfinite(inverse_inertia[6 * (size_t)r + k]))
+                return fail(w, DYN_ERR_INVALID, "dyn_set_mass_properties: inverse inertia must be finite");
+        }
+    }
+    std::vector<uint32_t> id_of_row(n, DYN_NO_BODY);
+    for (uint32_t id = 0; id < w->row_of_id.size(); ++id) {
+        if (w->row_of_id[id] < n) id_of_row[w->row_of_id[id]] = id;
+    }
+    std::vector<float> inertia(6 * (size_t)n, 0.0f);
+    for (uint32_t r = 0; r < n; ++r) {
+        const float* t = inverse_inertia + 6 * (size_t)r;
+        // the inertia is the inverse of the symmetric tensor (xx, xy, xz, yy, yz, zz); zero stays zero
+        const double a = t[0], b = t[1], c = t[2], d = t[3], e = t[4], f = t[5];
+        const double c00 = d * f - e * e, c01 = c * e - b * f, c02 = b * e - c * d;
+        const double det = a * c00 + b * c01 + c * c02;
+        float* I = &inertia[6 * (size_t)r];
+        if (det != 0.0) {
+            I[0] = (float)(c00 / det);
+            I[1] = (float)(c01 / det);
+            I[2] = (float)(c02 / det);
+            I[3] = (float)((a * f - c * c) / det);
+            I[4] = (float)((b * c - a * e) / det);
+            I[5] = (float)((a * d - b * b) / det);
+        }
+        dyn_body_descriptor_record& rec = w->descs[r];
+        rec.inverse_mass = inverse_mass[r];
+        for (int k = 0; k < 6; ++k) {
+            rec.inverse_inertia[k] = t[k];
+            rec.inertia[k] = I[k];
+        }
+        if (!w->raw_rows && id_of_row[r] < w->spawn_descs.size()) w->spawn_descs[id_of_row[r]] = rec;
+    }
+    DeviceState* d = w->dev;
+    if (d && d->uploaded) {
+        DYN_CUDA(cudaSetDevice(w->device));
+        float *dim = nullptr, *dii = nullptr, *din = nullptr;
+        DYN_CUDA(cudaMalloc(&dim, (size_t)n * 4));
+        DYN_CUDA(cudaMalloc(&dii, (size_t)n * 24));
+        DYN_CUDA(cudaMalloc(&din, (size_t)n * 24));
+        cudaMemcpyAsync(dim, inverse_mass, (size_t)n * 4, cudaMemcpyHostToDevice, d->stream);
+        cudaMemcpyAsync(dii, inverse_inertia, (size_t)n * 24, cudaMemcpyHostToDevice, d->stream);
+        cudaMemcpyAsync(din, inertia.data(), (size_t)n * 24, cudaMemcpyHostToDevice, d->stream);
+        k_set_mass<<<blocks_for(d, n, 256), 256, 0, d->stream>>>(d->dw, dim, dii, din, n);
+        cudaError_t e = cudaStreamSynchronize(d->stream);
+        cudaFree(dim);
+        cudaFree(dii);
+        cudaFree(din);
+        if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("dyn_set_mass_properties: ") + cudaGetErrorString(e));
+    }
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_set_friction(dyn_world* w, const float* friction, uint32_t k) {
+    if (!w || !friction) return fail(w, DYN_ERR_INVALID, "dyn_set_friction: null argument");
+    if (w->dev && w->dev->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_set_friction: a tape is recording");
+    rebuild_rows(w);
+    if (k != w->colliders.size()) return fail(w, DYN_ERR_INVALID, "dyn_set_friction: k differs from the colliders");
+    for (uint32_t c = 0; c < k; ++c) {
+        if (!(friction[c] >= 0.0f) || !std::isfinite(friction[c])) return fail(w, DYN_ERR_INVALID, "dyn_set_friction: friction must be >= 0");
+    }
+    for (uint32_t c = 0; c < k; ++c) w->colliders[c].friction = friction[c];
+    if (!w->raw_rows) {
+        uint32_t c = 0;
+        for (size_t i = 0; i < w->spawn_owner.size() && c < k; ++i) {
+            if (w->removed.size() > w->spawn_owner[i] && w->removed[w->spawn_owner[i]]) continue;
+            w->spawn_colliders[i].friction = friction[c++];
+        }
+    }
+    DeviceState* d = w->dev;
+    if (d && d->uploaded) {
+        DYN_CUDA(cudaSetDevice(w->device));
+        float* df = nullptr;
+        DYN_CUDA(cudaMalloc(&df, (size_t)k * 4));
+        cudaMemcpyAsync(df, friction, (size_t)k * 4, cudaMemcpyHostToDevice, d->stream);
+        k_set_friction<<<blocks_for(d, k, 256), 256, 0, d->stream>>>(d->dw, df, k);
+        cudaError_t e = cudaStreamSynchronize(d->stream);
+        cudaFree(df);
+        if (e != cudaSuccess) return fail(w, DYN_ERR_CUDA, std::string("dyn_set_friction: ") + cudaGetErrorString(e));
+    }
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_param_grads(dyn_world* w, float* inverse_mass, float* inertia_scale, uint32_t n, float* friction,
+                                   uint32_t k) {
+    if (!w) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    const bool have = d && d->tape.active && !d->tape.adj_allocs.empty();
+    if (have) DYN_CUDA(cudaStreamSynchronize(d->stream));
+    const uint32_t rows = have ? d->dw.n : 0u, colliders = have ? d->dw.k : 0u;
+    if (inverse_mass) {
+        std::memset(inverse_mass, 0, (size_t)n * 4);
+        if (have) DYN_CUDA(cudaMemcpy(inverse_mass, d->tape.adj.g_im, (size_t)std::min(n, rows) * 4, cudaMemcpyDeviceToHost));
+    }
+    if (inertia_scale) {
+        std::memset(inertia_scale, 0, (size_t)n * 4);
+        if (have) DYN_CUDA(cudaMemcpy(inertia_scale, d->tape.adj.g_scale, (size_t)std::min(n, rows) * 4, cudaMemcpyDeviceToHost));
+    }
+    if (friction) {
+        std::memset(friction, 0, (size_t)k * 4);
+        if (have) DYN_CUDA(cudaMemcpy(friction, d->tape.adj.g_friction, (size_t)std::min(k, colliders) * 4, cudaMemcpyDeviceToHost));
+    }
     return DYN_OK;
 }
 

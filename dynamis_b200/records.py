@@ -149,6 +149,12 @@ BODY_DESC = np.dtype([
 ])
 
 assert STEP_PARAMS.itemsize == 176 and BODY_STATE.itemsize == 144 and BODY_DESCRIPTOR.itemsize == 128
+# dynamis_cuda.h dyn_body_grad: d loss / d one body row's state (64 bytes)
+BODY_GRAD = _dtype(_fields([
+    ("position", "<f4", 3, 0), ("orientation", "<f4", 4, 16), ("velocity", "<f4", 3, 32),
+    ("angular_velocity", "<f4", 3, 48),
+]), 64)
+
 assert COLLIDER.itemsize == 112 and SHAPE_SOURCE.itemsize == 80 and CONTACT.itemsize == 352
 assert MANIFOLD_POINT.itemsize == 64 and AABB.itemsize == 32
 assert CONSTRAINT_DESCRIPTOR.itemsize == 400 and CONSTRAINT_ROWS.itemsize == 8 and CONSTRAINT_RUNTIME.itemsize == 160

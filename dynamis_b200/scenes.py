@@ -336,19 +336,23 @@ def batched_worlds(worlds: int = 4096, seed: int = 4) -> Scene:
 
 
 def tower_world(seed: int, levels: int = 8, footprint: int = 4, distance: float = 4.0, box_mass: float = 1.0,
-                friction: float = 0.5) -> Scene:
+                friction: float = 0.5, heading: float | None = None, gap: float = 0.0) -> Scene:
     """An `levels`-high tower of unit boxes (half-extent 0.5 m) on a `footprint` x `footprint` base,
     standing on a ground plane, and a sphere of radius 0.5 m resting on the ground `distance` metres
-    from the tower's axis, on a heading drawn from U(-0.2, 0.2) rad about -x. Every collider has the
-    given friction; boxes and sphere the given mass. The sphere is the last body before the plane."""
+    from the tower's axis, on a heading drawn from U(-0.2, 0.2) rad about -x (or the given heading).
+    Every collider has the given friction; boxes and sphere the given mass. Neighbouring columns stand
+    `gap` metres apart (0: face to face). The sphere is the last body before the plane."""
     rng = np.random.default_rng(seed)
     n = levels * footprint * footprint
     i, k, j = np.meshgrid(np.arange(footprint), np.arange(footprint), np.arange(levels), indexing="ij")
-    pos = np.stack([i.ravel() - (footprint - 1) / 2, 0.5 + j.ravel(), k.ravel() - (footprint - 1) / 2], axis=1)
+    pitch = 1.0 + gap
+    pos = np.stack([(i.ravel() - (footprint - 1) / 2) * pitch, 0.5 + j.ravel(), (k.ravel() - (footprint - 1) / 2) * pitch],
+                   axis=1)
     order = np.lexsort((pos[:, 2], pos[:, 0], pos[:, 1]))  # level by level
     bodies = R.body_defaults(n + 1)
     bodies["position"][:n] = pos[order].astype(np.float32)
-    heading = rng.uniform(-0.2, 0.2)
+    drawn = rng.uniform(-0.2, 0.2)
+    heading = drawn if heading is None else heading
     bodies["position"][n] = (-distance * np.cos(heading), 0.5, -distance * np.sin(heading))
     bodies["mass"] = box_mass
     bodies["collider_first"] = np.arange(n + 1)

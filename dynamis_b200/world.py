@@ -318,6 +318,49 @@ class World:
         self._check(lib.dyn_debug_islands(self._h, ptr(out), n.value, None))
         return out
 
+    # ---- differentiation (World::step_backward) ----
+    def set_mass_properties(self, inverse_mass, inverse_inertia) -> None:
+        """Every body row's inverse mass and inverse inertia tensor (rows x 6: xx, xy, xz, yy, yz, zz)."""
+        im = np.ascontiguousarray(inverse_mass, np.float32)
+        ii = np.ascontiguousarray(inverse_inertia, np.float32).reshape(len(im), 6)
+        self._check(lib.dyn_set_mass_properties(self._h, ptr(im), ptr(ii), len(im)))
+
+    def set_friction(self, friction) -> None:
+        """Every collider's friction, in dyn_export_scene's collider order."""
+        f = np.ascontiguousarray(friction, np.float32)
+        self._check(lib.dyn_set_friction(self._h, ptr(f), len(f)))
+
+    def tape_begin(self, checkpoint_interval: int = 10) -> None:
+        """Starts recording a differentiable trajectory (checkpoints every `checkpoint_interval` steps)."""
+        self._check(lib.dyn_tape_begin(self._h, int(checkpoint_interval)))
+
+    def tape_end(self) -> None:
+        """Restores the state after the last recorded step and releases the tape."""
+        self._check(lib.dyn_tape_end(self._h))
+
+    def tape_steps(self) -> tuple:
+        rec, rev = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(lib.dyn_tape_steps(self._h, ctypes.byref(rec), ctypes.byref(rev)))
+        return rec.value, rev.value
+
+    def step_backward(self, grad: np.ndarray, steps: int = 1) -> np.ndarray:
+        """World::step_backward over `steps` recorded steps: `grad` (BODY_GRAD per row) is d loss / d
+        state after the last unreversed step; returns d loss / d state its earliest reversed step's
+        solve started from."""
+        g = np.ascontiguousarray(grad, R.BODY_GRAD)
+        out = np.zeros(len(g), R.BODY_GRAD)
+        self._check(lib.dyn_backward(self._h, ptr(g), ptr(out), len(g), int(steps)))
+        return out
+
+    def param_grads(self) -> dict:
+        """Accumulated d loss / d inverse mass and d loss / d inverse-inertia scale per row, d loss / d
+        friction per collider."""
+        sizes = self.sizes()
+        n, k = sizes["bodies"], sizes["colliders"]
+        im, sc, fr = np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(k, np.float32)
+        self._check(lib.dyn_param_grads(self._h, ptr(im), ptr(sc), n, ptr(fr), k))
+        return {"inverse_mass": im, "inertia_scale": sc, "friction": fr}
+
     # ---- timing ----
     def step_kernel_count(self) -> int:
         """Kernel launches per step (kernel nodes of the captured step graph)."""

@@ -299,6 +299,7 @@ DYN_API dyn_status dyn_radix_sort_static_status(void* cuda_stream, uint32_t* out
 /* Device status bits (dyn_device_status, dyn_radix_sort_static_status). */
 #define DYN_STATUS_LOOKBACK_TIMEOUT 1u   /* a sort or scan look-back wait ran out of polls */
 #define DYN_STATUS_ISLAND_HOOKS 2u
+#define DYN_STATUS_ADJOINT_UNSUPPORTED 4u  /* a reversed step met a contact the adjoint does not cover */
 
 /* Clears the world's sticky device status word (dyn_sync keeps reporting it until this call or a
  * new scene upload). Synchronises the world's stream. No counterpart in the reference, which has
@@ -312,6 +313,61 @@ DYN_API dyn_status dyn_clear_device_status(dyn_world* world);
  * the limit with DYN_STATUS_LOOKBACK_TIMEOUT set and the output unsorted; every write stays inside
  * the caller's n keys. One call only; later sorts use the normal limit (2^22 polls). */
 DYN_API dyn_status dyn_debug_sort_fault(dyn_world* world, uint32_t skipped_tiles, uint32_t spin_limit);
+
+/* ---- differentiation: World::step_backward ----
+ * The adjoint of World::step over the frozen active contact set of each step, replacing the
+ * reference's differentiable rollout of its step (crates/dynamis-world/src/step.rs:34-39 run
+ * forward, the solver passes of crates/dynamis-rigid/src/solver.rs:304-333 reversed). A step
+ * differentiates from the state its substeps start from to the state it ends in: integration,
+ * warm start, the Jacobi contact blocks, advance and position correction, with each step's contact
+ * set (pairs, normals, anchors in the bodies' frames, active clamps) held as the narrowphase found
+ * it and each contact point's depth moving with the bodies to first order. Parameters: every
+ * body's inverse mass and the scale of its inverse inertia tensor, every collider's friction.
+ *
+ * dyn_tape_begin starts a recorded trajectory: it checkpoints the world and every
+ * checkpoint_interval-th later dyn_step checkpoints again (body rows, archived contacts, counters).
+ * dyn_step_backward reverses the last not yet reversed step: it restores the checkpoint of that
+ * step's segment, steps the segment again with its snapshots taped (narrowphase included), and runs
+ * the reverse graph. dyn_tape_end restores the state after the last recorded step and releases the
+ * tape. Requirements (DYN_ERR_INVALID otherwise): sleeping off (config sleep_time = +inf), no
+ * constraints, dynamic bodies with isotropic inverse inertia, while recording only body edits of
+ * kind PATCH and no spawns or removals, one timestep for every recorded step. Contacts with soft
+ * compliance, rolling or spin friction raise DYN_STATUS_ADJOINT_UNSUPPORTED (dyn_sync reports it).
+ * The world's bodies hold replayed states between dyn_step_backward calls. */
+typedef struct dyn_body_grad {
+    float position[3];
+    float _pad0;
+    float orientation[4];      /* x, y, z, w */
+    float velocity[3];
+    float _pad1;
+    float angular_velocity[3];
+    float _pad2;
+} dyn_body_grad;               /* 64 bytes: d loss / d one body row's state */
+
+DYN_API dyn_status dyn_tape_begin(dyn_world* world, uint32_t checkpoint_interval);
+DYN_API dyn_status dyn_tape_end(dyn_world* world);
+DYN_API dyn_status dyn_tape_steps(const dyn_world* world, uint32_t* recorded, uint32_t* reversed);
+/* World::step_backward: grad_in[row] = d loss / d (state after the step), n = body rows; writes
+ * grad_out[row] = d loss / d (state its solve starts from, after the step's queued edits), and
+ * adds the step's parameter gradients to the world's (dyn_param_grads). */
+DYN_API dyn_status dyn_step_backward(dyn_world* world, const dyn_body_grad* grad_in, dyn_body_grad* grad_out, uint32_t n);
+/* `steps` reversed steps in a row on the device (the state gradients stay in HBM between them;
+ * a field a step's PATCH edit replaced passes no gradient to the step before it). */
+DYN_API dyn_status dyn_backward(dyn_world* world, const dyn_body_grad* grad_in, dyn_body_grad* grad_out, uint32_t n,
+                                uint32_t steps);
+/* Parameter gradients accumulated since dyn_tape_begin: per body row d loss / d inverse mass and
+ * d loss / d s at s = 1 for the inverse inertia tensor scaled by s (so for a mass m with inertia
+ * proportional to it, d loss / d m = -(inverse_mass x g_inverse_mass + g_inertia_scale) / m); per
+ * collider d loss / d friction. Any output may be NULL. */
+DYN_API dyn_status dyn_param_grads(dyn_world* world, float* inverse_mass, float* inertia_scale, uint32_t n, float* friction,
+                                   uint32_t k);
+/* Sets body rows' inverse mass and inverse inertia tensor (6 per row: xx, xy, xz, yy, yz, zz; the
+ * inertia is its inverse) and colliders' friction, on the host records and the device. No
+ * counterpart in the reference (its bodies take mass at spawn); the parameters of a differentiable
+ * rollout. Refused while a tape is recording. */
+DYN_API dyn_status dyn_set_mass_properties(dyn_world* world, const float* inverse_mass, const float* inverse_inertia,
+                                           uint32_t n);
+DYN_API dyn_status dyn_set_friction(dyn_world* world, const float* friction, uint32_t k);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -31,9 +31,13 @@ def _lib():
         L.orc_solve_contacts.restype = U32
         L.orc_solve_contacts.argtypes = [P, P, P, P]
         L.adj_forward.restype = ctypes.c_double
-        L.adj_forward.argtypes = [U32, P, P, U32, P, P, P, P, P, P, P, U32, P, P]
+        L.adj_forward.argtypes = [U32, P, P, U32, P, P, P, P, P, P, P, P, P, P, U32, P, P]
         L.adj_directional.restype = None
-        L.adj_directional.argtypes = [U32, P, P, U32, P, P, P, P, P, P, P, U32, P, U32, P, P]
+        L.adj_directional.argtypes = [U32, P, P, U32, P, P, P, P, P, P, P, P, P, P, U32, P, U32, P, P]
+        L.orc_keep_snapshots.argtypes = [P, U32]
+        L.orc_step_snapshots.argtypes = [P, P, P, P, P]
+        L.orc_step_decisions.restype = None
+        L.orc_step_decisions.argtypes = [P, P, P, P, P]
         _bound = True
     return L
 
@@ -61,10 +65,17 @@ class FrozenTrajectory:
         self.start = oracle_world.states() if start is None else start
         self.counts, self.cint, self.cdouble, self.cpoints, self.sources = [], [], [], [], []
         self.contact_friction = []
+        self.decisions = []
+        self.follow_decisions = False  # True: branches as the recorded FP32 run took them
+        self.along_record = False      # True: derivatives along the recorded FP32 run's values (with its branches)
         descs = scene["descs"]
         dyn_rows = (descs["inverse_mass"] > 0) & ((descs["flags"] & 1) == 0) & (self.start["sleeping"] == 0)
         dyn_rows &= np.arange(self.n) < self.dynamic_count
         self.dynamic = dyn_rows
+        L.orc_keep_snapshots(oracle_world._h, 1)
+        pp = np.atleast_1d(params)
+        K, I, PI = int(pp["substeps"][0]), int(pp["solve_iterations"][0]), int(pp["position_iterations"][0])
+        self.snapshots = []
         for step in range(steps):
             oracle_world.step(dt)
             c = L.orc_solve_contacts(oracle_world._h, None, None, None)
@@ -94,7 +105,24 @@ class FrozenTrajectory:
             self.cpoints.append(per_point.reshape(c, 64))
             self.sources.append(src.reshape(c, 4))
             self.contact_friction.append(rec["friction"])
+            K = int(np.atleast_1d(params)["substeps"][0])
+            I = int(np.atleast_1d(params)["solve_iterations"][0])
+            PI = int(np.atleast_1d(params)["position_iterations"][0])
+            solve = np.zeros(K * I * 4 * c, np.uint8)
+            position = np.zeros(K * PI * 4 * c, np.uint8)
+            integrate = np.zeros(K * self.n, np.uint8)
+            target_flags = np.zeros(4 * c, np.uint8)
+            L.orc_step_decisions(oracle_world._h, _p(solve), _p(position), _p(integrate), _p(target_flags))
+            self.decisions.append(np.concatenate([solve, position, integrate, target_flags]))
+            snaps = [np.zeros(K * self.n * 13, np.float32), np.zeros(K * I * self.n * 6, np.float32),
+                     np.zeros(K * I * c * 12, np.float32), np.zeros(K * PI * self.n * 3, np.float32)]
+            L.orc_step_snapshots(oracle_world._h, *[_p(a) for a in snaps])
+            self.snapshots.append(np.concatenate(snaps))
         self.final = oracle_world.states()
+        L.orc_keep_snapshots(oracle_world._h, 0)
+        self.decisions = np.ascontiguousarray(np.concatenate(self.decisions) if self.decisions else np.zeros(0, np.uint8))
+        self.snapshots = np.ascontiguousarray(np.concatenate(self.snapshots) if self.snapshots else np.zeros(0, np.float32))
+        self.final_record = np.ascontiguousarray(state_vector(self.final).astype(np.float32))
         self.counts = np.array(self.counts, np.uint32)
         self.cint = np.ascontiguousarray(np.concatenate(self.cint) if self.cint else np.zeros((0, 5), np.int32))
         self.cdouble = np.ascontiguousarray(np.concatenate(self.cdouble) if self.cdouble else np.zeros((0, 8)))
@@ -131,8 +159,11 @@ class FrozenTrajectory:
         self._keep = (np.ascontiguousarray(bodies), np.ascontiguousarray(self.target, np.float64),
                       np.ascontiguousarray(friction, np.float64), np.ascontiguousarray(state, np.float64))
         b, t, f, s = self._keep
+        dec = _p(self.decisions) if (self.follow_decisions or self.along_record) else None
+        snaps = _p(self.snapshots) if self.along_record else None
+        fin = _p(self.final_record) if self.along_record else None
         return (len(self.bodies), _p(b), _p(self.params), len(self.counts), _p(self.counts), _p(self.cint),
-                _p(self.cdouble), _p(self.cpoints), _p(self.sources), _p(t), _p(f), len(f), _p(s))
+                _p(self.cdouble), _p(self.cpoints), _p(self.sources), _p(t), dec, snaps, fin, _p(f), len(f), _p(s))
 
     def forward(self, inverse_mass, inverse_inertia, friction, state):
         """The FP64 loss and final state (rows x 13) of the frozen-contact trajectory."""

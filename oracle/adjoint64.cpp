@@ -117,11 +117,35 @@ struct ContactIn {
     double la[4][3], lb[4][3], depth[4], position[4][3], acc[4][3];
     int32_t source[4];  // index of the relayed point in the previous step's points (4 x contact + point), or -1
 };
+// A recorded run's branch decisions per step (the FP32 oracle's, which are the device's): with them
+// the forward takes every clamp and threshold the recorded way, so its derivatives are those of
+// the step over the frozen active set.
+struct StepDecisions {
+    std::vector<uint8_t> solve;      // [substep][iteration][contact][point]
+    std::vector<uint8_t> position;   // [substep][iteration][contact][point]
+    std::vector<uint8_t> integrate;  // [substep][row]
+    std::vector<uint8_t> target;     // [contact][point]
+};
+// A recorded run's primal values (the FP32 oracle's, which are the device's): with them the forward
+// evaluates its derivatives along that run instead of along its own FP64 values, so they are what
+// the device's adjoint transposes. Per step: states at each substep's start [substep][row][13],
+// velocities at each velocity iteration's start [substep][iteration][row][6], accumulated impulses
+// there [substep][iteration][contact][point][3], resolutions at each position iteration's start
+// [substep][iteration][row][3].
+struct StepSnapshots {
+    std::vector<float> state, vel, acc, res;
+};
+inline void snap(double& x, double v) { x = v; }
+template <int K> void snap(Dual<K>& x, double v) { x.v = v; }
+
 struct Problem {
     Params p;
     std::vector<BodyConst> bodies;
     std::vector<std::vector<ContactIn>> steps;
     std::vector<double> target;  // 3 per row: the loss's target final positions
+    std::vector<StepDecisions> decisions;  // empty: every branch decided by the values
+    std::vector<StepSnapshots> snapshots;  // empty: the forward's own values
+    std::vector<float> final_state;        // with snapshots: the run's final states (13 per row)
 };
 
 template <class T>
@@ -181,6 +205,20 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
     for (size_t step = 0; step < P.steps.size(); ++step) {
         const std::vector<ContactIn>& cs = P.steps[step];
         const size_t c = cs.size();
+        const StepDecisions* dec = P.decisions.empty() ? nullptr : &P.decisions[step];
+        const StepSnapshots* sn = P.snapshots.empty() ? nullptr : &P.snapshots[step];
+        auto snap_states = [&](uint32_t sub) {
+            if (!sn) return;
+            for (size_t r = 0; r < n; ++r) {
+                if (!P.bodies[r].dynamic) continue;
+                const float* o = &sn->state[((size_t)sub * n + r) * 13];
+                snap(s.x[r].x, o[0]); snap(s.x[r].y, o[1]); snap(s.x[r].z, o[2]);
+                snap(s.q[r].x, o[3]); snap(s.q[r].y, o[4]); snap(s.q[r].z, o[5]); snap(s.q[r].w, o[6]);
+                snap(s.v[r].x, o[7]); snap(s.v[r].y, o[8]); snap(s.v[r].z, o[9]);
+                snap(s.w[r].x, o[10]); snap(s.w[r].y, o[11]); snap(s.w[r].z, o[12]);
+            }
+        };
+        snap_states(0);
         // depths of the frozen contacts at this step's start, target speeds, block counts, acc_in
         std::vector<T> depth(4 * c, T(0.0)), target(4 * c, T(0.0));
         std::vector<V3<T>> acc(4 * c, zero3<T>());
@@ -218,9 +256,11 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
                 };
                 T speed = dot(point_velocity(k.b) - point_velocity(k.a), nrm);
                 T d = depth[4 * i + pi];
-                if (val(d) < 0.0) {
+                const bool from_depth = dec ? dec->target[4 * i + pi] == 1u : val(d) < 0.0;
+                const bool from_restitution = dec ? dec->target[4 * i + pi] == 2u : val(speed) < -p.restitution_threshold;
+                if (from_depth) {
                     target[4 * i + pi] = d / dt;
-                } else if (val(speed) < -p.restitution_threshold) {
+                } else if (from_restitution) {
                     target[4 * i + pi] = -speed * T(k.restitution);
                 }
             }
@@ -240,7 +280,35 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
             return b;
         };
         std::vector<V3<T>> resolution(n, zero3<T>());
+        auto snap_iteration = [&](uint32_t sub, uint32_t it) {
+            if (!sn) return;
+            for (size_t r = 0; r < n; ++r) {
+                if (!P.bodies[r].dynamic) continue;
+                const float* o = &sn->vel[(((size_t)sub * p.iterations + it) * n + r) * 6];
+                snap(s.v[r].x, o[0]); snap(s.v[r].y, o[1]); snap(s.v[r].z, o[2]);
+                snap(s.w[r].x, o[3]); snap(s.w[r].y, o[4]); snap(s.w[r].z, o[5]);
+            }
+            for (size_t i = 0; i < c; ++i) {
+                for (uint32_t pi = 0; pi < 4; ++pi) {
+                    const float* o = &sn->acc[((((size_t)sub * p.iterations + it) * c + i) * 4 + pi) * 3];
+                    snap(acc[4 * i + pi].x, o[0]);
+                    snap(acc[4 * i + pi].y, o[1]);
+                    snap(acc[4 * i + pi].z, o[2]);
+                }
+            }
+        };
+        if (sn && p.iterations > 0) {  // the warm start reads the impulses iteration 0 starts from
+            for (size_t i = 0; i < c; ++i) {
+                for (uint32_t pi = 0; pi < 4; ++pi) {
+                    const float* o = &sn->acc[(i * 4 + pi) * 3];
+                    snap(acc[4 * i + pi].x, o[0]);
+                    snap(acc[4 * i + pi].y, o[1]);
+                    snap(acc[4 * i + pi].z, o[2]);
+                }
+            }
+        }
         for (uint32_t sub = 0; sub < p.substeps; ++sub) {
+            if (sub > 0) snap_states(sub);
             // substep_integrate.wgsl:15-76 (no force fields, no applied forces)
             for (size_t r = 0; r < n; ++r) {
                 const BodyConst& b = P.bodies[r];
@@ -268,9 +336,11 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
                 }
                 V3<T> angular = gyro;
                 T speed = length(velocity);
-                if (val(speed) > p.max_velocity) velocity = velocity * (T(p.max_velocity) / speed);
+                const uint8_t clamps = dec ? dec->integrate[(size_t)sub * n + r] : 0u;
+                if (dec ? (clamps & 1u) != 0u : val(speed) > p.max_velocity) velocity = velocity * (T(p.max_velocity) / speed);
                 T spin_speed = length(angular);
-                if (val(spin_speed) > p.max_angular_velocity) angular = angular * (T(p.max_angular_velocity) / spin_speed);
+                if (dec ? (clamps & 2u) != 0u : val(spin_speed) > p.max_angular_velocity)
+                    angular = angular * (T(p.max_angular_velocity) / spin_speed);
                 s.v[r] = velocity / (T(1.0) + T(b.linear_damping) * h);
                 s.w[r] = angular / (T(1.0) + T(b.angular_damping) * h);
             }
@@ -340,6 +410,7 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
                 apply_deltas(dv, dw);
             }
             for (uint32_t it = 0; it < p.iterations; ++it) {
+                snap_iteration(sub, it);
                 // solver_contact_block.wgsl:6-193, Jacobi over the blocks, then solver_block_apply.wgsl
                 std::vector<V3<T>> dv(n, zero3<T>()), dw(n, zero3<T>());
                 std::vector<V3<T>> next(acc);
@@ -371,13 +442,26 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
                             T wanted = (bias - (T(1.0) + drag) * prior) / (softness + (T(1.0) + drag) * m.truth[pi]);
                             delta = m.truth[pi] * (wanted - a.x) / m.normal_mass[pi];
                         }
-                        T an = wmax(T(0.0), a.x + delta);
-                        T limit = mu * an;
-                        T u1 = a.y - dot(rel, m.t1) / m.t1_mass[pi];
-                        T at1 = wclamp(u1, -limit, limit);
-                        T rem = sqrt(wmax(limit * limit - at1 * at1, T(0.0)));
-                        T u2 = a.z - dot(rel, m.t2) / m.t2_mass[pi];
-                        T at2 = wclamp(u2, -rem, rem);
+                        T an, at1, at2, rem;
+                        T limit, u1, u2;
+                        if (dec) {
+                            const uint8_t f = dec->solve[(((size_t)sub * p.iterations + it) * c + i) * 4 + pi];
+                            an = (f & 1u) ? a.x + delta : T(0.0);
+                            limit = mu * an;
+                            u1 = a.y - dot(rel, m.t1) / m.t1_mass[pi];
+                            at1 = (f & 2u) ? limit : ((f & 4u) ? -limit : u1);
+                            rem = (f & 8u) ? sqrt(wmax(limit * limit - at1 * at1, T(0.0))) : T(0.0);
+                            u2 = a.z - dot(rel, m.t2) / m.t2_mass[pi];
+                            at2 = (f & 16u) ? rem : ((f & 32u) ? -rem : u2);
+                        } else {
+                            an = wmax(T(0.0), a.x + delta);
+                            limit = mu * an;
+                            u1 = a.y - dot(rel, m.t1) / m.t1_mass[pi];
+                            at1 = wclamp(u1, -limit, limit);
+                            rem = sqrt(wmax(limit * limit - at1 * at1, T(0.0)));
+                            u2 = a.z - dot(rel, m.t2) / m.t2_mass[pi];
+                            at2 = wclamp(u2, -rem, rem);
+                        }
                         V3<T> j = nrm * (an - a.x) + m.t1 * (at1 - a.y) + m.t2 * (at2 - a.z);
                         next[4 * i + pi] = V3<T>{an, at1, at2};
                         fv = fv - j * f.inverse_mass(false);
@@ -429,6 +513,14 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
             }
             // position_correction.wgsl:5-46 + position_block.wgsl:11-33, position_apply.wgsl:12-27
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
+                if (sn) {
+                    for (size_t r = 0; r < n; ++r) {
+                        const float* o = &sn->res[(((size_t)sub * p.position_iterations + it) * n + r) * 3];
+                        snap(resolution[r].x, o[0]);
+                        snap(resolution[r].y, o[1]);
+                        snap(resolution[r].z, o[2]);
+                    }
+                }
                 std::vector<V3<T>> sum(n, zero3<T>());
                 std::vector<uint32_t> contributions(n, 0u);
                 for (size_t i = 0; i < c; ++i) {
@@ -442,17 +534,22 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
                     V3<T> total = zero3<T>();
                     uint32_t contributing = 0;
                     for (uint32_t pi = 0; pi < k.count; ++pi) {
-                        T error = wmax(depth[4 * i + pi] - T(p.slop) - resolved, T(0.0));
-                        if (!(val(error) > 0.0)) continue;
+                        T error = depth[4 * i + pi] - T(p.slop) - resolved;
                         T kk = ima + imb;
-                        if (val(kk) == 0.0) continue;
+                        if (dec) {
+                            if (dec->position[(((size_t)sub * p.position_iterations + it) * c + i) * 4 + pi] == 0u) continue;
+                        } else {
+                            error = wmax(error, T(0.0));
+                            if (!(val(error) > 0.0)) continue;
+                            if (val(kk) == 0.0) continue;
+                        }
                         total = total + nrm * (T(p.relaxation) * error / kk);
                         contributing += 1;
                     }
                     if (contributing == 0u) continue;
                     V3<T> correction = total / T((double)contributing);
                     V3<T> lf = -correction * ima, ls = correction * imb;
-                    if (!(val(dot(lf, lf)) > 0.0 || val(dot(ls, ls)) > 0.0)) continue;
+                    if (!dec && !(val(dot(lf, lf)) > 0.0 || val(dot(ls, ls)) > 0.0)) continue;
                     contributions[k.a] += 1u;
                     contributions[k.b] += 1u;
                     sum[k.a] = sum[k.a] + lf;
@@ -470,6 +567,13 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
         acc_prev.assign(c, std::vector<V3<T>>(4, zero3<T>()));
         for (size_t i = 0; i < c; ++i) {
             for (uint32_t pi = 0; pi < 4; ++pi) acc_prev[i][pi] = acc[4 * i + pi];
+        }
+    }
+    if (!P.final_state.empty()) {
+        for (size_t r = 0; r < n; ++r) {
+            if (!P.bodies[r].dynamic) continue;
+            const float* o = &P.final_state[r * 13];
+            snap(s.x[r].x, o[0]); snap(s.x[r].y, o[1]); snap(s.x[r].z, o[2]);
         }
     }
     T loss = T(0.0);
@@ -494,7 +598,7 @@ T run(const Problem& P, const Theta<T>& th, State<T>* final_state) {
 //   (index into the previous step's points, -1 = not relayed)
 Problem make_problem(uint32_t n, const double* bodies, const double* params, uint32_t steps, const uint32_t* counts,
                      const int32_t* cint, const double* cdouble, const double* cpoints, const int32_t* sources,
-                     const double* target) {
+                     const double* target, const uint8_t* decisions, const float* snapshots, const float* final_state) {
     Problem P;
     P.p.dt = params[0];
     for (int k = 0; k < 3; ++k) P.p.gravity[k] = params[1 + k];
@@ -550,6 +654,43 @@ Problem make_problem(uint32_t n, const double* bodies, const double* params, uin
         }
     }
     P.target.assign(target, target + 3 * (size_t)n);
+    if (decisions) {
+        // per step, back to back: solve, position, integrate, target flags
+        const size_t K = P.p.substeps, I = P.p.iterations, PI = P.p.position_iterations;
+        P.decisions.resize(steps);
+        const uint8_t* at = decisions;
+        for (uint32_t st = 0; st < steps; ++st) {
+            const size_t c = counts[st];
+            StepDecisions& d = P.decisions[st];
+            d.solve.assign(at, at + K * I * 4 * c);
+            at += K * I * 4 * c;
+            d.position.assign(at, at + K * PI * 4 * c);
+            at += K * PI * 4 * c;
+            d.integrate.assign(at, at + K * n);
+            at += K * n;
+            d.target.assign(at, at + 4 * c);
+            at += 4 * c;
+        }
+    }
+    if (snapshots) {
+        // per step, back to back: states, velocities, impulses, resolutions
+        const size_t K = P.p.substeps, I = P.p.iterations, PI = P.p.position_iterations;
+        P.snapshots.resize(steps);
+        const float* at = snapshots;
+        for (uint32_t st = 0; st < steps; ++st) {
+            const size_t c = counts[st];
+            StepSnapshots& sn = P.snapshots[st];
+            sn.state.assign(at, at + K * n * 13);
+            at += K * n * 13;
+            sn.vel.assign(at, at + K * I * n * 6);
+            at += K * I * n * 6;
+            sn.acc.assign(at, at + K * I * c * 12);
+            at += K * I * c * 12;
+            sn.res.assign(at, at + K * PI * n * 3);
+            at += K * PI * n * 3;
+        }
+    }
+    if (final_state) P.final_state.assign(final_state, final_state + 13 * (size_t)n);
     return P;
 }
 
@@ -587,10 +728,14 @@ extern "C" {
 
 // The FP64 forward over the frozen contact sets: returns the loss and writes the final state
 // (13 doubles per row) when out_state is not null. friction: one value per contact group.
+// decisions: null (branches decided by the values) or a recorded run's flags per step; snapshots and
+// final_state: null, or a recorded run's primal values along which the derivatives are taken.
 double adj_forward(uint32_t n, const double* bodies, const double* params, uint32_t steps, const uint32_t* counts,
                    const int32_t* cint, const double* cdouble, const double* cpoints, const int32_t* sources,
-                   const double* target, const double* friction, uint32_t groups, const double* state, double* out_state) {
-    adj::Problem P = adj::make_problem(n, bodies, params, steps, counts, cint, cdouble, cpoints, sources, target);
+                   const double* target, const uint8_t* decisions, const float* snapshots, const float* final_state,
+                   const double* friction, uint32_t groups, const double* state, double* out_state) {
+    adj::Problem P = adj::make_problem(n, bodies, params, steps, counts, cint, cdouble, cpoints, sources, target, decisions,
+                                       snapshots, final_state);
     adj::Theta<double> th = adj::make_theta<double>(P, bodies, friction, groups, state);
     adj::State<double> fin;
     double loss = adj::run(P, th, &fin);
@@ -611,10 +756,12 @@ double adj_forward(uint32_t n, const double* bodies, const double* params, uint3
 // directions x (20n + groups) doubles; writes one derivative per direction into out.
 void adj_directional(uint32_t n, const double* bodies, const double* params, uint32_t steps, const uint32_t* counts,
                      const int32_t* cint, const double* cdouble, const double* cpoints, const int32_t* sources,
-                     const double* target, const double* friction, uint32_t groups, const double* state,
-                     uint32_t directions, const double* tangent, double* out) {
+                     const double* target, const uint8_t* decisions, const float* snapshots, const float* final_state,
+                     const double* friction, uint32_t groups, const double* state, uint32_t directions,
+                     const double* tangent, double* out) {
     using D = adj::Dual<adj::kLanes>;
-    adj::Problem P = adj::make_problem(n, bodies, params, steps, counts, cint, cdouble, cpoints, sources, target);
+    adj::Problem P = adj::make_problem(n, bodies, params, steps, counts, cint, cdouble, cpoints, sources, target, decisions,
+                                       snapshots, final_state);
     const size_t dim = 20 * (size_t)n + groups;
     for (uint32_t first = 0; first < directions; first += adj::kLanes) {
         adj::Theta<D> th = adj::make_theta<D>(P, bodies, friction, groups, state);

@@ -210,6 +210,23 @@ struct OracleWorld {
     // (4 x held contact + held point, or -1): the frozen contact set of a differentiable step
     std::vector<dyn_contact_record> solve_contacts;
     std::vector<int32_t> relay_source;
+    // the last step's branch decisions, for the differentiable step's reference: solve [substep]
+    // [iteration][contact][point] (bit 0 normal impulse positive, 1/2 tangent-1 at its upper/lower
+    // limit, 3 the tangent-2 limit passes a derivative (it is above 5 % of the friction limit), 4/5
+    // tangent 2 at its upper/lower limit),
+    // position [substep][iteration][contact][point] (bit 0 the point corrects), integrate
+    // [substep][row] (bit 0 speed clamped, 1 spin clamped), targets [contact][point] (bit 0 from the
+    // depth, 1 from restitution)
+    std::vector<uint8_t> solve_flags, position_flags, integrate_flags, target_flags;
+    uint32_t flag_substep = 0, flag_iteration = 0;
+    // the last step's primal values where the differentiable step's reference evaluates its
+    // derivatives: states at each substep's start [substep][row] (position, orientation, velocity,
+    // angular velocity), velocities at
+    // each velocity iteration's start [substep][iteration][row] (velocity, angular velocity),
+    // accumulated impulses at each velocity iteration's start [substep][iteration][contact][point],
+    // resolutions at each position iteration's start [substep][iteration][row]
+    bool keep_snapshots = false;
+    std::vector<float> snap_pose, snap_vel, snap_acc, snap_res;
     std::vector<uint32_t> contact_matched;
     std::vector<uint32_t> island_parents, island_state;
     std::vector<uint32_t> wake_flags, body_activity, body_motion;
@@ -963,6 +980,13 @@ void solver_prepare(OracleWorld& w) {
     w.counters[DYN_COUNTER_SOLVER_ROWS] = 0;
     w.blocks.assign(2 * (size_t)c, 0);
     w.target_speeds.assign(4 * (size_t)c, 0.0f);
+    w.target_flags.assign(4 * (size_t)c, 0u);
+    {
+        const dyn_step_params& p = w.params;
+        w.solve_flags.assign((size_t)p.substeps * p.solve_iterations * 4 * c, 0u);
+        w.position_flags.assign((size_t)p.substeps * p.position_iterations * 4 * c, 0u);
+        w.integrate_flags.assign((size_t)p.substeps * n, 0u);
+    }
     w.solver_rows.clear();
     w.velocity_deltas.assign(8 * (size_t)n, 0);
     w.position_deltas.assign(8 * (size_t)n, 0);
@@ -982,8 +1006,10 @@ void solver_prepare(OracleWorld& w) {
             float target = 0.0f;
             if (contact.points[pi].depth < 0.0f) {
                 target = contact.points[pi].depth / w.params.dt;
+                w.target_flags[4 * (size_t)index + pi] = 1u;
             } else if (speed < -w.params.restitution_threshold) {
                 target = -speed * contact.restitution;
+                w.target_flags[4 * (size_t)index + pi] = 2u;
             }
             w.target_speeds[4 * (size_t)index + pi] = target;
         }
@@ -1141,18 +1167,31 @@ void solve_contact_block(OracleWorld& w, uint32_t index, bool residual) {
         float delta = contact_normal_delta(contact, normal_mass, normal_truth, w.params.dt,
                                            w.target_speeds[4 * (size_t)index + pi], p.depth, normal_speed, acc_n);
         float next_normal = fmaxw(0.0f, acc_n + delta);
+        uint8_t flags = acc_n + delta > 0.0f ? 1u : 0u;
         impulses[pi] = impulses[pi] + normal * (next_normal - acc_n);
         acc_n = next_normal;
         float friction_limit = contact.friction * acc_n;
         float t1_mass = point_momentum_mass(split_f, split_s, af, as, t.first) * (float)std::max(contact.point_count, 1u);
         float t1_speed = dot(relative_velocity(pf, ps, af, as), t.first);
-        float next_t1 = clampw(acc_t1 - t1_speed / t1_mass, -friction_limit, friction_limit);
+        const float want_t1 = acc_t1 - t1_speed / t1_mass;
+        float next_t1 = clampw(want_t1, -friction_limit, friction_limit);
+        flags |= want_t1 > friction_limit ? 2u : (want_t1 < -friction_limit ? 4u : 0u);
         impulses[pi] = impulses[pi] + t.first * (next_t1 - acc_t1);
         acc_t1 = next_t1;
         float t2_mass = point_momentum_mass(split_f, split_s, af, as, t.second) * (float)std::max(contact.point_count, 1u);
         float t2_speed = dot(relative_velocity(pf, ps, af, as), t.second);
-        float remaining = std::sqrt(fmaxw(friction_limit * friction_limit - acc_t1 * acc_t1, 0.0f));
-        float next_t2 = clampw(acc_t2 - t2_speed / t2_mass, -remaining, remaining);
+        const float remaining_sq = friction_limit * friction_limit - acc_t1 * acc_t1;
+        float remaining = std::sqrt(fmaxw(remaining_sq, 0.0f));
+        const float want_t2 = acc_t2 - t2_speed / t2_mass;
+        float next_t2 = clampw(want_t2, -remaining, remaining);
+        // the device adjoint's rule: below 5 % of the friction limit the tangent-2 limit is locally constant
+        flags |= (remaining_sq > 0.0f && remaining > 0.05f * friction_limit) ? 8u : 0u;
+        flags |= want_t2 > remaining ? 16u : (want_t2 < -remaining ? 32u : 0u);
+        {
+            const dyn_step_params& sp = w.params;
+            const size_t c = w.contacts.size();
+            w.solve_flags[(((size_t)w.flag_substep * sp.solve_iterations + w.flag_iteration) * c + index) * 4 + pi] = flags;
+        }
         impulses[pi] = impulses[pi] + t.second * (next_t2 - acc_t2);
         acc_t2 = next_t2;
         updated.points[pi].accumulated_normal = acc_n;
@@ -1250,6 +1289,10 @@ void substep_integrate(OracleWorld& w) {
         if (speed > p.max_velocity) velocity = velocity * (p.max_velocity / speed);
         float spin_speed = length(angular);
         if (spin_speed > p.max_angular_velocity) angular = angular * (p.max_angular_velocity / spin_speed);
+        if (!w.integrate_flags.empty()) {
+            w.integrate_flags[(size_t)w.flag_substep * w.states.size() + row] =
+                (uint8_t)((speed > p.max_velocity ? 1u : 0u) | (spin_speed > p.max_angular_velocity ? 2u : 0u));
+        }
         velocity = velocity / (1.0f + d.linear_damping * h);
         angular = angular / (1.0f + d.angular_damping * h);
         wr3(s.velocity, velocity);
@@ -1287,6 +1330,7 @@ void position_block(OracleWorld& w) {
         float resolved = dot(normal, w.resolution[sr] - w.resolution[fr]);
         V3 total = splat3(0.0f);
         uint32_t contributing = 0;
+        uint8_t corrects[4] = {0u, 0u, 0u, 0u};
         for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
             float error = fmaxw(contact.points[pi].depth - w.params.slop - resolved, 0.0f);
             if (error <= 0.0f) continue;
@@ -1294,6 +1338,7 @@ void position_block(OracleWorld& w) {
             if (k == 0.0f) continue;
             total = total + normal * (w.params.relaxation * error / k);
             contributing += 1;
+            corrects[pi] = 1u;
         }
         if (contributing == 0u) continue;
         V3 correction = total / (float)contributing;
@@ -1302,6 +1347,10 @@ void position_block(OracleWorld& w) {
         // correction.wgsl:18-31 pair_holds
         bool holds = dot(lin_f, lin_f) > 0.0f || dot(lin_s, lin_s) > 0.0f;
         if (!holds) continue;
+        for (uint32_t pi = 0; pi < 4; ++pi) {
+            w.position_flags[(((size_t)w.flag_substep * w.params.position_iterations + w.flag_iteration) * c + index) * 4 + pi] =
+                corrects[pi];
+        }
         atomic_add_u32(&w.contributions[fr], 1u);
         atomic_add_u32(&w.contributions[sr], 1u);
         accumulate(w.position_deltas, fr, lin_f, splat3(0.0f), DYN_SOLVER_POSITION_SCALE);
@@ -1630,7 +1679,25 @@ void walk_joints(OracleWorld& w, JointWalk mode, bool residual) {
 // solver.rs:304-333 SolveSubsteps.record
 void solve_substeps(OracleWorld& w) {
     uint32_t c = (uint32_t)w.contacts.size();
+    const size_t n = w.states.size();
+    const dyn_step_params& sp = w.params;
+    if (w.keep_snapshots) {
+        w.snap_pose.assign((size_t)sp.substeps * n * 13, 0.0f);
+        w.snap_vel.assign((size_t)sp.substeps * sp.solve_iterations * n * 6, 0.0f);
+        w.snap_acc.assign((size_t)sp.substeps * sp.solve_iterations * c * 12, 0.0f);
+        w.snap_res.assign((size_t)sp.substeps * sp.position_iterations * n * 3, 0.0f);
+    }
     for (uint32_t substep = 0; substep < w.params.substeps; ++substep) {
+        w.flag_substep = substep;
+        if (w.keep_snapshots) {
+            for (size_t r = 0; r < n; ++r) {
+                float* o = &w.snap_pose[((size_t)substep * n + r) * 13];
+                for (int k = 0; k < 3; ++k) o[k] = w.states[r].position[k];
+                for (int k = 0; k < 4; ++k) o[3 + k] = w.states[r].orientation[k];
+                for (int k = 0; k < 3; ++k) o[7 + k] = w.states[r].velocity[k];
+                for (int k = 0; k < 3; ++k) o[10 + k] = w.states[r].angular_velocity[k];
+            }
+        }
         substep_integrate(w);
         if (substep == 0) {
             walk_joints(w, JointWalk::Warm, false);
@@ -1639,6 +1706,22 @@ void solve_substeps(OracleWorld& w) {
             block_apply(w);
         }
         for (uint32_t it = 0; it < w.params.solve_iterations; ++it) {
+            w.flag_iteration = it;
+            if (w.keep_snapshots) {
+                for (size_t r = 0; r < n; ++r) {
+                    float* o = &w.snap_vel[(((size_t)substep * sp.solve_iterations + it) * n + r) * 6];
+                    for (int k = 0; k < 3; ++k) o[k] = w.states[r].velocity[k];
+                    for (int k = 0; k < 3; ++k) o[3 + k] = w.states[r].angular_velocity[k];
+                }
+                for (size_t i = 0; i < c; ++i) {
+                    for (uint32_t pi = 0; pi < 4; ++pi) {
+                        float* o = &w.snap_acc[((((size_t)substep * sp.solve_iterations + it) * c + i) * 4 + pi) * 3];
+                        o[0] = w.contacts[i].points[pi].accumulated_normal;
+                        o[1] = w.contacts[i].points[pi].accumulated_tangent_1;
+                        o[2] = w.contacts[i].points[pi].accumulated_tangent_2;
+                    }
+                }
+            }
             bool residual = w.solver_rounds == w.params.solve_iterations;
             walk_joints(w, JointWalk::Solve, residual);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -1647,6 +1730,15 @@ void solve_substeps(OracleWorld& w) {
         }
         substep_advance(w);
         for (uint32_t it = 0; it < w.params.position_iterations; ++it) {
+            w.flag_iteration = it;
+            if (w.keep_snapshots) {
+                for (size_t r = 0; r < n; ++r) {
+                    float* o = &w.snap_res[(((size_t)substep * sp.position_iterations + it) * n + r) * 3];
+                    o[0] = w.resolution[r].x;
+                    o[1] = w.resolution[r].y;
+                    o[2] = w.resolution[r].z;
+                }
+            }
             walk_joints(w, JointWalk::Project, false);
             position_block(w);
             position_apply(w);
@@ -1831,6 +1923,21 @@ uint32_t orc_solve_contacts(const OracleWorld* w, dyn_contact_record* out, float
     if (targets) std::copy(w->target_speeds.begin(), w->target_speeds.begin() + 4 * c, targets);
     if (sources) std::copy(w->relay_source.begin(), w->relay_source.begin() + 4 * c, sources);
     return (uint32_t)c;
+}
+// Keeps (or stops keeping) the primal snapshots of each step (OracleWorld::snap_pose ...).
+void orc_keep_snapshots(OracleWorld* w, uint32_t keep) { w->keep_snapshots = keep != 0u; }
+void orc_step_snapshots(const OracleWorld* w, float* pose, float* vel, float* acc, float* res) {
+    if (pose) std::copy(w->snap_pose.begin(), w->snap_pose.end(), pose);
+    if (vel) std::copy(w->snap_vel.begin(), w->snap_vel.end(), vel);
+    if (acc) std::copy(w->snap_acc.begin(), w->snap_acc.end(), acc);
+    if (res) std::copy(w->snap_res.begin(), w->snap_res.end(), res);
+}
+// The last step's branch decisions (OracleWorld::solve_flags ...); any output may be null.
+void orc_step_decisions(const OracleWorld* w, uint8_t* solve, uint8_t* position, uint8_t* integrate, uint8_t* targets) {
+    if (solve) std::copy(w->solve_flags.begin(), w->solve_flags.end(), solve);
+    if (position) std::copy(w->position_flags.begin(), w->position_flags.end(), position);
+    if (integrate) std::copy(w->integrate_flags.begin(), w->integrate_flags.end(), integrate);
+    if (targets) std::copy(w->target_flags.begin(), w->target_flags.end(), targets);
 }
 uint32_t orc_islands(const OracleWorld* w, uint32_t* out) {
     if (out) std::memcpy(out, w->island_parents.data(), w->island_parents.size() * 4);

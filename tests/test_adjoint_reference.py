@@ -16,18 +16,19 @@ from oracle.oracle import OracleWorld
 DT = 1.0 / 120.0
 
 
-def tower_batch(levels=2, footprint=2, worlds=2, seed=3, distance=2.2):
+def tower_batch(levels=2, footprint=2, worlds=2, seed=3, distance=2.2, heading=None, gap=0.0):
     rng = np.random.default_rng(seed)
     parts = []
     for w in range(worlds):
-        part = scenes.tower_world(100 + w, levels, footprint, distance=distance, friction=float(rng.uniform(0.3, 0.8)))
+        part = scenes.tower_world(100 + w, levels, footprint, distance=distance, friction=float(rng.uniform(0.3, 0.8)),
+                                  heading=heading, gap=gap)
         part.bodies["mass"][:-1] = rng.uniform(0.5, 2.0, len(part.bodies) - 1).astype(np.float32)
         parts.append(part)
     return scenes.batch(parts)
 
 
-def settled_trajectory(steps=24, settle=30, speed=4.0, distance=2.2):
-    scene = tower_batch(distance=distance)
+def settled_trajectory(steps=24, settle=30, speed=4.0, distance=2.2, heading=None, gap=0.0):
+    scene = tower_batch(distance=distance, heading=heading, gap=gap)
     world = World(sleep_time=np.inf)
     ids = scene.build(world)
     exported = world.export_scene()
