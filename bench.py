@@ -261,6 +261,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     }
     if args.workload.startswith("batched_worlds_"):
         result["batch"] = loop_baseline(args, DT, ms / args.steps, local_rank)
+    if not args.no_adjoint:
+        result["adjoint"] = adjoint_benchmark(local_rank, steps=args.adjoint_steps, settle=args.adjoint_setup)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
     world.close()
@@ -281,6 +283,88 @@ def max_over_ranks(value: float, dist, device) -> float:
 def whole_job_rate(units_per_rank: float, world_size: int, seconds: float) -> float:
     """Units all ranks processed per second of the slowest rank."""
     return units_per_rank * world_size / seconds
+
+
+ADJOINT_WORKLOAD = "differentiable_towers_256"
+
+
+def adjoint_benchmark(device: int, steps: int = 120, settle: int = 60, interval: int = 10) -> dict:
+    """The differentiable workload: 256 tower worlds (8-high, 4 x 4 unit boxes each, masses drawn
+    U(0.5, 2) kg, friction per world U(0.3, 0.8)) and a sphere per world launched at U(3, 8) m/s
+    toward its tower, sleeping off, dt 1/120 s. Two identical worlds settle `settle` steps; then one
+    steps `steps` times plainly (the plain forward) and the other records the same steps with
+    checkpoints every `interval` steps and reverses all of them (dyn_backward, which replays each
+    segment from its checkpoint, narrowphase included). Times are CUDA events on each world's stream."""
+    import torch
+
+    from dynamis_b200 import World, records as R, scenes
+
+    dt = 1.0 / 120.0
+    scene = scenes.WORKLOADS[ADJOINT_WORKLOAD]()
+    worlds, streams = [], []
+    for _ in range(2):
+        w = World(device=device, sleep_time=float("inf"))
+        scene.build(w)
+        stream = torch.cuda.Stream(device=device)
+        w.set_stream(stream.cuda_stream)
+        for _ in range(settle):
+            w.step(dt)
+        w.wait()
+        worlds.append(w)
+        streams.append(stream)
+    plain, taped = worlds
+    bodies = plain.sizes()["bodies"]
+    # warm-up: both worlds take the same `steps` steps; the taped one records them and reverses one,
+    # so its tape, checkpoint blocks and reverse graph exist before the timed run (a tape of the same
+    # shape allocates nothing), and the recorded end state is restored: the two stay identical
+    for _ in range(steps):
+        plain.step(dt)
+    taped.tape_begin(interval)
+    for _ in range(steps):
+        taped.step(dt)
+    taped.step_backward(np.zeros(bodies, R.BODY_GRAD), 1)
+    taped.tape_end()
+    for w in worlds:
+        exported = w.export_scene()
+        spheres = np.sort(exported["owners"][exported["colliders"]["kind"] == R.SHAPE_SPHERE]).astype(np.int64)
+        states = w.read_states()
+        states["velocity"][spheres] = scenes.sphere_launches(scene, states, spheres)
+        w.upload_states(states)
+    assert np.array_equal(plain.read_states()["position"], taped.read_states()["position"])
+
+    def timed(stream, body):
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        body()
+        end.record(stream)
+        end.synchronize()
+        return start.elapsed_time(end)
+
+    def forward(w):
+        for _ in range(steps):
+            w.step(dt)
+
+    forward_ms = timed(streams[0], lambda: forward(plain))
+    taped.tape_begin(interval)
+    taped_ms = timed(streams[1], lambda: forward(taped))
+    final = taped.read_states()
+    grad = np.zeros(bodies, R.BODY_GRAD)
+    grad["position"] = 2.0 * final["position"]  # d/dx of the summed squared final positions
+    holder = {}
+    backward_ms = timed(streams[1], lambda: holder.update(out=taped.step_backward(grad, steps)))
+    g = taped.param_grads()
+    taped.tape_end()
+    finite = bool(np.all(np.isfinite(holder["out"]["velocity"])) and np.all(np.isfinite(g["inverse_mass"])))
+    for w in worlds:
+        w.close()
+    log(f"adjoint: plain forward {forward_ms:.1f} ms, taped forward {taped_ms:.1f} ms, backward {backward_ms:.1f} ms "
+        f"for {steps} steps of {bodies} bodies")
+    return {"workload": ADJOINT_WORKLOAD, "bodies": bodies, "steps": steps, "dt": dt, "checkpoint_interval": interval,
+            "setup_steps": settle + steps, "forward_ms": forward_ms, "taped_forward_ms": taped_ms, "backward_ms": backward_ms,
+            "fwd_bwd_over_fwd": (taped_ms + backward_ms) / forward_ms,
+            "fwd_bwd_body_steps_per_s": bodies * steps / ((taped_ms + backward_ms) * 1e-3),
+            "forward_body_steps_per_s": bodies * steps / (forward_ms * 1e-3), "gradients_finite": finite}
 
 
 def loop_baseline(args, dt: float, batch_ms: float, device: int, sample_every: int = 16) -> dict:
@@ -393,6 +477,10 @@ def main():
     ap.add_argument("--workload", default="mixed_pile_262144")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-towers measurement")
+    ap.add_argument("--adjoint-only", action="store_true", help="print only the differentiable-towers measurement")
+    ap.add_argument("--adjoint-steps", type=int, default=120)
+    ap.add_argument("--adjoint-setup", type=int, default=60)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
@@ -400,6 +488,12 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)))
+        return
+    if args.adjoint_only:
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(adjoint_benchmark(local_rank, steps=args.adjoint_steps, settle=args.adjoint_setup)))
         return
     if world_size > 1:
         import datetime

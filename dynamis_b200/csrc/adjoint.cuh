@@ -96,10 +96,15 @@ struct AdjView {
     float4* gacc[2];   // [4c] d loss / d accumulated impulses (normal, tangent 1, tangent 2): this step, previous
     uint32_t* acc_flip;  // device word: which gacc is this step's
     float4* g_ra;      // [4c] d loss / d arm on the first body (xyz), d loss / d normal mass (w), one substep
-    float4* g_rb;      // [4c] d loss / d arm on the second body (xyz)
-    float4* g_m;       // [4c] d loss / d tangent-1 mass, tangent-2 mass
-    float4* g_pt;      // [4c] d loss / d target speed (x), d loss / d depth (y), whole step
+    float4* g_rb;      // [4c] d loss / d arm on the second body (xyz), d loss / d target speed (w, whole step)
+    float2* g_m;       // [4c] d loss / d tangent-1 mass, tangent-2 mass
+    float4* g_pt;      // [4c] d loss / d depth (y), whole step
     float4* g_param;   // [c] d loss / d inverse mass of the first and second body, of their inertia scales
+    float4* t_arm_a;   // [4c] a substep's pose-only terms (k_adj_terms): arm on the first body, normal mass
+    float4* t_arm_b;   // [4c] arm on the second body
+    float4* t_mass;    // [4c] tangent-1 mass, tangent-2 mass, target speed
+    float4* t_tan1;    // [c] tangent 1
+    float4* t_tan2;    // [c] tangent 2
     float* g_mu;       // [c] d loss / d contact friction
     uint32_t* status;
 };
@@ -154,8 +159,9 @@ struct TapeBlock {
     f3 reach_f, reach_s, spread_f, spread_s;
     float count_f;
 };
-__device__ __forceinline__ void tape_block(const TapeView& t, uint32_t s, uint32_t k, uint32_t i, uint4 r, const float4* vel,
-                                           TapeBlock* b) {
+// The block's bodies alone (what the impulses act on); tape_block adds the pose-only terms.
+__device__ __forceinline__ void tape_block_bodies(const TapeView& t, uint32_t s, uint32_t k, uint32_t i, uint4 r,
+                                                  const float4* vel, TapeBlock* b) {
     const BodyHot* hot = t.hot_at(s, k);
     const BodyHot& ha = hot[r.x];
     const BodyHot& hb = hot[r.y];
@@ -177,8 +183,12 @@ __device__ __forceinline__ void tape_block(const TapeView& t, uint32_t s, uint32
     const float4 nf = t.normal[t.cs(s) + i];
     b->normal = xyz(nf);
     b->friction = nf.w;
-    make_tangents(b->normal, &b->t1, &b->t2);
     b->count = r.z & 0xFFu;
+}
+__device__ __forceinline__ void tape_block(const TapeView& t, uint32_t s, uint32_t k, uint32_t i, uint4 r, const float4* vel,
+                                           TapeBlock* b) {
+    tape_block_bodies(t, s, k, i, r, vel, b);
+    make_tangents(b->normal, &b->t1, &b->t2);
     b->reach_f = s3(0.0f);
     b->reach_s = s3(0.0f);
     #pragma unroll
@@ -287,7 +297,7 @@ __global__ void k_adj_clear(TapeView t, AdjView a, uint32_t n) {
                 const size_t o = (size_t)p * t.c + i;
                 a.g_ra[o] = z;
                 a.g_rb[o] = z;
-                a.g_m[o] = z;
+                a.g_m[o] = make_float2(0.0f, 0.0f);
                 a.g_pt[o] = z;
             }
             a.g_param[i] = z;
@@ -419,24 +429,76 @@ __global__ void k_adj_advance(TapeView t, AdjView a, uint32_t n, dyn_step_params
     }
 }
 
+// The pose-only terms of substep `k`'s contact blocks (k_solve_prepare's), once for all of the
+// substep's reversed iterations.
+__global__ void k_adj_terms(TapeView t, AdjView a, uint32_t k) {
+    const uint32_t s = *t.slot;
+    const uint32_t count = t.counts[s];
+    GRID_STRIDE(i, count) {
+        const uint4 r = t.rows[t.cs(s) + i];
+        if (!resolves(r) || !block_supported(t, s, i)) continue;
+        TapeBlock b;
+        tape_block(t, s, k, i, r, nullptr, &b);
+        a.t_tan1[i] = mk4(b.t1, 0.0f);
+        a.t_tan2[i] = mk4(b.t2, 0.0f);
+#pragma unroll
+        for (uint32_t q = 0; q < 4u; ++q) if (q < b.count) {
+            const size_t o = (size_t)q * t.c + i;
+            a.t_arm_a[o] = mk4(b.ra[q], b.nm[q]);
+            a.t_arm_b[o] = mk4(b.rb[q], 0.0f);
+            a.t_mass[o] = make_float4(b.m1[q], b.m2[q], t.lb[t.ps(s) + o].w, 0.0f);
+        }
+    }
+}
+// The block's bodies with the terms k_adj_terms stored.
+__device__ __forceinline__ void tape_block_stored(const TapeView& t, const AdjView& a, uint32_t s, uint32_t k, uint32_t i,
+                                                  uint4 r, const float4* vel, TapeBlock* b) {
+    tape_block_bodies(t, s, k, i, r, vel, b);
+    b->t1 = xyz(a.t_tan1[i]);
+    b->t2 = xyz(a.t_tan2[i]);
+#pragma unroll
+    for (uint32_t q = 0; q < 4u; ++q) if (q < b->count) {
+        const size_t o = (size_t)q * t.c + i;
+        const float4 x = a.t_arm_a[o], y = a.t_arm_b[o], m = a.t_mass[o];
+        b->ra[q] = xyz(x);
+        b->nm[q] = x.w;
+        b->rb[q] = xyz(y);
+        b->m1[q] = m.x;
+        b->m2[q] = m.y;
+    }
+}
+
 // One contact block of velocity iteration `it` of substep `k` (solve_block of step.cuh), reversed.
 // Every point's impulse comes from the velocities the block started with, so each point reverses on
-// its own; the block's velocity changes are the sums of the points' impulses.
+// its own: a quad of lanes takes a block, one point per lane, and sums the block's velocity and
+// parameter gradients over the quad with shuffles; the quad's first lane adds them to the rows.
+__device__ __forceinline__ float quad_sum(float v, unsigned mask) {
+    v += __shfl_xor_sync(mask, v, 1);
+    v += __shfl_xor_sync(mask, v, 2);
+    return v;
+}
+__device__ __forceinline__ f3 quad_sum3(f3 v, unsigned mask) {
+    return mk3(quad_sum(v.x, mask), quad_sum(v.y, mask), quad_sum(v.z, mask));
+}
 __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_step_params p, uint32_t k, uint32_t it) {
     const uint32_t s = *t.slot;
     const uint32_t count = t.counts[s];
     const float4* vel = t.vel_at(s, k, it);
     const float4* accs = t.acc_at(s, k, it);
     float4* gacc = a.gacc[*a.acc_flip];
-    GRID_STRIDE(i, count) {
+    const uint32_t q = threadIdx.x & 3u;  // the lane's point
+    const unsigned mask = 0xFu << (threadIdx.x & 28u);
+    const uint32_t quads = (gridDim.x * blockDim.x) >> 2;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; i < count; i += quads) {
+        // every lane of a quad takes the same branches up to the point work
         const uint4 r = t.rows[t.cs(s) + i];
         if (!resolves(r)) continue;
         if (!block_supported(t, s, i)) {
-            atomicOr(a.status, DYN_STATUS_ADJOINT_UNSUPPORTED);
+            if (q == 0u) atomicOr(a.status, DYN_STATUS_ADJOINT_UNSUPPORTED);
             continue;
         }
         TapeBlock b;
-        tape_block(t, s, k, i, r, vel, &b);
+        tape_block_bodies(t, s, k, i, r, vel, &b);
         if (b.inert_f && b.inert_s) continue;
         const f3 dva = b.inert_f ? s3(0.0f) : xyz(a.gv[r.x]);
         const f3 dwa = b.inert_f ? s3(0.0f) : xyz(a.gw[r.x]);
@@ -447,16 +509,15 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
         const float ima = b.pf.inverse_mass, imb = b.ps.inverse_mass;
         f3 bva = s3(0.0f), bwa = s3(0.0f), bvb = s3(0.0f), bwb = s3(0.0f);
         float g_ima = 0.0f, g_imb = 0.0f, g_sa = 0.0f, g_sb = 0.0f, g_mu = 0.0f;
-        const f3 n = b.normal, t1 = b.t1, t2 = b.t2;
-        const float mu = b.friction;
-        #pragma unroll
-        for (uint32_t q = 0; q < 4u; ++q) if (q < b.count) {
+        if (q < b.count) {
+            const f3 n = b.normal, t1 = xyz(a.t_tan1[i]), t2 = xyz(a.t_tan2[i]);
+            const float mu = b.friction;
             const size_t o = (size_t)q * t.c + i;
+            const float4 arm_a = a.t_arm_a[o], arm_b = a.t_arm_b[o], masses = a.t_mass[o];
+            const f3 ra = xyz(arm_a), rb = xyz(arm_b);
+            const float nm = arm_a.w, m1 = masses.x, m2 = masses.y, target = masses.z;
             const float4 acc = accs[o];
             const float an = acc.x, at1 = acc.y, at2 = acc.z;
-            const f3 ra = b.ra[q], rb = b.rb[q];
-            const float nm = b.nm[q], m1 = b.m1[q], m2 = b.m2[q];
-            const float target = t.lb[t.ps(s) + o].w;
             // forward (solve_block, hard contact)
             const f3 rel = point_velocity_arm(b.ps, rb) - point_velocity_arm(b.pf, ra);
             const float ns = dot(rel, n);
@@ -474,10 +535,10 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
             const f3 j = s3(0.0f) + n * (an1 - an) + t1 * (at11 - at1) + t2 * (at21 - at2);
             // reverse: the impulse's effect on both bodies
             const f3 jb = imb * dvb - ima * dva + cross(ra, Wa) + cross(Wb, rb);
-            g_ima -= dot(dva, j);
-            g_imb += dot(dvb, j);
-            g_sa -= dot(Wa, cross(ra, j));
-            g_sb += dot(Wb, cross(rb, j));
+            g_ima = -dot(dva, j);
+            g_imb = dot(dvb, j);
+            g_sa = -dot(Wa, cross(ra, j));
+            g_sb = dot(Wb, cross(rb, j));
             f3 gra = cross(Wa, j), grb = cross(j, Wb);
             const float4 gout = gacc[o];
             float g_an1 = dot(n, jb) + gout.x, g_an0 = -dot(n, jb);
@@ -516,7 +577,7 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
             const float g_m1 = g_u1 * ts1 / (m1 * m1);
             // lim = mu an'
             g_an1 += mu * g_lim;
-            g_mu += an1 * g_lim;
+            g_mu = an1 * g_lim;
             // an' = max(0, an + delta)
             float g_delta = 0.0f;
             if (an + delta > 0.0f) {
@@ -528,33 +589,42 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
             const float g_ns = -g_delta / nm;
             const float g_nm = -g_delta * delta / nm;
             const f3 g_rel = n * g_ns + t1 * g_ts1 + t2 * g_ts2;
-            bvb = bvb + g_rel;
-            bva = bva - g_rel;
-            bwb = bwb + cross(rb, g_rel);
-            bwa = bwa - cross(ra, g_rel);
+            bvb = g_rel;
+            bva = -g_rel;
+            bwb = cross(rb, g_rel);
+            bwa = -cross(ra, g_rel);
             grb = grb + cross(g_rel, b.ps.angular_velocity);
             gra = gra - cross(g_rel, b.pf.angular_velocity);
             gacc[o] = make_float4(g_an0, g_at10, g_at20, 0.0f);
             float4 x = a.g_ra[o];
             a.g_ra[o] = make_float4(x.x + gra.x, x.y + gra.y, x.z + gra.z, x.w + g_nm);
             x = a.g_rb[o];
-            a.g_rb[o] = make_float4(x.x + grb.x, x.y + grb.y, x.z + grb.z, x.w);
-            x = a.g_m[o];
-            a.g_m[o] = make_float4(x.x + g_m1, x.y + g_m2, x.z, x.w);
-            x = a.g_pt[o];
-            a.g_pt[o] = make_float4(x.x + g_target, x.y, x.z, x.w);
+            a.g_rb[o] = make_float4(x.x + grb.x, x.y + grb.y, x.z + grb.z, x.w + g_target);
+            const float2 gm = a.g_m[o];
+            a.g_m[o] = make_float2(gm.x + g_m1, gm.y + g_m2);
         }
-        if (!b.inert_f) {
-            atomic_add3(&a.gv_acc[r.x], bva);
-            atomic_add3(&a.gw_acc[r.x], bwa);
+        bva = quad_sum3(bva, mask);
+        bwa = quad_sum3(bwa, mask);
+        bvb = quad_sum3(bvb, mask);
+        bwb = quad_sum3(bwb, mask);
+        g_ima = quad_sum(g_ima, mask);
+        g_imb = quad_sum(g_imb, mask);
+        g_sa = quad_sum(g_sa, mask);
+        g_sb = quad_sum(g_sb, mask);
+        g_mu = quad_sum(g_mu, mask);
+        if (q == 0u) {
+            if (!b.inert_f) {
+                atomic_add3(&a.gv_acc[r.x], bva);
+                atomic_add3(&a.gw_acc[r.x], bwa);
+            }
+            if (!b.inert_s) {
+                atomic_add3(&a.gv_acc[r.y], bvb);
+                atomic_add3(&a.gw_acc[r.y], bwb);
+            }
+            const float4 gp = a.g_param[i];
+            a.g_param[i] = make_float4(gp.x + g_ima, gp.y + g_imb, gp.z + g_sa, gp.w + g_sb);
+            a.g_mu[i] += g_mu;
         }
-        if (!b.inert_s) {
-            atomic_add3(&a.gv_acc[r.y], bvb);
-            atomic_add3(&a.gw_acc[r.y], bwb);
-        }
-        const float4 gp = a.g_param[i];
-        a.g_param[i] = make_float4(gp.x + g_ima, gp.y + g_imb, gp.z + g_sa, gp.w + g_sb);
-        a.g_mu[i] += g_mu;
     }
 }
 // solver_block_apply.wgsl reversed: v' = v + sum of the blocks' changes.
@@ -578,7 +648,7 @@ __global__ void k_adj_warm(TapeView t, AdjView a) {
         const uint4 r = t.rows[t.cs(s) + i];
         if (!resolves(r) || !block_supported(t, s, i)) continue;
         TapeBlock b;
-        tape_block(t, s, 0, i, r, nullptr, &b);
+        tape_block_stored(t, a, s, 0, i, r, nullptr, &b);
         if (b.inert_f && b.inert_s) continue;
         const f3 dva = b.inert_f ? s3(0.0f) : xyz(a.gv[r.x]);
         const f3 dwa = b.inert_f ? s3(0.0f) : xyz(a.gw[r.x]);
@@ -630,7 +700,8 @@ __global__ void k_adj_prepare(TapeView t, AdjView a, uint32_t k) {
         #pragma unroll
         for (uint32_t q = 0; q < 4u; ++q) if (q < b.count) {
             const size_t o = (size_t)q * t.c + i;
-            const float4 xa = a.g_ra[o], xb = a.g_rb[o], xm = a.g_m[o];
+            const float4 xa = a.g_ra[o], xb = a.g_rb[o];
+            const float2 xm = a.g_m[o];
             gra[q] = xyz(xa);
             grb[q] = xyz(xb);
             const f3 ra = b.ra[q], rb = b.rb[q];
@@ -656,8 +727,8 @@ __global__ void k_adj_prepare(TapeView t, AdjView a, uint32_t k) {
                 g_ssc_b += g * dot(rbx, sb);
             }
             a.g_ra[o] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            a.g_rb[o] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            a.g_m[o] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            a.g_rb[o] = make_float4(0.0f, 0.0f, 0.0f, xb.w);  // the target speed's gradient stays for the step's start
+            a.g_m[o] = make_float2(0.0f, 0.0f);
         }
         // spread = S_split (reach x n): reach = sum of the arms
         const f3 gxf = dbody_iinv(b.sf, g_spread_f), gxs = dbody_iinv(b.ss, g_spread_s);
@@ -739,17 +810,17 @@ __global__ void k_adj_start(DeviceWorld w, TapeView t, AdjView a, dyn_step_param
         const DBody fa = tape_body(ha, ha.vel, ha.ang), fb = tape_body(hb, hb.vel, hb.ang);
         for (uint32_t q = 0; q < pc; ++q) {
             const size_t o = (size_t)q * t.c + i;
-            const float4 gpt = a.g_pt[o];
+            const float g_target = a.g_rb[o].w;
             const float depth = t.la[t.ps(s) + o].w;
-            float g_depth = gpt.y;
+            float g_depth = a.g_pt[o].y;
             if (depth < 0.0f) {
-                g_depth += gpt.x / p.dt;
+                g_depth += g_target / p.dt;
             } else {
                 const f3 position = xyz(t.pos[t.ps(s) + o]);
                 const f3 arm_a = position - dbody_com(fa), arm_b = position - dbody_com(fb);
                 const float speed = dot(point_velocity_arm(fb, arm_b) - point_velocity_arm(fa, arm_a), n);
                 if (speed < -p.restitution_threshold) {
-                    const f3 g_rel = n * (-restitution * gpt.x);
+                    const f3 g_rel = n * (-restitution * g_target);
                     gvb = gvb + g_rel;
                     gva = gva - g_rel;
                     gwb = gwb + cross(arm_b, g_rel);

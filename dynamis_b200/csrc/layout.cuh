@@ -67,6 +67,7 @@ enum Ctl : uint32_t {
     CTL_GJK_PAIRS = 17,      // convex pairs past the centre-axis rejection
     CTL_PROBES = 18,         // separated convex pairs queued for the penetration probe
     CTL_EPA_NEXT = 19,       // next penetrating pair ticket of the EPA kernel
+    CTL_STAGED = 20,         // contacts the narrowphase staged (every contact it found: at most one per pair)
     CTL_COUNT = 32
 };
 
@@ -75,6 +76,7 @@ struct DeviceWorld {
     uint32_t nd;  // dynamic rows (rows [0, nd))
     uint32_t k;   // colliders
     uint32_t e_cap, p_cap, c_cap;
+    uint32_t s_cap;  // the staging set's capacity (the pair stream's: a pair yields at most one contact)
     uint32_t n_cap;  // body rows the per-row buffers hold
     // bodies
     BodyHot* hot;
@@ -119,12 +121,13 @@ struct DeviceWorld {
     float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits
     uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
     uint32_t cell_bits;
-    uint32_t* spill;  // host-mapped: [0] unused, [1] pairs attempted, [2] pairs refused (left by a refusing step)
+    uint32_t* spill;  // host-mapped: [0] unused, [1] pairs attempted, [2] pairs refused (left by a refusing step),
+                      // [3] contacts staged (the largest since the host looked)
     uint32_t* pmaj;  // candidate pairs in emission order (lower, higher collider slot)
     uint32_t* pmin;
-    // narrowphase, its staging set (append order) and the compaction into pair order
+    // narrowphase, its staging set (append order; point stride s_cap) and the compaction into pair order
     ContactSet tmp;
-    uint32_t* cmaj;  // [c_cap] staged contacts' (lower, higher) collider slot, then sorted
+    uint32_t* cmaj;  // [s_cap] staged contacts' (lower, higher) collider slot, then sorted
     uint32_t* cmin;
     uint32_t* cval;  // staged contact of each sorted key
     uint32_t* cmaj_alt;

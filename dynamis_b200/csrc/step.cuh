@@ -729,8 +729,8 @@ __device__ __forceinline__ void narrow_pair(const DeviceWorld& w, const dyn_step
     }
     if (m.count > 0u) {
         uint32_t slot = append_slot(&w.ctl[CTL_APPENDED]);
-        if (slot < w.c_cap) {
-            write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
+        if (slot < w.s_cap) {
+            write_contact(w.tmp, w.s_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
                           w.c_mat[ss], w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine,
                           p.restitution_combine);
         } else {
@@ -1055,10 +1055,10 @@ __global__ void __launch_bounds__(128) k_convex_manifold(DeviceWorld w, dyn_step
         }
         if (m.count > 0u) {
             uint32_t slot = append_slot(&w.ctl[CTL_APPENDED]);
-            if (slot < w.c_cap) {
+            if (slot < w.s_cap) {
                 uint4 fi = w.ident[fr], si = w.ident[sr];
                 bool sensor = (fc.flags & DYN_COLLIDER_SENSOR) != 0u || (sc.flags & DYN_COLLIDER_SENSOR) != 0u;
-                write_contact(w.tmp, w.c_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
+                write_contact(w.tmp, w.s_cap, slot, m, fr, sr, fs, ss, fb, sb, fi.x, si.x, fi.y, si.y, sensor, w.c_mat[fs],
                               w.c_mat[ss], w.c_mat2[fs], w.c_mat2[ss], fc.flags, sc.flags, p.friction_combine,
                               p.restitution_combine);
             } else {
@@ -1079,26 +1079,31 @@ __global__ void __launch_bounds__(128, 4) k_narrow_class(DeviceWorld w, dyn_step
 
 // ---- compaction (compact_scan.wgsl, compact_offsets.wgsl, compact_scatter.wgsl) ----
 // The reference sorts all candidate pairs and compacts the narrowphase output in pair order. Here
-// the pairs stay in emission order; the narrowphase appends its contacts to a staging set, and the
-// stored contacts alone are sorted by (lower, higher) collider slot and gathered. Each pair yields at
-// most one contact, so the contacts come out in the reference's order, for a sort of C keys instead
-// of P. When more contacts arrive than the capacity holds, which ones were stored depends on
-// completion order (the counts stay exact).
+// the pairs stay in emission order; the narrowphase appends its contacts to a staging set as large
+// as the pair stream (a pair yields at most one contact, so every contact found is staged), the
+// staged contacts alone are sorted by (lower, higher) collider slot, and the first c_cap of them in
+// that order are gathered: the contacts and the ones refused past the capacity are the reference's
+// (compact_scatter.wgsl keeps the first in pair order), whatever order the narrowphase finished in.
 __global__ void k_contact_keys(DeviceWorld w) {
-    const uint32_t c = min(w.ctl[CTL_APPENDED], w.c_cap);
+    const uint32_t appended = w.ctl[CTL_APPENDED];
+    const uint32_t staged = min(appended, w.s_cap);
+    const uint32_t c = min(staged, w.c_cap);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         w.counters[DYN_COUNTER_CONTACTS] = c;
+        w.ctl[CTL_STAGED] = staged;
         w.ctl[CTL_CONTACTS] = c;
         w.counters[DYN_COUNTER_BLOCKS] = c;
+        if (staged > c) w.counters[DYN_COUNTER_REFUSED_CONTACTS] += staged - c;
     }
-    GRID_STRIDE(i, c) {
+    GRID_STRIDE(i, staged) {
         const uint4 ids = w.tmp.ids[i];
         w.cmaj[i] = ids.x;
         w.cmin[i] = ids.y;
         w.cval[i] = i;
     }
 }
-__device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi, const ContactSet& to, uint32_t ti, uint32_t cap) {
+__device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi, uint32_t from_cap, const ContactSet& to,
+                                             uint32_t ti, uint32_t cap) {
     uint4 rows = from.rows[fi];
     to.normal[ti] = from.normal[fi];
     to.rows[ti] = rows;
@@ -1108,7 +1113,7 @@ __device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi
     to.extra[ti] = from.extra[fi];
     uint32_t count = rows.z & 0xFFu;
     for (uint32_t p = 0; p < count; ++p) {
-        size_t f = (size_t)p * cap + fi, t = (size_t)p * cap + ti;
+        size_t f = (size_t)p * from_cap + fi, t = (size_t)p * cap + ti;
         to.la[t] = from.la[f];
         to.lb[t] = from.lb[f];
         to.acc[t] = from.acc[f];
@@ -1118,7 +1123,7 @@ __device__ __forceinline__ void copy_contact(const ContactSet& from, uint32_t fi
 __global__ void k_contact_gather(DeviceWorld w) {
     const uint32_t c = w.ctl[CTL_CONTACTS];
     GRID_STRIDE(i, c) {
-        copy_contact(w.tmp, w.cval[i], w.cur, i, w.c_cap);
+        copy_contact(w.tmp, w.cval[i], w.s_cap, w.cur, i, w.c_cap);
         w.matched[i] = 0u;
     }
 }
@@ -1970,6 +1975,8 @@ __global__ void k_sleep(DeviceWorld w, dyn_step_params p) {
             const uint32_t demand = w.counters[DYN_COUNTER_PAIRS];
             if (demand > w.spill[1]) w.spill[1] = demand;
             if (refused != 0u) w.spill[2] = refused;
+            const uint32_t contacts = w.ctl[CTL_STAGED];
+            if (contacts > w.spill[3]) w.spill[3] = contacts;
         }
     }
     GRID_STRIDE(i, w.nd) {

@@ -46,7 +46,8 @@ static const char* kStageNames[ST_COUNT] = {"begin",       "aabb",     "entries"
 // A recorded trajectory for the adjoint (dyn_tape_begin ... dyn_tape_end): checkpoints on the
 // device, the taped segment and the gradient buffers.
 struct Checkpoint {
-    std::vector<void*> bufs;  // device copies, in the order save_checkpoint lists them
+    void* base = nullptr;  // one device block holding the parts save_checkpoint lists, 256-byte aligned
+    size_t bytes = 0;
     uint32_t parity = 0;
 };
 struct TapeHost {
@@ -55,8 +56,12 @@ struct TapeHost {
     uint32_t recorded = 0;  // steps recorded since dyn_tape_begin
     uint32_t reversed = 0;  // of those, the last ones already reversed
     float dt = 0.0f;        // every recorded step's timestep
-    std::vector<Checkpoint> checkpoints;  // checkpoint j: the world before recorded step j * interval
-    Checkpoint end;                       // the world after the last recorded step (kept from the first backward on)
+    // checkpoint j: the world before recorded step j * interval. The blocks, the tape, the gradient
+    // buffers and the graphs stay allocated from one tape to the next (a tape of the same shape
+    // allocates nothing) until the device state goes.
+    std::vector<Checkpoint> checkpoints;
+    uint32_t checkpoint_count = 0;  // of those, the current tape's
+    Checkpoint end;                 // the world after the last recorded step (kept from the first backward on)
     bool have_end = false;
     std::vector<std::vector<uint32_t>> edit_ids;  // each recorded step's queued edits, replayed with it
     std::vector<std::vector<dyn_body_edit_record>> edits;
@@ -87,7 +92,7 @@ struct DeviceState {
     cudaStream_t stream = nullptr;
     DeviceWorld dw{};
     std::vector<void*> allocs;
-    uint32_t* spill_host = nullptr;  // host-mapped mailbox of refused pairs (DeviceWorld::spill)
+    uint32_t* spill_host = nullptr;  // host-mapped mailbox of stream demand (DeviceWorld::spill)
     uint32_t n_cap = 0, k_cap = 0, e_cap = 0, p_cap = 0, c_cap = 0;
     uint32_t id_cap = 0;  // body ids the row_of_id table holds (ids of removed bodies are not reused)
     uint32_t src_cap = 0, vert_cap = 0;
@@ -132,6 +137,8 @@ struct DeviceState {
     float stage_ms[ST_COUNT] = {0};
     TapeHost tape;
 };
+// Frees every buffer and graph of the differentiation (destroy_device; defined with the tape code).
+void free_tape_memory(DeviceState* d);
 
 namespace {
 
@@ -234,7 +241,7 @@ dyn_status ensure_device(dyn_world* w) {
         d->k_cap = std::max(k, w->capacity.colliders);
         d->e_cap = 8u * std::max(d->k_cap, 1u);
         d->p_cap = w->capacity.pairs ? w->capacity.pairs : 16u * std::max(d->k_cap, 64u);
-        d->c_cap = w->capacity.contacts ? w->capacity.contacts : 8u * std::max(d->k_cap, 64u);
+        d->c_cap = w->capacity.contacts ? w->capacity.contacts : 16u * std::max(d->k_cap, 64u);
         d->src_cap = std::max(ns, 1u);
         d->vert_cap = std::max(nv, 1u);
         DeviceWorld& dw = d->dw;
@@ -285,12 +292,13 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.cell_table, (size_t)1 << dw.cell_bits);
         A(dw.pmaj, P);
         A(dw.pmin, P);
-        A(dw.cmaj, C);
-        A(dw.cmin, C);
-        A(dw.cval, C);
-        A(dw.cmaj_alt, C);
-        A(dw.cmin_alt, C);
-        A(dw.cval_alt, C);
+        // the staging set and its sort keys hold every contact the narrowphase finds: one per pair at most
+        A(dw.cmaj, P);
+        A(dw.cmin, P);
+        A(dw.cval, P);
+        A(dw.cmaj_alt, P);
+        A(dw.cmin_alt, P);
+        A(dw.cval_alt, P);
         A(dw.np_list, (PC_COUNT + 1) * (size_t)P);
         A(dw.epa_list, P);
         A(dw.epa_simplex, 4 * (size_t)P);
@@ -327,7 +335,8 @@ dyn_status ensure_device(dyn_world* w) {
         d->lookback_words = (size_t)8 * max_tiles * 256;
         A(d->lookback, d->lookback_words);
 #undef A
-        if ((st = alloc_contacts(w, d, &dw.tmp, C))) return st;
+        if ((st = alloc_contacts(w, d, &dw.tmp, P))) return st;
+        dw.s_cap = P;
         if ((st = alloc_contacts(w, d, &dw.cur, C))) return st;
         if ((st = alloc_contacts(w, d, &dw.arc, C))) return st;
         dw.e_cap = E;
@@ -707,7 +716,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     mark(ST_COMPACT);
     k_contact_keys<<<blocks_for(d, C, 256), 256, 0, s>>>(dw);
     const uint32_t words = key_words(std::max(dw.k, 1u));
-    record_sort(d, s, dw.cmaj, dw.cmin, dw.cval, dw.cmaj_alt, dw.cmin_alt, dw.cval_alt, dw.ctl + CTL_CONTACTS, 0, C, words,
+    record_sort(d, s, dw.cmaj, dw.cmin, dw.cval, dw.cmaj_alt, dw.cmin_alt, dw.cval_alt, dw.ctl + CTL_STAGED, 0, dw.s_cap, words,
                 words);
     k_contact_gather<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
     // the solver blocks (target speeds, row claims) beside the identity, islands and wake passes:
@@ -1014,6 +1023,7 @@ void destroy_device(dyn_world* w) {
     // the caller's stream may already be gone: wait for the whole device instead
     cudaDeviceSynchronize();
     release_graphs(d);
+    free_tape_memory(d);
     for (cudaEvent_t e : d->events) cudaEventDestroy(e);
     for (void* p : d->allocs) cudaFree(p);
     if (d->spill_host) cudaFreeHost(d->spill_host);
@@ -1179,7 +1189,26 @@ dyn_status widen_pair_stream(dyn_world* w) {
                      {reinterpret_cast<void**>(&dw.probe_list), P * sizeof(uint32_t), nullptr},
                      {reinterpret_cast<void**>(&dw.probe_data), 6 * P * sizeof(float4), nullptr},
                      {reinterpret_cast<void**>(&dw.hit_list), P * sizeof(uint32_t), nullptr},
-                     {reinterpret_cast<void**>(&dw.hit_data), 2 * P * sizeof(float4), nullptr}};
+                     {reinterpret_cast<void**>(&dw.hit_data), 2 * P * sizeof(float4), nullptr},
+                     // the staging set of the narrowphase's contacts (one per pair at most) and its sort
+                     {reinterpret_cast<void**>(&dw.tmp.normal), P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.rows), P * sizeof(uint4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.mat), P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.ids), P * sizeof(uint4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.ids2), P * sizeof(uint4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.extra), P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.la), 4 * P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.lb), 4 * P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.acc), 4 * P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.tmp.pos), 4 * P * sizeof(float4), nullptr},
+                     {reinterpret_cast<void**>(&dw.cmaj), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.cmin), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.cval), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.cmaj_alt), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.cmin_alt), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&dw.cval_alt), P * sizeof(uint32_t), nullptr},
+                     {reinterpret_cast<void**>(&d->lookback),
+                      (size_t)8 * std::max(div_up(std::max<size_t>(d->e_cap, P), kSortTile), 1u) * 256 * sizeof(uint32_t), nullptr}};
     for (Buffer& b : list) {
         if (cudaMalloc(&b.fresh, b.bytes) != cudaSuccess) {
             for (Buffer& f : list) if (f.fresh) cudaFree(f.fresh);
@@ -1195,8 +1224,98 @@ dyn_status widen_pair_stream(dyn_world* w) {
         d->allocs.push_back(b.fresh);
         *b.slot = b.fresh;
     }
-    d->p_cap = dw.p_cap = (uint32_t)P;
+    d->p_cap = dw.p_cap = dw.s_cap = (uint32_t)P;
+    d->lookback_words = (size_t)8 * std::max(div_up(std::max<size_t>(d->e_cap, P), kSortTile), 1u) * 256;
     release_graphs(d);  // the graphs hold the old buffers and capacity
+    return DYN_OK;
+}
+
+// The contact stream widens like the pair stream (crates/dynamis-broadphase/src/capacity.rs:27-90
+// grows every stream from its demand): once a step staged more contacts than the stream holds, or
+// more than three quarters of it, the next dyn_step waits for the queued steps and replaces the contact sets
+// and the solver's per-contact buffers with ones for twice the demand (at least twice the stream).
+// The archived set, which the next step's relay reads, is copied over with the new point stride.
+// Not while a tape is recording: its slots and checkpoints keep the stream's layout.
+constexpr uint64_t kMaxContactCapacity = 1ull << 26;
+dyn_status widen_contact_stream(dyn_world* w) {
+    DeviceState* d = w->dev;
+    volatile uint32_t* mail = d->spill_host;
+    if (!mail || d->c_cap >= kMaxContactCapacity || d->tape.active) return DYN_OK;
+    if (mail[3] <= d->c_cap - d->c_cap / 4) return DYN_OK;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    const uint64_t demand = mail[3];
+    mail[3] = 0u;
+    uint64_t want = std::max<uint64_t>(2ull * demand, 2ull * d->c_cap);
+    want = std::min<uint64_t>((want + 1023u) & ~1023ull, kMaxContactCapacity);
+    if (want <= d->c_cap) return DYN_OK;
+    const size_t C = (size_t)want, old = d->c_cap;
+    DeviceWorld& dw = d->dw;
+    ContactSet fresh_cur{}, fresh_arc{};
+    SolverRows fresh_rows{};
+    uint32_t *matched = nullptr, *cowner = nullptr;
+    std::vector<void*> made;
+    auto grab = [&](auto** ptr, size_t bytes) -> bool {
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) return false;
+        made.push_back(q);
+        *ptr = static_cast<std::remove_reference_t<decltype(**ptr)>*>(q);
+        return true;
+    };
+    bool ok = true;
+    for (ContactSet* set : {&fresh_cur, &fresh_arc}) {
+        ok = ok && grab(&set->normal, C * sizeof(float4)) && grab(&set->rows, C * sizeof(uint4)) &&
+             grab(&set->mat, C * sizeof(float4)) && grab(&set->ids, C * sizeof(uint4)) && grab(&set->ids2, C * sizeof(uint4)) &&
+             grab(&set->extra, C * sizeof(float4)) && grab(&set->la, 4 * C * sizeof(float4)) &&
+             grab(&set->lb, 4 * C * sizeof(float4)) && grab(&set->acc, 4 * C * sizeof(float4)) &&
+             grab(&set->pos, 4 * C * sizeof(float4));
+    }
+    ok = ok && grab(&fresh_rows.arm_a, 4 * C * sizeof(float4)) && grab(&fresh_rows.arm_b, 4 * C * sizeof(float4)) &&
+         grab(&fresh_rows.masses, 4 * C * sizeof(float4)) && grab(&fresh_rows.tangent1, C * sizeof(float4)) &&
+         grab(&fresh_rows.tangent2, C * sizeof(float4)) && grab(&matched, C * sizeof(uint32_t)) &&
+         grab(&cowner, C * sizeof(uint32_t));
+    if (!ok) {
+        for (void* q : made) cudaFree(q);
+        (void)cudaGetLastError();  // out of memory: keep the stream, keep counting refusals
+        return DYN_OK;
+    }
+    for (void* q : made) DYN_CUDA(cudaMemsetAsync(q, 0, 1, d->stream));  // (contents are written before read)
+    // the set the next step archives from: dw.arc at parity 0, dw.cur at parity 1 (record_step swaps)
+    const ContactSet& archived = d->parity == 0u ? dw.arc : dw.cur;
+    ContactSet& target = d->parity == 0u ? fresh_arc : fresh_cur;
+    const uint32_t count = std::min<uint32_t>((uint32_t)old, 0xFFFFFFFFu);
+    auto copy = [&](void* to, const void* from, size_t bytes) -> cudaError_t {
+        return cudaMemcpyAsync(to, from, bytes, cudaMemcpyDeviceToDevice, d->stream);
+    };
+    DYN_CUDA(copy(target.normal, archived.normal, count * sizeof(float4)));
+    DYN_CUDA(copy(target.rows, archived.rows, count * sizeof(uint4)));
+    DYN_CUDA(copy(target.mat, archived.mat, count * sizeof(float4)));
+    DYN_CUDA(copy(target.ids, archived.ids, count * sizeof(uint4)));
+    DYN_CUDA(copy(target.ids2, archived.ids2, count * sizeof(uint4)));
+    DYN_CUDA(copy(target.extra, archived.extra, count * sizeof(float4)));
+    for (size_t pt = 0; pt < 4; ++pt) {  // point slot pt of contact i sits at pt * capacity + i
+        DYN_CUDA(copy(target.la + pt * C, archived.la + pt * old, count * sizeof(float4)));
+        DYN_CUDA(copy(target.lb + pt * C, archived.lb + pt * old, count * sizeof(float4)));
+        DYN_CUDA(copy(target.acc + pt * C, archived.acc + pt * old, count * sizeof(float4)));
+        DYN_CUDA(copy(target.pos + pt * C, archived.pos + pt * old, count * sizeof(float4)));
+    }
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    std::vector<void*> stale = {dw.cur.normal, dw.cur.rows, dw.cur.mat, dw.cur.ids, dw.cur.ids2, dw.cur.extra, dw.cur.la,
+                                dw.cur.lb, dw.cur.acc, dw.cur.pos, dw.arc.normal, dw.arc.rows, dw.arc.mat, dw.arc.ids,
+                                dw.arc.ids2, dw.arc.extra, dw.arc.la, dw.arc.lb, dw.arc.acc, dw.arc.pos, dw.srows.arm_a,
+                                dw.srows.arm_b, dw.srows.masses, dw.srows.tangent1, dw.srows.tangent2, dw.matched, dw.cowner};
+    for (void* q : stale) {
+        auto it = std::find(d->allocs.begin(), d->allocs.end(), q);
+        if (it != d->allocs.end()) d->allocs.erase(it);
+        DYN_CUDA(cudaFree(q));
+    }
+    for (void* q : made) d->allocs.push_back(q);
+    dw.cur = fresh_cur;
+    dw.arc = fresh_arc;
+    dw.srows = fresh_rows;
+    dw.matched = matched;
+    dw.cowner = cowner;
+    d->c_cap = dw.c_cap = (uint32_t)C;
+    release_graphs(d);
     return DYN_OK;
 }
 
@@ -1219,6 +1338,7 @@ static dyn_status step_once(dyn_world* w, float dt, bool taped) {
     const uint32_t slot = d->inflight_next;
     if (d->inflight_used[slot]) DYN_CUDA(cudaEventSynchronize(d->inflight[slot]));
     if ((st = widen_pair_stream(w))) return st;
+    if ((st = widen_contact_stream(w))) return st;
     uint32_t parity = d->parity;
     const TapeView* tape = taped ? &d->tape.view : nullptr;
     if (w->timing) {
@@ -1281,18 +1401,29 @@ static std::vector<CheckpointPart> checkpoint_parts(DeviceState* d) {
             {arc.la, 4 * C * sizeof(float4)},     {arc.lb, 4 * C * sizeof(float4)},  {arc.acc, 4 * C * sizeof(float4)},
             {arc.pos, 4 * C * sizeof(float4)}};
 }
+static size_t checkpoint_bytes(const std::vector<CheckpointPart>& parts) {
+    size_t bytes = 0;
+    for (const CheckpointPart& part : parts) bytes += (part.bytes + 255u) & ~(size_t)255u;
+    return bytes;
+}
 static void free_checkpoint(Checkpoint* c) {
-    for (void* p : c->bufs) cudaFree(p);
-    c->bufs.clear();
+    if (c->base) cudaFree(c->base);
+    c->base = nullptr;
+    c->bytes = 0;
 }
 static dyn_status save_checkpoint(dyn_world* w, Checkpoint* c) {
     DeviceState* d = w->dev;
-    free_checkpoint(c);
-    for (const CheckpointPart& part : checkpoint_parts(d)) {
-        void* p = nullptr;
-        DYN_CUDA(cudaMalloc(&p, part.bytes));
-        c->bufs.push_back(p);
-        DYN_CUDA(cudaMemcpyAsync(p, part.ptr, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
+    const std::vector<CheckpointPart> parts = checkpoint_parts(d);
+    const size_t bytes = checkpoint_bytes(parts);
+    if (c->bytes != bytes) {
+        free_checkpoint(c);
+        DYN_CUDA(cudaMalloc(&c->base, bytes));
+        c->bytes = bytes;
+    }
+    char* at = static_cast<char*>(c->base);
+    for (const CheckpointPart& part : parts) {
+        DYN_CUDA(cudaMemcpyAsync(at, part.ptr, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
+        at += (part.bytes + 255u) & ~(size_t)255u;
     }
     c->parity = d->parity;
     return DYN_OK;
@@ -1301,9 +1432,11 @@ static dyn_status restore_checkpoint(dyn_world* w, const Checkpoint& c) {
     DeviceState* d = w->dev;
     DYN_CUDA(cudaStreamSynchronize(d->stream));
     d->parity = c.parity;  // before listing the parts: the archived set follows the parity
-    std::vector<CheckpointPart> parts = checkpoint_parts(d);
-    for (size_t i = 0; i < parts.size() && i < c.bufs.size(); ++i)
-        DYN_CUDA(cudaMemcpyAsync(parts[i].ptr, c.bufs[i], parts[i].bytes, cudaMemcpyDeviceToDevice, d->stream));
+    const char* at = static_cast<const char*>(c.base);
+    for (const CheckpointPart& part : checkpoint_parts(d)) {
+        DYN_CUDA(cudaMemcpyAsync(part.ptr, at, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
+        at += (part.bytes + 255u) & ~(size_t)255u;
+    }
     return DYN_OK;
 }
 static void free_tape_buffers(TapeHost& t) {
@@ -1319,8 +1452,20 @@ static void free_adjoint(TapeHost& t) {
     t.grad_staging = nullptr;
     t.patch_rows = t.patch_masks = nullptr;
 }
+// Ends the current tape; its memory and graphs stay for the next one.
 static void release_tape(DeviceState* d) {
     TapeHost& t = d->tape;
+    t.checkpoint_count = 0;
+    t.have_end = false;
+    t.segment = -1;
+    t.edit_ids.clear();
+    t.edits.clear();
+    t.active = false;
+    t.recorded = t.reversed = 0;
+}
+void dyn::free_tape_memory(DeviceState* d) {
+    TapeHost& t = d->tape;
+    release_tape(d);
     for (auto& e : t.taped) {
         if (e) cudaGraphExecDestroy(e);
         e = nullptr;
@@ -1330,13 +1475,8 @@ static void release_tape(DeviceState* d) {
     for (Checkpoint& c : t.checkpoints) free_checkpoint(&c);
     t.checkpoints.clear();
     free_checkpoint(&t.end);
-    t.have_end = false;
     free_tape_buffers(t);
     free_adjoint(t);
-    t.edit_ids.clear();
-    t.edits.clear();
-    t.active = false;
-    t.recorded = t.reversed = 0;
 }
 template <typename T>
 static dyn_status tape_alloc(dyn_world* w, std::vector<void*>& list, T** out, size_t count) {
@@ -1350,8 +1490,21 @@ static dyn_status tape_alloc(dyn_world* w, std::vector<void*>& list, T** out, si
 static dyn_status alloc_tape_buffers(dyn_world* w) {
     DeviceState* d = w->dev;
     TapeHost& t = d->tape;
-    if (!t.tape_allocs.empty()) return DYN_OK;
     const dyn_step_params& p = d->params;
+    if (!t.tape_allocs.empty()) {
+        const TapeView& v = t.view;
+        if (v.steps >= t.interval && v.substeps == p.substeps && v.iterations == p.solve_iterations &&
+            v.piterations == p.position_iterations && v.n == d->n_cap && v.c == d->c_cap)
+            return DYN_OK;
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        free_tape_buffers(t);
+        for (auto& e : t.taped) {
+            if (e) cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+        if (t.back) cudaGraphExecDestroy(t.back);
+        t.back = nullptr;
+    }
     TapeView& v = t.view;
     v.steps = t.interval;
     v.substeps = p.substeps;
@@ -1362,7 +1515,9 @@ static dyn_status alloc_tape_buffers(dyn_world* w) {
     const size_t S = v.steps, N = v.n, C = v.c, K = v.substeps;
     dyn_status st;
 #define TA(field, count) if ((st = tape_alloc(w, t.tape_allocs, &v.field, (count)))) return st
-    TA(slot, 1);
+    uint32_t* slot = nullptr;
+    if ((st = tape_alloc(w, t.tape_allocs, &slot, 1))) return st;
+    v.slot = slot;
     TA(counts, S);
     TA(rows, S * C);
     TA(normal, S * C);
@@ -1406,9 +1561,14 @@ static dyn_status alloc_adjoint(dyn_world* w) {
     AA(a.acc_flip, 1);
     AA(a.g_ra, 4 * C);
     AA(a.g_rb, 4 * C);
-    AA(a.g_m, 4 * C);
+    AA(a.g_m, 4 * C);  // float2
     AA(a.g_pt, 4 * C);
     AA(a.g_param, C);
+    AA(a.t_arm_a, 4 * C);
+    AA(a.t_arm_b, 4 * C);
+    AA(a.t_mass, 4 * C);
+    AA(a.t_tan1, C);
+    AA(a.t_tan2, C);
     AA(a.g_mu, C);
     AA(t.grad_staging, N);
     AA(t.patch_rows, N);
@@ -1427,9 +1587,11 @@ static void record_backward_step(dyn_world* w, cudaStream_t s) {
     const uint32_t n = std::max(d->dw.n, 1u);
     const uint32_t C = d->c_cap;
     const uint32_t rows_grid = blocks_for(d, n, 256), contact_grid = blocks_for(d, C, 128);
+    const uint32_t quad_grid = blocks_for(d, 4 * C, 128);  // a quad of lanes per contact block
     k_adj_begin<<<1, 32, 0, s>>>(t, a);
     k_adj_clear<<<blocks_for(d, std::max(4 * C, n), 256), 256, 0, s>>>(t, a, n);
     for (int32_t k = (int32_t)p.substeps - 1; k >= 0; --k) {
+        k_adj_terms<<<contact_grid, 128, 0, s>>>(t, a, (uint32_t)k);
         const uint32_t P = p.position_iterations;
         if (P > 0) {
             k_adj_prow<<<rows_grid, 256, 0, s>>>(t, a, n, (uint32_t)k, P - 1, false, true);
@@ -1440,7 +1602,7 @@ static void record_backward_step(dyn_world* w, cudaStream_t s) {
         }
         k_adj_advance<<<rows_grid, 256, 0, s>>>(t, a, n, p, (uint32_t)k);
         for (int32_t it = (int32_t)p.solve_iterations - 1; it >= 0; --it) {
-            k_adj_solve<<<contact_grid, 128, 0, s>>>(t, a, p, (uint32_t)k, (uint32_t)it);
+            k_adj_solve<<<quad_grid, 128, 0, s>>>(t, a, p, (uint32_t)k, (uint32_t)it);
             k_adj_vmerge<<<rows_grid, 256, 0, s>>>(a, n);
         }
         if (k == 0) k_adj_warm<<<contact_grid, 128, 0, s>>>(t, a);
@@ -1560,9 +1722,10 @@ DYN_API dyn_status dyn_step(dyn_world* w, float dt) {
         }
         if (w->rows_dirty && !w->raw_rows) return fail(w, DYN_ERR_INVALID, "dyn_step: the scene changed while recording");
         if (t.recorded > 0 && t.recorded % t.interval == 0u) {
-            t.checkpoints.emplace_back();
-            dyn_status st = save_checkpoint(w, &t.checkpoints.back());
+            if (t.checkpoints.size() <= t.checkpoint_count) t.checkpoints.emplace_back();
+            dyn_status st = save_checkpoint(w, &t.checkpoints[t.checkpoint_count]);
             if (st) return st;
+            t.checkpoint_count += 1;
         }
         t.edit_ids.push_back(w->edit_ids);
         t.edits.push_back(w->edits);
@@ -1598,12 +1761,13 @@ DYN_API dyn_status dyn_tape_begin(dyn_world* w, uint32_t checkpoint_interval) {
     t.interval = checkpoint_interval;
     t.active = true;
     DYN_CUDA(cudaStreamSynchronize(d->stream));
-    t.checkpoints.emplace_back();
-    dyn_status st = save_checkpoint(w, &t.checkpoints.back());
+    if (t.checkpoints.empty()) t.checkpoints.emplace_back();
+    dyn_status st = save_checkpoint(w, &t.checkpoints[0]);
     if (st) {
         release_tape(d);
         return st;
     }
+    t.checkpoint_count = 1;
     DYN_CUDA(cudaStreamSynchronize(d->stream));
     return DYN_OK;
 }

@@ -367,12 +367,14 @@ def tower_world(seed: int, levels: int = 8, footprint: int = 4, distance: float 
     return Scene(bodies, colliders, [], f"tower_{n}")
 
 
-def sphere_launch(scene_seed: int, speed_range=(3.0, 8.0)) -> tuple:
-    """The sphere's launch of tower_world(scene_seed): a speed drawn from U(3, 8) m/s along the
-    heading from the sphere to the tower's axis."""
-    rng = np.random.default_rng(scene_seed + 7919)
-    speed = rng.uniform(*speed_range)
-    return speed
+def sphere_launches(scene: Scene, states: np.ndarray, rows: np.ndarray, seed: int = 5) -> np.ndarray:
+    """Launch velocities of the spheres at body rows `rows` (states in row order): a speed drawn from
+    U(3, 8) m/s toward the vertical axis of the sphere's own world (x = z = 0)."""
+    rng = np.random.default_rng(seed + 7919)
+    direction = -states["position"][rows].astype(np.float64)
+    direction[:, 1] = 0.0
+    direction /= np.linalg.norm(direction, axis=1, keepdims=True)
+    return (direction * rng.uniform(3.0, 8.0, len(rows))[:, None]).astype(np.float32)
 
 
 def differentiable_towers(worlds: int = 256, seed: int = 5, levels: int = 8, footprint: int = 4) -> Scene:
@@ -398,4 +400,5 @@ WORKLOADS = {
     "hanging_chains_131072": lambda: hanging_chains(64, 64, 32),
     "batched_worlds_256": lambda: batched_worlds(256),
     "batched_worlds_4096": lambda: batched_worlds(4096),
+    "differentiable_towers_256": lambda: differentiable_towers(256),
 }
