@@ -16,7 +16,10 @@
 // Forward, a taped step (record_step with a tape) snapshots what the reverse needs into one slot of
 // the tape: the contact set with its target speeds and relay sources, the body rows at each
 // substep's start and at the step's end, the velocities and accumulated impulses at each velocity
-// iteration's start, and the resolution and contribution counts of each position iteration.
+// iteration's start, and the resolution and contribution counts of each position iteration. The
+// iteration snapshots are written by the forward kernels themselves (k_solve, k_position_fused,
+// k_papply_last through DeviceWorld::tape), and only for the rows and contacts a contact block
+// solves: the reverse reads no other entry of them.
 // Backward, one captured graph reverses one step: it takes the slot below the tape's counter and
 // runs the reverse of every pass in reverse order, one thread per contact block or body row, the
 // same decomposition as the forward; contact threads add their contributions to shared rows with
@@ -104,7 +107,8 @@ struct AdjView {
     float4* t_arm_b;   // [4c] arm on the second body
     float4* t_mass;    // [4c] tangent-1 mass, tangent-2 mass, target speed
     float4* t_tan1;    // [c] tangent 1
-    float4* t_tan2;    // [c] tangent 2
+    float4* t_tan2;    // [c] tangent 2, the block's kBlock* flags (w, as bits)
+    float4* t_body;    // [c] inverse mass of the first and second body, their inverse inertia scalars (0 when inert)
     float* g_mu;       // [c] d loss / d contact friction
     uint32_t* status;
 };
@@ -211,6 +215,10 @@ __device__ __forceinline__ void tape_block(const TapeView& t, uint32_t s, uint32
         b->m2[p] = momentum_mass_arms(b->sf, b->ss, b->ra[p], b->rb[p], b->t2) * b->count_f;
     }
 }
+// What k_adj_terms found of a contact block for one substep (AdjView::t_tan2.w): the velocity
+// iterations reverse it (resolves, supported, not both bodies inert), which body is inert, and
+// whether the position passes correct it (resolves, hard contact).
+constexpr uint32_t kBlockSolve = 1u, kBlockInertFirst = 2u, kBlockInertSecond = 4u, kBlockPosition = 8u;
 __device__ __forceinline__ bool block_supported(const TapeView& t, uint32_t s, uint32_t i) {
     const float4 mat = t.mat[t.cs(s) + i];
     return mat.z <= 0.0f && mat.x == 0.0f && mat.y == 0.0f;
@@ -247,33 +255,6 @@ __global__ void k_tape_hot(DeviceWorld w, TapeView t, uint32_t k) {
     const uint32_t s = *t.slot;
     BodyHot* dst = t.hot + ((size_t)s * (t.substeps + 1) + k) * t.n;
     GRID_STRIDE(i, w.n) dst[i] = w.hot[i];
-}
-// Velocities and accumulated impulses at the start of velocity iteration `it` of substep `k`.
-__global__ void k_tape_iteration(DeviceWorld w, TapeView t, uint32_t k, uint32_t it) {
-    const uint32_t s = *t.slot;
-    float4* vel = t.vel + ((size_t)s * t.substeps * t.iterations + (size_t)k * t.iterations + it) * 2 * t.n;
-    float4* acc = t.acc + ((size_t)s * t.substeps * t.iterations + (size_t)k * t.iterations + it) * 4 * t.c;
-    const uint32_t count = w.ctl[CTL_CONTACTS];
-    const uint32_t total = max(w.n, count);
-    GRID_STRIDE(i, total) {
-        if (i < w.n) {
-            vel[i] = w.hot[i].vel;
-            vel[t.n + i] = w.hot[i].ang;
-        }
-        if (i < count) {
-            for (uint32_t p = 0; p < 4u; ++p) acc[(size_t)p * t.c + i] = w.cur.acc[(size_t)p * w.c_cap + i];
-        }
-    }
-}
-// The resolution a position iteration starts from and the contributions it counted (run between
-// k_position and k_papply).
-__global__ void k_tape_position(DeviceWorld w, TapeView t, uint32_t k, uint32_t it) {
-    const uint32_t s = *t.slot;
-    const size_t o = ((size_t)s * t.substeps * t.piterations + (size_t)k * t.piterations + it) * t.n;
-    GRID_STRIDE(i, w.n) {
-        t.res[o + i] = w.resolution[i];
-        t.cnt[o + i] = w.contributions[i];
-    }
 }
 __global__ void k_tape_advance(TapeView t) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *t.slot += 1u;
@@ -317,6 +298,7 @@ __global__ void k_adj_clear(TapeView t, AdjView a, uint32_t n) {
 // orientation's renormalisation.
 __global__ void k_adj_prow(TapeView t, AdjView a, uint32_t n, uint32_t k, uint32_t it, bool fold, bool valid) {
     const uint32_t s = *t.slot;
+    const BodyHot* start = t.hot_at(s, k);
     const BodyHot* end = t.hot_at(s, k + 1);
     GRID_STRIDE(i, n) {
         if (fold) {
@@ -326,7 +308,8 @@ __global__ void k_adj_prow(TapeView t, AdjView a, uint32_t n, uint32_t k, uint32
             a.gres_acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         if (!valid) continue;
-        const uint32_t cnt = t.cnt[t.pslot(s, k, it) + i];
+        // a row no contact block claimed (aux.z) has no count on the tape and moved in no iteration
+        const uint32_t cnt = start[i].aux.z == 0u ? 0u : t.cnt[t.pslot(s, k, it) + i];
         const BodyHot& h = end[i];
         if (cnt == 0u || !row_live(h)) {
             a.gsum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -348,14 +331,22 @@ __global__ void k_adj_pcontact(TapeView t, AdjView a, dyn_step_params p, uint32_
     const BodyHot* hot = t.hot_at(s, k);
     const float4* res = t.res + t.pslot(s, k, it);
     GRID_STRIDE(i, count) {
+        const uint32_t flags = __float_as_uint(a.t_tan2[i].w);
+        if (!(flags & kBlockPosition)) continue;
         const uint4 r = t.rows[t.cs(s) + i];
-        if (!resolves(r)) continue;
-        const float4 mat = t.mat[t.cs(s) + i];
-        if (mat.z > 0.0f) continue;
-        const BodyHot& ha = hot[r.x];
-        const BodyHot& hb = hot[r.y];
-        const float ima = row_live(ha) ? ha.pos.w : 0.0f;
-        const float imb = row_live(hb) ? hb.pos.w : 0.0f;
+        // a live row's inverse mass, 0 for an inert one (k_adj_terms, from the same rows; the blocks
+        // the velocity iterations do not reverse read theirs)
+        float ima, imb;
+        if (flags & kBlockSolve) {
+            const float4 body = a.t_body[i];
+            ima = body.x;
+            imb = body.y;
+        } else {
+            const BodyHot& ha = hot[r.x];
+            const BodyHot& hb = hot[r.y];
+            ima = row_live(ha) ? ha.pos.w : 0.0f;
+            imb = row_live(hb) ? hb.pos.w : 0.0f;
+        }
         const f3 normal = xyz(t.normal[t.cs(s) + i]);
         const float resolved = dot(normal, xyz(res[r.y]) - xyz(res[r.x]));
         const uint32_t pc = r.z & 0xFFu;
@@ -431,16 +422,32 @@ __global__ void k_adj_advance(TapeView t, AdjView a, uint32_t n, dyn_step_params
 
 // The pose-only terms of substep `k`'s contact blocks (k_solve_prepare's), once for all of the
 // substep's reversed iterations.
+// Also the block's flags and its bodies' inverse masses and inverse inertia scalars (isotropic bodies:
+// the world inverse inertia is that scalar times the identity), so that the iterations read no body rows.
 __global__ void k_adj_terms(TapeView t, AdjView a, uint32_t k) {
     const uint32_t s = *t.slot;
     const uint32_t count = t.counts[s];
     GRID_STRIDE(i, count) {
         const uint4 r = t.rows[t.cs(s) + i];
-        if (!resolves(r) || !block_supported(t, s, i)) continue;
+        uint32_t flags = 0u;
+        if (resolves(r) && t.mat[t.cs(s) + i].z <= 0.0f) flags |= kBlockPosition;
+        if (!resolves(r)) {
+            a.t_tan2[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(flags));
+            continue;
+        }
+        if (!block_supported(t, s, i)) {
+            atomicOr(a.status, DYN_STATUS_ADJOINT_UNSUPPORTED);
+            a.t_tan2[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(flags));
+            continue;
+        }
         TapeBlock b;
         tape_block(t, s, k, i, r, nullptr, &b);
+        if (!(b.inert_f && b.inert_s)) flags |= kBlockSolve;
+        if (b.inert_f) flags |= kBlockInertFirst;
+        if (b.inert_s) flags |= kBlockInertSecond;
+        a.t_body[i] = make_float4(b.pf.inverse_mass, b.ps.inverse_mass, b.pf.ii0.x, b.ps.ii0.x);
         a.t_tan1[i] = mk4(b.t1, 0.0f);
-        a.t_tan2[i] = mk4(b.t2, 0.0f);
+        a.t_tan2[i] = mk4(b.t2, __uint_as_float(flags));
 #pragma unroll
         for (uint32_t q = 0; q < 4u; ++q) if (q < b.count) {
             const size_t o = (size_t)q * t.c + i;
@@ -480,7 +487,7 @@ __device__ __forceinline__ float quad_sum(float v, unsigned mask) {
 __device__ __forceinline__ f3 quad_sum3(f3 v, unsigned mask) {
     return mk3(quad_sum(v.x, mask), quad_sum(v.y, mask), quad_sum(v.z, mask));
 }
-__global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_step_params p, uint32_t k, uint32_t it) {
+__global__ void __launch_bounds__(128, 7) k_adj_solve(TapeView t, AdjView a, dyn_step_params p, uint32_t k, uint32_t it) {
     const uint32_t s = *t.slot;
     const uint32_t count = t.counts[s];
     const float4* vel = t.vel_at(s, k, it);
@@ -491,27 +498,32 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
     const uint32_t quads = (gridDim.x * blockDim.x) >> 2;
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; i < count; i += quads) {
         // every lane of a quad takes the same branches up to the point work
+        const float4 tan2 = a.t_tan2[i];
+        const uint32_t flags = __float_as_uint(tan2.w);
+        if (!(flags & kBlockSolve)) continue;
         const uint4 r = t.rows[t.cs(s) + i];
-        if (!resolves(r)) continue;
-        if (!block_supported(t, s, i)) {
-            if (q == 0u) atomicOr(a.status, DYN_STATUS_ADJOINT_UNSUPPORTED);
-            continue;
-        }
-        TapeBlock b;
-        tape_block_bodies(t, s, k, i, r, vel, &b);
-        if (b.inert_f && b.inert_s) continue;
-        const f3 dva = b.inert_f ? s3(0.0f) : xyz(a.gv[r.x]);
-        const f3 dwa = b.inert_f ? s3(0.0f) : xyz(a.gw[r.x]);
-        const f3 dvb = b.inert_s ? s3(0.0f) : xyz(a.gv[r.y]);
-        const f3 dwb = b.inert_s ? s3(0.0f) : xyz(a.gw[r.y]);
-        const f3 Wa = dbody_iinv(b.pf, dwa);
-        const f3 Wb = dbody_iinv(b.ps, dwb);
-        const float ima = b.pf.inverse_mass, imb = b.ps.inverse_mass;
+        const bool inert_f = (flags & kBlockInertFirst) != 0u, inert_s = (flags & kBlockInertSecond) != 0u;
+        const float4 body = a.t_body[i];
+        const float ima = body.x, imb = body.y;
+        // the bodies as the block saw them: only the velocities are read (dbody_iinv of an isotropic
+        // body is its scalar times the vector)
+        DBody pf, ps;
+        pf.velocity = xyz(vel[r.x]);
+        pf.angular_velocity = xyz(vel[t.n + r.x]);
+        ps.velocity = xyz(vel[r.y]);
+        ps.angular_velocity = xyz(vel[t.n + r.y]);
+        const f3 dva = inert_f ? s3(0.0f) : xyz(a.gv[r.x]);
+        const f3 dwa = inert_f ? s3(0.0f) : xyz(a.gw[r.x]);
+        const f3 dvb = inert_s ? s3(0.0f) : xyz(a.gv[r.y]);
+        const f3 dwb = inert_s ? s3(0.0f) : xyz(a.gw[r.y]);
+        const f3 Wa = dwa * body.z;
+        const f3 Wb = dwb * body.w;
         f3 bva = s3(0.0f), bwa = s3(0.0f), bvb = s3(0.0f), bwb = s3(0.0f);
         float g_ima = 0.0f, g_imb = 0.0f, g_sa = 0.0f, g_sb = 0.0f, g_mu = 0.0f;
-        if (q < b.count) {
-            const f3 n = b.normal, t1 = xyz(a.t_tan1[i]), t2 = xyz(a.t_tan2[i]);
-            const float mu = b.friction;
+        if (q < (r.z & 0xFFu)) {
+            const float4 nf = t.normal[t.cs(s) + i];
+            const f3 n = xyz(nf), t1 = xyz(a.t_tan1[i]), t2 = xyz(tan2);
+            const float mu = nf.w;
             const size_t o = (size_t)q * t.c + i;
             const float4 arm_a = a.t_arm_a[o], arm_b = a.t_arm_b[o], masses = a.t_mass[o];
             const f3 ra = xyz(arm_a), rb = xyz(arm_b);
@@ -519,7 +531,7 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
             const float4 acc = accs[o];
             const float an = acc.x, at1 = acc.y, at2 = acc.z;
             // forward (solve_block, hard contact)
-            const f3 rel = point_velocity_arm(b.ps, rb) - point_velocity_arm(b.pf, ra);
+            const f3 rel = point_velocity_arm(ps, rb) - point_velocity_arm(pf, ra);
             const float ns = dot(rel, n);
             const float delta = (target - ns) / nm;
             const float an1 = wmax(0.0f, an + delta);
@@ -593,8 +605,8 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
             bva = -g_rel;
             bwb = cross(rb, g_rel);
             bwa = -cross(ra, g_rel);
-            grb = grb + cross(g_rel, b.ps.angular_velocity);
-            gra = gra - cross(g_rel, b.pf.angular_velocity);
+            grb = grb + cross(g_rel, ps.angular_velocity);
+            gra = gra - cross(g_rel, pf.angular_velocity);
             gacc[o] = make_float4(g_an0, g_at10, g_at20, 0.0f);
             float4 x = a.g_ra[o];
             a.g_ra[o] = make_float4(x.x + gra.x, x.y + gra.y, x.z + gra.z, x.w + g_nm);
@@ -613,11 +625,11 @@ __global__ void __launch_bounds__(128) k_adj_solve(TapeView t, AdjView a, dyn_st
         g_sb = quad_sum(g_sb, mask);
         g_mu = quad_sum(g_mu, mask);
         if (q == 0u) {
-            if (!b.inert_f) {
+            if (!inert_f) {
                 atomic_add3(&a.gv_acc[r.x], bva);
                 atomic_add3(&a.gw_acc[r.x], bwa);
             }
-            if (!b.inert_s) {
+            if (!inert_s) {
                 atomic_add3(&a.gv_acc[r.y], bvb);
                 atomic_add3(&a.gw_acc[r.y], bwb);
             }

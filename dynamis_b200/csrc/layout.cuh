@@ -71,6 +71,22 @@ enum Ctl : uint32_t {
     CTL_COUNT = 32
 };
 
+// Where a taped step's kernels write the adjoint's snapshots (the tape of adjoint.cuh, slot *slot);
+// every pointer is null outside taped steps. Layouts: relay [slot][4c]; vel [slot][K*I][2n]
+// (velocities, then angular velocities, at each velocity iteration's start); acc [slot][K*I][4c]
+// (accumulated impulses there); res, cnt [slot][K*P][n] (resolution at each position iteration's
+// start, contributions that iteration counted), point p of contact i at p * c + i.
+struct TapeWrites {
+    const uint32_t* slot;
+    uint32_t* relay;
+    float4* vel;
+    float4* acc;
+    float4* res;
+    uint32_t* cnt;
+    uint32_t substeps, iterations, piterations;
+    size_t n, c;
+};
+
 struct DeviceWorld {
     uint32_t n;   // body rows
     uint32_t nd;  // dynamic rows (rows [0, nd))
@@ -181,10 +197,8 @@ struct DeviceWorld {
     // counters (reference slots) and control words
     uint32_t* counters;
     uint32_t* ctl;
-    // a taped step (differentiation): where k_relay records each point's relay source
-    // ([slot][4 c_cap], the slot read from *tape_slot); null outside taped steps
-    uint32_t* tape_relay;
-    const uint32_t* tape_slot;
+    // a taped step (differentiation): where the step's kernels write the adjoint's snapshots
+    TapeWrites tape;
 };
 
 }  // namespace dyn

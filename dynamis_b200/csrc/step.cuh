@@ -1196,7 +1196,7 @@ __global__ void k_relay(DeviceWorld w) {
             float4 nacc = cacc;
             if (picked != DYN_NO_SLOT) {
                 taken[picked] = true;
-                if (w.tape_relay) w.tape_relay[(size_t)(*w.tape_slot) * 4u * cap + co] = picked * cap + h;
+                if (w.tape.relay) w.tape.relay[(size_t)(*w.tape.slot) * 4u * cap + co] = picked * cap + h;
                 float4 hacc = w.arc.acc[(size_t)picked * cap + h];
                 nacc = make_float4(hacc.x, hacc.y, hacc.z, cacc.w);
                 w.cur.acc[co] = nacc;
@@ -1542,7 +1542,8 @@ __global__ void k_warm(DeviceWorld w) {
 
 // solver_contact_block.wgsl:6-193 (Jacobi block with mass splitting); the pose-only terms come
 // from k_solve_prepare.
-__device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step_params& p, uint32_t i, bool residual) {
+__device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step_params& p, uint32_t i, bool residual,
+                                            uint32_t tape_index) {
     const uint32_t cap = w.c_cap;
     const SolverRows& sr = w.srows;
     uint4 r = w.cur.rows[i];
@@ -1551,6 +1552,19 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
     const DBody& pf = b.pf;
     const DBody& ps = b.ps;
     if (dbody_inert(pf) && dbody_inert(ps)) return;
+    float4* tape_acc = nullptr;
+    if (w.tape.vel) {
+        // a taped step: the velocities and impulses this iteration starts from (every block of a
+        // row writes the same velocities)
+        const TapeWrites& t = w.tape;
+        const size_t slot = *t.slot;
+        float4* vel = t.vel + (slot * t.substeps * t.iterations + tape_index) * 2 * t.n;
+        vel[r.x] = w.hot[r.x].vel;
+        vel[t.n + r.x] = w.hot[r.x].ang;
+        vel[r.y] = w.hot[r.y].vel;
+        vel[t.n + r.y] = w.hot[r.y].ang;
+        tape_acc = t.acc + (slot * t.substeps * t.iterations + tape_index) * 4 * t.c;
+    }
     DBody first = pf, second = ps;
     float4 nf = w.cur.normal[i];
     f3 normal = xyz(nf);
@@ -1569,6 +1583,7 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
     for (uint32_t pi = 0; pi < 4u; ++pi) if (pi < pc) {
         size_t o = (size_t)pi * cap + i;
         float4 acc = w.cur.acc[o];
+        if (tape_acc) tape_acc[(size_t)pi * w.tape.c + i] = acc;
         normal_total = normal_total + wmax(acc.x, 0.0f);
         float4 a4 = sr.arm_a[o], b4 = sr.arm_b[o];
         float4 m2 = sr.masses[o];
@@ -1638,10 +1653,11 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
                     (uint32_t)solver_word(wmax(length(sa), length(sb)), DYN_SOLVER_VELOCITY_SCALE));
     }
 }
-__global__ void __launch_bounds__(128, 4) k_solve(DeviceWorld w, dyn_step_params p) {
+// tape_index: substep x iterations + iteration, where a taped step writes its snapshots
+__global__ void __launch_bounds__(128, 4) k_solve(DeviceWorld w, dyn_step_params p, uint32_t tape_index) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     const bool residual = w.ctl[CTL_ROUNDS] == p.solve_iterations;
-    GRID_STRIDE(i, count) solve_block(w, p, i, residual);
+    GRID_STRIDE(i, count) solve_block(w, p, i, residual, tape_index);
 }
 
 // solver_block_apply.wgsl:7-29
@@ -1898,8 +1914,17 @@ __device__ __forceinline__ void position_block_rows(const DeviceWorld& w, const 
         cnt[r.y] = 1u;
     }
 }
+// A taped step's position snapshots, written by each solver row's owner: the resolution iteration
+// k starts from, and the contributions iteration k - 1 counted.
+__device__ __forceinline__ void tape_position_row(const TapeWrites& t, uint32_t sub, uint32_t k, uint32_t row, float4 res,
+                                                  bool with_count, uint32_t count) {
+    const size_t slot = *t.slot;
+    const size_t base = slot * t.substeps * t.piterations + (size_t)sub * t.piterations;
+    t.res[(base + k) * t.n + row] = res;
+    if (with_count) t.cnt[(base + k - 1u) * t.n + row] = count;
+}
 template <bool kFirst>
-__global__ void k_position_fused(DeviceWorld w, dyn_step_params p, uint32_t k) {
+__global__ void k_position_fused(DeviceWorld w, dyn_step_params p, uint32_t k, uint32_t sub) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     const size_t n = w.n_cap;
     const int4* pd_prev = w.pd3 + ((k + 2u) % 3u) * n;
@@ -1916,12 +1941,21 @@ __global__ void k_position_fused(DeviceWorld w, dyn_step_params p, uint32_t k) {
         if (kFirst) {
             res_a = w.resolution[r.x];
             res_b = w.resolution[r.y];
+            if (w.tape.res) {
+                const uint32_t own = w.cowner[i];
+                if (own & 1u) tape_position_row(w.tape, sub, 0u, r.x, res_a, false, 0u);
+                if (own & 2u) tape_position_row(w.tape, sub, 0u, r.y, res_b, false, 0u);
+            }
         } else {
             const RowCorrection ca = row_correction(pd_prev, cnt_prev, r.x);
             const RowCorrection cb = row_correction(pd_prev, cnt_prev, r.y);
             res_a = corrected(res_prev[r.x], ca);
             res_b = corrected(res_prev[r.y], cb);
             const uint32_t own = w.cowner[i];
+            if (w.tape.res) {
+                if (own & 1u) tape_position_row(w.tape, sub, k, r.x, res_a, true, ca.contributing);
+                if (own & 2u) tape_position_row(w.tape, sub, k, r.y, res_b, true, cb.contributing);
+            }
             if (own & 1u) {
                 res_cur[r.x] = res_a;
                 move_row(w, r.x, ca);
@@ -1940,7 +1974,7 @@ __global__ void k_position_fused(DeviceWorld w, dyn_step_params p, uint32_t k) {
 }
 // The last iteration's correction of every solver row, into the resolution every later pass reads;
 // the three delta buffers are left cleared for the next substep.
-__global__ void k_papply_last(DeviceWorld w, uint32_t iterations) {
+__global__ void k_papply_last(DeviceWorld w, uint32_t iterations, uint32_t sub) {
     const uint32_t rows = w.ctl[CTL_SOLVER_ROWS];
     const size_t n = w.n_cap;
     const uint32_t last = iterations - 1u;
@@ -1950,6 +1984,11 @@ __global__ void k_papply_last(DeviceWorld w, uint32_t iterations) {
     GRID_STRIDE(i, rows) {
         const uint32_t row = w.solver_rows[i];
         const RowCorrection c = row_correction(pd_last, cnt_last, row);
+        if (w.tape.cnt) {  // a taped step: the last iteration's contributions
+            const size_t slot = *w.tape.slot;
+            w.tape.cnt[(slot * w.tape.substeps * w.tape.piterations + (size_t)sub * w.tape.piterations + last) * w.tape.n + row] =
+                c.contributing;
+        }
         const float4 res = corrected(res_last[row], c);
         w.resolution[row] = res;
         move_row(w, row, c);

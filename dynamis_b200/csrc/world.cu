@@ -640,15 +640,16 @@ struct Marker {
 };
 
 // Issues one step's kernels on `s`. parity selects which contact set is current. With a tape the
-// step also snapshots what its adjoint needs into the tape's current slot (adjoint.cuh) and runs
-// the position passes with their separate apply, which k_position_fused matches bit for bit.
+// step also snapshots what its adjoint needs into the tape's current slot (adjoint.cuh): the relay,
+// k_solve and the fused position kernels write theirs as they run; the contact set and the body
+// rows are copied by kernels of their own.
 void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, const TapeView* tape = nullptr) {
     DeviceState* d = w->dev;
     DeviceWorld dw = d->dw;
     if (parity) std::swap(dw.cur, dw.arc);
     if (tape) {
-        dw.tape_relay = tape->relay;
-        dw.tape_slot = tape->slot;
+        dw.tape = TapeWrites{tape->slot, tape->relay, tape->vel, tape->acc, tape->res, tape->cnt,
+                             tape->substeps, tape->iterations, tape->piterations, tape->n, tape->c};
     }
     const dyn_step_params p = d->params;
     Marker mark{d, s, timed};
@@ -756,29 +757,24 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
         mark(ST_VELOCITY);
         for (uint32_t it = 0; it < p.solve_iterations; ++it) {
             if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 32, 0, s>>>(dw, p);
-            if (tape) k_tape_iteration<<<blocks_for(d, std::max(N, C), 256), 256, 0, s>>>(dw, *tape, sub, it);
-            k_solve<<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p);
+            k_solve<<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, sub * p.solve_iterations + it);
             k_vapply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_ADVANCE);
         k_advance<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
         mark(ST_POSITION);
-        if (tape) {
-            for (uint32_t it = 0; it < p.position_iterations; ++it) {
-                k_position<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
-                k_tape_position<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, *tape, sub, it);
-                k_papply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
-            }
-        } else if (joint_blocks == 0u) {
+        if (joint_blocks == 0u) {
             // each iteration applies the one before it; one apply after the last
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 if (it == 0u) {
-                    k_position_fused<true><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it);
+                    k_position_fused<true><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it, sub);
                 } else {
-                    k_position_fused<false><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it);
+                    k_position_fused<false><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it, sub);
                 }
             }
-            if (p.position_iterations > 0u) k_papply_last<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p.position_iterations);
+            if (p.position_iterations > 0u) {
+                k_papply_last<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p.position_iterations, sub);
+            }
         } else {
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 k_joints<JP_POSITION><<<joint_blocks, 32, 0, s>>>(dw, p);
@@ -1569,6 +1565,7 @@ static dyn_status alloc_adjoint(dyn_world* w) {
     AA(a.t_mass, 4 * C);
     AA(a.t_tan1, C);
     AA(a.t_tan2, C);
+    AA(a.t_body, C);
     AA(a.g_mu, C);
     AA(t.grad_staging, N);
     AA(t.patch_rows, N);
