@@ -487,7 +487,7 @@ __device__ __forceinline__ float quad_sum(float v, unsigned mask) {
 __device__ __forceinline__ f3 quad_sum3(f3 v, unsigned mask) {
     return mk3(quad_sum(v.x, mask), quad_sum(v.y, mask), quad_sum(v.z, mask));
 }
-__global__ void __launch_bounds__(128, 7) k_adj_solve(TapeView t, AdjView a, dyn_step_params p, uint32_t k, uint32_t it) {
+__global__ void __launch_bounds__(128, 6) k_adj_solve(TapeView t, AdjView a, dyn_step_params p, uint32_t k, uint32_t it) {
     const uint32_t s = *t.slot;
     const uint32_t count = t.counts[s];
     const float4* vel = t.vel_at(s, k, it);
@@ -497,13 +497,23 @@ __global__ void __launch_bounds__(128, 7) k_adj_solve(TapeView t, AdjView a, dyn
     const unsigned mask = 0xFu << (threadIdx.x & 28u);
     const uint32_t quads = (gridDim.x * blockDim.x) >> 2;
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; i < count; i += quads) {
-        // every lane of a quad takes the same branches up to the point work
+        // every lane of a quad takes the same branches up to the point work. Everything that does not
+        // depend on the block's rows is loaded first, in one round trip (the point arrays hold 4c
+        // entries, so every lane's loads are in bounds whatever the block's point count)
         const float4 tan2 = a.t_tan2[i];
+        const uint4 r = t.rows[t.cs(s) + i];
+        const float4 body = a.t_body[i];
+        const float4 nf = t.normal[t.cs(s) + i];
+        const float4 tan1 = a.t_tan1[i];
+        const size_t o = (size_t)q * t.c + i;
+        const float4 arm_a = a.t_arm_a[o], arm_b = a.t_arm_b[o], masses = a.t_mass[o];
+        const float4 acc = accs[o];
+        const float4 gout = gacc[o];
+        const float4 gra0 = a.g_ra[o], grb0 = a.g_rb[o];
+        const float2 gm0 = a.g_m[o];
         const uint32_t flags = __float_as_uint(tan2.w);
         if (!(flags & kBlockSolve)) continue;
-        const uint4 r = t.rows[t.cs(s) + i];
         const bool inert_f = (flags & kBlockInertFirst) != 0u, inert_s = (flags & kBlockInertSecond) != 0u;
-        const float4 body = a.t_body[i];
         const float ima = body.x, imb = body.y;
         // the bodies as the block saw them: only the velocities are read (dbody_iinv of an isotropic
         // body is its scalar times the vector)
@@ -521,14 +531,10 @@ __global__ void __launch_bounds__(128, 7) k_adj_solve(TapeView t, AdjView a, dyn
         f3 bva = s3(0.0f), bwa = s3(0.0f), bvb = s3(0.0f), bwb = s3(0.0f);
         float g_ima = 0.0f, g_imb = 0.0f, g_sa = 0.0f, g_sb = 0.0f, g_mu = 0.0f;
         if (q < (r.z & 0xFFu)) {
-            const float4 nf = t.normal[t.cs(s) + i];
-            const f3 n = xyz(nf), t1 = xyz(a.t_tan1[i]), t2 = xyz(tan2);
+            const f3 n = xyz(nf), t1 = xyz(tan1), t2 = xyz(tan2);
             const float mu = nf.w;
-            const size_t o = (size_t)q * t.c + i;
-            const float4 arm_a = a.t_arm_a[o], arm_b = a.t_arm_b[o], masses = a.t_mass[o];
             const f3 ra = xyz(arm_a), rb = xyz(arm_b);
             const float nm = arm_a.w, m1 = masses.x, m2 = masses.y, target = masses.z;
-            const float4 acc = accs[o];
             const float an = acc.x, at1 = acc.y, at2 = acc.z;
             // forward (solve_block, hard contact)
             const f3 rel = point_velocity_arm(ps, rb) - point_velocity_arm(pf, ra);
@@ -552,7 +558,6 @@ __global__ void __launch_bounds__(128, 7) k_adj_solve(TapeView t, AdjView a, dyn
             g_sa = -dot(Wa, cross(ra, j));
             g_sb = dot(Wb, cross(rb, j));
             f3 gra = cross(Wa, j), grb = cross(j, Wb);
-            const float4 gout = gacc[o];
             float g_an1 = dot(n, jb) + gout.x, g_an0 = -dot(n, jb);
             float g_at11 = dot(t1, jb) + gout.y, g_at10 = -dot(t1, jb);
             const float g_at21 = dot(t2, jb) + gout.z;
@@ -608,12 +613,9 @@ __global__ void __launch_bounds__(128, 7) k_adj_solve(TapeView t, AdjView a, dyn
             grb = grb + cross(g_rel, ps.angular_velocity);
             gra = gra - cross(g_rel, pf.angular_velocity);
             gacc[o] = make_float4(g_an0, g_at10, g_at20, 0.0f);
-            float4 x = a.g_ra[o];
-            a.g_ra[o] = make_float4(x.x + gra.x, x.y + gra.y, x.z + gra.z, x.w + g_nm);
-            x = a.g_rb[o];
-            a.g_rb[o] = make_float4(x.x + grb.x, x.y + grb.y, x.z + grb.z, x.w + g_target);
-            const float2 gm = a.g_m[o];
-            a.g_m[o] = make_float2(gm.x + g_m1, gm.y + g_m2);
+            a.g_ra[o] = make_float4(gra0.x + gra.x, gra0.y + gra.y, gra0.z + gra.z, gra0.w + g_nm);
+            a.g_rb[o] = make_float4(grb0.x + grb.x, grb0.y + grb.y, grb0.z + grb.z, grb0.w + g_target);
+            a.g_m[o] = make_float2(gm0.x + g_m1, gm0.y + g_m2);
         }
         bva = quad_sum3(bva, mask);
         bwa = quad_sum3(bwa, mask);
