@@ -130,6 +130,8 @@ def stage_bytes(stage: str, m: dict, params: dict) -> float:
         return 12.0 * C + 24.0 * C * 2 * params["contact_words"] + 2 * 352.0 * C
     if stage == "integrate":
         return 152.0 * L
+    if stage == "islands":   # link over contacts (two passes), flatten and aggregate over the rows
+        return 44.0 * C + 20.0 * R_
     return 0.0
 
 
@@ -156,9 +158,27 @@ def build_world(workload: str, device: int):
     return world, scene, time.perf_counter() - t0
 
 
+def long_run_checks(world, dt: float, before: dict, top: float) -> dict:
+    """The long-run bounds at the end of the setup steps: total energy not above its start, no
+    body faster than free fall from the scene's top, the deepest contact overlap, the pile's mean
+    velocity."""
+    from dynamis_b200 import diagnostics
+
+    after = diagnostics.summary(world, dt)
+    speed = np.linalg.norm(world.read_states()["velocity"].astype(np.float64), axis=1)
+    bound = float(np.sqrt(2.0 * 9.81 * max(top, 0.0)))
+    faster = int((speed > bound).sum())
+    e0, e1 = before["energy"]["total"], after["energy"]["total"]
+    return {"energy_start": e0, "energy_after_setup": e1, "energy_ratio": e1 / e0 if e0 else None,
+            "free_fall_speed_bound": bound, "bodies_faster_than_free_fall": faster, "max_speed": float(speed.max()),
+            "deepest_penetration": after["deepest_penetration"], "mean_velocity": after["mean_velocity"],
+            "within_bounds": bool(e1 <= e0 * (1.0 + 1e-6) and faster == 0 and np.all(np.isfinite(speed)))}
+
+
 def run_ours(args, rank: int, world_size: int, local_rank: int):
     import torch
 
+    from dynamis_b200 import diagnostics
     from dynamis_b200 import records as R
 
     torch.cuda.set_device(local_rank)
@@ -168,6 +188,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     log(f"scene {args.workload}: {bodies} bodies built in {build_s:.1f}s")
     stream = torch.cuda.Stream(device=local_rank)
     world.set_stream(stream.cuda_stream)
+    before = diagnostics.summary(world, DT, stepped=False)
+    top = float(world.read_states()["position"][:, 1].max())
     for i in range(args.setup):
         world.step(DT)
         if i % 20 == 19:
@@ -175,6 +197,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
             log(f"setup step {i + 1}/{args.setup}")
     world.wait()
     log("setup done")
+    setup_checks = long_run_checks(world, DT, before, top)
+    log(f"setup checks {setup_checks}")
     for _ in range(args.warmup):
         world.step(DT)
     world.wait()
@@ -222,6 +246,11 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     algo = stage_bytes(dominant, counts, params)
     pk = peaks()
     achieved = algo / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    stage_frac = {}
+    for stage, stage_ms in stages.items():
+        moved = stage_bytes(stage, counts, params) * LAUNCHES.get(stage, lambda p: 1)(params)
+        if moved > 0 and stage_ms > 0:
+            stage_frac[stage] = round(moved / (stage_ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4)
     # end to end through the C ABI with pinned host buffers
     e2e_steps = max(3, min(args.steps, 10))
     host = torch.empty(bodies * R.BODY_STATE.itemsize, dtype=torch.uint8, pin_memory=True)
@@ -256,6 +285,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                      "peak_source": pk["source"],
                      "algorithmic_bytes_per_launch": algo, "ms_per_launch": per_launch_ms},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "stage_frac": stage_frac,
+        "setup_checks": setup_checks,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
     }

@@ -25,6 +25,7 @@ SHAPE_SPHERE, SHAPE_CUBOID, SHAPE_CAPSULE, SHAPE_CYLINDER, SHAPE_HULL, SHAPE_PLA
 NO_BODY = 0xFFFFFFFF
 NO_COLLISION_FILTER = 0xFFFFFFFF
 CONTACT_ANNOUNCED = 0x80000000
+BODY_KINEMATIC = 1  # BodyDescriptorRecord flags (constant.rs)
 
 
 def _dtype(fields, size):
