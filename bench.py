@@ -175,6 +175,41 @@ def long_run_checks(world, dt: float, before: dict, top: float) -> dict:
             "within_bounds": bool(e1 <= e0 * (1.0 + 1e-6) and faster == 0 and np.all(np.isfinite(speed)))}
 
 
+def guarded_run(args, dt: float, device: int) -> dict:
+    """The same workload with the row-mass guard on (dyn_set_solver_guard): the same setup, warm-up
+    and timed steps, its setup bounds, its device time per step."""
+    import torch
+
+    from dynamis_b200 import diagnostics
+    from dynamis_b200 import records as R
+
+    world, scene, _ = build_world(args.workload, device)
+    world.set_solver_guard(R.SOLVER_GUARD_ROW_MASS)
+    stream = torch.cuda.Stream(device=device)
+    world.set_stream(stream.cuda_stream)
+    before = diagnostics.summary(world, dt, stepped=False)
+    top = float(world.read_states()["position"][:, 1].max())
+    for _ in range(args.setup):
+        world.step(dt)
+    world.wait()
+    checks = long_run_checks(world, dt, before, top)
+    for _ in range(args.warmup):
+        world.step(dt)
+    world.wait()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        world.step(dt)
+    end.record(stream)
+    end.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    bodies = world.sizes()["bodies"]
+    world.close()
+    log(f"guarded: {ms:.3f} ms/step; setup checks {checks}")
+    return {"solver_guard": "row_mass", "ms_per_step": ms, "value": bodies / (ms * 1e-3), "unit": UNIT,
+            "setup_checks": checks}
+
+
 def run_ours(args, rank: int, world_size: int, local_rank: int):
     import torch
 
@@ -292,6 +327,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     }
     if args.workload.startswith("batched_worlds_"):
         result["batch"] = loop_baseline(args, DT, ms / args.steps, local_rank)
+    if not args.no_guarded:
+        result["guarded"] = guarded_run(args, DT, local_rank)
     if not args.no_adjoint:
         result["adjoint"] = adjoint_benchmark(local_rank, steps=args.adjoint_steps, settle=args.adjoint_setup)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -509,6 +546,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-towers measurement")
+    ap.add_argument("--no-guarded", action="store_true", help="skip the run with the row-mass guard")
     ap.add_argument("--adjoint-only", action="store_true", help="print only the differentiable-towers measurement")
     ap.add_argument("--adjoint-steps", type=int, default=120)
     ap.add_argument("--adjoint-setup", type=int, default=60)

@@ -199,6 +199,8 @@ struct DeviceWorld {
     uint32_t* ctl;
     // a taped step (differentiation): where the step's kernels write the adjoint's snapshots
     TapeWrites tape;
+    // DYN_SOLVER_GUARD_* bits (dyn_set_solver_guard); 0 is the reference's solver
+    uint32_t solver_guard;
 };
 
 }  // namespace dyn

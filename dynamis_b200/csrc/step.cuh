@@ -1466,6 +1466,54 @@ __device__ __forceinline__ BlockBodies block_bodies(const DeviceWorld& w, uint4 
     return b;
 }
 
+// The row-mass guard (DYN_SOLVER_GUARD_ROW_MASS, no counterpart in the reference). A block solves
+// its points' normal rows Jacobi-wise against the manifold row masses D_j = sum_k A_jk
+// (manifold_row_mass, solver_contact_block.wgsl:14-29), A being the points' coupling matrix
+// A_jk = m_a + m_b + (r_aj x n) . I_a (r_ak x n) + (r_bj x n) . I_b (r_bk x n) of the split bodies.
+// The iteration converges while the eigenvalues of S = D^-1/2 A D^-1/2 stay below 2; where a point's
+// arm opposes the others' (a tilted box landing on three points) they do not, and the impulses grow
+// twofold or more per iteration. The guard keeps a block's row masses when every D_j is positive
+// and kRowMassBound I - S is positive definite (its LDL^T pivots all positive), i.e. every
+// eigenvalue of S lies below kRowMassBound; otherwise each point takes count x A_jj, whose
+// normalised matrix has unit diagonal and off-diagonal entries within 1, so its eigenvalues stay
+// at or below count / count = 1.
+constexpr float kRowMassBound = 1.9f;
+__device__ __forceinline__ float coupling(const DBody& a, const DBody& b, f3 uj, f3 vj, f3 iuk, f3 ivk) {
+    return a.inverse_mass + b.inverse_mass + dot(uj, iuk) + dot(vj, ivk);
+}
+__device__ __forceinline__ void guard_row_masses(const BlockBodies& b, f3 normal, const f3* ra, const f3* rb, uint32_t pc,
+                                                 float count_f, float* nm) {
+    f3 u[4], v[4], iu[4], iv[4];
+    for (uint32_t j = 0; j < pc; ++j) {
+        u[j] = cross(ra[j], normal);
+        v[j] = cross(rb[j], normal);
+        iu[j] = dbody_iinv(b.sf, u[j]);
+        iv[j] = dbody_iinv(b.ss, v[j]);
+    }
+    bool converges = true;
+    for (uint32_t j = 0; j < pc; ++j) converges = converges && nm[j] > 0.0f;
+    if (converges) {
+        // M = bound I - S, factored M = L diag(d) L^T row by row
+        float m[4][4], l[4][4], d[4];
+        for (uint32_t j = 0; j < pc; ++j)
+            for (uint32_t k = 0; k < pc; ++k)
+                m[j][k] = (j == k ? kRowMassBound : 0.0f) - coupling(b.sf, b.ss, u[j], v[j], iu[k], iv[k]) / sqrtf(nm[j] * nm[k]);
+        for (uint32_t j = 0; j < pc && converges; ++j) {
+            float pivot = m[j][j];
+            for (uint32_t k = 0; k < j; ++k) pivot = pivot - l[j][k] * l[j][k] * d[k];
+            d[j] = pivot;
+            converges = pivot > 0.0f;
+            for (uint32_t i = j + 1; i < pc && converges; ++i) {
+                float x = m[i][j];
+                for (uint32_t k = 0; k < j; ++k) x = x - l[i][k] * l[j][k] * d[k];
+                l[i][j] = x / pivot;
+            }
+        }
+    }
+    if (converges) return;
+    for (uint32_t j = 0; j < pc; ++j) nm[j] = count_f * coupling(b.sf, b.ss, u[j], v[j], iu[j], iv[j]);
+}
+
 __global__ void k_solve_prepare(DeviceWorld w) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     const uint32_t cap = w.c_cap;
@@ -1493,11 +1541,16 @@ __global__ void k_solve_prepare(DeviceWorld w) {
         float count_f = (float)max(pc, 1u);
         f3 spread_f = dbody_iinv(b.sf, cross(reach_f, normal));
         f3 spread_s = dbody_iinv(b.ss, cross(reach_s, normal));
+        float nm[4];
         for (uint32_t pi = 0; pi < pc; ++pi) {
-            size_t o = (size_t)pi * cap + i;
             f3 arm_f = cross(ra[pi], normal);
             f3 arm_s = cross(rb[pi], normal);
-            float normal_mass = count_f * (b.sf.inverse_mass + b.ss.inverse_mass) + dot(spread_f, arm_f) + dot(spread_s, arm_s);
+            nm[pi] = count_f * (b.sf.inverse_mass + b.ss.inverse_mass) + dot(spread_f, arm_f) + dot(spread_s, arm_s);
+        }
+        if ((w.solver_guard & DYN_SOLVER_GUARD_ROW_MASS) && pc >= 2u) guard_row_masses(b, normal, ra, rb, pc, count_f, nm);
+        for (uint32_t pi = 0; pi < pc; ++pi) {
+            size_t o = (size_t)pi * cap + i;
+            float normal_mass = nm[pi];
             float truth = momentum_mass_arms(b.pf, b.ps, ra[pi], rb[pi], normal);
             float t1_mass = momentum_mass_arms(b.sf, b.ss, ra[pi], rb[pi], t1) * count_f;
             float t2_mass = momentum_mass_arms(b.sf, b.ss, ra[pi], rb[pi], t2) * count_f;

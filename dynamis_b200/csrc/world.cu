@@ -647,6 +647,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     DeviceState* d = w->dev;
     DeviceWorld dw = d->dw;
     if (parity) std::swap(dw.cur, dw.arc);
+    dw.solver_guard = w->solver_guard;
     if (tape) {
         dw.tape = TapeWrites{tape->slot, tape->relay, tape->vel, tape->acc, tape->res, tape->cnt,
                              tape->substeps, tape->iterations, tape->piterations, tape->n, tape->c};
@@ -1740,6 +1741,7 @@ DYN_API dyn_status dyn_tape_begin(dyn_world* w, uint32_t checkpoint_interval) {
     if (!w || checkpoint_interval == 0) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: the checkpoint interval must be > 0");
     if (std::isfinite(w->config.sleep_time)) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: sleeping must be off (sleep_time = inf)");
     if (!w->joint_descs.empty()) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: constraints are not differentiated");
+    if (w->solver_guard) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: the adjoint differentiates the reference's solver (no guard)");
     rebuild_rows(w);
     for (uint32_t i = 0; i < w->dynamic_count && i < w->descs.size(); ++i) {
         const float* ii = w->descs[i].inverse_inertia;
@@ -2212,6 +2214,20 @@ DYN_API dyn_status dyn_debug_islands(dyn_world* w, uint32_t* out, uint32_t cap, 
 }
 
 DYN_API uint32_t dyn_step_kernel_count(const dyn_world* w) { return (w && w->dev) ? w->dev->graph_kernels : 0u; }
+
+DYN_API dyn_status dyn_set_solver_guard(dyn_world* w, uint32_t flags) {
+    if (!w) return DYN_ERR_INVALID;
+    if (flags & ~DYN_SOLVER_GUARD_ROW_MASS) return fail(w, DYN_ERR_INVALID, "dyn_set_solver_guard: unknown flag");
+    if (w->dev && w->dev->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_set_solver_guard: a tape is recording");
+    if (flags == w->solver_guard) return DYN_OK;
+    w->solver_guard = flags;
+    if (w->dev) {
+        DYN_CUDA(cudaSetDevice(w->device));
+        DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+        release_graphs(w->dev);  // the step graphs carry the flag: record them again
+    }
+    return DYN_OK;
+}
 
 DYN_API dyn_status dyn_set_timing(dyn_world* w, int32_t enabled) {
     if (!w) return DYN_ERR_INVALID;

@@ -240,6 +240,12 @@ class World:
         self._check(lib.dyn_joint_plan(self._h, ptr(rows), ptr(layers), ptr(comps), None, None))
         return {"rows": rows, "layers": layers, "components": comps}
 
+    def set_solver_guard(self, flags: int) -> None:
+        """dyn_set_solver_guard: SOLVER_GUARD_ROW_MASS keeps every contact block's Jacobi iteration
+        convergent where the reference's manifold row masses would let it diverge; 0 (the default)
+        is the reference's solver."""
+        self._check(lib.dyn_set_solver_guard(self._h, int(flags)))
+
     def step_params(self, dt: float) -> np.ndarray:
         p = np.zeros(1, R.STEP_PARAMS)
         self._check(lib.dyn_step_params_for(self._h, float(dt), ptr(p)))

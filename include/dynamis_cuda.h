@@ -301,6 +301,20 @@ DYN_API dyn_status dyn_radix_sort_static_status(void* cuda_stream, uint32_t* out
 #define DYN_STATUS_ISLAND_HOOKS 2u
 #define DYN_STATUS_ADJOINT_UNSUPPORTED 4u  /* a reversed step met a contact the adjoint does not cover */
 
+/* Solver guards, no counterpart in the reference (0, the default, is the reference's solver).
+ * DYN_SOLVER_GUARD_ROW_MASS: the reference solves a contact's points together against manifold row
+ * masses (solver_contact_block.wgsl:14-29, manifold_row_mass), and for some manifolds (a tilted box
+ * landing on three points whose arms do not balance) that Jacobi iteration diverges: the impulses
+ * grow at least twofold per iteration and the bodies leave at hundreds of metres a second. With the
+ * guard, a block whose points' normalised coupling matrix D^-1/2 A D^-1/2 has an eigenvalue of 1.9
+ * or more (the reference's iteration diverges from 2) solves each point against count x its own
+ * mass instead; every other
+ * block, and so every step where no block fails, is bit for bit the reference's. Takes effect at
+ * the next dyn_step; refused while a tape records (the adjoint differentiates the reference's
+ * solver), and dyn_tape_begin refuses a guarded world. */
+#define DYN_SOLVER_GUARD_ROW_MASS 1u
+DYN_API dyn_status dyn_set_solver_guard(dyn_world* world, uint32_t flags);
+
 /* Clears the world's sticky device status word (dyn_sync keeps reporting it until this call or a
  * new scene upload). Synchronises the world's stream. No counterpart in the reference, which has
  * no device status word. */

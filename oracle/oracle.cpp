@@ -226,6 +226,7 @@ struct OracleWorld {
     // accumulated impulses at each velocity iteration's start [substep][iteration][contact][point],
     // resolutions at each position iteration's start [substep][iteration][row]
     bool keep_snapshots = false;
+    uint32_t solver_guard = 0;  // DYN_SOLVER_GUARD_* bits, the library's extension (0: the reference)
     std::vector<float> snap_pose, snap_vel, snap_acc, snap_res;
     std::vector<uint32_t> contact_matched;
     std::vector<uint32_t> island_parents, island_state;
@@ -1149,6 +1150,54 @@ void solve_contact_block(OracleWorld& w, uint32_t index, bool residual) {
         normal_total = normal_total + fmaxw(contact.points[pi].accumulated_normal, 0.0f);
     }
     V3 impulses[4] = {zero, zero, zero, zero};
+    // manifold_row_mass (solver_contact_block.wgsl:14-29) of every point, then the library's
+    // row-mass guard when it is on (DYN_SOLVER_GUARD_ROW_MASS): a block whose points' normalised
+    // coupling matrix has an eigenvalue of 1.9 or more (where the reference's Jacobi iteration stops
+    // converging at 2) takes count x each point's own coupling instead
+    float row_mass[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    V3 arm_fs[4], arm_ss[4];
+    for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
+        const dyn_manifold_point_record& p = contact.points[pi];
+        arm_fs[pi] = cross(manifold_arm(pf, p, true) - body_com(split_f), normal);
+        arm_ss[pi] = cross(manifold_arm(ps, p, false) - body_com(split_s), normal);
+        row_mass[pi] = point_count * (split_f.inverse_mass + split_s.inverse_mass)
+            + dot(apply_inverse_inertia(split_f, cross(reach_f, normal)), arm_fs[pi])
+            + dot(apply_inverse_inertia(split_s, cross(reach_s, normal)), arm_ss[pi]);
+    }
+    if ((w.solver_guard & 1u) && contact.point_count >= 2u) {
+        const uint32_t pc = contact.point_count;
+        V3 iu[4], iv[4];
+        for (uint32_t j = 0; j < pc; ++j) {
+            iu[j] = apply_inverse_inertia(split_f, arm_fs[j]);
+            iv[j] = apply_inverse_inertia(split_s, arm_ss[j]);
+        }
+        auto coupling = [&](uint32_t j, uint32_t k) {
+            return split_f.inverse_mass + split_s.inverse_mass + dot(arm_fs[j], iu[k]) + dot(arm_ss[j], iv[k]);
+        };
+        // the row masses stay while every one is positive and 1.9 I - D^-1/2 A D^-1/2 is positive
+        // definite (LDL^T pivots, row by row)
+        bool converges = true;
+        for (uint32_t j = 0; j < pc; ++j) converges = converges && row_mass[j] > 0.0f;
+        if (converges) {
+            float m[4][4], l[4][4], d[4];
+            for (uint32_t j = 0; j < pc; ++j)
+                for (uint32_t k = 0; k < pc; ++k)
+                    m[j][k] = (j == k ? 1.9f : 0.0f) - coupling(j, k) / std::sqrt(row_mass[j] * row_mass[k]);
+            for (uint32_t j = 0; j < pc && converges; ++j) {
+                float pivot = m[j][j];
+                for (uint32_t k = 0; k < j; ++k) pivot = pivot - l[j][k] * l[j][k] * d[k];
+                d[j] = pivot;
+                converges = pivot > 0.0f;
+                for (uint32_t i = j + 1; i < pc && converges; ++i) {
+                    float x = m[i][j];
+                    for (uint32_t k = 0; k < j; ++k) x = x - l[i][k] * l[j][k] * d[k];
+                    l[i][j] = x / pivot;
+                }
+            }
+        }
+        if (!converges)
+            for (uint32_t j = 0; j < pc; ++j) row_mass[j] = point_count * coupling(j, j);
+    }
     for (uint32_t pi = 0; pi < contact.point_count; ++pi) {
         const dyn_manifold_point_record& p = contact.points[pi];
         V3 af = manifold_arm(pf, p, true);
@@ -1157,12 +1206,7 @@ void solve_contact_block(OracleWorld& w, uint32_t index, bool residual) {
         float acc_t1 = p.accumulated_tangent_1;
         float acc_t2 = p.accumulated_tangent_2;
         float normal_speed = dot(relative_velocity(pf, ps, af, as), normal);
-        // manifold_row_mass (solver_contact_block.wgsl:14-29)
-        V3 arm_f = cross(af - body_com(split_f), normal);
-        V3 arm_s = cross(as - body_com(split_s), normal);
-        float normal_mass = point_count * (split_f.inverse_mass + split_s.inverse_mass)
-            + dot(apply_inverse_inertia(split_f, cross(reach_f, normal)), arm_f)
-            + dot(apply_inverse_inertia(split_s, cross(reach_s, normal)), arm_s);
+        float normal_mass = row_mass[pi];
         float normal_truth = point_momentum_mass(pf, ps, af, as, normal);
         float delta = contact_normal_delta(contact, normal_mass, normal_truth, w.params.dt,
                                            w.target_speeds[4 * (size_t)index + pi], p.depth, normal_speed, acc_n);
@@ -1926,6 +1970,7 @@ uint32_t orc_solve_contacts(const OracleWorld* w, dyn_contact_record* out, float
 }
 // Keeps (or stops keeping) the primal snapshots of each step (OracleWorld::snap_pose ...).
 void orc_keep_snapshots(OracleWorld* w, uint32_t keep) { w->keep_snapshots = keep != 0u; }
+void orc_set_solver_guard(OracleWorld* w, uint32_t flags) { w->solver_guard = flags; }
 void orc_step_snapshots(const OracleWorld* w, float* pose, float* vel, float* acc, float* res) {
     if (pose) std::copy(w->snap_pose.begin(), w->snap_pose.end(), pose);
     if (vel) std::copy(w->snap_vel.begin(), w->snap_vel.end(), vel);

@@ -96,6 +96,12 @@ class OracleWorld:
     def step(self, dt: float) -> None:
         lib().orc_step(self._h, float(dt))
 
+    def set_solver_guard(self, flags: int) -> None:
+        """The library's solver guards (dyn_set_solver_guard), restated: 1 = the row-mass guard."""
+        L = lib()
+        L.orc_set_solver_guard.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        L.orc_set_solver_guard(self._h, int(flags))
+
     def edit_bodies(self, body_ids, edits: np.ndarray) -> None:
         """Queues BodyEdit records for the next step (body ids mapped to this world's rows)."""
         ids = np.asarray(body_ids, np.int64)
