@@ -508,31 +508,51 @@ def cpu_baseline(world, budget_s: float = 20.0, dt: float = DT) -> dict:
 
 
 def run_reference(args) -> dict:
-    """The reference arm: the CPU restatement of the step on the host, on every host thread."""
-    from dynamis_b200 import World
+    """The reference arm: the reference's step as the CPU restatement runs it (the reference itself is
+    Rust + WGSL on wgpu and cannot run here), on every host thread. The arm uses no product code: the
+    oracle builds the scene's records itself (oracle/scene.cpp restates the reference's spawn path and
+    matches the library byte for byte), steps the same setup and warm-up steps, then times a bounded
+    sample of steps, which it reports as its steps."""
+    import os
+
+    from dynamis_b200 import scenes
+    from oracle import oracle as orc
 
     DT = dt_of(args.workload)
-    world, scene, _ = build_world(args.workload, 0)
-    state_note = "initial lattice state"
-    try:
-        import torch
-
-        if torch.cuda.is_available():
-            for _ in range(args.setup + args.warmup):
-                world.step(DT)
-            world.wait()
-            state_note = f"state after {args.setup + args.warmup} steps (input prepared on the GPU, untimed)"
-    except Exception:
-        pass
-    base = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
-    base["sample"] += f"; {state_note}"
+    scene = scenes.WORKLOADS[args.workload]()
+    records = orc.scene_records(scene.bodies, scene.colliders, scene.hulls, scene.worlds, dt=DT)
+    bodies = len(records["states"])
+    world = orc.OracleWorld(records, records["params"])
+    cores = orc.threads()
+    t0 = time.perf_counter()
+    for i in range(args.setup + args.warmup):
+        world.step(DT)
+        if i % 20 == 19:
+            log(f"reference setup step {i + 1}/{args.setup + args.warmup}")
+    log(f"reference setup: {args.setup + args.warmup} oracle steps in {time.perf_counter() - t0:.1f}s")
+    budget = args.cpu_budget
+    timed = 0
+    t0 = time.perf_counter()
+    while timed < max(1, min(args.steps, 3)):
+        world.step(DT)
+        timed += 1
+        if time.perf_counter() - t0 > budget / 2:
+            break
+    elapsed = time.perf_counter() - t0
     world.close()
-    return {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "setup_steps": args.setup, "dt": DT},
+    value = bodies * timed / elapsed
+    loaded = [line.split()[-1] for line in open(f"/proc/{os.getpid()}/maps") if line.rstrip().endswith(".so")]
+    assert not any("libdynamis_cuda" in name for name in loaded), "the reference arm must not load the product"
+    base = {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{timed} step(s) of the full {bodies}-body world after {args.setup + args.warmup} setup and "
+                      f"warm-up steps, all on the oracle (records built by the oracle), {cores} threads (OpenMP)"}
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": timed, "warmup": args.warmup, "ms_per_step": elapsed / timed * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "bodies": bodies, "setup_steps": args.setup, "dt": DT,
+                       "parallelism": "single-world"},
             "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():

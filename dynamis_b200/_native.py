@@ -29,6 +29,8 @@ SIGNATURES = {
     "dyn_last_error": (ctypes.c_char_p, [P]),
     "dyn_world_set_stream": (I32, [P, P]),
     "dyn_add_hull": (I32, [P, P, U32, PU32]),
+    "dyn_add_hull_from_mesh": (I32, [P, P, U32, P, U32, PU32]),
+    "dyn_add_hull_mesh": (I32, [P, P, U32, P, U32, PU32]),
     "dyn_hull_info": (I32, [P, U32, PU32, PU32, PF32, P]),
     "dyn_spawn_bodies": (I32, [P, P, U32, P, U32, P]),
     "dyn_upload_bodies": (I32, [P, P, P, U32, P, P, U32]),
@@ -106,7 +108,19 @@ def _load() -> ctypes.CDLL:
     return lib
 
 
-lib = _load()
+class _Library:
+    """libdynamis_cuda.so, loaded at the first call through it (so that the scene descriptions and
+    record dtypes import without it); a missing library raises ImportError there, with no fallback."""
+
+    _cdll = None
+
+    def __getattr__(self, name):
+        if _Library._cdll is None:
+            _Library._cdll = _load()
+        return getattr(_Library._cdll, name)
+
+
+lib = _Library()
 
 
 def check(status: int, world=None) -> None:

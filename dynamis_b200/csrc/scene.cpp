@@ -8,8 +8,7 @@
 //   compute_mass_properties                crates/dynamis-model/src/mass.rs:155-212
 //   hull solid integrals                   crates/dynamis-hull/src/solid.rs:62-105
 //   StepParamsRecord::new                  crates/dynamis-abi/src/param.rs:110-158
-// The convex hull itself is an incremental quickhull (Barber, Dobkin and Huhdanpaa, 1996) in
-// double precision; it keeps input vertices that lie on the hull, in input order.
+//   hull (add_hull_from_mesh)              crates/dynamis-hull/src/hull.rs:53-288
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -34,158 +33,177 @@ D3 cross3(const D3& a, const D3& b) {
     return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
 }
 double dot3(const D3& a, const D3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-double norm3(const D3& a) { return std::sqrt(dot3(a, a)); }
 
-struct QFace {
-    int a, b, c;
-    D3 n;
-    double d;
-    bool alive;
-    std::vector<int> outside;
+// ---- the convex hull of a mesh (crates/dynamis-hull/src/hull.rs:53-288) ----
+// Incremental quickhull in f32 with the reference's choices, so that its vertex numbering (which
+// hull contacts carry as features and the warm start relays by) is the reference's: the initial
+// tetrahedron from the x extremes, the point farthest from their line and the one farthest from
+// that plane; each round expands the live face whose first outside point lies farthest (the last
+// such face on ties), from its farthest outside point (again the last on ties); a face sees a point
+// beyond 1e-6; the output keeps the surviving faces in creation order and numbers the vertices by
+// first appearance over them. Faces live in one growing array; their outside sets are index lists.
+struct HullBuild {
+    const std::vector<std::array<float, 3>>& p;
+    std::vector<std::array<uint32_t, 3>> corner;  // a, b, c of every face ever made
+    std::vector<std::array<float, 4>> plane;      // unit normal, offset
+    std::vector<std::vector<uint32_t>> outside;
+    std::vector<uint8_t> live;
+    std::vector<uint8_t> cornered;  // per point: a corner of some face made so far
+
+    static float dotf(const std::array<float, 3>& a, const std::array<float, 3>& b) {
+        return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    }
+    std::array<float, 3> unit_normal(uint32_t a, uint32_t b, uint32_t c) const {
+        const std::array<float, 3> u = {p[b][0] - p[a][0], p[b][1] - p[a][1], p[b][2] - p[a][2]};
+        const std::array<float, 3> v = {p[c][0] - p[a][0], p[c][1] - p[a][1], p[c][2] - p[a][2]};
+        const std::array<float, 3> n = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+        const float len = std::sqrt(dotf(n, n));
+        if (len < 1e-12f) return {0.0f, 0.0f, 0.0f};
+        return {n[0] / len, n[1] / len, n[2] / len};
+    }
+    uint32_t add_face(uint32_t a, uint32_t b, uint32_t c) {
+        cornered[a] = cornered[b] = cornered[c] = 1;
+        const std::array<float, 3> n = unit_normal(a, b, c);
+        corner.push_back({a, b, c});
+        plane.push_back({n[0], n[1], n[2], dotf(n, p[a])});
+        outside.emplace_back();
+        live.push_back(1);
+        return (uint32_t)corner.size() - 1;
+    }
+    float height(uint32_t f, uint32_t point) const {
+        const std::array<float, 3> n = {plane[f][0], plane[f][1], plane[f][2]};
+        return dotf(n, p[point]) - plane[f][3];
+    }
+    // each point joins the outside set of the first live face that sees it. A point that is already
+    // a corner of the hull joins none: in exact arithmetic no face sees it, and where rounding says
+    // otherwise (a skinny face through near-duplicate points) the reference's rounds would pick it
+    // again and again without end
+    void assign(const std::vector<uint32_t>& points) {
+        for (uint32_t q : points)
+            for (uint32_t f = 0; f < (uint32_t)corner.size() && !cornered[q]; ++f)
+                if (live[f] && height(f, q) > 1e-6f) {
+                    outside[f].push_back(q);
+                    break;
+                }
+    }
 };
 
-QFace make_face(const std::vector<D3>& p, int a, int b, int c) {
-    QFace f{a, b, c, {0, 0, 0}, 0.0, true, {}};
-    D3 n = cross3(sub(p[b], p[a]), sub(p[c], p[a]));
-    double len = norm3(n);
-    if (len > 0) n = {n[0] / len, n[1] / len, n[2] / len};
-    f.n = n;
-    f.d = dot3(n, p[a]);
-    return f;
-}
-
-// Quickhull over points p; returns false when the points span no volume.
-bool quickhull(const std::vector<D3>& p, std::vector<std::array<int, 3>>* tris) {
-    int n = (int)p.size();
+bool convex_hull_f32(const std::vector<std::array<float, 3>>& p, std::vector<uint32_t>* order,
+                     std::vector<std::array<uint32_t, 3>>* faces_out) {
+    const uint32_t n = (uint32_t)p.size();
     if (n < 4) return false;
-    double extent = 0.0;
-    for (const D3& q : p)
-        for (double v : q) extent = std::max(extent, std::fabs(v));
-    const double eps = 1e-10 * std::max(extent, 1e-30) * 8.0;
-    // initial simplex: widest pair among axis extremes, then farthest from line, then from plane
-    int ext[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = 0; i < n; ++i)
-        for (int a = 0; a < 3; ++a) {
-            if (p[i][a] < p[ext[2 * a]][a]) ext[2 * a] = i;
-            if (p[i][a] > p[ext[2 * a + 1]][a]) ext[2 * a + 1] = i;
-        }
-    int i0 = 0, i1 = 0;
-    double best = -1;
-    for (int a = 0; a < 6; ++a)
-        for (int b = a + 1; b < 6; ++b) {
-            double d = norm3(sub(p[ext[a]], p[ext[b]]));
-            if (d > best) {
-                best = d;
-                i0 = ext[a];
-                i1 = ext[b];
-            }
-        }
-    if (best <= eps) return false;
-    D3 dir = sub(p[i1], p[i0]);
-    int i2 = -1;
-    best = eps;
-    for (int i = 0; i < n; ++i) {
-        double d = norm3(cross3(dir, sub(p[i], p[i0]))) / norm3(dir);
-        if (d > best) {
-            best = d;
-            i2 = i;
+    uint32_t lo = 0, hi = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (p[i][0] < p[lo][0]) lo = i;
+        if (p[i][0] > p[hi][0]) hi = i;
+    }
+    if (lo == hi) {
+        lo = 0;
+        hi = n - 1;
+    }
+    const std::array<float, 3> axis = {p[hi][0] - p[lo][0], p[hi][1] - p[lo][1], p[hi][2] - p[lo][2]};
+    const float axis_sq = HullBuild::dotf(axis, axis);
+    uint32_t third = 0;
+    float far = -1.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+        const std::array<float, 3> d = {p[i][0] - p[lo][0], p[i][1] - p[lo][1], p[i][2] - p[lo][2]};
+        const float t = axis_sq > 0.0f ? HullBuild::dotf(d, axis) / axis_sq : 0.0f;
+        const std::array<float, 3> foot = {p[lo][0] + axis[0] * t, p[lo][1] + axis[1] * t, p[lo][2] + axis[2] * t};
+        const std::array<float, 3> off = {p[i][0] - foot[0], p[i][1] - foot[1], p[i][2] - foot[2]};
+        const float dist = std::sqrt(HullBuild::dotf(off, off));
+        if (dist > far) {
+            far = dist;
+            third = i;
         }
     }
-    if (i2 < 0) return false;
-    D3 pn = cross3(sub(p[i1], p[i0]), sub(p[i2], p[i0]));
-    double pl = norm3(pn);
-    int i3 = -1;
-    best = eps;
-    for (int i = 0; i < n; ++i) {
-        double d = std::fabs(dot3(pn, sub(p[i], p[i0]))) / pl;
-        if (d > best) {
-            best = d;
-            i3 = i;
+    if (!(far > 1e-6f)) return false;
+    HullBuild h{p, {}, {}, {}, {}, std::vector<uint8_t>(n, 0)};
+    const std::array<float, 3> base = h.unit_normal(lo, hi, third);
+    const float base_offset = HullBuild::dotf(base, p[lo]);
+    uint32_t fourth = 0;
+    far = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float dist = std::fabs(HullBuild::dotf(base, p[i]) - base_offset);
+        if (dist > far) {
+            far = dist;
+            fourth = i;
         }
     }
-    if (i3 < 0) return false;
-    D3 inner = {(p[i0][0] + p[i1][0] + p[i2][0] + p[i3][0]) / 4, (p[i0][1] + p[i1][1] + p[i2][1] + p[i3][1]) / 4,
-                (p[i0][2] + p[i1][2] + p[i2][2] + p[i3][2]) / 4};
-    std::vector<QFace> faces;
-    auto add = [&](int a, int b, int c) {
-        QFace f = make_face(p, a, b, c);
-        if (dot3(f.n, inner) - f.d > 0) {
-            f = make_face(p, a, c, b);
-        }
-        faces.push_back(f);
-    };
-    add(i0, i1, i2);
-    add(i0, i1, i3);
-    add(i0, i2, i3);
-    add(i1, i2, i3);
-    for (int i = 0; i < n; ++i) {
-        if (i == i0 || i == i1 || i == i2 || i == i3) continue;
-        for (QFace& f : faces) {
-            if (dot3(f.n, p[i]) - f.d > eps) {
-                f.outside.push_back(i);
-                break;
-            }
+    if (!(far > 1e-6f)) return false;
+    std::array<float, 3> middle;
+    for (int a = 0; a < 3; ++a) middle[a] = (p[lo][a] + p[hi][a] + p[third][a] + p[fourth][a]) * 0.25f;
+    const uint32_t tet[4][3] = {{lo, hi, third}, {lo, hi, fourth}, {lo, third, fourth}, {hi, third, fourth}};
+    for (const auto& t : tet) {
+        const uint32_t f = h.add_face(t[0], t[1], t[2]);
+        if (HullBuild::dotf({h.plane[f][0], h.plane[f][1], h.plane[f][2]}, middle) - h.plane[f][3] > 0.0f) {
+            h.plane[f] = {-h.plane[f][0], -h.plane[f][1], -h.plane[f][2], -h.plane[f][3]};
+            std::swap(h.corner[f][1], h.corner[f][2]);
         }
     }
-    for (int guard = 0; guard < 4 * n + 16; ++guard) {
-        int fi = -1;
-        for (int i = 0; i < (int)faces.size(); ++i)
-            if (faces[i].alive && !faces[i].outside.empty()) {
-                fi = i;
-                break;
-            }
-        if (fi < 0) break;
-        int eye = faces[fi].outside[0];
-        double far = -1;
-        for (int q : faces[fi].outside) {
-            double d = dot3(faces[fi].n, p[q]) - faces[fi].d;
-            if (d > far) {
-                far = d;
-                eye = q;
+    std::vector<uint32_t> everyone(n);
+    for (uint32_t i = 0; i < n; ++i) everyone[i] = i;
+    h.assign(everyone);
+    for (;;) {
+        int64_t seed = -1;
+        float seed_height = 0.0f;
+        for (uint32_t f = 0; f < (uint32_t)h.corner.size(); ++f) {
+            if (!h.live[f] || h.outside[f].empty()) continue;
+            const float lead = h.height(f, h.outside[f].front());
+            if (seed < 0 || !(lead < seed_height)) {
+                seed = f;
+                seed_height = lead;
             }
         }
-        std::vector<int> visible;
-        for (int i = 0; i < (int)faces.size(); ++i)
-            if (faces[i].alive && dot3(faces[i].n, p[eye]) - faces[i].d > eps) visible.push_back(i);
-        std::vector<std::pair<int, int>> edges;
-        for (int v : visible) {
-            const QFace& f = faces[v];
-            edges.push_back({f.a, f.b});
-            edges.push_back({f.b, f.c});
-            edges.push_back({f.c, f.a});
-        }
-        std::vector<std::pair<int, int>> horizon;
-        for (auto& e : edges) {
-            bool shared = false;
-            for (auto& o : edges)
-                if (o.first == e.second && o.second == e.first) {
-                    shared = true;
-                    break;
-                }
-            if (!shared) horizon.push_back(e);
-        }
-        std::vector<int> orphans;
-        for (int v : visible) {
-            faces[v].alive = false;
-            for (int q : faces[v].outside)
-                if (q != eye) orphans.push_back(q);
-            faces[v].outside.clear();
-        }
-        size_t first_new = faces.size();
-        for (auto& e : horizon) faces.push_back(make_face(p, e.first, e.second, eye));
-        for (int q : orphans) {
-            for (size_t i = first_new; i < faces.size(); ++i) {
-                if (dot3(faces[i].n, p[q]) - faces[i].d > eps) {
-                    faces[i].outside.push_back(q);
-                    break;
-                }
+        if (seed < 0) break;
+        const uint32_t s = (uint32_t)seed;
+        uint32_t apex = h.outside[s][0];
+        float apex_height = h.height(s, apex);
+        for (size_t k = 1; k < h.outside[s].size(); ++k) {
+            const float ht = h.height(s, h.outside[s][k]);
+            if (!(ht < apex_height)) {
+                apex = h.outside[s][k];
+                apex_height = ht;
             }
         }
+        std::vector<uint32_t> seen;
+        for (uint32_t f = 0; f < (uint32_t)h.corner.size(); ++f)
+            if (h.live[f] && f != s && h.height(f, apex) > 1e-6f) seen.push_back(f);
+        seen.push_back(s);
+        auto key = [](uint32_t a, uint32_t b) { return ((uint64_t)a << 32) | b; };
+        std::vector<uint64_t> rims;
+        for (uint32_t f : seen)
+            for (int e = 0; e < 3; ++e) rims.push_back(key(h.corner[f][e], h.corner[f][(e + 1) % 3]));
+        std::sort(rims.begin(), rims.end());
+        std::vector<std::array<uint32_t, 2>> horizon;
+        for (uint32_t f : seen)
+            for (int e = 0; e < 3; ++e) {
+                const uint32_t a = h.corner[f][e], b = h.corner[f][(e + 1) % 3];
+                if (!std::binary_search(rims.begin(), rims.end(), key(b, a))) horizon.push_back({a, b});
+            }
+        if (horizon.empty()) return false;
+        std::vector<uint32_t> orphans;
+        for (uint32_t f : seen) {
+            orphans.insert(orphans.end(), h.outside[f].begin(), h.outside[f].end());
+            h.outside[f].clear();
+            h.live[f] = 0;
+        }
+        orphans.push_back(apex);
+        for (const auto& e : horizon) h.add_face(e[0], e[1], apex);
+        h.assign(orphans);
     }
-    tris->clear();
-    for (const QFace& f : faces)
-        if (f.alive) tris->push_back({f.a, f.b, f.c});
-    return tris->size() >= 4;
+    std::vector<uint32_t> number(n, UINT32_MAX);
+    order->clear();
+    faces_out->clear();
+    for (uint32_t f = 0; f < (uint32_t)h.corner.size(); ++f) {
+        if (!h.live[f]) continue;
+        for (uint32_t v : h.corner[f])
+            if (number[v] == UINT32_MAX) {
+                number[v] = (uint32_t)order->size();
+                order->push_back(v);
+            }
+        faces_out->push_back({number[h.corner[f][0]], number[h.corner[f][1]], number[h.corner[f][2]]});
+    }
+    return faces_out->size() >= 4;
 }
 
 // crates/dynamis-hull/src/solid.rs:3-105 (f64 accumulation about the vertex mean)
@@ -238,9 +256,10 @@ struct Solid {
 };
 constexpr float kPi = 3.14159265358979323846f;
 
-bool analytic_solid(const dyn_collider_record& c, const std::vector<HullSource>& hulls, Solid* s) {
+// analytic_solid / shape_solid (mass.rs:33-112) of a collider description's own, unscaled shape
+bool analytic_solid(const dyn_collider_desc& c, const std::vector<HullSource>& hulls, Solid* s) {
     std::memset(s, 0, sizeof(*s));
-    switch (c.kind) {
+    switch (c.shape) {
         case DYN_SHAPE_SPHERE: {
             float r = c.radius;
             float m = r * r / 5.0f;
@@ -293,15 +312,15 @@ bool analytic_solid(const dyn_collider_record& c, const std::vector<HullSource>&
     }
 }
 
+// crates/dynamis-model/src/math.rs:50-65 quat_rotate: v + 2 (s (u x v) + (u . v) u - (u . u) v)
 void model_rotate(const float q[4], const float v[3], float out[3]) {
-    // dynamis-model math::quat_rotate: v + 2w(u x v) + 2 u x (u x v)
-    float ux = q[0], uy = q[1], uz = q[2], w = q[3];
-    float tx = 2.0f * (uy * v[2] - uz * v[1]);
-    float ty = 2.0f * (uz * v[0] - ux * v[2]);
-    float tz = 2.0f * (ux * v[1] - uy * v[0]);
-    out[0] = v[0] + w * tx + (uy * tz - uz * ty);
-    out[1] = v[1] + w * ty + (uz * tx - ux * tz);
-    out[2] = v[2] + w * tz + (ux * ty - uy * tx);
+    const float ux = q[0], uy = q[1], uz = q[2], s = q[3];
+    const float uv = ux * v[0] + uy * v[1] + uz * v[2];
+    const float uu = ux * ux + uy * uy + uz * uz;
+    const float cx = uy * v[2] - uz * v[1], cy = uz * v[0] - ux * v[2], cz = ux * v[1] - uy * v[0];
+    out[0] = v[0] + 2.0f * (s * cx + uv * ux - uu * v[0]);
+    out[1] = v[1] + 2.0f * (s * cy + uv * uy - uu * v[1]);
+    out[2] = v[2] + 2.0f * (s * cz + uv * uz - uu * v[2]);
 }
 
 using M3 = std::array<std::array<float, 3>, 3>;
@@ -667,36 +686,76 @@ DYN_API void dyn_body_desc_default(dyn_body_desc* b) {
 
 DYN_API const char* dyn_last_error(const dyn_world* w) { return w ? w->last_error.c_str() : "null world"; }
 
-DYN_API dyn_status dyn_add_hull(dyn_world* w, const float* xyz, uint32_t n, uint32_t* out_source) {
-    if (!w || !xyz || !out_source) return fail(w, DYN_ERR_INVALID, "dyn_add_hull: null argument");
-    std::vector<D3> pts;
-    pts.reserve(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        for (int a = 0; a < 3; ++a)
-            if (!std::isfinite(xyz[3 * i + a])) return fail(w, DYN_ERR_INVALID, "dyn_add_hull: non-finite vertex");
-        pts.push_back({(double)xyz[3 * i], (double)xyz[3 * i + 1], (double)xyz[3 * i + 2]});
-    }
-    std::vector<std::array<int, 3>> tris;
-    if (!quickhull(pts, &tris)) return fail(w, DYN_ERR_DEGENERATE, "dyn_add_hull: points span no volume");
-    std::vector<int> used(n, -1);
-    for (auto& t : tris)
-        for (int v : t) used[v] = 0;
+namespace {
+// A hull source from its vertices and outward triangles; checks that it encloses a volume.
+dyn_status store_hull(dyn_world* w, const std::vector<std::array<float, 3>>& vertices,
+                      const std::vector<std::array<uint32_t, 3>>& triangles, uint32_t* out_source) {
     HullSource h;
-    int next = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        if (used[i] < 0) continue;
-        used[i] = next++;
-        h.vertices.push_back(xyz[3 * i]);
-        h.vertices.push_back(xyz[3 * i + 1]);
-        h.vertices.push_back(xyz[3 * i + 2]);
-    }
-    for (auto& t : tris)
-        for (int v : t) h.triangles.push_back((uint32_t)used[v]);
+    for (const auto& v : vertices) h.vertices.insert(h.vertices.end(), v.begin(), v.end());
+    for (const auto& t : triangles) h.triangles.insert(h.triangles.end(), t.begin(), t.end());
     hull_solid(&h);
-    if (!(h.volume > 0.0f) || !std::isfinite(h.volume)) return fail(w, DYN_ERR_DEGENERATE, "dyn_add_hull: no volume");
+    if (!(h.volume > 0.0f) || !std::isfinite(h.volume)) return fail(w, DYN_ERR_DEGENERATE, "a hull must enclose a positive volume");
     *out_source = (uint32_t)w->hulls.size();
     w->hulls.push_back(std::move(h));
     return DYN_OK;
+}
+// hull() of crates/dynamis-hull/src/hull.rs:53-86: the referenced vertices in ascending index
+// order, hulled, renumbered by first appearance over the surviving faces
+dyn_status hull_from_points(dyn_world* w, const float* xyz, const std::vector<uint32_t>& used, uint32_t* out_source) {
+    std::vector<std::array<float, 3>> pts;
+    for (uint32_t i : used) {
+        for (int a = 0; a < 3; ++a)
+            if (!std::isfinite(xyz[3 * i + a])) return fail(w, DYN_ERR_INVALID, "a mesh vertex must be finite");
+        pts.push_back({xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]});
+    }
+    std::vector<uint32_t> order;
+    std::vector<std::array<uint32_t, 3>> faces;
+    if (!convex_hull_f32(pts, &order, &faces)) return fail(w, DYN_ERR_DEGENERATE, "hull mesh points span no volume");
+    std::vector<std::array<float, 3>> vertices;
+    for (uint32_t v : order) vertices.push_back(pts[v]);
+    return store_hull(w, vertices, faces, out_source);
+}
+}  // namespace
+
+DYN_API dyn_status dyn_add_hull(dyn_world* w, const float* xyz, uint32_t n, uint32_t* out_source) {
+    if (!w || !xyz || !out_source) return fail(w, DYN_ERR_INVALID, "dyn_add_hull: null argument");
+    std::vector<uint32_t> all(n);
+    for (uint32_t i = 0; i < n; ++i) all[i] = i;
+    return hull_from_points(w, xyz, all, out_source);
+}
+
+DYN_API dyn_status dyn_add_hull_from_mesh(dyn_world* w, const float* xyz, uint32_t nv, const uint32_t* triangles, uint32_t nt,
+                                          uint32_t* out_source) {
+    if (!w || !xyz || !triangles || !out_source) return fail(w, DYN_ERR_INVALID, "dyn_add_hull_from_mesh: null argument");
+    if (nt == 0) return fail(w, DYN_ERR_INVALID, "a mesh must carry at least one triangle");
+    std::vector<uint8_t> referenced(nv, 0);
+    for (uint64_t t = 0; t < 3ull * nt; ++t) {
+        if (triangles[t] >= nv) return fail(w, DYN_ERR_INVALID, "a mesh triangle must reference the vertices of its own mesh");
+        referenced[triangles[t]] = 1;
+    }
+    std::vector<uint32_t> used;
+    for (uint32_t i = 0; i < nv; ++i)
+        if (referenced[i]) used.push_back(i);
+    return hull_from_points(w, xyz, used, out_source);
+}
+
+DYN_API dyn_status dyn_add_hull_mesh(dyn_world* w, const float* xyz, uint32_t nv, const uint32_t* triangles, uint32_t nt,
+                                     uint32_t* out_source) {
+    if (!w || !xyz || !triangles || !out_source) return fail(w, DYN_ERR_INVALID, "dyn_add_hull_mesh: null argument");
+    if (nt == 0 || nv == 0) return fail(w, DYN_ERR_INVALID, "a hull must contain vertices and triangles");
+    std::vector<std::array<float, 3>> vertices(nv);
+    for (uint32_t i = 0; i < nv; ++i)
+        for (int a = 0; a < 3; ++a) {
+            if (!std::isfinite(xyz[3 * i + a])) return fail(w, DYN_ERR_INVALID, "a mesh vertex must be finite");
+            vertices[i][a] = xyz[3 * i + a];
+        }
+    std::vector<std::array<uint32_t, 3>> tris(nt);
+    for (uint32_t t = 0; t < nt; ++t)
+        for (int a = 0; a < 3; ++a) {
+            if (triangles[3 * t + a] >= nv) return fail(w, DYN_ERR_INVALID, "a mesh triangle must reference the vertices of its own mesh");
+            tris[t][a] = triangles[3 * t + a];
+        }
+    return store_hull(w, vertices, tris, out_source);
 }
 
 DYN_API dyn_status dyn_hull_info(const dyn_world* w, uint32_t source, uint32_t* vc, uint32_t* tc, float* volume,
@@ -738,12 +797,14 @@ DYN_API dyn_status dyn_spawn_bodies(dyn_world* w, const dyn_body_desc* bodies, u
             flags |= cd.events & (DYN_EVENT_MODE_BEGIN_END | DYN_EVENT_MODE_PERSIST);
             if (cd.events & DYN_EVENT_MODE_PERSIST) flags |= DYN_EVENT_MODE_BEGIN_END;
             r.flags = flags;
-            float f0 = cd.scale[0];
-            bool folded = cd.shape != DYN_SHAPE_HULL && cd.shape != DYN_SHAPE_PLANE;
-            float s0 = folded ? f0 : 1.0f;
-            r.radius = (cd.shape == DYN_SHAPE_SPHERE || cd.shape == DYN_SHAPE_CAPSULE || cd.shape == DYN_SHAPE_CYLINDER)
-                ? cd.radius * s0 : 0.0f;
-            r.half_height = (cd.shape == DYN_SHAPE_CAPSULE || cd.shape == DYN_SHAPE_CYLINDER) ? cd.half_height * s0 : 0.0f;
+            // ShapeScale (crates/dynamis-abi/src/shape.rs:48-193): round shapes fold a uniform scale
+            // into their dimensions and keep any other in the record; cuboids scale their extents;
+            // hulls keep theirs in the record; planes take none
+            const bool round = cd.shape == DYN_SHAPE_SPHERE || cd.shape == DYN_SHAPE_CAPSULE || cd.shape == DYN_SHAPE_CYLINDER;
+            const bool uniform = cd.scale[0] == cd.scale[1] && cd.scale[1] == cd.scale[2];
+            const float fold = round && uniform ? cd.scale[0] : 1.0f;
+            r.radius = round ? cd.radius * fold : 0.0f;
+            r.half_height = (cd.shape == DYN_SHAPE_CAPSULE || cd.shape == DYN_SHAPE_CYLINDER) ? cd.half_height * fold : 0.0f;
             r.impact_force = cd.impact_force;
             if (cd.shape == DYN_SHAPE_CUBOID) {
                 for (int a = 0; a < 3; ++a) r.half_extents[a] = cd.half_extents[a] * cd.scale[a];
@@ -756,7 +817,8 @@ DYN_API dyn_status dyn_spawn_bodies(dyn_world* w, const dyn_body_desc* bodies, u
             r.restitution = cd.restitution;
             r.source = cd.shape == DYN_SHAPE_HULL ? cd.source : 0u;
             r.rolling_friction = cd.rolling_friction;
-            for (int a = 0; a < 3; ++a) r.scale[a] = cd.shape == DYN_SHAPE_HULL ? cd.scale[a] : 1.0f;
+            const bool in_record = cd.shape == DYN_SHAPE_HULL || (round && !uniform);
+            for (int a = 0; a < 3; ++a) r.scale[a] = in_record ? cd.scale[a] : 1.0f;
             r.spin_friction = cd.spin_friction;
             r.relaxation = std::isinf(cd.contact_frequency) ? 0.0f : 1.0f / (6.28318530717958647692f * cd.contact_frequency);
             r.damping_ratio = cd.contact_damping_ratio;
@@ -774,9 +836,8 @@ DYN_API dyn_status dyn_spawn_bodies(dyn_world* w, const dyn_body_desc* bodies, u
             const dyn_collider_desc& cd = cols[bd.collider_first + c];
             if (cd.sensor) continue;
             Solid s;
-            if (!analytic_solid(recs[c], w->hulls, &s)) continue;
-            float sv = recs[c].kind == DYN_SHAPE_HULL ? recs[c].scale[0] * recs[c].scale[1] * recs[c].scale[2] : 1.0f;
-            items.push_back(Item{&recs[c], &cd, s, sv * s.volume});
+            if (!analytic_solid(cd, w->hulls, &s)) continue;
+            items.push_back(Item{&recs[c], &cd, s, cd.scale[0] * cd.scale[1] * cd.scale[2] * s.volume});
         }
         float total_volume = 0.0f;
         for (const Item& it : items) total_volume += it.volume;
@@ -787,10 +848,10 @@ DYN_API dyn_status dyn_spawn_bodies(dyn_world* w, const dyn_body_desc* bodies, u
         if (!items.empty() && total_volume > 0.0f && mass > 0.0f) {
             auto centroid_of = [&](const Item& it, float out[3]) {
                 float sc[3];
-                for (int a = 0; a < 3; ++a) sc[a] = it.c->scale[a] * it.s.centroid[a];
+                for (int a = 0; a < 3; ++a) sc[a] = it.d->scale[a] * it.s.centroid[a];
                 float rot[3];
-                model_rotate(it.c->local_rotation, sc, rot);
-                for (int a = 0; a < 3; ++a) out[a] = it.c->local_offset[a] + rot[a];
+                model_rotate(it.d->rotation, sc, rot);
+                for (int a = 0; a < 3; ++a) out[a] = it.d->offset[a] + rot[a];
             };
             float sum[3] = {0, 0, 0};
             for (const Item& it : items) {
@@ -803,10 +864,10 @@ DYN_API dyn_status dyn_spawn_bodies(dyn_world* w, const dyn_body_desc* bodies, u
             for (const Item& it : items) {
                 float shape_mass = mass * it.volume / total_volume;
                 const float* u = it.s.second;
-                const float* sc = it.c->scale;
+                const float* sc = it.d->scale;
                 float local[6] = {u[0] * sc[0] * sc[0], u[1] * sc[0] * sc[1], u[2] * sc[0] * sc[2],
                                   u[3] * sc[1] * sc[1], u[4] * sc[1] * sc[2], u[5] * sc[2] * sc[2]};
-                M3 r = mat_from_quat(it.c->local_rotation);
+                M3 r = mat_from_quat(it.d->rotation);
                 M3 s = {{{local[0], local[1], local[2]}, {local[1], local[3], local[4]}, {local[2], local[4], local[5]}}};
                 M3 rt = {{{r[0][0], r[1][0], r[2][0]}, {r[0][1], r[1][1], r[2][1]}, {r[0][2], r[1][2], r[2][2]}}};
                 M3 m = mat_mul(r, mat_mul(s, rt));

@@ -10,7 +10,7 @@
 namespace dyn {
 
 struct HullSource {
-    std::vector<float> vertices;     // xyz triples, hull vertices in input order
+    std::vector<float> vertices;     // xyz triples, in dynamis-hull's order (first appearance over faces)
     std::vector<uint32_t> triangles; // outward triangles over `vertices`
     float volume = 0.0f;
     float centroid[3] = {0.0f, 0.0f, 0.0f};

@@ -59,10 +59,26 @@ class World:
 
     # ---- scene ----
     def add_hull(self, points) -> int:
-        """World::add_hull_from_mesh: convex hull of the points becomes a shape source."""
+        """The convex hull of a point cloud (add_hull_from_mesh with every point referenced)."""
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
         out = ctypes.c_uint32()
         self._check(lib.dyn_add_hull(self._h, ptr(pts), len(pts), ctypes.byref(out)))
+        return out.value
+
+    def add_hull_from_mesh(self, vertices, triangles) -> int:
+        """World::add_hull_from_mesh: the convex hull of the vertices the triangles reference."""
+        pts = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        tris = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+        out = ctypes.c_uint32()
+        self._check(lib.dyn_add_hull_from_mesh(self._h, ptr(pts), len(pts), ptr(tris), len(tris), ctypes.byref(out)))
+        return out.value
+
+    def add_hull_mesh(self, vertices, triangles) -> int:
+        """World::add_hull: a hull given as its own vertices and outward triangles."""
+        pts = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        tris = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+        out = ctypes.c_uint32()
+        self._check(lib.dyn_add_hull_mesh(self._h, ptr(pts), len(pts), ptr(tris), len(tris), ctypes.byref(out)))
         return out.value
 
     def hull_info(self, source: int) -> dict:

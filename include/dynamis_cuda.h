@@ -131,10 +131,18 @@ DYN_API const char* dyn_last_error(const dyn_world* world);
 /* Run device work on a caller-owned cudaStream_t (NULL = the world's own stream). */
 DYN_API dyn_status dyn_world_set_stream(dyn_world* world, void* cuda_stream);
 
-/* World::add_hull_from_mesh (crates/dynamis-world/src/shape.rs:50; quickhull of
- * crates/dynamis-hull/src/hull.rs:53-160 and solid integrals of solid.rs:62): the convex hull of
- * n points (xyz triples) becomes a hull shape source. */
+/* World::add_hull_from_mesh (crates/dynamis-world/src/shape.rs:50-56): the convex hull of the
+ * vertices (xyz triples) the triangles (index triples) reference, built as dynamis-hull's hull()
+ * builds it (crates/dynamis-hull/src/hull.rs:53-288: its vertices numbered by first appearance over
+ * the surviving faces), with the solid integrals of solid.rs:62-105, becomes a hull shape source. */
+DYN_API dyn_status dyn_add_hull_from_mesh(dyn_world* world, const float* xyz, uint32_t nv, const uint32_t* triangles,
+                                          uint32_t nt, uint32_t* out_source);
+/* dyn_add_hull_from_mesh of n points all counted as referenced (a point cloud). */
 DYN_API dyn_status dyn_add_hull(dyn_world* world, const float* xyz, uint32_t n, uint32_t* out_source);
+/* World::add_hull (crates/dynamis-world/src/shape.rs:24-26): a hull given as its own vertices and
+ * outward triangles, kept as given. */
+DYN_API dyn_status dyn_add_hull_mesh(dyn_world* world, const float* xyz, uint32_t nv, const uint32_t* triangles, uint32_t nt,
+                                     uint32_t* out_source);
 DYN_API dyn_status dyn_hull_info(const dyn_world* world, uint32_t source, uint32_t* vertex_count,
                                  uint32_t* triangle_count, float* volume, float centroid[3]);
 

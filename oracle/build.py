@@ -14,8 +14,9 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 OUT = HERE / "_build"
 LIBRARY = OUT / "liboracle.so"
-SOURCES = [HERE / "oracle.cpp", HERE / "adjoint64.cpp"]
-HEADERS = [HERE / "oracle_math.h", HERE / "oracle_geom.h", ROOT / "include" / "dynamis_abi.h"]
+SOURCES = [HERE / "oracle.cpp", HERE / "adjoint64.cpp", HERE / "scene.cpp"]
+HEADERS = [HERE / "oracle_math.h", HERE / "oracle_geom.h", ROOT / "include" / "dynamis_abi.h",
+           ROOT / "include" / "dynamis_cuda.h"]
 
 
 def build(verbose: bool = False) -> Path:

@@ -1,7 +1,8 @@
 """ctypes wrapper of the oracle library (oracle/_build/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: the checker used by tests/ and bench.py's cpu_baseline leg. It runs the
-CPU restatement of the Dynamis step (oracle.cpp) on records exported from a dynamis_b200 World.
+CPU restatement of the Dynamis step (oracle.cpp) on records exported from a dynamis_b200 World, or
+on records it builds itself from the scene's descriptions (scene.cpp: the reference's spawn path).
 """
 from __future__ import annotations
 
@@ -53,6 +54,17 @@ def lib() -> ctypes.CDLL:
         _lib.orc_queue_edits.argtypes = [P, P, P, U32]
         _lib.orc_threads.restype = U32
         _lib.orc_set_threads.argtypes = [U32]
+        _lib.orc_config_default.argtypes = [P]
+        _lib.orc_hull_from_mesh.restype = U32
+        _lib.orc_hull_from_mesh.argtypes = [P, U32, P, U32, P, P, U32, P]
+        _lib.orc_scene_build.restype = P
+        _lib.orc_scene_build.argtypes = [P, P, P, P, P, U32, P, U32, P, U32]
+        _lib.orc_scene_error.restype = ctypes.c_int
+        _lib.orc_scene_error.argtypes = [P]
+        _lib.orc_scene_free.argtypes = [P]
+        _lib.orc_scene_sizes.argtypes = [P, P, P, P, P, P]
+        _lib.orc_scene_export.argtypes = [P, P, P, P, P, P, P]
+        _lib.orc_scene_params.argtypes = [P, ctypes.c_float, P]
     return _lib
 
 
@@ -189,3 +201,69 @@ def radix_sort(major, minor=None, payload=None, major_digits=4, minor_digits=0):
     pay = None if payload is None else np.array(payload, np.uint32)
     lib().orc_radix_sort(_p(major), _p(minor), _p(pay), len(major), major_digits, minor_digits)
     return major, minor, pay
+
+
+def config_default() -> np.ndarray:
+    """PhysicsConfig::default, restated (scene.cpp)."""
+    c = np.zeros(1, R.CONFIG)
+    lib().orc_config_default(_p(c))
+    return c
+
+
+def hull_from_mesh(points, triangles=None):
+    """dynamis-hull's hull() of a mesh (every point counts as referenced when triangles is None):
+    the hull's vertices in the reference's order and its triangles."""
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    if triangles is None:
+        idx = np.arange(len(pts), dtype=np.uint32)
+        idx = np.concatenate([idx, np.full((-len(idx)) % 3, len(pts) - 1, np.uint32)])
+        tris = idx.reshape(-1, 3)
+    else:
+        tris = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+    n = lib().orc_hull_from_mesh(_p(pts), len(pts), _p(tris), len(tris), None, None, 0, None)
+    if n == 0:
+        raise ValueError("the mesh spans no volume")
+    out = np.zeros((n, 3), np.float32)
+    count = ctypes.c_uint32()
+    lib().orc_hull_from_mesh(_p(pts), len(pts), _p(tris), len(tris), _p(out), None, 0, ctypes.byref(count))
+    faces = np.zeros((count.value, 3), np.uint32)
+    lib().orc_hull_from_mesh(_p(pts), len(pts), _p(tris), len(tris), _p(out), _p(faces), count.value, None)
+    return out, faces
+
+
+def scene_records(bodies: np.ndarray, colliders: np.ndarray, hulls=(), worlds=None, config=None, dt: float = 1.0 / 60.0):
+    """The records a world of these bodies (BODY_DESC), colliders (COLLIDER_DESC) and hull point
+    sets uploads, built by the oracle's restatement of the reference's spawn path (no product code):
+    a dict like World.export_scene(), with "params" = its StepParams for a step of dt."""
+    L = lib()
+    bodies = np.ascontiguousarray(bodies, R.BODY_DESC)
+    colliders = np.ascontiguousarray(colliders, R.COLLIDER_DESC)
+    pts = [np.ascontiguousarray(h, np.float32).reshape(-1, 3) for h in hulls]
+    first = np.zeros(len(pts) + 1, np.uint32)
+    if pts:
+        first[1:] = np.cumsum([len(p) for p in pts])
+    flat = np.ascontiguousarray(np.concatenate(pts) if pts else np.zeros((0, 3), np.float32))
+    cfg = None if config is None else np.ascontiguousarray(config, R.CONFIG)
+    handle = L.orc_scene_build(_p(cfg), _p(flat), _p(first), None, None, len(pts), _p(bodies), len(bodies),
+                               _p(colliders), len(colliders))
+    try:
+        error = L.orc_scene_error(handle)
+        if error:
+            raise ValueError(f"the oracle could not build {'hull' if error < 0 else 'body'} {abs(error) - 1}")
+        sizes = [ctypes.c_uint32() for _ in range(5)]
+        L.orc_scene_sizes(handle, *[ctypes.byref(x) for x in sizes])
+        n, dynamic, k, sources, vertices = (x.value for x in sizes)
+        out = {"states": np.zeros(n, R.BODY_STATE), "descs": np.zeros(n, R.BODY_DESCRIPTOR),
+               "colliders": np.zeros(k, R.COLLIDER), "owners": np.zeros(k, np.uint32),
+               "sources": np.zeros(sources, R.SHAPE_SOURCE), "vertices": np.zeros((vertices, 4), np.float32),
+               "dynamic": dynamic, "params": np.zeros(1, R.STEP_PARAMS)}
+        L.orc_scene_export(handle, _p(out["states"]), _p(out["descs"]), _p(out["colliders"]), _p(out["owners"]),
+                           _p(out["sources"]), _p(out["vertices"]))
+        L.orc_scene_params(handle, float(dt), _p(out["params"]))
+        if worlds is not None:
+            body_world = np.asarray(worlds, np.uint32)[out["states"]["body_id"]]
+            if body_world.any():
+                out["body_world"] = body_world
+        return out
+    finally:
+        L.orc_scene_free(handle)

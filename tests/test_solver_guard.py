@@ -9,7 +9,8 @@ they do not, and the reference's own algorithm pumps energy into the pile. These
   (step 29, the box that left at 265 m/s): the iteration matrix I - D^-1 A has an eigenvalue of -2.01,
   and the guard's bound rejects the block; count x A_jj gives a spectral radius below 1;
 * the reference's algorithm (the oracle, guard off) on the 1,000-body mixed pile: within 90 steps
-  the total energy rises far above its start and a body outruns free fall from the top;
+  the total energy rises above its start (to 1.55 x) and a body outruns free fall from the top by
+  a factor of six;
 * the guard on the same pile: energy never above its start, no body faster than free fall;
 * the guard leaves converging blocks alone: on a tower of cubes resting face to face (four-point
   manifolds whose normalised coupling eigenvalues stay at 1.5 or below), 60 guarded steps are
@@ -80,8 +81,8 @@ def pile_run(guard: int, side: int = 10, steps: int = 90):
 
 def test_the_reference_solver_pumps_energy_into_the_mixed_pile():
     ratio, speed, bound = pile_run(guard=0)
-    assert ratio > 2.0, ratio
-    assert speed > bound, (speed, bound)
+    assert ratio > 1.2, ratio  # a passive system gains energy: measured 1.55 x its start
+    assert speed > 3.0 * bound, (speed, bound)  # measured 97 m/s against a 16 m/s free-fall bound
 
 
 def test_the_row_mass_guard_keeps_the_mixed_pile_within_bounds():
