@@ -1288,6 +1288,9 @@ __global__ void k_island_link(DeviceWorld w, dyn_step_params p) {
 // (pointer jumping doubles the reach each round and a chain is at most N long); one pass that
 // follows each chain to its root gives that same array. Roots no longer change here, and rows
 // rewritten concurrently only ever point further up their own chain.
+// After the last links (kAggregate) the root each row finds is final, so the same pass does
+// island_aggregate's work (island_aggregate.wgsl): count the islands and mark the ones to wake.
+template <bool kAggregate>
 __global__ void k_island_flatten(DeviceWorld w) {
     GRID_STRIDE(i, w.nd) {
         uint32_t root = i;
@@ -1297,14 +1300,9 @@ __global__ void k_island_flatten(DeviceWorld w) {
             parent = __ldcg(w.parents + root);
         }
         w.parents[i] = root;
-    }
-}
-__global__ void k_island_aggregate(DeviceWorld w) {
-    GRID_STRIDE(i, w.nd) {
-        uint32_t root = w.parents[i];
+        if (!kAggregate) continue;
         if (root == i) add_counter(&w.counters[DYN_COUNTER_ISLANDS], 1u);
         if (w.wake_flags[i] == 0u && w.motion[i] == 0u) continue;
-        // a large island's rows all aim at one word: once it holds the mark, the max is a no-op
         if (__ldcg(w.istate + root) >= DYN_ISLAND_WAKE) continue;
         atomicMax(&w.istate[root], DYN_ISLAND_WAKE);
     }

@@ -735,11 +735,10 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     k_contact_begin<<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
     mark(ST_ISLANDS);
     k_island_link<true><<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
-    k_island_flatten<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
+    k_island_flatten<false><<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     k_island_link<false><<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
     if (dw.jcount) k_island_link_joints<<<blocks_for(d, dw.jcount, 256), 256, 0, s>>>(dw);
-    k_island_flatten<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
-    k_island_aggregate<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
+    k_island_flatten<true><<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
     k_wake_live<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     join(2, side);

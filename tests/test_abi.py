@@ -106,3 +106,16 @@ def test_counter_slots_follow_the_reference_declaration_order():
     assert R.COUNTER["LIVE"] == 40
     assert R.COUNTER["REFUSED_SOFT_EVENTS"] == 51
     assert len(R.COUNTERS) == R.COUNTER_DEVICE_COUNT == 52
+
+
+def test_the_rust_binding_declares_every_entry_point():
+    """integration/dynamis-cuda-sys/src/lib.rs (the crate a Dynamis maintainer adds; no Rust toolchain
+    here) declares exactly the entry points include/dynamis_cuda.h exports."""
+    import re
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    header = re.sub(r"/\*.*?\*/", "", (root / "include" / "dynamis_cuda.h").read_text(), flags=re.S)
+    exported = set(re.findall(r"DYN_API\s+[^;(]*?\b(dyn_\w+)\s*\(", header))
+    rust = set(re.findall(r"pub fn (dyn_\w+)\(", (root / "integration" / "dynamis-cuda-sys" / "src" / "lib.rs").read_text()))
+    assert exported and rust == exported, (exported - rust, rust - exported)
