@@ -234,6 +234,14 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     log("setup done")
     setup_checks = long_run_checks(world, DT, before, top)
     log(f"setup checks {setup_checks}")
+    launch = {"tuned": False}
+    if not args.no_tune:
+        from dynamis_b200 import tuning
+
+        t0 = time.perf_counter()
+        shapes, tuned_ms, ran = tuning.tuned(world, args.workload, DT, args.tuning_cache)
+        launch = {**shapes, "tuned": ran, "tuner_ms_per_step": tuned_ms, "tune_s": round(time.perf_counter() - t0, 2)}
+        log(f"launch shapes {launch}")
     for _ in range(args.warmup):
         world.step(DT)
     world.wait()
@@ -321,15 +329,18 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
                      "algorithmic_bytes_per_launch": algo, "ms_per_launch": per_launch_ms},
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "stage_frac": stage_frac,
+        "launch_config": launch,
         "setup_checks": setup_checks,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks.summary(),
     }
-    if not args.no_batch:
+    # the measurements beside the headline run at N = 1 only (the scaling runs time the replicas)
+    extras = world_size == 1
+    if extras and not args.no_batch:
         result["batch"] = batch_benchmark(args, local_rank)
-    if not args.no_guarded:
+    if extras and not args.no_guarded:
         result["guarded"] = guarded_run(args, DT, local_rank)
-    if not args.no_adjoint:
+    if extras and not args.no_adjoint:
         result["adjoint"] = adjoint_benchmark(local_rank, steps=args.adjoint_steps, settle=args.adjoint_setup)
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(world, budget_s=args.cpu_budget, dt=DT)
@@ -435,7 +446,7 @@ def adjoint_benchmark(device: int, steps: int = 120, settle: int = 60, interval:
             "forward_body_steps_per_s": bodies * steps / (forward_ms * 1e-3), "gradients_finite": finite}
 
 
-def batch_benchmark(args, device: int, worlds: int = 4096, setup: int = 10, warmup: int = 3, steps: int = 10) -> dict:
+def batch_benchmark(args, device: int, worlds: int = 4096, setup: int = 5, warmup: int = 2, steps: int = 5) -> dict:
     """Batched worlds (the survey's fourth configuration): `worlds` sub-worlds in one World, one
     graph launch a step, against the same worlds as a loop of plain single-world steps (one World
     and one graph launch each, on one stream), every world of the loop timed, after the same setup
@@ -582,6 +593,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-towers measurement")
     ap.add_argument("--no-guarded", action="store_true", help="skip the run with the row-mass guard")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
+    ap.add_argument("--tuning-cache", default=None, help="JSON file of per-workload launch shapes to reuse and extend")
     ap.add_argument("--adjoint-only", action="store_true", help="print only the differentiable-towers measurement")
     ap.add_argument("--adjoint-steps", type=int, default=120)
     ap.add_argument("--adjoint-setup", type=int, default=60)

@@ -1705,7 +1705,7 @@ __device__ __forceinline__ void solve_block(const DeviceWorld& w, const dyn_step
     }
 }
 // tape_index: substep x iterations + iteration, where a taped step writes its snapshots
-__global__ void __launch_bounds__(128, 4) k_solve(DeviceWorld w, dyn_step_params p, uint32_t tape_index) {
+__global__ void __launch_bounds__(256, 2) k_solve(DeviceWorld w, dyn_step_params p, uint32_t tape_index) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     const bool residual = w.ctl[CTL_ROUNDS] == p.solve_iterations;
     GRID_STRIDE(i, count) solve_block(w, p, i, residual, tape_index);

@@ -130,6 +130,8 @@ struct DeviceState {
     bool uploaded = false;  // the current scene's records are on the device
     uint32_t graph_kernels = 0;  // kernel nodes in one step's graph
     uint32_t sms = 148;          // multiprocessors of the device (read when the device state is made)
+    dyn_launch_config launch{16u, 128u, 6u, 8u};  // dyn_set_launch_config / dyn_autotune
+    bool tuning = false;         // dyn_autotune is running trials: the contact stream keeps its layout
     dyn_step_params params{};
     // timing
     std::vector<cudaEvent_t> events;
@@ -184,7 +186,7 @@ inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) /
 // Grid-stride launches: enough blocks for n threads, at most 16 blocks per SM of the device.
 inline uint32_t blocks_for(const DeviceState* d, uint32_t n, uint32_t threads) {
     uint32_t b = div_up(std::max<uint32_t>(n, 1), threads);
-    return std::min<uint32_t>(b, d->sms * 16u);
+    return std::min<uint32_t>(b, d->sms * d->launch.grid_blocks_per_sm);
 }
 
 void release_graphs(DeviceState* d) {
@@ -225,6 +227,7 @@ dyn_status ensure_device(dyn_world* w) {
         int sm_count = 0;
         DYN_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, w->device));
         d->sms = (uint32_t)std::max(sm_count, 1);
+        d->launch = w->launch;
         DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream2, cudaStreamNonBlocking));
@@ -707,11 +710,11 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     k_narrow_class<PC_BOXES><<<blocks_for(d, P, 128), 128, 0, side>>>(dw, p);
     k_convex_reject<<<blocks_for(d, P, 128), 128, 0, s>>>(dw, p);
     // persistent: lanes draw pairs from a ticket; six blocks per SM is the occupancy its registers allow
-    k_convex_gjk<<<d->sms * 6u, 128, 0, s>>>(dw, p);
+    k_convex_gjk<<<d->sms * d->launch.gjk_blocks_per_sm, 128, 0, s>>>(dw, p);
     // separated pairs (probe) and penetrating ones (EPA) are disjoint queues
     fork(3, side2);
     k_convex_probe<<<blocks_for(d, P, 128), 128, 0, side2>>>(dw, p);
-    k_convex_epa<<<d->sms * 8u, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
+    k_convex_epa<<<d->sms * d->launch.epa_blocks_per_sm, 32 * kEpaWarpsPerBlock, 0, s>>>(dw, p);
     join(3, side2);
     k_convex_manifold<<<blocks_for(d, P, 128), 128, 0, s>>>(dw, p);
     join(1, side);
@@ -747,17 +750,18 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
         mark(ST_INTEGRATE);
         if (tape) k_tape_hot<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, *tape, sub);
         k_integrate<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, p);
-        k_solve_prepare<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
+        const uint32_t st = d->launch.solve_threads;
+        k_solve_prepare<<<blocks_for(d, C, st), st, 0, s>>>(dw);
         if (sub == 0) {
             mark(ST_WARM);
             if (joint_blocks) k_joints<JP_WARM><<<joint_blocks, 32, 0, s>>>(dw, p);
-            k_warm<<<blocks_for(d, C, 128), 128, 0, s>>>(dw);
+            k_warm<<<blocks_for(d, C, st), st, 0, s>>>(dw);
             k_vapply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_VELOCITY);
         for (uint32_t it = 0; it < p.solve_iterations; ++it) {
             if (joint_blocks) k_joints<JP_SOLVE><<<joint_blocks, 32, 0, s>>>(dw, p);
-            k_solve<<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, sub * p.solve_iterations + it);
+            k_solve<<<blocks_for(d, C, st), st, 0, s>>>(dw, p, sub * p.solve_iterations + it);
             k_vapply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
         }
         mark(ST_ADVANCE);
@@ -767,9 +771,9 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
             // each iteration applies the one before it; one apply after the last
             for (uint32_t it = 0; it < p.position_iterations; ++it) {
                 if (it == 0u) {
-                    k_position_fused<true><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it, sub);
+                    k_position_fused<true><<<blocks_for(d, C, st), st, 0, s>>>(dw, p, it, sub);
                 } else {
-                    k_position_fused<false><<<blocks_for(d, C, 128), 128, 0, s>>>(dw, p, it, sub);
+                    k_position_fused<false><<<blocks_for(d, C, st), st, 0, s>>>(dw, p, it, sub);
                 }
             }
             if (p.position_iterations > 0u) {
@@ -1236,7 +1240,7 @@ constexpr uint64_t kMaxContactCapacity = 1ull << 26;
 dyn_status widen_contact_stream(dyn_world* w) {
     DeviceState* d = w->dev;
     volatile uint32_t* mail = d->spill_host;
-    if (!mail || d->c_cap >= kMaxContactCapacity || d->tape.active) return DYN_OK;
+    if (!mail || d->c_cap >= kMaxContactCapacity || d->tape.active || d->tuning) return DYN_OK;
     if (mail[3] <= d->c_cap - d->c_cap / 4) return DYN_OK;
     DYN_CUDA(cudaStreamSynchronize(d->stream));
     const uint64_t demand = mail[3];
@@ -2213,6 +2217,100 @@ DYN_API dyn_status dyn_debug_islands(dyn_world* w, uint32_t* out, uint32_t cap, 
 }
 
 DYN_API uint32_t dyn_step_kernel_count(const dyn_world* w) { return (w && w->dev) ? w->dev->graph_kernels : 0u; }
+
+DYN_API dyn_status dyn_set_launch_config(dyn_world* w, const dyn_launch_config* c) {
+    if (!w || !c) return DYN_ERR_INVALID;
+    if (c->grid_blocks_per_sm < 1u || c->grid_blocks_per_sm > 64u || c->gjk_blocks_per_sm < 1u || c->gjk_blocks_per_sm > 16u ||
+        c->epa_blocks_per_sm < 1u || c->epa_blocks_per_sm > 16u ||
+        (c->solve_threads != 64u && c->solve_threads != 128u && c->solve_threads != 256u))
+        return fail(w, DYN_ERR_INVALID, "dyn_set_launch_config: a field is out of its range");
+    if (!w->dev) {
+        w->launch = *c;
+        return DYN_OK;
+    }
+    if (w->dev->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_set_launch_config: a tape is recording");
+    w->launch = *c;
+    if (std::memcmp(&w->dev->launch, c, sizeof(*c)) != 0) {
+        DYN_CUDA(cudaSetDevice(w->device));
+        DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
+        w->dev->launch = *c;
+        release_graphs(w->dev);  // the step graphs carry the launch shapes: record them again
+    }
+    return DYN_OK;
+}
+DYN_API dyn_status dyn_get_launch_config(const dyn_world* w, dyn_launch_config* out) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    *out = w->dev ? w->dev->launch : w->launch;
+    return DYN_OK;
+}
+
+// Coordinate descent over the launch shapes, each trial from the same checkpoint: every candidate
+// value of one field with the others at their best so far, two rounds over the fields.
+DYN_API dyn_status dyn_autotune(dyn_world* w, float dt, uint32_t steps, dyn_launch_config* best, float* best_ms) {
+    if (!w || steps == 0u) return DYN_ERR_INVALID;
+    if (!w->dev || !w->dev->uploaded) return fail(w, DYN_ERR_INVALID, "dyn_autotune: step the world once first");
+    DeviceState* d = w->dev;
+    if (d->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_autotune: a tape is recording");
+    if (!w->edits.empty()) return fail(w, DYN_ERR_INVALID, "dyn_autotune: body edits are queued");
+    DYN_CUDA(cudaSetDevice(w->device));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    Checkpoint saved;
+    dyn_status st = save_checkpoint(w, &saved);
+    if (st) return st;
+    d->tuning = true;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    auto trial = [&](const dyn_launch_config& c, float* ms) -> dyn_status {
+        dyn_status s2 = dyn_set_launch_config(w, &c);
+        if (s2) return s2;
+        if ((s2 = restore_checkpoint(w, saved))) return s2;
+        if ((s2 = step_once(w, dt, false))) return s2;  // records the graph, warms the caches
+        DYN_CUDA(cudaEventRecord(t0, d->stream));
+        for (uint32_t k = 0; k < steps; ++k)
+            if ((s2 = step_once(w, dt, false))) return s2;
+        DYN_CUDA(cudaEventRecord(t1, d->stream));
+        DYN_CUDA(cudaEventSynchronize(t1));
+        DYN_CUDA(cudaEventElapsedTime(ms, t0, t1));
+        *ms /= (float)steps;
+        return DYN_OK;
+    };
+    dyn_launch_config top = d->launch;
+    float top_ms = 0.0f;
+    st = trial(top, &top_ms);
+    const uint32_t grids[] = {4u, 8u, 16u, 32u}, threads[] = {64u, 128u, 256u}, gjks[] = {4u, 6u, 8u, 12u}, epas[] = {4u, 8u, 12u};
+    for (int round = 0; round < 2 && !st; ++round) {
+        for (int field = 0; field < 4 && !st; ++field) {
+            const uint32_t* values = field == 0 ? grids : field == 1 ? threads : field == 2 ? gjks : epas;
+            const int count = field == 1 || field == 3 ? 3 : 4;
+            for (int v = 0; v < count && !st; ++v) {
+                dyn_launch_config c = top;
+                uint32_t* slot = field == 0 ? &c.grid_blocks_per_sm : field == 1 ? &c.solve_threads
+                                 : field == 2 ? &c.gjk_blocks_per_sm : &c.epa_blocks_per_sm;
+                if (*slot == values[v]) continue;
+                *slot = values[v];
+                float ms = 0.0f;
+                st = trial(c, &ms);
+                if (!st && ms < top_ms) {
+                    top = c;
+                    top_ms = ms;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    d->tuning = false;
+    if (!st) st = dyn_set_launch_config(w, &top);
+    dyn_status restored = restore_checkpoint(w, saved);
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    free_checkpoint(&saved);
+    if (st) return st;
+    if (restored) return restored;
+    if (best) *best = top;
+    if (best_ms) *best_ms = top_ms;
+    return DYN_OK;
+}
 
 DYN_API dyn_status dyn_set_solver_guard(dyn_world* w, uint32_t flags) {
     if (!w) return DYN_ERR_INVALID;

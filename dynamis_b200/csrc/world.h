@@ -96,6 +96,7 @@ struct dyn_world {
     std::vector<dyn_body_edit_record> edits;
     bool timing = false;
     uint32_t solver_guard = 0;  // DYN_SOLVER_GUARD_* bits (dyn_set_solver_guard)
+    dyn_launch_config launch{16u, 128u, 6u, 8u};  // applied when the device state is made
     void* user_stream = nullptr;  // caller's cudaStream_t (dyn_world_set_stream)
     uint64_t steps_taken = 0;     // dyn_step calls since creation
     dyn::Observer observer;

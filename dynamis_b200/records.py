@@ -135,6 +135,8 @@ CONFIG = np.dtype([
     ("sleep_time", "<f4"), ("friction_combine", "<u4"), ("restitution_combine", "<u4"),
 ])
 CAPACITY = np.dtype([("bodies", "<u4"), ("colliders", "<u4"), ("pairs", "<u4"), ("contacts", "<u4")])
+LAUNCH_CONFIG = np.dtype([("grid_blocks_per_sm", "<u4"), ("solve_threads", "<u4"), ("gjk_blocks_per_sm", "<u4"),
+                          ("epa_blocks_per_sm", "<u4")])
 COLLIDER_DESC = np.dtype([
     ("shape", "<u4"), ("radius", "<f4"), ("half_height", "<f4"), ("half_extents", "<f4", 3), ("source", "<u4"),
     ("offset", "<f4", 3), ("rotation", "<f4", 4), ("scale", "<f4", 3), ("friction", "<f4"),

@@ -256,6 +256,27 @@ class World:
         self._check(lib.dyn_joint_plan(self._h, ptr(rows), ptr(layers), ptr(comps), None, None))
         return {"rows": rows, "layers": layers, "components": comps}
 
+    def launch_config(self) -> dict:
+        """dyn_get_launch_config: the launch shapes the step uses."""
+        c = np.zeros(1, R.LAUNCH_CONFIG)
+        self._check(lib.dyn_get_launch_config(self._h, ptr(c)))
+        return {k: int(c[k][0]) for k in R.LAUNCH_CONFIG.names}
+
+    def set_launch_config(self, **fields) -> None:
+        """dyn_set_launch_config: change any of the launch shapes (no result changes)."""
+        c = np.zeros(1, R.LAUNCH_CONFIG)
+        for k, v in {**self.launch_config(), **fields}.items():
+            c[k] = v
+        self._check(lib.dyn_set_launch_config(self._h, ptr(c)))
+
+    def autotune(self, dt: float, steps: int = 3) -> tuple[dict, float]:
+        """dyn_autotune: the fastest launch shapes for this world as it stands (kept), with their
+        device time per step in ms; the world's state is left as it was."""
+        c = np.zeros(1, R.LAUNCH_CONFIG)
+        ms = ctypes.c_float()
+        self._check(lib.dyn_autotune(self._h, float(dt), int(steps), ptr(c), ctypes.byref(ms)))
+        return {k: int(c[k][0]) for k in R.LAUNCH_CONFIG.names}, ms.value
+
     def set_solver_guard(self, flags: int) -> None:
         """dyn_set_solver_guard: SOLVER_GUARD_ROW_MASS keeps every contact block's Jacobi iteration
         convergent where the reference's manifold row masses would let it diverge; 0 (the default)

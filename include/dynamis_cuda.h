@@ -309,6 +309,29 @@ DYN_API dyn_status dyn_radix_sort_static_status(void* cuda_stream, uint32_t* out
 #define DYN_STATUS_ISLAND_HOOKS 2u
 #define DYN_STATUS_ADJOINT_UNSUPPORTED 4u  /* a reversed step met a contact the adjoint does not cover */
 
+/* Launch shapes of the step's kernels, no counterpart in the reference (its wgpu passes use fixed
+ * workgroup sizes). None of them changes a result, only the time a step takes. grid_blocks_per_sm:
+ * the blocks per SM a grid-stride launch is capped at (1-64, default 16); solve_threads: threads per
+ * block of the contact blocks' kernels, the solve, its prepare, the warm start and the position
+ * passes (64, 128 or 256, default 128); gjk_blocks_per_sm, epa_blocks_per_sm: blocks per SM of the
+ * persistent GJK and EPA kernels (1-16, defaults 6 and 8). Takes effect at the next dyn_step;
+ * refused while a tape records. */
+typedef struct dyn_launch_config {
+    uint32_t grid_blocks_per_sm;
+    uint32_t solve_threads;
+    uint32_t gjk_blocks_per_sm;
+    uint32_t epa_blocks_per_sm;
+} dyn_launch_config;
+DYN_API dyn_status dyn_set_launch_config(dyn_world* world, const dyn_launch_config* config);
+DYN_API dyn_status dyn_get_launch_config(const dyn_world* world, dyn_launch_config* out);
+/* The autotuner, no counterpart in the reference: on the world as it stands, times `steps` steps of
+ * dt for each candidate launch configuration (coordinate descent over the four fields, two rounds,
+ * every trial from the same saved state), and keeps the fastest (also written to best, its device
+ * time per step to best_ms; either may be NULL). Afterwards the world holds the state it had before
+ * the call, counters included. Needs a world that has stepped (its device state exists), no tape
+ * recording and no queued body edits. Synchronises the world's stream. */
+DYN_API dyn_status dyn_autotune(dyn_world* world, float dt, uint32_t steps, dyn_launch_config* best, float* best_ms);
+
 /* Solver guards, no counterpart in the reference (0, the default, is the reference's solver).
  * DYN_SOLVER_GUARD_ROW_MASS: the reference solves a contact's points together against manifold row
  * masses (solver_contact_block.wgsl:14-29, manifold_row_mass), and for some manifolds (a tilted box

@@ -154,6 +154,16 @@ pub struct DynConstraintRows {
     pub second_row: u32,
 }
 
+/// Launch shapes of the step's kernels (dyn_launch_config); dyn_autotune picks them.
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
+pub struct DynLaunchConfig {
+    pub grid_blocks_per_sm: u32,
+    pub solve_threads: u32,
+    pub gjk_blocks_per_sm: u32,
+    pub epa_blocks_per_sm: u32,
+}
+
 pub const DYN_OK: DynStatus = 0;
 pub const DYN_SOLVER_GUARD_ROW_MASS: u32 = 1;
 
@@ -213,6 +223,9 @@ extern "C" {
     pub fn dyn_joint_plan(world: *const DynWorld, rows: *mut u32, layers: *mut u32, components: *mut u32, layer_count: *mut u32, component_count: *mut u32) -> DynStatus;
     pub fn dyn_radix_sort_static(major: *mut u32, minor: *mut u32, payload: *mut u32, n: u32, major_digits: u32, minor_digits: u32, cuda_stream: *mut c_void) -> DynStatus;
     pub fn dyn_radix_sort_static_status(cuda_stream: *mut c_void, out: *mut u32) -> DynStatus;
+    pub fn dyn_set_launch_config(world: *mut DynWorld, config: *const DynLaunchConfig) -> DynStatus;
+    pub fn dyn_get_launch_config(world: *const DynWorld, out: *mut DynLaunchConfig) -> DynStatus;
+    pub fn dyn_autotune(world: *mut DynWorld, dt: f32, steps: u32, best: *mut DynLaunchConfig, best_ms: *mut f32) -> DynStatus;
     pub fn dyn_set_solver_guard(world: *mut DynWorld, flags: u32) -> DynStatus;
     pub fn dyn_clear_device_status(world: *mut DynWorld) -> DynStatus;
     pub fn dyn_debug_sort_fault(world: *mut DynWorld, skipped_tiles: u32, spin_limit: u32) -> DynStatus;
