@@ -52,6 +52,7 @@ SIGNATURES = {
     "dyn_debug_islands": (I32, [P, P, U32, PU32]),
     "dyn_set_timing": (I32, [P, I32]),
     "dyn_set_solver_guard": (I32, [P, U32]),
+    "dyn_set_ccd": (I32, [P, U32, I32]),
     "dyn_set_launch_config": (I32, [P, P]),
     "dyn_get_launch_config": (I32, [P, P]),
     "dyn_autotune": (I32, [P, ctypes.c_float, U32, P, P]),

@@ -174,6 +174,9 @@ DYN_HD float datan2(float y, float x) {
     }
     return w + datan(y / x);
 }
+// acos through the identity acos(x) = atan2(sqrt((1 - x)(1 + x)), x) on [-1, 1], so that it rests on
+// the same Cephes atan as the rest of the step.
+DYN_HD float dacos(float value) { return datan2(sqrtf((1.0f - value) * (1.0f + value)), value); }
 
 // ---- quaternions (xyz = vector part, w = scalar) ----
 DYN_HD float4 quat_mul(float4 a, float4 b) {

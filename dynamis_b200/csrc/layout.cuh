@@ -68,6 +68,7 @@ enum Ctl : uint32_t {
     CTL_PROBES = 18,         // separated convex pairs queued for the penetration probe
     CTL_EPA_NEXT = 19,       // next penetrating pair ticket of the EPA kernel
     CTL_STAGED = 20,         // contacts the narrowphase staged (every contact it found: at most one per pair)
+    CTL_CCD_HITS = 21,       // sweep hits the continuous-collision pass recorded
     CTL_COUNT = 32
 };
 
@@ -112,6 +113,12 @@ struct DeviceWorld {
     uint32_t* row_of_id;
     uint32_t id_count;
     uint32_t* body_world;  // sub-world of each row (all 0 outside a batch)
+    // continuous collision (ccd.cuh), per row: the bitwise complement of the earliest sweep hit's
+    // time bits and of its (lower, higher collider) pair key, 0 when the row has none this step,
+    // and that hit (normal + restitution, point + time)
+    uint32_t* ccd_time;
+    unsigned long long* ccd_key;
+    float4* ccd_impact;  // [2n]
     // colliders
     uint32_t* c_owner;
     uint4* c_kind;     // kind, flags, source, 0

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "ccd.cuh"
 #include "joints.cuh"
 #include "step.cuh"
 #include "world.h"
@@ -35,13 +36,14 @@ enum Stage : uint32_t {
     ST_VELOCITY,
     ST_ADVANCE,
     ST_POSITION,
+    ST_CCD,
     ST_SLEEP,
     ST_COUNT
 };
 static const char* kStageNames[ST_COUNT] = {"begin",       "aabb",     "entries",   "entry_sort",     "pairs",
                                             "narrowphase", "compact",  "identity",       "islands",
                                             "wake_live",   "solver_prepare", "integrate", "warm_start", "velocity",
-                                            "advance",     "position", "sleep"};
+                                            "advance",     "position", "ccd",       "sleep"};
 
 // A recorded trajectory for the adjoint (dyn_tape_begin ... dyn_tape_end): checkpoints on the
 // device, the taped segment and the gradient buffers.
@@ -268,6 +270,9 @@ dyn_status ensure_device(dyn_world* w) {
         d->id_cap = std::max(N, ids + ids / 2);  // room for spawns after removals
         A(dw.row_of_id, d->id_cap);
         A(dw.body_world, N);
+        A(dw.ccd_time, N);
+        A(dw.ccd_key, N);
+        A(dw.ccd_impact, 2 * (size_t)N);
         A(dw.edit_count, 1);
         A(dw.c_owner, K);
         A(dw.c_kind, K);
@@ -642,6 +647,15 @@ struct Marker {
     }
 };
 
+// Does any body of the world declare continuous collision (the reference's CCD gate,
+// crates/dynamis-rigid/src/domain.rs:85-96 from World::ccd_active, crates/dynamis-world/src/body.rs:503-514)?
+bool world_has_ccd(const dyn_world* w) {
+    for (const dyn_body_descriptor_record& desc : w->descs) {
+        if (desc.flags & DYN_BODY_CCD) return true;
+    }
+    return false;
+}
+
 // Issues one step's kernels on `s`. parity selects which contact set is current. With a tape the
 // step also snapshots what its adjoint needs into the tape's current slot (adjoint.cuh): the relay,
 // k_solve and the fused position kernels write theirs as they run; the contact set and the body
@@ -786,6 +800,14 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
                 k_papply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
             }
         }
+    }
+    if (world_has_ccd(w)) {
+        // continuous collision of the bodies that declare it (ccd.cuh): sweep, pick, impact, retreat
+        mark(ST_CCD);
+        k_ccd_sweep<<<blocks_for(d, P, 128), 128, 0, s>>>(dw, p);
+        k_ccd_pick<<<blocks_for(d, 2 * P, 256), 256, 0, s>>>(dw);
+        k_ccd_impact<<<blocks_for(d, 2 * P, 256), 256, 0, s>>>(dw);
+        k_ccd_apply<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
     }
     mark(ST_SLEEP);
     k_sleep<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw, p);
@@ -1746,6 +1768,7 @@ DYN_API dyn_status dyn_tape_begin(dyn_world* w, uint32_t checkpoint_interval) {
     if (!w->joint_descs.empty()) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: constraints are not differentiated");
     if (w->solver_guard) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: the adjoint differentiates the reference's solver (no guard)");
     rebuild_rows(w);
+    if (world_has_ccd(w)) return fail(w, DYN_ERR_INVALID, "dyn_tape_begin: continuous collision is not differentiated");
     for (uint32_t i = 0; i < w->dynamic_count && i < w->descs.size(); ++i) {
         const float* ii = w->descs[i].inverse_inertia;
         if (w->descs[i].inverse_mass > 0.0f && !(ii[1] == 0.0f && ii[2] == 0.0f && ii[4] == 0.0f && ii[0] == ii[3] && ii[3] == ii[5]))
@@ -2323,6 +2346,41 @@ DYN_API dyn_status dyn_set_solver_guard(dyn_world* w, uint32_t flags) {
         DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
         release_graphs(w->dev);  // the step graphs carry the flag: record them again
     }
+    return DYN_OK;
+}
+
+// World::set_ccd (crates/dynamis-world/src/body.rs:496-501): only a simulated body may declare
+// continuous collision; a changed descriptor wakes the body (install_body, body.rs:284-290). The
+// flag is patched into the device's body row in place, so the archived contacts and the simulated
+// states stay; the step graph is recorded again when the world gains its first CCD body or loses
+// its last.
+DYN_API dyn_status dyn_set_ccd(dyn_world* w, uint32_t body_id, int32_t enabled) {
+    if (!w) return DYN_ERR_INVALID;
+    if (w->dev && w->dev->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_set_ccd: a tape is recording");
+    rebuild_rows(w);
+    if (body_id >= w->row_of_id.size() || w->row_of_id[body_id] == DYN_NO_BODY)
+        return fail(w, DYN_ERR_INVALID, "dyn_set_ccd: unknown body id");
+    const uint32_t row = w->row_of_id[body_id];
+    dyn_body_descriptor_record& desc = w->descs[row];
+    if (enabled && !(desc.inverse_mass > 0.0f && (desc.flags & DYN_BODY_KINEMATIC) == 0u))
+        return fail(w, DYN_ERR_INVALID, "dyn_set_ccd: only a simulated body can declare continuous collision");
+    const uint32_t flags = enabled ? (desc.flags | DYN_BODY_CCD) : (desc.flags & ~DYN_BODY_CCD);
+    if (flags == desc.flags) return DYN_OK;
+    const bool gate_before = world_has_ccd(w);
+    desc.flags = flags;
+    if (body_id < w->spawn_descs.size()) w->spawn_descs[body_id].flags = flags;
+    // rows or scene out of date: the next step uploads the scene, flags included
+    if (w->dev && w->dev->uploaded && !w->scene_dirty && !(w->rows_dirty && !w->raw_rows)) {
+        DeviceState* d = w->dev;
+        DYN_CUDA(cudaSetDevice(w->device));
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        DYN_CUDA(cudaMemcpy(&d->dw.hot[row].aux.y, &flags, sizeof(flags), cudaMemcpyHostToDevice));
+        if (gate_before != world_has_ccd(w)) release_graphs(d);
+    }
+    dyn_body_edit_record wake{};
+    wake.kind = DYN_EDIT_WAKE;
+    w->edit_ids.push_back(body_id);
+    w->edits.push_back(wake);
     return DYN_OK;
 }
 

@@ -26,6 +26,7 @@ NO_BODY = 0xFFFFFFFF
 NO_COLLISION_FILTER = 0xFFFFFFFF
 CONTACT_ANNOUNCED = 0x80000000
 BODY_KINEMATIC = 1  # BodyDescriptorRecord flags (constant.rs)
+BODY_CCD = 2
 SOLVER_GUARD_ROW_MASS = 1  # dyn_set_solver_guard
 
 

@@ -283,6 +283,11 @@ class World:
         is the reference's solver."""
         self._check(lib.dyn_set_solver_guard(self._h, int(flags)))
 
+    def set_ccd(self, body_id: int, enabled: bool = True) -> None:
+        """dyn_set_ccd (World::set_ccd): declares or clears continuous collision for a simulated body;
+        a changed flag wakes the body at the next step."""
+        self._check(lib.dyn_set_ccd(self._h, int(body_id), 1 if enabled else 0))
+
     def step_params(self, dt: float) -> np.ndarray:
         p = np.zeros(1, R.STEP_PARAMS)
         self._check(lib.dyn_step_params_for(self._h, float(dt), ptr(p)))

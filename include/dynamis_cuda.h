@@ -346,6 +346,15 @@ DYN_API dyn_status dyn_autotune(dyn_world* world, float dt, uint32_t steps, dyn_
 #define DYN_SOLVER_GUARD_ROW_MASS 1u
 DYN_API dyn_status dyn_set_solver_guard(dyn_world* world, uint32_t flags);
 
+/* World::set_ccd (crates/dynamis-world/src/body.rs:496-501): declares or clears continuous collision
+ * for one body (also settable at spawn, dyn_body_desc.ccd). Only a simulated (dynamic, not
+ * kinematic) body may declare it (DYN_ERR_INVALID otherwise); a changed flag queues a wake of the
+ * body for the next step, as the reference's install_body does (body.rs:284-290). While any body
+ * declares it, every step sweeps the candidate pairs of those bodies over the step's motion and
+ * moves each to its earliest impact (ccd_sweep.wgsl, ccd_apply.wgsl), after the substeps and
+ * before sleep. Refused while a tape records; dyn_tape_begin refuses a world with a CCD body. */
+DYN_API dyn_status dyn_set_ccd(dyn_world* world, uint32_t body_id, int32_t enabled);
+
 /* Clears the world's sticky device status word (dyn_sync keeps reporting it until this call or a
  * new scene upload). Synchronises the world's stream. No counterpart in the reference, which has
  * no device status word. */

@@ -227,6 +227,7 @@ extern "C" {
     pub fn dyn_get_launch_config(world: *const DynWorld, out: *mut DynLaunchConfig) -> DynStatus;
     pub fn dyn_autotune(world: *mut DynWorld, dt: f32, steps: u32, best: *mut DynLaunchConfig, best_ms: *mut f32) -> DynStatus;
     pub fn dyn_set_solver_guard(world: *mut DynWorld, flags: u32) -> DynStatus;
+    pub fn dyn_set_ccd(world: *mut DynWorld, body_id: u32, enabled: i32) -> DynStatus;
     pub fn dyn_clear_device_status(world: *mut DynWorld) -> DynStatus;
     pub fn dyn_debug_sort_fault(world: *mut DynWorld, skipped_tiles: u32, spin_limit: u32) -> DynStatus;
     pub fn dyn_tape_begin(world: *mut DynWorld, checkpoint_interval: u32) -> DynStatus;

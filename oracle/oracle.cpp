@@ -1791,6 +1791,188 @@ void solve_substeps(OracleWorld& w) {
 }
 
 // island_sleep.wgsl:10-29 (core.wgsl:218-227 freeze_body)
+// ---- continuous collision: crates/dynamis-rigid/shaders/ccd_sweep.wgsl, ccd_apply.wgsl ----
+
+// core.wgsl:149-163
+V4 quat_slerp(V4 a, V4 b, float t) {
+    float cosine = dot(a, b);
+    if (cosine < 0.0f) {
+        b = -b;
+        cosine = -cosine;
+    }
+    if (cosine > 0.9995f) return normalize(a + (b - a) * t);
+    float angle = oacos(clampw(cosine, -1.0f, 1.0f));
+    float sine = osin(angle);
+    return (a * (osin((1.0f - t) * angle) / sine)) + (b * (osin(t * angle) / sine));
+}
+// core.wgsl:165-168
+float quat_angle(V4 a, V4 b) { return 2.0f * oacos(std::fabs(clampw(dot(a, b), -1.0f, 1.0f))); }
+
+struct SweepPose {
+    Body body;
+    V3 prev_position;
+    V4 prev_orientation;
+};
+SweepPose sweep_body(const OracleWorld& w, uint32_t row) {
+    const dyn_body_state_record& s = w.states[row];
+    return SweepPose{body_at(w, row), rd3(s.prev_position), rd4(s.prev_orientation)};
+}
+// ccd_sweep.wgsl:40-45
+WorldShape sweep_collider(const SweepPose& s, const dyn_collider_record& c, float t) {
+    V3 position = s.prev_position + (s.body.position - s.prev_position) * t;
+    return world_collider(position, quat_slerp(s.prev_orientation, s.body.orientation, t), c);
+}
+// ccd_sweep.wgsl:47-54
+float sweep_radius(const OracleWorld& w, const Body& b, const dyn_collider_record& c) {
+    if (c.kind == DYN_SHAPE_PLANE) return 0.0f;
+    Aabb bounds = world_aabb_of(w.shapes, world_collider(b.position, b.orientation, c));
+    V3 center = b.position + quat_rotate(b.orientation, rd3(c.local_offset));
+    return length((bounds.max - bounds.min) * 0.5f) + length(center - body_com(b));
+}
+// ccd_sweep.wgsl:56-61: (travel, spin)
+void sweep_reach(const OracleWorld& w, const SweepPose& s, const dyn_collider_record& c, float* travel, float* spin) {
+    *travel = length(s.body.position - s.prev_position);
+    *spin = quat_angle(s.prev_orientation, s.body.orientation) * sweep_radius(w, s.body, c);
+}
+// ccd_sweep.wgsl:63-69
+ShapeHit plane_convex_gap(const OracleWorld& w, const WorldShape& plane, const WorldShape& convex) {
+    V3 normal = quat_rotate(plane.rotation, V3{0.0f, 1.0f, 0.0f});
+    float side = dot(convex.center - plane.center, normal);
+    V3 facing = side < 0.0f ? -normal : normal;
+    float extent = dot(support(w.shapes, convex, facing) - convex.center, facing);
+    return ShapeHit{std::fabs(side) - extent, convex.center + facing * extent, facing, DYN_NO_TRIANGLE};
+}
+// ccd_sweep.wgsl:71-98 (triangle scenes are refused at scene set-up: no hit)
+ShapeHit pair_gap(const OracleWorld& w, const WorldShape& first, const WorldShape& second) {
+    if (first.kind == DYN_SHAPE_PLANE) {
+        ShapeHit swapped = plane_convex_gap(w, first, second);
+        return ShapeHit{swapped.distance, swapped.point, -swapped.normal, DYN_NO_TRIANGLE};
+    }
+    if (second.kind == DYN_SHAPE_PLANE) return plane_convex_gap(w, second, first);
+    if (shape_world_geometry(first.kind) || shape_world_geometry(second.kind))
+        return ShapeHit{kNoHit, splat3(0.0f), splat3(0.0f), DYN_NO_TRIANGLE};
+    return convex_hit(w.shapes, first, second);
+}
+
+struct SweepHit {
+    float time;
+    V3 normal, point;
+};
+// ccd_sweep.wgsl:100-147
+SweepHit rigid_sweep(const OracleWorld& w, const SweepPose& moving, const dyn_collider_record& mc, const SweepPose& other,
+                     const dyn_collider_record& oc) {
+    const SweepHit none{1.0f, V3{0.0f, 1.0f, 0.0f}, splat3(0.0f)};
+    if (!body_has_ccd(moving.body)) return none;
+    float free_travel_len = 0.0f, free_spin = 0.0f, other_travel_len = 0.0f, other_spin = 0.0f;
+    sweep_reach(w, moving, mc, &free_travel_len, &free_spin);
+    bool other_movable = body_moves(other.body);
+    if (other_movable) sweep_reach(w, other, oc, &other_travel_len, &other_spin);
+    float closing_floor = free_spin + other_spin;
+    if (free_travel_len + closing_floor + other_travel_len <= 0.0f) return none;
+    V3 free_travel = moving.body.position - moving.prev_position;
+    V3 other_travel = other_movable ? other.body.position - other.prev_position : splat3(0.0f);
+    float t = 0.0f;
+    for (uint32_t iteration = 0; iteration < 16u; ++iteration) {
+        WorldShape free = sweep_collider(moving, mc, t);
+        WorldShape fixed = other_movable ? sweep_collider(other, oc, t)
+                                         : world_collider(other.body.position, other.body.orientation, oc);
+        ShapeHit gap = pair_gap(w, free, fixed);
+        if (gap.distance <= 1e-4f) {  // SWEEP_TOLERANCE, scene.wgsl:1
+            if (iteration == 0u && gap.distance <= 0.0f) return none;
+            V3 point = free.kind == DYN_SHAPE_PLANE ? free.center : support(w.shapes, free, gap.normal);
+            return SweepHit{t, gap.normal, point};
+        }
+        float closing = dot(free_travel - other_travel, gap.normal) + closing_floor;
+        if (closing <= 0.0f) return none;
+        t = t + gap.distance / closing;
+        if (t >= 1.0f) return none;
+    }
+    return none;
+}
+
+float combine_material(float a, float b, uint32_t mode) {
+    if (mode == 1u) return fminw(a, b);
+    if (mode == 2u) return fmaxw(a, b);
+    if (mode == 3u) return (a + b) * 0.5f;
+    return std::sqrt(a * b);
+}
+
+// ccd_sweep.wgsl:149-211 over the pairs in sorted order, then ccd_apply.wgsl:7-37 over the dynamic
+// rows. The reference keeps the hit that lowers the time first (an atomicMin and a store,
+// :158-168), so equal times race on the GPU; here the first pair in (lower, higher collider) order
+// keeps it, the rule the library applies.
+void ccd(OracleWorld& w) {
+    const uint32_t n = (uint32_t)w.states.size();
+    std::vector<float> best_time(n, 1.0f);
+    std::vector<V4> best_normal(n), best_point(n);
+    auto retreat = [&](uint32_t row, const SweepPose& moving, const dyn_collider_record& mc, const SweepPose& other,
+                       const dyn_collider_record& oc) {
+        SweepHit hit = rigid_sweep(w, moving, mc, other, oc);
+        if (!(hit.time < 1.0f) || !(hit.time < best_time[row])) return;
+        best_time[row] = hit.time;
+        V3 normal = sign_normalize(hit.normal);
+        float restitution = combine_material(mc.restitution, oc.restitution, w.params.restitution_combine);
+        best_normal[row] = V4{normal.x, normal.y, normal.z, restitution};
+        best_point[row] = V4{hit.point.x, hit.point.y, hit.point.z, hit.time};
+    };
+    for (size_t i = 0; i < w.pair_major.size(); ++i) {
+        uint32_t first_slot = w.pair_major[i], second_slot = w.pair_minor[i];
+        uint32_t fb = w.owners[first_slot], sb = w.owners[second_slot];
+        if (fb == DYN_NO_BODY || sb == DYN_NO_BODY || fb == sb) continue;
+        SweepPose first = sweep_body(w, fb), second = sweep_body(w, sb);
+        if (!body_moves(first.body) && !body_moves(second.body)) continue;
+        const dyn_collider_record& fc = w.colliders[first_slot];
+        const dyn_collider_record& sc = w.colliders[second_slot];
+        if (fc.kind == DYN_SHAPE_NONE || sc.kind == DYN_SHAPE_NONE) continue;
+        uint32_t fg = fc.collision_group != DYN_NO_COLLISION_FILTER ? fc.collision_group : first.body.group;
+        uint32_t fm = fc.collision_mask != DYN_NO_COLLISION_FILTER ? fc.collision_mask : first.body.mask;
+        uint32_t sg = sc.collision_group != DYN_NO_COLLISION_FILTER ? sc.collision_group : second.body.group;
+        uint32_t sm = sc.collision_mask != DYN_NO_COLLISION_FILTER ? sc.collision_mask : second.body.mask;
+        if (!((fg & sm) != 0u && (sg & fm) != 0u)) continue;
+        if (joined_by_joint(w, fb, sb)) continue;
+        retreat(fb, first, fc, second, sc);
+        retreat(sb, second, sc, first, fc);
+    }
+    for (uint32_t row = 0; row < w.params.dynamic_count && row < n; ++row) {
+        float time = best_time[row];
+        if (!(time < 1.0f)) continue;
+        dyn_body_state_record& s = w.states[row];
+        const dyn_body_descriptor_record& d = w.descs[row];
+        Body b = body_at(w, row);
+        V3 axis = xyz(best_normal[row]);
+        float restitution = best_normal[row].w;
+        V3 lever = xyz(best_point[row]) - body_com(b);
+        V3 arm = cross(lever, axis);
+        float linear_speed = dot(b.velocity, axis);
+        float angular_speed = dot(b.angular_velocity, arm);
+        if (linear_speed <= 0.0f && angular_speed <= 0.0f) continue;
+        V3 prev_position = rd3(s.prev_position);
+        V3 position = prev_position + (b.position - prev_position) * time;
+        V4 orientation = quat_slerp(rd4(s.prev_orientation), b.orientation, time);
+        V3 velocity = b.velocity, angular = b.angular_velocity;
+        if (linear_speed > 0.0f) velocity = velocity - axis * (linear_speed * (1.0f + restitution));
+        if (angular_speed > 0.0f) {
+            float mass = d.inverse_mass + dot(arm, apply_inverse_inertia_of(d.inverse_inertia, orientation, arm));
+            if (mass > 0.0f) {
+                float impulse = angular_speed * (1.0f + restitution) / mass;
+                velocity = velocity - axis * (impulse * d.inverse_mass);
+                angular = angular - apply_inverse_inertia_of(d.inverse_inertia, orientation, arm * impulse);
+            }
+        }
+        wr3(s.position, position);
+        wr4(s.orientation, orientation);
+        wr3(s.velocity, velocity);
+        wr3(s.angular_velocity, angular);
+    }
+}
+
+bool world_has_ccd(const OracleWorld& w) {
+    for (const dyn_body_descriptor_record& d : w.descs) {
+        if (d.flags & DYN_BODY_CCD) return true;
+    }
+    return false;
+}
+
 void sleep(OracleWorld& w) {
     for (uint32_t i = 0; i < w.params.dynamic_count; ++i) {
         dyn_body_state_record& s = w.states[i];
@@ -1914,6 +2096,7 @@ void orc_step(OracleWorld* w, float dt) {
     solver_prepare(*w);
     w->solve_contacts = w->contacts;
     solve_substeps(*w);
+    if (world_has_ccd(*w)) ccd(*w);
     sleep(*w);
     w->archive = w->contacts;  // commit: contact_archive.wgsl + archive_count_sync.wgsl
     w->counters[DYN_COUNTER_ARCHIVED] = (uint32_t)w->archive.size();
@@ -1971,6 +2154,15 @@ uint32_t orc_solve_contacts(const OracleWorld* w, dyn_contact_record* out, float
 // Keeps (or stops keeping) the primal snapshots of each step (OracleWorld::snap_pose ...).
 void orc_keep_snapshots(OracleWorld* w, uint32_t keep) { w->keep_snapshots = keep != 0u; }
 void orc_set_solver_guard(OracleWorld* w, uint32_t flags) { w->solver_guard = flags; }
+// World::set_ccd on a row's descriptor (the library's dyn_set_ccd); the caller queues the wake.
+void orc_set_ccd(OracleWorld* w, uint32_t row, uint32_t enabled) {
+    if (row >= w->descs.size()) return;
+    if (enabled) {
+        w->descs[row].flags |= DYN_BODY_CCD;
+    } else {
+        w->descs[row].flags &= ~DYN_BODY_CCD;
+    }
+}
 void orc_step_snapshots(const OracleWorld* w, float* pose, float* vel, float* acc, float* res) {
     if (pose) std::copy(w->snap_pose.begin(), w->snap_pose.end(), pose);
     if (vel) std::copy(w->snap_vel.begin(), w->snap_vel.end(), vel);

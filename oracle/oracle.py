@@ -114,6 +114,14 @@ class OracleWorld:
         L.orc_set_solver_guard.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
         L.orc_set_solver_guard(self._h, int(flags))
 
+    def set_ccd(self, body_id: int, enabled: bool = True) -> None:
+        """World::set_ccd on the body's descriptor (dyn_set_ccd), with the wake it queues."""
+        row = {int(b): r for r, b in enumerate(self.states()["body_id"])}[int(body_id)]
+        L = lib()
+        L.orc_set_ccd.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_set_ccd(self._h, row, 1 if enabled else 0)
+        self.edit_bodies([body_id], R.body_edit(R.EDIT_WAKE))
+
     def edit_bodies(self, body_ids, edits: np.ndarray) -> None:
         """Queues BodyEdit records for the next step (body ids mapped to this world's rows)."""
         ids = np.asarray(body_ids, np.int64)

@@ -180,6 +180,9 @@ inline float oatan2(float y, float x) {
     }
     return w + oatan(y / x);
 }
+// acos(x) = atan2(sqrt((1 - x)(1 + x)), x) on [-1, 1]: the WGSL acos of quat_slerp / quat_angle
+// (core.wgsl:149-168), resting on the same Cephes atan as the rest of the restatement.
+inline float oacos(float x) { return oatan2(std::sqrt((1.0f - x) * (1.0f + x)), x); }
 
 // ---- quaternions: crates/dynamis-shader/shaders/core.wgsl:132-178 ----
 inline V4 quat_mul(V4 a, V4 b) {

@@ -1,0 +1,150 @@
+"""Continuous collision on the GPU (dyn_set_ccd; the ccd.cuh kernels) against the oracle, every step.
+
+Each of the reference's CCD behaviours (crates/dynamis-world/tests/suite/dynamics.rs:241-386, 693-710;
+filter.rs:145-170, restated on the oracle in test_ccd.py) is run through the C ABI and compared
+with the oracle step by step with the full parity check (pairs, contacts, islands, counters, body
+states within 1e-5 relative + 1e-6 absolute), then held to the behaviour itself. A mixed heap of
+fast CCD boxes, spheres, capsules and hulls landing on the ground plane covers every shape pair of
+the sweep; two targets met at the same sweep time cover the equal-time rule; and the flag set and
+cleared on a world already on the device covers the in-place descriptor patch and the graph
+re-recording.
+"""
+import numpy as np
+import pytest
+
+from dynamis_b200 import World, scenes
+from oracle.oracle import oracle_from_world
+from test_ccd import DT, bullet_scene, deepest_rod_tip, make, quat_rotate, state, symmetric_targets
+from test_gpu_parity import compare_step
+
+pytestmark = pytest.mark.gpu
+
+
+def lockstep(world, steps, oracle=None, dt=DT):
+    oracle = oracle or oracle_from_world(world, dt)
+    for step in range(steps):
+        world.step(dt)
+        oracle.step(dt)
+        world.wait()
+        compare_step(world, oracle, step)
+    return oracle
+
+
+def gpu_state(world, body_id):
+    s = world.read_states()
+    return s[s["body_id"] == body_id][0]
+
+
+def test_a_ccd_bullet_stops_at_the_target_and_an_unflagged_one_tunnels():
+    for ccd in (False, True):
+        w, ids = bullet_scene(ccd)
+        lockstep(w, 20)
+        x = gpu_state(w, ids[1])["position"][0]
+        assert (-0.6 < x < -0.45) if ccd else (x > 1.0), (ccd, x)
+        w.close()
+
+
+def test_a_ccd_rod_is_stopped_by_its_leading_face():
+    from test_ccd import R
+    w, ids = make([dict(shape=R.SHAPE_CUBOID, half_extents=(0.05, 5.0, 5.0), mass=0.0),
+                   dict(shape=R.SHAPE_CUBOID, half_extents=(1.0, 0.05, 0.05), position=(-4, 0, 0), velocity=(240, 0, 0),
+                        restitution=0.0, ccd=1)])
+    o = lockstep(w, 1)
+    assert gpu_state(w, ids[1])["position"][0] + 1.0 < 0.05
+    lockstep(w, 20, o)
+    tip = gpu_state(w, ids[1])["position"][0] + 1.0
+    assert -0.2 < tip < 0.05, tip
+    w.close()
+
+
+def test_a_spinning_ccd_rod_stays_out_of_the_wall():
+    from test_ccd import R
+    angle = np.pi / 3.0
+    w, ids = make([dict(shape=R.SHAPE_CUBOID, half_extents=(0.05, 2.0, 2.0), mass=0.0, position=(0.9, 0, 0)),
+                   dict(shape=R.SHAPE_CUBOID, half_extents=(1.0, 0.05, 0.05),
+                        orientation=(0, 0, np.sin(0.5 * angle), np.cos(0.5 * angle)), angular_velocity=(0, 0, -120),
+                        ccd=1)])
+    o = oracle_from_world(w, DT)
+    deepest = -np.inf
+    for step in range(30):
+        w.step(DT)
+        o.step(DT)
+        w.wait()
+        compare_step(w, o, step)
+        s = gpu_state(w, ids[1])
+        for end in ((1.0, 0, 0), (-1.0, 0, 0)):
+            deepest = max(deepest, s["position"][0] + quat_rotate(s["orientation"], end)[0])
+    assert 0.75 < deepest < 0.85, deepest
+    assert deepest == pytest.approx(deepest_rod_tip(True), rel=1e-5, abs=1e-6)
+    w.close()
+
+
+def test_a_ccd_bullet_stops_at_the_nearest_obstacle_of_a_chain():
+    from test_ccd import R
+    specs = [dict(shape=R.SHAPE_SPHERE, radius=0.15, mass=0.0, position=(-2.0 + i * 0.05, 0, 0)) for i in range(81)]
+    specs.append(dict(shape=R.SHAPE_SPHERE, radius=0.3, position=(-12.6, 0, 0), velocity=(90, 0, 0), restitution=0.0,
+                      ccd=1))
+    w, ids = make(specs)
+    o = oracle_from_world(w, DT)
+    for step in range(20):
+        w.step(DT)
+        o.step(DT)
+        w.wait()
+        compare_step(w, o, step)
+        assert gpu_state(w, ids[-1])["position"][0] < -2.4
+    w.close()
+
+
+def test_a_ccd_bullet_stops_at_the_anchor_it_may_touch():
+    from test_ccd import R
+    w, ids = make([dict(shape=R.SHAPE_SPHERE, radius=0.5, mass=0.0),
+                   dict(shape=R.SHAPE_SPHERE, radius=0.5, position=(0, 8, 0), velocity=(0, -200, 0), ccd=1)])
+    lockstep(w, 4)
+    assert 0.6 < gpu_state(w, ids[1])["position"][1] < 1.4
+    w.close()
+
+
+def test_equal_sweep_times_keep_the_first_pair_in_collider_order():
+    w, ids = symmetric_targets()
+    lockstep(w, 3)
+    assert gpu_state(w, ids[2])["position"][0] < 0.0
+    w.close()
+
+
+def test_the_flag_set_and_cleared_on_the_device_world():
+    # the world is on the device and stepping when the flag changes: the body row is patched in
+    # place (archived contacts and states kept), the step graph gains or loses the CCD kernels,
+    # and the wake edit queued with each change reaches both sides
+    from test_ccd import R
+    w, ids = bullet_scene(False)
+    o = lockstep(w, 2)
+    w.set_ccd(int(ids[1]), True)
+    o.set_ccd(int(ids[1]), True)
+    lockstep(w, 18, o)
+    x = gpu_state(w, ids[1])["position"][0]
+    assert -0.6 < x < -0.45, x
+    w.set_ccd(int(ids[1]), False)
+    o.set_ccd(int(ids[1]), False)
+    w.edit_bodies([int(ids[1])], R.body_edit(R.EDIT_PATCH, R.PATCH_POSITION | R.PATCH_VELOCITY, position=(-12.6, 0, 0),
+                                              velocity=(90, 0, 0)))
+    o.edit_bodies([int(ids[1])], R.body_edit(R.EDIT_PATCH, R.PATCH_POSITION | R.PATCH_VELOCITY, position=(-12.6, 0, 0),
+                                              velocity=(90, 0, 0)))
+    lockstep(w, 20, o)
+    assert gpu_state(w, ids[1])["position"][0] > 1.0  # tunnels again
+    w.close()
+
+
+def test_a_fast_heap_of_every_shape_lands_like_the_oracle():
+    scene = scenes.random_mix(48, seed=21)
+    dynamic = scene.bodies["mass"] > 0
+    rng = np.random.default_rng(2)
+    flagged = dynamic & (rng.random(len(scene.bodies)) < 0.6)
+    scene.bodies["ccd"][flagged] = 1
+    scene.bodies["velocity"][flagged] = (rng.normal(0, 4, size=(int(flagged.sum()), 3)) + (0, -70, 0)).astype(np.float32)
+    scene.bodies["angular_velocity"][flagged] = rng.normal(0, 20, size=(int(flagged.sum()), 3)).astype(np.float32)
+    w = World()
+    scene.build(w)
+    o = lockstep(w, 12)
+    s = o.states()
+    assert np.all(s["position"][:, 1] > -1.0), "a CCD body passed through the ground plane"
+    w.close()
