@@ -50,6 +50,7 @@ SIGNATURES = {
     "dyn_debug_pairs": (I32, [P, P, P, U32, PU32]),
     "dyn_debug_contacts": (I32, [P, P, U32, PU32]),
     "dyn_debug_islands": (I32, [P, P, U32, PU32]),
+    "dyn_debug_resting": (I32, [P, P, U32, PU32]),
     "dyn_set_timing": (I32, [P, I32]),
     "dyn_set_solver_guard": (I32, [P, U32]),
     "dyn_set_ccd": (I32, [P, U32, I32]),

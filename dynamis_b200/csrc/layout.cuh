@@ -69,6 +69,8 @@ enum Ctl : uint32_t {
     CTL_EPA_NEXT = 19,       // next penetrating pair ticket of the EPA kernel
     CTL_STAGED = 20,         // contacts the narrowphase staged (every contact it found: at most one per pair)
     CTL_CCD_HITS = 21,       // sweep hits the continuous-collision pass recorded
+    CTL_RESTING = 22,        // frozen contacts in the store the next step reads (kept across steps)
+    CTL_REST_NEXT = 23,      // frozen contacts this step's commit wrote
     CTL_COUNT = 32
 };
 
@@ -119,6 +121,16 @@ struct DeviceWorld {
     uint32_t* ccd_time;
     unsigned long long* ccd_key;
     float4* ccd_impact;  // [2n]
+    // frozen contacts (freeze_contacts.wgsl, thaw_contacts.wgsl, island_link_resting.wgsl): the
+    // contacts of body pairs that were both at rest when a step ended, kept across steps by body id
+    // and generation. Two stores swap roles every step: a step reads rest_in (and its islands join
+    // through it), and its commit writes the contacts that stay frozen, then the newly frozen ones,
+    // into rest_out.
+    uint4* rest_in;         // first_body_id, first_generation, second_body_id, second_generation
+    uint2* rest_in_slots;   // collider a, collider b
+    uint4* rest_out;
+    uint2* rest_out_slots;
+    uint32_t rest_cap;
     // colliders
     uint32_t* c_owner;
     uint4* c_kind;     // kind, flags, source, 0

@@ -48,11 +48,11 @@ __device__ __forceinline__ void or_counter(uint32_t* counter, uint32_t value) {
 // Counters that persist across steps (crates/dynamis-abi/src/counter.rs: Maintained).
 __global__ void k_reset(DeviceWorld w) {
     for (uint32_t i = threadIdx.x; i < DYN_COUNTER_DEVICE_COUNT; i += blockDim.x) {
-        if (i == DYN_COUNTER_ARCHIVED || i == DYN_COUNTER_STEP) continue;
+        if (i == DYN_COUNTER_ARCHIVED || i == DYN_COUNTER_STEP || i == DYN_COUNTER_RESTING) continue;
         w.counters[i] = 0u;
     }
     for (uint32_t i = threadIdx.x; i < CTL_COUNT; i += blockDim.x) {
-        if (i == CTL_ARCHIVED || i == CTL_STATUS) continue;
+        if (i == CTL_ARCHIVED || i == CTL_STATUS || i == CTL_RESTING) continue;
         w.ctl[i] = 0u;
     }
 }
@@ -1210,7 +1210,8 @@ __global__ void k_relay(DeviceWorld w) {
     }
 }
 
-// contact_begin.wgsl:41-71 (no resting archive): unmatched touching contacts are announced.
+// contact_begin.wgsl:41-71 (the resting index, which only decides event announcements, is not
+// consulted): unmatched touching contacts are announced.
 __global__ void k_contact_begin(DeviceWorld w, dyn_step_params p) {
     const uint32_t count = w.ctl[CTL_CONTACTS];
     GRID_STRIDE(i, count) {

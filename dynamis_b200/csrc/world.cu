@@ -14,6 +14,7 @@
 #include "adjoint.cuh"
 #include "ccd.cuh"
 #include "joints.cuh"
+#include "rest.cuh"
 #include "step.cuh"
 #include "world.h"
 
@@ -115,6 +116,10 @@ struct DeviceState {
     uint32_t sort_fault_skip = 0;
     uint32_t sort_fault_limit = kLookbackSpinLimit;
     dyn_body_state_record* staging = nullptr;  // n_cap ABI state records
+    // the two frozen-contact stores (rest.cuh); a step reads rest_*[parity] and writes the other
+    uint4* rest_ids[2] = {nullptr, nullptr};
+    uint2* rest_slots[2] = {nullptr, nullptr};
+    uint32_t rest_cap = 0;
     std::vector<void*> joint_allocs;  // constraint buffers, rebuilt whenever the constraint set changes
     // body edits: once a world has taken edits its step graph runs k_clear_inputs, k_body_edits and
     // k_begin<false>; before that, k_begin<true> alone
@@ -334,6 +339,12 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.cnt3, 3 * (size_t)N);
         A(dw.resolution_alt, N);
         A(dw.cowner, C);
+        // the frozen-contact stores: as many as the contact stream held when the world was made
+        d->rest_cap = C;
+        for (int r = 0; r < 2; ++r) {
+            A(d->rest_ids[r], C);
+            A(d->rest_slots[r], C);
+        }
         A(dw.counters, 64);
         A(dw.ctl, CTL_COUNT);
         A(d->staging, N);
@@ -532,9 +543,17 @@ dyn_status upload_scene(dyn_world* w) {
         DYN_CUDA(cudaMemcpyAsync(d->sources, srcs.data(), srcs.size() * sizeof(dyn_shape_source_record), cudaMemcpyHostToDevice, s));
         DYN_CUDA(cudaMemcpyAsync(d->vertices, verts.data(), verts.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     }
-    // a fresh scene has no archived contacts and no device status
-    DYN_CUDA(cudaMemsetAsync(dw.ctl, 0, CTL_COUNT * 4, s));
-    DYN_CUDA(cudaMemsetAsync(dw.counters, 0, 64 * 4, s));
+    // a fresh scene has no archived contacts and no device status; the frozen contacts, kept by
+    // body id and generation, carry over (a spawn or a removal does not thaw them), so the store the
+    // next step reads moves to the one parity 0 reads
+    if (d->parity != 0u && d->rest_cap) {
+        DYN_CUDA(cudaMemcpyAsync(d->rest_ids[0], d->rest_ids[1], (size_t)d->rest_cap * sizeof(uint4), cudaMemcpyDeviceToDevice, s));
+        DYN_CUDA(cudaMemcpyAsync(d->rest_slots[0], d->rest_slots[1], (size_t)d->rest_cap * sizeof(uint2), cudaMemcpyDeviceToDevice, s));
+    }
+    DYN_CUDA(cudaMemsetAsync(dw.ctl, 0, CTL_RESTING * 4, s));
+    DYN_CUDA(cudaMemsetAsync(dw.ctl + CTL_RESTING + 1, 0, (CTL_COUNT - CTL_RESTING - 1) * 4, s));
+    DYN_CUDA(cudaMemsetAsync(dw.counters, 0, DYN_COUNTER_RESTING * 4, s));
+    DYN_CUDA(cudaMemsetAsync(dw.counters + DYN_COUNTER_RESTING + 1, 0, (64 - DYN_COUNTER_RESTING - 1) * 4, s));
     DYN_CUDA(cudaStreamSynchronize(s));
     if ((st = upload_joints(w))) return st;
     w->scene_dirty = false;
@@ -674,6 +693,12 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     const uint32_t N = std::max(dw.n, 1u), K = std::max(dw.k, 1u), ND = std::max(dw.nd, 1u);
     const uint32_t E = dw.e_cap, P = dw.p_cap, C = dw.c_cap;
     const uint32_t joint_blocks = dw.jgroup_count;  // one warp group per 32-thread block
+    // the frozen-contact store this step reads is the one the previous step's commit wrote
+    dw.rest_cap = d->rest_cap;
+    dw.rest_in = d->rest_ids[parity];
+    dw.rest_in_slots = d->rest_slots[parity];
+    dw.rest_out = d->rest_ids[1u - parity];
+    dw.rest_out_slots = d->rest_slots[1u - parity];
     mark(ST_BEGIN);
     k_reset<<<1, 64, 0, s>>>(dw);
     if (dw.jcount) k_joint_count<<<blocks_for(d, std::max(dw.jfilter_count, 1u), 256), 256, 0, s>>>(dw);
@@ -755,6 +780,7 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     k_island_flatten<false><<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     k_island_link<false><<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
     if (dw.jcount) k_island_link_joints<<<blocks_for(d, dw.jcount, 256), 256, 0, s>>>(dw);
+    k_island_link_resting<<<blocks_for(d, dw.rest_cap, 256), 256, 0, s>>>(dw);
     k_island_flatten<true><<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
     k_wake_live<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
@@ -811,6 +837,11 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     }
     mark(ST_SLEEP);
     k_sleep<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw, p);
+    // commit (crates/dynamis-rigid/src/commit.rs:187-208): thaw, static wake flags, freeze
+    k_rest_thaw<<<blocks_for(d, dw.rest_cap, 256), 256, 0, s>>>(dw);
+    k_static_wake_clear<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
+    k_rest_freeze<<<blocks_for(d, C, 256), 256, 0, s>>>(dw);
+    k_rest_commit<<<1, 32, 0, s>>>(dw);
     if (tape) {
         k_tape_hot<<<blocks_for(d, N, 256), 256, 0, s>>>(dw, *tape, p.substeps);
         k_tape_advance<<<1, 32, 0, s>>>(*tape);
@@ -1421,7 +1452,9 @@ static std::vector<CheckpointPart> checkpoint_parts(DeviceState* d) {
             {arc.normal, C * sizeof(float4)},     {arc.rows, C * sizeof(uint4)},     {arc.mat, C * sizeof(float4)},
             {arc.ids, C * sizeof(uint4)},         {arc.ids2, C * sizeof(uint4)},     {arc.extra, C * sizeof(float4)},
             {arc.la, 4 * C * sizeof(float4)},     {arc.lb, 4 * C * sizeof(float4)},  {arc.acc, 4 * C * sizeof(float4)},
-            {arc.pos, 4 * C * sizeof(float4)}};
+            {arc.pos, 4 * C * sizeof(float4)},
+            {d->rest_ids[d->parity], (size_t)d->rest_cap * sizeof(uint4)},
+            {d->rest_slots[d->parity], (size_t)d->rest_cap * sizeof(uint2)}};
 }
 static size_t checkpoint_bytes(const std::vector<CheckpointPart>& parts) {
     size_t bytes = 0;
@@ -2236,6 +2269,29 @@ DYN_API dyn_status dyn_debug_islands(dyn_world* w, uint32_t* out, uint32_t cap, 
     if (!out) return DYN_OK;
     DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
     DYN_CUDA(cudaMemcpy(out, dw.parents, std::min(cap, dw.nd) * 4, cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+// The frozen contacts the next step reads (rest.cuh), six words each: first body id, its
+// generation, second body id, its generation, collider a, collider b; in store order.
+DYN_API dyn_status dyn_debug_resting(dyn_world* w, uint32_t* out, uint32_t cap, uint32_t* count) {
+    if (!w || !w->dev) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    uint32_t live = 0;
+    DYN_CUDA(cudaMemcpy(&live, d->dw.ctl + CTL_RESTING, 4, cudaMemcpyDeviceToHost));
+    live = std::min(live, d->rest_cap);
+    if (count) *count = live;
+    if (!out || live == 0) return DYN_OK;
+    const uint32_t m = std::min(live, cap);
+    std::vector<uint4> ids(m);
+    std::vector<uint2> slots(m);
+    DYN_CUDA(cudaMemcpy(ids.data(), d->rest_ids[d->parity], m * sizeof(uint4), cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(slots.data(), d->rest_slots[d->parity], m * sizeof(uint2), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < m; ++i) {
+        const uint32_t row[6] = {ids[i].x, ids[i].y, ids[i].z, ids[i].w, slots[i].x, slots[i].y};
+        std::memcpy(out + 6 * (size_t)i, row, sizeof(row));
+    }
     return DYN_OK;
 }
 

@@ -366,6 +366,16 @@ class World:
         self._check(lib.dyn_debug_islands(self._h, ptr(out), n.value, None))
         return out
 
+    def debug_resting(self) -> np.ndarray:
+        """The frozen contacts the next step reads, one row each: first body id, its generation,
+        second body id, its generation, collider a, collider b (store order)."""
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_debug_resting(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 6), np.uint32)
+        if n.value:
+            self._check(lib.dyn_debug_resting(self._h, ptr(out), n.value, None))
+        return out
+
     # ---- differentiation (World::step_backward) ----
     def set_mass_properties(self, inverse_mass, inverse_inertia) -> None:
         """Every body row's inverse mass and inverse inertia tensor (rows x 6: xx, xy, xz, yy, yz, zz)."""

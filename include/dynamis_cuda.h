@@ -197,6 +197,11 @@ DYN_API dyn_status dyn_debug_entries(dyn_world* world, uint32_t* keys, uint32_t*
 DYN_API dyn_status dyn_debug_pairs(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t cap, uint32_t* count);
 DYN_API dyn_status dyn_debug_contacts(dyn_world* world, dyn_contact_record* out, uint32_t cap, uint32_t* count);
 DYN_API dyn_status dyn_debug_islands(dyn_world* world, uint32_t* out, uint32_t cap, uint32_t* count);
+/* The frozen contacts the next step reads (freeze_contacts.wgsl / thaw_contacts.wgsl: contacts of
+ * body pairs that were both at rest when a step ended), six words each: first body id, its
+ * generation, second body id, its generation, collider a, collider b. Order is not meaningful.
+ * The reference reads them through World::inspect_contacts with its live contacts. */
+DYN_API dyn_status dyn_debug_resting(dyn_world* world, uint32_t* out, uint32_t cap, uint32_t* count);
 
 /* Per-stage timing (World::gpu_pass_timings, step.rs:187-190). With timing on, dyn_step runs the
  * stages eagerly with CUDA events between them instead of the graph; dyn_stage_timings returns

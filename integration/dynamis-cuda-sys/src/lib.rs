@@ -200,6 +200,7 @@ extern "C" {
     pub fn dyn_debug_pairs(world: *mut DynWorld, major: *mut u32, minor: *mut u32, cap: u32, count: *mut u32) -> DynStatus;
     pub fn dyn_debug_contacts(world: *mut DynWorld, out: *mut ContactRecord, cap: u32, count: *mut u32) -> DynStatus;
     pub fn dyn_debug_islands(world: *mut DynWorld, out: *mut u32, cap: u32, count: *mut u32) -> DynStatus;
+    pub fn dyn_debug_resting(world: *mut DynWorld, out: *mut u32, cap: u32, count: *mut u32) -> DynStatus;
     pub fn dyn_set_timing(world: *mut DynWorld, enabled: i32) -> DynStatus;
     pub fn dyn_step_kernel_count(world: *const DynWorld) -> u32;
     pub fn dyn_stage_count() -> u32;

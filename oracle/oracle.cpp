@@ -244,6 +244,12 @@ struct OracleWorld {
     std::vector<dyn_constraint_runtime_record> joint_runtime;
     std::vector<uint32_t> plan_rows, plan_layers, plan_components;
     std::vector<uint32_t> body_world;  // sub-world of every row (empty: one world)
+    // frozen contacts (freeze_contacts.wgsl): pairs of bodies both at rest when a step ended, by
+    // body id and generation with their colliders, kept across steps in the order they were frozen
+    struct Frozen {
+        uint32_t first_id, first_generation, second_id, second_generation, a, b;
+    };
+    std::vector<Frozen> resting;
     // body commands queued for the next step: (row, edit), in command order
     std::vector<std::pair<uint32_t, dyn_body_edit_record>> edits;
     uint32_t world_of(uint32_t row) const { return body_world.empty() ? 0u : body_world[row]; }
@@ -917,6 +923,13 @@ void build_islands(OracleWorld& w) {
     for (size_t j = 0; j < w.joint_descs.size(); ++j) {
         if (w.joint_runtime[j].broken != 0u) continue;
         island_couple(w, w.joint_rows[j].first_row, w.joint_rows[j].second_row);
+    }
+    // island_link_resting.wgsl:10-21: the frozen contacts keep their sleeping bodies in one island
+    for (const OracleWorld::Frozen& f : w.resting) {
+        uint32_t first = resolve_row(w, f.first_id, f.first_generation);
+        uint32_t second = resolve_row(w, f.second_id, f.second_generation);
+        if (first == DYN_NO_BODY || second == DYN_NO_BODY) continue;
+        island_couple(w, first, second);
     }
     uint32_t rounds = 32 - (uint32_t)__builtin_clz(std::max(dc, 2u));  // ilog2(max(N,2)) + 1
     for (uint32_t r = 0; r < rounds; ++r) {
@@ -1966,6 +1979,39 @@ void ccd(OracleWorld& w) {
     }
 }
 
+// The commit's frozen-contact passes (crates/dynamis-rigid/src/commit.rs:187-208): thaw_contacts.wgsl
+// (a frozen contact stays while both bodies were inactive when the step began; one whose body is gone
+// is released and its other body disturbed), static_wake_clear.wgsl, freeze_contacts.wgsl (every
+// contact whose bodies are both inactive after the step). COUNTER_RESTING is the reference's slot
+// count, the most contacts held frozen at once.
+void commit_resting(OracleWorld& w) {
+    const uint32_t n = (uint32_t)w.states.size();
+    std::vector<OracleWorld::Frozen> kept;
+    for (const OracleWorld::Frozen& f : w.resting) {
+        uint32_t first = resolve_row(w, f.first_id, f.first_generation);
+        uint32_t second = resolve_row(w, f.second_id, f.second_generation);
+        if (first == DYN_NO_BODY || second == DYN_NO_BODY) {
+            if (first != DYN_NO_BODY) w.wake_flags[first] = 1u;
+            if (second != DYN_NO_BODY) w.wake_flags[second] = 1u;
+            continue;
+        }
+        if (w.body_activity[first] != 0u || w.body_activity[second] != 0u) continue;
+        kept.push_back(f);
+    }
+    for (uint32_t i = w.params.dynamic_count; i < n; ++i) w.wake_flags[i] = 0u;
+    for (const dyn_contact_record& c : w.contacts) {
+        uint32_t first = w.owners[c.a], second = w.owners[c.b];
+        if (body_is_active(w.states[first], w.descs[first]) || body_is_active(w.states[second], w.descs[second])) continue;
+        if (kept.size() >= w.contact_capacity) {
+            w.counters[DYN_COUNTER_REFUSED_RESTING] += 1;
+            continue;
+        }
+        kept.push_back(OracleWorld::Frozen{c.first_body_id, c.first_generation, c.second_body_id, c.second_generation, c.a, c.b});
+    }
+    w.resting.swap(kept);
+    w.counters[DYN_COUNTER_RESTING] = std::max(w.counters[DYN_COUNTER_RESTING], (uint32_t)w.resting.size());
+}
+
 bool world_has_ccd(const OracleWorld& w) {
     for (const dyn_body_descriptor_record& d : w.descs) {
         if (d.flags & DYN_BODY_CCD) return true;
@@ -2098,6 +2144,7 @@ void orc_step(OracleWorld* w, float dt) {
     solve_substeps(*w);
     if (world_has_ccd(*w)) ccd(*w);
     sleep(*w);
+    commit_resting(*w);
     w->archive = w->contacts;  // commit: contact_archive.wgsl + archive_count_sync.wgsl
     w->counters[DYN_COUNTER_ARCHIVED] = (uint32_t)w->archive.size();
     w->counters[DYN_COUNTER_STEP] += 1;
@@ -2176,6 +2223,19 @@ void orc_step_decisions(const OracleWorld* w, uint8_t* solve, uint8_t* position,
     if (integrate) std::copy(w->integrate_flags.begin(), w->integrate_flags.end(), integrate);
     if (targets) std::copy(w->target_flags.begin(), w->target_flags.end(), targets);
 }
+// The frozen contacts, six words each (first id, its generation, second id, its generation,
+// collider a, collider b), in the order they were frozen.
+uint32_t orc_resting(const OracleWorld* w, uint32_t* out) {
+    if (out) {
+        for (size_t i = 0; i < w->resting.size(); ++i) {
+            const OracleWorld::Frozen& f = w->resting[i];
+            const uint32_t row[6] = {f.first_id, f.first_generation, f.second_id, f.second_generation, f.a, f.b};
+            std::memcpy(out + 6 * i, row, sizeof(row));
+        }
+    }
+    return (uint32_t)w->resting.size();
+}
+
 uint32_t orc_islands(const OracleWorld* w, uint32_t* out) {
     if (out) std::memcpy(out, w->island_parents.data(), w->island_parents.size() * 4);
     return (uint32_t)w->island_parents.size();

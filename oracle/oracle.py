@@ -181,6 +181,17 @@ class OracleWorld:
         lib().orc_joint_plan(self._h, _p(rows), _p(layers), _p(comps), None)
         return {"rows": rows, "layers": layers, "components": comps}
 
+    def resting(self) -> np.ndarray:
+        """The frozen contacts: first id, its generation, second id, its generation, collider a, collider b."""
+        L = lib()
+        L.orc_resting.restype = ctypes.c_uint32
+        L.orc_resting.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        n = L.orc_resting(self._h, None)
+        out = np.zeros((n, 6), np.uint32)
+        if n:
+            L.orc_resting(self._h, _p(out))
+        return out
+
     def islands(self) -> np.ndarray:
         n = lib().orc_islands(self._h, None)
         out = np.zeros(n, np.uint32)
