@@ -143,6 +143,8 @@ struct DeviceWorld {
     float4* c_scale;   // scale.xyz, 0
     const dyn_shape_source_record* sources;
     const float4* vertices;
+    const uint4* hull_tris;        // every hull's outward triangles (vertex indices within its hull), hull by hull
+    const uint2* hull_tri_range;   // [source]: first triangle, triangle count
     // broadphase
     float4* aabb;  // [2k]: min.xyz, max.xyz
     uint4* c_class;  // [k] per step: owner row, collision group, collision mask, kind | moves << 8 | unscaled << 9

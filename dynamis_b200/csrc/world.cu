@@ -14,6 +14,7 @@
 #include "adjoint.cuh"
 #include "ccd.cuh"
 #include "joints.cuh"
+#include "query.cuh"
 #include "rest.cuh"
 #include "step.cuh"
 #include "world.h"
@@ -98,9 +99,15 @@ struct DeviceState {
     uint32_t* spill_host = nullptr;  // host-mapped mailbox of stream demand (DeviceWorld::spill)
     uint32_t n_cap = 0, k_cap = 0, e_cap = 0, p_cap = 0, c_cap = 0;
     uint32_t id_cap = 0;  // body ids the row_of_id table holds (ids of removed bodies are not reused)
-    uint32_t src_cap = 0, vert_cap = 0;
+    uint32_t src_cap = 0, vert_cap = 0, tri_cap = 0;
     dyn_shape_source_record* sources = nullptr;
     float4* vertices = nullptr;
+    uint4* hull_tris = nullptr;       // the hulls' triangles (scene queries)
+    uint2* hull_tri_range = nullptr;  // [source]: first triangle, count
+    // a query batch's records and hits on the device (dyn_query), grown as batches need
+    dyn_query_record* query_buf = nullptr;
+    dyn_query_hit_record* hit_buf = nullptr;
+    uint32_t query_cap = 0, hit_cap = 0;
     // sort and scan scratch
     uint32_t* hist = nullptr;          // 8 x 256
     uint32_t* tile_counters = nullptr; // 16
@@ -218,9 +225,12 @@ dyn_status ensure_device(dyn_world* w) {
     std::vector<float> verts;
     std::vector<dyn_shape_source_record> srcs = shape_sources(w, &verts);
     uint32_t ns = (uint32_t)srcs.size(), nv = (uint32_t)(verts.size() / 4);
+    uint32_t nt = 0;
+    for (const HullSource& h : w->hulls) nt += (uint32_t)(h.triangles.size() / 3);
     const uint32_t ids = (uint32_t)w->row_of_id.size();
     DeviceState* d = w->dev;
-    bool fits = d && n <= d->n_cap && k <= d->k_cap && ns <= d->src_cap && nv <= d->vert_cap && ids <= d->id_cap;
+    bool fits = d && n <= d->n_cap && k <= d->k_cap && ns <= d->src_cap && nv <= d->vert_cap && nt <= d->tri_cap &&
+                ids <= d->id_cap;
     if (!fits) {
         if (d) destroy_device(w);
         int count = 0;
@@ -254,6 +264,7 @@ dyn_status ensure_device(dyn_world* w) {
         d->c_cap = w->capacity.contacts ? w->capacity.contacts : 16u * std::max(d->k_cap, 64u);
         d->src_cap = std::max(ns, 1u);
         d->vert_cap = std::max(nv, 1u);
+        d->tri_cap = std::max(nt, 1u);
         DeviceWorld& dw = d->dw;
         dyn_status st;
 #define A(ptr, count) if ((st = alloc(w, d, &(ptr), (count)))) return st
@@ -290,6 +301,8 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.c_scale, K);
         A(d->sources, d->src_cap);
         A(d->vertices, d->vert_cap);
+        A(d->hull_tris, d->tri_cap);
+        A(d->hull_tri_range, d->src_cap);
         A(dw.aabb, 2 * (size_t)K);
         A(dw.c_class, K);
         A(dw.c_level, K);
@@ -364,6 +377,8 @@ dyn_status ensure_device(dyn_world* w) {
         dw.c_cap = C;
         dw.sources = d->sources;
         dw.vertices = d->vertices;
+        dw.hull_tris = d->hull_tris;
+        dw.hull_tri_range = d->hull_tri_range;
     }
     return DYN_OK;
 }
@@ -539,9 +554,20 @@ dyn_status upload_scene(dyn_world* w) {
     DYN_CUDA(cudaMemcpyAsync(dw.c_mat2, cmat2.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
     DYN_CUDA(cudaMemcpyAsync(dw.c_filter, cfilter.data(), k * sizeof(uint2), cudaMemcpyHostToDevice, s));
     DYN_CUDA(cudaMemcpyAsync(dw.c_scale, cscale.data(), k * sizeof(float4), cudaMemcpyHostToDevice, s));
+    std::vector<uint4> tris;
+    std::vector<uint2> tri_range(srcs.size());
+    for (size_t h = 0; h < w->hulls.size(); ++h) {
+        const std::vector<uint32_t>& t = w->hulls[h].triangles;
+        tri_range[h] = make_uint2((uint32_t)tris.size(), (uint32_t)(t.size() / 3));
+        for (size_t i = 0; i + 2 < t.size(); i += 3) tris.push_back(make_uint4(t[i], t[i + 1], t[i + 2], 0u));
+    }
     if (!srcs.empty()) {
         DYN_CUDA(cudaMemcpyAsync(d->sources, srcs.data(), srcs.size() * sizeof(dyn_shape_source_record), cudaMemcpyHostToDevice, s));
         DYN_CUDA(cudaMemcpyAsync(d->vertices, verts.data(), verts.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+        DYN_CUDA(cudaMemcpyAsync(d->hull_tri_range, tri_range.data(), tri_range.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+    }
+    if (!tris.empty()) {
+        DYN_CUDA(cudaMemcpyAsync(d->hull_tris, tris.data(), tris.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
     }
     // a fresh scene has no archived contacts and no device status; the frozen contacts, kept by
     // body id and generation, carry over (a spawn or a removal does not thaw them), so the store the
@@ -1083,6 +1109,8 @@ void destroy_device(dyn_world* w) {
     for (void* p : d->joint_allocs) cudaFree(p);
     if (d->edit_buffer) cudaFree(d->edit_buffer);
     if (d->edit_run_buffer) cudaFree(d->edit_run_buffer);
+    if (d->query_buf) cudaFree(d->query_buf);
+    if (d->hit_buf) cudaFree(d->hit_buf);
     for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
         if (p) cudaFree(p);
     }
@@ -2269,6 +2297,116 @@ DYN_API dyn_status dyn_debug_islands(dyn_world* w, uint32_t* out, uint32_t cap, 
     if (!out) return DYN_OK;
     DYN_CUDA(cudaStreamSynchronize(w->dev->stream));
     DYN_CUDA(cudaMemcpy(out, dw.parents, std::min(cap, dw.nd) * 4, cudaMemcpyDeviceToHost));
+    return DYN_OK;
+}
+
+// The grid counters a query's index rebuilds (the step's other counters stay as the step left them).
+static __global__ void k_query_index_reset(DeviceWorld w) {
+    if (threadIdx.x != 0) return;
+    const uint32_t counters[] = {DYN_COUNTER_GRID_LEVELS, DYN_COUNTER_IMMOVABLE_LEVELS, DYN_COUNTER_GRID_SCALE,
+                                 DYN_COUNTER_GRID_EXTENT, DYN_COUNTER_ENTRIES, DYN_COUNTER_IMMOVABLE_ENTRIES,
+                                 DYN_COUNTER_IMMOVABLE_EMITTED, DYN_COUNTER_COARSE_ACTIVE, DYN_COUNTER_ENTRY_FAULTS};
+    for (uint32_t c : counters) w.counters[c] = 0u;
+    w.ctl[CTL_ENTRIES] = 0u;
+    w.ctl[CTL_CELL_OVERFLOW] = 0u;
+}
+
+// Validates one query as the reference's constructors assert (crates/dynamis-abi/src/query.rs:103-181,
+// crates/dynamis-world/src/query.rs:82-125): finite vectors, a non-zero direction, positive lengths,
+// a convex probe shape.
+static bool query_valid(const dyn_world* w, const dyn_query_record& q) {
+    auto finite3 = [](const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); };
+    if (q.kind > DYN_QUERY_CONVEX || q.max_hits == 0u || !finite3(q.origin)) return false;
+    const bool directed = q.kind == DYN_QUERY_RAY || q.kind == DYN_QUERY_SWEEP;
+    if (directed && (!finite3(q.direction) || (q.direction[0] == 0.0f && q.direction[1] == 0.0f && q.direction[2] == 0.0f)))
+        return false;
+    if (directed && !(q.extent > 0.0f && std::isfinite(q.extent))) return false;
+    if (q.kind == DYN_QUERY_SPHERE && !(q.radius > 0.0f && q.extent > 0.0f)) return false;
+    if (q.kind == DYN_QUERY_CUBOID && !(q.half_extents[0] > 0.0f && q.half_extents[1] > 0.0f && q.half_extents[2] > 0.0f))
+        return false;
+    if (q.kind == DYN_QUERY_CONVEX || q.kind == DYN_QUERY_SWEEP || q.kind == DYN_QUERY_CUBOID) {
+        const uint32_t k = q.shape_kind;
+        if (!(k == DYN_SHAPE_SPHERE || k == DYN_SHAPE_CUBOID || k == DYN_SHAPE_CAPSULE || k == DYN_SHAPE_CYLINDER ||
+              k == DYN_SHAPE_HULL))
+            return false;
+        if (k == DYN_SHAPE_HULL && q.source >= w->hulls.size()) return false;
+        const float* o = q.orientation;
+        const float norm = o[0] * o[0] + o[1] * o[1] + o[2] * o[2] + o[3] * o[3];
+        if (!(std::fabs(norm - 1.0f) <= 1e-3f)) return false;
+    }
+    return true;
+}
+
+// World::ray_query ... sweep_query, resolve_queries and query_hits (crates/dynamis-world/src/query.rs:50-175,
+// the Query pass of crates/dynamis-scene/src/passes.rs:15-39) as one call.
+DYN_API dyn_status dyn_query(dyn_world* w, dyn_query_record* queries, uint32_t n, dyn_query_hit_record* hits, uint32_t hit_capacity) {
+    if (!w || (n && (!queries || !hits))) return fail(w, DYN_ERR_INVALID, "dyn_query: null argument");
+    if (n == 0) return DYN_OK;
+    rebuild_rows(w);
+    for (uint32_t b : w->body_world) {
+        if (b != 0u) return fail(w, DYN_ERR_INVALID, "dyn_query: a world of batched sub-worlds takes no scene queries");
+    }
+    uint64_t base = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!query_valid(w, queries[i])) return fail(w, DYN_ERR_INVALID, "dyn_query: a query record is invalid");
+        queries[i].hit_base = (uint32_t)base;
+        queries[i].count = 0u;
+        queries[i].overflow = 0u;
+        base += std::min(queries[i].max_hits, DYN_QUERY_CANDIDATES);
+    }
+    if (base > hit_capacity) return fail(w, DYN_ERR_CAPACITY, "dyn_query: the hit array is smaller than the batch's hit bound");
+    if (w->states.empty()) return fail(w, DYN_ERR_INVALID, "dyn_query: the world holds no bodies");
+    if (!w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows) || w->scene_dirty) {
+        if (dyn_status st = upload_scene(w)) return st;
+    }
+    DeviceState* d = w->dev;
+    DYN_CUDA(cudaSetDevice(w->device));
+    if (n > d->query_cap) {
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        if (d->query_buf) cudaFree(d->query_buf);
+        d->query_buf = nullptr;
+        DYN_CUDA(cudaMalloc(&d->query_buf, (size_t)n * sizeof(dyn_query_record)));
+        d->query_cap = n;
+    }
+    if (base > d->hit_cap) {
+        DYN_CUDA(cudaStreamSynchronize(d->stream));
+        if (d->hit_buf) cudaFree(d->hit_buf);
+        d->hit_buf = nullptr;
+        DYN_CUDA(cudaMalloc(&d->hit_buf, (size_t)std::max<uint64_t>(base, 1) * sizeof(dyn_query_hit_record)));
+        d->hit_cap = (uint32_t)std::max<uint64_t>(base, 1);
+    }
+    // the grid of the current states, as a query run builds it (AABBs, entries, their sort, the cell table)
+    dyn_step_params p;
+    dyn_step_params_for(w, d->graph_dt > 0.0f ? d->graph_dt : 1.0f / 60.0f, &p);
+    DeviceWorld dw = d->dw;
+    const uint32_t K = std::max(dw.k, 1u), E = dw.e_cap;
+    cudaStream_t s = d->stream;
+    k_query_index_reset<<<1, 32, 0, s>>>(dw);
+    k_aabb<<<blocks_for(d, K, 128), 128, 0, s>>>(dw, p);
+    k_entry_count<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, K, dw.ctl + CTL_ENTRIES);
+    k_entry_emit<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
+    k_cell_clear<<<blocks_for(d, 1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
+    k_cell_insert<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);
+    DYN_CUDA(cudaMemcpyAsync(d->query_buf, queries, (size_t)n * sizeof(dyn_query_record), cudaMemcpyHostToDevice, s));
+    const size_t smem = sizeof(QueryShared);
+    DYN_CUDA(cudaFuncSetAttribute(k_scene_query, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_scene_query<<<std::min<uint32_t>(n, d->sms * 4u), kQueryThreads, smem, s>>>(dw, d->query_buf, d->hit_buf, n);
+    DYN_CUDA(cudaGetLastError());
+    DYN_CUDA(cudaMemcpyAsync(queries, d->query_buf, (size_t)n * sizeof(dyn_query_record), cudaMemcpyDeviceToHost, s));
+    if (base) DYN_CUDA(cudaMemcpyAsync(hits, d->hit_buf, (size_t)base * sizeof(dyn_query_hit_record), cudaMemcpyDeviceToHost, s));
+    DYN_CUDA(cudaStreamSynchronize(s));
+    return DYN_OK;
+}
+
+// The triangles of a hull source (index triples over its vertices, dyn_hull_info's order).
+DYN_API dyn_status dyn_hull_triangles(const dyn_world* w, uint32_t source, uint32_t* out, uint32_t cap, uint32_t* count) {
+    if (!w || source >= w->hulls.size()) return DYN_ERR_INVALID;
+    const std::vector<uint32_t>& t = w->hulls[source].triangles;
+    const uint32_t m = (uint32_t)(t.size() / 3);
+    if (count) *count = m;
+    if (out) std::memcpy(out, t.data(), (size_t)std::min(m, cap) * 3 * sizeof(uint32_t));
     return DYN_OK;
 }
 

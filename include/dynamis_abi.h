@@ -446,6 +446,70 @@ typedef struct dyn_constraint_runtime_record {
     uint32_t _pad0;
 } dyn_constraint_runtime_record;
 
+/* Scene queries: crates/dynamis-abi/src/constant.rs:84-120 (query kinds, targets, filter flags),
+ * records.wgsl:5 (QUERY_CANDIDATES) */
+#define DYN_QUERY_RAY 0u
+#define DYN_QUERY_SPHERE 1u
+#define DYN_QUERY_CUBOID 2u
+#define DYN_QUERY_SWEEP 3u
+#define DYN_QUERY_POINT 4u
+#define DYN_QUERY_CONVEX 5u
+#define DYN_QUERY_TARGET_COLLIDERS 1u
+#define DYN_QUERY_TARGET_PARTICLES 2u
+#define DYN_FILTER_IGNORE_SENSORS 1u
+#define DYN_FILTER_IGNORE_SLEEPING 2u
+#define DYN_FILTER_IGNORE_STATIC 4u
+#define DYN_FILTER_IGNORE_KINEMATIC 8u
+#define DYN_QUERY_CANDIDATES 4096u
+
+/* records.wgsl:456-469 (48 bytes) */
+typedef struct dyn_query_filter_record {
+    uint32_t flags;    /* DYN_FILTER_* */
+    uint32_t targets;  /* DYN_QUERY_TARGET_* */
+    uint32_t group;    /* 0: no group filter */
+    uint32_t mask;
+    uint32_t exclude_id;  /* DYN_NO_BODY: none */
+    uint32_t exclude_generation;
+    uint32_t include_id;  /* DYN_NO_BODY: none */
+    uint32_t include_generation;
+    uint32_t exclude_soft_id;
+    uint32_t exclude_soft_generation;
+    uint32_t include_soft_id;
+    uint32_t include_soft_generation;
+} dyn_query_filter_record;
+
+/* records.wgsl:471-488 (144 bytes): QueryRecord. count and overflow are written back. */
+typedef struct dyn_query_record {
+    uint32_t kind;        /* DYN_QUERY_* */
+    uint32_t shape_kind;  /* the probe's DYN_SHAPE_* (sphere, cuboid, capsule, cylinder, hull) */
+    uint32_t source;      /* the probe's hull source */
+    uint32_t max_hits;
+    dyn_query_filter_record filters;
+    float origin[3];
+    float _pad0;
+    float direction[3];
+    float extent;         /* ray length, sphere radius, sweep length */
+    float radius;
+    float half_height;
+    uint32_t count;       /* hits written */
+    uint32_t hit_base;    /* first hit slot of this query in the batch's hit array */
+    float half_extents[3];
+    uint32_t overflow;    /* 1: more hits existed than were written */
+    float orientation[4];
+} dyn_query_record;
+
+/* records.wgsl:490-499 (48 bytes): QueryHit */
+typedef struct dyn_query_hit_record {
+    uint32_t body_id;
+    uint32_t body_generation;
+    float distance;
+    uint32_t scene_target;  /* the candidate: kind << DYN_ENTRY_KIND_SHIFT | collider slot */
+    float point[3];
+    uint32_t triangle;
+    float normal[3];
+    uint32_t surface;
+} dyn_query_hit_record;
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
@@ -499,5 +563,14 @@ DYN_ABI_ASSERT(offsetof(dyn_constraint_runtime_record, accumulated) == 80, "Cons
 DYN_ABI_ASSERT(offsetof(dyn_constraint_runtime_record, broken) == 144, "ConstraintRuntime.broken @144");
 DYN_ABI_ASSERT(offsetof(dyn_constraint_descriptor_record, axis_a) == 48, "ConstraintDescriptor.axis_a @48");
 DYN_ABI_ASSERT(offsetof(dyn_constraint_descriptor_record, break_force) == 116, "ConstraintDescriptor.break_force @116");
+DYN_ABI_ASSERT(sizeof(dyn_query_filter_record) == 48, "QueryFilter is 48 bytes");
+DYN_ABI_ASSERT(sizeof(dyn_query_record) == 144, "Query is 144 bytes");
+DYN_ABI_ASSERT(offsetof(dyn_query_record, origin) == 64, "Query.origin @64");
+DYN_ABI_ASSERT(offsetof(dyn_query_record, extent) == 92, "Query.extent @92");
+DYN_ABI_ASSERT(offsetof(dyn_query_record, hit_base) == 108, "Query.hit_base @108");
+DYN_ABI_ASSERT(offsetof(dyn_query_record, overflow) == 124, "Query.overflow @124");
+DYN_ABI_ASSERT(offsetof(dyn_query_record, orientation) == 128, "Query.orientation @128");
+DYN_ABI_ASSERT(sizeof(dyn_query_hit_record) == 48, "QueryHit is 48 bytes");
+DYN_ABI_ASSERT(offsetof(dyn_query_hit_record, normal) == 32, "QueryHit.normal @32");
 
 #endif /* DYNAMIS_ABI_H */
