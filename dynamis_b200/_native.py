@@ -51,6 +51,8 @@ SIGNATURES = {
     "dyn_debug_contacts": (I32, [P, P, U32, PU32]),
     "dyn_debug_islands": (I32, [P, P, U32, PU32]),
     "dyn_debug_resting": (I32, [P, P, U32, PU32]),
+    "dyn_query": (I32, [P, P, U32, P, U32]),
+    "dyn_hull_triangles": (I32, [P, U32, P, U32, PU32]),
     "dyn_set_timing": (I32, [P, I32]),
     "dyn_set_solver_guard": (I32, [P, U32]),
     "dyn_set_ccd": (I32, [P, U32, I32]),

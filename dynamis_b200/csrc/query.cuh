@@ -286,6 +286,20 @@ __device__ __forceinline__ WShape query_shape(const dyn_query_record& q, f3 cent
     s.scale = s3(1.0f);
     return s;
 }
+// The shape a query tests with. QueryRecord::sphere, ::point and ::cuboid leave the orientation zero
+// (crates/dynamis-abi/src/query.rs:115-144 over a zeroed record), and a zero quaternion rotates every
+// support offset to nothing, so the reference's probe answers with its centre point (the
+// normalisation of the zero direction that precedes it is left to the backend: here it is skipped,
+// and the probe is that point). The query's box (query_box) keeps the record's own shape.
+__device__ __forceinline__ WShape query_probe(const dyn_query_record& q, f3 center) {
+    WShape s = query_shape(q, center);
+    if (s.rotation.x == 0.0f && s.rotation.y == 0.0f && s.rotation.z == 0.0f && s.rotation.w == 0.0f) {
+        s.kind = DYN_SHAPE_SPHERE;
+        s.radius = 0.0f;
+        s.rotation = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    }
+    return s;
+}
 __device__ __forceinline__ f3 q_origin(const dyn_query_record& q) { return mk3(q.origin[0], q.origin[1], q.origin[2]); }
 __device__ __forceinline__ f3 q_direction(const dyn_query_record& q) {
     return mk3(q.direction[0], q.direction[1], q.direction[2]);
@@ -334,7 +348,7 @@ __device__ float overlap_world_geom(const DeviceWorld& w, const dyn_query_record
     float distance = kQNoHit;
     if (shape_has_source(scene.kind)) {
         const float4 qc = quat_conj(scene.rotation);
-        WShape local = query_shape(q, quat_rotate(qc, q_origin(q) - scene.center));
+        WShape local = query_probe(q, quat_rotate(qc, q_origin(q) - scene.center));
         local.rotation = quat_mul(qc, local.rotation);
         const dyn_shape_source_record& src = w.sources[scene.source];
         const uint2 range = w.hull_tri_range[scene.source];
@@ -356,11 +370,11 @@ __device__ float overlap_world_geom(const DeviceWorld& w, const dyn_query_record
 
 // overlap_hit (scene_cast.wgsl:160-178)
 __device__ float overlap_hit(const DeviceWorld& w, const dyn_query_record& q, const WShape& world, f3* out_normal) {
-    WShape probe = query_shape(q, q_origin(q));
+    WShape probe = query_probe(q, q_origin(q));
     probe.radius = 0.0f;
     const GjkOut closest = gjk_phase(w, probe, world);
     if (closest.pen) {
-        const Hit hit = penetration_hit(w, query_shape(q, q_origin(q)), world);
+        const Hit hit = penetration_hit(w, query_probe(q, q_origin(q)), world);
         *out_normal = hit.normal;
         return -q.extent + wmax(hit.distance + q.extent, 0.0f);
     }
@@ -411,7 +425,7 @@ __device__ QHit resolve_hit(const DeviceWorld& w, const dyn_query_record& q, con
     }
     const bool world_geom = shape_world_geometry(world.kind);
     if (kind == DYN_QUERY_SWEEP) {
-        const QHit hit = shape_sweep(w, query_shape(q, q_origin(q)), world, q_origin(q), q_direction(q), q.extent);
+        const QHit hit = shape_sweep(w, query_probe(q, q_origin(q)), world, q_origin(q), q_direction(q), q.extent);
         return hit.distance < kQNoHit ? hit : q_no_hit();
     }
     f3 normal = s3(0.0f);
@@ -427,7 +441,7 @@ __device__ QHit resolve_hit(const DeviceWorld& w, const dyn_query_record& q, con
         if (separation < kQNoHit) return QHit{separation, world.center, normal, DYN_NO_TRIANGLE};
         return q_no_hit();
     }
-    const WShape probe = query_shape(q, q_origin(q));
+    const WShape probe = query_probe(q, q_origin(q));
     const GjkOut closest = gjk_phase(w, probe, world);
     if (closest.pen) {
         const Hit hit = penetration_hit(w, probe, world);

@@ -120,6 +120,105 @@ CONSTRAINT_RUNTIME = _dtype(_fields([
 ]), 160)
 CONSTRAINT_BALL = 0
 # records.wgsl BodyEdit: a command kind, a patch mask and the state it carries (160 bytes)
+# scene queries (records.wgsl:456-499; constant.rs:84-120)
+QUERY_RAY, QUERY_SPHERE, QUERY_CUBOID, QUERY_SWEEP, QUERY_POINT, QUERY_CONVEX = 0, 1, 2, 3, 4, 5
+QUERY_TARGET_COLLIDERS, QUERY_TARGET_PARTICLES = 1, 2
+FILTER_IGNORE_SENSORS, FILTER_IGNORE_SLEEPING, FILTER_IGNORE_STATIC, FILTER_IGNORE_KINEMATIC = 1, 2, 4, 8
+QUERY_CANDIDATES = 4096
+NO_TRIANGLE = 0xFFFFFFFF
+QUERY_FILTER = np.dtype([(name, "<u4") for name in (
+    "flags", "targets", "group", "mask", "exclude_id", "exclude_generation", "include_id", "include_generation",
+    "exclude_soft_id", "exclude_soft_generation", "include_soft_id", "include_soft_generation")])
+QUERY = _dtype(_fields([
+    ("kind", "<u4", 1, 0), ("shape_kind", "<u4", 1, 4), ("source", "<u4", 1, 8), ("max_hits", "<u4", 1, 12),
+]) + [("filters", QUERY_FILTER, 16)] + _fields([
+    ("origin", "<f4", 3, 64), ("direction", "<f4", 3, 80), ("extent", "<f4", 1, 92), ("radius", "<f4", 1, 96),
+    ("half_height", "<f4", 1, 100), ("count", "<u4", 1, 104), ("hit_base", "<u4", 1, 108),
+    ("half_extents", "<f4", 3, 112), ("overflow", "<u4", 1, 124), ("orientation", "<f4", 4, 128),
+]), 144)
+QUERY_HIT = _dtype(_fields([
+    ("body_id", "<u4", 1, 0), ("body_generation", "<u4", 1, 4), ("distance", "<f4", 1, 8), ("scene_target", "<u4", 1, 12),
+    ("point", "<f4", 3, 16), ("triangle", "<u4", 1, 28), ("normal", "<f4", 3, 32), ("surface", "<u4", 1, 44),
+]), 48)
+assert QUERY_FILTER.itemsize == 48 and QUERY.itemsize == 144 and QUERY_HIT.itemsize == 48
+
+
+def query_filter(max_hits: int = 4, group: int = 0, mask: int = 0xFFFFFFFF, ignore_sensors: bool = True,
+                 ignore_sleeping: bool = False, ignore_static: bool = False, ignore_kinematic: bool = False,
+                 exclude=None, include=None, colliders: bool = True, particles: bool = True) -> dict:
+    """QueryFilter::default (crates/dynamis-model/src/query.rs:41-58) with overrides; exclude and
+    include are (body id, generation) pairs."""
+    return dict(max_hits=max_hits, group=group, mask=mask, ignore_sensors=ignore_sensors,
+                ignore_sleeping=ignore_sleeping, ignore_static=ignore_static, ignore_kinematic=ignore_kinematic,
+                exclude=exclude, include=include, colliders=colliders, particles=particles)
+
+
+def _query_record(kind: int, filt: dict | None) -> np.ndarray:
+    """query_record (crates/dynamis-abi/src/query.rs:44-74)."""
+    f = query_filter() if filt is None else filt
+    q = np.zeros(1, QUERY)
+    q["kind"] = kind
+    flags = ((FILTER_IGNORE_SENSORS if f["ignore_sensors"] else 0) | (FILTER_IGNORE_SLEEPING if f["ignore_sleeping"] else 0)
+             | (FILTER_IGNORE_STATIC if f["ignore_static"] else 0) | (FILTER_IGNORE_KINEMATIC if f["ignore_kinematic"] else 0))
+    fr = q["filters"]
+    fr["flags"] = flags
+    fr["targets"] = (QUERY_TARGET_COLLIDERS if f["colliders"] else 0) | (QUERY_TARGET_PARTICLES if f["particles"] else 0)
+    fr["group"], fr["mask"] = f["group"], f["mask"]
+    fr["exclude_id"], fr["exclude_generation"] = f["exclude"] if f["exclude"] is not None else (NO_BODY, 0)
+    fr["include_id"], fr["include_generation"] = f["include"] if f["include"] is not None else (NO_BODY, 0)
+    fr["exclude_soft_id"] = fr["include_soft_id"] = NO_BODY
+    q["filters"] = fr
+    q["max_hits"] = f["max_hits"]
+    return q
+
+
+def _probe_shape(q: np.ndarray, shape: dict) -> None:
+    """shape_fields (query.rs:76-98): shape = dict(kind=SHAPE_*, radius, half_height, half_extents, source)."""
+    q["shape_kind"] = shape["kind"]
+    q["source"] = shape.get("source", 0)
+    q["radius"] = shape.get("radius", 0.0)
+    q["half_height"] = shape.get("half_height", 0.0)
+    q["half_extents"] = shape.get("half_extents", (0.0, 0.0, 0.0))
+
+
+def ray_query(origin, direction, max_t: float, filt: dict | None = None) -> np.ndarray:
+    q = _query_record(QUERY_RAY, filt)
+    q["origin"], q["direction"], q["extent"] = origin, direction, max_t
+    return q
+
+
+def sphere_query(center, radius: float, filt: dict | None = None) -> np.ndarray:
+    q = _query_record(QUERY_SPHERE, filt)
+    q["shape_kind"], q["origin"], q["extent"], q["radius"] = SHAPE_SPHERE, center, radius, radius
+    return q
+
+
+def point_query(origin, filt: dict | None = None) -> np.ndarray:
+    q = _query_record(QUERY_POINT, filt)
+    q["shape_kind"], q["origin"] = SHAPE_SPHERE, origin
+    return q
+
+
+def cuboid_query(center, half_extents, filt: dict | None = None) -> np.ndarray:
+    q = _query_record(QUERY_CUBOID, filt)
+    q["shape_kind"], q["origin"], q["half_extents"] = SHAPE_CUBOID, center, half_extents
+    return q
+
+
+def overlap_query(shape: dict, orientation, position, filt: dict | None = None) -> np.ndarray:
+    q = _query_record(QUERY_CONVEX, filt)
+    q["origin"], q["orientation"] = position, orientation
+    _probe_shape(q, shape)
+    return q
+
+
+def sweep_query(shape: dict, orientation, start, direction, length: float, filt: dict | None = None) -> np.ndarray:
+    q = _query_record(QUERY_SWEEP, filt)
+    q["origin"], q["direction"], q["extent"], q["orientation"] = start, direction, length, orientation
+    _probe_shape(q, shape)
+    return q
+
+
 BODY_EDIT = np.dtype({"names": ["kind", "mask", "state"], "formats": ["<u4", "<u4", BODY_STATE],
                       "offsets": [0, 4, 16], "itemsize": 160})
 EDIT_PATCH, EDIT_FORCE, EDIT_TORQUE, EDIT_IMPULSE, EDIT_SLEEP, EDIT_WAKE = 0, 1, 2, 3, 4, 5

@@ -131,7 +131,8 @@ class World:
         self._check(lib.dyn_export_scene(self._h, ptr(states), ptr(descs), ptr(colliders), ptr(owners), ptr(sources),
                                          ptr(vertices)))
         scene = {"states": states, "descs": descs, "colliders": colliders, "owners": owners, "sources": sources,
-                 "vertices": vertices, "dynamic": s["dynamic"]}
+                 "vertices": vertices, "dynamic": s["dynamic"],
+                 "hull_triangles": [self.hull_triangles(i) for i in range(s["sources"])]}
         body_world = np.zeros(s["bodies"], np.uint32)
         self._check(lib.dyn_export_body_worlds(self._h, ptr(body_world)))
         if body_world.any():
@@ -364,6 +365,25 @@ class World:
         self._check(lib.dyn_debug_islands(self._h, None, 0, ctypes.byref(n)))
         out = np.zeros(n.value, np.uint32)
         self._check(lib.dyn_debug_islands(self._h, ptr(out), n.value, None))
+        return out
+
+    def query(self, queries: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """dyn_query: a batch of scene queries (records.QUERY, e.g. from records.ray_query) against the
+        current states. Returns the records (hit_base, count and overflow set) and the hit array
+        (records.QUERY_HIT); query i's hits are hits[hit_base : hit_base + count], nearest first."""
+        q = np.array(queries, R.QUERY).reshape(-1)
+        bound = int(np.minimum(q["max_hits"], R.QUERY_CANDIDATES).sum())
+        hits = np.zeros(max(bound, 1), R.QUERY_HIT)
+        self._check(lib.dyn_query(self._h, ptr(q), len(q), ptr(hits), len(hits)))
+        return q, hits[:bound]
+
+    def hull_triangles(self, source: int) -> np.ndarray:
+        """dyn_hull_triangles: the hull's triangles, (m, 3) vertex indices."""
+        n = ctypes.c_uint32()
+        self._check(lib.dyn_hull_triangles(self._h, int(source), None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 3), np.uint32)
+        if n.value:
+            self._check(lib.dyn_hull_triangles(self._h, int(source), ptr(out), n.value, None))
         return out
 
     def debug_resting(self) -> np.ndarray:

@@ -197,6 +197,23 @@ DYN_API dyn_status dyn_debug_entries(dyn_world* world, uint32_t* keys, uint32_t*
 DYN_API dyn_status dyn_debug_pairs(dyn_world* world, uint32_t* major, uint32_t* minor, uint32_t cap, uint32_t* count);
 DYN_API dyn_status dyn_debug_contacts(dyn_world* world, dyn_contact_record* out, uint32_t cap, uint32_t* count);
 DYN_API dyn_status dyn_debug_islands(dyn_world* world, uint32_t* out, uint32_t cap, uint32_t* count);
+/* Scene queries: World::ray_query, sphere_query, cuboid_query, point_query, overlap_query and
+ * sweep_query, then resolve_queries and query_hits (crates/dynamis-world/src/query.rs:50-175;
+ * scene_cast.wgsl), as one synchronous call against the world's current body states. Each record
+ * is a QueryRecord as crates/dynamis-abi/src/query.rs:103-181 builds it (kind, probe shape, filters,
+ * origin, direction, extent, max_hits). The library gives query i the hit slots
+ * [hit_base, hit_base + min(max_hits, DYN_QUERY_CANDIDATES)) in submission order (hit_capacity must
+ * hold their sum, else DYN_ERR_CAPACITY), writes its hits nearest first, and sets count and overflow
+ * (1 when more hits existed than were written, or the candidate walk passed DYN_QUERY_CANDIDATES).
+ * Targets are colliders (particles belong to soft bodies, outside this library). The call rebuilds
+ * the grid index from the current states first, as the reference's query run does, so
+ * dyn_read_counters then shows that index's ENTRIES and GRID_* counters. Refused (DYN_ERR_INVALID)
+ * for an invalid record and for a world of batched sub-worlds. */
+DYN_API dyn_status dyn_query(dyn_world* world, dyn_query_record* queries, uint32_t n, dyn_query_hit_record* hits,
+                             uint32_t hit_capacity);
+/* The triangles of a hull source: index triples over its vertices (dyn_hull_info's numbering). */
+DYN_API dyn_status dyn_hull_triangles(const dyn_world* world, uint32_t source, uint32_t* out, uint32_t cap, uint32_t* count);
+
 /* The frozen contacts the next step reads (freeze_contacts.wgsl / thaw_contacts.wgsl: contacts of
  * body pairs that were both at rest when a step ended), six words each: first body id, its
  * generation, second body id, its generation, collider a, collider b. Order is not meaningful.

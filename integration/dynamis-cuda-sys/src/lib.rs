@@ -9,7 +9,7 @@ use std::os::raw::{c_char, c_void};
 
 pub use dynamis_abi::{
     BodyDescriptorRecord, BodyEditRecord, BodyStateRecord, ColliderRecord, ConstraintDescriptorRecord,
-    ConstraintRuntimeRecord, ContactRecord, StepParamsRecord,
+    ConstraintRuntimeRecord, ContactRecord, QueryHitRecord, QueryRecord, StepParamsRecord,
 };
 
 /// An opaque world handle (dyn_world).
@@ -201,6 +201,8 @@ extern "C" {
     pub fn dyn_debug_contacts(world: *mut DynWorld, out: *mut ContactRecord, cap: u32, count: *mut u32) -> DynStatus;
     pub fn dyn_debug_islands(world: *mut DynWorld, out: *mut u32, cap: u32, count: *mut u32) -> DynStatus;
     pub fn dyn_debug_resting(world: *mut DynWorld, out: *mut u32, cap: u32, count: *mut u32) -> DynStatus;
+    pub fn dyn_query(world: *mut DynWorld, queries: *mut QueryRecord, n: u32, hits: *mut QueryHitRecord, hit_capacity: u32) -> DynStatus;
+    pub fn dyn_hull_triangles(world: *const DynWorld, source: u32, out: *mut u32, cap: u32, count: *mut u32) -> DynStatus;
     pub fn dyn_set_timing(world: *mut DynWorld, enabled: i32) -> DynStatus;
     pub fn dyn_step_kernel_count(world: *const DynWorld) -> u32;
     pub fn dyn_stage_count() -> u32;

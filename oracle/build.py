@@ -15,7 +15,7 @@ ROOT = HERE.parent
 OUT = HERE / "_build"
 LIBRARY = OUT / "liboracle.so"
 SOURCES = [HERE / "oracle.cpp", HERE / "adjoint64.cpp", HERE / "scene.cpp"]
-HEADERS = [HERE / "oracle_math.h", HERE / "oracle_geom.h", ROOT / "include" / "dynamis_abi.h",
+HEADERS = [HERE / "oracle_math.h", HERE / "oracle_geom.h", HERE / "oracle_query.h", ROOT / "include" / "dynamis_abi.h",
            ROOT / "include" / "dynamis_cuda.h"]
 
 

@@ -35,6 +35,7 @@
 
 #include "dynamis_abi.h"
 #include "oracle_geom.h"
+#include "oracle_query.h"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -250,6 +251,8 @@ struct OracleWorld {
         uint32_t first_id, first_generation, second_id, second_generation, a, b;
     };
     std::vector<Frozen> resting;
+    // every hull's triangles (index triples over its vertices) and each source's (first, count)
+    std::vector<uint32_t> hull_tris, hull_tri_ranges;
     // body commands queued for the next step: (row, edit), in command order
     std::vector<std::pair<uint32_t, dyn_body_edit_record>> edits;
     uint32_t world_of(uint32_t row) const { return body_world.empty() ? 0u : body_world[row]; }
@@ -2270,6 +2273,82 @@ void orc_radix_sort(uint32_t* major, uint32_t* minor, uint32_t* payload, uint32_
     std::memcpy(major, a.data(), n * 4);
     std::memcpy(minor, b.data(), n * 4);
     if (payload) std::memcpy(payload, c.data(), n * 4);
+}
+
+// The triangles of hull source `source` (index triples), for the scene queries' hull tests.
+void orc_set_hull_triangles(OracleWorld* w, uint32_t source, const uint32_t* tris, uint32_t n) {
+    if (w->hull_tri_ranges.size() < 2 * ((size_t)source + 1)) w->hull_tri_ranges.resize(2 * ((size_t)source + 1), 0u);
+    w->hull_tri_ranges[2 * (size_t)source] = (uint32_t)(w->hull_tris.size() / 3);
+    w->hull_tri_ranges[2 * (size_t)source + 1] = n;
+    w->hull_tris.insert(w->hull_tris.end(), tris, tris + 3 * (size_t)n);
+}
+
+// A batch of scene queries against the world's current states (scene_cast.wgsl:434-533): every
+// collider is tested (the library walks the grid cells under the query's box instead, which holds
+// every collider a test can hit), the hits are ordered by (distance key, collider slot) and at most
+// min(max_hits, QUERY_CANDIDATES) are written from hit_base; count and overflow (hits left out) are
+// set. hit_base is assigned in submission order, as World::submit_query does.
+void orc_query(const OracleWorld* cw, dyn_query_record* queries, uint32_t n, dyn_query_hit_record* hits) {
+    const OracleWorld& w = *cw;
+    HullTriangles ht{w.hull_tris.data(), w.hull_tri_ranges.data(), (uint32_t)(w.hull_tri_ranges.size() / 2)};
+    uint32_t base = 0;
+    for (uint32_t qi = 0; qi < n; ++qi) {
+        dyn_query_record& q = queries[qi];
+        q.hit_base = base;
+        const uint32_t capacity = std::min(q.max_hits, DYN_QUERY_CANDIDATES);
+        base += capacity;
+        struct Found {
+            uint64_t key;
+            ShapeHit hit;
+            uint32_t slot;
+        };
+        std::vector<Found> found;
+        const bool colliders = (q.filters.targets & DYN_QUERY_TARGET_COLLIDERS) != 0u;
+        for (uint32_t slot = 0; colliders && slot < w.colliders.size(); ++slot) {
+            const uint32_t row = w.owners[slot];
+            if (row == DYN_NO_BODY) continue;
+            const dyn_body_state_record& st = w.states[row];
+            const dyn_body_descriptor_record& d = w.descs[row];
+            const dyn_collider_record& c = w.colliders[slot];
+            const dyn_query_filter_record& f = q.filters;
+            if (f.exclude_id != DYN_NO_BODY && st.body_id == f.exclude_id && st.generation == f.exclude_generation) continue;
+            if (f.include_id != DYN_NO_BODY && (st.body_id != f.include_id || st.generation != f.include_generation)) continue;
+            if ((f.flags & DYN_FILTER_IGNORE_SENSORS) && (c.flags & DYN_COLLIDER_SENSOR)) continue;
+            if ((f.flags & DYN_FILTER_IGNORE_SLEEPING) && st.sleeping != 0u) continue;
+            if ((f.flags & DYN_FILTER_IGNORE_STATIC) && !body_moves_d(d.inverse_mass, d.flags)) continue;
+            if ((f.flags & DYN_FILTER_IGNORE_KINEMATIC) && body_moves_d(d.inverse_mass, d.flags) &&
+                !body_simulates_d(d.inverse_mass, d.flags))
+                continue;
+            if (f.group != 0u) {
+                uint32_t group = c.collision_group != DYN_NO_COLLISION_FILTER ? c.collision_group : d.collision_group;
+                uint32_t mask = c.collision_mask != DYN_NO_COLLISION_FILTER ? c.collision_mask : d.collision_mask;
+                if (!((f.group & mask) != 0u && (group & f.mask) != 0u)) continue;
+            }
+            if (c.kind == DYN_SHAPE_NONE) continue;
+            WorldShape world = world_collider(rd3(st.position), rd4(st.orientation), c);
+            ShapeHit hit = resolve_hit(w.shapes, ht, q, world);
+            if (!(hit.distance < kNoHit)) continue;
+            found.push_back(Found{((uint64_t)hit_key(hit.distance) << 32) | slot, hit, slot});
+        }
+        std::sort(found.begin(), found.end(), [](const Found& a, const Found& b) { return a.key < b.key; });
+        const uint32_t emitted = std::min<uint32_t>(capacity, (uint32_t)found.size());
+        for (uint32_t i = 0; i < emitted; ++i) {
+            const Found& h = found[i];
+            const dyn_body_state_record& st = w.states[w.owners[h.slot]];
+            dyn_query_hit_record r{};
+            r.body_id = st.body_id;
+            r.body_generation = st.generation;
+            r.distance = h.hit.distance;
+            r.scene_target = (DYN_ENTRY_KIND_COLLIDER << DYN_ENTRY_KIND_SHIFT) | h.slot;
+            wr3(r.point, h.hit.point);
+            r.triangle = h.hit.triangle;
+            wr3(r.normal, h.hit.normal);
+            r.surface = DYN_NO_SURFACE;
+            hits[q.hit_base + i] = r;
+        }
+        q.count = emitted;
+        q.overflow = emitted < found.size() ? 1u : 0u;
+    }
 }
 
 // One pair through the narrowphase restatement (bodies/colliders from the world).

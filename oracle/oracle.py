@@ -88,6 +88,11 @@ class OracleWorld:
             raise ValueError("oracle refused the scene: collider owners or hull sources out of range")
         if "body_world" in s:
             L.orc_set_body_worlds(self._h, _p(s["body_world"]), len(s["body_world"]))
+        L.orc_set_hull_triangles.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32]
+        for source, tris in enumerate(scene.get("hull_triangles", [])):
+            tris = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+            self._keep[f"hull_triangles_{source}"] = tris
+            L.orc_set_hull_triangles(self._h, source, _p(tris), len(tris))
         if "constraint_descs" in s:
             m = len(s["constraint_descs"])
             if not L.orc_set_constraints(self._h, _p(s["constraint_descs"]), _p(s["constraint_rows"]),
@@ -180,6 +185,17 @@ class OracleWorld:
         comps = np.zeros((sizes[2], 2), np.uint32)
         lib().orc_joint_plan(self._h, _p(rows), _p(layers), _p(comps), None)
         return {"rows": rows, "layers": layers, "components": comps}
+
+    def query(self, queries: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """A batch of scene queries (records.QUERY) against this world's current states: the records
+        with hit_base, count and overflow set, and the hit array (records.QUERY_HIT)."""
+        q = np.array(queries, R.QUERY).reshape(-1)
+        bound = int(np.minimum(q["max_hits"], R.QUERY_CANDIDATES).sum())
+        hits = np.zeros(max(bound, 1), R.QUERY_HIT)
+        L = lib()
+        L.orc_query.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+        L.orc_query(self._h, _p(q), len(q), _p(hits))
+        return q, hits[:bound]
 
     def resting(self) -> np.ndarray:
         """The frozen contacts: first id, its generation, second id, its generation, collider a, collider b."""
