@@ -175,6 +175,33 @@ def long_run_checks(world, dt: float, before: dict, top: float) -> dict:
             "within_bounds": bool(e1 <= e0 * (1.0 + 1e-6) and faster == 0 and np.all(np.isfinite(speed)))}
 
 
+def query_benchmark(world, batch: int = 16384, repeats: int = 3, seed: int = 9) -> dict:
+    """Scene queries on the world as it stands (the formed pile): a batch of rays cast down onto it
+    from above the lattice and a batch of sphere overlaps inside it, each through dyn_query (which
+    first rebuilds the grid index from the current states), timed on the host around the whole call,
+    best of `repeats`."""
+    from dynamis_b200 import records as R
+
+    rng = np.random.default_rng(seed)
+    s = world.read_states()["position"]
+    lo, hi = s.min(axis=0), s.max(axis=0)
+    origins = rng.uniform(lo, hi, size=(batch, 3)).astype(np.float32)
+    rays = np.concatenate([R.ray_query((o[0], hi[1] + 5.0, o[2]), (0, -1, 0), float(hi[1] - lo[1] + 10.0),
+                                       R.query_filter(max_hits=4)) for o in origins])
+    spheres = np.concatenate([R.sphere_query(o, 0.75, R.query_filter(max_hits=8)) for o in origins])
+    out = {"batch": batch}
+    for name, records in (("rays", rays), ("spheres", spheres)):
+        best = float("inf")
+        hits = 0
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            q, _ = world.query(records)
+            best = min(best, time.perf_counter() - t0)
+            hits = int(q["count"].sum())
+        out[name] = {"ms": round(best * 1e3, 3), "queries_per_s": round(batch / best, 1), "hits": hits}
+    return out
+
+
 def guarded_run(args, dt: float, device: int) -> dict:
     """The same workload with the row-mass guard on (dyn_set_solver_guard): the same setup, warm-up
     and timed steps, its setup bounds, its device time per step."""
@@ -336,6 +363,9 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     }
     # the measurements beside the headline run at N = 1 only (the scaling runs time the replicas)
     extras = world_size == 1
+    if extras and not args.no_queries:
+        result["queries"] = query_benchmark(world)
+        log(f"queries {result['queries']}")
     if extras and not args.no_batch:
         result["batch"] = batch_benchmark(args, local_rank)
     if extras and not args.no_guarded:
@@ -592,6 +622,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-towers measurement")
     ap.add_argument("--no-guarded", action="store_true", help="skip the run with the row-mass guard")
+    ap.add_argument("--no-queries", action="store_true", help="skip the scene-query measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
     ap.add_argument("--tuning-cache", default=None, help="JSON file of per-workload launch shapes to reuse and extend")
