@@ -2324,7 +2324,9 @@ static bool query_valid(const dyn_world* w, const dyn_query_record& q) {
     if (q.kind == DYN_QUERY_SPHERE && !(q.radius > 0.0f && q.extent > 0.0f)) return false;
     if (q.kind == DYN_QUERY_CUBOID && !(q.half_extents[0] > 0.0f && q.half_extents[1] > 0.0f && q.half_extents[2] > 0.0f))
         return false;
-    if (q.kind == DYN_QUERY_CONVEX || q.kind == DYN_QUERY_SWEEP || q.kind == DYN_QUERY_CUBOID) {
+    // QueryRecord::cuboid, ::sphere and ::point leave the orientation zero (query.rs:115-144); the
+    // shaped probes of overlap and sweep queries carry a unit one (query.rs:146-181)
+    if (q.kind == DYN_QUERY_CONVEX || q.kind == DYN_QUERY_SWEEP) {
         const uint32_t k = q.shape_kind;
         if (!(k == DYN_SHAPE_SPHERE || k == DYN_SHAPE_CUBOID || k == DYN_SHAPE_CAPSULE || k == DYN_SHAPE_CYLINDER ||
               k == DYN_SHAPE_HULL))

@@ -166,6 +166,27 @@ def test_filters_select_bodies():
     assert list(found[5]["body_id"]) == [ids[3]]
 
 
+def test_the_host_accepts_every_record_the_builders_make():
+    # validation runs on the host before any device work: a valid batch gets past it (and on a
+    # machine without a GPU stops at the device), an invalid one is refused as invalid
+    from dynamis_b200._native import DynamisError
+    w, _ = make([static_sphere(0.5, (0, 0, 0))])
+    probe = dict(kind=R.SHAPE_CAPSULE, radius=0.2, half_height=0.3)
+    valid = np.concatenate([R.ray_query((0, 0, 0), (0, 0, 1), 20.0), R.sphere_query((0, 0, 0), 0.5),
+                            R.point_query((0, 0, 0)), R.cuboid_query((0, 0, 0), (1, 1, 1)),
+                            R.overlap_query(probe, (0, 0, 0, 1), (0, 0, 0)),
+                            R.sweep_query(probe, (0, 0, 0, 1), (0, 0, 0), (1, 0, 0), 2.0)])
+    try:
+        w.query(valid)
+    except DynamisError as e:
+        assert e.status != 1, "a valid query batch was refused as invalid"
+    for bad in (R.ray_query((0, 0, 0), (0, 0, 1), -1.0), R.sphere_query((0, 0, 0), 0.0),
+                R.overlap_query(probe, (0, 0, 0, 2), (0, 0, 0)), R.overlap_query(dict(kind=R.SHAPE_PLANE), (0, 0, 0, 1), (0, 0, 0))):
+        with pytest.raises(DynamisError) as e:
+            w.query(bad)
+        assert e.value.status == 1
+
+
 def test_invalid_queries_are_refused():
     from dynamis_b200._native import DynamisError
     w, _ = make([static_sphere(0.5, (0, 0, 0))])
