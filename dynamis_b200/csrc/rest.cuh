@@ -22,29 +22,24 @@ __device__ __forceinline__ bool row_active(const DeviceWorld& w, uint32_t row) {
     return moves(h.pos.w, h.aux.y) && h.aux.x == 0u;  // body_is_active, core.wgsl:229-231
 }
 
-// island_link_resting.wgsl:10-21: every frozen contact couples its two rows (after the contacts and
-// the constraints, before the last flatten).
-__global__ void k_island_link_resting(DeviceWorld w) {
-    const uint32_t count = min(w.ctl[CTL_RESTING], w.rest_cap);
-    GRID_STRIDE(i, count) {
-        const uint4 r = w.rest_in[i];
-        const uint32_t a = resolve_row(w, r.x, r.y), b = resolve_row(w, r.z, r.w);
-        if (a == DYN_NO_BODY || b == DYN_NO_BODY) continue;
-        if (!island_couple(w, a, b)) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
-    }
-}
+// island_link_resting.wgsl runs inside the second contact-link pass (k_island_link<false>, step.cuh).
 
 // thaw_contacts.wgsl:47-76: a frozen contact stays while both of its bodies were inactive when the
 // step began (activity.wgsl, written by k_begin); one whose body is gone is released and its other
 // body disturbed (a wake flag the next step acts on). Contact events are not published here.
+// The same launch clears the static rows' wake flags (static_wake_clear.wgsl), which the reference
+// runs right after the thaw: a disturbed static row would lose its flag there at once, so the thaw
+// here disturbs dynamic rows only, and the two loops need no order between them.
 __global__ void k_rest_thaw(DeviceWorld w) {
+    const uint32_t statics = w.n - w.nd;
+    GRID_STRIDE(i, statics) w.wake_flags[w.nd + i] = 0u;
     const uint32_t count = min(w.ctl[CTL_RESTING], w.rest_cap);
     GRID_STRIDE(i, count) {
         const uint4 r = w.rest_in[i];
         const uint32_t a = resolve_row(w, r.x, r.y), b = resolve_row(w, r.z, r.w);
         if (a == DYN_NO_BODY || b == DYN_NO_BODY) {
-            if (a != DYN_NO_BODY) atomicOr(&w.wake_flags[a], 1u);
-            if (b != DYN_NO_BODY) atomicOr(&w.wake_flags[b], 1u);
+            if (a != DYN_NO_BODY && a < w.nd) atomicOr(&w.wake_flags[a], 1u);
+            if (b != DYN_NO_BODY && b < w.nd) atomicOr(&w.wake_flags[b], 1u);
             continue;
         }
         if (w.activity[a] != 0u || w.activity[b] != 0u) continue;
@@ -53,12 +48,6 @@ __global__ void k_rest_thaw(DeviceWorld w) {
         w.rest_out[slot] = r;
         w.rest_out_slots[slot] = w.rest_in_slots[i];
     }
-}
-
-// static_wake_clear.wgsl: a static row's wake flag lasts the step that set it.
-__global__ void k_static_wake_clear(DeviceWorld w) {
-    const uint32_t statics = w.n - w.nd;
-    GRID_STRIDE(i, statics) w.wake_flags[w.nd + i] = 0u;
 }
 
 // freeze_contacts.wgsl:29-45: every contact of this step whose bodies are both inactive after it

@@ -1284,6 +1284,16 @@ __global__ void k_island_link(DeviceWorld w, dyn_step_params p) {
         }
         if (!island_union(w, r.x, r.y)) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
     }
+    if (kSample) return;
+    // island_link_resting.wgsl:10-21 in the same pass: every frozen contact (rest.cuh) couples its
+    // two rows; unions commute, so sharing the launch with the contacts changes no island
+    const uint32_t frozen = min(w.ctl[CTL_RESTING], w.rest_cap);
+    GRID_STRIDE(i, frozen) {
+        const uint4 r = w.rest_in[i];
+        const uint32_t a = resolve_row(w, r.x, r.y), b = resolve_row(w, r.z, r.w);
+        if (a == DYN_NO_BODY || b == DYN_NO_BODY) continue;
+        if (!island_couple(w, a, b)) add_counter(&w.counters[DYN_COUNTER_ISLAND_FAULTS], 1u);
+    }
 }
 // island_flatten.wgsl:4-8 repeated ilog2(max(N,2))+1 times leaves every row pointing at its root
 // (pointer jumping doubles the reach each round and a chain is at most N long); one pass that

@@ -806,7 +806,6 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     k_island_flatten<false><<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     k_island_link<false><<<blocks_for(d, C, 256), 256, 0, s>>>(dw, p);
     if (dw.jcount) k_island_link_joints<<<blocks_for(d, dw.jcount, 256), 256, 0, s>>>(dw);
-    k_island_link_resting<<<blocks_for(d, dw.rest_cap, 256), 256, 0, s>>>(dw);
     k_island_flatten<true><<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
     mark(ST_WAKE_LIVE);
     k_wake_live<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw);
@@ -863,9 +862,8 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     }
     mark(ST_SLEEP);
     k_sleep<<<blocks_for(d, ND, 256), 256, 0, s>>>(dw, p);
-    // commit (crates/dynamis-rigid/src/commit.rs:187-208): thaw, static wake flags, freeze
-    k_rest_thaw<<<blocks_for(d, dw.rest_cap, 256), 256, 0, s>>>(dw);
-    k_static_wake_clear<<<blocks_for(d, N, 256), 256, 0, s>>>(dw);
+    // commit (crates/dynamis-rigid/src/commit.rs:187-208): thaw with the static wake flags, freeze
+    k_rest_thaw<<<blocks_for(d, std::max(dw.rest_cap, N), 256), 256, 0, s>>>(dw);
     k_rest_freeze<<<blocks_for(d, C, 256), 256, 0, s>>>(dw);
     k_rest_commit<<<1, 32, 0, s>>>(dw);
     if (tape) {
