@@ -2283,13 +2283,80 @@ void orc_set_hull_triangles(OracleWorld* w, uint32_t source, const uint32_t* tri
     w->hull_tris.insert(w->hull_tris.end(), tris, tris + 3 * (size_t)n);
 }
 
-// A batch of scene queries against the world's current states (scene_cast.wgsl:434-533): every
-// collider is tested (the library walks the grid cells under the query's box instead, which holds
-// every collider a test can hit), the hits are ordered by (distance key, collider slot) and at most
-// min(max_hits, QUERY_CANDIDATES) are written from hit_base; count and overflow (hits left out) are
-// set. hit_base is assigned in submission order, as World::submit_query does.
+// query_world_aabb (scene_cast.wgsl:341-362)
+Aabb query_world_box(const OracleWorld& w, const dyn_query_record& q) {
+    V3 origin = q_origin(q);
+    if (q.kind == DYN_QUERY_RAY) {
+        V3 end = origin + normalize(q_direction(q)) * q.extent;
+        return Aabb{vmin(origin, end), vmax(origin, end)};
+    }
+    if (q.kind == DYN_QUERY_SWEEP) {
+        Aabb a = world_aabb_of(w.shapes, query_shape(q, origin));
+        Aabb b = world_aabb_of(w.shapes, query_shape(q, origin + normalize(q_direction(q)) * q.extent));
+        return Aabb{vmin(a.min, b.min), vmax(a.max, b.max)};
+    }
+    return world_aabb_of(w.shapes, query_shape(q, origin));
+}
+
+// The candidates of one query (grid_index.wgsl:289-388, scene_cast.wgsl:90-134): the colliders with
+// an entry in a cell the query's box covers, level by level; a level under which the box covers
+// more than GRID_WALK_CELLS cells is taken whole, its entries tested against the box. `grid` is the
+// world's index rebuilt from its current states. Sets *spilled when more than QUERY_CANDIDATES
+// entries were gathered (the reference then keeps whichever landed first; here all are kept).
+std::vector<uint32_t> query_candidates(const OracleWorld& grid, const Aabb& box, bool* spilled) {
+    std::vector<uint32_t> out;
+    const float base = grid_base_cell(grid);
+    uint32_t occupied = grid.counters[DYN_COUNTER_GRID_LEVELS] | grid.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
+    const std::vector<uint32_t>& keys = grid.entry_keys;
+    while (occupied != 0u) {
+        const uint32_t level = (uint32_t)__builtin_ctz(occupied);
+        occupied &= occupied - 1u;
+        const float cs = level_cell_size(level, base);
+        const I3 lo = floor_div(box.min, cs), hi = floor_div(box.max, cs);
+        const int64_t sx = (int64_t)hi.x - lo.x + 1, sy = (int64_t)hi.y - lo.y + 1, sz = (int64_t)hi.z - lo.z + 1;
+        const int64_t cells = sx * sy * sz;
+        if (cells <= 0) continue;
+        if (cells > 4096) {
+            auto first = std::lower_bound(keys.begin(), keys.end(), level << DYN_LEVEL_KEY_SHIFT);
+            auto end = std::lower_bound(keys.begin(), keys.end(), (level + 1u) << DYN_LEVEL_KEY_SHIFT);
+            for (auto it = first; it != end; ++it) {
+                const Entry& e = grid.entries[grid.entry_order[it - keys.begin()]];
+                if (aabb_overlaps(e.box, box)) out.push_back(e.info & DYN_ENTRY_INDEX_MASK);
+            }
+        } else {
+            for (int x = lo.x; x <= hi.x; ++x)
+                for (int y = lo.y; y <= hi.y; ++y)
+                    for (int z = lo.z; z <= hi.z; ++z) {
+                        const uint32_t key = cell_key_in(level, I3{x, y, z}, 0u);
+                        auto it = std::lower_bound(keys.begin(), keys.end(), key);
+                        for (; it != keys.end() && *it == key; ++it)
+                            out.push_back(grid.entries[grid.entry_order[it - keys.begin()]].info & DYN_ENTRY_INDEX_MASK);
+                    }
+        }
+    }
+    *spilled = out.size() > DYN_QUERY_CANDIDATES;
+    std::sort(out.begin(), out.end());
+    out.erase(std::unique(out.begin(), out.end()), out.end());
+    return out;
+}
+
+// A batch of scene queries against the world's current states (scene_cast.wgsl:434-533): the grid
+// index is rebuilt from the current states on a copy of the world (the AABB and entry passes of a
+// step, as the reference's query run and dyn_query rebuild it), each query's candidates are walked
+// from it, the hits are ordered by (distance key, collider slot) and at most
+// min(max_hits, QUERY_CANDIDATES) are written from hit_base; count and overflow are set. hit_base is
+// assigned in submission order, as World::submit_query does.
 void orc_query(const OracleWorld* cw, dyn_query_record* queries, uint32_t n, dyn_query_hit_record* hits) {
     const OracleWorld& w = *cw;
+    OracleWorld grid = w;
+    for (uint32_t c : {DYN_COUNTER_GRID_LEVELS, DYN_COUNTER_IMMOVABLE_LEVELS, DYN_COUNTER_GRID_SCALE, DYN_COUNTER_GRID_EXTENT,
+                       DYN_COUNTER_ENTRIES, DYN_COUNTER_IMMOVABLE_ENTRIES, DYN_COUNTER_IMMOVABLE_EMITTED,
+                       DYN_COUNTER_COARSE_ACTIVE, DYN_COUNTER_ENTRY_FAULTS})
+        grid.counters[c] = 0u;
+    grid.body_activity.resize(grid.states.size(), 0u);
+    grid.wake_flags.resize(grid.states.size(), 0u);
+    prepare(grid);
+    emit_entries(grid);
     HullTriangles ht{w.hull_tris.data(), w.hull_tri_ranges.data(), (uint32_t)(w.hull_tri_ranges.size() / 2)};
     uint32_t base = 0;
     for (uint32_t qi = 0; qi < n; ++qi) {
@@ -2304,7 +2371,10 @@ void orc_query(const OracleWorld* cw, dyn_query_record* queries, uint32_t n, dyn
         };
         std::vector<Found> found;
         const bool colliders = (q.filters.targets & DYN_QUERY_TARGET_COLLIDERS) != 0u;
-        for (uint32_t slot = 0; colliders && slot < w.colliders.size(); ++slot) {
+        bool spilled = false;
+        const std::vector<uint32_t> candidates =
+            colliders ? query_candidates(grid, query_world_box(w, q), &spilled) : std::vector<uint32_t>();
+        for (uint32_t slot : candidates) {
             const uint32_t row = w.owners[slot];
             if (row == DYN_NO_BODY) continue;
             const dyn_body_state_record& st = w.states[row];
@@ -2347,7 +2417,7 @@ void orc_query(const OracleWorld* cw, dyn_query_record* queries, uint32_t n, dyn
             hits[q.hit_base + i] = r;
         }
         q.count = emitted;
-        q.overflow = emitted < found.size() ? 1u : 0u;
+        q.overflow = (spilled || emitted < found.size()) ? 1u : 0u;
     }
 }
 

@@ -1,7 +1,8 @@
 """Scene queries on the GPU (dyn_query; query.cuh) against the oracle.
 
-The oracle tests every collider for every query; the library walks the grid cells under the
-query's box, so agreement also checks that the walk finds every collider a test can hit. Compared
+The oracle rebuilds the grid index from the same states and restates the candidate walk over it
+(binary searches in the sorted keys where the library uses its cell table), so agreement checks the
+walk, the tests and the selection together. Compared
 per query: hit_base, count, overflow; per hit: body id and generation, the candidate (collider),
 the triangle, and distance / point / normal within 1e-5 relative + 1e-6 absolute.
 """
