@@ -272,6 +272,9 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     for _ in range(args.warmup):
         world.step(DT)
     world.wait()
+    # the end-to-end run below starts again from this state (World::snapshot / restore), so both
+    # numbers describe the same steps of a pile that keeps getting denser
+    start_state = world.snapshot()
     dist = None
     if world_size > 1:
         import torch.distributed as dist
@@ -321,15 +324,23 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
         moved = stage_bytes(stage, counts, params) * LAUNCHES.get(stage, lambda p: 1)(params)
         if moved > 0 and stage_ms > 0:
             stage_frac[stage] = round(moved / (stage_ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4)
-    # end to end through the C ABI with pinned host buffers
-    e2e_steps = max(3, min(args.steps, 10))
+    # end to end through the C ABI with pinned host buffers, over the same steps as `value`: the world
+    # goes back to the post-warm-up snapshot; one untimed round trip first, then back again
+    e2e_steps = args.steps
     host = torch.empty(bodies * R.BODY_STATE.itemsize, dtype=torch.uint8, pin_memory=True)
     host_out = torch.empty_like(host, pin_memory=True)
     states_in = host.numpy().view(R.BODY_STATE)
     states_out = host_out.numpy().view(R.BODY_STATE)
-    states_in[:] = world.read_states()
     from dynamis_b200._native import lib, ptr
 
+    world.restore(start_state)
+    states_in[:] = world.read_states()
+    world.upload_states(states_in)
+    world.step(DT)
+    world._check(lib.dyn_download_states(world._h, ptr(states_out), bodies))
+    world.restore(start_state)
+    start_state.close()
+    states_in[:] = world.read_states()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         world.upload_states(states_in)

@@ -59,6 +59,9 @@ SIGNATURES = {
     "dyn_set_launch_config": (I32, [P, P]),
     "dyn_get_launch_config": (I32, [P, P]),
     "dyn_autotune": (I32, [P, ctypes.c_float, U32, P, P]),
+    "dyn_snapshot_take": (I32, [P, P]),
+    "dyn_snapshot_restore": (I32, [P, P]),
+    "dyn_snapshot_free": (I32, [P]),
     "dyn_step_kernel_count": (U32, [P]),
     "dyn_stage_count": (U32, []),
     "dyn_stage_name": (ctypes.c_char_p, [U32]),

@@ -143,6 +143,7 @@ struct DeviceState {
     bool stepped = false;
     bool uploaded = false;  // the current scene's records are on the device
     uint32_t graph_kernels = 0;  // kernel nodes in one step's graph
+    uint64_t scene_epoch = 0;    // scene uploads so far (a snapshot belongs to one scene)
     uint32_t sms = 148;          // multiprocessors of the device (read when the device state is made)
     dyn_launch_config launch{16u, 128u, 6u, 8u};  // dyn_set_launch_config / dyn_autotune
     bool tuning = false;         // dyn_autotune is running trials: the contact stream keeps its layout
@@ -408,6 +409,7 @@ dyn_status upload_joints(dyn_world* w) {
     dw.jcount = dw.jgroup_count = dw.jfilter_count = 0;
     release_graphs(d);
     w->joints_dirty = false;
+    d->scene_epoch += 1;  // the constraint set is part of what a snapshot restores
     const uint32_t m = (uint32_t)w->joint_descs.size();
     if (m == 0) return DYN_OK;
     const JointPlan& plan = w->joint_plan;
@@ -586,6 +588,7 @@ dyn_status upload_scene(dyn_world* w) {
     d->parity = 0;
     d->stepped = false;
     d->uploaded = true;
+    d->scene_epoch += 1;
     release_graphs(d);
     return DYN_OK;
 }
@@ -1480,7 +1483,9 @@ static std::vector<CheckpointPart> checkpoint_parts(DeviceState* d) {
             {arc.la, 4 * C * sizeof(float4)},     {arc.lb, 4 * C * sizeof(float4)},  {arc.acc, 4 * C * sizeof(float4)},
             {arc.pos, 4 * C * sizeof(float4)},
             {d->rest_ids[d->parity], (size_t)d->rest_cap * sizeof(uint4)},
-            {d->rest_slots[d->parity], (size_t)d->rest_cap * sizeof(uint2)}};
+            {d->rest_slots[d->parity], (size_t)d->rest_cap * sizeof(uint2)},
+            // the joints' accumulated impulses and broken flags (an empty part without joints)
+            {dw.jruntime, (size_t)dw.jcount * sizeof(dyn_constraint_runtime_record)}};
 }
 static size_t checkpoint_bytes(const std::vector<CheckpointPart>& parts) {
     size_t bytes = 0;
@@ -1503,7 +1508,7 @@ static dyn_status save_checkpoint(dyn_world* w, Checkpoint* c) {
     }
     char* at = static_cast<char*>(c->base);
     for (const CheckpointPart& part : parts) {
-        DYN_CUDA(cudaMemcpyAsync(at, part.ptr, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
+        if (part.bytes) DYN_CUDA(cudaMemcpyAsync(at, part.ptr, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
         at += (part.bytes + 255u) & ~(size_t)255u;
     }
     c->parity = d->parity;
@@ -1515,7 +1520,7 @@ static dyn_status restore_checkpoint(dyn_world* w, const Checkpoint& c) {
     d->parity = c.parity;  // before listing the parts: the archived set follows the parity
     const char* at = static_cast<const char*>(c.base);
     for (const CheckpointPart& part : checkpoint_parts(d)) {
-        DYN_CUDA(cudaMemcpyAsync(part.ptr, at, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
+        if (part.bytes) DYN_CUDA(cudaMemcpyAsync(part.ptr, at, part.bytes, cudaMemcpyDeviceToDevice, d->stream));
         at += (part.bytes + 255u) & ~(size_t)255u;
     }
     return DYN_OK;
@@ -2526,6 +2531,89 @@ DYN_API dyn_status dyn_autotune(dyn_world* w, float dt, uint32_t steps, dyn_laun
     if (restored) return restored;
     if (best) *best = top;
     if (best_ms) *best_ms = top_ms;
+    return DYN_OK;
+}
+
+// World::snapshot / World::restore (crates/dynamis-world/src/snapshot.rs:64-90): the simulated state
+// of the world as it is once the queued steps finish (every body row and cold body field, the
+// archived contacts the next step warm-starts from, the frozen contacts, the joints' runtime, the
+// counters and control words, the contact-set parity), kept on the device, plus the body commands
+// queued for the next step and the step clock. Restoring puts it back, so the steps that follow
+// repeat the ones that followed the snapshot bit for bit. A snapshot belongs to the world it was
+// taken from and to its scene: after a spawn, a removal, a constraint change or a contact-stream
+// widening it is refused (DYN_ERR_INVALID); the reference carries its whole scene in the snapshot
+// instead. Observations are abandoned on restore, as the reference's are.
+struct dyn_snapshot {
+    dyn_world* world = nullptr;
+    dyn::DeviceState* dev = nullptr;
+    uint64_t scene_epoch = 0;
+    uint64_t steps_taken = 0;
+    dyn::Checkpoint state;
+    std::vector<uint32_t> edit_ids;
+    std::vector<dyn_body_edit_record> edits;
+};
+
+DYN_API dyn_status dyn_snapshot_take(dyn_world* w, dyn_snapshot** out) {
+    if (!w || !out) return DYN_ERR_INVALID;
+    *out = nullptr;
+    if (!w->dev || !w->dev->uploaded || (w->rows_dirty && !w->raw_rows) || w->scene_dirty || w->joints_dirty)
+        return fail(w, DYN_ERR_INVALID, "dyn_snapshot_take: step the world (its current scene) once first");
+    DeviceState* d = w->dev;
+    if (d->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_snapshot_take: a tape is recording");
+    DYN_CUDA(cudaSetDevice(w->device));
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    dyn_snapshot* snap = new dyn_snapshot();
+    if (dyn_status st = save_checkpoint(w, &snap->state)) {
+        delete snap;
+        return st;
+    }
+    if (cudaStreamSynchronize(d->stream) != cudaSuccess) {
+        free_checkpoint(&snap->state);
+        delete snap;
+        return fail(w, DYN_ERR_CUDA, "dyn_snapshot_take: the copies failed");
+    }
+    snap->world = w;
+    snap->dev = d;
+    snap->scene_epoch = d->scene_epoch;
+    snap->steps_taken = w->steps_taken;
+    snap->edit_ids = w->edit_ids;
+    snap->edits = w->edits;
+    *out = snap;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_snapshot_restore(dyn_world* w, const dyn_snapshot* snap) {
+    if (!w || !snap) return DYN_ERR_INVALID;
+    DeviceState* d = w->dev;
+    if (snap->world != w || snap->dev != d || !d || d->scene_epoch != snap->scene_epoch || w->scene_dirty || w->joints_dirty ||
+        (w->rows_dirty && !w->raw_rows))
+        return fail(w, DYN_ERR_INVALID, "dyn_snapshot_restore: the snapshot belongs to another world or scene");
+    if (d->tape.active) return fail(w, DYN_ERR_INVALID, "dyn_snapshot_restore: a tape is recording");
+    if (checkpoint_bytes(checkpoint_parts(d)) != snap->state.bytes)
+        return fail(w, DYN_ERR_INVALID, "dyn_snapshot_restore: the contact stream grew since the snapshot");
+    DYN_CUDA(cudaSetDevice(w->device));
+    if (dyn_status st = restore_checkpoint(w, snap->state)) return st;
+    DYN_CUDA(cudaStreamSynchronize(d->stream));
+    for (uint32_t i = 0; i < kStepsInFlight; ++i) d->inflight_used[i] = false;
+    w->edit_ids = snap->edit_ids;
+    w->edits = snap->edits;
+    w->steps_taken = snap->steps_taken;
+    Observer& o = w->observer;
+    for (ObservationSlot& slot : o.slots) {
+        slot.pending = false;
+        slot.ready = false;
+    }
+    o.latest = -1;
+    return DYN_OK;
+}
+
+DYN_API dyn_status dyn_snapshot_free(dyn_snapshot* snap) {
+    if (!snap) return DYN_OK;
+    if (snap->state.base) {
+        cudaFree(snap->state.base);
+        snap->state.base = nullptr;
+    }
+    delete snap;
     return DYN_OK;
 }
 

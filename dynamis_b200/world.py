@@ -278,6 +278,16 @@ class World:
         self._check(lib.dyn_autotune(self._h, float(dt), int(steps), ptr(c), ctypes.byref(ms)))
         return {k: int(c[k][0]) for k in R.LAUNCH_CONFIG.names}, ms.value
 
+    def snapshot(self) -> "Snapshot":
+        """World::snapshot: the simulated state once the queued steps finish (dyn_snapshot_take)."""
+        handle = ctypes.c_void_p()
+        self._check(lib.dyn_snapshot_take(self._h, ctypes.byref(handle)))
+        return Snapshot(handle)
+
+    def restore(self, snapshot: "Snapshot") -> None:
+        """World::restore: back to the snapshot's state; later steps repeat the ones that followed it."""
+        self._check(lib.dyn_snapshot_restore(self._h, snapshot._h))
+
     def set_solver_guard(self, flags: int) -> None:
         """dyn_set_solver_guard: SOLVER_GUARD_ROW_MASS keeps every contact block's Jacobi iteration
         convergent where the reference's manifold row masses would let it diverge; 0 (the default)
@@ -455,3 +465,21 @@ class World:
 
 
 __all__ = ["World", "DynamisError", "default_config"]
+
+
+class Snapshot:
+    """A world's device-side snapshot (dyn_snapshot); freed when closed or collected."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+
+    def close(self) -> None:
+        if self._h:
+            lib.dyn_snapshot_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

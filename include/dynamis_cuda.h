@@ -354,6 +354,19 @@ DYN_API dyn_status dyn_get_launch_config(const dyn_world* world, dyn_launch_conf
  * recording and no queued body edits. Synchronises the world's stream. */
 DYN_API dyn_status dyn_autotune(dyn_world* world, float dt, uint32_t steps, dyn_launch_config* best, float* best_ms);
 
+/* World::snapshot / World::restore (crates/dynamis-world/src/snapshot.rs:64-90). dyn_snapshot_take
+ * waits for the queued steps and copies the world's simulated state on the device (body rows and
+ * cold fields, the archived contacts the next step warm-starts from, the frozen contacts, the
+ * joints' runtime, counters), with the queued body commands and the step clock. dyn_snapshot_restore
+ * puts it back, after which the steps repeat the ones that followed the snapshot bit for bit; it
+ * abandons observations. A snapshot is tied to its world and scene: after a spawn, a removal, a
+ * constraint change or a contact-stream widening, restore returns DYN_ERR_INVALID. Both are refused
+ * while a tape records. The caller frees a snapshot with dyn_snapshot_free. */
+typedef struct dyn_snapshot dyn_snapshot;
+DYN_API dyn_status dyn_snapshot_take(dyn_world* world, dyn_snapshot** out);
+DYN_API dyn_status dyn_snapshot_restore(dyn_world* world, const dyn_snapshot* snapshot);
+DYN_API dyn_status dyn_snapshot_free(dyn_snapshot* snapshot);
+
 /* Solver guards, no counterpart in the reference (0, the default, is the reference's solver).
  * DYN_SOLVER_GUARD_ROW_MASS: the reference solves a contact's points together against manifold row
  * masses (solver_contact_block.wgsl:14-29, manifold_row_mass), and for some manifolds (a tilted box

@@ -12,6 +12,12 @@ pub use dynamis_abi::{
     ConstraintRuntimeRecord, ContactRecord, QueryHitRecord, QueryRecord, StepParamsRecord,
 };
 
+/// An opaque world snapshot (dyn_snapshot).
+#[repr(C)]
+pub struct DynSnapshot {
+    _private: [u8; 0],
+}
+
 /// An opaque world handle (dyn_world).
 #[repr(C)]
 pub struct DynWorld {
@@ -229,6 +235,9 @@ extern "C" {
     pub fn dyn_set_launch_config(world: *mut DynWorld, config: *const DynLaunchConfig) -> DynStatus;
     pub fn dyn_get_launch_config(world: *const DynWorld, out: *mut DynLaunchConfig) -> DynStatus;
     pub fn dyn_autotune(world: *mut DynWorld, dt: f32, steps: u32, best: *mut DynLaunchConfig, best_ms: *mut f32) -> DynStatus;
+    pub fn dyn_snapshot_take(world: *mut DynWorld, out: *mut *mut DynSnapshot) -> DynStatus;
+    pub fn dyn_snapshot_restore(world: *mut DynWorld, snapshot: *const DynSnapshot) -> DynStatus;
+    pub fn dyn_snapshot_free(snapshot: *mut DynSnapshot) -> DynStatus;
     pub fn dyn_set_solver_guard(world: *mut DynWorld, flags: u32) -> DynStatus;
     pub fn dyn_set_ccd(world: *mut DynWorld, body_id: u32, enabled: i32) -> DynStatus;
     pub fn dyn_clear_device_status(world: *mut DynWorld) -> DynStatus;
