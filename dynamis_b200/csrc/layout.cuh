@@ -74,6 +74,29 @@ enum Ctl : uint32_t {
     CTL_COUNT = 32
 };
 
+// The grid index in three sorted runs (grid_resting_*.wgsl, immovable_entries.wgsl): the entries of
+// awake movable colliders, emitted and sorted every step; the immovable colliders' and the resting
+// (movable, asleep) colliders' entries, kept sorted across steps and emitted again only when a
+// member, its box or the grid resolution changed. Every collider owns the entry slots
+// [8 * collider, 8 * collider + 8), so a kept run's entries stay where it left them; the step merges
+// the three runs into one sorted list for the pair and cell kernels.
+enum GridRun : uint32_t { RUN_AWAKE = 0, RUN_IMMOVABLE = 1, RUN_RESTING = 2, RUN_NONE = 3 };
+// Words of the kept runs (`DeviceWorld::held`): outside the control words and counters, because a
+// checkpoint restores those while the runs stay as the last step left them.
+enum Held : uint32_t {
+    HELD_STALE = 0,        // per step: bit r set when kept run r must be emitted again
+    HELD_AWAKE = 1,        // entries of the awake run this step
+    HELD_IMMOVABLE = 2,    // entries in the kept immovable run
+    HELD_RESTING = 3,      // entries in the kept resting run
+    HELD_BASE = 4,         // bits of the base cell size the kept runs were emitted at
+    HELD_SCAN_IMMOVABLE = 5,  // per step: colliders the immovable run's scan covers (0 when it is kept)
+    HELD_SCAN_RESTING = 6,
+    HELD_SORT_IMMOVABLE = 7,  // per step: entries the immovable run's sort covers (0 when it is kept)
+    HELD_SORT_RESTING = 8,
+    HELD_SCRATCH = 9,      // a scan total nothing reads
+    HELD_COUNT = 16
+};
+
 // Where a taped step's kernels write the adjoint's snapshots (the tape of adjoint.cuh, slot *slot);
 // every pointer is null outside taped steps. Layouts: relay [slot][4c]; vel [slot][K*I][2n]
 // (velocities, then angular velocities, at each velocity iteration's start); acc [slot][K*I][4c]
@@ -155,7 +178,14 @@ struct DeviceWorld {
     uint32_t* eval;
     uint32_t* ekey_alt;
     uint32_t* eval_alt;
-    float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits
+    float4* entries;  // [2e]: min.xyz + group bits, max.xyz + info bits; collider i's at slots [8i, 8i + 8)
+    uint32_t* c_run;    // [k] per step: the GridRun a collider's entries belong to
+    uint32_t* c_held;   // [k] the kept run whose entries the collider's slots hold (RUN_AWAKE: none)
+    uint32_t* run_count;   // [3k] entries per collider and run this step emits (the scans' input)
+    uint32_t* run_offset;  // [3k] their exclusive scans
+    uint32_t* run_key;     // [3e] the runs' cell keys, run r at [r * e_cap], sorted
+    uint32_t* run_val;     // [3e] the runs' entry slots
+    uint32_t* held;        // [HELD_COUNT]
     uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
     uint32_t cell_bits;
     uint32_t* spill;  // host-mapped: [0] unused, [1] pairs attempted, [2] pairs refused (left by a refusing step),

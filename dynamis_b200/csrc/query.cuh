@@ -553,7 +553,8 @@ __global__ void __launch_bounds__(kQueryThreads) k_scene_query(DeviceWorld w, dy
         const uint32_t bits = cell_table_bits(w, live);
         const bool table_overflow = w.ctl[CTL_CELL_OVERFLOW] != 0u;
         const bool wants_colliders = (q.filters.targets & DYN_QUERY_TARGET_COLLIDERS) != 0u;
-        uint32_t occupied = wants_colliders ? (w.counters[DYN_COUNTER_GRID_LEVELS] | w.counters[DYN_COUNTER_IMMOVABLE_LEVELS]) : 0u;
+        uint32_t occupied = wants_colliders ? (w.counters[DYN_COUNTER_GRID_LEVELS] | w.counters[DYN_COUNTER_RESTING_LEVELS] |
+                                                       w.counters[DYN_COUNTER_IMMOVABLE_LEVELS]) : 0u;
         while (occupied != 0u) {
             const uint32_t level = (uint32_t)__ffs(occupied) - 1u;
             occupied &= occupied - 1u;

@@ -51,6 +51,7 @@ __global__ void k_reset(DeviceWorld w) {
         if (i == DYN_COUNTER_ARCHIVED || i == DYN_COUNTER_STEP || i == DYN_COUNTER_RESTING) continue;
         w.counters[i] = 0u;
     }
+    if (threadIdx.x == 0) w.held[HELD_STALE] = 0u;
     for (uint32_t i = threadIdx.x; i < CTL_COUNT; i += blockDim.x) {
         if (i == CTL_ARCHIVED || i == CTL_STATUS || i == CTL_RESTING) continue;
         w.ctl[i] = 0u;
@@ -303,12 +304,38 @@ __device__ __forceinline__ uint32_t shape_levels(f3 mn, f3 mx, float base) {
     return level;
 }
 
-// collider_emit.wgsl:6-29 (level, cell budget) for every collider: entry counts for the scan.
+// The run a live collider's entries belong to this step (grid_resting_entries.wgsl:11-19: a
+// movable body that is not active goes to the resting run; immovable_entries.wgsl: a body that does
+// not move to the immovable run).
+__device__ __forceinline__ uint32_t grid_run(bool mv, bool awake) {
+    return !mv ? RUN_IMMOVABLE : (awake ? RUN_AWAKE : RUN_RESTING);
+}
+// The info word of collider i's entry at cell offset `offset` (collider_emit.wgsl:31-63).
+__device__ __forceinline__ uint32_t entry_info(uint32_t i, uint32_t offset, bool mv, bool awake) {
+    uint32_t info = i | (offset << DYN_ENTRY_CELL_SHIFT) | (DYN_ENTRY_KIND_COLLIDER << DYN_ENTRY_KIND_SHIFT);
+    if (mv && awake) info |= DYN_ENTRY_AWAKE;
+    if (mv) info |= DYN_ENTRY_MOBILE;
+    if (offset == 0u) info |= DYN_ENTRY_PRIMARY;
+    return info;
+}
+__device__ __forceinline__ bool same_bits(f3 a, float4 b) {
+    return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+           __float_as_uint(a.z) == __float_as_uint(b.z);
+}
+
+// collider_emit.wgsl:6-29 (level, cell budget) for every collider, and the counters of the three
+// runs. A step (kStep) also sorts each collider into its run and checks that a kept run still holds
+// the entries its members would emit now: the same members, each with the box, owner and info its
+// first slot holds (the rest of its slots follow from them at an unchanged resolution, which the
+// gate checks). A collider that left a kept run, joined one, or whose box moved marks that run
+// stale. A query (not kStep) counts every collider's entries for one compact scan.
+template <bool kStep>
 __global__ void k_entry_count(DeviceWorld w) {
     float base = base_cell(w);
+    uint32_t stale = 0u;
     GRID_STRIDE(i, w.k) {
         uint32_t owner = w.c_owner[i];
-        uint32_t emitted = 0;
+        uint32_t emitted = 0, run = RUN_NONE;
         if (owner != DYN_NO_BODY) {
             float4 a = w.aabb[2 * i], b = w.aabb[2 * i + 1];
             f3 mn = xyz(a), mx = xyz(b);
@@ -317,37 +344,106 @@ __global__ void k_entry_count(DeviceWorld w) {
             const BodyHot& h = w.hot[owner];
             bool mv = moves(h.pos.w, h.aux.y);
             bool awake = w.activity[owner] != 0u || w.wake_flags[owner] != 0u;
-            // aggregated updates need one target per coalesced group: branch first
-            if (mv) {
-                or_counter(&w.counters[DYN_COUNTER_GRID_LEVELS], 1u << level);
-            } else {
-                or_counter(&w.counters[DYN_COUNTER_IMMOVABLE_LEVELS], 1u << level);
-            }
+            run = grid_run(mv, awake);
             float cs = level_size(level, base);
             I3 lo = floor_div(mn, cs), hi = floor_div(mx, cs);
             uint32_t count = (uint32_t)(hi.x - lo.x + 1) * (uint32_t)(hi.y - lo.y + 1) * (uint32_t)(hi.z - lo.z + 1);
             emitted = min(count, DYN_MAX_CELLS_PER_COLLIDER);
             if (count > emitted) add_counter(&w.counters[DYN_COUNTER_ENTRY_FAULTS], count - emitted);
             if (level > 0u && awake) add_counter(&w.counters[DYN_COUNTER_COARSE_ACTIVE], 1u);
-            if (mv) {
+            // aggregated updates need one target per coalesced group: branch first
+            if (run == RUN_AWAKE) {
+                or_counter(&w.counters[DYN_COUNTER_GRID_LEVELS], 1u << level);
                 add_counter(&w.counters[DYN_COUNTER_ENTRIES], emitted);
+            } else if (run == RUN_RESTING) {
+                or_counter(&w.counters[DYN_COUNTER_RESTING_LEVELS], 1u << level);
+                add_counter(&w.counters[DYN_COUNTER_RESTING_ENTRIES], emitted);
             } else {
+                or_counter(&w.counters[DYN_COUNTER_IMMOVABLE_LEVELS], 1u << level);
                 add_counter(&w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES], emitted);
-                add_counter(&w.counters[DYN_COUNTER_IMMOVABLE_EMITTED], emitted);
+            }
+            if (kStep && run != RUN_AWAKE) {
+                const float4 first_lo = w.entries[16u * i], first_hi = w.entries[16u * i + 1u];
+                const bool kept = w.c_held[i] == run && same_bits(mn, first_lo) && same_bits(mx, first_hi) &&
+                                  __float_as_uint(first_lo.w) == owner &&
+                                  __float_as_uint(first_hi.w) == entry_info(i, 0u, mv, false);
+                if (!kept) stale |= 1u << run;
             }
         }
-        w.entry_count[i] = emitted;
+        if (kStep) {
+            const uint32_t held = w.c_held[i];
+            if (held != RUN_AWAKE && held != run) stale |= 1u << held;
+            w.c_run[i] = run;
+            w.run_count[i] = run == RUN_AWAKE ? emitted : 0u;
+            w.run_count[w.k + i] = run == RUN_IMMOVABLE ? emitted : 0u;
+            w.run_count[2u * w.k + i] = run == RUN_RESTING ? emitted : 0u;
+        } else {
+            w.entry_count[i] = emitted;
+        }
+    }
+    if (kStep) {
+        stale = __reduce_or_sync(0xFFFFFFFFu, stale);
+        if ((threadIdx.x & 31u) == 0u && stale != 0u) atomicOr(&w.held[HELD_STALE], stale);
     }
 }
 
-// collider_emit.wgsl:31-63 at the scanned slots (collider order): key, payload = slot, GridEntry.
+// grid_resting_gate.wgsl / grid_resting_commit.wgsl in one thread: which kept runs this step emits
+// again (a stale member, or a grid resolution other than the one they were emitted at), the sizes
+// and counts the scans, sorts and merge read, and the counters of what was derived. A kept run has
+// exactly the entries its members count now, rebuilt or not.
+__global__ void k_grid_gate(DeviceWorld w) {
+    if (threadIdx.x != 0u) return;
+    uint32_t stale = w.held[HELD_STALE];
+    const uint32_t base = __float_as_uint(base_cell(w));
+    if (base != w.held[HELD_BASE]) stale |= (1u << RUN_IMMOVABLE) | (1u << RUN_RESTING);
+    const bool immovable = (stale >> RUN_IMMOVABLE) & 1u, resting = (stale >> RUN_RESTING) & 1u;
+    const uint32_t ni = w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES], nr = w.counters[DYN_COUNTER_RESTING_ENTRIES];
+    w.held[HELD_STALE] = stale;
+    w.held[HELD_BASE] = base;
+    w.held[HELD_IMMOVABLE] = ni;
+    w.held[HELD_RESTING] = nr;
+    w.held[HELD_SCAN_IMMOVABLE] = immovable ? w.k : 0u;
+    w.held[HELD_SCAN_RESTING] = resting ? w.k : 0u;
+    w.held[HELD_SORT_IMMOVABLE] = immovable ? ni : 0u;
+    w.held[HELD_SORT_RESTING] = resting ? nr : 0u;
+    w.counters[DYN_COUNTER_IMMOVABLE_EMITTED] = immovable ? ni : 0u;
+    w.counters[DYN_COUNTER_RESTING_REBUILD] = resting ? 1u : 0u;
+    w.counters[DYN_COUNTER_RESTING_SORT] = resting ? nr : 0u;
+    w.ctl[CTL_ENTRIES] = min(w.held[HELD_AWAKE] + ni + nr, w.e_cap);
+}
+
+// collider_emit.wgsl:31-63 for the colliders whose entries this launch writes, in collider order at
+// their scanned key positions. A step writes the awake run and every kept run the gate marked
+// stale, each entry into its collider's own slots (8 * collider + ordinal), and records which kept
+// run a collider's slots now hold. A query writes every collider's entries compactly.
+template <bool kStep>
 __global__ void k_entry_emit(DeviceWorld w) {
     float base = base_cell(w);
+    const uint32_t stale = kStep ? w.held[HELD_STALE] : 0u;
     GRID_STRIDE(i, w.k) {
-        uint32_t emitted = w.entry_count[i];
+        uint32_t emitted, first;
+        uint32_t* keys;
+        uint32_t* vals;
+        if (kStep) {
+            const uint32_t run = w.c_run[i];
+            if (run == RUN_NONE) {
+                w.c_held[i] = RUN_AWAKE;
+                continue;
+            }
+            if (run != RUN_AWAKE && ((stale >> run) & 1u) == 0u) continue;  // kept: its slots hold these entries
+            w.c_held[i] = run;
+            emitted = w.run_count[run * w.k + i];
+            first = w.run_offset[run * w.k + i];
+            keys = w.run_key + (size_t)run * w.e_cap;
+            vals = w.run_val + (size_t)run * w.e_cap;
+        } else {
+            emitted = w.entry_count[i];
+            first = w.entry_offset[i];
+            keys = w.ekey;
+            vals = w.eval;
+        }
         if (emitted == 0u) continue;
         uint32_t owner = w.c_owner[i];
-        uint32_t first = w.entry_offset[i];
         float4 a = w.aabb[2 * i], b = w.aabb[2 * i + 1];
         f3 mn = xyz(a), mx = xyz(b);
         uint32_t level = w.c_level[i];
@@ -362,15 +458,61 @@ __global__ void k_entry_emit(DeviceWorld w) {
         for (uint32_t ordinal = 0; ordinal < emitted; ++ordinal) {
             I3 c = I3{lo.x + (int)(ordinal / rows), lo.y + (int)((ordinal / sz) % sy), lo.z + (int)(ordinal % sz)};
             uint32_t offset = (uint32_t)(c.x - lo.x) | ((uint32_t)(c.y - lo.y) << 1) | ((uint32_t)(c.z - lo.z) << 2);
-            uint32_t info = i | (offset << DYN_ENTRY_CELL_SHIFT) | (DYN_ENTRY_KIND_COLLIDER << DYN_ENTRY_KIND_SHIFT);
-            if (mv && awake) info |= DYN_ENTRY_AWAKE;
-            if (mv) info |= DYN_ENTRY_MOBILE;
-            if (offset == 0u) info |= DYN_ENTRY_PRIMARY;
-            uint32_t slot = first + ordinal;
-            w.ekey[slot] = cell_key_in(level, c, world);
-            w.eval[slot] = slot;
+            uint32_t slot = kStep ? 8u * i + ordinal : first + ordinal;
+            keys[first + ordinal] = cell_key_in(level, c, world);
+            vals[first + ordinal] = slot;
             w.entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(owner));
-            w.entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(info));
+            w.entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(entry_info(i, offset, mv, awake)));
+        }
+    }
+}
+
+// Entries of a run sorted by (cell key, slot) that come before (key, slot).
+__device__ __forceinline__ uint32_t run_rank(const uint32_t* keys, const uint32_t* vals, uint32_t n, uint32_t key,
+                                             uint32_t val) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t k = __ldg(keys + mid);
+        if (k < key || (k == key && __ldg(vals + mid) < val)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The three sorted runs merged into the entry list the cell table and the pair kernels read. Each
+// run is sorted by cell key and, within a key, by slot (its keys were scanned in collider and cell
+// order and the sort is stable), so an entry's place is its index in its run plus the entries of
+// the other runs before (key, slot): the list one sort of every entry would give.
+__global__ void k_entry_merge(DeviceWorld w) {
+    const uint32_t na = w.held[HELD_AWAKE], ni = w.held[HELD_IMMOVABLE], nr = w.held[HELD_RESTING];
+    const uint32_t total = min(na + ni + nr, w.e_cap);
+    const uint32_t* ka = w.run_key;
+    const uint32_t* va = w.run_val;
+    const uint32_t* ki = w.run_key + w.e_cap;
+    const uint32_t* vi = w.run_val + w.e_cap;
+    const uint32_t* kr = w.run_key + 2u * (size_t)w.e_cap;
+    const uint32_t* vr = w.run_val + 2u * (size_t)w.e_cap;
+    GRID_STRIDE(t, total) {
+        uint32_t key, val, pos;
+        if (t < na) {
+            key = __ldg(ka + t);
+            val = __ldg(va + t);
+            pos = t + run_rank(ki, vi, ni, key, val) + run_rank(kr, vr, nr, key, val);
+        } else if (t < na + ni) {
+            const uint32_t j = t - na;
+            key = __ldg(ki + j);
+            val = __ldg(vi + j);
+            pos = j + run_rank(ka, va, na, key, val) + run_rank(kr, vr, nr, key, val);
+        } else {
+            const uint32_t j = t - na - ni;
+            key = __ldg(kr + j);
+            val = __ldg(vr + j);
+            pos = j + run_rank(ka, va, na, key, val) + run_rank(ki, vi, ni, key, val);
+        }
+        if (pos < w.e_cap) {
+            w.ekey[pos] = key;
+            w.eval[pos] = val;
         }
     }
 }
@@ -503,9 +645,8 @@ __global__ void __launch_bounds__(128) k_pairs_coarse(DeviceWorld w) {
     const uint32_t bits = cell_table_bits(w, live);
     const bool overflow = w.ctl[CTL_CELL_OVERFLOW] != 0u;
     GRID_STRIDE(i, w.k) {
-        if (w.entry_count[i] == 0u) continue;
-        const uint32_t node = w.entry_offset[i];
-        if (node >= live) continue;
+        if (w.c_run[i] == RUN_NONE) continue;
+        const uint32_t node = 8u * i;  // the first of the collider's slots: its primary entry
         GEntry e = load_entry(w, node);
         if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;
         if ((e.info & DYN_ENTRY_PRIMARY) == 0u) continue;

@@ -107,6 +107,10 @@ struct DeviceState {
     // a query batch's records and hits on the device (dyn_query), grown as batches need
     dyn_query_record* query_buf = nullptr;
     dyn_query_hit_record* hit_buf = nullptr;
+    // a query's own grid: its entries and its counters and control words, so that a query between
+    // steps leaves the step's kept grid runs and counters as they were
+    float4* query_entries = nullptr;
+    uint32_t* query_words = nullptr;
     uint32_t query_cap = 0, hit_cap = 0;
     // sort and scan scratch
     uint32_t* hist = nullptr;          // 8 x 256
@@ -314,6 +318,13 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.ekey_alt, E);
         A(dw.eval_alt, E);
         A(dw.entries, 2 * (size_t)E);
+        A(dw.c_run, K);
+        A(dw.c_held, K);
+        A(dw.run_count, 3 * (size_t)K);
+        A(dw.run_offset, 3 * (size_t)K);
+        A(dw.run_key, 3 * (size_t)E);
+        A(dw.run_val, 3 * (size_t)E);
+        A(dw.held, HELD_COUNT);
         dw.cell_bits = 10u;
         while (dw.cell_bits < 31u && ((size_t)1 << dw.cell_bits) < 2 * (size_t)E) ++dw.cell_bits;
         A(dw.cell_table, (size_t)1 << dw.cell_bits);
@@ -582,6 +593,9 @@ dyn_status upload_scene(dyn_world* w) {
     DYN_CUDA(cudaMemsetAsync(dw.ctl + CTL_RESTING + 1, 0, (CTL_COUNT - CTL_RESTING - 1) * 4, s));
     DYN_CUDA(cudaMemsetAsync(dw.counters, 0, DYN_COUNTER_RESTING * 4, s));
     DYN_CUDA(cudaMemsetAsync(dw.counters + DYN_COUNTER_RESTING + 1, 0, (64 - DYN_COUNTER_RESTING - 1) * 4, s));
+    // colliders may have moved between slots: no kept grid run survives a scene upload
+    DYN_CUDA(cudaMemsetAsync(dw.c_held, 0, (size_t)d->k_cap * 4, s));
+    DYN_CUDA(cudaMemsetAsync(dw.held, 0, HELD_COUNT * 4, s));
     DYN_CUDA(cudaStreamSynchronize(s));
     if ((st = upload_joints(w))) return st;
     w->scene_dirty = false;
@@ -741,11 +755,24 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     mark(ST_AABB);
     k_aabb<<<blocks_for(d, K, 128), 128, 0, s>>>(dw, p);
     mark(ST_ENTRIES);
-    k_entry_count<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
-    record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, std::max(dw.k, 1u), dw.ctl + CTL_ENTRIES);
-    k_entry_emit<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    // the awake run every step; the kept runs (immovable, resting) only when the gate finds them
+    // stale, their scans and sorts otherwise covering nothing
+    k_entry_count<true><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    record_scan(d, s, dw.run_count, dw.run_offset, nullptr, dw.k, K, dw.held + HELD_AWAKE);
+    k_grid_gate<<<1, 32, 0, s>>>(dw);
+    record_scan(d, s, dw.run_count + dw.k, dw.run_offset + dw.k, dw.held + HELD_SCAN_IMMOVABLE, 0, K,
+                dw.held + HELD_SCRATCH);
+    record_scan(d, s, dw.run_count + 2 * (size_t)dw.k, dw.run_offset + 2 * (size_t)dw.k, dw.held + HELD_SCAN_RESTING, 0, K,
+                dw.held + HELD_SCRATCH);
+    k_entry_emit<true><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     mark(ST_ENTRY_SORT);
-    record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
+    for (uint32_t run = 0; run < 3; ++run) {
+        const uint32_t* count = dw.held + (run == RUN_AWAKE ? HELD_AWAKE
+                                           : run == RUN_IMMOVABLE ? HELD_SORT_IMMOVABLE : HELD_SORT_RESTING);
+        record_sort(d, s, dw.run_key + (size_t)run * E, nullptr, dw.run_val + (size_t)run * E, dw.ekey_alt, nullptr,
+                    dw.eval_alt, count, 0, E, 4, 0);
+    }
+    k_entry_merge<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);
     mark(ST_PAIRS);
     k_cell_clear<<<blocks_for(d, 1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
     k_cell_insert<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);
@@ -1112,6 +1139,8 @@ void destroy_device(dyn_world* w) {
     if (d->edit_run_buffer) cudaFree(d->edit_run_buffer);
     if (d->query_buf) cudaFree(d->query_buf);
     if (d->hit_buf) cudaFree(d->hit_buf);
+    if (d->query_entries) cudaFree(d->query_entries);
+    if (d->query_words) cudaFree(d->query_words);
     for (uint32_t* p : {d->sort_alt0, d->sort_alt1, d->sort_alt2}) {
         if (p) cudaFree(p);
     }
@@ -2177,10 +2206,10 @@ DYN_API dyn_status dyn_debug_entries(dyn_world* w, uint32_t* keys, uint32_t* inf
     if (!keys) return DYN_OK;
     uint32_t m = std::min(cap, e);
     std::vector<uint32_t> order(m);
-    std::vector<float4> ent(2 * (size_t)e);
+    std::vector<float4> ent(2 * (size_t)dw.e_cap);  // slots are the colliders' windows, up to e_cap
     DYN_CUDA(cudaMemcpy(keys, dw.ekey, m * 4, cudaMemcpyDeviceToHost));
     DYN_CUDA(cudaMemcpy(order.data(), dw.eval, m * 4, cudaMemcpyDeviceToHost));
-    DYN_CUDA(cudaMemcpy(ent.data(), dw.entries, 2 * (size_t)e * sizeof(float4), cudaMemcpyDeviceToHost));
+    DYN_CUDA(cudaMemcpy(ent.data(), dw.entries, ent.size() * sizeof(float4), cudaMemcpyDeviceToHost));
     if (infos) {
         for (uint32_t i = 0; i < m; ++i) {
             float f = ent[2 * (size_t)order[i] + 1].w;
@@ -2303,17 +2332,6 @@ DYN_API dyn_status dyn_debug_islands(dyn_world* w, uint32_t* out, uint32_t cap, 
     return DYN_OK;
 }
 
-// The grid counters a query's index rebuilds (the step's other counters stay as the step left them).
-static __global__ void k_query_index_reset(DeviceWorld w) {
-    if (threadIdx.x != 0) return;
-    const uint32_t counters[] = {DYN_COUNTER_GRID_LEVELS, DYN_COUNTER_IMMOVABLE_LEVELS, DYN_COUNTER_GRID_SCALE,
-                                 DYN_COUNTER_GRID_EXTENT, DYN_COUNTER_ENTRIES, DYN_COUNTER_IMMOVABLE_ENTRIES,
-                                 DYN_COUNTER_IMMOVABLE_EMITTED, DYN_COUNTER_COARSE_ACTIVE, DYN_COUNTER_ENTRY_FAULTS};
-    for (uint32_t c : counters) w.counters[c] = 0u;
-    w.ctl[CTL_ENTRIES] = 0u;
-    w.ctl[CTL_CELL_OVERFLOW] = 0u;
-}
-
 // Validates one query as the reference's constructors assert (crates/dynamis-abi/src/query.rs:103-181,
 // crates/dynamis-world/src/query.rs:82-125): finite vectors, a non-zero direction, positive lengths,
 // a convex probe shape.
@@ -2386,11 +2404,20 @@ DYN_API dyn_status dyn_query(dyn_world* w, dyn_query_record* queries, uint32_t n
     DeviceWorld dw = d->dw;
     const uint32_t K = std::max(dw.k, 1u), E = dw.e_cap;
     cudaStream_t s = d->stream;
-    k_query_index_reset<<<1, 32, 0, s>>>(dw);
+    if (!d->query_entries) {
+        DYN_CUDA(cudaStreamSynchronize(s));
+        DYN_CUDA(cudaMalloc(&d->query_entries, 2 * (size_t)E * sizeof(float4)));
+        DYN_CUDA(cudaMalloc(&d->query_words, (64 + CTL_COUNT) * sizeof(uint32_t)));
+    }
+    // the query's grid in its own entries, counters and control words (every collider in one run)
+    dw.entries = d->query_entries;
+    dw.counters = d->query_words;
+    dw.ctl = d->query_words + 64;
+    DYN_CUDA(cudaMemsetAsync(d->query_words, 0, (64 + CTL_COUNT) * sizeof(uint32_t), s));
     k_aabb<<<blocks_for(d, K, 128), 128, 0, s>>>(dw, p);
-    k_entry_count<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    k_entry_count<false><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, K, dw.ctl + CTL_ENTRIES);
-    k_entry_emit<<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    k_entry_emit<false><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
     k_cell_clear<<<blocks_for(d, 1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
     k_cell_insert<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);

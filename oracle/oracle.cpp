@@ -245,6 +245,12 @@ struct OracleWorld {
     std::vector<dyn_constraint_runtime_record> joint_runtime;
     std::vector<uint32_t> plan_rows, plan_layers, plan_components;
     std::vector<uint32_t> body_world;  // sub-world of every row (empty: one world)
+    // the kept grid runs (grid_resting_*.wgsl, immovable_entries.wgsl): the run whose entries each
+    // collider's slots hold (0 none, 1 immovable, 2 resting), the box they were emitted with, and the
+    // base cell size both kept runs were emitted at
+    std::vector<uint32_t> held_run;
+    std::vector<Aabb> held_box;
+    uint32_t held_base = 0;
     // frozen contacts (freeze_contacts.wgsl): pairs of bodies both at rest when a step ended, by
     // body id and generation with their colliders, kept across steps in the order they were frozen
     struct Frozen {
@@ -437,13 +443,31 @@ float grid_base_cell(const OracleWorld& w) {
 
 // immovable_entries.wgsl:8-29, collider_entries.wgsl:9-35, collider_emit.wgsl:6-63, then the
 // entry sort (broadphase/src/passes.rs:76-90: 4 digit passes over the cell key, payload = slot).
+//
+// The entries fall in three runs: awake movable colliders', emitted every step; immovable colliders'
+// and resting (movable, asleep) colliders', which the library keeps sorted across steps and emits
+// again only when a member joined or left, a member's box changed, or the grid resolution moved.
+// The entry list is the same either way; what the runs change are the counters: ENTRIES and
+// GRID_LEVELS count the awake run, RESTING_ENTRIES / RESTING_LEVELS and IMMOVABLE_ENTRIES /
+// IMMOVABLE_LEVELS the kept runs, and IMMOVABLE_EMITTED, RESTING_REBUILD and RESTING_SORT what this
+// step emitted again (grid_resting_gate.wgsl, grid_resting_commit.wgsl).
 void emit_entries(OracleWorld& w) {
     float base = grid_base_cell(w);
     w.counters[DYN_COUNTER_IMMOVABLE_LEVELS] = 0;
     w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES] = 0;
+    w.counters[DYN_COUNTER_RESTING_LEVELS] = 0;
+    w.counters[DYN_COUNTER_RESTING_ENTRIES] = 0;
     std::vector<uint32_t> keys, order;
     w.entries.clear();
     uint32_t k = (uint32_t)w.colliders.size();
+    if (w.held_run.size() != k) {
+        w.held_run.assign(k, 0u);
+        w.held_box.assign(k, Aabb{});
+    }
+    constexpr uint32_t kAwake = 0, kImmovable = 1, kResting = 2, kNone = 3;
+    std::vector<uint32_t> run_of(k, kNone);
+    uint32_t stale = 0;
+    auto bits_equal = [](const Aabb& a, const Aabb& b) { return std::memcmp(&a, &b, sizeof(Aabb)) == 0; };
     // slots in collider order (the reference takes them from an atomic counter, so any order is
     // one of its possible layouts; the sorted keys do not depend on it).
     {
@@ -455,11 +479,12 @@ void emit_entries(OracleWorld& w) {
             bool awake = w.body_activity[owner] != 0u || w.wake_flags[owner] != 0u;
             const Aabb& box = w.aabbs[i];
             uint32_t level = shape_levels(box, base);
-            if (!moves) {
-                w.counters[DYN_COUNTER_IMMOVABLE_LEVELS] |= 1u << level;
-            } else {
-                w.counters[DYN_COUNTER_GRID_LEVELS] |= 1u << level;
-            }
+            const uint32_t run = !moves ? kImmovable : (awake ? kAwake : kResting);
+            run_of[i] = run;
+            uint32_t level_counter = run == kAwake ? DYN_COUNTER_GRID_LEVELS
+                                     : run == kResting ? DYN_COUNTER_RESTING_LEVELS : DYN_COUNTER_IMMOVABLE_LEVELS;
+            w.counters[level_counter] |= 1u << level;
+            if (run != kAwake && !(w.held_run[i] == run && bits_equal(w.held_box[i], box))) stale |= 1u << run;
             GridCells cells = grid_cells(box, level_cell_size(level, base));
             uint32_t count = grid_cell_count(cells);
             uint32_t emitted = std::min(count, DYN_MAX_CELLS_PER_COLLIDER);
@@ -476,15 +501,32 @@ void emit_entries(OracleWorld& w) {
                 w.entries.push_back(Entry{box, owner, info});
                 keys.push_back(cell_key_in(level, coord, w.world_of(owner)));
                 order.push_back(slot);
-                if (!moves) {
-                    w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES] += 1;
-                    w.counters[DYN_COUNTER_IMMOVABLE_EMITTED] += 1;
-                } else {
-                    w.counters[DYN_COUNTER_ENTRIES] += 1;
-                }
+                w.counters[run == kAwake ? DYN_COUNTER_ENTRIES
+                           : run == kResting ? DYN_COUNTER_RESTING_ENTRIES : DYN_COUNTER_IMMOVABLE_ENTRIES] += 1;
             }
         }
     }
+    // a collider that left a kept run makes it stale; so does a new grid resolution
+    for (uint32_t i = 0; i < k; ++i) {
+        if (w.held_run[i] != kAwake && w.held_run[i] != run_of[i]) stale |= 1u << w.held_run[i];
+    }
+    uint32_t base_bits;
+    std::memcpy(&base_bits, &base, 4);
+    if (base_bits != w.held_base) stale |= (1u << kImmovable) | (1u << kResting);
+    w.held_base = base_bits;
+    for (uint32_t i = 0; i < k; ++i) {
+        const uint32_t run = run_of[i];
+        if (run == kAwake || run == kNone) {
+            w.held_run[i] = kAwake;
+        } else if ((stale >> run) & 1u) {
+            w.held_run[i] = run;
+            w.held_box[i] = w.aabbs[i];
+        }
+    }
+    const bool immovable = (stale >> kImmovable) & 1u, resting = (stale >> kResting) & 1u;
+    w.counters[DYN_COUNTER_IMMOVABLE_EMITTED] = immovable ? w.counters[DYN_COUNTER_IMMOVABLE_ENTRIES] : 0u;
+    w.counters[DYN_COUNTER_RESTING_REBUILD] = resting ? 1u : 0u;
+    w.counters[DYN_COUNTER_RESTING_SORT] = resting ? w.counters[DYN_COUNTER_RESTING_ENTRIES] : 0u;
     std::vector<uint32_t> zero(keys.size(), 0);
     radix_sort_pairs(keys, zero, &order, 4, 0);
     w.entry_keys = keys;
@@ -2114,6 +2156,8 @@ void orc_queue_edits(OracleWorld* w, const uint32_t* rows, const dyn_body_edit_r
 
 void orc_set_body_worlds(OracleWorld* w, const uint32_t* rows, uint32_t n) {
     w->body_world.assign(rows, rows + n);
+    w->held_run.clear();  // the library uploads the scene again, which keeps no grid run
+    w->held_base = 0;
 }
 
 uint32_t orc_constraints(const OracleWorld* w, dyn_constraint_runtime_record* out) {
@@ -2306,7 +2350,8 @@ Aabb query_world_box(const OracleWorld& w, const dyn_query_record& q) {
 std::vector<uint32_t> query_candidates(const OracleWorld& grid, const Aabb& box, bool* spilled) {
     std::vector<uint32_t> out;
     const float base = grid_base_cell(grid);
-    uint32_t occupied = grid.counters[DYN_COUNTER_GRID_LEVELS] | grid.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
+    uint32_t occupied = grid.counters[DYN_COUNTER_GRID_LEVELS] | grid.counters[DYN_COUNTER_RESTING_LEVELS] |
+                        grid.counters[DYN_COUNTER_IMMOVABLE_LEVELS];
     const std::vector<uint32_t>& keys = grid.entry_keys;
     while (occupied != 0u) {
         const uint32_t level = (uint32_t)__builtin_ctz(occupied);
@@ -2349,9 +2394,10 @@ std::vector<uint32_t> query_candidates(const OracleWorld& grid, const Aabb& box,
 void orc_query(const OracleWorld* cw, dyn_query_record* queries, uint32_t n, dyn_query_hit_record* hits) {
     const OracleWorld& w = *cw;
     OracleWorld grid = w;
-    for (uint32_t c : {DYN_COUNTER_GRID_LEVELS, DYN_COUNTER_IMMOVABLE_LEVELS, DYN_COUNTER_GRID_SCALE, DYN_COUNTER_GRID_EXTENT,
-                       DYN_COUNTER_ENTRIES, DYN_COUNTER_IMMOVABLE_ENTRIES, DYN_COUNTER_IMMOVABLE_EMITTED,
-                       DYN_COUNTER_COARSE_ACTIVE, DYN_COUNTER_ENTRY_FAULTS})
+    for (uint32_t c : {DYN_COUNTER_GRID_LEVELS, DYN_COUNTER_IMMOVABLE_LEVELS, DYN_COUNTER_RESTING_LEVELS,
+                       DYN_COUNTER_GRID_SCALE, DYN_COUNTER_GRID_EXTENT, DYN_COUNTER_ENTRIES, DYN_COUNTER_IMMOVABLE_ENTRIES,
+                       DYN_COUNTER_RESTING_ENTRIES, DYN_COUNTER_IMMOVABLE_EMITTED, DYN_COUNTER_COARSE_ACTIVE,
+                       DYN_COUNTER_ENTRY_FAULTS})
         grid.counters[c] = 0u;
     grid.body_activity.resize(grid.states.size(), 0u);
     grid.wake_flags.resize(grid.states.size(), 0u);

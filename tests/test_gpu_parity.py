@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 RTOL, ATOL = 1e-5, 1e-6
 DT = 1.0 / 60.0
-EXACT_COUNTERS = ["ENTRIES", "IMMOVABLE_ENTRIES", "PAIRS", "GRID_LEVELS", "IMMOVABLE_LEVELS", "CONTACTS",
+EXACT_COUNTERS = ["ENTRIES", "IMMOVABLE_ENTRIES", "RESTING_ENTRIES", "RESTING_LEVELS", "PAIRS", "GRID_LEVELS", "IMMOVABLE_LEVELS", "CONTACTS",
                   "ISLANDS", "LIVE", "SOLVER_ROWS", "BLOCKS", "SLEPT", "WOKE", "ACTIVE", "COARSE_ACTIVE",
                   "GRID_SCALE", "GRID_EXTENT", "REFUSED_PAIRS", "REFUSED_CONTACTS", "ENTRY_FAULTS", "ARCHIVED"]
 
