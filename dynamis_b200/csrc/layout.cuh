@@ -187,6 +187,7 @@ struct DeviceWorld {
     uint32_t* run_val;     // [3e] the runs' entry slots
     uint32_t* held;        // [HELD_COUNT]
     uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
+    uint2* erun;        // [e] per sorted entry: the first sorted entry of its cell run, the run's length
     uint32_t cell_bits;
     uint32_t* spill;  // host-mapped: [0] unused, [1] pairs attempted, [2] pairs refused (left by a refusing step),
                       // [3] contacts staged (the largest since the host looked)

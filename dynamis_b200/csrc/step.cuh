@@ -596,6 +596,10 @@ __global__ void k_cell_insert(DeviceWorld w) {
     GRID_STRIDE(i, live) {
         uint32_t key = w.ekey[i];
         if (i > 0u && w.ekey[i - 1u] == key) continue;
+        // the run's extent for every member, so the pair kernels walk a run without testing keys
+        uint32_t end = i + 1u;
+        while (end < live && w.ekey[end] == key) ++end;
+        for (uint32_t t = i; t < end; ++t) w.erun[t] = make_uint2(i, end - i);
         uint32_t slot = cell_slot(key, bits);
         bool placed = false;
         for (uint32_t probe = 0; probe < kCellProbeLimit; ++probe) {
@@ -636,6 +640,8 @@ __device__ __forceinline__ uint32_t cell_find(const DeviceWorld& w, uint32_t liv
 // levels whose rank among the occupied levels is y, y + gridDim.y, ... (the walk of one collider is
 // a chain of dependent lookups; splitting it by level shortens the chain a thread waits through).
 constexpr uint32_t kCoarseLevelSlices = 4u;
+constexpr uint32_t kRunBatch = 4u;            // entries of a cell run loaded together by the pair kernels
+constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
 __global__ void __launch_bounds__(128) k_pairs_coarse(DeviceWorld w) {
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
     const float grid = base_cell(w);
@@ -676,15 +682,28 @@ __global__ void __launch_bounds__(128) k_pairs_coarse(DeviceWorld w) {
                         I3 cell = I3{x, y, z};
                         uint32_t key = cell_key_in(link, cell, world);
                         uint32_t j = cell_find(w, live, bits, overflow, key);
-                        for (; j < live && __ldg(w.ekey + j) == key; ++j) {
-                            uint32_t other = w.eval[j];
-                            if (other == node) continue;
-                            GEntry o = load_entry(w, other);
-                            if (!awake && !entry_awake(w, o)) continue;
-                            if (!overlaps(e, o)) continue;
-                            if (!same_cell(entry_cell(o, cs), cell)) continue;
-                            if (!overlap_cell_is(e, o, cs, cell)) continue;
-                            emit_pair(w, e, o, false);
+                        if (j >= live) continue;
+                        const uint32_t end = j + __ldg(&w.erun[j].y);
+                        // the run's entries four at a time: their loads are independent, so they
+                        // are all in flight before the first test
+                        for (; j < end; j += kRunBatch) {
+                            uint32_t others[kRunBatch];
+                            GEntry o[kRunBatch];
+#pragma unroll
+                            for (uint32_t u = 0; u < kRunBatch; ++u) others[u] = j + u < end ? __ldg(w.eval + j + u) : node;
+#pragma unroll
+                            for (uint32_t u = 0; u < kRunBatch; ++u) {
+                                if (others[u] != node) o[u] = load_entry(w, others[u]);
+                            }
+#pragma unroll
+                            for (uint32_t u = 0; u < kRunBatch; ++u) {
+                                if (others[u] == node) continue;
+                                if (!awake && !entry_awake(w, o[u])) continue;
+                                if (!overlaps(e, o[u])) continue;
+                                if (!same_cell(entry_cell(o[u], cs), cell)) continue;
+                                if (!overlap_cell_is(e, o[u], cs, cell)) continue;
+                                emit_pair(w, e, o[u], false);
+                            }
                         }
                     }
         }
@@ -702,18 +721,26 @@ __global__ void k_pairs_cell(DeviceWorld w) {
         uint32_t level = w.c_level[e.info & DYN_ENTRY_INDEX_MASK];
         float cs = level_size(level, grid);
         I3 cell = entry_cell(e, cs);
-        uint32_t key = __ldg(w.ekey + index);
-        uint32_t j = index;
-        while (j > 0u && __ldg(w.ekey + j - 1u) == key) --j;
-        for (; j < live && __ldg(w.ekey + j) == key; ++j) {
-            if (j == index) continue;
-            uint32_t other = w.eval[j];
-            GEntry o = load_entry(w, other);
-            if (j < index && entry_awake(w, o)) continue;
-            if (!overlaps(e, o)) continue;
-            if (!same_cell(entry_cell(o, cs), cell)) continue;
-            if (!overlap_cell_is(e, o, cs, cell)) continue;
-            emit_pair(w, e, o, node == other);
+        const uint2 run = __ldg(&w.erun[index]);
+        const uint32_t end = run.x + run.y;
+        for (uint32_t j = run.x; j < end; j += kRunBatch) {
+            uint32_t others[kRunBatch];
+            GEntry o[kRunBatch];
+#pragma unroll
+            for (uint32_t u = 0; u < kRunBatch; ++u) others[u] = (j + u < end && j + u != index) ? __ldg(w.eval + j + u) : kNoEntry;
+#pragma unroll
+            for (uint32_t u = 0; u < kRunBatch; ++u) {
+                if (others[u] != kNoEntry) o[u] = load_entry(w, others[u]);
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kRunBatch; ++u) {
+                if (others[u] == kNoEntry) continue;
+                if (j + u < index && entry_awake(w, o[u])) continue;
+                if (!overlaps(e, o[u])) continue;
+                if (!same_cell(entry_cell(o[u], cs), cell)) continue;
+                if (!overlap_cell_is(e, o[u], cs, cell)) continue;
+                emit_pair(w, e, o[u], node == others[u]);
+            }
         }
     }
 }

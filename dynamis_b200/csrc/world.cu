@@ -328,6 +328,7 @@ dyn_status ensure_device(dyn_world* w) {
         dw.cell_bits = 10u;
         while (dw.cell_bits < 31u && ((size_t)1 << dw.cell_bits) < 2 * (size_t)E) ++dw.cell_bits;
         A(dw.cell_table, (size_t)1 << dw.cell_bits);
+        A(dw.erun, E);
         A(dw.pmaj, P);
         A(dw.pmin, P);
         // the staging set and its sort keys hold every contact the narrowphase finds: one per pair at most
