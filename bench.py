@@ -202,6 +202,47 @@ def query_benchmark(world, batch: int = 16384, repeats: int = 3, seed: int = 9) 
     return out
 
 
+def resting_benchmark(device: int, side: int = 512, steps: int = 50) -> dict:
+    """A resting world: the 262,144 boxes of scenes.resting_field stepped until every body sleeps,
+    then `steps` steps timed with CUDA events on the world's stream, with the grid counters of the
+    last one (a resting world emits and sorts no grid entry: its entries stay in the kept resting
+    run)."""
+    import torch
+
+    from dynamis_b200 import World, records as R, scenes
+
+    dt = 1.0 / 60.0
+    world = World(device=device)
+    scenes.resting_field(side).build(world)
+    stream = torch.cuda.Stream(device=device)
+    world.set_stream(stream.cuda_stream)
+    slept = None
+    for i in range(600):
+        world.step(dt)
+        if i % 20 == 19:
+            world.wait()
+            if world.measured()[R.COUNTER["ACTIVE"]] == 0:
+                slept = i + 1
+                break
+    for _ in range(3):
+        world.step(dt)
+    world.wait()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        world.step(dt)
+    end.record(stream)
+    end.synchronize()
+    ms = start.elapsed_time(end) / steps
+    m = world.measured()
+    out = {"bodies": world.sizes()["bodies"], "asleep_after_steps": slept, "ms_per_step": round(ms, 4),
+           "counters": {k: int(m[R.COUNTER[k]]) for k in ("ACTIVE", "ENTRIES", "RESTING_ENTRIES", "RESTING_REBUILD",
+                                                          "IMMOVABLE_EMITTED", "PAIRS")}}
+    world.close()
+    log(f"resting field: {out}")
+    return out
+
+
 def guarded_run(args, dt: float, device: int) -> dict:
     """The same workload with the row-mass guard on (dyn_set_solver_guard): the same setup, warm-up
     and timed steps, its setup bounds, its device time per step."""
@@ -377,6 +418,8 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     if extras and not args.no_queries:
         result["queries"] = query_benchmark(world)
         log(f"queries {result['queries']}")
+    if extras and not args.no_resting:
+        result["resting"] = resting_benchmark(local_rank)
     if extras and not args.no_batch:
         result["batch"] = batch_benchmark(args, local_rank)
     if extras and not args.no_guarded:
@@ -634,6 +677,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-towers measurement")
     ap.add_argument("--no-guarded", action="store_true", help="skip the run with the row-mass guard")
     ap.add_argument("--no-queries", action="store_true", help="skip the scene-query measurement")
+    ap.add_argument("--no-resting", action="store_true", help="skip the resting-world measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
     ap.add_argument("--tuning-cache", default=None, help="JSON file of per-workload launch shapes to reuse and extend")

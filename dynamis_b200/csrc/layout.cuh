@@ -186,6 +186,7 @@ struct DeviceWorld {
     uint32_t* run_key;     // [3e] the runs' cell keys, run r at [r * e_cap], sorted
     uint32_t* run_val;     // [3e] the runs' entry slots
     uint32_t* held;        // [HELD_COUNT]
+    uint32_t* init_pos;    // [e] merged places of the entries that can start a same-cell pair: the awake run's, then the immovable run's
     uint2* cell_table;  // [1 << cell_bits]: (cell key, first sorted entry) per occupied cell
     uint2* erun;        // [e] per sorted entry: the first sorted entry of its cell run, the run's length
     uint32_t cell_bits;

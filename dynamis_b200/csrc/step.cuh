@@ -514,6 +514,7 @@ __global__ void k_entry_merge(DeviceWorld w) {
             w.ekey[pos] = key;
             w.eval[pos] = val;
         }
+        if (t < na + ni) w.init_pos[t] = pos;
     }
 }
 
@@ -710,10 +711,14 @@ __global__ void __launch_bounds__(128) k_pairs_coarse(DeviceWorld w) {
     }
 }
 
+// One thread per entry that can start a pair (an awake entry, or an immovable one, whose owner's
+// wake flag makes it awake): a resting entry is never awake, so it only answers.
 __global__ void k_pairs_cell(DeviceWorld w) {
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
+    const uint32_t starts = min(w.held[HELD_AWAKE] + w.held[HELD_IMMOVABLE], live);
     const float grid = base_cell(w);
-    GRID_STRIDE(index, live) {
+    GRID_STRIDE(t, starts) {
+        const uint32_t index = __ldg(w.init_pos + t);
         uint32_t node = w.eval[index];
         GEntry e = load_entry(w, node);
         if (((e.info & DYN_ENTRY_KIND_MASK) >> DYN_ENTRY_KIND_SHIFT) != DYN_ENTRY_KIND_COLLIDER) continue;

@@ -325,6 +325,7 @@ dyn_status ensure_device(dyn_world* w) {
         A(dw.run_key, 3 * (size_t)E);
         A(dw.run_val, 3 * (size_t)E);
         A(dw.held, HELD_COUNT);
+        A(dw.init_pos, E);
         dw.cell_bits = 10u;
         while (dw.cell_bits < 31u && ((size_t)1 << dw.cell_bits) < 2 * (size_t)E) ++dw.cell_bits;
         A(dw.cell_table, (size_t)1 << dw.cell_bits);

@@ -118,6 +118,24 @@ def falling_boxes(seed: int = 0, side: int = 10, spacing: float = 1.1) -> Scene:
     return Scene(bodies, colliders, [], f"falling_boxes_{n}")
 
 
+def resting_field(side: int = 512, spacing: float = 1.1) -> Scene:
+    """side x side unit cubes (half-extent 0.5 m, density 1000) standing on a static ground plane at
+    1.1 m spacing, none touching another: every box falls asleep within a second and the world then
+    rests (the kept grid runs' case)."""
+    n = side * side
+    i, k = np.meshgrid(np.arange(side), np.arange(side), indexing="ij")
+    pos = np.stack([(i.ravel() - (side - 1) / 2) * spacing, np.full(n, 0.5), (k.ravel() - (side - 1) / 2) * spacing],
+                   axis=1)
+    bodies = R.body_defaults(n)
+    bodies["position"] = pos.astype(np.float32)
+    bodies["density"] = 1000.0
+    colliders = R.collider_defaults(n)
+    colliders["shape"] = R.SHAPE_CUBOID
+    colliders["half_extents"] = 0.5
+    bodies, colliders = _ground(bodies, colliders, 0.0, 0.5, 0.0)
+    return Scene(bodies, colliders, [], f"resting_field_{n}")
+
+
 def mixed_pile(side: int = 64, seed: int = 1, spacing: float = 1.3) -> Scene:
     """side^3 bodies on a lattice at 1.3 m spacing with +-0.1 m jitter and uniform random
     orientations: 50% boxes (half-extents U[0.2, 0.6] per axis), 30% spheres (radius U[0.2, 0.5]),
