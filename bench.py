@@ -337,7 +337,7 @@ def run_ours(args, rank: int, world_size: int, local_rank: int):
     if dist:
         dist.barrier()
     m = world.measured()
-    counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
+    counts = {"K": world.sizes()["colliders"], "E": int(m[R.COUNTER["ENTRIES"]] + m[R.COUNTER["RESTING_ENTRIES"]] + m[R.COUNTER["IMMOVABLE_ENTRIES"]]),
               "P": int(m[R.COUNTER["PAIRS"]]), "C": int(m[R.COUNTER["CONTACTS"]]), "R": int(m[R.COUNTER["SOLVER_ROWS"]]),
               "L": int(m[R.COUNTER["LIVE"]]), "J": world.constraint_count(),
               "refused_pairs": int(m[R.COUNTER["REFUSED_PAIRS"]]),
