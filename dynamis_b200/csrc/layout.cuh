@@ -94,6 +94,8 @@ enum Held : uint32_t {
     HELD_SORT_IMMOVABLE = 7,  // per step: entries the immovable run's sort covers (0 when it is kept)
     HELD_SORT_RESTING = 8,
     HELD_SCRATCH = 9,      // a scan total nothing reads
+    HELD_LIST_KEPT = 10,   // per step: the merged list, cell table and run extents are the previous step's
+    HELD_LIST_CLEAN = 11,  // the merged list holds no awake entry and only the kept runs as they stand
     HELD_COUNT = 16
 };
 

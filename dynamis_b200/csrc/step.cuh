@@ -410,6 +410,11 @@ __global__ void k_grid_gate(DeviceWorld w) {
     w.counters[DYN_COUNTER_RESTING_REBUILD] = resting ? 1u : 0u;
     w.counters[DYN_COUNTER_RESTING_SORT] = resting ? nr : 0u;
     w.ctl[CTL_ENTRIES] = min(w.held[HELD_AWAKE] + ni + nr, w.e_cap);
+    // an empty awake run over kept runs that the last merge already listed alone: the merged list,
+    // its cell table and run extents stand as they are (a resting world merges nothing)
+    const bool empty = w.held[HELD_AWAKE] == 0u;
+    w.held[HELD_LIST_KEPT] = (empty && !immovable && !resting && w.held[HELD_LIST_CLEAN] != 0u) ? 1u : 0u;
+    w.held[HELD_LIST_CLEAN] = empty ? 1u : 0u;
 }
 
 // collider_emit.wgsl:31-63 for the colliders whose entries this launch writes, in collider order at
@@ -485,6 +490,7 @@ __device__ __forceinline__ uint32_t run_rank(const uint32_t* keys, const uint32_
 // order and the sort is stable), so an entry's place is its index in its run plus the entries of
 // the other runs before (key, slot): the list one sort of every entry would give.
 __global__ void k_entry_merge(DeviceWorld w) {
+    if (w.held[HELD_LIST_KEPT] != 0u) return;
     const uint32_t na = w.held[HELD_AWAKE], ni = w.held[HELD_IMMOVABLE], nr = w.held[HELD_RESTING];
     const uint32_t total = min(na + ni + nr, w.e_cap);
     const uint32_t* ka = w.run_key;
@@ -585,12 +591,14 @@ __device__ __forceinline__ uint32_t cell_table_bits(const DeviceWorld& w, uint32
 __device__ __forceinline__ uint32_t cell_slot(uint32_t key, uint32_t bits) { return (key * 0x9E3779B1u) >> (32u - bits); }
 
 __global__ void k_cell_clear(DeviceWorld w) {
+    if (w.held[HELD_LIST_KEPT] != 0u) return;
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
     const uint32_t slots = 1u << cell_table_bits(w, live);
     GRID_STRIDE(i, slots) w.cell_table[i] = make_uint2(kCellEmpty, 0u);
 }
 
 __global__ void k_cell_insert(DeviceWorld w) {
+    if (w.held[HELD_LIST_KEPT] != 0u) return;
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
     const uint32_t bits = cell_table_bits(w, live);
     const uint32_t mask = (1u << bits) - 1u;

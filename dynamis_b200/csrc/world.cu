@@ -2416,6 +2416,8 @@ DYN_API dyn_status dyn_query(dyn_world* w, dyn_query_record* queries, uint32_t n
     dw.counters = d->query_words;
     dw.ctl = d->query_words + 64;
     DYN_CUDA(cudaMemsetAsync(d->query_words, 0, (64 + CTL_COUNT) * sizeof(uint32_t), s));
+    // the query's grid takes the merged list, cell table and run extents: the next step lists again
+    DYN_CUDA(cudaMemsetAsync(d->dw.held + HELD_LIST_KEPT, 0, 2 * sizeof(uint32_t), s));
     k_aabb<<<blocks_for(d, K, 128), 128, 0, s>>>(dw, p);
     k_entry_count<false><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, K, dw.ctl + CTL_ENTRIES);
