@@ -649,7 +649,8 @@ __device__ __forceinline__ uint32_t cell_find(const DeviceWorld& w, uint32_t liv
 // levels whose rank among the occupied levels is y, y + gridDim.y, ... (the walk of one collider is
 // a chain of dependent lookups; splitting it by level shortens the chain a thread waits through).
 constexpr uint32_t kCoarseLevelSlices = 4u;
-constexpr uint32_t kRunBatch = 4u;            // entries of a cell run loaded together by the pair kernels
+constexpr uint32_t kRunBatch = 4u;            // entries of a cell run the coarse walk loads together
+constexpr uint32_t kCellBatch = 2u;           // the same for the same-cell scan, whose runs are short
 constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
 __global__ void __launch_bounds__(128) k_pairs_coarse(DeviceWorld w) {
     const uint32_t live = min(w.ctl[CTL_ENTRIES], w.e_cap);
@@ -736,17 +737,17 @@ __global__ void k_pairs_cell(DeviceWorld w) {
         I3 cell = entry_cell(e, cs);
         const uint2 run = __ldg(&w.erun[index]);
         const uint32_t end = run.x + run.y;
-        for (uint32_t j = run.x; j < end; j += kRunBatch) {
-            uint32_t others[kRunBatch];
-            GEntry o[kRunBatch];
+        for (uint32_t j = run.x; j < end; j += kCellBatch) {
+            uint32_t others[kCellBatch];
+            GEntry o[kCellBatch];
 #pragma unroll
-            for (uint32_t u = 0; u < kRunBatch; ++u) others[u] = (j + u < end && j + u != index) ? __ldg(w.eval + j + u) : kNoEntry;
+            for (uint32_t u = 0; u < kCellBatch; ++u) others[u] = (j + u < end && j + u != index) ? __ldg(w.eval + j + u) : kNoEntry;
 #pragma unroll
-            for (uint32_t u = 0; u < kRunBatch; ++u) {
+            for (uint32_t u = 0; u < kCellBatch; ++u) {
                 if (others[u] != kNoEntry) o[u] = load_entry(w, others[u]);
             }
 #pragma unroll
-            for (uint32_t u = 0; u < kRunBatch; ++u) {
+            for (uint32_t u = 0; u < kCellBatch; ++u) {
                 if (others[u] == kNoEntry) continue;
                 if (j + u < index && entry_awake(w, o[u])) continue;
                 if (!overlaps(e, o[u])) continue;
