@@ -391,9 +391,7 @@ __global__ void k_entry_count(DeviceWorld w) {
 // again (a stale member, or a grid resolution other than the one they were emitted at), the sizes
 // and counts the scans, sorts and merge read, and the counters of what was derived. A kept run has
 // exactly the entries its members count now, rebuilt or not.
-// With `conditional`, the gate also opens the graph's conditional node that holds the kept runs'
-// derivation, only when one of them is stale.
-__global__ void k_grid_gate(DeviceWorld w, cudaGraphConditionalHandle kept_node, uint32_t conditional) {
+__global__ void k_grid_gate(DeviceWorld w) {
     if (threadIdx.x != 0u) return;
     uint32_t stale = w.held[HELD_STALE];
     const uint32_t base = __float_as_uint(base_cell(w));
@@ -417,18 +415,14 @@ __global__ void k_grid_gate(DeviceWorld w, cudaGraphConditionalHandle kept_node,
     const bool empty = w.held[HELD_AWAKE] == 0u;
     w.held[HELD_LIST_KEPT] = (empty && !immovable && !resting && w.held[HELD_LIST_CLEAN] != 0u) ? 1u : 0u;
     w.held[HELD_LIST_CLEAN] = empty ? 1u : 0u;
-    if (conditional) cudaGraphSetConditional(kept_node, (immovable || resting) ? 1u : 0u);
 }
 
 // collider_emit.wgsl:31-63 for the colliders whose entries this launch writes, in collider order at
-// their scanned key positions. A step writes the awake run (kEmitAwake) and every kept run the gate
-// marked stale (kEmitKept), each entry into its collider's own slots (8 * collider + ordinal), and
-// records which kept run a collider's slots now hold. A query writes every collider's entries
-// compactly (kEmitQuery).
-constexpr int kEmitQuery = 0, kEmitAwake = 1, kEmitKept = 2;
-template <int kMode>
+// their scanned key positions. A step writes the awake run and every kept run the gate marked
+// stale, each entry into its collider's own slots (8 * collider + ordinal), and records which kept
+// run a collider's slots now hold. A query writes every collider's entries compactly.
+template <bool kStep>
 __global__ void k_entry_emit(DeviceWorld w) {
-    constexpr bool kStep = kMode != kEmitQuery;
     float base = base_cell(w);
     const uint32_t stale = kStep ? w.held[HELD_STALE] : 0u;
     GRID_STRIDE(i, w.k) {
@@ -438,10 +432,9 @@ __global__ void k_entry_emit(DeviceWorld w) {
         if (kStep) {
             const uint32_t run = w.c_run[i];
             if (run == RUN_NONE) {
-                if (kMode == kEmitAwake) w.c_held[i] = RUN_AWAKE;
+                w.c_held[i] = RUN_AWAKE;
                 continue;
             }
-            if ((run == RUN_AWAKE) != (kMode == kEmitAwake)) continue;  // the other launch's run
             if (run != RUN_AWAKE && ((stale >> run) & 1u) == 0u) continue;  // kept: its slots hold these entries
             w.c_held[i] = run;
             emitted = w.run_count[run * w.k + i];

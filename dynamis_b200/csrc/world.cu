@@ -86,7 +86,6 @@ struct DeviceState {
     // a second stream the captured step forks onto for kernels independent of the main line
     cudaStream_t side_stream = nullptr;
     cudaStream_t side_stream2 = nullptr;
-    cudaStream_t kept_stream = nullptr;  // captures the kept grid runs' derivation into its conditional node
     cudaEvent_t fork_events[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t join_events[4] = {nullptr, nullptr, nullptr, nullptr};
     // the last kStepsInFlight steps' completion events: dyn_step waits for the oldest before it
@@ -148,7 +147,6 @@ struct DeviceState {
     bool stepped = false;
     bool uploaded = false;  // the current scene's records are on the device
     uint32_t graph_kernels = 0;  // kernel nodes in one step's graph
-    uint32_t kept_kernels = 0;   // kernel nodes in its conditional kept-run derivation (run on the steps that derive)
     uint64_t scene_epoch = 0;    // scene uploads so far (a snapshot belongs to one scene)
     uint32_t sms = 148;          // multiprocessors of the device (read when the device state is made)
     dyn_launch_config launch{16u, 128u, 6u, 8u};  // dyn_set_launch_config / dyn_autotune
@@ -255,7 +253,6 @@ dyn_status ensure_device(dyn_world* w) {
         DYN_CUDA(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream, cudaStreamNonBlocking));
         DYN_CUDA(cudaStreamCreateWithFlags(&d->side_stream2, cudaStreamNonBlocking));
-        DYN_CUDA(cudaStreamCreateWithFlags(&d->kept_stream, cudaStreamNonBlocking));
         for (uint32_t i = 0; i < 4; ++i) {
             DYN_CUDA(cudaEventCreateWithFlags(&d->fork_events[i], cudaEventDisableTiming));
             DYN_CUDA(cudaEventCreateWithFlags(&d->join_events[i], cudaEventDisableTiming));
@@ -700,79 +697,6 @@ void record_scan(DeviceState* d, cudaStream_t s, const uint32_t* in, uint32_t* o
                                                     d->dw.ctl + CTL_STATUS, kLookbackSpinLimit);
 }
 
-// The conditional node of the kept grid runs' derivation, added to the graph `s` is capturing.
-struct KeptBody {
-    bool open = false;
-    cudaGraphConditionalHandle handle = 0;
-    cudaGraph_t graph = nullptr;  // the node's body graph
-    cudaGraph_t parent = nullptr;
-    cudaStream_t parent_stream = nullptr;
-};
-// Creates the handle the gate sets (reset to 0 at every launch of the graph). On any error the
-// derivation is captured inline instead, with the same results.
-KeptBody open_kept_body(DeviceState* d, cudaStream_t s) {
-    KeptBody k;
-    cudaStreamCaptureStatus status;
-    cudaGraph_t graph = nullptr;
-    if (cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, nullptr, nullptr) != cudaSuccess ||
-        status != cudaStreamCaptureStatusActive || !graph) {
-        cudaGetLastError();
-        return k;
-    }
-    if (cudaGraphConditionalHandleCreate(&k.handle, graph, 0u, cudaGraphCondAssignDefault) != cudaSuccess) {
-        cudaGetLastError();
-        return k;
-    }
-    k.parent = graph;
-    k.parent_stream = s;
-    k.open = true;
-    (void)d;
-    return k;
-}
-// Adds the IF node after what `s` captured so far (the gate), makes it what `s` continues from,
-// and starts capturing its body on the world's kept stream, which the caller records into.
-cudaStream_t begin_kept_body(DeviceState* d, cudaStream_t s, KeptBody* k) {
-    cudaStreamCaptureStatus status;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphNodeParams params = {};
-    params.type = cudaGraphNodeTypeConditional;
-    params.conditional.handle = k->handle;
-    params.conditional.type = cudaGraphCondTypeIf;
-    params.conditional.size = 1;
-    cudaGraphNode_t node = nullptr;
-    if (cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps) != cudaSuccess ||
-        cudaGraphAddNode(&node, graph, deps, ndeps, &params) != cudaSuccess ||
-        cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess ||
-        cudaStreamBeginCaptureToGraph(d->kept_stream, params.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                      cudaStreamCaptureModeRelaxed) != cudaSuccess) {
-        // the node could not be placed: the gate's handle is never read, record inline
-        cudaGetLastError();
-        k->open = false;
-        return s;
-    }
-    k->graph = params.conditional.phGraph_out[0];
-    return d->kept_stream;
-}
-void end_kept_body(DeviceState* d, KeptBody* k) {
-    cudaGraph_t body = nullptr;
-    if (cudaStreamEndCapture(d->kept_stream, &body) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
-    size_t nodes = 0;
-    cudaGraphGetNodes(k->graph, nullptr, &nodes);
-    std::vector<cudaGraphNode_t> list(nodes);
-    cudaGraphGetNodes(k->graph, list.data(), &nodes);
-    uint32_t kernels = 0;
-    for (cudaGraphNode_t node : list) {
-        cudaGraphNodeType type;
-        if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernels;
-    }
-    d->kept_kernels = kernels;
-}
-
 struct Marker {
     DeviceState* d;
     cudaStream_t s;
@@ -837,26 +761,19 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     // stale, their scans and sorts otherwise covering nothing
     k_entry_count<true><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_scan(d, s, dw.run_count, dw.run_offset, nullptr, dw.k, K, dw.held + HELD_AWAKE);
-    // The kept runs' derivation (scans, emission, sorts; each covering nothing for a run that is not
-    // stale) sits in a conditional graph node that k_grid_gate opens only when a kept run is stale,
-    // so a step that keeps both runs launches none of it. Eager steps launch it inline.
-    KeptBody kept = !timed ? open_kept_body(d, s) : KeptBody{};
-    k_grid_gate<<<1, 32, 0, s>>>(dw, kept.handle, kept.open ? 1u : 0u);
-    cudaStream_t ks = kept.open ? begin_kept_body(d, s, &kept) : s;
-    record_scan(d, ks, dw.run_count + dw.k, dw.run_offset + dw.k, dw.held + HELD_SCAN_IMMOVABLE, 0, K,
+    k_grid_gate<<<1, 32, 0, s>>>(dw);
+    record_scan(d, s, dw.run_count + dw.k, dw.run_offset + dw.k, dw.held + HELD_SCAN_IMMOVABLE, 0, K,
                 dw.held + HELD_SCRATCH);
-    record_scan(d, ks, dw.run_count + 2 * (size_t)dw.k, dw.run_offset + 2 * (size_t)dw.k, dw.held + HELD_SCAN_RESTING, 0, K,
+    record_scan(d, s, dw.run_count + 2 * (size_t)dw.k, dw.run_offset + 2 * (size_t)dw.k, dw.held + HELD_SCAN_RESTING, 0, K,
                 dw.held + HELD_SCRATCH);
-    k_entry_emit<kEmitKept><<<blocks_for(d, K, 256), 256, 0, ks>>>(dw);
-    for (uint32_t run = RUN_IMMOVABLE; run <= RUN_RESTING; ++run) {
-        const uint32_t* count = dw.held + (run == RUN_IMMOVABLE ? HELD_SORT_IMMOVABLE : HELD_SORT_RESTING);
-        record_sort(d, ks, dw.run_key + (size_t)run * E, nullptr, dw.run_val + (size_t)run * E, dw.ekey_alt, nullptr,
+    k_entry_emit<true><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    mark(ST_ENTRY_SORT);
+    for (uint32_t run = 0; run < 3; ++run) {
+        const uint32_t* count = dw.held + (run == RUN_AWAKE ? HELD_AWAKE
+                                           : run == RUN_IMMOVABLE ? HELD_SORT_IMMOVABLE : HELD_SORT_RESTING);
+        record_sort(d, s, dw.run_key + (size_t)run * E, nullptr, dw.run_val + (size_t)run * E, dw.ekey_alt, nullptr,
                     dw.eval_alt, count, 0, E, 4, 0);
     }
-    if (kept.open) end_kept_body(d, &kept);
-    k_entry_emit<kEmitAwake><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
-    mark(ST_ENTRY_SORT);
-    record_sort(d, s, dw.run_key, nullptr, dw.run_val, dw.ekey_alt, nullptr, dw.eval_alt, dw.held + HELD_AWAKE, 0, E, 4, 0);
     k_entry_merge<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);
     mark(ST_PAIRS);
     k_cell_clear<<<blocks_for(d, 1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
@@ -1236,7 +1153,6 @@ void destroy_device(dyn_world* w) {
     }
     if (d->side_stream) cudaStreamDestroy(d->side_stream);
     if (d->side_stream2) cudaStreamDestroy(d->side_stream2);
-    if (d->kept_stream) cudaStreamDestroy(d->kept_stream);
     if (d->own_stream) cudaStreamDestroy(d->own_stream);
     delete d;
     w->dev = nullptr;
@@ -2505,7 +2421,7 @@ DYN_API dyn_status dyn_query(dyn_world* w, dyn_query_record* queries, uint32_t n
     k_aabb<<<blocks_for(d, K, 128), 128, 0, s>>>(dw, p);
     k_entry_count<false><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_scan(d, s, dw.entry_count, dw.entry_offset, nullptr, dw.k, K, dw.ctl + CTL_ENTRIES);
-    k_entry_emit<kEmitQuery><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
+    k_entry_emit<false><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     record_sort(d, s, dw.ekey, nullptr, dw.eval, dw.ekey_alt, nullptr, dw.eval_alt, dw.ctl + CTL_ENTRIES, 0, E, 4, 0);
     k_cell_clear<<<blocks_for(d, 1u << dw.cell_bits, 256), 256, 0, s>>>(dw);
     k_cell_insert<<<blocks_for(d, E, 256), 256, 0, s>>>(dw);
