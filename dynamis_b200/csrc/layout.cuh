@@ -89,8 +89,6 @@ enum Held : uint32_t {
     HELD_IMMOVABLE = 2,    // entries in the kept immovable run
     HELD_RESTING = 3,      // entries in the kept resting run
     HELD_BASE = 4,         // bits of the base cell size the kept runs were emitted at
-    HELD_SCAN_IMMOVABLE = 5,  // per step: colliders the immovable run's scan covers (0 when it is kept)
-    HELD_SCAN_RESTING = 6,
     HELD_SORT_IMMOVABLE = 7,  // per step: entries the immovable run's sort covers (0 when it is kept)
     HELD_SORT_RESTING = 8,
     HELD_SCRATCH = 9,      // a scan total nothing reads
@@ -184,7 +182,7 @@ struct DeviceWorld {
     uint32_t* c_run;    // [k] per step: the GridRun a collider's entries belong to
     uint32_t* c_held;   // [k] the kept run whose entries the collider's slots hold (RUN_AWAKE: none)
     uint32_t* run_count;   // [3k] entries per collider and run this step emits (the scans' input)
-    uint32_t* run_offset;  // [3k] their exclusive scans
+    uint32_t* run_offset;  // [3k] their exclusive scan, the three runs' counts back to back
     uint32_t* run_key;     // [3e] the runs' cell keys, run r at [r * e_cap], sorted
     uint32_t* run_val;     // [3e] the runs' entry slots
     uint32_t* held;        // [HELD_COUNT]

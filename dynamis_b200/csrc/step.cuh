@@ -389,11 +389,12 @@ __global__ void k_entry_count(DeviceWorld w) {
 
 // grid_resting_gate.wgsl / grid_resting_commit.wgsl in one thread: which kept runs this step emits
 // again (a stale member, or a grid resolution other than the one they were emitted at), the sizes
-// and counts the scans, sorts and merge read, and the counters of what was derived. A kept run has
-// exactly the entries its members count now, rebuilt or not.
+// and counts the sorts and merge read, and the counters of what was derived. A kept run has exactly
+// the entries its members count now, rebuilt or not.
 __global__ void k_grid_gate(DeviceWorld w) {
     if (threadIdx.x != 0u) return;
     uint32_t stale = w.held[HELD_STALE];
+    w.held[HELD_AWAKE] = w.k ? w.run_offset[w.k - 1u] + w.run_count[w.k - 1u] : 0u;
     const uint32_t base = __float_as_uint(base_cell(w));
     if (base != w.held[HELD_BASE]) stale |= (1u << RUN_IMMOVABLE) | (1u << RUN_RESTING);
     const bool immovable = (stale >> RUN_IMMOVABLE) & 1u, resting = (stale >> RUN_RESTING) & 1u;
@@ -402,8 +403,6 @@ __global__ void k_grid_gate(DeviceWorld w) {
     w.held[HELD_BASE] = base;
     w.held[HELD_IMMOVABLE] = ni;
     w.held[HELD_RESTING] = nr;
-    w.held[HELD_SCAN_IMMOVABLE] = immovable ? w.k : 0u;
-    w.held[HELD_SCAN_RESTING] = resting ? w.k : 0u;
     w.held[HELD_SORT_IMMOVABLE] = immovable ? ni : 0u;
     w.held[HELD_SORT_RESTING] = resting ? nr : 0u;
     w.counters[DYN_COUNTER_IMMOVABLE_EMITTED] = immovable ? ni : 0u;
@@ -438,7 +437,7 @@ __global__ void k_entry_emit(DeviceWorld w) {
             if (run != RUN_AWAKE && ((stale >> run) & 1u) == 0u) continue;  // kept: its slots hold these entries
             w.c_held[i] = run;
             emitted = w.run_count[run * w.k + i];
-            first = w.run_offset[run * w.k + i];
+            first = w.run_offset[run * w.k + i] - (run != RUN_AWAKE ? w.run_offset[run * w.k] : 0u);
             keys = w.run_key + (size_t)run * w.e_cap;
             vals = w.run_val + (size_t)run * w.e_cap;
         } else {

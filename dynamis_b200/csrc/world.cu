@@ -760,12 +760,10 @@ void record_step(dyn_world* w, cudaStream_t s, uint32_t parity, bool timed, cons
     // the awake run every step; the kept runs (immovable, resting) only when the gate finds them
     // stale, their scans and sorts otherwise covering nothing
     k_entry_count<true><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
-    record_scan(d, s, dw.run_count, dw.run_offset, nullptr, dw.k, K, dw.held + HELD_AWAKE);
+    // one scan over the three runs' counts back to back; each run's key positions are its offsets
+    // less the offset at the start of its third
+    record_scan(d, s, dw.run_count, dw.run_offset, nullptr, 3 * dw.k, 3 * K, dw.held + HELD_SCRATCH);
     k_grid_gate<<<1, 32, 0, s>>>(dw);
-    record_scan(d, s, dw.run_count + dw.k, dw.run_offset + dw.k, dw.held + HELD_SCAN_IMMOVABLE, 0, K,
-                dw.held + HELD_SCRATCH);
-    record_scan(d, s, dw.run_count + 2 * (size_t)dw.k, dw.run_offset + 2 * (size_t)dw.k, dw.held + HELD_SCAN_RESTING, 0, K,
-                dw.held + HELD_SCRATCH);
     k_entry_emit<true><<<blocks_for(d, K, 256), 256, 0, s>>>(dw);
     mark(ST_ENTRY_SORT);
     for (uint32_t run = 0; run < 3; ++run) {
