@@ -81,3 +81,20 @@ def test_moving_a_static_body_derives_the_immovable_run():
     o.edit_bodies([int(ids[0])], R.body_edit(R.EDIT_PATCH, R.PATCH_POSITION, position=(0.0, -0.6, 0.0)))
     o.step(DT)
     assert counter(o, "IMMOVABLE_EMITTED") == counter(o, "IMMOVABLE_ENTRIES") > 0
+
+
+def test_the_resting_field_falls_asleep_into_one_kept_run():
+    # scenes.resting_field, the bench's resting world, at 8 x 8 boxes: no box touches another, so
+    # every box sleeps within a second and then sits in the resting run, which no step derives again
+    from dynamis_b200 import World, scenes
+
+    w = World()
+    scenes.resting_field(8).build(w)
+    o = O.oracle_from_world(w, DT)
+    assert settle_until_asleep(o, 120) < 120
+    o.step(DT)
+    assert counter(o, "PAIRS") == 0  # asleep against a static plane: no candidate pair
+    for _ in range(10):
+        o.step(DT)
+        assert counter(o, "ENTRIES") == 0 and counter(o, "RESTING_REBUILD") == 0
+    assert counter(o, "RESTING_ENTRIES") >= 64 and counter(o, "IMMOVABLE_EMITTED") == 0
